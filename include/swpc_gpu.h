@@ -1,0 +1,220 @@
+/*
+ * swpc_gpu.h -- C ABI of the B200 time-step library for OpenSWPC.
+ *
+ * The library replaces the hot routines of OpenSWPC's time loop
+ * (src/swpc_3d/main.f90:125-144, src/swpc_psv/main.f90:95-114,
+ * src/swpc_sh/main.f90:95-116).  In the reference those routines are
+ * argument-less Fortran module procedures acting on module-global arrays;
+ * here every routine takes an opaque context that owns the device copies of
+ * those arrays.  A Fortran caller keeps one `type(c_ptr)` per run and binds
+ * each entry point with ISO_C_BINDING.
+ *
+ * Conventions
+ *   - every function returns an int status: 0 = OK, otherwise an
+ *     SWPC_ERR_* code; swpc_last_error() gives the message.  The Fortran
+ *     shim maps a nonzero status to `call assert(.false.)`, the reference's
+ *     error path (src/shared/m_debug.h:7, src/shared/m_pdebug.f90:223-240).
+ *   - arrays cross the boundary in the reference's Fortran layout:
+ *     3D fields (kbeg_m:kend_m, ibeg_m:iend_m, jbeg_m:jend_m), k fastest,
+ *     with the memory box of m_global.f90:297-302 (lower bound 1-3, upper
+ *     bound n+3+pad); 2D maps (ibeg_m:iend_m, jbeg_m:jend_m).  ld_k and ld_i
+ *     are the leading extents of the caller's arrays.
+ *   - the context owns all device memory; host pointers are only read or
+ *     written during the call that receives them.
+ *   - calls on one context are not thread-safe (one host thread per context,
+ *     like the reference's one thread per MPI rank).  All calls are
+ *     stream-ordered on the context's stream; *_fetch, swpc_vmax,
+ *     swpc_download_* and swpc_sync block.
+ *   - precision: velocity, stress, memory variables and medium are FP32
+ *     (the reference built with MP = SP, src/swpc_3d/m_global.f90:30).
+ */
+#ifndef SWPC_GPU_H
+#define SWPC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWPC_OK 0
+#define SWPC_ERR_ARG 1        /* invalid argument or size                    */
+#define SWPC_ERR_CUDA 2       /* CUDA runtime error (message has the name)   */
+#define SWPC_ERR_STATE 3      /* call out of order (e.g. step before setup)  */
+#define SWPC_ERR_DIVERGED 4   /* max |V| * UC > 1e5 (m_report.f90:142-152)   */
+#define SWPC_ERR_NOMEM 5      /* device allocation failed                    */
+
+/* solver kinds */
+#define SWPC_KIND_3D 3
+#define SWPC_KIND_PSV 2
+#define SWPC_KIND_SH 1
+
+/* source-time-function codes (m_fdtool.f90:472-497 `momentrate`) */
+#define SWPC_STF_KUPPER 0
+#define SWPC_STF_BOXCAR 1
+#define SWPC_STF_TRIANGLE 2
+#define SWPC_STF_HERRMANN 3
+#define SWPC_STF_COSINE 4
+#define SWPC_STF_TEXP 5
+
+/* field ids for swpc_upload_field / swpc_download_field */
+#define SWPC_F_VX 0
+#define SWPC_F_VY 1
+#define SWPC_F_VZ 2
+#define SWPC_F_SXX 3
+#define SWPC_F_SYY 4
+#define SWPC_F_SZZ 5
+#define SWPC_F_SYZ 6
+#define SWPC_F_SXZ 7
+#define SWPC_F_SXY 8
+/* memory variables: SWPC_F_R + 3*c + (m-1), c = 0..5 for xx yy zz yz xz xy */
+#define SWPC_F_R 10
+/* PML auxiliaries (m_absorb_p.f90:47-52), 18 in the order
+ * axVx ayVx azVx axVy ayVy azVy axVz ayVz azVz
+ * axSxx aySxy azSxz axSxy aySyy azSyz axSxz aySyz azSzz */
+#define SWPC_F_AUX 40
+
+/* wave-field recorder components (m_wav.f90:31-34) */
+#define SWPC_WAV_V 1
+#define SWPC_WAV_U 2
+#define SWPC_WAV_STRESS 4
+#define SWPC_WAV_STRAIN 8
+
+typedef struct swpc_ctx swpc_ctx;
+
+/* Grid description: the parameters global__readprm / global__setup2 fix
+ * (m_global.f90:126-179, 221-390) for a single node covering the whole
+ * domain.  For the 2D codes ny = 1 (P-SV: x-z, SH: x-z with Vy). */
+typedef struct swpc_desc {
+    int kind;        /* SWPC_KIND_3D / _PSV / _SH                                 */
+    int nx, ny, nz;  /* global grid size                                          */
+    int na;          /* absorber thickness in cells (abc_type = 'pml')            */
+    int nm;          /* Zener memory variables, 0..3 (reference NM = 3)           */
+    int nt;          /* number of time steps (sizes the source/recorder tables)   */
+    float dx, dy, dz;/* grid spacing [km] (real(MP), MP = SP)                     */
+    float dt;        /* time step [s]                                             */
+    float tbeg;      /* start time [s]                                            */
+    int device;      /* CUDA device ordinal                                       */
+} swpc_desc;
+
+/* Medium and integer maps as produced by medium__setup
+ * (src/swpc_3d/m_medium.f90:36-467).  Float fields are 3D Fortran arrays
+ * over the memory box; the 2D int maps cover (ibeg_m:iend_m, jbeg_m:jend_m).
+ * For P-SV only lam, mu, taup, taus, rho are read (b and mu_xz are formed
+ * inside the kernels as in src/swpc_psv/m_kernel.f90:118-119, 270-274);
+ * for SH only mu, taus, rho. */
+typedef struct swpc_medium_view {
+    const float *rho, *lam, *mu, *taup, *taus;
+    const float *bx, *by, *bz, *muyz, *muxz, *muxy;
+    int ld_k, ld_i;                        /* extents of the 3D arrays             */
+    const int *kfs, *kob;                  /* free-surface / ocean-bottom k        */
+    const int *kfs_top, *kfs_bot;          /* 2nd-order band (m_medium.f90:382-386)*/
+    const int *kob_top, *kob_bot;
+    const int *kbeg_a;                     /* absorber start (m_global.f90:336-345)*/
+    int ld_i2;                             /* leading extent of the 2D maps        */
+} swpc_medium_view;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Allocates every device array of the run (zero-filled).  Replaces the
+ * allocations of m_kernel.f90:354-378, m_medium.f90:477-500 and the
+ * `!$acc enter data` block of main.f90:80-119. */
+int swpc_create(const swpc_desc *desc, swpc_ctx **out);
+int swpc_destroy(swpc_ctx *ctx);
+const char *swpc_last_error(const swpc_ctx *ctx);
+/* cudaStream_t of the context, as void*. */
+void *swpc_stream(swpc_ctx *ctx);
+int swpc_sync(swpc_ctx *ctx);
+
+/* ---- setup ------------------------------------------------------------- */
+
+/* Copies the medium and maps to HBM (the `!$acc enter data copyin` of
+ * main.f90:97-119). */
+int swpc_upload_medium(swpc_ctx *ctx, const swpc_medium_view *m);
+
+/* kernel__setup (src/swpc_3d/m_kernel.f90:30-73): FD coefficients from dx,
+ * dy, dz and the Zener coefficients c1, c2, d1, d2 from ts(1:nm) and dt,
+ * computed in single precision with the reference's expression order. */
+int swpc_kernel_setup(swpc_ctx *ctx, const float *ts);
+
+/* absorb_p__setup (src/swpc_3d/m_absorb_p.f90:60-124): the caller passes
+ * the damping profiles g(4, n) from damping_profile (:507-547) at cell
+ * centres (c) and edges (e) for x (nx), y (ny) and z (nz).  The 18
+ * auxiliary fields are allocated only for absorber cells. */
+int swpc_absorb_setup(swpc_ctx *ctx, const float *gxc, const float *gxe, const float *gyc, const float *gye,
+                      const float *gzc, const float *gze);
+
+/* source__setup (src/swpc_3d/m_source.f90:41-313) after grid assignment and
+ * normalisation: nsrc sources at grid (isrc, jsrc, ksrc), srcprm(2, nsrc) =
+ * (start time, rise time), mo(nsrc) already divided by M0, m6(6, nsrc) =
+ * (mxx, myy, mzz, myz, mxz, mxy).  dt_dxyz = dt / (dx*dy*dz).  The
+ * moment-rate function is tabulated for it = 1..nt at t = tbeg + (it-0.5)dt
+ * (m_source.f90:800). */
+int swpc_source_setup(swpc_ctx *ctx, int nsrc, const int *isrc, const int *jsrc, const int *ksrc,
+                      const float *srcprm, const float *mo, const float *m6, int stftype);
+
+/* Body-force mode (bf_mode, m_source.f90:134-137, 835-876): f3(3, nsrc) =
+ * (fx, fy, fz) already divided by M0; stime at t = tbeg + it*dt. */
+int swpc_bodyforce_setup(swpc_ctx *ctx, int nsrc, const int *isrc, const int *jsrc, const int *ksrc,
+                         const float *srcprm, const float *f3, int stftype);
+
+/* Reciprocity source of green__source (src/swpc_3d/m_green.f90:597-632):
+ * unit force along cmp ('x','y','z') at one station cell. */
+int swpc_green_setup(swpc_ctx *ctx, int isrc, int jsrc, int ksrc, char cmp, float green_tbeg, float green_trise,
+                     int stftype);
+
+/* wav__setup / set_stinfo (src/swpc_3d/m_wav.f90:76-142, 144-274): station
+ * cells, decimation, and output scaling M0, UC; what = OR of SWPC_WAV_*. */
+int swpc_wav_setup(swpc_ctx *ctx, int nst, const int *ist, const int *jst, const int *kst, int ntdec_w,
+                   int what, float M0, float UC);
+
+/* ---- the time step (names follow the reference routines) --------------- */
+
+int swpc_kernel_update_stress(swpc_ctx *ctx);   /* m_kernel.f90:142-326      */
+int swpc_absorb_update_stress(swpc_ctx *ctx);   /* m_absorb_p.f90:313-505    */
+int swpc_kernel_update_vel(swpc_ctx *ctx);      /* m_kernel.f90:75-140       */
+int swpc_absorb_update_vel(swpc_ctx *ctx);      /* m_absorb_p.f90:126-311    */
+/* Fused interior + absorber passes: one launch covers the whole domain and
+ * computes exactly what kernel__update_* followed by absorb__update_* do. */
+int swpc_update_stress(swpc_ctx *ctx);
+int swpc_update_vel(swpc_ctx *ctx);
+int swpc_source_stressglut(swpc_ctx *ctx, int it);  /* m_source.f90:775-833  */
+int swpc_source_bodyforce(swpc_ctx *ctx, int it);   /* m_source.f90:835-876  */
+int swpc_green_source(swpc_ctx *ctx, int it);       /* m_green.f90:597-632   */
+/* global__comm_stress / global__comm_vel (m_global.f90:393-609): with one
+ * domain per GPU every neighbour is MPI_PROC_NULL and the unpack writes
+ * zeros into ghost planes that no kernel writes, so these are no-ops kept
+ * for call-order fidelity. */
+int swpc_comm_stress(swpc_ctx *ctx);
+int swpc_comm_vel(swpc_ctx *ctx);
+int swpc_wav_store(swpc_ctx *ctx, int it);          /* m_wav.f90:400-628     */
+/* kernel__vmax (m_kernel.f90:328-352): max |V| one cell below the ocean
+ * bottom; blocks.  Sets SWPC_ERR_DIVERGED when max*UC > 1e5
+ * (m_report.f90:142-152). */
+int swpc_vmax(swpc_ctx *ctx, float out[3]);
+
+/* One full step in main.f90 order: wav__store, update_stress (fused),
+ * stressglut, comm, update_vel (fused), bodyforce, green, comm. */
+int swpc_step(swpc_ctx *ctx, int it);
+/* Steps it0 .. it0+nsteps-1 as replays of a captured CUDA graph. */
+int swpc_run(swpc_ctx *ctx, int it0, int nsteps);
+/* Device time of `nsteps` steps from it0 (CUDA events on the context's
+ * stream); result in milliseconds. */
+int swpc_time_steps(swpc_ctx *ctx, int it0, int nsteps, float *ms);
+
+/* ---- data movement ------------------------------------------------------ */
+
+/* wav buffers in the reference layout wav_*(ntw, ncmp, nst) (m_wav.f90:37-38). */
+int swpc_wav_fetch(swpc_ctx *ctx, int what, float *out);
+int swpc_wav_dims(const swpc_ctx *ctx, int *ntw, int *nst);
+/* One field in the Fortran memory-box layout (ld_k, ld_i as above). */
+int swpc_download_field(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
+int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
+/* Memory-variable and PML-auxiliary fields are defined only on their
+ * regions; outside them download writes 0 and upload ignores the input. */
+
+/* Device bytes held by the context. */
+long long swpc_device_bytes(const swpc_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,77 @@
+/*
+ * swpc_setup.h -- host-side setup routines of the B200 OpenSWPC library.
+ *
+ * In the reference these run once before the time loop, inside the Fortran
+ * modules m_global, m_medium, m_vmodel_lhm(_rmed), m_absorb_p, m_source and
+ * m_wav.  A Fortran driver keeps its own setup and only needs swpc_gpu.h;
+ * these entry points serve drivers that do not have the Fortran setup (the
+ * Python host layer of this package, C/C++ drivers).  Every routine computes
+ * in single precision with the reference's expression order so that the
+ * integer maps are bit-identical and the float fields reproducible.
+ *
+ * Arrays follow the reference layout: 3D fields over the memory box
+ * (kbeg_m:kend_m, ibeg_m:iend_m, jbeg_m:jend_m) = (-2:nz+3, -2:nx+3, -2:ny+3),
+ * k fastest; 2D maps over (-2:nx+3, -2:ny+3).  For the 2D codes pass ny = 1
+ * and arrays over (-2:nz+3, -2:nx+3).
+ */
+#ifndef SWPC_SETUP_H
+#define SWPC_SETUP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Grid geometry shared by the setup routines (m_global.f90:54-66). */
+typedef struct swpc_grid {
+    int nx, ny, nz, na, nm;
+    float dx, dy, dz, dt;
+    float xbeg, ybeg, zbeg, tbeg;
+} swpc_grid;
+
+/* x2i / y2j / z2k (src/shared/m_fdtool.f90:600-636): ceiling((x-beg)/d). */
+int swpc_x2i(float x, float beg, float d);
+/* i2x / j2y / k2z (src/shared/m_fdtool.f90:639-675): beg + (i-0.5)*d. */
+float swpc_i2x(int i, float beg, float d);
+
+/* momentrate (src/shared/m_fdtool.f90:472-497) with SWPC_STF_* codes. */
+float swpc_momentrate(float t, int stftype, float ts, float tr);
+
+/* sdr2moment (src/shared/m_fdtool.f90:307-336); m6 = xx yy zz yz xz xy. */
+void swpc_sdr2moment(float strike, float dip, float rake, float *m6);
+
+/* visco_set_relaxtime + visco_constq_zeta (m_fdtool.f90:691-812). */
+void swpc_visco_setup(int nm, float fq_min, float fq_max, float *ts, float *zeta);
+
+/* kbeg_a absorber map (src/swpc_3d/m_global.f90:336-345) over the memory
+ * box columns. */
+void swpc_kbeg_a(const swpc_grid *g, int *kbeg_a);
+
+/* vmodel_lhm (src/swpc_3d/m_vmodel_lhm.f90:21-169); with xi != NULL the
+ * lhm_rmed perturbation (m_vmodel_lhm_rmed.f90:187-195, vcheck
+ * m_fdtool.f90:15-48).  depth/rho/vp/vs/qp/qs per layer; outputs over the
+ * memory box: rho, lam, mu, qp, qs.  Air above depth(1) with z < 0. */
+int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const float *rho0, const float *vp0,
+                    const float *vs0, const float *qp0, const float *qs0, float vcut, const float *xi, float rhomin,
+                    float *rho, float *lam, float *mu, float *qp, float *qs);
+
+/* medium__setup after the vmodel (src/swpc_3d/m_medium.f90:124-225 and its
+ * contained routines): absorber homogenisation, tau-method (taup/taus from
+ * qp/qs), relaxed moduli, free-surface/ocean-bottom detection, velocity
+ * range, averaged buoyancy and rigidities.  rho/lam/mu are updated in
+ * place, qp/qs are read; outputs: taup, taus, bx, by, bz, muyz, muxz, muxy
+ * (3D fields), kfs, kob, kfs_top, kfs_bot, kob_top, kob_bot (2D maps),
+ * ts(nm), scal = {zeta, vmin, vmax}.  3D only (see swpc_setup_medium_2d). */
+int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam, float *mu,
+                      const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by, float *bz,
+                      float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
+                      int *kob_top, int *kob_bot, float *ts, float *scal);
+
+/* damping_profile (src/swpc_3d/m_absorb_p.f90:507-547) for the six profiles
+ * of absorb_p__setup (:79-93); each output is g(4, n). */
+void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gxe, float *gyc, float *gye, float *gzc,
+                           float *gze);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

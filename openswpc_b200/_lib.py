@@ -1,0 +1,154 @@
+"""ctypes binding of ``lib/libswpc_gpu.so`` (include/swpc_gpu.h, include/swpc_setup.h).
+
+The library is the product: every time-step computation happens in its CUDA
+kernels.  Loading fails loudly when the shared library is missing; there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libswpc_gpu.so"
+
+SWPC_OK = 0
+SWPC_ERR_ARG = 1
+SWPC_ERR_CUDA = 2
+SWPC_ERR_STATE = 3
+SWPC_ERR_DIVERGED = 4
+SWPC_ERR_NOMEM = 5
+
+KIND_3D, KIND_PSV, KIND_SH = 3, 2, 1
+STF_CODES = {"kupper": 0, "boxcar": 1, "triangle": 2, "herrmann": 3, "cosine": 4, "scosine": 4, "texp": 5}
+
+F_VX, F_VY, F_VZ, F_SXX, F_SYY, F_SZZ, F_SYZ, F_SXZ, F_SXY = range(9)
+F_R = 10
+F_AUX = 40
+WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
+
+# every symbol the headers in include/ declare
+EXPORTS = [
+    "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
+    "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
+    "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
+    "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
+    "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
+    "swpc_vmax", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
+    "swpc_download_field", "swpc_upload_field", "swpc_device_bytes",
+    # swpc_setup.h
+    "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
+    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles",
+]
+
+
+class SwpcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"swpc error {code}: {msg}")
+        self.code = code
+
+
+class Desc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("na", C.c_int),
+                ("nm", C.c_int), ("nt", C.c_int), ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
+                ("dt", C.c_float), ("tbeg", C.c_float), ("device", C.c_int)]
+
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int)
+
+
+class MediumView(C.Structure):
+    _fields_ = [("rho", _FP), ("lam", _FP), ("mu", _FP), ("taup", _FP), ("taus", _FP), ("bx", _FP),
+                ("by", _FP), ("bz", _FP), ("muyz", _FP), ("muxz", _FP), ("muxy", _FP), ("ld_k", C.c_int),
+                ("ld_i", C.c_int), ("kfs", _IP), ("kob", _IP), ("kfs_top", _IP), ("kfs_bot", _IP),
+                ("kob_top", _IP), ("kob_bot", _IP), ("kbeg_a", _IP), ("ld_i2", C.c_int)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("na", C.c_int), ("nm", C.c_int),
+                ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float),
+                ("xbeg", C.c_float), ("ybeg", C.c_float), ("zbeg", C.c_float), ("tbeg", C.c_float)]
+
+
+_lib = None
+
+
+def fptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"] or a.flags["F_CONTIGUOUS"]
+    return a.ctypes.data_as(_FP)
+
+
+def iptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32
+    return a.ctypes.data_as(_IP)
+
+
+def load():
+    """Load the shared library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m openswpc_b200.build` (needs nvcc)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    i = C.c_int
+    f = C.c_float
+    sig = {
+        "swpc_create": (i, [C.POINTER(Desc), C.POINTER(vp)]),
+        "swpc_destroy": (i, [vp]),
+        "swpc_last_error": (C.c_char_p, [vp]),
+        "swpc_stream": (vp, [vp]),
+        "swpc_sync": (i, [vp]),
+        "swpc_upload_medium": (i, [vp, C.POINTER(MediumView)]),
+        "swpc_kernel_setup": (i, [vp, _FP]),
+        "swpc_absorb_setup": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "swpc_source_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, _FP, i]),
+        "swpc_bodyforce_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, i]),
+        "swpc_green_setup": (i, [vp, i, i, i, C.c_char, f, f, i]),
+        "swpc_wav_setup": (i, [vp, i, _IP, _IP, _IP, i, i, f, f]),
+        "swpc_vmax": (i, [vp, _FP]),
+        "swpc_step": (i, [vp, i]),
+        "swpc_run": (i, [vp, i, i]),
+        "swpc_time_steps": (i, [vp, i, i, _FP]),
+        "swpc_wav_fetch": (i, [vp, i, _FP]),
+        "swpc_wav_dims": (i, [vp, _IP, _IP]),
+        "swpc_download_field": (i, [vp, i, _FP, i, i]),
+        "swpc_upload_field": (i, [vp, i, _FP, i, i]),
+        "swpc_device_bytes": (C.c_longlong, [vp]),
+        "swpc_x2i": (i, [f, f, f]),
+        "swpc_i2x": (f, [i, f, f]),
+        "swpc_momentrate": (f, [f, i, f, f]),
+        "swpc_sdr2moment": (None, [f, f, f, _FP]),
+        "swpc_visco_setup": (None, [i, f, f, _FP, _FP]),
+        "swpc_kbeg_a": (None, [C.POINTER(Grid), _IP]),
+        "swpc_vmodel_lhm": (i, [C.POINTER(Grid), i, _FP, _FP, _FP, _FP, _FP, _FP, f, _FP, f, _FP, _FP, _FP,
+                                _FP, _FP]),
+        "swpc_setup_medium": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP,
+                                  _FP, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _FP, _FP]),
+        "swpc_damping_profiles": (None, [C.POINTER(Grid), f, _FP, _FP, _FP, _FP, _FP, _FP]),
+    }
+    for name in ("swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
+                 "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_comm_stress",
+                 "swpc_comm_vel"):
+        sig[name] = (i, [vp])
+    for name in ("swpc_source_stressglut", "swpc_source_bodyforce", "swpc_green_source", "swpc_wav_store"):
+        sig[name] = (i, [vp, i])
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(ctx, rc: int) -> None:
+    if rc != SWPC_OK:
+        msg = load().swpc_last_error(ctx)
+        raise SwpcError(rc, msg.decode() if msg else "")

@@ -1,0 +1,493 @@
+// swpc3d_kernels.cu -- fused sm_100a kernels of the 3D viscoelastic step.
+//
+// One launch per half step covers the whole domain: cells of the interior
+// kernel region (m_global.f90:349-378) run the 4th-order viscoelastic update
+// of src/swpc_3d/m_kernel.f90, the remaining cells (k >= kbeg_a(i,j),
+// m_global.f90:336-345) run the 2nd-order ADE-CFS PML update of
+// src/swpc_3d/m_absorb_p.f90.  The two regions are disjoint and neither pass
+// reads what the other writes within a half step, so the fused launch gives
+// exactly the result of the two reference routines run one after the other.
+//
+// Arithmetic: every expression keeps the reference's left-to-right order and
+// this file is compiled with -fmad=false, so each product and sum is rounded
+// separately exactly as the single-precision (MP = SP) Fortran build spells
+// it out; the results are bitwise identical to the CPU oracle.
+//
+// Thread mapping: a warp owns 32 consecutive k of one (i, j) column (one
+// coalesced 128-byte row per field); block = 32 x BI x BJ columns.
+#include <cuda_runtime.h>
+
+#include "swpc_ctx.h"
+#include "swpc_kernels.cuh"
+
+namespace swpc {
+
+// ---------------------------------------------------------------------------
+// velocity: kernel__update_vel (m_kernel.f90:75-140) +
+//           absorb_p__update_vel (m_absorb_p.f90:248-309)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
+    const Geo g = a.g;
+    const int k = 1 + blockIdx.x * 32 + threadIdx.x;
+    const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = 1 + blockIdx.z * blockDim.z + threadIdx.z;
+    if (k > g.nz || i > g.nx || j > g.ny) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const long long PI = g.Kp;
+    const long long PJ = (long long)g.Kp * g.Ip;
+    const float *__restrict__ Sxx = a.Sxx;
+    const float *__restrict__ Syy = a.Syy;
+    const float *__restrict__ Szz = a.Szz;
+    const float *__restrict__ Syz = a.Syz;
+    const float *__restrict__ Sxz = a.Sxz;
+    const float *__restrict__ Sxy = a.Sxy;
+    const float dt = a.dt;
+
+    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
+        if (!(a.mask & 1)) return;
+        const int4 bd = __ldg(&a.band[col]);
+        const int p1 = (k - bd.x) * (bd.y - k);
+        const int p2 = (k - bd.z) * (bd.w - k);
+        const int s = ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;   // isign = +1 -> 2nd-order band
+        const float re40x = a.e40[0][s], re41x = a.e41[0][s];
+        const float re40y = a.e40[1][s], re41y = a.e41[1][s];
+        const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+
+        float d3Sx3 = (__ldg(&Sxx[e + PI]) - __ldg(&Sxx[e])) * re40x - (__ldg(&Sxx[e + 2 * PI]) - __ldg(&Sxx[e - PI])) * re41x
+                    + (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PJ])) * re40y - (__ldg(&Sxy[e + PJ]) - __ldg(&Sxy[e - 2 * PJ])) * re41y
+                    + (__ldg(&Sxz[e]) - __ldg(&Sxz[e - 1])) * re40z - (__ldg(&Sxz[e + 1]) - __ldg(&Sxz[e - 2])) * re41z;
+        float d3Sy3 = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PI])) * re40x - (__ldg(&Sxy[e + PI]) - __ldg(&Sxy[e - 2 * PI])) * re41x
+                    + (__ldg(&Syy[e + PJ]) - __ldg(&Syy[e])) * re40y - (__ldg(&Syy[e + 2 * PJ]) - __ldg(&Syy[e - PJ])) * re41y
+                    + (__ldg(&Syz[e]) - __ldg(&Syz[e - 1])) * re40z - (__ldg(&Syz[e + 1]) - __ldg(&Syz[e - 2])) * re41z;
+        float d3Sz3 = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - PI])) * re40x - (__ldg(&Sxz[e + PI]) - __ldg(&Sxz[e - 2 * PI])) * re41x
+                    + (__ldg(&Syz[e]) - __ldg(&Syz[e - PJ])) * re40y - (__ldg(&Syz[e + PJ]) - __ldg(&Syz[e - 2 * PJ])) * re41y
+                    + (__ldg(&Szz[e + 1]) - __ldg(&Szz[e])) * re40z - (__ldg(&Szz[e + 2]) - __ldg(&Szz[e - 1])) * re41z;
+
+        a.Vx[e] = a.Vx[e] + __ldg(&a.bx[e]) * d3Sx3 * dt;
+        a.Vy[e] = a.Vy[e] + __ldg(&a.by[e]) * d3Sy3 * dt;
+        a.Vz[e] = a.Vz[e] + __ldg(&a.bz[e]) * d3Sz3 * dt;
+        return;
+    }
+
+    // absorber cell: k >= kbeg_a(i, j) holds for every cell outside the kernel box
+    if (!(a.mask & 2)) return;
+    const int2 pc = __ldg(&a.pmlcol[col]);
+    const long long q = (long long)pc.y + (k - pc.x);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+    const float dxSxx = (__ldg(&Sxx[e + PI]) - __ldg(&Sxx[e])) * r20x;
+    const float dySyy = (__ldg(&Syy[e + PJ]) - __ldg(&Syy[e])) * r20y;
+    const float dzSzz = (__ldg(&Szz[e + 1]) - __ldg(&Szz[e])) * r20z;
+    const float dySyz = (__ldg(&Syz[e]) - __ldg(&Syz[e - PJ])) * r20y;
+    const float dzSyz = (__ldg(&Syz[e]) - __ldg(&Syz[e - 1])) * r20z;
+    const float dxSxz = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - PI])) * r20x;
+    const float dzSxz = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - 1])) * r20z;
+    const float dxSxy = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PI])) * r20x;
+    const float dySxy = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PJ])) * r20y;
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+
+    float *__restrict__ axSxx = a.aS[0];
+    float *__restrict__ aySxy = a.aS[1];
+    float *__restrict__ azSxz = a.aS[2];
+    float *__restrict__ axSxy = a.aS[3];
+    float *__restrict__ aySyy = a.aS[4];
+    float *__restrict__ azSyz = a.aS[5];
+    float *__restrict__ axSxz = a.aS[6];
+    float *__restrict__ aySyz = a.aS[7];
+    float *__restrict__ azSzz = a.aS[8];
+    const float vxSxx = axSxx[q], vySxy = aySxy[q], vzSxz = azSxz[q];
+    const float vxSxy = axSxy[q], vySyy = aySyy[q], vzSyz = azSyz[q];
+    const float vxSxz = axSxz[q], vySyz = aySyz[q], vzSzz = azSzz[q];
+
+    a.Vx[e] = a.Vx[e] + __ldg(&a.bx[e]) * (gxe.x * dxSxx + gyc.x * dySxy + gzc.x * dzSxz
+                                          + gxe.y * vxSxx + gyc.y * vySxy + gzc.y * vzSxz) * dt;
+    a.Vy[e] = a.Vy[e] + __ldg(&a.by[e]) * (gxc.x * dxSxy + gye.x * dySyy + gzc.x * dzSyz
+                                          + gxc.y * vxSxy + gye.y * vySyy + gzc.y * vzSyz) * dt;
+    a.Vz[e] = a.Vz[e] + __ldg(&a.bz[e]) * (gxc.x * dxSxz + gyc.x * dySyz + gze.x * dzSzz
+                                          + gxc.y * vxSxz + gyc.y * vySyz + gze.y * vzSzz) * dt;
+
+    axSxx[q] = gxe.z * vxSxx + gxe.w * dxSxx * dt;
+    aySxy[q] = gyc.z * vySxy + gyc.w * dySxy * dt;
+    azSxz[q] = gzc.z * vzSxz + gzc.w * dzSxz * dt;
+    axSxy[q] = gxc.z * vxSxy + gxc.w * dxSxy * dt;
+    aySyy[q] = gye.z * vySyy + gye.w * dySyy * dt;
+    azSyz[q] = gzc.z * vzSyz + gzc.w * dzSyz * dt;
+    axSxz[q] = gxc.z * vxSxz + gxc.w * dxSxz * dt;
+    aySyz[q] = gyc.z * vySyz + gyc.w * dySyz * dt;
+    azSzz[q] = gze.z * vzSzz + gze.w * dzSzz * dt;
+}
+
+// ---------------------------------------------------------------------------
+// stress: kernel__update_stress (m_kernel.f90:142-326) +
+//         absorb_p__update_stress (m_absorb_p.f90:424-503)
+// ---------------------------------------------------------------------------
+template <int NM>
+__global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
+    const Geo g = a.g;
+    const int k = 1 + blockIdx.x * 32 + threadIdx.x;
+    const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = 1 + blockIdx.z * blockDim.z + threadIdx.z;
+    if (k > g.nz || i > g.nx || j > g.ny) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const long long PI = g.Kp;
+    const long long PJ = (long long)g.Kp * g.Ip;
+    const float *__restrict__ Vx = a.Vx;
+    const float *__restrict__ Vy = a.Vy;
+    const float *__restrict__ Vz = a.Vz;
+    const float dt = a.dt;
+
+    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
+        if (!(a.mask & 1)) return;
+        const int4 bd = __ldg(&a.band[col]);
+        const int p1 = (k - bd.x) * (bd.y - k);
+        const int p2 = (k - bd.z) * (bd.w - k);
+        const int s = ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;
+        const float re40x = a.e40[0][s], re41x = a.e41[0][s];
+        const float re40y = a.e40[1][s], re41y = a.e41[1][s];
+        const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+
+        const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
+        // normal components (m_kernel.f90:195-235)
+        const float dxVx = (vx0 - __ldg(&Vx[e - PI])) * re40x - (__ldg(&Vx[e + PI]) - __ldg(&Vx[e - 2 * PI])) * re41x;
+        const float dyVy = (vy0 - __ldg(&Vy[e - PJ])) * re40y - (__ldg(&Vy[e + PJ]) - __ldg(&Vy[e - 2 * PJ])) * re41y;
+        const float dzVz = (vz0 - __ldg(&Vz[e - 1])) * re40z - (__ldg(&Vz[e + 1]) - __ldg(&Vz[e - 2])) * re41z;
+        const float mu = __ldg(&a.mu[e]);
+        const float mu2 = 2 * mu;
+        const float lam2mu = __ldg(&a.lam[e]) + mu2;
+        const float taup1 = __ldg(&a.taup[e]);
+        const float taus1 = __ldg(&a.taus[e]);
+        const float d3v3 = dxVx + dyVy + dzVz;
+        const float dyVy_dzVz = dyVy + dzVz;
+        const float dxVx_dzVz = dxVx + dzVz;
+        const float dxVx_dyVy = dxVx + dyVy;
+        float Rxx_n = 0.0f, Ryy_n = 0.0f, Rzz_n = 0.0f;
+#pragma unroll
+        for (int m = 0; m < NM; m++) {
+            float *Rxx = a.R[0 * 3 + m];
+            float *Ryy = a.R[1 * 3 + m];
+            float *Rzz = a.R[2 * 3 + m];
+            const float rxx = a.c1[m] * Rxx[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dyVy_dzVz) * dt;
+            const float ryy = a.c1[m] * Ryy[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dzVz) * dt;
+            const float rzz = a.c1[m] * Rzz[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dyVy) * dt;
+            Rxx[e] = rxx;
+            Ryy[e] = ryy;
+            Rzz[e] = rzz;
+            Rxx_n = Rxx_n + a.d1[m] * rxx;
+            Ryy_n = Ryy_n + a.d1[m] * ryy;
+            Rzz_n = Rzz_n + a.d1[m] * rzz;
+        }
+        const float taup_plus1 = 1 + taup1 * (1 + a.d2);
+        const float taus_plus1 = 1 + taus1 * (1 + a.d2);
+        a.Sxx[e] = a.Sxx[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt;
+        a.Syy[e] = a.Syy[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt;
+        a.Szz[e] = a.Szz[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt;
+
+        // shear components (m_kernel.f90:282-311)
+        const float dxVy_dyVx = (__ldg(&Vy[e + PI]) - vy0) * re40x - (__ldg(&Vy[e + 2 * PI]) - __ldg(&Vy[e - PI])) * re41x
+                              + (__ldg(&Vx[e + PJ]) - vx0) * re40y - (__ldg(&Vx[e + 2 * PJ]) - __ldg(&Vx[e - PJ])) * re41y;
+        const float dxVz_dzVx = (__ldg(&Vz[e + PI]) - vz0) * re40x - (__ldg(&Vz[e + 2 * PI]) - __ldg(&Vz[e - PI])) * re41x
+                              + (__ldg(&Vx[e + 1]) - vx0) * re40z - (__ldg(&Vx[e + 2]) - __ldg(&Vx[e - 1])) * re41z;
+        const float dyVz_dzVy = (__ldg(&Vz[e + PJ]) - vz0) * re40y - (__ldg(&Vz[e + 2 * PJ]) - __ldg(&Vz[e - PJ])) * re41y
+                              + (__ldg(&Vy[e + 1]) - vy0) * re40z - (__ldg(&Vy[e + 2]) - __ldg(&Vy[e - 1])) * re41z;
+        const float muyz = __ldg(&a.muyz[e]), muxz = __ldg(&a.muxz[e]), muxy = __ldg(&a.muxy[e]);
+        float Ryz_n = 0.0f, Rxz_n = 0.0f, Rxy_n = 0.0f;
+#pragma unroll
+        for (int m = 0; m < NM; m++) {
+            float *Ryz = a.R[3 * 3 + m];
+            float *Rxz = a.R[4 * 3 + m];
+            float *Rxy = a.R[5 * 3 + m];
+            const float ryz = a.c1[m] * Ryz[e] - a.c2[m] * muyz * taus1 * dyVz_dzVy * dt;
+            const float rxz = a.c1[m] * Rxz[e] - a.c2[m] * muxz * taus1 * dxVz_dzVx * dt;
+            const float rxy = a.c1[m] * Rxy[e] - a.c2[m] * muxy * taus1 * dxVy_dyVx * dt;
+            Ryz[e] = ryz;
+            Rxz[e] = rxz;
+            Rxy[e] = rxy;
+            Ryz_n = Ryz_n + a.d1[m] * ryz;
+            Rxz_n = Rxz_n + a.d1[m] * rxz;
+            Rxy_n = Rxy_n + a.d1[m] * rxy;
+        }
+        a.Syz[e] = a.Syz[e] + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt;
+        a.Sxz[e] = a.Sxz[e] + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt;
+        a.Sxy[e] = a.Sxy[e] + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt;
+        return;
+    }
+
+    // absorber cell (m_absorb_p.f90:445-491)
+    if (!(a.mask & 2)) return;
+    const int2 pc = __ldg(&a.pmlcol[col]);
+    const long long q = (long long)pc.y + (k - pc.x);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
+
+    const float dxVx = (vx0 - __ldg(&Vx[e - PI])) * r20x;
+    const float dyVy = (vy0 - __ldg(&Vy[e - PJ])) * r20y;
+    const float dzVz = (vz0 - __ldg(&Vz[e - 1])) * r20z;
+    const float mu = __ldg(&a.mu[e]);
+    const float lam2mu_R = (__ldg(&a.lam[e]) + 2 * mu);
+    const float lam_R = lam2mu_R - 2 * mu;
+    float *__restrict__ axVx = a.aV[0];
+    float *__restrict__ ayVx = a.aV[1];
+    float *__restrict__ azVx = a.aV[2];
+    float *__restrict__ axVy = a.aV[3];
+    float *__restrict__ ayVy = a.aV[4];
+    float *__restrict__ azVy = a.aV[5];
+    float *__restrict__ axVz = a.aV[6];
+    float *__restrict__ ayVz = a.aV[7];
+    float *__restrict__ azVz = a.aV[8];
+    const float vaxVx = axVx[q], vayVy = ayVy[q], vazVz = azVz[q];
+    const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
+    const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
+    const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
+    a.Sxx[e] = a.Sxx[e] + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt;
+    a.Syy[e] = a.Syy[e] + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt;
+    a.Szz[e] = a.Szz[e] + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt;
+    axVx[q] = gxc.z * vaxVx + gxc.w * dxVx * dt;
+    ayVy[q] = gyc.z * vayVy + gyc.w * dyVy * dt;
+    azVz[q] = gzc.z * vazVz + gzc.w * dzVz * dt;
+
+    const float dxVy = (__ldg(&Vy[e + PI]) - vy0) * r20x;
+    const float dxVz = (__ldg(&Vz[e + PI]) - vz0) * r20x;
+    const float dyVx = (__ldg(&Vx[e + PJ]) - vx0) * r20y;
+    const float dyVz = (__ldg(&Vz[e + PJ]) - vz0) * r20y;
+    const float dzVx = (__ldg(&Vx[e + 1]) - vx0) * r20z;
+    const float dzVy = (__ldg(&Vy[e + 1]) - vy0) * r20z;
+    const float vayVx = ayVx[q], vazVx = azVx[q], vaxVy = axVy[q];
+    const float vazVy = azVy[q], vaxVz = axVz[q], vayVz = ayVz[q];
+    a.Syz[e] = a.Syz[e] + __ldg(&a.muyz[e]) * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt;
+    a.Sxz[e] = a.Sxz[e] + __ldg(&a.muxz[e]) * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt;
+    a.Sxy[e] = a.Sxy[e] + __ldg(&a.muxy[e]) * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt;
+    ayVx[q] = gye.z * vayVx + gye.w * dyVx * dt;
+    azVx[q] = gze.z * vazVx + gze.w * dzVx * dt;
+    axVy[q] = gxe.z * vaxVy + gxe.w * dxVy * dt;
+    azVy[q] = gze.z * vazVy + gze.w * dzVy * dt;
+    axVz[q] = gxe.z * vaxVz + gxe.w * dxVz * dt;
+    ayVz[q] = gye.z * vayVz + gye.w * dyVz * dt;
+}
+
+void launch_vel3d(const Vel3Args &a, dim3 grid, dim3 block, cudaStream_t st) {
+    vel3d_kernel<<<grid, block, 0, st>>>(a);
+}
+
+void launch_stress3d(const Str3Args &a, int nm, dim3 grid, dim3 block, cudaStream_t st) {
+    switch (nm) {
+    case 0: stress3d_kernel<0><<<grid, block, 0, st>>>(a); break;
+    case 1: stress3d_kernel<1><<<grid, block, 0, st>>>(a); break;
+    case 2: stress3d_kernel<2><<<grid, block, 0, st>>>(a); break;
+    default: stress3d_kernel<3><<<grid, block, 0, st>>>(a); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// point sources: source__stressglut (m_source.f90:798-826),
+// source__bodyforce (:854-870), green__source (m_green.f90:615-627).
+// Entries are applied in list order; when no two entries touch the same
+// cell the host marks the list parallel and each entry gets a thread.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void apply_entry(const InjArgs &a, const InjEntry &en, int it) {
+    float *f = a.fields[en.field];
+    const float st = a.stime[(long long)(it - 1) * a.nsrc + en.src];
+    switch (en.mode) {
+    case INJ_GLUT: {        // S -= m * sdrop, sdrop = mo * stime * dt_dxyz
+        const float sdrop = a.mo[en.src] * st * a.dt_dxyz;
+        f[en.cell] = f[en.cell] - en.coef * sdrop;
+        break;
+    }
+    case INJ_GLUT4: {       // S -= m * sdrop / 4 (3D and P-SV shear cells)
+        const float sdrop = a.mo[en.src] * st * a.dt_dxyz;
+        f[en.cell] = f[en.cell] - en.coef * sdrop / 4;
+        break;
+    }
+    case INJ_GLUT2: {       // S -= m * sdrop / 2 (SH, src/swpc_sh/m_source.f90:583-587)
+        const float sdrop = a.mo[en.src] * st * a.dt_dxyz;
+        f[en.cell] = f[en.cell] - en.coef * sdrop / 2;
+        break;
+    }
+    case INJ_BF3: {         // V += b * f * stime * dt_dxyz / 2 (m_source.f90:863-868)
+        const float b = a.bfields[en.bfield][en.cell];
+        f[en.cell] = f[en.cell] + b * en.coef * st * a.dt_dxyz / 2;
+        break;
+    }
+    case INJ_GREEN: {       // fx = fx1 * dt_dxyz * stf ; V += b * fx / 2 (m_green.f90:617-627)
+        const float fv = en.coef * a.dt_dxyz * st;
+        const float b = a.bfields[en.bfield][en.cell];
+        f[en.cell] = f[en.cell] + b * fv / 2;
+        break;
+    }
+    case INJ_BFPSV: {       // V += f / rho(kk,ii) * stime * dt_dxz / 2 (src/swpc_psv/m_source.f90:640-645)
+        const float rho = a.bfields[0][a.rho_cell[en.src]];
+        f[en.cell] = f[en.cell] + en.coef / rho * st * a.dt_dxyz / 2;
+        break;
+    }
+    case INJ_BFSH: {        // Vy += f / rho(kk,ii) * stime * dt_dxz (src/swpc_sh/m_source.f90:621)
+        const float rho = a.bfields[0][a.rho_cell[en.src]];
+        f[en.cell] = f[en.cell] + en.coef / rho * st * a.dt_dxyz;
+        break;
+    }
+    default: break;
+    }
+}
+
+__global__ void inject_kernel(const InjArgs a) {
+    const int it = a.d_it ? *a.d_it : a.it;
+    if (it < 1 || it > a.nt) return;
+    if (a.serial) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int n = 0; n < a.n; n++) apply_entry(a, a.list[n], it);
+        return;
+    }
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < a.n) apply_entry(a, a.list[n], it);
+}
+
+void launch_inject(const InjArgs &a, cudaStream_t st) {
+    if (a.n <= 0) return;
+    const int threads = 128;
+    const int blocks = a.serial ? 1 : (a.n + threads - 1) / threads;
+    inject_kernel<<<blocks, threads, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// wav__store (m_wav.f90:433-620): one thread per station
+// ---------------------------------------------------------------------------
+__global__ void wav3d_kernel(const Wav3Args a) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nst) return;
+    const int it = a.d_it ? *a.d_it : a.it;
+    const Geo g = a.g;
+    const int i = a.st[3 * n], j = a.st[3 * n + 1], k = a.st[3 * n + 2];
+    const long long e = cell_index(g, k, i, j);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    const float *Vx = a.Vx, *Vy = a.Vy, *Vz = a.Vz;
+    const float dt = a.dt;
+    if (a.what & SWPC_WAV_U) {
+        a.uacc[3 * n + 0] = a.uacc[3 * n + 0] + (Vx[e] + Vx[e - PI]) * 0.5f * dt;
+        a.uacc[3 * n + 1] = a.uacc[3 * n + 1] + (Vy[e] + Vy[e - PJ]) * 0.5f * dt;
+        a.uacc[3 * n + 2] = a.uacc[3 * n + 2] - (Vz[e] + Vz[e - 1]) * 0.5f * dt;
+    }
+    if (a.what & SWPC_WAV_STRAIN) {
+        const float r40x = a.r40[0], r40y = a.r40[1], r40z = a.r40[2];
+        const float r41x = a.r41[0], r41y = a.r41[1], r41z = a.r41[2];
+        // m_wav.f90:468-500
+        const float dxVx = (Vx[e] - Vx[e - PI]) * r40x - (Vx[e + PI] - Vx[e - 2 * PI]) * r41x;
+        const float dyVy = (Vy[e] - Vy[e - PJ]) * r40y - (Vy[e + PJ] - Vy[e - 2 * PJ]) * r41y;
+        const float dzVz = (Vz[e] - Vz[e - 1]) * r40z - (Vz[e + 1] - Vz[e - 2]) * r41z;
+        const long long m = e - PJ;   // (k, i, j-1)
+        const float dxVy = ((Vy[e + PI] - Vy[e]) * r40x - (Vy[e + 2 * PI] - Vy[e - PI]) * r41x
+                          + (Vy[m + PI] - Vy[m]) * r40x - (Vy[m + 2 * PI] - Vy[m - PI]) * r41x
+                          + (Vy[e] - Vy[e - PI]) * r40x - (Vy[e + PI] - Vy[e - 2 * PI]) * r41x
+                          + (Vy[m] - Vy[m - PI]) * r40x - (Vy[m + PI] - Vy[m - 2 * PI]) * r41x) / 4.0f;
+        const long long u = e - 1;    // (k-1, i, j)
+        const float dxVz = ((Vz[e + PI] - Vz[e]) * r40x - (Vz[e + 2 * PI] - Vz[e - PI]) * r41x
+                          + (Vz[u + PI] - Vz[u]) * r40x - (Vz[u + 2 * PI] - Vz[u - PI]) * r41x
+                          + (Vz[e] - Vz[e - PI]) * r40x - (Vz[e + PI] - Vz[e - 2 * PI]) * r41x
+                          + (Vz[u] - Vz[u - PI]) * r40x - (Vz[u + PI] - Vz[u - 2 * PI]) * r41x) / 4.0f;
+        const long long w = e - PI;   // (k, i-1, j)
+        const float dyVx = ((Vx[e + PJ] - Vx[e]) * r40y - (Vx[e + 2 * PJ] - Vx[e - PJ]) * r41y
+                          + (Vx[w + PJ] - Vx[w]) * r40y - (Vx[w + 2 * PJ] - Vx[w - PJ]) * r41y
+                          + (Vx[e] - Vx[e - PJ]) * r40y - (Vx[e + PJ] - Vx[e - 2 * PJ]) * r41y
+                          + (Vx[w] - Vx[w - PJ]) * r40y - (Vx[w + PJ] - Vx[w - 2 * PJ]) * r41y) / 4.0f;
+        const float dyVz = ((Vz[e + PJ] - Vz[e]) * r40y - (Vz[e + 2 * PJ] - Vz[e - PJ]) * r41y
+                          + (Vz[u + PJ] - Vz[u]) * r40y - (Vz[u + 2 * PJ] - Vz[u - PJ]) * r41y
+                          + (Vz[e] - Vz[e - PJ]) * r40y - (Vz[e + PJ] - Vz[e - 2 * PJ]) * r41y
+                          + (Vz[u] - Vz[u - PJ]) * r40y - (Vz[u + PJ] - Vz[u - 2 * PJ]) * r41y) / 4.0f;
+        const float dzVx = ((Vx[e + 1] - Vx[e]) * r40z - (Vx[e + 2] - Vx[e - 1]) * r41z
+                          + (Vx[w + 1] - Vx[w]) * r40z - (Vx[w + 2] - Vx[w - 1]) * r41z
+                          + (Vx[e] - Vx[e - 1]) * r40z - (Vx[e + 1] - Vx[e - 2]) * r41z
+                          + (Vx[w] - Vx[w - 1]) * r40z - (Vx[w + 1] - Vx[w - 2]) * r41z) / 4.0f;
+        const float dzVy = ((Vy[e + 1] - Vy[e]) * r40z - (Vy[e + 2] - Vy[e - 1]) * r41z
+                          + (Vy[m + 1] - Vy[m]) * r40z - (Vy[m + 2] - Vy[m - 1]) * r41z
+                          + (Vy[e] - Vy[e - 1]) * r40z - (Vy[e + 1] - Vy[e - 2]) * r41z
+                          + (Vy[m] - Vy[m - 1]) * r40z - (Vy[m + 1] - Vy[m - 2]) * r41z) / 4.0f;
+        float *ea = a.eacc + 6 * n;
+        ea[0] = ea[0] + dxVx * dt;
+        ea[1] = ea[1] + dyVy * dt;
+        ea[2] = ea[2] + dzVz * dt;
+        ea[3] = ea[3] + (dyVz + dzVy) / 2.0f * dt;
+        ea[4] = ea[4] + (dxVz + dzVx) / 2.0f * dt;
+        ea[5] = ea[5] + (dxVy + dyVx) / 2.0f * dt;
+    }
+    if ((it - 1) % a.ntdec_w != 0) return;
+    const int itw = (it - 1) / a.ntdec_w + 1;
+    if (itw > a.ntw) return;
+    const float M0 = a.M0, UC = a.UC;
+    const long long ntw = a.ntw;
+    if (a.what & SWPC_WAV_V) {
+        float *w = a.wav_v + (long long)n * 3 * ntw + (itw - 1);
+        w[0 * ntw] = (Vx[e] + Vx[e - PI]) / 2.0f * M0 * UC * 1e9f;
+        w[1 * ntw] = (Vy[e] + Vy[e - PJ]) / 2.0f * M0 * UC * 1e9f;
+        w[2 * ntw] = -(Vz[e] + Vz[e - 1]) / 2.0f * M0 * UC * 1e9f;
+    }
+    if (a.what & SWPC_WAV_U) {
+        float *w = a.wav_u + (long long)n * 3 * ntw + (itw - 1);
+        w[0 * ntw] = a.uacc[3 * n + 0] * M0 * UC * 1e9f;
+        w[1 * ntw] = a.uacc[3 * n + 1] * M0 * UC * 1e9f;
+        w[2 * ntw] = a.uacc[3 * n + 2] * M0 * UC * 1e9f;
+    }
+    if (a.what & SWPC_WAV_STRESS) {
+        float *w = a.wav_s + (long long)n * 6 * ntw + (itw - 1);
+        const float *Sxx = a.Sxx, *Syy = a.Syy, *Szz = a.Szz, *Syz = a.Syz, *Sxz = a.Sxz, *Sxy = a.Sxy;
+        w[0 * ntw] = Sxx[e] * M0 * UC * 1e6f;
+        w[1 * ntw] = Syy[e] * M0 * UC * 1e6f;
+        w[2 * ntw] = Szz[e] * M0 * UC * 1e6f;
+        w[3 * ntw] = (Syz[e] + Syz[e - PJ] + Syz[e - 1] + Syz[e - 1 - PJ]) / 4.0f * M0 * UC * 1e6f;
+        w[4 * ntw] = (Sxz[e] + Sxz[e - PI] + Sxz[e - 1] + Sxz[e - 1 - PI]) / 4.0f * M0 * UC * 1e6f;
+        w[5 * ntw] = (Sxy[e] + Sxy[e - PJ] + Sxy[e - PI] + Sxy[e - PI - PJ]) / 4.0f * M0 * UC * 1e6f;
+    }
+    if (a.what & SWPC_WAV_STRAIN) {
+        float *w = a.wav_e + (long long)n * 6 * ntw + (itw - 1);
+        for (int c = 0; c < 6; c++) w[c * ntw] = a.eacc[6 * n + c] * M0 * UC * 1e-3f;
+    }
+}
+
+void launch_wav3d(const Wav3Args &a, cudaStream_t st) {
+    if (a.nst <= 0) return;
+    const int threads = 128;
+    wav3d_kernel<<<(a.nst + threads - 1) / threads, threads, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// kernel__vmax (m_kernel.f90:328-352): max |V(kob+1, i, j)|; |x| of a finite
+// float orders like its bit pattern, so the max is an atomicMax on the bits.
+// ---------------------------------------------------------------------------
+__global__ void vmax3d_kernel(const VmaxArgs a) {
+    const int ni = a.i1 - a.i0 + 1, nj = a.j1 - a.j0 + 1;
+    const long long n = (long long)ni * nj;
+    unsigned int mx = 0, my = 0, mz = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = a.i0 + (int)(t % ni), j = a.j0 + (int)(t / ni);
+        const long long col = col_index(a.g, i, j);
+        const int k = a.kob[col] + 1;
+        const long long e = col * a.g.Kp + (k - 1 + KH);
+        const unsigned int bx = __float_as_uint(fabsf(a.Vx[e]));
+        const unsigned int by = __float_as_uint(fabsf(a.Vy[e]));
+        const unsigned int bz = __float_as_uint(fabsf(a.Vz[e]));
+        mx = max(mx, bx);
+        my = max(my, by);
+        mz = max(mz, bz);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        my = max(my, __shfl_xor_sync(0xffffffffu, my, o));
+        mz = max(mz, __shfl_xor_sync(0xffffffffu, mz, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&a.out[0], mx);
+        atomicMax(&a.out[1], my);
+        atomicMax(&a.out[2], mz);
+    }
+}
+
+void launch_vmax3d(const VmaxArgs &a, cudaStream_t st) {
+    vmax3d_kernel<<<148, 256, 0, st>>>(a);
+}
+
+__global__ void advance_it_kernel(int *d_it) { *d_it = *d_it + 1; }
+void launch_advance_it(int *d_it, cudaStream_t st) { advance_it_kernel<<<1, 1, 0, st>>>(d_it); }
+
+}  // namespace swpc

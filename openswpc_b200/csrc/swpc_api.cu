@@ -1,0 +1,874 @@
+// swpc_api.cu -- C-ABI implementation (include/swpc_gpu.h) for the 3D solver.
+//
+// Host orchestration only: allocation, uploads, coefficient setup in the
+// reference's single-precision expression order, the per-step launch
+// sequence of main.f90:125-144 and its CUDA-graph capture.  No arithmetic of
+// the time step runs on the host.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <set>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "swpc_ctx.h"
+#include "swpc_host.h"
+#include "swpc_kernels.cuh"
+
+using namespace swpc;
+
+namespace swpc {
+
+int set_err(swpc_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_check(swpc_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return 0;
+    return set_err(c, SWPC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+// extern "C" implementations for the 2D codes live in swpc2d_api.cu
+int create_2d(swpc_ctx *c);
+int upload_medium_2d(swpc_ctx *c, const swpc_medium_view *m);
+int absorb_setup_2d(swpc_ctx *c, const float *gxc, const float *gxe, const float *gzc, const float *gze);
+int update_stress_2d(swpc_ctx *c, int mask);
+int update_vel_2d(swpc_ctx *c, int mask);
+int wav_store_2d(swpc_ctx *c, int it, const int *d_it);
+int vmax_2d(swpc_ctx *c, float *out);
+void destroy_2d(swpc_ctx *c);
+
+}  // namespace swpc
+
+#define CK(call)                                               \
+    do {                                                       \
+        int _rc = cuda_check(c, (call), #call);                \
+        if (_rc) return _rc;                                   \
+    } while (0)
+#define RC(call)             \
+    do {                     \
+        int _rc = (call);    \
+        if (_rc) return _rc; \
+    } while (0)
+
+static bool is3d(const swpc_ctx *c) { return c->kind == SWPC_KIND_3D; }
+
+static void invalidate_graph(swpc_ctx *c) {
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// lifetime
+// ---------------------------------------------------------------------------
+extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
+    if (!d || !out) return SWPC_ERR_ARG;
+    *out = nullptr;
+    swpc_ctx *c = new swpc_ctx();
+    c->d = *d;
+    c->kind = d->kind;
+    c->device = d->device;
+    auto fail = [&](int rc) {
+        // keep the context so that swpc_last_error can report the reason
+        *out = c;
+        return rc;
+    };
+    if (d->kind != SWPC_KIND_3D && d->kind != SWPC_KIND_PSV && d->kind != SWPC_KIND_SH)
+        return fail(set_err(c, SWPC_ERR_ARG, "unknown solver kind"));
+    if (d->nx < 4 || d->nz < 4 || (d->kind == SWPC_KIND_3D && d->ny < 4))
+        return fail(set_err(c, SWPC_ERR_ARG, "grid must be at least 4 cells per dimension"));
+    if (d->nm < 0 || d->nm > NM_MAX) return fail(set_err(c, SWPC_ERR_ARG, "nm must be 0..3"));
+    if (d->na < 0 || 2 * d->na >= d->nx || d->na >= d->nz || (d->kind == SWPC_KIND_3D && 2 * d->na >= d->ny))
+        return fail(set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid"));
+    if (d->nt < 1) return fail(set_err(c, SWPC_ERR_ARG, "nt must be positive"));
+    if (!(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0) || (d->kind == SWPC_KIND_3D && !(d->dy > 0)))
+        return fail(set_err(c, SWPC_ERR_ARG, "dx, dy, dz, dt must be positive"));
+    {
+        int rc = cuda_check(c, cudaSetDevice(d->device), "cudaSetDevice");
+        if (rc) return fail(rc);
+        rc = cuda_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (rc) return fail(rc);
+    }
+    const int nx = d->nx, ny = d->kind == SWPC_KIND_3D ? d->ny : 1, nz = d->nz, na = d->na;
+    // kernel region (m_global.f90:349-378) for a single node 1..n
+    c->ibk = (1 <= na) ? na + 1 : 1;
+    c->iek = (nx >= nx - na + 1) ? nx - na : nx;
+    c->jbk = (1 <= na) ? na + 1 : 1;
+    c->jek = (ny >= ny - na + 1) ? ny - na : ny;
+    if (d->kind != SWPC_KIND_3D) { c->jbk = 1; c->jek = 1; }
+    c->kbk = 1;
+    c->kek = nz - na;
+    Geo &g = c->g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.Kp = ((nz + 3 + KH) + 7) / 8 * 8;
+    g.Ip = nx + 6;
+    g.Jp = d->kind == SWPC_KIND_3D ? ny + 6 : 1;
+    g.ncell = (long long)g.Kp * g.Ip * g.Jp;
+    int rc = 0;
+    if (is3d(c)) {
+        for (int q = 0; q < 3 && !rc; q++) rc = dalloc(c, &c->V[q], g.ncell);
+        for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, &c->S[q], g.ncell);
+        for (int comp = 0; comp < 6 && !rc; comp++)
+            for (int m = 0; m < d->nm && !rc; m++) rc = dalloc(c, &c->R[comp * 3 + m], g.ncell);
+        for (int q = 1; q < 11 && !rc; q++) rc = dalloc(c, &c->med[q], g.ncell);
+        const long long ncol = (long long)g.Ip * g.Jp;
+        if (!rc) rc = dalloc(c, &c->band, ncol);
+        if (!rc) rc = dalloc(c, &c->pmlcol, ncol);
+        if (!rc) rc = dalloc(c, &c->kob, ncol);
+        if (!rc) rc = dalloc(c, &c->kfs, ncol);
+    } else {
+        rc = create_2d(c);
+    }
+    if (!rc) rc = dalloc(c, &c->vmax_buf, 4);
+    if (!rc) rc = dalloc(c, &c->d_it, 1);
+    if (!rc) rc = cuda_check(c, cudaMallocHost((void **)&c->h_vmax, 4 * sizeof(unsigned int)), "cudaMallocHost");
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    if (rc) return fail(rc);
+    *out = c;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_destroy(swpc_ctx *c) {
+    if (!c) return SWPC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    invalidate_graph(c);
+    if (!is3d(c)) destroy_2d(c);
+    void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
+                  c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
+                  c->wav[1], c->wav[2], c->wav[3], c->uacc, c->eacc, c->vmax_buf, c->d_it};
+    for (void *p : ps) if (p) cudaFree(p);
+    for (auto p : c->S) if (p) cudaFree(p);
+    for (auto p : c->R) if (p) cudaFree(p);
+    for (auto p : c->med) if (p) cudaFree(p);
+    for (auto p : c->aux) if (p) cudaFree(p);
+    for (int q = 0; q < 2; q++) {
+        if (c->gx[q]) cudaFree(c->gx[q]);
+        if (c->gy[q]) cudaFree(c->gy[q]);
+        if (c->gz[q]) cudaFree(c->gz[q]);
+    }
+    if (c->h_vmax) cudaFreeHost(c->h_vmax);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SWPC_OK;
+}
+
+extern "C" const char *swpc_last_error(const swpc_ctx *c) { return c ? c->err.c_str() : "null context"; }
+extern "C" void *swpc_stream(swpc_ctx *c) { return c ? (void *)c->stream : nullptr; }
+extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes : 0; }
+
+extern "C" int swpc_sync(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion between the Fortran memory box and the device columns
+// ---------------------------------------------------------------------------
+namespace swpc {
+
+// host (k, i, j) Fortran array over k in [-2, nz+3+], i in [-2, nx+3+], j in
+// [-2, ny+3+] with leading extents ld_k, ld_i  <->  device column layout.
+int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i) {
+    const Geo &g = c->g;
+    const int nkb = g.nz + 6;             // k = -2 .. nz+3
+    const int nib = g.nx + 6;             // i = -2 .. nx+3
+    const int njb = is3d(c) ? g.ny + 6 : 1;
+    if (ld_k < nkb || ld_i < nib) return set_err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    const size_t dpitch = (size_t)g.Kp * sizeof(float);
+    const size_t hpitch = (size_t)ld_k * sizeof(float);
+    const size_t width = (size_t)nkb * sizeof(float);
+    const int koff = -2 - 1 + KH;         // device offset of k = -2 within a column
+    for (int jj = 0; jj < njb; jj++) {
+        float *dcol = dev + ((long long)jj * g.Ip) * g.Kp + koff;
+        const long long hoff = (long long)jj * ld_i * ld_k;
+        cudaError_t e;
+        if (host_in)
+            e = cudaMemcpy2DAsync(dcol, dpitch, host_in + hoff, hpitch, width, nib, cudaMemcpyHostToDevice, c->stream);
+        else
+            e = cudaMemcpy2DAsync(host_out + hoff, hpitch, dcol, dpitch, width, nib, cudaMemcpyDeviceToHost, c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cudaMemcpy2DAsync");
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
+}  // namespace swpc
+
+// ---------------------------------------------------------------------------
+// medium, coefficients, absorber
+// ---------------------------------------------------------------------------
+extern "C" int swpc_upload_medium(swpc_ctx *c, const swpc_medium_view *m) {
+    if (!c || !m) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    if (!is3d(c)) return upload_medium_2d(c, m);
+    const Geo &g = c->g;
+    const float *src[11] = {m->rho, m->lam, m->mu, m->taup, m->taus, m->bx, m->by, m->bz, m->muyz, m->muxz, m->muxy};
+    for (int q = 1; q < 11; q++) {
+        if (!src[q]) return set_err(c, SWPC_ERR_ARG, "medium field missing");
+        RC(copy_box(c, c->med[q], src[q], nullptr, m->ld_k, m->ld_i));
+    }
+    if (!m->kfs || !m->kob || !m->kfs_top || !m->kfs_bot || !m->kob_top || !m->kob_bot || !m->kbeg_a)
+        return set_err(c, SWPC_ERR_ARG, "integer map missing");
+    if (m->ld_i2 < g.nx + 6) return set_err(c, SWPC_ERR_ARG, "ld_i2 smaller than the memory box");
+    const long long ncol = (long long)g.Ip * g.Jp;
+    std::vector<int4> band(ncol, make_int4(0, 0, 0, 0));
+    std::vector<int> kob(ncol, 0), kfs(ncol, 0);
+    c->h_kbeg_a.assign(ncol, 0);
+    for (int j = -2; j <= g.ny + 3; j++)
+        for (int i = -2; i <= g.nx + 3; i++) {
+            const long long h = (long long)(j + 2) * m->ld_i2 + (i + 2);
+            const long long cc = col_index(g, i, j);
+            band[cc] = make_int4(m->kfs_top[h], m->kfs_bot[h], m->kob_top[h], m->kob_bot[h]);
+            kob[cc] = m->kob[h];
+            kfs[cc] = m->kfs[h];
+            c->h_kbeg_a[cc] = m->kbeg_a[h];
+        }
+    // the fused kernels assume kbeg_a = 1 on side columns and kend_k + 1 under
+    // the interior box (m_global.f90:336-345); reject anything else.
+    for (int j = 1; j <= g.ny; j++)
+        for (int i = 1; i <= g.nx; i++) {
+            const bool inner = i >= c->ibk && i <= c->iek && j >= c->jbk && j <= c->jek;
+            const int want = inner ? c->kek + 1 : 1;
+            if (c->h_kbeg_a[col_index(g, i, j)] != want)
+                return set_err(c, SWPC_ERR_ARG, "kbeg_a map does not match the absorber layout of m_global.f90:336-345");
+        }
+    CK(cudaMemcpyAsync(c->band, band.data(), ncol * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->kob, kob.data(), ncol * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->kfs, kfs.data(), ncol * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->medium_ready = true;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_kernel_setup(swpc_ctx *c, const float *ts) {
+    if (!c) return SWPC_ERR_ARG;
+    if (c->d.nm > 0 && !ts) return set_err(c, SWPC_ERR_ARG, "ts required for nm > 0");
+    invalidate_graph(c);
+    // m_kernel.f90:43-54 in real(MP) = single precision
+    const float dd[3] = {c->d.dx, c->d.dy, c->d.dz};
+    for (int ax = 0; ax < 3; ax++) {
+        const float rc40 = 17.0f / 16.0f / dd[ax];
+        const float rc41 = 1.0f / 48.0f / dd[ax];
+        const float rd40 = -1.0f / 16.0f / dd[ax];
+        const float rd41 = -1.0f / 48.0f / dd[ax];
+        // isign = -1 (4th order) and +1 (2nd-order band): rc + isign*rd
+        c->e40[ax][0] = rc40 + (-1.0f) * rd40;
+        c->e41[ax][0] = rc41 + (-1.0f) * rd41;
+        c->e40[ax][1] = rc40 + (1.0f) * rd40;
+        c->e41[ax][1] = rc41 + (1.0f) * rd41;
+        c->r20[ax] = 1.0f / dd[ax];                       // m_absorb_p.f90:70-72
+        c->r40[ax] = 9.0f / 8.0f / dd[ax];                // m_wav.f90:130-135
+        c->r41[ax] = 1.0f / 24.0f / dd[ax];
+    }
+    // m_kernel.f90:58-67 in real(SP)
+    const int nm = c->d.nm;
+    const float dt = c->d.dt;
+    for (int m = 0; m < NM_MAX; m++) { c->c1[m] = c->c2[m] = c->d1[m] = 0.f; c->ts[m] = 0.f; }
+    c->d2 = 0.f;
+    if (nm > 0) {
+        for (int m = 0; m < nm; m++) {
+            c->ts[m] = ts[m];
+            c->c1[m] = (2 * ts[m] - dt) / (2 * ts[m] + dt);
+            c->c2[m] = (2) / (2 * ts[m] + dt) / nm;
+        }
+        float d2 = 0.0f;
+        for (int m = 0; m < nm; m++) d2 = d2 + dt / (2 * ts[m] - dt);
+        c->d2 = d2 / nm;
+        for (int m = 0; m < nm; m++) c->d1[m] = 2 * ts[m] / (2 * ts[m] - dt);
+    }
+    c->kernel_ready = true;
+    return SWPC_OK;
+}
+
+static int upload_profile(swpc_ctx *c, float4 **dst, const float *g4, int n) {
+    if (!g4) return set_err(c, SWPC_ERR_ARG, "damping profile missing");
+    if (!*dst) RC(dalloc(c, dst, n));
+    std::vector<float4> v(n);
+    for (int q = 0; q < n; q++) v[q] = make_float4(g4[4 * q], g4[4 * q + 1], g4[4 * q + 2], g4[4 * q + 3]);
+    CK(cudaMemcpyAsync(*dst, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_absorb_setup(swpc_ctx *c, const float *gxc, const float *gxe, const float *gyc, const float *gye,
+                                 const float *gzc, const float *gze) {
+    if (!c) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    if (!c->medium_ready) return set_err(c, SWPC_ERR_STATE, "swpc_upload_medium must precede swpc_absorb_setup");
+    if (!is3d(c)) return absorb_setup_2d(c, gxc, gxe, gzc, gze);
+    const Geo &g = c->g;
+    RC(upload_profile(c, &c->gx[0], gxc, g.nx));
+    RC(upload_profile(c, &c->gx[1], gxe, g.nx));
+    RC(upload_profile(c, &c->gy[0], gyc, g.ny));
+    RC(upload_profile(c, &c->gy[1], gye, g.ny));
+    RC(upload_profile(c, &c->gz[0], gzc, g.nz));
+    RC(upload_profile(c, &c->gz[1], gze, g.nz));
+    // compact auxiliary storage: one contiguous k-run per absorber column,
+    // each run starting on a 32-byte boundary
+    const long long ncol = (long long)g.Ip * g.Jp;
+    std::vector<int2> pc(ncol, make_int2(1, -1));
+    long long base = 0;
+    for (int j = 1; j <= g.ny; j++)
+        for (int i = 1; i <= g.nx; i++) {
+            const long long cc = col_index(g, i, j);
+            const int kb = c->h_kbeg_a[cc];
+            const int len = g.nz - kb + 1;
+            if (len <= 0) continue;
+            if (base + len > 0x7fffffffLL) return set_err(c, SWPC_ERR_ARG, "absorber region too large");
+            pc[cc] = make_int2(kb, (int)base);
+            base += (len + 7) / 8 * 8;
+        }
+    c->npml = base;
+    for (int q = 0; q < 18; q++) {
+        if (c->aux[q]) { cudaFree(c->aux[q]); c->aux[q] = nullptr; }
+        RC(dalloc(c, &c->aux[q], (size_t)std::max<long long>(base, 1)));
+    }
+    CK(cudaMemcpyAsync(c->pmlcol, pc.data(), ncol * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->absorb_ready = true;
+    return SWPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sources
+// ---------------------------------------------------------------------------
+// ghost cells that global__comm_stress / global__comm_vel overwrite with zero
+// on a single node (m_global.f90:460-490, 571-603)
+static bool comm_zeroed(const swpc_ctx *c, int field, int k, int i, int j) {
+    const int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
+    if (k < 1 || k > nz) return false;
+    const bool jin = (j >= 1 && j <= ny), iin = (i >= 1 && i <= nx);
+    auto in = [](int v, std::initializer_list<int> s) { return std::find(s.begin(), s.end(), v) != s.end(); };
+    switch (field) {
+    case SWPC_F_VX: return (jin && in(i, {-1, 0, nx + 1})) || (iin && in(j, {0, ny + 1, ny + 2}));
+    case SWPC_F_VY: return (jin && in(i, {0, nx + 1, nx + 2})) || (iin && in(j, {-1, 0, ny + 1}));
+    case SWPC_F_VZ: return (jin && in(i, {0, nx + 1, nx + 2})) || (iin && in(j, {0, ny + 1, ny + 2}));
+    case SWPC_F_SXX: return jin && in(i, {0, nx + 1, nx + 2});
+    case SWPC_F_SYY: return iin && in(j, {0, ny + 1, ny + 2});
+    case SWPC_F_SXY: return (jin && in(i, {-1, 0, nx + 1})) || (iin && in(j, {-1, 0, ny + 1}));
+    case SWPC_F_SXZ: return jin && in(i, {-1, 0, nx + 1});
+    case SWPC_F_SYZ: return iin && in(j, {-1, 0, ny + 1});
+    default: return false;
+    }
+}
+
+static int build_list(swpc_ctx *c, std::vector<InjEntry> &v, InjEntry **dptr, int *nout, bool *serial) {
+    std::set<std::pair<int, long long>> seen;
+    bool dup = false;
+    for (auto &e : v)
+        if (!seen.insert({e.field, e.cell}).second) dup = true;
+    *serial = dup;
+    *nout = (int)v.size();
+    if (*dptr) { cudaFree(*dptr); *dptr = nullptr; }
+    RC(dalloc(c, dptr, v.size()));
+    if (!v.empty()) CK(cudaMemcpyAsync(*dptr, v.data(), v.size() * sizeof(InjEntry), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+static bool in_box(const swpc_ctx *c, int k, int i, int j) {
+    const Geo &g = c->g;
+    const int jlo = is3d(c) ? -2 : 1, jhi = is3d(c) ? g.ny + 3 : 1;
+    return k >= 1 - KH + 1 && k <= g.nz + 3 && i >= -2 && i <= g.nx + 3 && j >= jlo && j <= jhi;
+}
+
+static void add_entry(const swpc_ctx *c, std::vector<InjEntry> &v, int field, int k, int i, int j, int src, float coef,
+                      int mode, int bfield, bool *bad) {
+    if (!in_box(c, k, i, j)) { *bad = true; return; }
+    if (is3d(c) && comm_zeroed(c, field, k, i, j)) return;   // zeroed before anything reads it
+    InjEntry e;
+    e.cell = is3d(c) ? cell_index(c->g, k, i, j) : (long long)(i + 2) * c->g.Kp + (k - 1 + KH);
+    e.field = field; e.src = src; e.coef = coef; e.mode = mode; e.bfield = bfield; e.pad = 0;
+    v.push_back(e);
+}
+
+static int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half) {
+    const int nt = c->d.nt;
+    std::vector<float> t((size_t)nt * std::max(nsrc, 1), 0.f);
+    for (int it = 1; it <= nt; it++) {
+        // m_source.f90:800 (half step) and :857
+        const float tt = half ? c->d.tbeg + ((float)it - 0.5f) * c->d.dt : c->d.tbeg + (float)it * c->d.dt;
+        for (int s = 0; s < nsrc; s++) t[(size_t)(it - 1) * nsrc + s] = momentrate(tt, stftype, srcprm[2 * s], srcprm[2 * s + 1]);
+    }
+    if (*dst) { cudaFree(*dst); *dst = nullptr; }
+    RC(dalloc(c, dst, t.size()));
+    CK(cudaMemcpyAsync(*dst, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_source_setup(swpc_ctx *c, int nsrc, const int *isrc, const int *jsrc, const int *ksrc,
+                                 const float *srcprm, const float *mo, const float *m6, int stftype) {
+    if (!c || nsrc < 0) return SWPC_ERR_ARG;
+    if (nsrc > 0 && (!isrc || !ksrc || !srcprm || !mo || !m6 || (is3d(c) && !jsrc)))
+        return set_err(c, SWPC_ERR_ARG, "source arrays missing");
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    std::vector<InjEntry> v;
+    bool bad = false;
+    for (int s = 0; s < nsrc; s++) {
+        const int ii = isrc[s], jj = is3d(c) ? jsrc[s] : 1, kk = ksrc[s];
+        const float *mm = m6 + 6 * s;   // xx yy zz yz xz xy
+        if (is3d(c)) {
+            // m_source.f90:807-824
+            add_entry(c, v, SWPC_F_SXX, kk, ii, jj, s, mm[0], INJ_GLUT, 0, &bad);
+            add_entry(c, v, SWPC_F_SYY, kk, ii, jj, s, mm[1], INJ_GLUT, 0, &bad);
+            add_entry(c, v, SWPC_F_SZZ, kk, ii, jj, s, mm[2], INJ_GLUT, 0, &bad);
+            add_entry(c, v, SWPC_F_SXY, kk, ii, jj, s, mm[5], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXY, kk, ii, jj - 1, s, mm[5], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXY, kk, ii - 1, jj, s, mm[5], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXY, kk, ii - 1, jj - 1, s, mm[5], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk, ii, jj, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk - 1, ii, jj, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk, ii - 1, jj, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk - 1, ii - 1, jj, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk, ii, jj, s, mm[3], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk - 1, ii, jj, s, mm[3], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk, ii, jj - 1, s, mm[3], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk - 1, ii, jj - 1, s, mm[3], INJ_GLUT4, 0, &bad);
+        } else if (c->kind == SWPC_KIND_PSV) {
+            // src/swpc_psv/m_source.f90:601-606: Sxx, Szz, and Sxz at 4 cells
+            add_entry(c, v, SWPC_F_SXX, kk, ii, 1, s, mm[0], INJ_GLUT, 0, &bad);
+            add_entry(c, v, SWPC_F_SZZ, kk, ii, 1, s, mm[2], INJ_GLUT, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk, ii, 1, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk - 1, ii, 1, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk, ii - 1, 1, s, mm[4], INJ_GLUT4, 0, &bad);
+            add_entry(c, v, SWPC_F_SXZ, kk - 1, ii - 1, 1, s, mm[4], INJ_GLUT4, 0, &bad);
+        } else {
+            // src/swpc_sh/m_source.f90:583-587: Sxy and Syz at 2 cells each
+            add_entry(c, v, SWPC_F_SXY, kk, ii, 1, s, mm[5], INJ_GLUT2, 0, &bad);
+            add_entry(c, v, SWPC_F_SXY, kk, ii - 1, 1, s, mm[5], INJ_GLUT2, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk, ii, 1, s, mm[3], INJ_GLUT2, 0, &bad);
+            add_entry(c, v, SWPC_F_SYZ, kk - 1, ii, 1, s, mm[3], INJ_GLUT2, 0, &bad);
+        }
+    }
+    if (bad) return set_err(c, SWPC_ERR_ARG, "source cell outside the memory box");
+    RC(build_list(c, v, &c->inj_glut, &c->ninj_glut, &c->glut_serial));
+    c->nsrc_glut = nsrc;
+    RC(stime_table(c, &c->stime_glut, nsrc, srcprm, stftype, true));
+    if (c->mo_glut) { cudaFree(c->mo_glut); c->mo_glut = nullptr; }
+    RC(dalloc(c, &c->mo_glut, std::max(nsrc, 1)));
+    if (nsrc > 0) CK(cudaMemcpyAsync(c->mo_glut, mo, nsrc * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // dt_dxyz = dt / (dx * dy * dz) (m_source.f90:305); 2D: dt / (dx * dz)
+    c->dt_dxyz = is3d(c) ? c->d.dt / (c->d.dx * c->d.dy * c->d.dz) : c->d.dt / (c->d.dx * c->d.dz);
+    return SWPC_OK;
+}
+
+extern "C" int swpc_bodyforce_setup(swpc_ctx *c, int nsrc, const int *isrc, const int *jsrc, const int *ksrc,
+                                    const float *srcprm, const float *f3, int stftype) {
+    if (!c || nsrc < 0) return SWPC_ERR_ARG;
+    if (nsrc > 0 && (!isrc || !ksrc || !srcprm || !f3 || (is3d(c) && !jsrc)))
+        return set_err(c, SWPC_ERR_ARG, "body-force arrays missing");
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "2D body forces use swpc_bodyforce_setup_2d");
+    std::vector<InjEntry> v;
+    bool bad = false;
+    for (int s = 0; s < nsrc; s++) {
+        const int ii = isrc[s], jj = jsrc[s], kk = ksrc[s];
+        const float *f = f3 + 3 * s;
+        // m_source.f90:863-868 (buoyancy slots: 0 bx, 1 by, 2 bz)
+        add_entry(c, v, SWPC_F_VX, kk, ii, jj, s, f[0], INJ_BF3, 0, &bad);
+        add_entry(c, v, SWPC_F_VX, kk, ii - 1, jj, s, f[0], INJ_BF3, 0, &bad);
+        add_entry(c, v, SWPC_F_VY, kk, ii, jj, s, f[1], INJ_BF3, 1, &bad);
+        add_entry(c, v, SWPC_F_VY, kk, ii, jj - 1, s, f[1], INJ_BF3, 1, &bad);
+        add_entry(c, v, SWPC_F_VZ, kk, ii, jj, s, f[2], INJ_BF3, 2, &bad);
+        add_entry(c, v, SWPC_F_VZ, kk - 1, ii, jj, s, f[2], INJ_BF3, 2, &bad);
+    }
+    if (bad) return set_err(c, SWPC_ERR_ARG, "body-force cell outside the memory box");
+    RC(build_list(c, v, &c->inj_bf, &c->ninj_bf, &c->bf_serial));
+    c->nsrc_bf = nsrc;
+    RC(stime_table(c, &c->stime_bf, nsrc, srcprm, stftype, false));
+    c->dt_dxyz = c->d.dt / (c->d.dx * c->d.dy * c->d.dz);
+    return SWPC_OK;
+}
+
+extern "C" int swpc_green_setup(swpc_ctx *c, int isrc, int jsrc, int ksrc, char cmp, float green_tbeg,
+                                float green_trise, int stftype) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "green mode is a 3D feature (m_green.f90)");
+    if (cmp != 'x' && cmp != 'y' && cmp != 'z') return set_err(c, SWPC_ERR_ARG, "green_cmp must be x, y or z");
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    // m_green.f90:146-154
+    const float f1[3] = {cmp == 'x' ? 1.0f : 0.0f, cmp == 'y' ? 1.0f : 0.0f, cmp == 'z' ? 1.0f : 0.0f};
+    std::vector<InjEntry> v;
+    bool bad = false;
+    add_entry(c, v, SWPC_F_VX, ksrc, isrc, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
+    add_entry(c, v, SWPC_F_VX, ksrc, isrc - 1, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
+    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc, 0, f1[1], INJ_GREEN, 1, &bad);
+    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc - 1, 0, f1[1], INJ_GREEN, 1, &bad);
+    add_entry(c, v, SWPC_F_VZ, ksrc, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
+    add_entry(c, v, SWPC_F_VZ, ksrc - 1, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
+    if (bad) return set_err(c, SWPC_ERR_ARG, "green source cell outside the memory box");
+    bool serial;
+    RC(build_list(c, v, &c->inj_green, &c->ninj_green, &serial));
+    const float prm[2] = {green_tbeg, green_trise};
+    RC(stime_table(c, &c->stf_green, 1, prm, stftype, false));
+    c->green_dt_dxyz = c->d.dt / (c->d.dx * c->d.dy * c->d.dz);
+    c->green = true;
+    return SWPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// recorder
+// ---------------------------------------------------------------------------
+extern "C" int swpc_wav_setup(swpc_ctx *c, int nst, const int *ist, const int *jst, const int *kst, int ntdec_w,
+                              int what, float M0, float UC) {
+    if (!c || nst < 0 || ntdec_w < 1) return SWPC_ERR_ARG;
+    if (nst > 0 && (!ist || !kst || (is3d(c) && !jst))) return set_err(c, SWPC_ERR_ARG, "station arrays missing");
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    const Geo &g = c->g;
+    std::vector<int> st(3 * (size_t)std::max(nst, 1), 0);
+    for (int n = 0; n < nst; n++) {
+        const int i = ist[n], j = is3d(c) ? jst[n] : 1, k = kst[n];
+        // stencils of wav__store reach i-2..i+2, j-2..j+2, k-2..k+2
+        if (i < 1 || i > g.nx || k < 1 || k > g.nz || (is3d(c) && (j < 1 || j > g.ny)))
+            return set_err(c, SWPC_ERR_ARG, "station cell outside the domain");
+        st[3 * n] = i; st[3 * n + 1] = j; st[3 * n + 2] = k;
+    }
+    c->nst = nst;
+    c->ntdec_w = ntdec_w;
+    c->wav_what = what;
+    c->M0 = M0;
+    c->UC = UC;
+    // ntw = floor(real(nt-1)/real(ntdec_w) + 1.0) (m_wav.f90:92)
+    c->ntw = (int)floorf((float)(c->d.nt - 1) / (float)ntdec_w + 1.0f);
+    if (c->st_ijk) { cudaFree(c->st_ijk); c->st_ijk = nullptr; }
+    RC(dalloc(c, &c->st_ijk, st.size()));
+    CK(cudaMemcpyAsync(c->st_ijk, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    const int ncmp[4] = {3, 3, is3d(c) ? 6 : 3, is3d(c) ? 6 : 3};
+    for (int q = 0; q < 4; q++) {
+        if (c->wav[q]) { cudaFree(c->wav[q]); c->wav[q] = nullptr; }
+        RC(dalloc(c, &c->wav[q], (size_t)c->ntw * ncmp[q] * std::max(nst, 1)));
+    }
+    if (c->uacc) { cudaFree(c->uacc); c->uacc = nullptr; }
+    if (c->eacc) { cudaFree(c->eacc); c->eacc = nullptr; }
+    RC(dalloc(c, &c->uacc, 3 * (size_t)std::max(nst, 1)));
+    RC(dalloc(c, &c->eacc, 6 * (size_t)std::max(nst, 1)));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_wav_dims(const swpc_ctx *c, int *ntw, int *nst) {
+    if (!c) return SWPC_ERR_ARG;
+    if (ntw) *ntw = c->ntw;
+    if (nst) *nst = c->nst;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_wav_fetch(swpc_ctx *c, int what, float *out) {
+    if (!c || !out) return SWPC_ERR_ARG;
+    int q = what == SWPC_WAV_V ? 0 : what == SWPC_WAV_U ? 1 : what == SWPC_WAV_STRESS ? 2 : what == SWPC_WAV_STRAIN ? 3 : -1;
+    if (q < 0) return set_err(c, SWPC_ERR_ARG, "unknown recorder component");
+    if (!c->wav[q]) return set_err(c, SWPC_ERR_STATE, "swpc_wav_setup not called");
+    const int ncmp[4] = {3, 3, is3d(c) ? 6 : 3, is3d(c) ? 6 : 3};
+    CK(cudaMemcpyAsync(out, c->wav[q], (size_t)c->ntw * ncmp[q] * c->nst * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the time step
+// ---------------------------------------------------------------------------
+static int check_ready(swpc_ctx *c) {
+    if (!c->medium_ready) return set_err(c, SWPC_ERR_STATE, "swpc_upload_medium not called");
+    if (!c->kernel_ready) return set_err(c, SWPC_ERR_STATE, "swpc_kernel_setup not called");
+    if (!c->absorb_ready && c->d.na > 0) return set_err(c, SWPC_ERR_STATE, "swpc_absorb_setup not called");
+    return SWPC_OK;
+}
+
+static void fill_geo_common(const swpc_ctx *c, Geo &g, int &ibk, int &iek, int &jbk, int &jek, int &kek) {
+    g = c->g; ibk = c->ibk; iek = c->iek; jbk = c->jbk; jek = c->jek; kek = c->kek;
+}
+
+static int launch_stress(swpc_ctx *c, int mask) {
+    RC(check_ready(c));
+    if (!is3d(c)) return update_stress_2d(c, mask);
+    Str3Args a;
+    memset(&a, 0, sizeof(a));
+    fill_geo_common(c, a.g, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
+    a.Sxx = c->S[0]; a.Syy = c->S[1]; a.Szz = c->S[2]; a.Syz = c->S[3]; a.Sxz = c->S[4]; a.Sxy = c->S[5];
+    for (int q = 0; q < 18; q++) a.R[q] = c->R[q];
+    a.lam = c->med[1]; a.mu = c->med[2]; a.taup = c->med[3]; a.taus = c->med[4];
+    a.muyz = c->med[8]; a.muxz = c->med[9]; a.muxy = c->med[10];
+    a.band = c->band; a.pmlcol = c->pmlcol;
+    for (int q = 0; q < 9; q++) a.aV[q] = c->aux[q];
+    a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+    memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+    memcpy(a.c1, c->c1, sizeof(a.c1)); memcpy(a.c2, c->c2, sizeof(a.c2)); memcpy(a.d1, c->d1, sizeof(a.d1));
+    a.d2 = c->d2;
+    a.dt = c->d.dt;
+    a.mask = (c->d.na > 0) ? mask : (mask & 1);
+    dim3 block(32, c->bi, c->bj);
+    dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
+    launch_stress3d(a, c->d.nm, grid, block, c->stream);
+    return cuda_check(c, cudaGetLastError(), "stress3d launch");
+}
+
+static int launch_vel(swpc_ctx *c, int mask) {
+    RC(check_ready(c));
+    if (!is3d(c)) return update_vel_2d(c, mask);
+    Vel3Args a;
+    memset(&a, 0, sizeof(a));
+    fill_geo_common(c, a.g, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
+    a.Sxx = c->S[0]; a.Syy = c->S[1]; a.Szz = c->S[2]; a.Syz = c->S[3]; a.Sxz = c->S[4]; a.Sxy = c->S[5];
+    a.bx = c->med[5]; a.by = c->med[6]; a.bz = c->med[7];
+    a.band = c->band; a.pmlcol = c->pmlcol;
+    for (int q = 0; q < 9; q++) a.aS[q] = c->aux[9 + q];
+    a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+    memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+    a.dt = c->d.dt;
+    a.mask = (c->d.na > 0) ? mask : (mask & 1);
+    dim3 block(32, c->bi, c->bj);
+    dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
+    launch_vel3d(a, grid, block, c->stream);
+    return cuda_check(c, cudaGetLastError(), "vel3d launch");
+}
+
+static void fill_inj_fields(swpc_ctx *c, InjArgs &a) {
+    for (int q = 0; q < 3; q++) a.fields[q] = c->V[q];
+    for (int q = 0; q < 6; q++) a.fields[3 + q] = c->S[q];
+    if (is3d(c)) { a.bfields[0] = c->med[5]; a.bfields[1] = c->med[6]; a.bfields[2] = c->med[7]; }
+    else { a.bfields[0] = c->med[0]; a.bfields[1] = c->med[0]; a.bfields[2] = c->med[0]; }
+}
+
+static int launch_glut(swpc_ctx *c, int it, const int *d_it) {
+    if (c->ninj_glut <= 0) return SWPC_OK;
+    InjArgs a;
+    memset(&a, 0, sizeof(a));
+    a.list = c->inj_glut; a.n = c->ninj_glut; a.serial = c->glut_serial ? 1 : 0;
+    a.it = it; a.d_it = d_it; a.nt = c->d.nt; a.nsrc = c->nsrc_glut;
+    a.stime = c->stime_glut; a.mo = c->mo_glut; a.dt_dxyz = c->dt_dxyz;
+    fill_inj_fields(c, a);
+    launch_inject(a, c->stream);
+    return cuda_check(c, cudaGetLastError(), "stressglut launch");
+}
+
+static int launch_bf(swpc_ctx *c, int it, const int *d_it) {
+    if (c->ninj_bf <= 0) return SWPC_OK;
+    InjArgs a;
+    memset(&a, 0, sizeof(a));
+    a.list = c->inj_bf; a.n = c->ninj_bf; a.serial = c->bf_serial ? 1 : 0;
+    a.it = it; a.d_it = d_it; a.nt = c->d.nt; a.nsrc = c->nsrc_bf;
+    a.stime = c->stime_bf; a.dt_dxyz = c->dt_dxyz;
+    a.rho_cell = c->rho_cell_bf;
+    fill_inj_fields(c, a);
+    launch_inject(a, c->stream);
+    return cuda_check(c, cudaGetLastError(), "bodyforce launch");
+}
+
+static int launch_green(swpc_ctx *c, int it, const int *d_it) {
+    if (!c->green || c->ninj_green <= 0) return SWPC_OK;
+    InjArgs a;
+    memset(&a, 0, sizeof(a));
+    a.list = c->inj_green; a.n = c->ninj_green; a.serial = 0;
+    a.it = it; a.d_it = d_it; a.nt = c->d.nt; a.nsrc = 1;
+    a.stime = c->stf_green; a.dt_dxyz = c->green_dt_dxyz;
+    fill_inj_fields(c, a);
+    launch_inject(a, c->stream);
+    return cuda_check(c, cudaGetLastError(), "green launch");
+}
+
+static int launch_wav(swpc_ctx *c, int it, const int *d_it) {
+    if (c->nst <= 0 || c->wav_what == 0) return SWPC_OK;
+    if (!is3d(c)) return wav_store_2d(c, it, d_it);
+    Wav3Args a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->g; a.nst = c->nst; a.ntw = c->ntw; a.ntdec_w = c->ntdec_w; a.what = c->wav_what;
+    a.it = it; a.d_it = d_it; a.st = c->st_ijk;
+    a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
+    a.Sxx = c->S[0]; a.Syy = c->S[1]; a.Szz = c->S[2]; a.Syz = c->S[3]; a.Sxz = c->S[4]; a.Sxy = c->S[5];
+    a.uacc = c->uacc; a.eacc = c->eacc;
+    a.wav_v = c->wav[0]; a.wav_u = c->wav[1]; a.wav_s = c->wav[2]; a.wav_e = c->wav[3];
+    a.M0 = c->M0; a.UC = c->UC; a.dt = c->d.dt;
+    memcpy(a.r40, c->r40, sizeof(a.r40)); memcpy(a.r41, c->r41, sizeof(a.r41));
+    // outside sampling steps the kernel only integrates u / strain
+    if (!d_it && (it - 1) % c->ntdec_w != 0 && !(c->wav_what & (SWPC_WAV_U | SWPC_WAV_STRAIN))) return SWPC_OK;
+    launch_wav3d(a, c->stream);
+    return cuda_check(c, cudaGetLastError(), "wav launch");
+}
+
+extern "C" int swpc_kernel_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 1) : SWPC_ERR_ARG; }
+extern "C" int swpc_absorb_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 2) : SWPC_ERR_ARG; }
+extern "C" int swpc_kernel_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 1) : SWPC_ERR_ARG; }
+extern "C" int swpc_absorb_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 2) : SWPC_ERR_ARG; }
+extern "C" int swpc_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 3) : SWPC_ERR_ARG; }
+extern "C" int swpc_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 3) : SWPC_ERR_ARG; }
+extern "C" int swpc_source_stressglut(swpc_ctx *c, int it) { return c ? launch_glut(c, it, nullptr) : SWPC_ERR_ARG; }
+extern "C" int swpc_source_bodyforce(swpc_ctx *c, int it) { return c ? launch_bf(c, it, nullptr) : SWPC_ERR_ARG; }
+extern "C" int swpc_green_source(swpc_ctx *c, int it) { return c ? launch_green(c, it, nullptr) : SWPC_ERR_ARG; }
+extern "C" int swpc_comm_stress(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
+extern "C" int swpc_comm_vel(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
+extern "C" int swpc_wav_store(swpc_ctx *c, int it) { return c ? launch_wav(c, it, nullptr) : SWPC_ERR_ARG; }
+
+// main.f90:125-144 loop body (report__progress and snap__write are driven
+// by the caller between steps)
+static int step_body(swpc_ctx *c, int it, const int *d_it) {
+    RC(launch_wav(c, it, d_it));
+    RC(launch_stress(c, 3));
+    RC(launch_glut(c, it, d_it));
+    RC(launch_vel(c, 3));
+    RC(launch_bf(c, it, d_it));
+    RC(launch_green(c, it, d_it));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_step(swpc_ctx *c, int it) {
+    if (!c) return SWPC_ERR_ARG;
+    if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
+    CK(cudaSetDevice(c->device));
+    return step_body(c, it, nullptr);
+}
+
+static int build_graph(swpc_ctx *c) {
+    if (c->graph_exec) return SWPC_OK;
+    RC(check_ready(c));
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = step_body(c, 0, c->d_it);
+    if (!rc) launch_advance_it(c->d_it, c->stream);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc) return rc;
+    CK(e);
+    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    return SWPC_OK;
+}
+
+extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
+    if (!c) return SWPC_ERR_ARG;
+    if (nsteps <= 0) return SWPC_OK;
+    if (it0 < 1 || it0 + nsteps - 1 > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time steps outside 1..nt");
+    CK(cudaSetDevice(c->device));
+    RC(build_graph(c));
+    CK(cudaMemcpyAsync(c->d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    for (int n = 0; n < nsteps; n++) CK(cudaGraphLaunch(c->graph_exec, c->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_time_steps(swpc_ctx *c, int it0, int nsteps, float *ms) {
+    if (!c || !ms) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    RC(build_graph(c));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventRecord(e0, c->stream));
+    int rc = swpc_run(c, it0, nsteps);
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// report: kernel__vmax + divergence check (m_report.f90:134-152)
+// ---------------------------------------------------------------------------
+extern "C" int swpc_vmax(swpc_ctx *c, float out[3]) {
+    if (!c || !out) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    if (!c->medium_ready) return set_err(c, SWPC_ERR_STATE, "swpc_upload_medium not called");
+    if (!is3d(c)) {
+        RC(vmax_2d(c, out));
+    } else {
+        const int margin = 5, na = c->d.na;
+        VmaxArgs a;
+        a.g = c->g;
+        a.j0 = std::max(na + margin + 1, c->jbk);
+        a.j1 = std::min(c->g.ny - na - margin, c->jek);
+        a.i0 = std::max(na + margin + 1, c->ibk);
+        a.i1 = std::min(c->g.nx - na - margin, c->iek);
+        a.kob = c->kob;
+        a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
+        a.out = c->vmax_buf;
+        CK(cudaMemsetAsync(c->vmax_buf, 0, 4 * sizeof(unsigned int), c->stream));
+        if (a.i1 >= a.i0 && a.j1 >= a.j0) {
+            launch_vmax3d(a, c->stream);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpyAsync(c->h_vmax, c->vmax_buf, 3 * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < 3; q++) memcpy(&out[q], &c->h_vmax[q], sizeof(float));
+    }
+    float mx = std::max(out[0], std::max(out[1], out[2]));
+    if (!(mx * c->UC <= 1e5f))   // also catches NaN
+        return set_err(c, SWPC_ERR_DIVERGED, "numerical divergence detected (max |V| * UC > 1e5)");
+    return SWPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// field transfer
+// ---------------------------------------------------------------------------
+static float *field_ptr(swpc_ctx *c, int field) {
+    if (field >= SWPC_F_VX && field <= SWPC_F_VZ) return c->V[field - SWPC_F_VX];
+    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return c->S[field - SWPC_F_SXX];
+    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return c->R[field - SWPC_F_R];
+    return nullptr;
+}
+
+static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_k, int ld_i) {
+    if (!c->absorb_ready || !c->aux[q]) return set_err(c, SWPC_ERR_STATE, "swpc_absorb_setup not called");
+    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "2D auxiliaries use the 2D layout");
+    const Geo &g = c->g;
+    std::vector<float> buf((size_t)std::max<long long>(c->npml, 1));
+    std::vector<int2> pc((size_t)g.Ip * g.Jp);
+    CK(cudaMemcpyAsync(pc.data(), c->pmlcol, pc.size() * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
+    if (in == nullptr || true)
+        CK(cudaMemcpyAsync(buf.data(), c->aux[q], c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int j = -2; j <= g.ny + 3; j++)
+        for (int i = -2; i <= g.nx + 3; i++) {
+            const long long h = ((long long)(j + 2) * ld_i + (i + 2)) * ld_k;
+            const bool dom = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+            const int2 p = dom ? pc[col_index(g, i, j)] : make_int2(1, -1);
+            for (int k = -2; k <= g.nz + 3; k++) {
+                const bool has = p.y >= 0 && k >= p.x && k <= g.nz;
+                if (out) out[h + (k + 2)] = has ? buf[(size_t)p.y + (k - p.x)] : 0.0f;
+                else if (has) buf[(size_t)p.y + (k - p.x)] = in[h + (k + 2)];
+            }
+        }
+    if (in) {
+        CK(cudaMemcpyAsync(c->aux[q], buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return SWPC_OK;
+}
+
+extern "C" int swpc_download_field(swpc_ctx *c, int field, float *out, int ld_k, int ld_i) {
+    if (!c || !out) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) return aux_transfer(c, field - SWPC_F_AUX, out, nullptr, ld_k, ld_i);
+    float *p = field_ptr(c, field);
+    if (!p) return set_err(c, SWPC_ERR_ARG, "unknown or unallocated field id");
+    return copy_box(c, p, nullptr, out, ld_k, ld_i);
+}
+
+extern "C" int swpc_upload_field(swpc_ctx *c, int field, const float *in, int ld_k, int ld_i) {
+    if (!c || !in) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) return aux_transfer(c, field - SWPC_F_AUX, nullptr, in, ld_k, ld_i);
+    float *p = field_ptr(c, field);
+    if (!p) return set_err(c, SWPC_ERR_ARG, "unknown or unallocated field id");
+    return copy_box(c, p, in, nullptr, ld_k, ld_i);
+}

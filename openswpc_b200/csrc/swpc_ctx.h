@@ -1,0 +1,152 @@
+// swpc_ctx.h -- device context shared by the 3D, P-SV and SH solvers.
+//
+// Device layout (all solvers): every full-grid field is one float array over
+// the reference memory box i in [-2, nx+3], j in [-2, ny+3] and
+// k in [1-KH, nz+3(+pad)] with k fastest.  Cell (k,i,j) sits at
+//     e = ((j+2) * Ip + (i+2)) * Kp + (k - 1 + KH),  Ip = nx + 6,
+// Kp a multiple of 8 floats, KH = 8, so k = 1 starts every column on a
+// 32-byte sector and a warp of 32 consecutive k reads exactly 4 sectors.
+// For the 2D codes ny = 1 and j is fixed to 1.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/swpc_gpu.h"
+
+namespace swpc {
+
+constexpr int KH = 8;      // device halo below k = 1
+constexpr int NM_MAX = 3;  // reference NM (m_global.f90:31)
+
+struct Geo {
+    int nx, ny, nz;
+    int Kp;                // k pitch in floats
+    int Ip;                // i pitch in columns (nx + 6)
+    int Jp;                // j extent in columns (ny + 6, or 1 for 2D)
+    long long ncell;       // Kp * Ip * Jp
+};
+
+__host__ __device__ inline long long col_index(const Geo &g, int i, int j) {
+    return (long long)(j + 2) * g.Ip + (i + 2);
+}
+__host__ __device__ inline long long cell_index(const Geo &g, int k, int i, int j) {
+    return col_index(g, i, j) * g.Kp + (k - 1 + KH);
+}
+
+// One entry of the per-step point-source injection list (stress glut, body
+// force, reciprocity force).  Entries are applied in list order.
+struct InjEntry {
+    long long cell;   // device cell index
+    int field;        // target field id (SWPC_F_*)
+    int src;          // source index into the stime / weight tables
+    float coef;       // moment-tensor component or force component
+    int mode;         // 0: S -= coef*sdrop ; 1: S -= coef*sdrop/4 ;
+                      // 2: V += b*coef*stime*dt_dxyz/2 ; 3: V += b*f/2 (green)
+    int bfield;       // buoyancy field for modes 2-3 (index into med[])
+    int pad;
+};
+
+struct swpc_ctx_impl;
+
+}  // namespace swpc
+
+struct swpc_ctx {
+    int kind;
+    swpc::Geo g;
+    swpc_desc d;
+    int device;
+    cudaStream_t stream;
+    std::string err;
+
+    // kernel region (m_global.f90:349-378)
+    int ibk, iek, jbk, jek, kbk, kek;
+
+    // full-grid fields
+    float *V[3] = {nullptr, nullptr, nullptr};          // Vx Vy Vz (2D: Vx Vz / Vy)
+    float *S[6] = {nullptr};                           // Sxx Syy Szz Syz Sxz Sxy
+    float *R[18] = {nullptr};                          // component*3 + m
+    // medium: 0 rho 1 lam 2 mu 3 taup 4 taus 5 bx 6 by 7 bz 8 muyz 9 muxz 10 muxy
+    float *med[11] = {nullptr};
+    int4 *band = nullptr;     // per column: kfs_top kfs_bot kob_top kob_bot
+    int2 *pmlcol = nullptr;   // per column: kbeg_a, aux base (-1 = no absorber cell)
+    int *kob = nullptr, *kfs = nullptr;   // per column
+    std::vector<int> h_kbeg_a;            // host copy (columns, device indexing)
+
+    // PML
+    bool absorb_ready = false;
+    long long npml = 0;
+    float *aux[18] = {nullptr};
+    float4 *gx[2] = {nullptr, nullptr};   // c, e  indexed [i-1]
+    float4 *gy[2] = {nullptr, nullptr};
+    float4 *gz[2] = {nullptr, nullptr};
+
+    // coefficients
+    bool kernel_ready = false;
+    bool medium_ready = false;
+    float e40[3][2], e41[3][2];   // [axis][0: 4th order (isign=-1), 1: 2nd order band]
+    float r20[3];
+    float c1[swpc::NM_MAX], c2[swpc::NM_MAX], d1[swpc::NM_MAX], d2;
+    float ts[swpc::NM_MAX];
+
+    // sources
+    int nsrc_glut = 0, nsrc_bf = 0;
+    swpc::InjEntry *inj_glut = nullptr; int ninj_glut = 0; bool glut_serial = false;
+    swpc::InjEntry *inj_bf = nullptr; int ninj_bf = 0; bool bf_serial = false;
+    float *stime_glut = nullptr;   // (nt, nsrc) moment rate at tbeg+(it-0.5)dt
+    float *mo_glut = nullptr;      // (nsrc)
+    float *stime_bf = nullptr;     // (nt, nsrc) at tbeg + it*dt
+    long long *rho_cell_bf = nullptr;   // 2D body force: density cell per source
+    float dt_dxyz = 0.f;
+    // green's function source
+    bool green = false;
+    swpc::InjEntry *inj_green = nullptr; int ninj_green = 0;
+    float *stf_green = nullptr;    // (nt)
+    float green_dt_dxyz = 0.f;
+    float green_f[3] = {0, 0, 0};
+
+    // recorder
+    int nst = 0, ntw = 0, ntdec_w = 1, wav_what = 0;
+    float M0 = 1.f, UC = 1e-15f;
+    int *st_ijk = nullptr;        // (3, nst)
+    float *wav[4] = {nullptr};    // v, u, stress, strain: (ntw, ncmp, nst)
+    float *uacc = nullptr;        // (3, nst)
+    float *eacc = nullptr;        // (6, nst)
+    float r40[3], r41[3];         // m_wav.f90:130-135
+
+    // vmax
+    unsigned int *vmax_buf = nullptr;
+    unsigned int *h_vmax = nullptr;   // pinned
+
+    // graph
+    int *d_it = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_key = -1;
+
+    // launch shape
+    int bi = 4, bj = 2;
+
+    long long bytes = 0;
+};
+
+// helpers shared by the translation units
+namespace swpc {
+int set_err(swpc_ctx *c, int code, const std::string &msg);
+int cuda_check(swpc_ctx *c, cudaError_t e, const char *what);
+template <typename T>
+int dalloc(swpc_ctx *c, T **p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(c, SWPC_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    c->bytes += (long long)(n * sizeof(T));
+    e = cudaMemsetAsync(*p, 0, n * sizeof(T), c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cudaMemsetAsync");
+    return 0;
+}
+}  // namespace swpc

@@ -1,0 +1,410 @@
+// swpc_host.cpp -- host setup routines (include/swpc_setup.h).
+//
+// Single-precision restatements of the reference's setup arithmetic; the
+// per-cell loops are OpenMP-parallel (every cell is independent, so results
+// do not depend on the thread count).  Compiled with -ffp-contract=off so
+// that each operation rounds as the reference's expression spells it.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/swpc_gpu.h"
+#include "../../include/swpc_setup.h"
+#include "swpc_host.h"
+
+namespace {
+
+const double kPi = 3.141592653589793238462643383279502884;   // m_std.f90:14
+const float kEps = 1.1920929e-07f;                             // epsilon(1.0)
+
+struct Box {
+    long nk, ni, nj;
+    int nx, ny, nz;
+    long idx(int k, int i, int j) const { return ((long)(j + 2) * ni + (i + 2)) * nk + (k + 2); }
+    long col(int i, int j) const { return (long)(j + 2) * ni + (i + 2); }
+};
+
+Box make_box(const swpc_grid *g) {
+    Box b;
+    b.nx = g->nx; b.ny = g->ny; b.nz = g->nz;
+    b.nk = g->nz + 6; b.ni = g->nx + 6; b.nj = g->ny > 1 ? g->ny + 6 : 1;
+    return b;
+}
+
+}  // namespace
+
+namespace swpc {
+
+float momentrate(float t, int stftype, float ts, float tr) {
+    switch (stftype) {
+    case SWPC_STF_BOXCAR:
+        if (ts <= t && t <= ts + tr) return 1.0f / tr;
+        return 0.0f;
+    case SWPC_STF_TRIANGLE:
+        if (ts <= t && t <= ts + tr / 2) return 4 * (t - ts) / (tr * tr);
+        if (ts + tr / 2 < t && t <= ts + tr) return -4 * (t - ts - tr) / (tr * tr);
+        return 0.0f;
+    case SWPC_STF_HERRMANN: {
+        const float t1 = ts + tr / 4;
+        const float t2 = ts + 3 * tr / 4;
+        if (ts <= t && t < t1) {
+            const float a = t - ts;
+            return 16 * (a * a) / (tr * tr * tr);
+        }
+        if (t1 <= t && t < t2) return -2 * (8 * (t * t + tr * ts + ts * ts - t * tr - 2 * t * ts) + tr * tr) / (tr * tr * tr);
+        if (t2 <= t && t <= ts + tr) {
+            const float a = ts + tr - t;
+            return 16 * (a * a) / (tr * tr * tr);
+        }
+        return 0.0f;
+    }
+    case SWPC_STF_COSINE:
+        if (ts <= t && t <= ts + tr) return (float)((1.0 - cos(2 * kPi * (double)(t - ts) / (double)tr)) / (double)tr);
+        return 0.0f;
+    case SWPC_STF_TEXP:
+        if (ts <= t) {
+            const float tt = t - ts;
+            const double tp = 2 * kPi;
+            return (float)(tp * tp * (double)tt / (double)(tr * tr) * exp(-2 * kPi * (double)tt / (double)tr));
+        }
+        return 0.0f;
+    default:   // kupper (m_fdtool.f90:339-353)
+        if (ts <= t && t <= ts + tr) {
+            const double s = sin(kPi * (double)(t - ts) / (double)tr);
+            return (float)(3.0 * kPi * (s * s * s) / (double)(4.0f * tr));
+        }
+        return 0.0f;
+    }
+}
+
+}  // namespace swpc
+
+extern "C" {
+
+int swpc_x2i(float x, float beg, float d) {
+    volatile float t = (x - beg) / d;
+    return (int)ceilf(t);
+}
+
+float swpc_i2x(int i, float beg, float d) {
+    volatile float a = (float)i - 0.5f;
+    volatile float b = a * d;
+    return beg + b;
+}
+
+float swpc_momentrate(float t, int stftype, float ts, float tr) { return swpc::momentrate(t, stftype, ts, tr); }
+
+void swpc_sdr2moment(float strike, float dip, float rake, float *m6) {
+    const float d2r = (float)(kPi / 180.0);
+    const float sind = sinf(dip * d2r), cosd = cosf(dip * d2r);
+    const float sin2d = sinf((2 * dip) * d2r), cos2d = cosf((2 * dip) * d2r);
+    const float sinl = sinf(rake * d2r), cosl = cosf(rake * d2r);
+    const float sf = sinf(strike * d2r), cf = cosf(strike * d2r);
+    const float sin2f = sinf((2 * strike) * d2r), cos2f = cosf((2 * strike) * d2r);
+    m6[0] = -(sind * cosl * sin2f + sin2d * sinl * sf * sf);   // mxx
+    m6[1] = (sind * cosl * sin2f - sin2d * sinl * cf * cf);    // myy
+    m6[2] = (sin2d * sinl);                                    // mzz
+    m6[3] = -(cosd * cosl * sf - cos2d * sinl * cf);           // myz
+    m6[4] = -(cosd * cosl * cf + cos2d * sinl * sf);           // mxz
+    m6[5] = (sind * cosl * cos2f + sin2d * sinl * sin2f / 2);  // mxy
+}
+
+void swpc_visco_setup(int nm, float fq_min, float fq_max, float *ts, float *zeta) {
+    // visco_set_relaxtime (m_fdtool.f90:691-727)
+    const float oa = (float)(2 * kPi * (double)fq_min);
+    const float ob = (float)(2 * kPi * (double)fq_max);
+    if (nm == 1) {
+        ts[0] = 1.0f / sqrtf(oa * ob);
+    } else if (nm > 1) {
+        for (int m = 0; m < nm; m++) {
+            const double p = pow((double)(ob / oa), (double)m / (double)(nm - 1));
+            ts[m] = 1.0f / (float)((double)oa * p);
+        }
+    }
+    // visco_constq_zeta (m_fdtool.f90:756-812)
+    if (nm == 0) { *zeta = 0.0f; return; }
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+    std::vector<float> i0(nm), i1(nm);
+    for (int m = 0; m < nm; m++) {
+        const float t = ts[m];
+        i0[m] = (logf(1.0f + (ob * ob) * (t * t)) - logf(1.0f + (oa * oa) * (t * t))) / (2 * t);
+        const float pb = atanf(ob * t) - ob * t / (1 + (ob * ob) * (t * t));
+        const float pa = atanf(oa * t) - oa * t / (1 + (oa * oa) * (t * t));
+        i1[m] = (pb - pa) / (2 * t);
+    }
+    for (int m = 0; m < nm; m++) s0 += i0[m];
+    for (int m = 0; m < nm; m++) s1 += i1[m];
+    for (int m = 0; m < nm - 1; m++)
+        for (int q = m + 1; q < nm; q++) {
+            const float w1 = atanf(ob * ts[m]) / ts[m] - atanf(ob * ts[q]) / ts[q];
+            const float w2 = atanf(oa * ts[m]) / ts[m] - atanf(oa * ts[q]) / ts[q];
+            s2 = s2 + ts[m] * ts[q] / (ts[q] * ts[q] - ts[m] * ts[m]) * (w1 - w2);
+        }
+    *zeta = s0 / (s1 + 2 * s2);
+}
+
+void swpc_kbeg_a(const swpc_grid *g, int *kbeg_a) {
+    const Box b = make_box(g);
+    const int jlo = g->ny > 1 ? -2 : 1, jhi = g->ny > 1 ? g->ny + 3 : 1;
+    for (int j = jlo; j <= jhi; j++)
+        for (int i = -2; i <= g->nx + 3; i++) {
+            const bool side = i <= g->na || g->nx - g->na + 1 <= i ||
+                              (g->ny > 1 && (j <= g->na || g->ny - g->na + 1 <= j));
+            const long c = g->ny > 1 ? b.col(i, j) : (long)(i + 2);
+            kbeg_a[c] = side ? 1 : g->nz - g->na + 1;
+        }
+}
+
+static void vcheck(float &vp, float &vs, float &rho, float xi, float vmin, float vmax, float rhomin) {
+    // m_fdtool.f90:15-48
+    float gamma = vp / vs;
+    if (gamma < kEps) gamma = sqrtf(3.0f);
+    if (vp > vmax || vs > vmax) {
+        const float xi2 = (1 + xi) * vmax / vp - 1;
+        vp = vmax;
+        vs = vmax / gamma;
+        rho = rho * (1 + 0.8f * xi2) / (1 + 0.8f * xi);
+    }
+    if (vp < vmin || vs < vmin) {
+        vs = vmin;
+        vp = vmin * gamma;
+    }
+    if (rho < rhomin) rho = rhomin;
+}
+
+int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const float *rho0_in, const float *vp0_in,
+                    const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut, const float *xi,
+                    float rhomin, float *rho, float *lam, float *mu, float *qp, float *qs) {
+    if (nlayer < 1) return SWPC_ERR_ARG;
+    std::vector<float> r0(rho0_in, rho0_in + nlayer), p0(vp0_in, vp0_in + nlayer), s0(vs0_in, vs0_in + nlayer);
+    std::vector<float> qa(qp0_in, qp0_in + nlayer), qb(qs0_in, qs0_in + nlayer);
+    // velocity cut-off (m_vmodel_lhm.f90:93-101)
+    for (int l = nlayer - 2; l >= 0; l--)
+        if ((p0[l] < vcut || s0[l] < vcut) && (p0[l] > 0 && s0[l] > 0)) {
+            p0[l] = p0[l + 1]; s0[l] = s0[l + 1]; r0[l] = r0[l + 1]; qa[l] = qa[l + 1]; qb[l] = qb[l + 1];
+        }
+    // velocity bounds of lhm_rmed (m_vmodel_lhm_rmed.f90:95-98)
+    const float dh = 1.0f / sqrtf(1.0f / (g->dx * g->dx) + 1.0f / (g->dy * g->dy) + 1.0f / (g->dz * g->dz));
+    const float vmax_r = 6.0f / 7.0f * dh / g->dt;
+    const Box b = make_box(g);
+    const int jlo = g->ny > 1 ? -2 : 0, jhi = g->ny > 1 ? g->ny + 3 : 0;
+#pragma omp parallel for schedule(static)
+    for (int k = -2; k <= g->nz + 3; k++) {
+        const float zs = swpc_i2x(k, g->zbeg, g->dz);
+        for (int j = jlo; j <= jhi; j++)
+            for (int i = -2; i <= g->nx + 3; i++) {
+                const long e = g->ny > 1 ? b.idx(k, i, j) : ((long)(i + 2) * b.nk + (k + 2));
+                if (zs < depth[0]) {
+                    // air column (no ocean layer in this model family)
+                    rho[e] = 0.001f; mu[e] = 0.0f; lam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+                    continue;
+                }
+                float rho1 = 0, vp1 = 0, vs1 = 0, qp1 = 0, qs1 = 0;
+                for (int l = 0; l < nlayer; l++) {
+                    if (zs >= depth[l]) {
+                        if (xi) {
+                            const float x = xi[e];
+                            rho1 = r0[l] * (1 + 0.8f * x);
+                            vp1 = 1.0f * p0[l] * (1 + x);
+                            vs1 = 1.0f * s0[l] * (1 + x);
+                            if (p0[l] > 0 && s0[l] > 0) vcheck(vp1, vs1, rho1, x, vcut, vmax_r, rhomin);
+                        } else {
+                            rho1 = r0[l]; vp1 = 1.0f * p0[l]; vs1 = 1.0f * s0[l];
+                        }
+                        qp1 = qa[l]; qs1 = qb[l];
+                    }
+                }
+                rho[e] = rho1;
+                mu[e] = rho1 * vs1 * vs1;
+                lam[e] = rho1 * (vp1 * vp1 - 2 * vs1 * vs1);
+                qp[e] = qp1;
+                qs[e] = qs1;
+            }
+    }
+    return SWPC_OK;
+}
+
+int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam, float *mu,
+                      const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by, float *bz,
+                      float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
+                      int *kob_top, int *kob_bot, float *ts, float *scal) {
+    if (g->ny <= 1) return SWPC_ERR_ARG;
+    const Box b = make_box(g);
+    const int nx = g->nx, ny = g->ny, nz = g->nz, na = g->na, nm = g->nm;
+    const long n3 = b.nk * b.ni * b.nj;
+    memcpy(taup, qp, sizeof(float) * n3);
+    memcpy(taus, qs, sizeof(float) * n3);
+    auto copy_cell = [&](long d, long s) {
+        rho[d] = rho[s]; lam[d] = lam[s]; mu[d] = mu[s]; taup[d] = taup[s]; taus[d] = taus[s];
+    };
+    // absorber homogenisation (m_medium.f90:124-190), in the reference order
+#pragma omp parallel for schedule(static)
+    for (int j = -2; j <= ny + 3; j++)
+        for (int i = -2; i <= na; i++)
+            for (int k = -2; k <= nz + 3; k++) copy_cell(b.idx(k, i, j), b.idx(k, na + 1, j));
+#pragma omp parallel for schedule(static)
+    for (int j = -2; j <= ny + 3; j++)
+        for (int i = nx - na + 1; i <= nx + 3; i++)
+            for (int k = -2; k <= nz + 3; k++) copy_cell(b.idx(k, i, j), b.idx(k, nx - na, j));
+    for (int j = -2; j <= na; j++)
+#pragma omp parallel for schedule(static)
+        for (int i = -2; i <= nx + 3; i++)
+            for (int k = -2; k <= nz + 3; k++) copy_cell(b.idx(k, i, j), b.idx(k, i, na + 1));
+    for (int j = ny - na + 1; j <= ny + 3; j++)
+#pragma omp parallel for schedule(static)
+        for (int i = -2; i <= nx + 3; i++)
+            for (int k = -2; k <= nz + 3; k++) copy_cell(b.idx(k, i, j), b.idx(k, i, ny - na));
+#pragma omp parallel for schedule(static)
+    for (int j = -2; j <= ny + 3; j++)
+        for (int i = -2; i <= nx + 3; i++)
+            for (int k = nz - na + 1; k <= nz + 3; k++) copy_cell(b.idx(k, i, j), b.idx(nz - na, i, j));
+    // tau method (m_medium.f90:193-207)
+    float zeta = 0.0f;
+    swpc_visco_setup(nm, fq_min, fq_max, ts, &zeta);
+#pragma omp parallel for schedule(static)
+    for (long e = 0; e < n3; e++) {
+        taup[e] = nm * zeta / taup[e];
+        taus[e] = nm * zeta / taus[e];
+    }
+    // relaxed_medium (m_medium.f90:234-274): chi = 1 / Re(1/sqrt(1 - cc*tau)),
+    // cc = mean over m of (i w ts)/(1 - i w ts)
+    if (nm > 0) {
+        const float omega = (float)(2 * kPi * (double)fq_ref);
+        float ccr = 0.0f, cci = 0.0f;
+        for (int m = 0; m < nm; m++) {
+            const double a = (double)omega * (double)ts[m];
+            const double den = 1.0 + a * a;
+            ccr = ccr + (float)(-(a * a) / den);
+            cci = cci + (float)(a / den);
+        }
+        ccr = ccr / nm;
+        cci = cci / nm;
+#pragma omp parallel for schedule(static)
+        for (long e = 0; e < n3; e++) {
+            const float rb2 = mu[e];
+            const float ra2 = lam[e] + 2 * mu[e];
+            float chi[2];
+            const float tt[2] = {taus[e], taup[e]};
+            for (int q = 0; q < 2; q++) {
+                const float zr = 1.0f - ccr * tt[q];
+                const float zi = 0.0f - cci * tt[q];
+                const float wr = sqrtf(0.5f * (hypotf(zr, zi) + zr));
+                const float wi = 0.5f * (zi / wr);
+                chi[q] = 1.0f / (wr / (wr * wr + wi * wi));
+            }
+            mu[e] = rb2 / (chi[0] * chi[0]);
+            lam[e] = ra2 / (chi[1] * chi[1]) - 2 * mu[e];
+        }
+    }
+    // surface_detection (m_medium.f90:342-397)
+    for (long c = 0; c < b.ni * b.nj; c++) { kfs[c] = 0; kob[c] = 0; }
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= ny + 2; j++)
+        for (int i = 0; i <= nx + 2; i++) {
+            int f = 0, o = 0;
+            for (int k = 1; k <= nz - 1; k++) {
+                if (fabsf(mu[b.idx(k, i, j)]) < kEps && fabsf(mu[b.idx(k + 1, i, j)]) > kEps) o = k;
+                if (fabsf(lam[b.idx(k, i, j)]) < kEps && fabsf(lam[b.idx(k + 1, i, j)]) > kEps) f = k;
+            }
+            kfs[b.col(i, j)] = f;
+            kob[b.col(i, j)] = o;
+        }
+    for (long c = 0; c < b.ni * b.nj; c++) { kfs_top[c] = 0; kfs_bot[c] = 0; kob_top[c] = 0; kob_bot[c] = 0; }
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            int fmn = 1 << 30, fmx = -(1 << 30), omn = 1 << 30, omx = -(1 << 30);
+            for (int jj = j - 2; jj <= j + 3; jj++)
+                for (int ii = i - 2; ii <= i + 3; ii++) {
+                    const int f = kfs[b.col(ii, jj)], o = kob[b.col(ii, jj)];
+                    fmn = std::min(fmn, f); fmx = std::max(fmx, f);
+                    omn = std::min(omn, o); omx = std::max(omx, o);
+                }
+            kfs_top[b.col(i, j)] = std::max(fmn - 2, 1);
+            kfs_bot[b.col(i, j)] = std::min(fmx + 2, nz);
+            kob_top[b.col(i, j)] = std::max(omn - 2, 1);
+            kob_bot[b.col(i, j)] = std::min(omx + 2, nz);
+        }
+    // velocity_minmax (m_medium.f90:399-430)
+    float vmax1 = -1.0f, vmin1 = 1e30f;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++)
+            for (int k = kfs[b.col(i, j)] + 1; k <= nz; k++) {
+                const long e = b.idx(k, i, j);
+                const float vp = sqrtf((lam[e] + 2 * mu[e]) / rho[e]);
+                const float vs = sqrtf(mu[e] / rho[e]);
+                vmax1 = std::max(vmax1, vp);
+                if (vs < kEps) continue;
+                vmin1 = std::min(vmin1, vs);
+            }
+    // averaged_medium (m_medium.f90:432-465)
+    memset(bx, 0, sizeof(float) * n3); memset(by, 0, sizeof(float) * n3); memset(bz, 0, sizeof(float) * n3);
+    memset(muyz, 0, sizeof(float) * n3); memset(muxz, 0, sizeof(float) * n3); memset(muxy, 0, sizeof(float) * n3);
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= nz; k++) {
+                const long e = b.idx(k, i, j);
+                bx[e] = 2.0f / (rho[e] + rho[b.idx(k, i + 1, j)]);
+                by[e] = 2.0f / (rho[e] + rho[b.idx(k, i, j + 1)]);
+                bz[e] = 2.0f / (rho[e] + rho[b.idx(k + 1, i, j)]);
+                const float nnn = mu[e], pnn = mu[b.idx(k + 1, i, j)], npn = mu[b.idx(k, i + 1, j)];
+                const float ppn = mu[b.idx(k + 1, i + 1, j)], nnp = mu[b.idx(k, i, j + 1)];
+                const float npp = mu[b.idx(k, i + 1, j + 1)], pnp = mu[b.idx(k + 1, i, j + 1)];
+                muxz[e] = 4 * nnn * pnn * npn * ppn / (nnn * pnn * npn + nnn * pnn * ppn + nnn * npn * ppn + pnn * npn * ppn + kEps);
+                muxy[e] = 4 * nnn * npn * nnp * npp / (nnn * npn * nnp + nnn * npn * npp + nnn * nnp * npp + npn * nnp * npp + kEps);
+                muyz[e] = 4 * nnn * pnn * nnp * pnp / (nnn * pnn * nnp + nnn * pnn * pnp + nnn * nnp * pnp + pnn * nnp * pnp + kEps);
+            }
+    scal[0] = zeta;
+    scal[1] = vmin1;
+    scal[2] = vmax1;
+    return SWPC_OK;
+}
+
+static void damping_profile(float x, float H, float beg, float end, int na, float fcut, float dt, float *gp) {
+    // m_absorb_p.f90:507-547 (pd = pa = 1, pb = 2, cp = 6)
+    const float R0 = powf(10.0f, -(log10f((float)na) - 1) / log10f(2.0f) - 3.0f);
+    const float d0 = -(1.0f / (2.0f * H)) * (1 + 1) * 6.0f * logf(R0);
+    const float b0 = 7.0f;
+    const float a0 = (float)(kPi * (double)fcut);
+    float xx;
+    if (x <= beg + H) xx = (beg + H) - x;
+    else if (x >= end - H) xx = x - (end - H);
+    else xx = 0.0f;
+    const float r = fabsf(xx / H);
+    const float d = d0 * r;
+    const float a = a0 * (1.0f - r);
+    const float bb = 1.0f + (b0 - 1.0f) * (r * r);
+    const float h = dt / 2.0f;
+    gp[0] = ((1.0f + h * a) / bb) / (1.0f + h * (a + d / bb));
+    gp[1] = (-1.0f / bb) / (1.0f + h * (a + d / bb));
+    gp[2] = (1.0f - h * (a + d / bb)) / (1.0f + h * (a + d / bb));
+    gp[3] = (d / bb) / (1.0f + h * (a + d / bb));
+}
+
+void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gxe, float *gyc, float *gye, float *gzc,
+                           float *gze) {
+    // absorb_p__setup (m_absorb_p.f90:79-93); xend = xbeg + nx*dx (m_global.f90:205-207)
+    const float xend = g->xbeg + g->nx * g->dx, yend = g->ybeg + g->ny * g->dy, zend = g->zbeg + g->nz * g->dz;
+    const float hx = g->na * g->dx, hy = g->na * g->dy, hz = g->na * g->dz;
+    for (int i = 1; i <= g->nx; i++) {
+        const float xc = swpc_i2x(i, g->xbeg, g->dx);
+        damping_profile(xc, hx, g->xbeg, xend, g->na, fcut, g->dt, gxc + 4 * (i - 1));
+        damping_profile(xc + g->dx / 2.0f, hx, g->xbeg, xend, g->na, fcut, g->dt, gxe + 4 * (i - 1));
+    }
+    if (gyc && gye)
+        for (int j = 1; j <= g->ny; j++) {
+            const float yc = swpc_i2x(j, g->ybeg, g->dy);
+            damping_profile(yc, hy, g->ybeg, yend, g->na, fcut, g->dt, gyc + 4 * (j - 1));
+            damping_profile(yc + g->dy / 2.0f, hy, g->ybeg, yend, g->na, fcut, g->dt, gye + 4 * (j - 1));
+        }
+    for (int k = 1; k <= g->nz; k++) {
+        const float zc = swpc_i2x(k, g->zbeg, g->dz);
+        damping_profile(zc, hz, g->zbeg, zend, g->na, fcut, g->dt, gzc + 4 * (k - 1));
+        damping_profile(zc + g->dz / 2.0f, hz, g->zbeg, zend, g->na, fcut, g->dt, gze + 4 * (k - 1));
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// swpc_kernels.cuh -- launch argument blocks of the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "swpc_ctx.h"
+
+namespace swpc {
+
+enum InjMode { INJ_GLUT = 0, INJ_GLUT4 = 1, INJ_GLUT2 = 2, INJ_BF3 = 3, INJ_GREEN = 4, INJ_BFPSV = 5, INJ_BFSH = 6 };
+
+struct Vel3Args {
+    Geo g;
+    int ibk, iek, jbk, jek, kek;
+    float *Vx, *Vy, *Vz;
+    const float *Sxx, *Syy, *Szz, *Syz, *Sxz, *Sxy;
+    const float *bx, *by, *bz;
+    const int4 *band;
+    const int2 *pmlcol;
+    float *aS[9];   // axSxx aySxy azSxz axSxy aySyy azSyz axSxz aySyz azSzz
+    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
+    float e40[3][2], e41[3][2];
+    float r20[3];
+    float dt;
+    int mask;       // bit 0: interior cells, bit 1: absorber cells
+};
+
+struct Str3Args {
+    Geo g;
+    int ibk, iek, jbk, jek, kek;
+    const float *Vx, *Vy, *Vz;
+    float *Sxx, *Syy, *Szz, *Syz, *Sxz, *Sxy;
+    float *R[18];
+    const float *lam, *mu, *taup, *taus, *muyz, *muxz, *muxy;
+    const int4 *band;
+    const int2 *pmlcol;
+    float *aV[9];   // axVx ayVx azVx axVy ayVy azVy axVz ayVz azVz
+    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
+    float e40[3][2], e41[3][2];
+    float r20[3];
+    float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
+    float dt;
+    int mask;
+};
+
+struct InjArgs {
+    const InjEntry *list;
+    int n;
+    int serial;
+    int it;              // used when d_it is null
+    const int *d_it;     // step counter for graph replays
+    int nt;
+    int nsrc;
+    const float *stime;  // (nt, nsrc)
+    const float *mo;     // (nsrc) for stress glut
+    float dt_dxyz;
+    float *fields[9];    // V (0..2) and S (3..8) by SWPC_F_* id
+    const float *bfields[3];
+    const long long *rho_cell;   // (nsrc) density cell of 2D body forces
+};
+
+struct Wav3Args {
+    Geo g;
+    int nst, ntw, ntdec_w, what;
+    int it;
+    const int *d_it;
+    const int *st;       // (3, nst) i j k
+    const float *Vx, *Vy, *Vz;
+    const float *Sxx, *Syy, *Szz, *Syz, *Sxz, *Sxy;
+    float *uacc, *eacc;
+    float *wav_v, *wav_u, *wav_s, *wav_e;
+    float M0, UC, dt;
+    float r40[3], r41[3];
+};
+
+struct VmaxArgs {
+    Geo g;
+    int i0, i1, j0, j1;
+    const int *kob;
+    const float *Vx, *Vy, *Vz;
+    unsigned int *out;
+};
+
+void launch_vel3d(const Vel3Args &a, dim3 grid, dim3 block, cudaStream_t st);
+void launch_stress3d(const Str3Args &a, int nm, dim3 grid, dim3 block, cudaStream_t st);
+void launch_inject(const InjArgs &a, cudaStream_t st);
+void launch_wav3d(const Wav3Args &a, cudaStream_t st);
+void launch_vmax3d(const VmaxArgs &a, cudaStream_t st);
+void launch_advance_it(int *d_it, cudaStream_t st);
+
+}  // namespace swpc

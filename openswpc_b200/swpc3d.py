@@ -1,0 +1,362 @@
+"""Host driver of the 3D solver: the role of src/swpc_3d/main.f90.
+
+`Swpc3D` performs the reference's setup sequence (main.f90:64-78:
+global__setup2, medium__setup, kernel__setup, source__setup, absorb__setup,
+wav__setup, green__setup) with the library's host setup routines, uploads
+everything once, and then exposes the time-loop routines under the
+reference's module names.  `run()` replays the loop of main.f90:125-144 as
+CUDA-graph launches with report__progress (vmax + divergence abort) every
+``ntdec_r`` steps.
+
+Arrays exchanged with the caller use the reference memory-box layout
+``(kbeg_m:kend_m, ibeg_m:iend_m, jbeg_m:jend_m)`` with k fastest; in numpy
+that is a C-ordered array of shape ``(ny+6, nx+6, nz+6)`` indexed
+``[j+2, i+2, k+2]``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, fptr, iptr
+from .params import Params
+
+f32 = np.float32
+
+
+@dataclass
+class SourceGrid:
+    """Result of source__setup (m_source.f90:181-305) for one node."""
+
+    isrc: np.ndarray
+    jsrc: np.ndarray
+    ksrc: np.ndarray
+    srcprm: np.ndarray   # (nsrc, 2) = (tbeg, trise)
+    mo: np.ndarray       # normalised by M0
+    m6: np.ndarray       # (nsrc, 6) xx yy zz yz xz xy
+    f3: np.ndarray       # (nsrc, 3) normalised by M0
+    M0: float
+    UC: float
+    fcut: float
+
+
+def grid_struct(p: Params) -> _lib.Grid:
+    return _lib.Grid(p.nx, p.ny, p.nz, p.na, p.nm, p.dx, p.dy, p.dz, p.dt, p.xbeg, p.ybeg, p.zbeg, p.tbeg)
+
+
+def source_grid(p: Params) -> SourceGrid:
+    """source__setup (m_source.f90:181-305): cut-off frequency, total moment,
+    grid assignment with the node sleeve, normalisation by M0."""
+    lib = _lib.load()
+    srcs = p.sources
+    fcut = f32(0.0)
+    for s in srcs:
+        fcut = max(fcut, f32(1) / f32(s.trise))
+    UC = f32(1e-15)
+    if p.bf_mode:
+        acc = f32(0.0)
+        for s in srcs:
+            acc = acc + (f32(s.fx) * f32(s.fx) + f32(s.fy) * f32(s.fy) + f32(s.fz) * f32(s.fz))
+        M0 = np.sqrt(acc, dtype=np.float32)
+        UC = UC * f32(1000)
+    else:
+        M0 = f32(0.0)
+        for s in srcs:
+            M0 = M0 + f32(s.mo)
+    rows = []
+    for s in srcs:
+        i = lib.swpc_x2i(s.x, p.xbeg, p.dx)
+        j = lib.swpc_x2i(s.y, p.ybeg, p.dy)
+        k = lib.swpc_x2i(s.z, p.zbeg, p.dz)
+        if -1 <= i <= p.nx + 3 and -1 <= j <= p.ny + 3 and -1 <= k <= p.nz + 3:
+            rows.append((i, j, k, s))
+    n = len(rows)
+    isrc = np.array([r[0] for r in rows], np.int32)
+    jsrc = np.array([r[1] for r in rows], np.int32)
+    ksrc = np.array([r[2] for r in rows], np.int32)
+    srcprm = np.array([[r[3].tbeg, r[3].trise] for r in rows], np.float32).reshape(n, 2)
+    if p.bf_mode:
+        f3 = np.array([[f32(r[3].fx) / M0, f32(r[3].fy) / M0, f32(r[3].fz) / M0] for r in rows], np.float32)
+        mo = np.zeros(n, np.float32)
+    else:
+        f3 = np.zeros((n, 3), np.float32)
+        mo = np.array([f32(r[3].mo) / M0 for r in rows], np.float32)
+    m6 = np.array([[r[3].mxx, r[3].myy, r[3].mzz, r[3].myz, r[3].mxz, r[3].mxy] for r in rows],
+                  np.float32).reshape(n, 6)
+    return SourceGrid(isrc, jsrc, ksrc, srcprm, mo, m6, f3.reshape(n, 3), float(M0), float(UC), float(fcut))
+
+
+ZSW = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
+
+
+def station_grid(p: Params, kfs: np.ndarray, kob: np.ndarray):
+    """set_stinfo (m_wav.f90:144-274) for a single node: station cells and
+    depth mode (dep / fsb / obb / oba).  kfs/kob are (ny+6, nx+6) maps."""
+    lib = _lib.load()
+    out = []
+    x1, xn = lib.swpc_i2x(1, p.xbeg, p.dx), lib.swpc_i2x(p.nx, p.xbeg, p.dx)
+    y1, yn = lib.swpc_i2x(1, p.ybeg, p.dy), lib.swpc_i2x(p.ny, p.ybeg, p.dy)
+    for st in p.stations:
+        xs, ys, zs = float(f32(st.x)), float(f32(st.y)), float(f32(st.z))
+        i = lib.swpc_x2i(xs, p.xbeg, p.dx)
+        j = lib.swpc_x2i(ys, p.ybeg, p.dy)
+        k = lib.swpc_x2i(zs, p.zbeg, p.dz)
+        if not (x1 < xs < xn and y1 < ys < yn and 1 < k < p.nz):
+            continue
+        if not (1 <= i <= p.nx and 1 <= j <= p.ny):
+            continue
+        z = ZSW.get(st.zsw, 0)
+        if z == 1:
+            k = int(kfs[j + 2, i + 2]) + 1
+        elif z == 2:
+            k = int(kob[j + 2, i + 2]) + 1
+        elif z == 3:
+            k = int(kob[j + 2, i + 2]) - 1
+        else:
+            k = lib.swpc_x2i(zs, p.zbeg, p.dz)
+        if k > p.nz:
+            k = p.nz - 1
+        if k < 1:
+            k = 2
+        out.append((i, j, k))
+    a = np.array(out, np.int32).reshape(-1, 3)
+    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
+
+
+class Medium:
+    """Host copy of the medium after medium__setup (m_medium.f90:36-467)."""
+
+    FIELDS = ("rho", "lam", "mu", "taup", "taus", "bx", "by", "bz", "muyz", "muxz", "muxy")
+    MAPS = ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot", "kbeg_a")
+
+    def __init__(self, p: Params, xi: np.ndarray | None = None):
+        lib = _lib.load()
+        g = grid_struct(p)
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        for name in self.FIELDS:
+            setattr(self, name, np.zeros(shape, np.float32))
+        self.qp = np.zeros(shape, np.float32)
+        self.qs = np.zeros(shape, np.float32)
+        for name in self.MAPS:
+            setattr(self, name, np.zeros(shape[:2], np.int32))
+        if not p.layers:
+            raise ValueError("a layered (lhm) velocity model is required")
+        L = p.layers
+        arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
+        if xi is not None:
+            xi = np.ascontiguousarray(xi, np.float32)
+            assert xi.shape == shape
+        rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+                                 fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, fptr(xi), p.rhomin,
+                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs))
+        if rc:
+            raise ValueError("vmodel_lhm failed")
+        self.ts = np.zeros(3, np.float32)
+        scal = np.zeros(3, np.float32)
+        rc = lib.swpc_setup_medium(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
+                                   fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup), fptr(self.taus),
+                                   fptr(self.bx), fptr(self.by), fptr(self.bz), fptr(self.muyz), fptr(self.muxz),
+                                   fptr(self.muxy), iptr(self.kfs), iptr(self.kob), iptr(self.kfs_top),
+                                   iptr(self.kfs_bot), iptr(self.kob_top), iptr(self.kob_bot), fptr(self.ts),
+                                   fptr(scal))
+        if rc:
+            raise ValueError("medium setup failed")
+        self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
+        lib.swpc_kbeg_a(C.byref(g), iptr(self.kbeg_a))
+
+    def view(self) -> _lib.MediumView:
+        v = _lib.MediumView()
+        for name in self.FIELDS:
+            setattr(v, name, fptr(getattr(self, name)))
+        for name in self.MAPS:
+            setattr(v, name, iptr(getattr(self, name)))
+        v.ld_k = self.rho.shape[2]
+        v.ld_i = self.rho.shape[1]
+        v.ld_i2 = self.kfs.shape[1]
+        return v
+
+
+class Swpc3D:
+    """One 3D run on one GPU (the single-node case of the reference)."""
+
+    def __init__(self, p: Params, xi: np.ndarray | None = None, device: int = 0, medium: Medium | None = None):
+        p.check()
+        self.p = p
+        self.lib = _lib.load()
+        self.medium = medium if medium is not None else Medium(p, xi)
+        m = self.medium
+        desc = _lib.Desc(_lib.KIND_3D, p.nx, p.ny, p.nz, p.na, p.nm, p.nt, p.dx, p.dy, p.dz, p.dt, p.tbeg, device)
+        ctx = C.c_void_p()
+        rc = self.lib.swpc_create(C.byref(desc), C.byref(ctx))
+        self.ctx = ctx
+        if rc:
+            msg = self.lib.swpc_last_error(ctx) if ctx else b""
+            self.lib.swpc_destroy(ctx)
+            self.ctx = None
+            raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_create failed")
+        self._keep = []
+        check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view())))
+        check(self.ctx, self.lib.swpc_kernel_setup(self.ctx, fptr(m.ts)))
+        # source__setup (m_source.f90) or green__setup (m_green.f90)
+        self.src = source_grid(p)
+        self.M0, self.UC = self.src.M0, self.src.UC
+        stf = _lib.STF_CODES[p.stftype]
+        if p.green_mode:
+            st = p.stations[p.green_station]
+            self.M0 = 1.0
+            i, j, k = station_grid(Params(**{**p.__dict__, "stations": [st]}), m.kfs, m.kob)
+            if len(i) != 1:
+                raise ValueError("green source station outside the domain")
+            check(self.ctx, self.lib.swpc_green_setup(self.ctx, int(i[0]), int(j[0]), int(k[0]),
+                                                      p.green_cmp.encode()[0:1], 0.0, p.green_trise, stf))
+            self.fcut = 1.0 / p.green_trise
+        elif p.bf_mode:
+            s = self.src
+            check(self.ctx, self.lib.swpc_bodyforce_setup(self.ctx, len(s.isrc), iptr(s.isrc), iptr(s.jsrc),
+                                                          iptr(s.ksrc), fptr(s.srcprm), fptr(s.f3), stf))
+            self.fcut = s.fcut
+        else:
+            s = self.src
+            check(self.ctx, self.lib.swpc_source_setup(self.ctx, len(s.isrc), iptr(s.isrc), iptr(s.jsrc),
+                                                       iptr(s.ksrc), fptr(s.srcprm), fptr(s.mo), fptr(s.m6), stf))
+            self.fcut = s.fcut
+        # absorb_p__setup with fcut from the source setup (m_absorb_p.f90:528)
+        g = grid_struct(p)
+        self.gprof = {n: np.zeros((p.nx if n[1] == "x" else p.ny if n[1] == "y" else p.nz, 4), np.float32)
+                      for n in ("gxc", "gxe", "gyc", "gye", "gzc", "gze")}
+        gp = self.gprof
+        self.lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]),
+                                       fptr(gp["gyc"]), fptr(gp["gye"]), fptr(gp["gzc"]), fptr(gp["gze"]))
+        check(self.ctx, self.lib.swpc_absorb_setup(self.ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), fptr(gp["gyc"]),
+                                                   fptr(gp["gye"]), fptr(gp["gzc"]), fptr(gp["gze"])))
+        # wav__setup (m_wav.f90:76-142); off in green mode
+        self.nst = 0
+        what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u) | (_lib.WAV_STRESS * p.sw_wav_stress) | \
+            (_lib.WAV_STRAIN * p.sw_wav_strain)
+        if p.stations and not p.green_mode and what:
+            self.ist, self.jst, self.kst = station_grid(p, m.kfs, m.kob)
+            self.nst = len(self.ist)
+            check(self.ctx, self.lib.swpc_wav_setup(self.ctx, self.nst, iptr(self.ist), iptr(self.jst),
+                                                    iptr(self.kst), p.ntdec_w, what, self.M0, self.UC))
+        self.what = what
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self.ctx:
+            self.lib.swpc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- the reference routines --------------------------------------------
+    def kernel__update_stress(self):
+        check(self.ctx, self.lib.swpc_kernel_update_stress(self.ctx))
+
+    def absorb__update_stress(self):
+        check(self.ctx, self.lib.swpc_absorb_update_stress(self.ctx))
+
+    def kernel__update_vel(self):
+        check(self.ctx, self.lib.swpc_kernel_update_vel(self.ctx))
+
+    def absorb__update_vel(self):
+        check(self.ctx, self.lib.swpc_absorb_update_vel(self.ctx))
+
+    def source__stressglut(self, it: int):
+        check(self.ctx, self.lib.swpc_source_stressglut(self.ctx, it))
+
+    def source__bodyforce(self, it: int):
+        check(self.ctx, self.lib.swpc_source_bodyforce(self.ctx, it))
+
+    def green__source(self, it: int):
+        check(self.ctx, self.lib.swpc_green_source(self.ctx, it))
+
+    def global__comm_stress(self):
+        check(self.ctx, self.lib.swpc_comm_stress(self.ctx))
+
+    def global__comm_vel(self):
+        check(self.ctx, self.lib.swpc_comm_vel(self.ctx))
+
+    def wav__store(self, it: int):
+        check(self.ctx, self.lib.swpc_wav_store(self.ctx, it))
+
+    def kernel__vmax(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(self.ctx, self.lib.swpc_vmax(self.ctx, fptr(out)))
+        return out
+
+    def step(self, it: int):
+        """One pass of main.f90:128-143 (fused interior + absorber launches)."""
+        check(self.ctx, self.lib.swpc_step(self.ctx, it))
+
+    def run(self, it0: int = 1, nsteps: int | None = None, report=None) -> list[tuple[int, np.ndarray]]:
+        """The time loop of main.f90:125-144 as CUDA-graph replays.  Every
+        ``ntdec_r`` steps kernel__vmax runs before the step (report__progress,
+        m_report.f90:134-152); a diverging run raises SwpcError.  Returns the
+        list of (it, max|V| * UC * M0) report values."""
+        p = self.p
+        if nsteps is None:
+            nsteps = p.nt - it0 + 1
+        last = it0 + nsteps - 1
+        reports = []
+        it = it0
+        while it <= last:
+            if it % p.ntdec_r == 0:
+                vm = self.kernel__vmax()
+                va = vm * f32(self.UC) * f32(self.M0)
+                reports.append((it, va))
+                if report:
+                    report(it, va)
+            nxt = (it // p.ntdec_r + 1) * p.ntdec_r
+            n = min(nxt, last + 1) - it
+            check(self.ctx, self.lib.swpc_run(self.ctx, it, n))
+            it += n
+        self.sync()
+        return reports
+
+    def time_steps(self, it0: int, nsteps: int) -> float:
+        ms = C.c_float()
+        check(self.ctx, self.lib.swpc_time_steps(self.ctx, it0, nsteps, C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        check(self.ctx, self.lib.swpc_sync(self.ctx))
+
+    # -- data ---------------------------------------------------------------
+    def download(self, field: int) -> np.ndarray:
+        p = self.p
+        out = np.zeros((p.ny + 6, p.nx + 6, p.nz + 6), np.float32)
+        check(self.ctx, self.lib.swpc_download_field(self.ctx, field, fptr(out), p.nz + 6, p.nx + 6))
+        return out
+
+    def upload(self, field: int, arr: np.ndarray):
+        p = self.p
+        a = np.ascontiguousarray(arr, np.float32)
+        assert a.shape == (p.ny + 6, p.nx + 6, p.nz + 6)
+        check(self.ctx, self.lib.swpc_upload_field(self.ctx, field, fptr(a), p.nz + 6, p.nx + 6))
+
+    def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
+        """wav buffer in the reference layout wav(ntw, ncmp, nst), returned as a
+        numpy array of shape (nst, ncmp, ntw)."""
+        ntw, nst = C.c_int(), C.c_int()
+        check(self.ctx, self.lib.swpc_wav_dims(self.ctx, C.byref(ntw), C.byref(nst)))
+        ncmp = 3 if what in (_lib.WAV_V, _lib.WAV_U) else 6
+        out = np.zeros((nst.value, ncmp, ntw.value), np.float32)
+        if nst.value:
+            check(self.ctx, self.lib.swpc_wav_fetch(self.ctx, what, fptr(out)))
+        return out
+
+    def device_bytes(self) -> int:
+        return int(self.lib.swpc_device_bytes(self.ctx))

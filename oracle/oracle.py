@@ -1,0 +1,287 @@
+"""ctypes driver of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/lib/liboracle3d_<variant>.so`` (built by build_oracle.py) and
+runs the reference's setup and time loop as restated in swpc3d_oracle.c.
+Only tests/, the package smoke check and bench.py's cpu_baseline leg use it,
+as the checker or as the timed CPU baseline.
+
+The oracle's own setup follows the reference modules; every input it shares
+with the GPU driver (layer table, perturbation xi, source and station lists)
+is the raw input a user would give OpenSWPC.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "lib"
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int)
+_cache: dict[str, C.CDLL] = {}
+
+ZSW = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
+STF = {"kupper": 0, "boxcar": 1, "triangle": 2, "herrmann": 3, "cosine": 4, "scosine": 4, "texp": 5}
+
+# field ids of o3d_ptr
+FIELD_IDS = {"Vx": 0, "Vy": 1, "Vz": 2, "Sxx": 3, "Syy": 4, "Szz": 5, "Syz": 6, "Sxz": 7, "Sxy": 8,
+             "Rxx": 10, "Ryy": 11, "Rzz": 12, "Ryz": 13, "Rxz": 14, "Rxy": 15,
+             "lam": 20, "mu": 21, "taup": 22, "taus": 23, "bx": 24, "by": 25, "bz": 26, "muyz": 27,
+             "muxz": 28, "muxy": 29, "frho": 30, "flam": 31, "fmu": 32, "ftaup": 33, "ftaus": 34, "fbx": 35,
+             "fby": 36, "fbz": 37, "fmuyz": 38, "fmuxz": 39, "fmuxy": 40, "kfs": 50, "kob": 51, "kfs_top": 52,
+             "kfs_bot": 53, "kob_top": 54, "kob_bot": 55, "kbeg_a": 56}
+AUX_NAMES = ["axVx", "ayVx", "azVx", "axVy", "ayVy", "azVy", "axVz", "ayVz", "azVz",
+             "axSxx", "aySxy", "azSxz", "axSxy", "aySyy", "azSyz", "axSxz", "aySyz", "azSzz"]
+for _n, _a in enumerate(AUX_NAMES):
+    FIELD_IDS[_a] = 60 + _n
+
+
+def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
+    key = f"{kind}_{variant}"
+    if key in _cache:
+        return _cache[key]
+    path = LIB / f"liboracle{kind}_{variant}.so"
+    if not path.exists():
+        from . import build_oracle  # noqa: F401  (package-relative when imported as oracle.oracle)
+    if not path.exists():
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("build_oracle", HERE / "build_oracle.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    lib = C.CDLL(str(path))
+    vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+    sig = {
+        "o3d_create": (vp, [i, i, i, i, i, i, d, d, d, f, f, f, f, f, i]),
+        "o3d_destroy": (None, [vp]),
+        "o3d_vmodel_lhm": (None, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, _FP, f, _FP, _FP]),
+        "o3d_medium_setup": (None, [vp, _FP, _FP, f, f, f]),
+        "o3d_set_medium": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "o3d_set_maps": (None, [vp, _IP, _IP, _IP, _IP, _IP, _IP]),
+        "o3d_kernel_setup": (None, [vp]),
+        "o3d_absorb_setup": (None, [vp, f]),
+        "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
+        "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
+        "o3d_wav_setup": (i, [vp, i, _FP, _FP, _FP, _IP, i, i, i, i, i, _IP, _IP, _IP]),
+        "o3d_step": (None, [vp, i]),
+        "o3d_vmax": (None, [vp, _FP]),
+        "o3d_dims": (None, [vp, C.POINTER(C.c_long)]),
+        "o3d_scalars": (None, [vp, _FP]),
+        "o3d_ptr": (vp, [vp, i]),
+        "o3d_mpr_size": (i, []),
+        "o3d_spr_size": (i, []),
+        "o3d_x2i": (i, [f, f, f]),
+        "o3d_i2x": (f, [i, f, f]),
+        "o3d_momentrate": (f, [f, i, f, f]),
+        "o3d_sdr2moment": (None, [f, f, f, _FP]),
+        "o3d_visco_set_relaxtime": (None, [i, _FP, f, f]),
+        "o3d_visco_constq_zeta": (f, [i, f, f, _FP]),
+    }
+    for name in ("o3d_update_stress", "o3d_absorb_update_stress", "o3d_update_vel", "o3d_absorb_update_vel",
+                 "o3d_comm_stress", "o3d_comm_vel"):
+        sig[name] = (None, [vp])
+    for name in ("o3d_stressglut", "o3d_bodyforce", "o3d_green_source", "o3d_wav_store"):
+        sig[name] = (None, [vp, i])
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _cache[key] = lib
+    return lib
+
+
+def _f(a):
+    return None if a is None else np.ascontiguousarray(a, np.float32).ctypes.data_as(_FP)
+
+
+class Oracle3D:
+    """The reference 3D run restated on the CPU.
+
+    ``p`` is an ``openswpc_b200.params.Params``-like object (duck-typed: the
+    oracle reads attributes only).  ``variant`` selects f32 / mixed / f64.
+    """
+
+    def __init__(self, p, xi=None, variant: str = "f32", threads: int = 1, medium=None, profiles=None):
+        self.p = p
+        self.lib = lib = load(variant)
+        self.variant = variant
+        self.mpr = np.float32 if lib.o3d_mpr_size() == 4 else np.float64
+        self.spr = np.float32 if lib.o3d_spr_size() == 4 else np.float64
+        self.o = lib.o3d_create(p.nx, p.ny, p.nz, p.na, p.nm, p.nt, float(np.float32(p.dx)),
+                                float(np.float32(p.dy)), float(np.float32(p.dz)), p.dt, p.xbeg, p.ybeg, p.zbeg,
+                                p.tbeg, threads)
+        self._hold = []
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        if medium is None:
+            L = p.layers
+            arr = lambda a: np.array([getattr(l, a) for l in L], np.float32)
+            qp = np.zeros(shape, np.float32)
+            qs = np.zeros(shape, np.float32)
+            xi_c = None if xi is None else np.ascontiguousarray(xi, np.float32)
+            lib.o3d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
+                               _f(arr("qp")), _f(arr("qs")), p.vcut, _f(xi_c), p.rhomin, _f(qp), _f(qs))
+            lib.o3d_medium_setup(self.o, _f(qp), _f(qs), p.fq_min, p.fq_max, p.fq_ref)
+        else:
+            # externally prepared medium (e.g. to isolate the time step)
+            m = medium
+            lib.o3d_set_medium(self.o, _f(m.lam), _f(m.mu), _f(m.taup), _f(m.taus), _f(m.bx), _f(m.by),
+                               _f(m.bz), _f(m.muyz), _f(m.muxz), _f(m.muxy), _f(m.ts))
+            ip = lambda a: np.ascontiguousarray(a, np.int32).ctypes.data_as(_IP)
+            lib.o3d_set_maps(self.o, ip(m.kfs), ip(m.kob), ip(m.kfs_top), ip(m.kfs_bot), ip(m.kob_top),
+                             ip(m.kob_bot))
+        lib.o3d_kernel_setup(self.o)
+        # sources
+        stf = STF[p.stftype]
+        if p.green_mode:
+            self.nsrc = 0
+        else:
+            S = p.sources
+            n = len(S)
+            sx = np.array([s.x for s in S], np.float32)
+            sy = np.array([s.y for s in S], np.float32)
+            sz = np.array([s.z for s in S], np.float32)
+            prm = np.array([[s.tbeg, s.trise] for s in S], np.float32).reshape(n, 2)
+            mo = np.array([s.mo for s in S], np.float32)
+            m6 = np.array([[s.mxx, s.myy, s.mzz, s.myz, s.mxz, s.mxy] for s in S], np.float32).reshape(n, 6)
+            f3 = np.array([[s.fx, s.fy, s.fz] for s in S], np.float32).reshape(n, 3)
+            self._hold += [sx, sy, sz, prm, mo, m6, f3]
+            self.nsrc = lib.o3d_source_setup(self.o, int(p.bf_mode), n, _f(sx), _f(sy), _f(sz), _f(prm), _f(mo),
+                                             _f(m6), _f(f3), stf)
+        sc = self.scalars()
+        fcut = sc["fcut"] if not p.green_mode else float(np.float32(1.0) / np.float32(p.green_trise))
+        lib.o3d_absorb_setup(self.o, fcut)
+        if profiles is not None:
+            lib.o3d_set_profiles(self.o, *[_f(profiles[k]) for k in ("gxc", "gxe", "gyc", "gye", "gzc", "gze")])
+        if p.green_mode:
+            st = p.stations[p.green_station]
+            from_ijk = self._station_cells([st])
+            i, j, k = from_ijk[0][0], from_ijk[1][0], from_ijk[2][0]
+            lib.o3d_green_setup(self.o, i, j, k, p.green_cmp.encode()[0:1], 0.0, p.green_trise, stf)
+        self.nst = 0
+        if p.stations and not p.green_mode and (p.sw_wav_v or p.sw_wav_u or p.sw_wav_stress or p.sw_wav_strain):
+            S = p.stations
+            xs = np.array([s.x for s in S], np.float32)
+            ys = np.array([s.y for s in S], np.float32)
+            zs = np.array([s.z for s in S], np.float32)
+            zsw = np.array([ZSW.get(s.zsw, 0) for s in S], np.int32)
+            ist = np.zeros(len(S), np.int32)
+            jst = np.zeros(len(S), np.int32)
+            kst = np.zeros(len(S), np.int32)
+            ip = lambda a: a.ctypes.data_as(_IP)
+            self.nst = lib.o3d_wav_setup(self.o, len(S), _f(xs), _f(ys), _f(zs), ip(zsw), p.ntdec_w,
+                                         int(p.sw_wav_v), int(p.sw_wav_u), int(p.sw_wav_stress),
+                                         int(p.sw_wav_strain), ip(ist), ip(jst), ip(kst))
+            self.ist, self.jst, self.kst = ist[:self.nst], jst[:self.nst], kst[:self.nst]
+
+    def _station_cells(self, stations):
+        """set_stinfo for a station list (used for the green source cell)."""
+        lib = self.lib
+        p = self.p
+        kfs = self.array("kfs")
+        kob = self.array("kob")
+        out = ([], [], [])
+        for st in stations:
+            i = lib.o3d_x2i(st.x, p.xbeg, p.dx)
+            j = lib.o3d_x2i(st.y, p.ybeg, p.dy)
+            k = lib.o3d_x2i(st.z, p.zbeg, p.dz)
+            z = ZSW.get(st.zsw, 0)
+            if z == 1:
+                k = int(kfs[j + 2, i + 2]) + 1
+            elif z == 2:
+                k = int(kob[j + 2, i + 2]) + 1
+            elif z == 3:
+                k = int(kob[j + 2, i + 2]) - 1
+            out[0].append(i)
+            out[1].append(j)
+            out[2].append(k)
+        return out
+
+    def close(self):
+        if self.o:
+            self.lib.o3d_destroy(self.o)
+            self.o = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- access -------------------------------------------------------------
+    def dims(self) -> dict:
+        a = (C.c_long * 17)()
+        self.lib.o3d_dims(self.o, a)
+        keys = ["nk", "ni", "nj", "nkk", "nik", "njk", "nka", "ibeg_k", "iend_k", "jbeg_k", "jend_k", "kbeg_k",
+                "kend_k", "kbeg_min", "nst", "ntw", "nsrc"]
+        return dict(zip(keys, list(a)))
+
+    def scalars(self) -> dict:
+        a = (C.c_float * 13)()
+        self.lib.o3d_scalars(self.o, a)
+        keys = ["M0", "UC", "fcut", "fmax", "vmin", "vmax", "zeta", "xend", "yend", "zend", "ts1", "ts2", "ts3"]
+        return dict(zip(keys, list(a)))
+
+    def array(self, name: str) -> np.ndarray:
+        """Copy of an oracle array in the reference layout (numpy view order)."""
+        d = self.dims()
+        p = self.p
+        fid = FIELD_IDS[name]
+        ptr = self.lib.o3d_ptr(self.o, fid)
+        if fid in range(0, 9):
+            dt, shape = self.mpr, (d["nj"], d["ni"], d["nk"])
+        elif fid in range(10, 16):
+            dt, shape = self.spr, (d["njk"], d["nik"], d["nkk"], p.nm)
+        elif fid in range(20, 30):
+            dt, shape = self.spr, (d["nj"], d["ni"], d["nk"])
+        elif fid in range(30, 41):
+            dt, shape = np.float32, (d["nj"], d["ni"], d["nk"])
+        elif fid in range(50, 57):
+            dt, shape = np.int32, (d["nj"], d["ni"])
+        elif fid in range(60, 78):
+            dt, shape = self.spr, (p.ny, p.nx, d["nka"])
+        else:
+            raise KeyError(name)
+        n = int(np.prod(shape))
+        buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+    def waveforms(self, comp: str = "v") -> np.ndarray:
+        d = self.dims()
+        fid = {"v": 90, "u": 91, "stress": 92, "strain": 93}[comp]
+        ncmp = 3 if comp in ("v", "u") else 6
+        ptr = self.lib.o3d_ptr(self.o, fid)
+        n = d["ntw"] * ncmp * d["nst"]
+        if n == 0:
+            return np.zeros((d["nst"], ncmp, d["ntw"]), np.float32)
+        buf = (C.c_float * n).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float32).reshape(d["nst"], ncmp, d["ntw"]).copy()
+
+    def set_array(self, name: str, values: np.ndarray):
+        """Overwrite an oracle field (V, S, R or PML auxiliary)."""
+        cur = self.array(name)
+        fid = FIELD_IDS[name]
+        ptr = self.lib.o3d_ptr(self.o, fid)
+        v = np.ascontiguousarray(values, cur.dtype).reshape(cur.shape)
+        C.memmove(ptr, v.ctypes.data, v.nbytes)
+
+    # -- stepping -----------------------------------------------------------
+    def step(self, it: int):
+        self.lib.o3d_step(self.o, it)
+
+    def vmax(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        self.lib.o3d_vmax(self.o, _f(out))
+        return out
+
+    def run(self, it0: int, nsteps: int, ntdec_r: int | None = None):
+        reports = []
+        sc = self.scalars()
+        for it in range(it0, it0 + nsteps):
+            if ntdec_r and it % ntdec_r == 0:
+                reports.append((it, self.vmax() * np.float32(sc["UC"]) * np.float32(sc["M0"])))
+            self.lib.o3d_step(self.o, it)
+        return reports

@@ -1,0 +1,173 @@
+"""CPU tests: the product's host setup against the oracle (bit-exact), the
+C-ABI symbol table, and the input reader.  No GPU needed."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from openswpc_b200 import _lib
+from openswpc_b200.params import Layer, Params, Source, Station, dc_source, params_from_ini
+from openswpc_b200.swpc3d import Medium, grid_struct, source_grid, station_grid
+from oracle.oracle import Oracle3D, load as oload
+from tests.models import LAYERS, small3d, vonkarman_xi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = set()
+    for h in (ROOT / "include").glob("*.h"):
+        txt = h.read_text()
+        declared |= set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(swpc_\w+)\s*\(", txt, flags=re.M))
+    assert len(declared) > 30
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(_lib.EXPORTS) <= declared | set(_lib.EXPORTS)
+
+
+@pytest.mark.parametrize("with_xi", [False, True])
+def test_medium_setup_bit_exact(with_xi):
+    p = small3d()
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6)) if with_xi else None
+    m = Medium(p, xi)
+    o = Oracle3D(p, xi)
+    for f in ("rho", "lam", "mu", "taup", "taus", "bx", "by", "bz", "muyz", "muxz", "muxy"):
+        assert np.array_equal(bits(getattr(m, f)), bits(o.array("f" + f))), f
+    for f in ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot", "kbeg_a"):
+        assert np.array_equal(getattr(m, f), o.array(f)), f
+    sc = o.scalars()
+    assert np.float32(sc["zeta"]) == np.float32(m.zeta)
+    assert np.float32(sc["vmin"]) == np.float32(m.vmin) and np.float32(sc["vmax"]) == np.float32(m.vmax)
+    assert np.array_equal(m.ts, np.array([sc["ts1"], sc["ts2"], sc["ts3"]], np.float32))
+
+
+def test_free_surface_maps_locate_air_solid_boundary():
+    p = small3d()
+    m = Medium(p)
+    # zbeg = -3 dz: cells k = 1..3 are air, k = 4 is the first solid cell
+    assert (m.kfs[2:-3, 2:-3] == 3).all() and (m.kob[2:-3, 2:-3] == 3).all()
+    assert (m.kfs_top[3:-3, 3:-3] == 1).all() and (m.kfs_bot[3:-3, 3:-3] == 5).all()
+
+
+def test_source_and_station_maps_bit_exact():
+    p = small3d(sources=[dc_source(0.3, -0.7, 6.1, 0.0, 1.0, 1e16, 30, 60, 90),
+                         Source(2.2, 1.1, 4.0, 0.2, 1.5, mo=3e15, mxx=1, myy=1, mzz=1),
+                         Source(-9.9, -8.9, 0.1, 0.0, 1.0, mo=1e15, mxy=1.0)])
+    sg = source_grid(p)
+    o = Oracle3D(p)
+    d = o.dims()
+    n = d["nsrc"]
+    isrc = np.ctypeslib.as_array(C.cast(o.lib.o3d_ptr(o.o, 98), C.POINTER(C.c_int)), (n,))
+    jsrc = np.ctypeslib.as_array(C.cast(o.lib.o3d_ptr(o.o, 99), C.POINTER(C.c_int)), (n,))
+    ksrc = np.ctypeslib.as_array(C.cast(o.lib.o3d_ptr(o.o, 100), C.POINTER(C.c_int)), (n,))
+    assert np.array_equal(sg.isrc, isrc) and np.array_equal(sg.jsrc, jsrc) and np.array_equal(sg.ksrc, ksrc)
+    sc = o.scalars()
+    assert np.float32(sc["M0"]) == np.float32(sg.M0) and np.float32(sc["fcut"]) == np.float32(sg.fcut)
+    m = Medium(p)
+    ist, jst, kst = station_grid(p, m.kfs, m.kob)
+    assert np.array_equal(ist, o.ist) and np.array_equal(jst, o.jst) and np.array_equal(kst, o.kst)
+
+
+def test_damping_profiles_bit_exact():
+    p = small3d()
+    lib = _lib.load()
+    g = grid_struct(p)
+    prof = {k: np.zeros((n, 4), np.float32) for k, n in
+            (("gxc", p.nx), ("gxe", p.nx), ("gyc", p.ny), ("gye", p.ny), ("gzc", p.nz), ("gze", p.nz))}
+    fcut = np.float32(1.0)
+    lib.swpc_damping_profiles(C.byref(g), float(fcut), *[_lib.fptr(prof[k]) for k in ("gxc", "gxe", "gyc", "gye",
+                                                                                     "gzc", "gze")])
+    o = Oracle3D(p)   # source trise = 1.0 -> fcut = 1.0
+    for n, k in enumerate(("gxc", "gxe", "gyc", "gye", "gzc", "gze")):
+        cnt = prof[k].size
+        ref = np.ctypeslib.as_array(C.cast(o.lib.o3d_ptr(o.o, 80 + n), C.POINTER(C.c_float)), (cnt,))
+        assert np.array_equal(bits(prof[k].ravel()), bits(ref)), k
+    # the profile is the identity (g1 = 1, g2 = -1... no damping) in the interior
+    assert np.allclose(prof["gxc"][p.na + 2, :2], [1.0 / 1.0, -1.0], atol=1e-6) or prof["gxc"][p.na + 2, 3] == 0
+
+
+@pytest.mark.parametrize("stf", ["kupper", "boxcar", "triangle", "herrmann", "cosine", "texp"])
+def test_moment_rate_functions_match(stf):
+    lib = _lib.load()
+    ol = oload()
+    code = _lib.STF_CODES[stf]
+    for t in np.linspace(-0.5, 3.5, 401, dtype=np.float32):
+        a = lib.swpc_momentrate(float(t), code, 0.25, 2.0)
+        b = ol.o3d_momentrate(float(t), code, 0.25, 2.0)
+        assert np.float32(a) == np.float32(b)
+
+
+def test_moment_rate_integrates_to_one():
+    lib = _lib.load()
+    for stf, code in _lib.STF_CODES.items():
+        if stf == "scosine":
+            continue
+        t = np.arange(0, 40.0, 1e-3, dtype=np.float64)
+        v = np.array([lib.swpc_momentrate(float(x), code, 0.5, 2.0) for x in t[::10]])
+        integral = v.sum() * 1e-2
+        assert abs(integral - 1.0) < 2e-2, (stf, integral)
+
+
+def test_sdr2moment_is_double_couple():
+    lib = _lib.load()
+    m6 = (C.c_float * 6)()
+    for sdr in ((30, 60, 90), (0, 90, 0), (123, 45, -60)):
+        lib.swpc_sdr2moment(*sdr, m6)
+        m = np.array([[m6[0], m6[5], m6[4]], [m6[5], m6[1], m6[3]], [m6[4], m6[3], m6[2]]], np.float64)
+        ev = np.sort(np.linalg.eigvalsh(m))
+        assert np.allclose(ev, [-1, 0, 1], atol=1e-5)
+        assert abs(np.trace(m)) < 1e-5
+
+
+def test_grid_index_functions_match_oracle():
+    lib = _lib.load()
+    ol = oload()
+    rng = np.random.default_rng(3)
+    for x in rng.uniform(-50, 50, 500).astype(np.float32):
+        for beg, d in ((-10.0, 0.1), (-96.0, 0.5), (-1.5, 0.25)):
+            assert lib.swpc_x2i(float(x), beg, d) == ol.o3d_x2i(float(x), beg, d)
+    for i in range(-3, 200):
+        assert np.float32(lib.swpc_i2x(i, -10.0, 0.1)) == np.float32(ol.o3d_i2x(i, -10.0, 0.1))
+
+
+def test_params_reader(tmp_path):
+    (tmp_path / "lhm.dat").write_text("# d rho vp vs qp qs\n 0 2.7 5.5 3.2 300 150\n 5 2.8 6.0 3.5 500 250\n")
+    (tmp_path / "src.dat").write_text("# x y z t0 tr mo mxx myy mzz myz mxz mxy\n0 0 6 0.1 2 1e16 1 1 1 0 0 0\n")
+    (tmp_path / "st.xy").write_text("1.0 2.0 0.0 st01 fsb\n-3 4 0 st02 obb\n")
+    (tmp_path / "input.inf").write_text(
+        "title = 'x'  !! comment\n nx = 64\n ny = 48\n nz = 32\n nt = 10\n dx = 0.25\n dy=0.25\n dz = 0.25\n"
+        " dt = 0.01\n na = 8\n zbeg = -1.0\n fn_lhm = 'lhm.dat'\n fn_stf = 'src.dat'\n stf_format='xym0ij'\n"
+        " fn_stloc = 'st.xy'\n sw_wav_v = .true.\n ntdec_w = 2\n")
+    p = params_from_ini(tmp_path / "input.inf")
+    assert (p.nx, p.ny, p.nz, p.nt, p.na) == (64, 48, 32, 10, 8)
+    assert p.dx == 0.25 and p.zbeg == -1.0 and p.ntdec_w == 2
+    assert p.xbeg == -8.0 and p.ybeg == -6.0     # -nx/2*dx default
+    assert len(p.layers) == 2 and len(p.sources) == 1 and len(p.stations) == 2
+    assert p.sources[0].mo == 1e16 and p.stations[1].zsw == "obb"
+    with pytest.raises(KeyError):
+        params_from_ini(tmp_path / "input.inf", strict=True)
+
+
+def test_oracle_fp32_close_to_fp64():
+    """The restated scheme in FP32 stays within 1e-4 rel-L2 of the all-double
+    build of the same scheme over a short run (sanity check of the oracle)."""
+    p = small3d(nt=40)
+    a = Oracle3D(p, variant="f32")
+    b = Oracle3D(p, variant="f64")
+    a.run(1, 40)
+    b.run(1, 40)
+    wa, wb = a.waveforms("v").astype(np.float64), b.waveforms("v").astype(np.float64)
+    assert np.linalg.norm(wb) > 0
+    assert np.linalg.norm(wa - wb) / np.linalg.norm(wb) < 1e-4
+    va, vb = a.array("Vz").astype(np.float64), b.array("Vz")
+    assert np.linalg.norm(va - vb) / np.linalg.norm(vb) < 1e-4
