@@ -214,6 +214,15 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
 /* Device bytes held by the context. */
 long long swpc_device_bytes(const swpc_ctx *ctx);
 
+/* Launch shape of a fused kernel (kernel 0 = stress, 1 = velocity): block =
+ * 32 (k) x bi (i) x bj (j) threads (32*bi*bj <= 256); minb = minimum
+ * resident blocks per SM the kernel variant is compiled for (1..4; fewer
+ * blocks leave more registers for operands in flight).  Defaults come from a
+ * sweep on B200 (stress: minb 2, 2 x 1; velocity: minb 4, 2 x 2).  No
+ * counterpart in the reference (its OpenMP/OpenACC schedules are fixed at
+ * compile time); results do not depend on the shape. */
+int swpc_set_launch(swpc_ctx *ctx, int kernel, int minb, int bi, int bj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,7 @@ EXPORTS = [
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
     "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
     "swpc_vmax", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
-    "swpc_download_field", "swpc_upload_field", "swpc_device_bytes",
+    "swpc_download_field", "swpc_upload_field", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles",
@@ -122,6 +122,7 @@ def load():
         "swpc_download_field": (i, [vp, i, _FP, i, i]),
         "swpc_upload_field": (i, [vp, i, _FP, i, i]),
         "swpc_device_bytes": (C.c_longlong, [vp]),
+        "swpc_set_launch": (i, [vp, i, i, i, i]),
         "swpc_x2i": (i, [f, f, f]),
         "swpc_i2x": (f, [i, f, f]),
         "swpc_momentrate": (f, [f, i, f, f]),

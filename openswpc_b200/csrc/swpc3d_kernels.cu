@@ -22,11 +22,21 @@
 
 namespace swpc {
 
+// streaming accesses: every value below is touched once per launch, so they
+// are loaded and stored with the evict-first hint and leave L2 to the
+// stencil operands that neighbouring blocks re-read
+__device__ __forceinline__ float lds(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
+
 // ---------------------------------------------------------------------------
 // velocity: kernel__update_vel (m_kernel.f90:75-140) +
 //           absorb_p__update_vel (m_absorb_p.f90:248-309)
+// All loads of a cell are issued before its first store: the arrays never
+// alias, and with every operand in flight at once the kernel is limited by
+// HBM bandwidth instead of by load latency.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) vel3d_kernel(const Vel3Args a) {
     const Geo g = a.g;
     const int k = 1 + blockIdx.x * 32 + threadIdx.x;
     const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -42,10 +52,27 @@ __global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
     const float *__restrict__ Syz = a.Syz;
     const float *__restrict__ Sxz = a.Sxz;
     const float *__restrict__ Sxy = a.Sxy;
+    float *__restrict__ Vx = a.Vx;
+    float *__restrict__ Vy = a.Vy;
+    float *__restrict__ Vz = a.Vz;
     const float dt = a.dt;
 
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         if (!(a.mask & 1)) return;
+        const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
+        const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
+        const float xx0 = __ldg(&Sxx[e]), xxp = __ldg(&Sxx[e + PI]), xxp2 = __ldg(&Sxx[e + 2 * PI]), xxm = __ldg(&Sxx[e - PI]);
+        const float yy0 = __ldg(&Syy[e]), yyp = __ldg(&Syy[e + PJ]), yyp2 = __ldg(&Syy[e + 2 * PJ]), yym = __ldg(&Syy[e - PJ]);
+        const float zz0 = __ldg(&Szz[e]), zzp = __ldg(&Szz[e + 1]), zzp2 = __ldg(&Szz[e + 2]), zzm = __ldg(&Szz[e - 1]);
+        const float xy0 = __ldg(&Sxy[e]);
+        const float xyjm = __ldg(&Sxy[e - PJ]), xyjp = __ldg(&Sxy[e + PJ]), xyjm2 = __ldg(&Sxy[e - 2 * PJ]);
+        const float xyim = __ldg(&Sxy[e - PI]), xyip = __ldg(&Sxy[e + PI]), xyim2 = __ldg(&Sxy[e - 2 * PI]);
+        const float xz0 = __ldg(&Sxz[e]);
+        const float xzkm = __ldg(&Sxz[e - 1]), xzkp = __ldg(&Sxz[e + 1]), xzkm2 = __ldg(&Sxz[e - 2]);
+        const float xzim = __ldg(&Sxz[e - PI]), xzip = __ldg(&Sxz[e + PI]), xzim2 = __ldg(&Sxz[e - 2 * PI]);
+        const float yz0 = __ldg(&Syz[e]);
+        const float yzkm = __ldg(&Syz[e - 1]), yzkp = __ldg(&Syz[e + 1]), yzkm2 = __ldg(&Syz[e - 2]);
+        const float yzjm = __ldg(&Syz[e - PJ]), yzjp = __ldg(&Syz[e + PJ]), yzjm2 = __ldg(&Syz[e - 2 * PJ]);
         const int4 bd = __ldg(&a.band[col]);
         const int p1 = (k - bd.x) * (bd.y - k);
         const int p2 = (k - bd.z) * (bd.w - k);
@@ -54,19 +81,18 @@ __global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
         const float re40y = a.e40[1][s], re41y = a.e41[1][s];
         const float re40z = a.e40[2][s], re41z = a.e41[2][s];
 
-        float d3Sx3 = (__ldg(&Sxx[e + PI]) - __ldg(&Sxx[e])) * re40x - (__ldg(&Sxx[e + 2 * PI]) - __ldg(&Sxx[e - PI])) * re41x
-                    + (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PJ])) * re40y - (__ldg(&Sxy[e + PJ]) - __ldg(&Sxy[e - 2 * PJ])) * re41y
-                    + (__ldg(&Sxz[e]) - __ldg(&Sxz[e - 1])) * re40z - (__ldg(&Sxz[e + 1]) - __ldg(&Sxz[e - 2])) * re41z;
-        float d3Sy3 = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PI])) * re40x - (__ldg(&Sxy[e + PI]) - __ldg(&Sxy[e - 2 * PI])) * re41x
-                    + (__ldg(&Syy[e + PJ]) - __ldg(&Syy[e])) * re40y - (__ldg(&Syy[e + 2 * PJ]) - __ldg(&Syy[e - PJ])) * re41y
-                    + (__ldg(&Syz[e]) - __ldg(&Syz[e - 1])) * re40z - (__ldg(&Syz[e + 1]) - __ldg(&Syz[e - 2])) * re41z;
-        float d3Sz3 = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - PI])) * re40x - (__ldg(&Sxz[e + PI]) - __ldg(&Sxz[e - 2 * PI])) * re41x
-                    + (__ldg(&Syz[e]) - __ldg(&Syz[e - PJ])) * re40y - (__ldg(&Syz[e + PJ]) - __ldg(&Syz[e - 2 * PJ])) * re41y
-                    + (__ldg(&Szz[e + 1]) - __ldg(&Szz[e])) * re40z - (__ldg(&Szz[e + 2]) - __ldg(&Szz[e - 1])) * re41z;
-
-        a.Vx[e] = a.Vx[e] + __ldg(&a.bx[e]) * d3Sx3 * dt;
-        a.Vy[e] = a.Vy[e] + __ldg(&a.by[e]) * d3Sy3 * dt;
-        a.Vz[e] = a.Vz[e] + __ldg(&a.bz[e]) * d3Sz3 * dt;
+        const float d3Sx3 = (xxp - xx0) * re40x - (xxp2 - xxm) * re41x
+                          + (xy0 - xyjm) * re40y - (xyjp - xyjm2) * re41y
+                          + (xz0 - xzkm) * re40z - (xzkp - xzkm2) * re41z;
+        const float d3Sy3 = (xy0 - xyim) * re40x - (xyip - xyim2) * re41x
+                          + (yyp - yy0) * re40y - (yyp2 - yym) * re41y
+                          + (yz0 - yzkm) * re40z - (yzkp - yzkm2) * re41z;
+        const float d3Sz3 = (xz0 - xzim) * re40x - (xzip - xzim2) * re41x
+                          + (yz0 - yzjm) * re40y - (yzjp - yzjm2) * re41y
+                          + (zzp - zz0) * re40z - (zzp2 - zzm) * re41z;
+        sts(&Vx[e], vx + bx * d3Sx3 * dt);
+        sts(&Vy[e], vy + by * d3Sy3 * dt);
+        sts(&Vz[e], vz + bz * d3Sz3 * dt);
         return;
     }
 
@@ -74,20 +100,6 @@ __global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
     if (!(a.mask & 2)) return;
     const int2 pc = __ldg(&a.pmlcol[col]);
     const long long q = (long long)pc.y + (k - pc.x);
-    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
-    const float dxSxx = (__ldg(&Sxx[e + PI]) - __ldg(&Sxx[e])) * r20x;
-    const float dySyy = (__ldg(&Syy[e + PJ]) - __ldg(&Syy[e])) * r20y;
-    const float dzSzz = (__ldg(&Szz[e + 1]) - __ldg(&Szz[e])) * r20z;
-    const float dySyz = (__ldg(&Syz[e]) - __ldg(&Syz[e - PJ])) * r20y;
-    const float dzSyz = (__ldg(&Syz[e]) - __ldg(&Syz[e - 1])) * r20z;
-    const float dxSxz = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - PI])) * r20x;
-    const float dzSxz = (__ldg(&Sxz[e]) - __ldg(&Sxz[e - 1])) * r20z;
-    const float dxSxy = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PI])) * r20x;
-    const float dySxy = (__ldg(&Sxy[e]) - __ldg(&Sxy[e - PJ])) * r20y;
-    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
-    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
-    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
-
     float *__restrict__ axSxx = a.aS[0];
     float *__restrict__ aySxy = a.aS[1];
     float *__restrict__ azSxz = a.aS[2];
@@ -97,34 +109,55 @@ __global__ void __launch_bounds__(256) vel3d_kernel(const Vel3Args a) {
     float *__restrict__ axSxz = a.aS[6];
     float *__restrict__ aySyz = a.aS[7];
     float *__restrict__ azSzz = a.aS[8];
-    const float vxSxx = axSxx[q], vySxy = aySxy[q], vzSxz = azSxz[q];
-    const float vxSxy = axSxy[q], vySyy = aySyy[q], vzSyz = azSyz[q];
-    const float vxSxz = axSxz[q], vySyz = aySyz[q], vzSzz = azSzz[q];
+    const float vxSxx = lds(&axSxx[q]), vySxy = lds(&aySxy[q]), vzSxz = lds(&azSxz[q]);
+    const float vxSxy = lds(&axSxy[q]), vySyy = lds(&aySyy[q]), vzSyz = lds(&azSyz[q]);
+    const float vxSxz = lds(&axSxz[q]), vySyz = lds(&aySyz[q]), vzSzz = lds(&azSzz[q]);
+    const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
+    const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
+    const float xx0 = __ldg(&Sxx[e]), xxp = __ldg(&Sxx[e + PI]);
+    const float yy0 = __ldg(&Syy[e]), yyp = __ldg(&Syy[e + PJ]);
+    const float zz0 = __ldg(&Szz[e]), zzp = __ldg(&Szz[e + 1]);
+    const float yz0 = __ldg(&Syz[e]), yzjm = __ldg(&Syz[e - PJ]), yzkm = __ldg(&Syz[e - 1]);
+    const float xz0 = __ldg(&Sxz[e]), xzim = __ldg(&Sxz[e - PI]), xzkm = __ldg(&Sxz[e - 1]);
+    const float xy0 = __ldg(&Sxy[e]), xyim = __ldg(&Sxy[e - PI]), xyjm = __ldg(&Sxy[e - PJ]);
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+    const float dxSxx = (xxp - xx0) * r20x;
+    const float dySyy = (yyp - yy0) * r20y;
+    const float dzSzz = (zzp - zz0) * r20z;
+    const float dySyz = (yz0 - yzjm) * r20y;
+    const float dzSyz = (yz0 - yzkm) * r20z;
+    const float dxSxz = (xz0 - xzim) * r20x;
+    const float dzSxz = (xz0 - xzkm) * r20z;
+    const float dxSxy = (xy0 - xyim) * r20x;
+    const float dySxy = (xy0 - xyjm) * r20y;
 
-    a.Vx[e] = a.Vx[e] + __ldg(&a.bx[e]) * (gxe.x * dxSxx + gyc.x * dySxy + gzc.x * dzSxz
-                                          + gxe.y * vxSxx + gyc.y * vySxy + gzc.y * vzSxz) * dt;
-    a.Vy[e] = a.Vy[e] + __ldg(&a.by[e]) * (gxc.x * dxSxy + gye.x * dySyy + gzc.x * dzSyz
-                                          + gxc.y * vxSxy + gye.y * vySyy + gzc.y * vzSyz) * dt;
-    a.Vz[e] = a.Vz[e] + __ldg(&a.bz[e]) * (gxc.x * dxSxz + gyc.x * dySyz + gze.x * dzSzz
-                                          + gxc.y * vxSxz + gyc.y * vySyz + gze.y * vzSzz) * dt;
+    sts(&Vx[e], vx + bx * (gxe.x * dxSxx + gyc.x * dySxy + gzc.x * dzSxz
+                           + gxe.y * vxSxx + gyc.y * vySxy + gzc.y * vzSxz) * dt);
+    sts(&Vy[e], vy + by * (gxc.x * dxSxy + gye.x * dySyy + gzc.x * dzSyz
+                           + gxc.y * vxSxy + gye.y * vySyy + gzc.y * vzSyz) * dt);
+    sts(&Vz[e], vz + bz * (gxc.x * dxSxz + gyc.x * dySyz + gze.x * dzSzz
+                           + gxc.y * vxSxz + gyc.y * vySyz + gze.y * vzSzz) * dt);
 
-    axSxx[q] = gxe.z * vxSxx + gxe.w * dxSxx * dt;
-    aySxy[q] = gyc.z * vySxy + gyc.w * dySxy * dt;
-    azSxz[q] = gzc.z * vzSxz + gzc.w * dzSxz * dt;
-    axSxy[q] = gxc.z * vxSxy + gxc.w * dxSxy * dt;
-    aySyy[q] = gye.z * vySyy + gye.w * dySyy * dt;
-    azSyz[q] = gzc.z * vzSyz + gzc.w * dzSyz * dt;
-    axSxz[q] = gxc.z * vxSxz + gxc.w * dxSxz * dt;
-    aySyz[q] = gyc.z * vySyz + gyc.w * dySyz * dt;
-    azSzz[q] = gze.z * vzSzz + gze.w * dzSzz * dt;
+    sts(&axSxx[q], gxe.z * vxSxx + gxe.w * dxSxx * dt);
+    sts(&aySxy[q], gyc.z * vySxy + gyc.w * dySxy * dt);
+    sts(&azSxz[q], gzc.z * vzSxz + gzc.w * dzSxz * dt);
+    sts(&axSxy[q], gxc.z * vxSxy + gxc.w * dxSxy * dt);
+    sts(&aySyy[q], gye.z * vySyy + gye.w * dySyy * dt);
+    sts(&azSyz[q], gzc.z * vzSyz + gzc.w * dzSyz * dt);
+    sts(&axSxz[q], gxc.z * vxSxz + gxc.w * dxSxz * dt);
+    sts(&aySyz[q], gyc.z * vySyz + gyc.w * dySyz * dt);
+    sts(&azSzz[q], gze.z * vzSzz + gze.w * dzSzz * dt);
 }
 
 // ---------------------------------------------------------------------------
 // stress: kernel__update_stress (m_kernel.f90:142-326) +
 //         absorb_p__update_stress (m_absorb_p.f90:424-503)
 // ---------------------------------------------------------------------------
-template <int NM>
-__global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
+template <int NM, int MINB>
+__global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const Geo g = a.g;
     const int k = 1 + blockIdx.x * 32 + threadIdx.x;
     const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -137,10 +170,37 @@ __global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
     const float *__restrict__ Vx = a.Vx;
     const float *__restrict__ Vy = a.Vy;
     const float *__restrict__ Vz = a.Vz;
+    float *__restrict__ Sxx = a.Sxx;
+    float *__restrict__ Syy = a.Syy;
+    float *__restrict__ Szz = a.Szz;
+    float *__restrict__ Syz = a.Syz;
+    float *__restrict__ Sxz = a.Sxz;
+    float *__restrict__ Sxy = a.Sxy;
     const float dt = a.dt;
 
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         if (!(a.mask & 1)) return;
+        // every operand of the cell first (see the velocity kernel)
+        float r[6][NM > 0 ? NM : 1];
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+#pragma unroll
+            for (int m = 0; m < NM; m++) r[c][m] = lds(&a.R[c * 3 + m][e]);
+        const float sxx = lds(&Sxx[e]), syy = lds(&Syy[e]), szz = lds(&Szz[e]);
+        const float syz = lds(&Syz[e]), sxz = lds(&Sxz[e]), sxy = lds(&Sxy[e]);
+        const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
+        const float taup1 = lds(&a.taup[e]), taus1 = lds(&a.taus[e]);
+        const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
+        const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
+        const float vxim = __ldg(&Vx[e - PI]), vxip = __ldg(&Vx[e + PI]), vxim2 = __ldg(&Vx[e - 2 * PI]);
+        const float vxjp = __ldg(&Vx[e + PJ]), vxjp2 = __ldg(&Vx[e + 2 * PJ]), vxjm = __ldg(&Vx[e - PJ]);
+        const float vxkp = __ldg(&Vx[e + 1]), vxkp2 = __ldg(&Vx[e + 2]), vxkm = __ldg(&Vx[e - 1]);
+        const float vyjm = __ldg(&Vy[e - PJ]), vyjp = __ldg(&Vy[e + PJ]), vyjm2 = __ldg(&Vy[e - 2 * PJ]);
+        const float vyip = __ldg(&Vy[e + PI]), vyip2 = __ldg(&Vy[e + 2 * PI]), vyim = __ldg(&Vy[e - PI]);
+        const float vykp = __ldg(&Vy[e + 1]), vykp2 = __ldg(&Vy[e + 2]), vykm = __ldg(&Vy[e - 1]);
+        const float vzkm = __ldg(&Vz[e - 1]), vzkp = __ldg(&Vz[e + 1]), vzkm2 = __ldg(&Vz[e - 2]);
+        const float vzip = __ldg(&Vz[e + PI]), vzip2 = __ldg(&Vz[e + 2 * PI]), vzim = __ldg(&Vz[e - PI]);
+        const float vzjp = __ldg(&Vz[e + PJ]), vzjp2 = __ldg(&Vz[e + 2 * PJ]), vzjm = __ldg(&Vz[e - PJ]);
         const int4 bd = __ldg(&a.band[col]);
         const int p1 = (k - bd.x) * (bd.y - k);
         const int p2 = (k - bd.z) * (bd.w - k);
@@ -149,16 +209,12 @@ __global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
         const float re40y = a.e40[1][s], re41y = a.e41[1][s];
         const float re40z = a.e40[2][s], re41z = a.e41[2][s];
 
-        const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
         // normal components (m_kernel.f90:195-235)
-        const float dxVx = (vx0 - __ldg(&Vx[e - PI])) * re40x - (__ldg(&Vx[e + PI]) - __ldg(&Vx[e - 2 * PI])) * re41x;
-        const float dyVy = (vy0 - __ldg(&Vy[e - PJ])) * re40y - (__ldg(&Vy[e + PJ]) - __ldg(&Vy[e - 2 * PJ])) * re41y;
-        const float dzVz = (vz0 - __ldg(&Vz[e - 1])) * re40z - (__ldg(&Vz[e + 1]) - __ldg(&Vz[e - 2])) * re41z;
-        const float mu = __ldg(&a.mu[e]);
+        const float dxVx = (vx0 - vxim) * re40x - (vxip - vxim2) * re41x;
+        const float dyVy = (vy0 - vyjm) * re40y - (vyjp - vyjm2) * re41y;
+        const float dzVz = (vz0 - vzkm) * re40z - (vzkp - vzkm2) * re41z;
         const float mu2 = 2 * mu;
-        const float lam2mu = __ldg(&a.lam[e]) + mu2;
-        const float taup1 = __ldg(&a.taup[e]);
-        const float taus1 = __ldg(&a.taus[e]);
+        const float lam2mu = lam + mu2;
         const float d3v3 = dxVx + dyVy + dzVz;
         const float dyVy_dzVz = dyVy + dzVz;
         const float dxVx_dzVz = dxVx + dzVz;
@@ -166,52 +222,43 @@ __global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
         float Rxx_n = 0.0f, Ryy_n = 0.0f, Rzz_n = 0.0f;
 #pragma unroll
         for (int m = 0; m < NM; m++) {
-            float *Rxx = a.R[0 * 3 + m];
-            float *Ryy = a.R[1 * 3 + m];
-            float *Rzz = a.R[2 * 3 + m];
-            const float rxx = a.c1[m] * Rxx[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dyVy_dzVz) * dt;
-            const float ryy = a.c1[m] * Ryy[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dzVz) * dt;
-            const float rzz = a.c1[m] * Rzz[e] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dyVy) * dt;
-            Rxx[e] = rxx;
-            Ryy[e] = ryy;
-            Rzz[e] = rzz;
-            Rxx_n = Rxx_n + a.d1[m] * rxx;
-            Ryy_n = Ryy_n + a.d1[m] * ryy;
-            Rzz_n = Rzz_n + a.d1[m] * rzz;
+            r[0][m] = a.c1[m] * r[0][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dyVy_dzVz) * dt;
+            r[1][m] = a.c1[m] * r[1][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dzVz) * dt;
+            r[2][m] = a.c1[m] * r[2][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dyVy) * dt;
+            Rxx_n = Rxx_n + a.d1[m] * r[0][m];
+            Ryy_n = Ryy_n + a.d1[m] * r[1][m];
+            Rzz_n = Rzz_n + a.d1[m] * r[2][m];
         }
         const float taup_plus1 = 1 + taup1 * (1 + a.d2);
         const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-        a.Sxx[e] = a.Sxx[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt;
-        a.Syy[e] = a.Syy[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt;
-        a.Szz[e] = a.Szz[e] + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt;
+        sts(&Sxx[e], sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt);
+        sts(&Syy[e], syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt);
+        sts(&Szz[e], szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt);
 
         // shear components (m_kernel.f90:282-311)
-        const float dxVy_dyVx = (__ldg(&Vy[e + PI]) - vy0) * re40x - (__ldg(&Vy[e + 2 * PI]) - __ldg(&Vy[e - PI])) * re41x
-                              + (__ldg(&Vx[e + PJ]) - vx0) * re40y - (__ldg(&Vx[e + 2 * PJ]) - __ldg(&Vx[e - PJ])) * re41y;
-        const float dxVz_dzVx = (__ldg(&Vz[e + PI]) - vz0) * re40x - (__ldg(&Vz[e + 2 * PI]) - __ldg(&Vz[e - PI])) * re41x
-                              + (__ldg(&Vx[e + 1]) - vx0) * re40z - (__ldg(&Vx[e + 2]) - __ldg(&Vx[e - 1])) * re41z;
-        const float dyVz_dzVy = (__ldg(&Vz[e + PJ]) - vz0) * re40y - (__ldg(&Vz[e + 2 * PJ]) - __ldg(&Vz[e - PJ])) * re41y
-                              + (__ldg(&Vy[e + 1]) - vy0) * re40z - (__ldg(&Vy[e + 2]) - __ldg(&Vy[e - 1])) * re41z;
-        const float muyz = __ldg(&a.muyz[e]), muxz = __ldg(&a.muxz[e]), muxy = __ldg(&a.muxy[e]);
+        const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
+                              + (vxjp - vx0) * re40y - (vxjp2 - vxjm) * re41y;
+        const float dxVz_dzVx = (vzip - vz0) * re40x - (vzip2 - vzim) * re41x
+                              + (vxkp - vx0) * re40z - (vxkp2 - vxkm) * re41z;
+        const float dyVz_dzVy = (vzjp - vz0) * re40y - (vzjp2 - vzjm) * re41y
+                              + (vykp - vy0) * re40z - (vykp2 - vykm) * re41z;
         float Ryz_n = 0.0f, Rxz_n = 0.0f, Rxy_n = 0.0f;
 #pragma unroll
         for (int m = 0; m < NM; m++) {
-            float *Ryz = a.R[3 * 3 + m];
-            float *Rxz = a.R[4 * 3 + m];
-            float *Rxy = a.R[5 * 3 + m];
-            const float ryz = a.c1[m] * Ryz[e] - a.c2[m] * muyz * taus1 * dyVz_dzVy * dt;
-            const float rxz = a.c1[m] * Rxz[e] - a.c2[m] * muxz * taus1 * dxVz_dzVx * dt;
-            const float rxy = a.c1[m] * Rxy[e] - a.c2[m] * muxy * taus1 * dxVy_dyVx * dt;
-            Ryz[e] = ryz;
-            Rxz[e] = rxz;
-            Rxy[e] = rxy;
-            Ryz_n = Ryz_n + a.d1[m] * ryz;
-            Rxz_n = Rxz_n + a.d1[m] * rxz;
-            Rxy_n = Rxy_n + a.d1[m] * rxy;
+            r[3][m] = a.c1[m] * r[3][m] - a.c2[m] * muyz * taus1 * dyVz_dzVy * dt;
+            r[4][m] = a.c1[m] * r[4][m] - a.c2[m] * muxz * taus1 * dxVz_dzVx * dt;
+            r[5][m] = a.c1[m] * r[5][m] - a.c2[m] * muxy * taus1 * dxVy_dyVx * dt;
+            Ryz_n = Ryz_n + a.d1[m] * r[3][m];
+            Rxz_n = Rxz_n + a.d1[m] * r[4][m];
+            Rxy_n = Rxy_n + a.d1[m] * r[5][m];
         }
-        a.Syz[e] = a.Syz[e] + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt;
-        a.Sxz[e] = a.Sxz[e] + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt;
-        a.Sxy[e] = a.Sxy[e] + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt;
+        sts(&Syz[e], syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt);
+        sts(&Sxz[e], sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt);
+        sts(&Sxy[e], sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt);
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+#pragma unroll
+            for (int m = 0; m < NM; m++) sts(&a.R[c * 3 + m][e], r[c][m]);
         return;
     }
 
@@ -219,18 +266,6 @@ __global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
     if (!(a.mask & 2)) return;
     const int2 pc = __ldg(&a.pmlcol[col]);
     const long long q = (long long)pc.y + (k - pc.x);
-    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
-    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
-    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
-    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
-    const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
-
-    const float dxVx = (vx0 - __ldg(&Vx[e - PI])) * r20x;
-    const float dyVy = (vy0 - __ldg(&Vy[e - PJ])) * r20y;
-    const float dzVz = (vz0 - __ldg(&Vz[e - 1])) * r20z;
-    const float mu = __ldg(&a.mu[e]);
-    const float lam2mu_R = (__ldg(&a.lam[e]) + 2 * mu);
-    const float lam_R = lam2mu_R - 2 * mu;
     float *__restrict__ axVx = a.aV[0];
     float *__restrict__ ayVx = a.aV[1];
     float *__restrict__ azVx = a.aV[2];
@@ -240,46 +275,82 @@ __global__ void __launch_bounds__(256) stress3d_kernel(const Str3Args a) {
     float *__restrict__ axVz = a.aV[6];
     float *__restrict__ ayVz = a.aV[7];
     float *__restrict__ azVz = a.aV[8];
-    const float vaxVx = axVx[q], vayVy = ayVy[q], vazVz = azVz[q];
+    const float vaxVx = lds(&axVx[q]), vayVy = lds(&ayVy[q]), vazVz = lds(&azVz[q]);
+    const float vayVx = lds(&ayVx[q]), vazVx = lds(&azVx[q]), vaxVy = lds(&axVy[q]);
+    const float vazVy = lds(&azVy[q]), vaxVz = lds(&axVz[q]), vayVz = lds(&ayVz[q]);
+    const float sxx = lds(&Sxx[e]), syy = lds(&Syy[e]), szz = lds(&Szz[e]);
+    const float syz = lds(&Syz[e]), sxz = lds(&Sxz[e]), sxy = lds(&Sxy[e]);
+    const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
+    const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
+    const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
+    const float vxim = __ldg(&Vx[e - PI]), vyjm = __ldg(&Vy[e - PJ]), vzkm = __ldg(&Vz[e - 1]);
+    const float vyip = __ldg(&Vy[e + PI]), vzip = __ldg(&Vz[e + PI]);
+    const float vxjp = __ldg(&Vx[e + PJ]), vzjp = __ldg(&Vz[e + PJ]);
+    const float vxkp = __ldg(&Vx[e + 1]), vykp = __ldg(&Vy[e + 1]);
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+
+    const float dxVx = (vx0 - vxim) * r20x;
+    const float dyVy = (vy0 - vyjm) * r20y;
+    const float dzVz = (vz0 - vzkm) * r20z;
+    const float lam2mu_R = (lam + 2 * mu);
+    const float lam_R = lam2mu_R - 2 * mu;
     const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
     const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
     const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
-    a.Sxx[e] = a.Sxx[e] + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt;
-    a.Syy[e] = a.Syy[e] + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt;
-    a.Szz[e] = a.Szz[e] + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt;
-    axVx[q] = gxc.z * vaxVx + gxc.w * dxVx * dt;
-    ayVy[q] = gyc.z * vayVy + gyc.w * dyVy * dt;
-    azVz[q] = gzc.z * vazVz + gzc.w * dzVz * dt;
+    sts(&Sxx[e], sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt);
+    sts(&Syy[e], syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt);
+    sts(&Szz[e], szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt);
+    sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
+    sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
+    sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
 
-    const float dxVy = (__ldg(&Vy[e + PI]) - vy0) * r20x;
-    const float dxVz = (__ldg(&Vz[e + PI]) - vz0) * r20x;
-    const float dyVx = (__ldg(&Vx[e + PJ]) - vx0) * r20y;
-    const float dyVz = (__ldg(&Vz[e + PJ]) - vz0) * r20y;
-    const float dzVx = (__ldg(&Vx[e + 1]) - vx0) * r20z;
-    const float dzVy = (__ldg(&Vy[e + 1]) - vy0) * r20z;
-    const float vayVx = ayVx[q], vazVx = azVx[q], vaxVy = axVy[q];
-    const float vazVy = azVy[q], vaxVz = axVz[q], vayVz = ayVz[q];
-    a.Syz[e] = a.Syz[e] + __ldg(&a.muyz[e]) * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt;
-    a.Sxz[e] = a.Sxz[e] + __ldg(&a.muxz[e]) * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt;
-    a.Sxy[e] = a.Sxy[e] + __ldg(&a.muxy[e]) * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt;
-    ayVx[q] = gye.z * vayVx + gye.w * dyVx * dt;
-    azVx[q] = gze.z * vazVx + gze.w * dzVx * dt;
-    axVy[q] = gxe.z * vaxVy + gxe.w * dxVy * dt;
-    azVy[q] = gze.z * vazVy + gze.w * dzVy * dt;
-    axVz[q] = gxe.z * vaxVz + gxe.w * dxVz * dt;
-    ayVz[q] = gye.z * vayVz + gye.w * dyVz * dt;
+    const float dxVy = (vyip - vy0) * r20x;
+    const float dxVz = (vzip - vz0) * r20x;
+    const float dyVx = (vxjp - vx0) * r20y;
+    const float dyVz = (vzjp - vz0) * r20y;
+    const float dzVx = (vxkp - vx0) * r20z;
+    const float dzVy = (vykp - vy0) * r20z;
+    sts(&Syz[e], syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt);
+    sts(&Sxz[e], sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt);
+    sts(&Sxy[e], sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt);
+    sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
+    sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
+    sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
+    sts(&azVy[q], gze.z * vazVy + gze.w * dzVy * dt);
+    sts(&axVz[q], gxe.z * vaxVz + gxe.w * dxVz * dt);
+    sts(&ayVz[q], gye.z * vayVz + gye.w * dyVz * dt);
 }
 
-void launch_vel3d(const Vel3Args &a, dim3 grid, dim3 block, cudaStream_t st) {
-    vel3d_kernel<<<grid, block, 0, st>>>(a);
+// MINB (minimum resident blocks per SM) trades registers for occupancy; the
+// launch table picks it per kernel (swpc_set_launch)
+void launch_vel3d(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st) {
+    switch (minb) {
+    case 1: vel3d_kernel<1><<<grid, block, 0, st>>>(a); break;
+    case 2: vel3d_kernel<2><<<grid, block, 0, st>>>(a); break;
+    case 3: vel3d_kernel<3><<<grid, block, 0, st>>>(a); break;
+    default: vel3d_kernel<4><<<grid, block, 0, st>>>(a); break;
+    }
 }
 
-void launch_stress3d(const Str3Args &a, int nm, dim3 grid, dim3 block, cudaStream_t st) {
+template <int NM>
+static void stress_minb(const Str3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st) {
+    switch (minb) {
+    case 1: stress3d_kernel<NM, 1><<<grid, block, 0, st>>>(a); break;
+    case 2: stress3d_kernel<NM, 2><<<grid, block, 0, st>>>(a); break;
+    case 3: stress3d_kernel<NM, 3><<<grid, block, 0, st>>>(a); break;
+    default: stress3d_kernel<NM, 4><<<grid, block, 0, st>>>(a); break;
+    }
+}
+
+void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st) {
     switch (nm) {
-    case 0: stress3d_kernel<0><<<grid, block, 0, st>>>(a); break;
-    case 1: stress3d_kernel<1><<<grid, block, 0, st>>>(a); break;
-    case 2: stress3d_kernel<2><<<grid, block, 0, st>>>(a); break;
-    default: stress3d_kernel<3><<<grid, block, 0, st>>>(a); break;
+    case 0: stress_minb<0>(a, minb, grid, block, st); break;
+    case 1: stress_minb<1>(a, minb, grid, block, st); break;
+    case 2: stress_minb<2>(a, minb, grid, block, st); break;
+    default: stress_minb<3>(a, minb, grid, block, st); break;
     }
 }
 

@@ -164,6 +164,16 @@ extern "C" const char *swpc_last_error(const swpc_ctx *c) { return c ? c->err.c_
 extern "C" void *swpc_stream(swpc_ctx *c) { return c ? (void *)c->stream : nullptr; }
 extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes : 0; }
 
+extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj) {
+    if (!c) return SWPC_ERR_ARG;
+    if (kernel < 0 || kernel > 1 || minb < 1 || minb > 4 || bi < 1 || bj < 1 || 32 * bi * bj > 256)
+        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0/1, minb 1..4, 32*bi*bj <= 256)");
+    invalidate_graph(c);
+    if (kernel == 0) { c->stress_minb = minb; c->bi = bi; c->bj = bj; }
+    else { c->vel_minb = minb; c->vbi = bi; c->vbj = bj; }
+    return SWPC_OK;
+}
+
 extern "C" int swpc_sync(swpc_ctx *c) {
     if (!c) return SWPC_ERR_ARG;
     CK(cudaStreamSynchronize(c->stream));
@@ -615,7 +625,7 @@ static int launch_stress(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
-    launch_stress3d(a, c->d.nm, grid, block, c->stream);
+    launch_stress3d(a, c->d.nm, c->stress_minb, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "stress3d launch");
 }
 
@@ -634,9 +644,9 @@ static int launch_vel(swpc_ctx *c, int mask) {
     memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
     a.dt = c->d.dt;
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
-    dim3 block(32, c->bi, c->bj);
-    dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
-    launch_vel3d(a, grid, block, c->stream);
+    dim3 block(32, c->vbi, c->vbj);
+    dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
+    launch_vel3d(a, c->vel_minb, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "vel3d launch");
 }
 

@@ -126,8 +126,10 @@ struct swpc_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_key = -1;
 
-    // launch shape
-    int bi = 4, bj = 2;
+    // launch shape (swpc_set_launch): block = 32 x bi x bj threads; minb =
+    // minimum resident blocks per SM the kernels are compiled for
+    int bi = 2, bj = 1, vbi = 2, vbj = 2;
+    int stress_minb = 2, vel_minb = 4;
 
     long long bytes = 0;
 };

@@ -81,8 +81,8 @@ struct VmaxArgs {
     unsigned int *out;
 };
 
-void launch_vel3d(const Vel3Args &a, dim3 grid, dim3 block, cudaStream_t st);
-void launch_stress3d(const Str3Args &a, int nm, dim3 grid, dim3 block, cudaStream_t st);
+void launch_vel3d(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st);
+void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st);
 void launch_inject(const InjArgs &a, cudaStream_t st);
 void launch_wav3d(const Wav3Args &a, cudaStream_t st);
 void launch_vmax3d(const VmaxArgs &a, cudaStream_t st);

@@ -48,12 +48,12 @@ def oracle_aux_as_box(o, name, p):
     a = o.array(name)   # (ny, nx, nka) from kbeg_min
     box = np.zeros((p.ny + 6, p.nx + 6, p.nz + 6), np.float32)
     kb = d["kbeg_min"]
-    box[2:p.ny + 2, 2:p.nx + 2, kb + 2:p.nz + 3] = a
+    box[3:p.ny + 3, 3:p.nx + 3, kb + 2:p.nz + 3] = a
     # only absorber cells are defined
     kbeg_a = o.array("kbeg_a")
     mask = np.zeros_like(box, bool)
     kk = np.arange(p.nz + 6)[None, None, :] - 2
-    mask[2:p.ny + 2, 2:p.nx + 2, :] = True
+    mask[3:p.ny + 3, 3:p.nx + 3, :] = True
     mask &= kk >= kbeg_a[:, :, None]
     mask &= kk <= p.nz
     return np.where(mask, box, 0.0).astype(np.float32)
@@ -121,7 +121,10 @@ def test_random_state_single_step_all_paths():
     for q, name in enumerate(AUX_NAMES):
         a = rng.standard_normal((p.ny, p.nx, d["nka"])).astype(np.float32)
         o.set_array(name, a)
-        g.upload(_lib.F_AUX + q, oracle_aux_as_box(o, name, p))
+        box = oracle_aux_as_box(o, name, p)
+        o.set_array(name, box[3:p.ny + 3, 3:p.nx + 3, d["kbeg_min"] + 2:p.nz + 3])   # zero outside the absorber
+        g.upload(_lib.F_AUX + q, box)
+        assert same_bits(g.download(_lib.F_AUX + q), box)
     for it in (1, 2):
         g.step(it)
         o.step(it)
@@ -222,7 +225,7 @@ def test_vmax_and_divergence_detection():
     o.run(1, 20)
     assert same_bits(g.kernel__vmax(), o.vmax())
     v = g.download(_lib.F_VZ)
-    v[p.ny // 2 + 2, p.nx // 2 + 2, 5] = 1e25
+    v[p.ny // 2 + 2, p.nx // 2 + 2, 3 + 1 + 2] = 1e25   # k = kob + 1 = 4
     g.upload(_lib.F_VZ, v)
     with pytest.raises(_lib.SwpcError) as e:
         g.kernel__vmax()
