@@ -214,13 +214,15 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
 /* Device bytes held by the context. */
 long long swpc_device_bytes(const swpc_ctx *ctx);
 
-/* Launch shape of a fused kernel (kernel 0 = stress, 1 = velocity): block =
- * 32 (k) x bi (i) x bj (j) threads (32*bi*bj <= 256); minb = minimum
- * resident blocks per SM the kernel variant is compiled for (1..4; fewer
- * blocks leave more registers for operands in flight).  Defaults come from a
- * sweep on B200 (stress: minb 2, 2 x 1; velocity: minb 4, 2 x 2).  No
- * counterpart in the reference (its OpenMP/OpenACC schedules are fixed at
- * compile time); results do not depend on the shape. */
+/* Launch variant of the fused kernels.  kernel 0 / 1 select the flat stress /
+ * velocity kernels (one thread per cell, block = 32 (k) x bi (i) x bj (j)
+ * threads, 32*bi*bj <= 256); kernel 2 / 3 select the 2.5D marching stress /
+ * velocity kernels (a 32 x 8 (k, i) tile walking bj planes along j; bi is
+ * ignored).  minb = minimum resident blocks per SM the variant is compiled
+ * for (1..4; fewer blocks leave more registers for operands in flight).
+ * The defaults come from sweeps on B200.  No counterpart in the reference
+ * (its OpenMP/OpenACC schedules are fixed at compile time); results are
+ * bitwise independent of the variant. */
 int swpc_set_launch(swpc_ctx *ctx, int kernel, int minb, int bi, int bj);
 
 #ifdef __cplusplus

@@ -166,11 +166,16 @@ extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes 
 
 extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj) {
     if (!c) return SWPC_ERR_ARG;
-    if (kernel < 0 || kernel > 1 || minb < 1 || minb > 4 || bi < 1 || bj < 1 || 32 * bi * bj > 256)
-        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0/1, minb 1..4, 32*bi*bj <= 256)");
+    if (kernel < 0 || kernel > 3 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
+        (kernel < 2 && 32 * bi * bj > 256))
+        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..3, minb 1..4, 32*bi*bj <= 256)");
     invalidate_graph(c);
-    if (kernel == 0) { c->stress_minb = minb; c->bi = bi; c->bj = bj; }
-    else { c->vel_minb = minb; c->vbi = bi; c->vbj = bj; }
+    switch (kernel) {
+    case 0: c->stress_march = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
+    case 1: c->vel_march = false; c->vel_minb = minb; c->vbi = bi; c->vbj = bj; break;
+    case 2: c->stress_march = true; c->stress_mminb = minb; c->stress_jc = bj; break;
+    default: c->vel_march = true; c->vel_mminb = minb; c->vel_jc = bj; break;
+    }
     return SWPC_OK;
 }
 
@@ -625,7 +630,8 @@ static int launch_stress(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
-    launch_stress3d(a, c->d.nm, c->stress_minb, grid, block, c->stream);
+    if (c->stress_march) launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
+    else launch_stress3d(a, c->d.nm, c->stress_minb, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "stress3d launch");
 }
 
@@ -646,7 +652,8 @@ static int launch_vel(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
-    launch_vel3d(a, c->vel_minb, grid, block, c->stream);
+    if (c->vel_march) launch_vel3d_march(a, c->vel_mminb, c->vel_jc, c->stream);
+    else launch_vel3d(a, c->vel_minb, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "vel3d launch");
 }
 

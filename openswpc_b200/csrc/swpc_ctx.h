@@ -130,6 +130,9 @@ struct swpc_ctx {
     // minimum resident blocks per SM the kernels are compiled for
     int bi = 2, bj = 1, vbi = 2, vbj = 2;
     int stress_minb = 2, vel_minb = 4;
+    // 2.5D marching variants (32 x 8 plane tile walking jc planes along j)
+    bool stress_march = false, vel_march = false;
+    int stress_jc = 8, vel_jc = 8, stress_mminb = 2, vel_mminb = 2;
 
     long long bytes = 0;
 };

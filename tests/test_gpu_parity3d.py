@@ -242,3 +242,21 @@ def test_larger_grid_against_oracle_few_steps():
         g.step(it)
         o.step(it)
     compare_state(g, o, p)
+
+
+@pytest.mark.parametrize("variant", [(0, 2, 2, 1, 1, 4, 2, 2), (0, 1, 4, 2, 1, 3, 8, 1), (2, 2, 1, 16, 3, 2, 1, 7),
+                                     (2, 1, 1, 64, 3, 1, 1, 3)])
+def test_launch_variants_are_bitwise_identical(variant):
+    """Flat and marching kernels, any block shape or chunk length: same bits."""
+    ks, ms, bis, bjs, kv, mv, biv, bjv = variant
+    p = small3d(nx=44, ny=38, nz=70, na=8, nt=25)
+    g0 = Swpc3D(p)
+    g1 = Swpc3D(p)
+    _lib.check(g1.ctx, g1.lib.swpc_set_launch(g1.ctx, ks, ms, bis, bjs))
+    _lib.check(g1.ctx, g1.lib.swpc_set_launch(g1.ctx, kv, mv, biv, bjv))
+    g0.run(1, p.nt)
+    g1.run(1, p.nt)
+    for n in range(9):
+        assert same_bits(g0.download(n), g1.download(n)), n
+    for q in range(18):
+        assert same_bits(g0.download(_lib.F_AUX + q), g1.download(_lib.F_AUX + q)), q
