@@ -225,6 +225,26 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * bitwise independent of the variant. */
 int swpc_set_launch(swpc_ctx *ctx, int kernel, int minb, int bi, int bj);
 
+/* ---- batched 2D ensemble ----------------------------------------------- */
+
+/* Many independent 2D runs (P-SV or SH, same nm and device, each a fully set
+ * up context with its own medium, sources and stations) advanced together:
+ * every half step is ONE persistent launch over the tiles of all members,
+ * and swpc_batch_run replays the captured step as a CUDA graph.  This
+ * replaces the reference's one-process-per-run ensemble loop
+ * (work/auto_chengyu.py:68-110) and has no counterpart inside the solver.
+ * The batch snapshots its members at creation: set every member up first.
+ * Batch work runs on the batch's own stream; call swpc_batch_sync before
+ * reading a member's fields or traces. */
+typedef struct swpc_batch swpc_batch;
+int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **out);
+int swpc_batch_step(swpc_batch *b, int it);
+int swpc_batch_run(swpc_batch *b, int it0, int nsteps);
+int swpc_batch_sync(swpc_batch *b);
+int swpc_batch_time_steps(swpc_batch *b, int it0, int nsteps, float *ms);
+const char *swpc_batch_last_error(const swpc_batch *b);
+int swpc_batch_destroy(swpc_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,18 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
                       float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
                       int *kob_top, int *kob_bot, float *ts, float *scal);
 
+/* medium__setup of the 2D codes after the vmodel (src/swpc_psv/m_medium.f90:124-281,
+ * src/swpc_sh/m_medium.f90): absorber homogenisation in x and at the bottom,
+ * tau-method, relaxed moduli through visco_chi (m_fdtool.f90:730-753),
+ * free-surface / ocean-bottom detection and velocity range.  Arrays over
+ * (-2:nz+3, -2:nx+3); maps over (-2:nx+3).  The 2nd-order band is formed as
+ * in the 3D code (kfs_top = max(min-2, 1), kfs_bot = min(max+2, nz)): the 2D
+ * reference assigns kfs_top twice and leaves kfs_bot undefined
+ * (src/swpc_psv/m_medium.f90:241-242, src/swpc_sh/m_medium.f90:247-248). */
+int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                         float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs, int *kob,
+                         int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal);
+
 /* damping_profile (src/swpc_3d/m_absorb_p.f90:507-547) for the six profiles
  * of absorb_p__setup (:79-93); each output is g(4, n). */
 void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gxe, float *gyc, float *gye, float *gzc,

@@ -39,7 +39,9 @@ EXPORTS = [
     "swpc_download_field", "swpc_upload_field", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
-    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles",
+    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
+    "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps",
+    "swpc_batch_last_error", "swpc_batch_destroy",
 ]
 
 
@@ -134,6 +136,15 @@ def load():
         "swpc_setup_medium": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP,
                                   _FP, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _FP, _FP]),
         "swpc_damping_profiles": (None, [C.POINTER(Grid), f, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "swpc_setup_medium_2d": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _IP, _IP, _IP,
+                                     _IP, _IP, _IP, _FP, _FP]),
+        "swpc_batch_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),
+        "swpc_batch_step": (i, [vp, i]),
+        "swpc_batch_run": (i, [vp, i, i]),
+        "swpc_batch_sync": (i, [vp]),
+        "swpc_batch_time_steps": (i, [vp, i, i, _FP]),
+        "swpc_batch_last_error": (C.c_char_p, [vp]),
+        "swpc_batch_destroy": (i, [vp]),
     }
     for name in ("swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
                  "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_comm_stress",

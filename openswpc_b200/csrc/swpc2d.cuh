@@ -1,0 +1,53 @@
+// swpc2d.cuh -- device descriptors of the 2D P-SV / SH solvers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "swpc_ctx.h"
+
+namespace swpc {
+
+// One 2D model as the kernels see it (device-resident, one per ensemble
+// member).  Cell (k, i) of a field is at (i + 2) * Kp + (k - 1 + KH).
+//   P-SV: V0 = Vx, V1 = Vz; S0 = Sxx, S1 = Szz, S2 = Sxz; R[c*3+m], c = xx zz xz
+//         aux = axVx azVx axVz azVz axSxx azSxz axSxz azSzz
+//   SH:   V0 = Vy;          S0 = Syz, S1 = Sxy;          R[c*3+m], c = yz xy
+//         aux = axVy azVy axSxy azSyz
+struct Model2D {
+    int nx, nz, Kp, nm;
+    int ibk, iek, kek;
+    float dt;
+    float *V0, *V1;
+    float *S0, *S1, *S2;
+    float *R[9];
+    const float *rho, *lam, *mu, *taup, *taus;
+    const int4 *band;     // [i + 2]: kfs_top kfs_bot kob_top kob_bot
+    const int2 *pmlcol;   // [i + 2]: kbeg_a, aux base
+    float *aux[8];
+    const float4 *gxc, *gxe, *gzc, *gze;
+    float e40[2][2], e41[2][2];   // [axis x/z][0: 4th order, 1: 2nd-order band]
+    float r20[2];
+    float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
+};
+
+struct Tile2D {
+    int model, k0, i0, pad;
+};
+
+struct Wav2Args {
+    int Kp, nst, ntw, ntdec_w, what, psv;
+    const int *st;            // (2, nst) i k
+    const float *V0, *V1;
+    float *uacc;              // (2, nst)
+    float *wav_v, *wav_u;     // (ntw, ncmp, nst)
+    float M0, UC, dt;
+};
+
+void launch_stress2d(int kind, int nm, const Model2D *models, const Tile2D *tiles, int ntiles, int mask,
+                     cudaStream_t st);
+void launch_vel2d(int kind, const Model2D *models, const Tile2D *tiles, int ntiles, int mask, cudaStream_t st);
+void launch_wav2d(const Wav2Args *list, int nlist, int max_nst, int it, const int *d_it, cudaStream_t st);
+void launch_vmax2d(const float *V0, const float *V1, const int *kob, int Kp, int i0, int i1, unsigned int *out,
+                   cudaStream_t st);
+
+}  // namespace swpc

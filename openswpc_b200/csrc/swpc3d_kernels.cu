@@ -416,6 +416,30 @@ __global__ void inject_kernel(const InjArgs a) {
     if (n < a.n) apply_entry(a, a.list[n], it);
 }
 
+// many injection lists in one launch (batched ensembles): blockIdx.y picks
+// the list; each list keeps its own serial / parallel mode
+__global__ void inject_multi_kernel(const InjArgs *__restrict__ list, int nlist, const int *d_it, int it_arg) {
+    const int it = d_it ? *d_it : it_arg;
+    for (int b = blockIdx.y; b < nlist; b += gridDim.y) {
+        const InjArgs &a = list[b];
+        if (it < 1 || it > a.nt) continue;
+        if (a.serial) {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+                for (int n = 0; n < a.n; n++) apply_entry(a, a.list[n], it);
+            continue;
+        }
+        for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.n; n += gridDim.x * blockDim.x)
+            apply_entry(a, a.list[n], it);
+    }
+}
+
+void launch_inject_multi(const InjArgs *list, int nlist, int max_n, const int *d_it, int it, cudaStream_t st) {
+    if (!list || nlist <= 0 || max_n <= 0) return;
+    const int threads = 128;
+    const dim3 grid((max_n + threads - 1) / threads, nlist < 65535 ? nlist : 65535);
+    inject_multi_kernel<<<grid, threads, 0, st>>>(list, nlist, d_it, it);
+}
+
 void launch_inject(const InjArgs &a, cudaStream_t st) {
     if (a.n <= 0) return;
     const int threads = 128;

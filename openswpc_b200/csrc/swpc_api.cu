@@ -42,6 +42,7 @@ int update_vel_2d(swpc_ctx *c, int mask);
 int wav_store_2d(swpc_ctx *c, int it, const int *d_it);
 int vmax_2d(swpc_ctx *c, float *out);
 void destroy_2d(swpc_ctx *c);
+int refresh_2d(swpc_ctx *c);
 
 }  // namespace swpc
 
@@ -59,6 +60,7 @@ void destroy_2d(swpc_ctx *c);
 static bool is3d(const swpc_ctx *c) { return c->kind == SWPC_KIND_3D; }
 
 static void invalidate_graph(swpc_ctx *c) {
+    c->desc_dirty = true;
     if (c->graph_exec) {
         cudaGraphExecDestroy(c->graph_exec);
         c->graph_exec = nullptr;
@@ -269,7 +271,7 @@ extern "C" int swpc_kernel_setup(swpc_ctx *c, const float *ts) {
     if (c->d.nm > 0 && !ts) return set_err(c, SWPC_ERR_ARG, "ts required for nm > 0");
     invalidate_graph(c);
     // m_kernel.f90:43-54 in real(MP) = single precision
-    const float dd[3] = {c->d.dx, c->d.dy, c->d.dz};
+    const float dd[3] = {c->d.dx, is3d(c) ? c->d.dy : c->d.dx, c->d.dz};
     for (int ax = 0; ax < 3; ax++) {
         const float rc40 = 17.0f / 16.0f / dd[ax];
         const float rc41 = 1.0f / 48.0f / dd[ax];
@@ -362,6 +364,23 @@ extern "C" int swpc_absorb_setup(swpc_ctx *c, const float *gxc, const float *gxe
 static bool comm_zeroed(const swpc_ctx *c, int field, int k, int i, int j) {
     const int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
     if (k < 1 || k > nz) return false;
+    auto in1 = [](int v, std::initializer_list<int> s) { return std::find(s.begin(), s.end(), v) != s.end(); };
+    if (c->kind == SWPC_KIND_PSV) {   // src/swpc_psv/m_global.f90:356-361, 409-414
+        switch (field) {
+        case SWPC_F_VX: return in1(i, {-1, 0, nx + 1});
+        case SWPC_F_VZ: return in1(i, {0, nx + 1, nx + 2});
+        case SWPC_F_SXX: return in1(i, {0, nx + 1, nx + 2});
+        case SWPC_F_SXZ: return in1(i, {-1, 0, nx + 1});
+        default: return false;
+        }
+    }
+    if (c->kind == SWPC_KIND_SH) {    // src/swpc_sh/m_global.f90:340-342, 386-388
+        switch (field) {
+        case SWPC_F_VY: return in1(i, {0, nx + 1, nx + 2});
+        case SWPC_F_SXY: return in1(i, {-1, 0, nx + 1});
+        default: return false;
+        }
+    }
     const bool jin = (j >= 1 && j <= ny), iin = (i >= 1 && i <= nx);
     auto in = [](int v, std::initializer_list<int> s) { return std::find(s.begin(), s.end(), v) != s.end(); };
     switch (field) {
@@ -400,7 +419,7 @@ static bool in_box(const swpc_ctx *c, int k, int i, int j) {
 static void add_entry(const swpc_ctx *c, std::vector<InjEntry> &v, int field, int k, int i, int j, int src, float coef,
                       int mode, int bfield, bool *bad) {
     if (!in_box(c, k, i, j)) { *bad = true; return; }
-    if (is3d(c) && comm_zeroed(c, field, k, i, j)) return;   // zeroed before anything reads it
+    if (comm_zeroed(c, field, k, i, j)) return;   // zeroed before anything reads it
     InjEntry e;
     e.cell = is3d(c) ? cell_index(c->g, k, i, j) : (long long)(i + 2) * c->g.Kp + (k - 1 + KH);
     e.field = field; e.src = src; e.coef = coef; e.mode = mode; e.bfield = bfield; e.pad = 0;
@@ -487,9 +506,37 @@ extern "C" int swpc_bodyforce_setup(swpc_ctx *c, int nsrc, const int *isrc, cons
         return set_err(c, SWPC_ERR_ARG, "body-force arrays missing");
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
-    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "2D body forces use swpc_bodyforce_setup_2d");
     std::vector<InjEntry> v;
     bool bad = false;
+    if (!is3d(c)) {
+        // src/swpc_psv/m_source.f90:642-645 and src/swpc_sh/m_source.f90:621:
+        // V += f / rho(kk, ii) * stime * dt_dxz (/2 for P-SV)
+        std::vector<long long> rc(std::max(nsrc, 1), 0);
+        for (int s = 0; s < nsrc; s++) {
+            const int ii = isrc[s], kk = ksrc[s];
+            const float *f = f3 + 3 * s;
+            if (!in_box(c, kk, ii, 1)) bad = true;
+            rc[s] = (long long)(ii + 2) * c->g.Kp + (kk - 1 + KH);
+            if (c->kind == SWPC_KIND_PSV) {
+                add_entry(c, v, SWPC_F_VX, kk, ii, 1, s, f[0], INJ_BFPSV, 0, &bad);
+                add_entry(c, v, SWPC_F_VX, kk, ii - 1, 1, s, f[0], INJ_BFPSV, 0, &bad);
+                add_entry(c, v, SWPC_F_VZ, kk, ii, 1, s, f[2], INJ_BFPSV, 0, &bad);
+                add_entry(c, v, SWPC_F_VZ, kk - 1, ii, 1, s, f[2], INJ_BFPSV, 0, &bad);
+            } else {
+                add_entry(c, v, SWPC_F_VY, kk, ii, 1, s, f[1], INJ_BFSH, 0, &bad);
+            }
+        }
+        if (bad) return set_err(c, SWPC_ERR_ARG, "body-force cell outside the memory box");
+        RC(build_list(c, v, &c->inj_bf, &c->ninj_bf, &c->bf_serial));
+        c->nsrc_bf = nsrc;
+        RC(stime_table(c, &c->stime_bf, nsrc, srcprm, stftype, false));
+        if (c->rho_cell_bf) { cudaFree(c->rho_cell_bf); c->rho_cell_bf = nullptr; }
+        RC(dalloc(c, &c->rho_cell_bf, rc.size()));
+        CK(cudaMemcpyAsync(c->rho_cell_bf, rc.data(), rc.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->dt_dxyz = c->d.dt / (c->d.dx * c->d.dz);
+        return SWPC_OK;
+    }
     for (int s = 0; s < nsrc; s++) {
         const int ii = isrc[s], jj = jsrc[s], kk = ksrc[s];
         const float *f = f3 + 3 * s;
@@ -546,13 +593,17 @@ extern "C" int swpc_wav_setup(swpc_ctx *c, int nst, const int *ist, const int *j
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
     const Geo &g = c->g;
-    std::vector<int> st(3 * (size_t)std::max(nst, 1), 0);
+    if (!is3d(c) && (what & (SWPC_WAV_STRESS | SWPC_WAV_STRAIN)))
+        return set_err(c, SWPC_ERR_ARG, "2D recorders support velocity and displacement");
+    const int per = is3d(c) ? 3 : 2;
+    std::vector<int> st(per * (size_t)std::max(nst, 1), 0);
     for (int n = 0; n < nst; n++) {
         const int i = ist[n], j = is3d(c) ? jst[n] : 1, k = kst[n];
         // stencils of wav__store reach i-2..i+2, j-2..j+2, k-2..k+2
         if (i < 1 || i > g.nx || k < 1 || k > g.nz || (is3d(c) && (j < 1 || j > g.ny)))
             return set_err(c, SWPC_ERR_ARG, "station cell outside the domain");
-        st[3 * n] = i; st[3 * n + 1] = j; st[3 * n + 2] = k;
+        if (is3d(c)) { st[3 * n] = i; st[3 * n + 1] = j; st[3 * n + 2] = k; }
+        else { st[2 * n] = i; st[2 * n + 1] = k; }
     }
     c->nst = nst;
     c->ntdec_w = ntdec_w;
@@ -564,7 +615,8 @@ extern "C" int swpc_wav_setup(swpc_ctx *c, int nst, const int *ist, const int *j
     if (c->st_ijk) { cudaFree(c->st_ijk); c->st_ijk = nullptr; }
     RC(dalloc(c, &c->st_ijk, st.size()));
     CK(cudaMemcpyAsync(c->st_ijk, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    const int ncmp[4] = {3, 3, is3d(c) ? 6 : 3, is3d(c) ? 6 : 3};
+    const int nc2 = c->kind == SWPC_KIND_PSV ? 2 : 1;
+    const int ncmp[4] = {is3d(c) ? 3 : nc2, is3d(c) ? 3 : nc2, 6, 6};
     for (int q = 0; q < 4; q++) {
         if (c->wav[q]) { cudaFree(c->wav[q]); c->wav[q] = nullptr; }
         RC(dalloc(c, &c->wav[q], (size_t)c->ntw * ncmp[q] * std::max(nst, 1)));
@@ -589,7 +641,8 @@ extern "C" int swpc_wav_fetch(swpc_ctx *c, int what, float *out) {
     int q = what == SWPC_WAV_V ? 0 : what == SWPC_WAV_U ? 1 : what == SWPC_WAV_STRESS ? 2 : what == SWPC_WAV_STRAIN ? 3 : -1;
     if (q < 0) return set_err(c, SWPC_ERR_ARG, "unknown recorder component");
     if (!c->wav[q]) return set_err(c, SWPC_ERR_STATE, "swpc_wav_setup not called");
-    const int ncmp[4] = {3, 3, is3d(c) ? 6 : 3, is3d(c) ? 6 : 3};
+    const int nc2 = c->kind == SWPC_KIND_PSV ? 2 : 1;
+    const int ncmp[4] = {is3d(c) ? 3 : nc2, is3d(c) ? 3 : nc2, 6, 6};
     CK(cudaMemcpyAsync(out, c->wav[q], (size_t)c->ntw * ncmp[q] * c->nst * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return SWPC_OK;
@@ -664,20 +717,18 @@ static void fill_inj_fields(swpc_ctx *c, InjArgs &a) {
     else { a.bfields[0] = c->med[0]; a.bfields[1] = c->med[0]; a.bfields[2] = c->med[0]; }
 }
 
-static int launch_glut(swpc_ctx *c, int it, const int *d_it) {
-    if (c->ninj_glut <= 0) return SWPC_OK;
+namespace swpc {
+InjArgs glut_args(swpc_ctx *c, int it, const int *d_it) {
     InjArgs a;
     memset(&a, 0, sizeof(a));
     a.list = c->inj_glut; a.n = c->ninj_glut; a.serial = c->glut_serial ? 1 : 0;
     a.it = it; a.d_it = d_it; a.nt = c->d.nt; a.nsrc = c->nsrc_glut;
     a.stime = c->stime_glut; a.mo = c->mo_glut; a.dt_dxyz = c->dt_dxyz;
     fill_inj_fields(c, a);
-    launch_inject(a, c->stream);
-    return cuda_check(c, cudaGetLastError(), "stressglut launch");
+    return a;
 }
 
-static int launch_bf(swpc_ctx *c, int it, const int *d_it) {
-    if (c->ninj_bf <= 0) return SWPC_OK;
+InjArgs bf_args(swpc_ctx *c, int it, const int *d_it) {
     InjArgs a;
     memset(&a, 0, sizeof(a));
     a.list = c->inj_bf; a.n = c->ninj_bf; a.serial = c->bf_serial ? 1 : 0;
@@ -685,7 +736,19 @@ static int launch_bf(swpc_ctx *c, int it, const int *d_it) {
     a.stime = c->stime_bf; a.dt_dxyz = c->dt_dxyz;
     a.rho_cell = c->rho_cell_bf;
     fill_inj_fields(c, a);
-    launch_inject(a, c->stream);
+    return a;
+}
+}  // namespace swpc
+
+static int launch_glut(swpc_ctx *c, int it, const int *d_it) {
+    if (c->ninj_glut <= 0) return SWPC_OK;
+    launch_inject(glut_args(c, it, d_it), c->stream);
+    return cuda_check(c, cudaGetLastError(), "stressglut launch");
+}
+
+static int launch_bf(swpc_ctx *c, int it, const int *d_it) {
+    if (c->ninj_bf <= 0) return SWPC_OK;
+    launch_inject(bf_args(c, it, d_it), c->stream);
     return cuda_check(c, cudaGetLastError(), "bodyforce launch");
 }
 
@@ -720,18 +783,26 @@ static int launch_wav(swpc_ctx *c, int it, const int *d_it) {
     return cuda_check(c, cudaGetLastError(), "wav launch");
 }
 
-extern "C" int swpc_kernel_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 1) : SWPC_ERR_ARG; }
-extern "C" int swpc_absorb_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 2) : SWPC_ERR_ARG; }
-extern "C" int swpc_kernel_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 1) : SWPC_ERR_ARG; }
-extern "C" int swpc_absorb_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 2) : SWPC_ERR_ARG; }
-extern "C" int swpc_update_stress(swpc_ctx *c) { return c ? launch_stress(c, 3) : SWPC_ERR_ARG; }
-extern "C" int swpc_update_vel(swpc_ctx *c) { return c ? launch_vel(c, 3) : SWPC_ERR_ARG; }
+static int prepare(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    if (!is3d(c)) RC(refresh_2d(c));
+    return SWPC_OK;
+}
+#define PREP(c) do { int _rc = prepare(c); if (_rc) return _rc; } while (0)
+
+extern "C" int swpc_kernel_update_stress(swpc_ctx *c) { PREP(c); return launch_stress(c, 1); }
+extern "C" int swpc_absorb_update_stress(swpc_ctx *c) { PREP(c); return launch_stress(c, 2); }
+extern "C" int swpc_kernel_update_vel(swpc_ctx *c) { PREP(c); return launch_vel(c, 1); }
+extern "C" int swpc_absorb_update_vel(swpc_ctx *c) { PREP(c); return launch_vel(c, 2); }
+extern "C" int swpc_update_stress(swpc_ctx *c) { PREP(c); return launch_stress(c, 3); }
+extern "C" int swpc_update_vel(swpc_ctx *c) { PREP(c); return launch_vel(c, 3); }
 extern "C" int swpc_source_stressglut(swpc_ctx *c, int it) { return c ? launch_glut(c, it, nullptr) : SWPC_ERR_ARG; }
 extern "C" int swpc_source_bodyforce(swpc_ctx *c, int it) { return c ? launch_bf(c, it, nullptr) : SWPC_ERR_ARG; }
 extern "C" int swpc_green_source(swpc_ctx *c, int it) { return c ? launch_green(c, it, nullptr) : SWPC_ERR_ARG; }
 extern "C" int swpc_comm_stress(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
 extern "C" int swpc_comm_vel(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
-extern "C" int swpc_wav_store(swpc_ctx *c, int it) { return c ? launch_wav(c, it, nullptr) : SWPC_ERR_ARG; }
+extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(c, it, nullptr); }
 
 // main.f90:125-144 loop body (report__progress and snap__write are driven
 // by the caller between steps)
@@ -739,8 +810,16 @@ static int step_body(swpc_ctx *c, int it, const int *d_it) {
     RC(launch_wav(c, it, d_it));
     RC(launch_stress(c, 3));
     RC(launch_glut(c, it, d_it));
-    RC(launch_vel(c, 3));
-    RC(launch_bf(c, it, d_it));
+    if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) {
+        // P-SV applies body forces between the interior and absorber velocity
+        // updates (src/swpc_psv/main.f90:106-110)
+        RC(launch_vel(c, 1));
+        RC(launch_bf(c, it, d_it));
+        RC(launch_vel(c, 2));
+    } else {
+        RC(launch_vel(c, 3));
+        RC(launch_bf(c, it, d_it));
+    }
     RC(launch_green(c, it, d_it));
     return SWPC_OK;
 }
@@ -748,13 +827,14 @@ static int step_body(swpc_ctx *c, int it, const int *d_it) {
 extern "C" int swpc_step(swpc_ctx *c, int it) {
     if (!c) return SWPC_ERR_ARG;
     if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
-    CK(cudaSetDevice(c->device));
+    PREP(c);
     return step_body(c, it, nullptr);
 }
 
 static int build_graph(swpc_ctx *c) {
     if (c->graph_exec) return SWPC_OK;
     RC(check_ready(c));
+    PREP(c);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = step_body(c, 0, c->d_it);
@@ -844,8 +924,28 @@ static float *field_ptr(swpc_ctx *c, int field) {
 
 static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_k, int ld_i) {
     if (!c->absorb_ready || !c->aux[q]) return set_err(c, SWPC_ERR_STATE, "swpc_absorb_setup not called");
-    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "2D auxiliaries use the 2D layout");
     const Geo &g = c->g;
+    if (!is3d(c)) {
+        std::vector<float> buf((size_t)std::max<long long>(c->npml, 1));
+        std::vector<int2> pc(g.Ip);
+        CK(cudaMemcpyAsync(pc.data(), c->pmlcol, pc.size() * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(buf.data(), c->aux[q], c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int i = -2; i <= g.nx + 3; i++) {
+            const long long h = (long long)(i + 2) * ld_k;
+            const int2 p = (i >= 1 && i <= g.nx) ? pc[i + 2] : make_int2(1, -1);
+            for (int k = -2; k <= g.nz + 3; k++) {
+                const bool has = p.y >= 0 && k >= p.x && k <= g.nz;
+                if (out) out[h + (k + 2)] = has ? buf[(size_t)p.y + (k - p.x)] : 0.0f;
+                else if (has) buf[(size_t)p.y + (k - p.x)] = in[h + (k + 2)];
+            }
+        }
+        if (in) {
+            CK(cudaMemcpyAsync(c->aux[q], buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+        }
+        return SWPC_OK;
+    }
     std::vector<float> buf((size_t)std::max<long long>(c->npml, 1));
     std::vector<int2> pc((size_t)g.Ip * g.Jp);
     CK(cudaMemcpyAsync(pc.data(), c->pmlcol, pc.size() * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));

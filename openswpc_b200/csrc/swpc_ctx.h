@@ -50,7 +50,9 @@ struct InjEntry {
     int pad;
 };
 
-struct swpc_ctx_impl;
+struct Model2D;
+struct Tile2D;
+struct Wav2Args;
 
 }  // namespace swpc
 
@@ -125,6 +127,14 @@ struct swpc_ctx {
     int *d_it = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_key = -1;
+
+    // 2D solvers: device model descriptor, tile list, recorder descriptor
+    swpc::Model2D *d_model2d = nullptr;
+    swpc::Tile2D *d_tiles2d = nullptr;
+    int ntiles2d = 0;
+    swpc::Wav2Args *d_wav2d = nullptr;
+    int nm2d_aux = 0;
+    bool desc_dirty = true;   // device descriptors must be refreshed before the next launch
 
     // launch shape (swpc_set_launch): block = 32 x bi x bj threads; minb =
     // minimum resident blocks per SM the kernels are compiled for

@@ -363,6 +363,93 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
     return SWPC_OK;
 }
 
+// visco_chi (m_fdtool.f90:730-753): cc = mean_m (1 - i w ts (1+tau)) / (1 - i w ts)
+// with each term in complex DP and the running sum in complex SP;
+// chi = 1 / Re(cc**(-0.5)) with the principal power taken in SP
+static float visco_chi(int nm, const float *ts, float tau, float f) {
+    const float omega = (float)(2 * kPi * (double)f);
+    float ccr = 0.0f, cci = 0.0f;
+    for (int m = 0; m < nm; m++) {
+        const double a = (double)omega * (double)ts[m];
+        const double ni = -(a * (1.0 + (double)tau)), di = -a;
+        const double den = 1.0 * 1.0 + di * di;
+        const double re = (1.0 * 1.0 + ni * di) / den;
+        const double im = (ni * 1.0 - 1.0 * di) / den;
+        ccr = (float)((double)ccr + re);
+        cci = (float)((double)cci + im);
+    }
+    ccr = ccr / nm;
+    cci = cci / nm;
+    const float r = hypotf(ccr, cci);
+    const float th = atan2f(cci, ccr);
+    return 1.0f / (cosf(-0.5f * th) / sqrtf(r));
+}
+
+int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                         float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs, int *kob,
+                         int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal) {
+    const int nx = g->nx, nz = g->nz, na = g->na, nm = g->nm;
+    const long nk = nz + 6, ni = nx + 6;
+    auto id = [&](int k, int i) { return (long)(i + 2) * nk + (k + 2); };
+    memcpy(taup, qp, sizeof(float) * nk * ni);
+    memcpy(taus, qs, sizeof(float) * nk * ni);
+    auto cp = [&](long d, long s) {
+        rho[d] = rho[s]; lam[d] = lam[s]; mu[d] = mu[s]; taup[d] = taup[s]; taus[d] = taus[s];
+    };
+    for (int i = -2; i <= na; i++)
+        for (int k = -2; k <= nz + 3; k++) cp(id(k, i), id(k, na + 1));
+    for (int i = nx - na + 1; i <= nx + 3; i++)
+        for (int k = -2; k <= nz + 3; k++) cp(id(k, i), id(k, nx - na));
+    for (int i = -2; i <= nx + 3; i++)
+        for (int k = nz - na + 1; k <= nz + 3; k++) cp(id(k, i), id(nz - na, i));
+    float zeta = 0.0f;
+    swpc_visco_setup(nm, fq_min, fq_max, ts, &zeta);
+    for (long e = 0; e < nk * ni; e++) {
+        taup[e] = nm * zeta / taup[e];
+        taus[e] = nm * zeta / taus[e];
+    }
+    if (nm > 0)
+#pragma omp parallel for schedule(static)
+        for (int i = -2; i <= nx + 3; i++)
+            for (int k = -2; k <= nz + 3; k++) {
+                const long e = id(k, i);
+                const float rb2 = mu[e], ra2 = lam[e] + 2 * mu[e];
+                const float cm = visco_chi(nm, ts, taus[e], fq_ref);
+                mu[e] = rb2 / (cm * cm);
+                const float cl = visco_chi(nm, ts, taup[e], fq_ref);
+                lam[e] = ra2 / (cl * cl) - 2 * mu[e];
+            }
+    for (int i = -2; i <= nx + 3; i++) { kfs[i + 2] = 0; kob[i + 2] = 0; kfs_top[i + 2] = kfs_bot[i + 2] = kob_top[i + 2] = kob_bot[i + 2] = 0; }
+    for (int i = 0; i <= nx + 2; i++)
+        for (int k = 1; k <= nz - 1; k++) {
+            if (fabsf(mu[id(k, i)]) < kEps && fabsf(mu[id(k + 1, i)]) > kEps) kob[i + 2] = k;
+            if (fabsf(lam[id(k, i)]) < kEps && fabsf(lam[id(k + 1, i)]) > kEps) kfs[i + 2] = k;
+        }
+    for (int i = 1; i <= nx; i++) {
+        int fmn = 1 << 30, fmx = -(1 << 30), omn = 1 << 30, omx = -(1 << 30);
+        for (int ii = i - 2; ii <= i + 3; ii++) {
+            fmn = std::min(fmn, kfs[ii + 2]); fmx = std::max(fmx, kfs[ii + 2]);
+            omn = std::min(omn, kob[ii + 2]); omx = std::max(omx, kob[ii + 2]);
+        }
+        kfs_top[i + 2] = std::max(fmn - 2, 1);
+        kfs_bot[i + 2] = std::min(fmx + 2, nz);
+        kob_top[i + 2] = std::max(omn - 2, 1);
+        kob_bot[i + 2] = std::min(omx + 2, nz);
+    }
+    float vmax1 = -1.0f, vmin1 = 1e30f;
+    for (int i = 1; i <= nx; i++)
+        for (int k = kfs[i + 2] + 1; k <= nz; k++) {
+            const long e = id(k, i);
+            const float vp = sqrtf((lam[e] + 2 * mu[e]) / rho[e]);
+            vmax1 = std::max(vmax1, vp);
+            const float vs = sqrtf(mu[e] / rho[e]);
+            if (vs < kEps) continue;
+            vmin1 = std::min(vmin1, vs);
+        }
+    scal[0] = zeta; scal[1] = vmin1; scal[2] = vmax1;
+    return SWPC_OK;
+}
+
 static void damping_profile(float x, float H, float beg, float end, int na, float fcut, float dt, float *gp) {
     // m_absorb_p.f90:507-547 (pd = pa = 1, pb = 2, cp = 6)
     const float R0 = powf(10.0f, -(log10f((float)na) - 1) / log10f(2.0f) - 3.0f);

@@ -86,6 +86,7 @@ void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block,
 void launch_stress3d_march(const Str3Args &a, int nm, int minb, int jc, cudaStream_t st);
 void launch_vel3d_march(const Vel3Args &a, int minb, int jc, cudaStream_t st);
 void launch_inject(const InjArgs &a, cudaStream_t st);
+void launch_inject_multi(const InjArgs *list, int nlist, int max_n, const int *d_it, int it, cudaStream_t st);
 void launch_wav3d(const Wav3Args &a, cudaStream_t st);
 void launch_vmax3d(const VmaxArgs &a, cudaStream_t st);
 void launch_advance_it(int *d_it, cudaStream_t st);

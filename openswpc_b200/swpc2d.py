@@ -1,0 +1,270 @@
+"""Host driver of the 2D solvers (src/swpc_psv/main.f90, src/swpc_sh/main.f90)
+and of the batched 2D ensemble.
+
+`Swpc2D` runs the reference's 2D setup sequence (global__setup2,
+medium__setup, kernel__setup, source__setup, absorb__setup, wav__setup) with
+the library's host routines and exposes the time-loop routines under their
+module names.  Arrays use the 2D memory box ``(kbeg_m:kend_m, ibeg_m:iend_m)``
+with k fastest: a numpy array of shape ``(nx+6, nz+6)`` indexed
+``[i+2, k+2]``.
+
+`Batch2D` joins many set-up 2D runs (same kind and nm) into one persistent
+launch per half step, replayed as a CUDA graph (swpc_batch_*).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, fptr, iptr
+from .params import Params
+
+f32 = np.float32
+KINDS = {"psv": _lib.KIND_PSV, "sh": _lib.KIND_SH}
+
+
+def grid2d(p: Params) -> _lib.Grid:
+    return _lib.Grid(p.nx, 1, p.nz, p.na, p.nm, p.dx, p.dx, p.dz, p.dt, p.xbeg, 0.0, p.zbeg, p.tbeg)
+
+
+class Medium2D:
+    """Host copy of the 2D medium after medium__setup."""
+
+    FIELDS = ("rho", "lam", "mu", "taup", "taus")
+    MAPS = ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot", "kbeg_a")
+
+    def __init__(self, p: Params):
+        lib = _lib.load()
+        g = grid2d(p)
+        shape = (p.nx + 6, p.nz + 6)
+        for name in self.FIELDS:
+            setattr(self, name, np.zeros(shape, np.float32))
+        self.qp = np.zeros(shape, np.float32)
+        self.qs = np.zeros(shape, np.float32)
+        for name in self.MAPS:
+            setattr(self, name, np.zeros(p.nx + 6, np.int32))
+        L = p.layers
+        arr = lambda a: np.array([getattr(l, a) for l in L], np.float32)
+        rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+                                 fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, None, p.rhomin,
+                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs))
+        if rc:
+            raise ValueError("vmodel_lhm failed")
+        self.ts = np.zeros(3, np.float32)
+        scal = np.zeros(3, np.float32)
+        rc = lib.swpc_setup_medium_2d(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
+                                      fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup),
+                                      fptr(self.taus), iptr(self.kfs), iptr(self.kob), iptr(self.kfs_top),
+                                      iptr(self.kfs_bot), iptr(self.kob_top), iptr(self.kob_bot), fptr(self.ts),
+                                      fptr(scal))
+        if rc:
+            raise ValueError("2D medium setup failed")
+        self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
+        lib.swpc_kbeg_a(C.byref(g), iptr(self.kbeg_a))
+
+    def view(self) -> _lib.MediumView:
+        v = _lib.MediumView()
+        for name in self.FIELDS:
+            setattr(v, name, fptr(getattr(self, name)))
+        for name in self.MAPS:
+            setattr(v, name, iptr(getattr(self, name)))
+        v.ld_k = self.rho.shape[1]
+        v.ld_i = self.rho.shape[0]
+        v.ld_i2 = self.kfs.shape[0]
+        return v
+
+
+class Swpc2D:
+    """One 2D run (kind 'psv' or 'sh') on one GPU."""
+
+    def __init__(self, p: Params, kind: str = "psv", device: int = 0):
+        p.check()
+        self.p, self.kind = p, kind
+        lib = self.lib = _lib.load()
+        m = self.medium = Medium2D(p)
+        desc = _lib.Desc(KINDS[kind], p.nx, 1, p.nz, p.na, p.nm, p.nt, p.dx, p.dx, p.dz, p.dt, p.tbeg, device)
+        ctx = C.c_void_p()
+        rc = lib.swpc_create(C.byref(desc), C.byref(ctx))
+        self.ctx = ctx
+        if rc:
+            msg = lib.swpc_last_error(ctx) if ctx else b""
+            lib.swpc_destroy(ctx)
+            self.ctx = None
+            raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_create failed")
+        check(ctx, lib.swpc_upload_medium(ctx, C.byref(m.view())))
+        check(ctx, lib.swpc_kernel_setup(ctx, fptr(m.ts)))
+        # source__setup of the 2D codes (src/swpc_psv/m_source.f90:150-268)
+        srcs = p.sources
+        fcut = f32(0.0)
+        for s in srcs:
+            fcut = max(fcut, f32(1) / f32(s.trise))
+        UC = f32(1e-15)
+        if p.bf_mode:
+            acc = f32(0.0)
+            if kind == "psv":
+                for s in srcs:
+                    acc = acc + (f32(s.fx) * f32(s.fx) + f32(s.fz) * f32(s.fz))
+                M0 = np.sqrt(acc, dtype=np.float32)
+            else:
+                for s in srcs:
+                    acc = acc + f32(s.fy)
+                M0 = np.sqrt(acc * acc, dtype=np.float32)
+            UC = UC * f32(1000)
+        else:
+            M0 = f32(0.0)
+            for s in srcs:
+                M0 = M0 + f32(s.mo)
+        rows = []
+        for s in srcs:
+            i = lib.swpc_x2i(s.x, p.xbeg, p.dx)
+            k = lib.swpc_x2i(s.z, p.zbeg, p.dz)
+            if -1 <= i <= p.nx + 3 and -1 <= k <= p.nz + 3:
+                rows.append((i, k, s))
+        n = len(rows)
+        isrc = np.array([r[0] for r in rows], np.int32)
+        ksrc = np.array([r[1] for r in rows], np.int32)
+        prm = np.array([[r[2].tbeg, r[2].trise] for r in rows], np.float32).reshape(n, 2)
+        stf = _lib.STF_CODES[p.stftype]
+        if p.bf_mode:
+            f3 = np.array([[f32(r[2].fx) / M0, f32(r[2].fy) / M0, f32(r[2].fz) / M0] for r in rows],
+                          np.float32).reshape(n, 3)
+            check(ctx, lib.swpc_bodyforce_setup(ctx, n, iptr(isrc), None, iptr(ksrc), fptr(prm), fptr(f3), stf))
+        else:
+            mo = np.array([f32(r[2].mo) / M0 for r in rows], np.float32)
+            m6 = np.array([[r[2].mxx, r[2].myy, r[2].mzz, r[2].myz, r[2].mxz, r[2].mxy] for r in rows],
+                          np.float32).reshape(n, 6)
+            check(ctx, lib.swpc_source_setup(ctx, n, iptr(isrc), None, iptr(ksrc), fptr(prm), fptr(mo), fptr(m6),
+                                             stf))
+        self.M0, self.UC, self.fcut = float(M0), float(UC), float(fcut)
+        g = grid2d(p)
+        self.gprof = {k: np.zeros((p.nx if k[1] == "x" else p.nz, 4), np.float32) for k in ("gxc", "gxe", "gzc", "gze")}
+        gp = self.gprof
+        lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]), None, None,
+                                  fptr(gp["gzc"]), fptr(gp["gze"]))
+        check(ctx, lib.swpc_absorb_setup(ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), None, None, fptr(gp["gzc"]),
+                                         fptr(gp["gze"])))
+        # wav__setup / set_stinfo (src/swpc_psv/m_wav.f90:480-540)
+        self.nst = 0
+        what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u)
+        if p.stations and what:
+            x1, xn = lib.swpc_i2x(1, p.xbeg, p.dx), lib.swpc_i2x(p.nx, p.xbeg, p.dx)
+            cells = []
+            zsw = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
+            for st in p.stations:
+                xs, zs = float(f32(st.x)), float(f32(st.z))
+                i = lib.swpc_x2i(xs, p.xbeg, p.dx)
+                k = lib.swpc_x2i(zs, p.zbeg, p.dz)
+                if not (x1 < xs < xn and 1 < k < p.nz and 1 <= i <= p.nx):
+                    continue
+                z = zsw.get(st.zsw, 0)
+                if z == 1:
+                    k = int(m.kfs[i + 2]) + 1
+                elif z == 2:
+                    k = int(m.kob[i + 2]) + 1
+                elif z == 3:
+                    k = int(m.kob[i + 2]) - 1
+                k = p.nz - 1 if k > p.nz else (2 if k < 1 else k)
+                cells.append((i, k))
+            a = np.array(cells, np.int32).reshape(-1, 2)
+            self.ist, self.kst = a[:, 0].copy(), a[:, 1].copy()
+            self.nst = len(cells)
+            check(ctx, lib.swpc_wav_setup(ctx, self.nst, iptr(self.ist), None, iptr(self.kst), p.ntdec_w, what,
+                                          self.M0, self.UC))
+        self.what = what
+
+    def close(self):
+        if self.ctx:
+            self.lib.swpc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, it: int):
+        check(self.ctx, self.lib.swpc_step(self.ctx, it))
+
+    def run(self, it0: int = 1, nsteps: int | None = None):
+        if nsteps is None:
+            nsteps = self.p.nt - it0 + 1
+        check(self.ctx, self.lib.swpc_run(self.ctx, it0, nsteps))
+        check(self.ctx, self.lib.swpc_sync(self.ctx))
+
+    def kernel__vmax(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(self.ctx, self.lib.swpc_vmax(self.ctx, fptr(out)))
+        return out[:2] if self.kind == "psv" else out[:1]
+
+    def download(self, field: int) -> np.ndarray:
+        p = self.p
+        out = np.zeros((p.nx + 6, p.nz + 6), np.float32)
+        check(self.ctx, self.lib.swpc_download_field(self.ctx, field, fptr(out), p.nz + 6, p.nx + 6))
+        return out
+
+    def upload(self, field: int, arr: np.ndarray):
+        p = self.p
+        a = np.ascontiguousarray(arr, np.float32)
+        check(self.ctx, self.lib.swpc_upload_field(self.ctx, field, fptr(a), p.nz + 6, p.nx + 6))
+
+    def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
+        ntw, nst = C.c_int(), C.c_int()
+        check(self.ctx, self.lib.swpc_wav_dims(self.ctx, C.byref(ntw), C.byref(nst)))
+        nc = 2 if self.kind == "psv" else 1
+        out = np.zeros((nst.value, nc, ntw.value), np.float32)
+        if nst.value:
+            check(self.ctx, self.lib.swpc_wav_fetch(self.ctx, what, fptr(out)))
+        return out
+
+    # field ids of this kind
+    @property
+    def field_ids(self) -> dict:
+        if self.kind == "psv":
+            return {"Vx": _lib.F_VX, "Vz": _lib.F_VZ, "Sxx": _lib.F_SXX, "Szz": _lib.F_SZZ, "Sxz": _lib.F_SXZ}
+        return {"Vy": _lib.F_VY, "Syz": _lib.F_SYZ, "Sxy": _lib.F_SXY}
+
+
+class Batch2D:
+    """Many 2D runs advanced by one persistent launch per half step."""
+
+    def __init__(self, runs: list[Swpc2D]):
+        self.runs = runs
+        self.lib = _lib.load()
+        arr = (C.c_void_p * len(runs))(*[r.ctx.value for r in runs])
+        b = C.c_void_p()
+        rc = self.lib.swpc_batch_create(arr, len(runs), C.byref(b))
+        self.b = b
+        if rc:
+            msg = self.lib.swpc_batch_last_error(b) if b else b""
+            raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_batch_create failed")
+
+    def _check(self, rc):
+        if rc:
+            raise _lib.SwpcError(rc, self.lib.swpc_batch_last_error(self.b).decode())
+
+    def run(self, it0: int, nsteps: int):
+        self._check(self.lib.swpc_batch_run(self.b, it0, nsteps))
+        self._check(self.lib.swpc_batch_sync(self.b))
+
+    def step(self, it: int):
+        self._check(self.lib.swpc_batch_step(self.b, it))
+        self._check(self.lib.swpc_batch_sync(self.b))
+
+    def time_steps(self, it0: int, nsteps: int) -> float:
+        ms = C.c_float()
+        self._check(self.lib.swpc_batch_time_steps(self.b, it0, nsteps, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if self.b:
+            self.lib.swpc_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

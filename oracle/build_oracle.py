@@ -21,7 +21,7 @@ VARIANTS = {
     "mixed": ("double", "float"),
     "f64": ("double", "double"),
 }
-SOURCES = {"3d": "swpc3d_oracle.c", "psv": "swpcpsv_oracle.c", "sh": "swpcsh_oracle.c"}
+SOURCES = {"3d": "swpc3d_oracle.c", "2d": "swpc2d_oracle.c"}
 
 
 def build(verbose: bool = False) -> list[Path]:

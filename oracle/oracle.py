@@ -45,8 +45,6 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         return _cache[key]
     path = LIB / f"liboracle{kind}_{variant}.so"
     if not path.exists():
-        from . import build_oracle  # noqa: F401  (package-relative when imported as oracle.oracle)
-    if not path.exists():
         import importlib.util
         spec = importlib.util.spec_from_file_location("build_oracle", HERE / "build_oracle.py")
         mod = importlib.util.module_from_spec(spec)
@@ -285,3 +283,163 @@ class Oracle3D:
                 reports.append((it, self.vmax() * np.float32(sc["UC"]) * np.float32(sc["M0"])))
             self.lib.o3d_step(self.o, it)
         return reports
+
+
+def load2d(variant: str = "f32") -> C.CDLL:
+    key = f"2d_{variant}"
+    if key in _cache:
+        return _cache[key]
+    path = LIB / f"liboracle2d_{variant}.so"
+    if not path.exists():
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("build_oracle", HERE / "build_oracle.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    lib = C.CDLL(str(path))
+    vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+    sig = {
+        "o2d_create": (vp, [i, i, i, i, i, i, d, d, f, f, f, f, i]),
+        "o2d_destroy": (None, [vp]),
+        "o2d_vmodel_lhm": (None, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, _FP, f, _FP, _FP]),
+        "o2d_medium_setup": (None, [vp, _FP, _FP, f, f, f]),
+        "o2d_kernel_setup": (None, [vp]),
+        "o2d_absorb_setup": (None, [vp, f]),
+        "o2d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, i]),
+        "o2d_wav_setup": (i, [vp, i, _FP, _FP, _IP, i, i, i]),
+        "o2d_step": (None, [vp, i]),
+        "o2d_vmax": (None, [vp, _FP]),
+        "o2d_dims": (None, [vp, C.POINTER(C.c_long)]),
+        "o2d_scalars": (None, [vp, _FP]),
+        "o2d_ptr": (vp, [vp, i]),
+        "o2d_mpr_size": (i, []),
+        "o2d_spr_size": (i, []),
+        "o2d_visco_chi": (f, [i, _FP, f, f]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _cache[key] = lib
+    return lib
+
+
+class Oracle2D:
+    """The reference P-SV (kind 'psv') or SH ('sh') run restated on the CPU."""
+
+    KIND = {"psv": 2, "sh": 1}
+
+    def __init__(self, p, kind: str = "psv", variant: str = "f32", threads: int = 1):
+        self.p, self.kind = p, kind
+        self.lib = lib = load2d(variant)
+        self.mpr = np.float32 if lib.o2d_mpr_size() == 4 else np.float64
+        self.spr = np.float32 if lib.o2d_spr_size() == 4 else np.float64
+        self.o = lib.o2d_create(self.KIND[kind], p.nx, p.nz, p.na, p.nm, p.nt, float(np.float32(p.dx)),
+                                float(np.float32(p.dz)), p.dt, p.xbeg, p.zbeg, p.tbeg, threads)
+        shape = (p.nx + 6, p.nz + 6)
+        L = p.layers
+        arr = lambda a: np.array([getattr(l, a) for l in L], np.float32)
+        qp = np.zeros(shape, np.float32)
+        qs = np.zeros(shape, np.float32)
+        lib.o2d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
+                           _f(arr("qp")), _f(arr("qs")), p.vcut, None, p.rhomin, _f(qp), _f(qs))
+        lib.o2d_medium_setup(self.o, _f(qp), _f(qs), p.fq_min, p.fq_max, p.fq_ref)
+        lib.o2d_kernel_setup(self.o)
+        S = p.sources
+        n = len(S)
+        sx = np.array([s.x for s in S], np.float32)
+        sz = np.array([s.z for s in S], np.float32)
+        prm = np.array([[s.tbeg, s.trise] for s in S], np.float32).reshape(n, 2)
+        mo = np.array([s.mo for s in S], np.float32)
+        m6 = np.array([[s.mxx, s.myy, s.mzz, s.myz, s.mxz, s.mxy] for s in S], np.float32).reshape(n, 6)
+        f3 = np.array([[s.fx, s.fy, s.fz] for s in S], np.float32).reshape(n, 3)
+        self._hold = [sx, sz, prm, mo, m6, f3]
+        self.nsrc = lib.o2d_source_setup(self.o, int(p.bf_mode), n, _f(sx), _f(sz), _f(prm), _f(mo), _f(m6), _f(f3),
+                                         STF[p.stftype])
+        lib.o2d_absorb_setup(self.o, self.scalars()["fcut"])
+        self.nst = 0
+        if p.stations and (p.sw_wav_v or p.sw_wav_u):
+            St = p.stations
+            xs = np.array([s.x for s in St], np.float32)
+            zs = np.array([s.z for s in St], np.float32)
+            zsw = np.array([ZSW.get(s.zsw, 0) for s in St], np.int32)
+            self.nst = lib.o2d_wav_setup(self.o, len(St), _f(xs), _f(zs), zsw.ctypes.data_as(_IP), p.ntdec_w,
+                                         int(p.sw_wav_v), int(p.sw_wav_u))
+
+    def close(self):
+        if self.o:
+            self.lib.o2d_destroy(self.o)
+            self.o = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def dims(self) -> dict:
+        a = (C.c_long * 10)()
+        self.lib.o2d_dims(self.o, a)
+        return dict(zip(["nk", "ni", "nka", "kbeg_min", "nst", "ntw", "nsrc", "ibeg_k", "iend_k", "kend_k"], list(a)))
+
+    def scalars(self) -> dict:
+        a = (C.c_float * 9)()
+        self.lib.o2d_scalars(self.o, a)
+        return dict(zip(["M0", "UC", "fcut", "vmin", "vmax", "zeta", "ts1", "ts2", "ts3"], list(a)))
+
+    # names -> (id, kind of storage)
+    def _spec(self, name: str):
+        psv = self.kind == "psv"
+        ids = ({"Vx": 0, "Vz": 1, "Sxx": 2, "Szz": 3, "Sxz": 4, "Rxx": 10, "Rzz": 11, "Rxz": 12} if psv else
+               {"Vy": 0, "Syz": 2, "Sxy": 3, "Ryz": 10, "Rxy": 11})
+        ids.update({"rho": 20, "lam": 21, "mu": 22, "taup": 23, "taus": 24, "frho": 30, "flam": 31, "fmu": 32,
+                    "ftaup": 33, "ftaus": 34, "kfs": 50, "kob": 51, "kfs_top": 52, "kfs_bot": 53, "kob_top": 54,
+                    "kob_bot": 55, "kbeg_a": 56})
+        aux = (["axVx", "azVx", "axVz", "azVz", "axSxx", "azSxz", "axSxz", "azSzz"] if psv else
+               ["axVy", "azVy", "axSxy", "azSyz"])
+        for n, a in enumerate(aux):
+            ids[a] = 60 + n
+        return ids[name]
+
+    def array(self, name: str) -> np.ndarray:
+        d = self.dims()
+        p = self.p
+        fid = self._spec(name)
+        ptr = self.lib.o2d_ptr(self.o, fid)
+        if fid < 10:
+            dt, shape = self.mpr, (d["ni"], d["nk"])
+        elif fid < 20:
+            dt, shape = self.spr, (d["ni"], d["nk"], max(p.nm, 1))
+        elif fid < 30:
+            dt, shape = self.spr, (d["ni"], d["nk"])
+        elif fid < 50:
+            dt, shape = np.float32, (d["ni"], d["nk"])
+        elif fid < 60:
+            dt, shape = np.int32, (d["ni"],)
+        else:
+            dt, shape = self.spr, (p.nx, d["nka"])
+        n = int(np.prod(shape))
+        buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+    def waveforms(self, comp: str = "v") -> np.ndarray:
+        d = self.dims()
+        nc = 2 if self.kind == "psv" else 1
+        ptr = self.lib.o2d_ptr(self.o, 90 if comp == "v" else 91)
+        n = d["ntw"] * nc * d["nst"]
+        if n == 0:
+            return np.zeros((d["nst"], nc, d["ntw"]), np.float32)
+        buf = (C.c_float * n).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float32).reshape(d["nst"], nc, d["ntw"]).copy()
+
+    def step(self, it: int):
+        self.lib.o2d_step(self.o, it)
+
+    def run(self, it0: int, nsteps: int):
+        for it in range(it0, it0 + nsteps):
+            self.lib.o2d_step(self.o, it)
+
+    def vmax(self) -> np.ndarray:
+        out = np.zeros(2, np.float32)
+        self.lib.o2d_vmax(self.o, _f(out))
+        return out

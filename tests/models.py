@@ -40,3 +40,20 @@ def vonkarman_xi(shape, eps=0.05, seed=7):
         x = (x + np.roll(x, 1, ax) + np.roll(x, -1, ax)) / 3
     x *= eps / max(float(x.std()), 1e-12)
     return x.astype(np.float32)
+
+
+def small2d(kind="psv", nx=120, nz=60, na=10, nt=80, dx=0.25, dt=0.02, nm=3, seed=5, **kw) -> Params:
+    """A small layered 2D run (P-SV: explosion + double couple; SH: mxy/myz)."""
+    rng = np.random.default_rng(seed)
+    xb = -nx // 2 * dx
+    st = [Station(float(rng.uniform(xb + (na + 2) * dx, xb + (nx - na - 2) * dx)), 0.0,
+                  0.0 if n < 3 else 2.0, f"s{n}", ["fsb", "obb", "oba", "dep", "dep"][n]) for n in range(5)]
+    if kind == "psv":
+        src = [Source(0.3, 0.0, 4.0, 0.0, 0.8, mo=1e15, mxx=1.0, mzz=0.7, mxz=0.4)]
+    else:
+        src = [Source(0.3, 0.0, 4.0, 0.0, 0.8, mo=1e15, mxy=1.0, myz=0.6)]
+    args = dict(nx=nx, ny=1, nz=nz, nt=nt, dx=dx, dy=dx, dz=dx, dt=dt, na=na, nm=nm, xbeg=xb, ybeg=0.0,
+                zbeg=-3 * dx, fq_min=0.05, fq_max=2.0, layers=list(LAYERS), sources=src, stations=st, ntdec_w=1,
+                ntdec_r=10, sw_wav_u=True)
+    args.update(kw)
+    return Params(**args)

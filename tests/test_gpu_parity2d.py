@@ -1,0 +1,115 @@
+"""GPU parity of the 2D P-SV and SH steps against the CPU oracle, and of the
+batched 2D ensemble against independent runs (bitwise)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from openswpc_b200 import _lib
+from openswpc_b200.params import Source
+from openswpc_b200.swpc2d import Batch2D, Swpc2D
+from oracle.oracle import Oracle2D
+from tests.models import small2d
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_TOL = 1e-5
+
+
+def same_bits(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def aux_box(o, name, p):
+    d = o.dims()
+    a = o.array(name)
+    box = np.zeros((p.nx + 6, p.nz + 6), np.float32)
+    box[3:p.nx + 3, d["kbeg_min"] + 2:p.nz + 3] = a
+    kb = o.array("kbeg_a")
+    kk = np.arange(p.nz + 6)[None, :] - 2
+    mask = np.zeros_like(box, bool)
+    mask[3:p.nx + 3, :] = True
+    mask &= (kk >= kb[:, None]) & (kk <= p.nz)
+    return np.where(mask, box, 0).astype(np.float32)
+
+
+def compare(g: Swpc2D, o: Oracle2D, p):
+    for name, fid in g.field_ids.items():
+        a, b = g.download(fid), o.array(name)
+        assert rel_l2(a, b) <= REL_L2_TOL, (name, rel_l2(a, b))
+        assert same_bits(a, b), (name, np.abs(a - b).max())
+    rn = ["Rxx", "Rzz", "Rxz"] if g.kind == "psv" else ["Ryz", "Rxy"]
+    rc = [0, 2, 4] if g.kind == "psv" else [3, 5]
+    for name, c in zip(rn, rc):
+        ref = o.array(name)
+        for m in range(p.nm):
+            a = g.download(_lib.F_R + 3 * c + m)
+            b = np.zeros_like(a)
+            d = o.dims()
+            b[d["ibeg_k"] + 2:d["iend_k"] + 3, 3:d["kend_k"] + 3] = ref[d["ibeg_k"] + 2:d["iend_k"] + 3, 3:d["kend_k"] + 3, m]
+            assert same_bits(a, b), (name, m)
+    auxn = (["axVx", "azVx", "axVz", "azVz", "axSxx", "azSxz", "axSxz", "azSzz"] if g.kind == "psv" else
+            ["axVy", "azVy", "axSxy", "azSyz"])
+    for q, name in enumerate(auxn):
+        assert same_bits(g.download(_lib.F_AUX + q), aux_box(o, name, p)), name
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_2d_forward_matches_oracle(kind):
+    p = small2d(kind, nt=120)
+    g = Swpc2D(p, kind)
+    o = Oracle2D(p, kind)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    for what, comp in ((_lib.WAV_V, "v"), (_lib.WAV_U, "u")):
+        a, b = g.waveforms(what), o.waveforms(comp)
+        assert np.linalg.norm(b) > 0, comp
+        assert rel_l2(a, b) <= REL_L2_TOL
+        assert same_bits(a, b), comp
+    compare(g, o, p)
+    vm = g.kernel__vmax()
+    assert same_bits(vm, o.vmax()[:len(vm)])
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_2d_body_force_and_absorber_sources(kind):
+    """Body forces, one inside the absorber (P-SV injects it between the
+    interior and absorber velocity updates, like the reference)."""
+    srcs = [Source(0.4, 0.0, 3.0, 0.0, 0.7, fx=1.0, fy=0.8, fz=-0.5),
+            Source(-13.9, 0.0, 1.0, 0.1, 0.6, fx=0.3, fy=1.0, fz=1.0)]
+    p = small2d(kind, nt=80, bf_mode=True, sources=srcs)
+    g = Swpc2D(p, kind)
+    o = Oracle2D(p, kind)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    assert np.linalg.norm(o.waveforms()) > 0
+    assert same_bits(g.waveforms(), o.waveforms())
+    compare(g, o, p)
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_batched_ensemble_equals_independent_runs(kind):
+    """Uneven 2D models advanced by one launch per half step give the same
+    bits as running each model alone, and as the oracle."""
+    sizes = [(96, 48), (160, 40), (72, 90), (128, 64)]
+    ps = [small2d(kind, nx=nx, nz=nz, na=8, nt=50, seed=s) for s, (nx, nz) in enumerate(sizes)]
+    runs = [Swpc2D(p, kind) for p in ps]
+    alone = [Swpc2D(p, kind) for p in ps]
+    batch = Batch2D(runs)
+    batch.run(1, 50)
+    for r, a, p in zip(runs, alone, ps):
+        a.run(1, 50)
+        assert same_bits(r.waveforms(), a.waveforms())
+        for fid in r.field_ids.values():
+            assert same_bits(r.download(fid), a.download(fid))
+    o = Oracle2D(ps[2], kind)
+    o.run(1, 50)
+    assert same_bits(runs[2].waveforms(), o.waveforms())
+    batch.close()

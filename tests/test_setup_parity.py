@@ -171,3 +171,35 @@ def test_oracle_fp32_close_to_fp64():
     assert np.linalg.norm(wa - wb) / np.linalg.norm(wb) < 1e-4
     va, vb = a.array("Vz").astype(np.float64), b.array("Vz")
     assert np.linalg.norm(va - vb) / np.linalg.norm(vb) < 1e-4
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_medium_setup_2d_bit_exact(kind):
+    from openswpc_b200.swpc2d import Medium2D
+    from oracle.oracle import Oracle2D
+    from tests.models import small2d
+
+    p = small2d(kind)
+    m = Medium2D(p)
+    o = Oracle2D(p, kind)
+    for f in ("rho", "lam", "mu", "taup", "taus"):
+        assert np.array_equal(bits(getattr(m, f)), bits(o.array("f" + f))), f
+    for f in ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot", "kbeg_a"):
+        assert np.array_equal(getattr(m, f), o.array(f)), f
+    # the band follows the 3D formulation: [min(kfs)-2, max(kfs)+2]
+    assert (m.kfs_top[5:-5] == 1).all() and (m.kfs_bot[5:-5] == 5).all()
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_oracle_2d_fp32_close_to_fp64(kind):
+    from oracle.oracle import Oracle2D
+    from tests.models import small2d
+
+    p = small2d(kind, nt=60)
+    a = Oracle2D(p, kind, "f32")
+    b = Oracle2D(p, kind, "f64")
+    a.run(1, 60)
+    b.run(1, 60)
+    wa, wb = a.waveforms("v").astype(np.float64), b.waveforms("v").astype(np.float64)
+    assert np.linalg.norm(wb) > 0
+    assert np.linalg.norm(wa - wb) / np.linalg.norm(wb) < 1e-4
