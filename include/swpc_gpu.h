@@ -41,6 +41,7 @@ extern "C" {
 #define SWPC_ERR_STATE 3      /* call out of order (e.g. step before setup)  */
 #define SWPC_ERR_DIVERGED 4   /* max |V| * UC > 1e5 (m_report.f90:142-152)   */
 #define SWPC_ERR_NOMEM 5      /* device allocation failed                    */
+#define SWPC_ERR_LIMIT 6      /* size above a fixed limit of swpc_vmax_noalloc */
 
 /* solver kinds */
 #define SWPC_KIND_3D 3
@@ -190,6 +191,29 @@ int swpc_wav_store(swpc_ctx *ctx, int it);          /* m_wav.f90:400-628     */
  * bottom; blocks.  Sets SWPC_ERR_DIVERGED when max*UC > 1e5
  * (m_report.f90:142-152). */
 int swpc_vmax(swpc_ctx *ctx, float out[3]);
+
+/* The same maximum for callers that may not allocate device memory: a solver
+ * that keeps Vx, Vy, Vz and kob in device arrays of its own (an OpenACC build
+ * of the reference holds them resident for the whole run) and has its device
+ * memory claimed up front, so it has no context and cannot have the library
+ * call cudaMalloc or cudaFree (which waits for the whole device) at every
+ * report.  No counterpart in the reference: it has one kernel__vmax over
+ * module arrays.  vx, vy, vz are device arrays over the memory box, k
+ * fastest, with leading extents ld_k (>= nz+6) and ld_i (>= nx+6); kob is a
+ * device map over (ibeg_m:iend_m, jbeg_m:jend_m) with leading extent ld_i.
+ * The range and the result are those of swpc_vmax, and
+ * SWPC_ERR_DIVERGED is returned when max*uc > 1e5 or a maximum is NaN.  Work
+ * runs on `stream` (a cudaStream_t; NULL = the default stream) of the calling
+ * thread's current device, and the call blocks until out[3] (host) is set.
+ * Allocates nothing: its scratch is a fixed device array of the library,
+ * 3 words per row j, held by every GPU that loads the library until exit, so
+ * ny above SWPC_NOALLOC_MAX_NY returns SWPC_ERR_LIMIT.  The first call on a
+ * device looks the array's address up; make that first call before any
+ * stream capture.  All calls on a device share the array: calls that overlap
+ * on the GPU (other streams or threads) race and must be serialised. */
+#define SWPC_NOALLOC_MAX_NY 16384
+int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const int *kob, int nx, int ny, int nz,
+                      int na, int ld_k, int ld_i, float uc, void *stream, float out[3]);
 
 /* One full step in main.f90 order: wav__store, update_stress (fused),
  * stressglut, comm, update_vel (fused), bodyforce, green, comm. */

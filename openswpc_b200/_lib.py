@@ -19,6 +19,8 @@ SWPC_ERR_CUDA = 2
 SWPC_ERR_STATE = 3
 SWPC_ERR_DIVERGED = 4
 SWPC_ERR_NOMEM = 5
+SWPC_ERR_LIMIT = 6
+SWPC_NOALLOC_MAX_NY = 16384
 
 KIND_3D, KIND_PSV, KIND_SH = 3, 2, 1
 STF_CODES = {"kupper": 0, "boxcar": 1, "triangle": 2, "herrmann": 3, "cosine": 4, "scosine": 4, "texp": 5}
@@ -35,7 +37,7 @@ EXPORTS = [
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
     "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
-    "swpc_vmax", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
+    "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_download_field", "swpc_upload_field", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
@@ -116,6 +118,7 @@ def load():
         "swpc_green_setup": (i, [vp, i, i, i, C.c_char, f, f, i]),
         "swpc_wav_setup": (i, [vp, i, _IP, _IP, _IP, i, i, f, f]),
         "swpc_vmax": (i, [vp, _FP]),
+        "swpc_vmax_noalloc": (i, [vp, vp, vp, vp, i, i, i, i, i, i, f, vp, _FP]),
         "swpc_step": (i, [vp, i]),
         "swpc_run": (i, [vp, i, i]),
         "swpc_time_steps": (i, [vp, i, i, _FP]),
