@@ -46,6 +46,10 @@ UNIT = "Gcell-updates/s"
 B_STRESS_INT, B_STRESS_PML = 58 * 4, 38 * 4
 B_VEL_INT, B_VEL_PML = 15 * 4, 33 * 4
 FALLBACK_HBM_GBS = 6650.0
+# DRAM traffic of one launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the c1 mix scaled
+# down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
+# algorithmic bytes; profiles/stress3d_kernel_256x256x128_na8.md and profiles/vel3d_kernel_256x256x128_na8.md
+TRAFFIC_PER_ALGORITHMIC = {"stress": 1.988e9 / 1.828028416e9, "vel": 0.652e9 / 0.609632256e9}
 
 
 def make_params(name: str):
@@ -197,6 +201,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4"])
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
+    ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
     args = ap.parse_args()
@@ -218,6 +223,8 @@ def main():
             s.z = min(s.z, (nz - p.na - 4) * p.dz + p.zbeg)
         p.stations = [st for st in p.stations if p.xbeg + (p.na + 2) * p.dx < st.x < p.xbeg + (nx - p.na - 2) * p.dx
                       and p.ybeg + (p.na + 2) * p.dy < st.y < p.ybeg + (ny - p.na - 2) * p.dy]
+    if args.na is not None:
+        p.na = args.na
     n_int, n_pml = cell_counts(p)
     cells = p.nx * p.ny * p.nz
     wl = {"workload": f"3D viscoelastic forward {p.nx}x{p.ny}x{p.nz} (nm=3, PML {p.na}, von Karman medium, "
@@ -362,9 +369,12 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "stress3d_kernel (fused interior + PML stress update)",
                          "achieved": ach_stress, "peak": peak, "unit": "GB/s", "frac": ach_stress / peak,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                         else "fallback 6650 GB/s", "traffic": None,
+                         else "fallback 6650 GB/s",
+                         "traffic": b_stress * TRAFFIC_PER_ALGORITHMIC["stress"],
+                         "traffic_source": "ncu DRAM bytes of the 1/64-scale case times 64 (same interior/PML mix)",
                          "algorithmic_bytes_per_launch": b_stress, "launch_ms": t_stress},
             "roofline_vel": {"kernel": "vel3d_kernel", "achieved": ach_vel, "frac": ach_vel / peak,
+                             "traffic": b_vel * TRAFFIC_PER_ALGORITHMIC["vel"],
                              "algorithmic_bytes_per_launch": b_vel, "launch_ms": t_vel},
             "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
                               "algorithmic_bytes_per_step": b_stress + b_vel},
