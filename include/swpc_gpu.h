@@ -215,8 +215,52 @@ int swpc_vmax(swpc_ctx *ctx, float out[3]);
 int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const int *kob, int nx, int ny, int nz,
                       int na, int ld_k, int ld_i, float uc, void *stream, float out[3]);
 
-/* One full step in main.f90 order: wav__store, update_stress (fused),
- * stressglut, comm, update_vel (fused), bodyforce, green, comm. */
+/* ---- snapshots (3D) ------------------------------------------------------ */
+
+/* Snapshot planes of snap__setup (src/swpc_3d/m_snap.f90:95-322): a plane is
+ * a section (yz at i0_yz, xz at j0_xz, xy at k0_xy, fs one cell below the
+ * free surface, ob one cell below the ocean bottom) times a quantity (ps:
+ * div, rot_x, rot_y, rot_z masked by lam/mu; v: Vx, Vy, Vz; u: displacement),
+ * bit SWPC_SNP_BIT(section, quantity) of `planes`.  Samples are decimated by
+ * idec/jdec/kdec (nxs = (nx + idec/2)/idec, ...); frames are taken at
+ * it = 1, 1 + ntdec_s, ... <= nt.  i0_yz, j0_xz, k0_xy are grid indices
+ * (x2i / y2j / z2k of x0_yz, y0_xz, z0_xy, m_snap.f90:157-159).  M0 and UC
+ * scale to physical units as wav__store does.  The frames stay in HBM for the
+ * run; the file writers (native .snp / NetCDF) stay with the caller. */
+#define SWPC_SNP_YZ 0
+#define SWPC_SNP_XZ 1
+#define SWPC_SNP_XY 2
+#define SWPC_SNP_FS 3
+#define SWPC_SNP_OB 4
+#define SWPC_SNP_PS 0
+#define SWPC_SNP_V 1
+#define SWPC_SNP_U 2
+#define SWPC_SNP_BIT(section, quantity) (1 << (3 * (section) + (quantity)))
+typedef struct swpc_snap_desc {
+    int planes;                 /* OR of SWPC_SNP_BIT(...)                     */
+    int idec, jdec, kdec;       /* spatial decimation                          */
+    int ntdec_s;                /* time decimation                             */
+    int i0_yz, j0_xz, k0_xy;    /* section positions (grid indices)            */
+    float M0, UC;               /* output scaling (m_snap.f90:1022-1025)       */
+} swpc_snap_desc;
+int swpc_snap_setup(swpc_ctx *ctx, const swpc_snap_desc *d);
+/* snap__write (m_snap.f90:911-939) for step it (1..nt; nt+1 updates the
+ * displacement sums and maxima once more, as snap__closefiles does before the
+ * NetCDF maxima are written).  swpc_step / swpc_run call it after wav__store
+ * once snapshots are set up. */
+int swpc_snap_write(swpc_ctx *ctx, int it);
+/* plane = 3*section + quantity: buffer (n1, n2, nvar) per frame in Fortran
+ * order, n1 fastest (yz: nys x nzs, xz: nxs x nzs, xy/fs/ob: nxs x nys). */
+int swpc_snap_dims(const swpc_ctx *ctx, int plane, int *nvar, int *n1, int *n2, int *nframes);
+/* All frames of a plane: out(n1, n2, nvar, nframes), Fortran order; blocks. */
+int swpc_snap_fetch(swpc_ctx *ctx, int plane, float *out);
+/* Running maxima max_fs_v, max_fs_u, max_ob_v, max_ob_u (which = 0..3) as
+ * (nxs, nys, 3): vertical, horizontal, vector (m_snap.f90:1691-1703,
+ * output__put_maxval :2291-2344); needs the matching fs/ob v or u plane. */
+int swpc_snap_fetch_max(swpc_ctx *ctx, int which, float *out);
+
+/* One full step in main.f90 order: wav__store, snap__write, update_stress
+ * (fused), stressglut, comm, update_vel (fused), bodyforce, green, comm. */
 int swpc_step(swpc_ctx *ctx, int it);
 /* Steps it0 .. it0+nsteps-1 as replays of a captured CUDA graph. */
 int swpc_run(swpc_ctx *ctx, int it0, int nsteps);

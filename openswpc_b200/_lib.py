@@ -38,6 +38,7 @@ EXPORTS = [
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
     "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
+    "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
     "swpc_download_field", "swpc_upload_field", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
@@ -68,6 +69,12 @@ class MediumView(C.Structure):
                 ("by", _FP), ("bz", _FP), ("muyz", _FP), ("muxz", _FP), ("muxy", _FP), ("ld_k", C.c_int),
                 ("ld_i", C.c_int), ("kfs", _IP), ("kob", _IP), ("kfs_top", _IP), ("kfs_bot", _IP),
                 ("kob_top", _IP), ("kob_bot", _IP), ("kbeg_a", _IP), ("ld_i2", C.c_int)]
+
+
+class SnapDesc(C.Structure):
+    _fields_ = [("planes", C.c_int), ("idec", C.c_int), ("jdec", C.c_int), ("kdec", C.c_int),
+                ("ntdec_s", C.c_int), ("i0_yz", C.c_int), ("j0_xz", C.c_int), ("k0_xy", C.c_int),
+                ("M0", C.c_float), ("UC", C.c_float)]
 
 
 class Grid(C.Structure):
@@ -124,6 +131,11 @@ def load():
         "swpc_time_steps": (i, [vp, i, i, _FP]),
         "swpc_wav_fetch": (i, [vp, i, _FP]),
         "swpc_wav_dims": (i, [vp, _IP, _IP]),
+        "swpc_snap_setup": (i, [vp, C.POINTER(SnapDesc)]),
+        "swpc_snap_write": (i, [vp, i]),
+        "swpc_snap_dims": (i, [vp, i, _IP, _IP, _IP, _IP]),
+        "swpc_snap_fetch": (i, [vp, i, _FP]),
+        "swpc_snap_fetch_max": (i, [vp, i, _FP]),
         "swpc_download_field": (i, [vp, i, _FP, i, i]),
         "swpc_upload_field": (i, [vp, i, _FP, i, i]),
         "swpc_device_bytes": (C.c_longlong, [vp]),

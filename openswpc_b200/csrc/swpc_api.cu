@@ -66,6 +66,12 @@ static void invalidate_graph(swpc_ctx *c) {
         c->graph_exec = nullptr;
     }
 }
+namespace swpc {
+int graph_invalidate(swpc_ctx *c) {
+    invalidate_graph(c);
+    return SWPC_OK;
+}
+}  // namespace swpc
 
 // ---------------------------------------------------------------------------
 // lifetime
@@ -142,6 +148,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     invalidate_graph(c);
+    snap_free(c);
     if (!is3d(c)) destroy_2d(c);
     void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
                   c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
@@ -808,6 +815,7 @@ extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(
 // by the caller between steps)
 static int step_body(swpc_ctx *c, int it, const int *d_it) {
     RC(launch_wav(c, it, d_it));
+    RC(snap_launch(c, it, d_it));
     RC(launch_stress(c, 3));
     RC(launch_glut(c, it, d_it));
     if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) {

@@ -56,6 +56,8 @@ struct Wav2Args;
 
 }  // namespace swpc
 
+struct swpc_snap_state;
+
 struct swpc_ctx {
     int kind;
     swpc::Geo g;
@@ -119,6 +121,9 @@ struct swpc_ctx {
     float *eacc = nullptr;        // (6, nst)
     float r40[3], r41[3];         // m_wav.f90:130-135
 
+    // snapshot planes (swpc_snap.cu)
+    swpc_snap_state *snp = nullptr;
+
     // vmax
     unsigned int *vmax_buf = nullptr;
     unsigned int *h_vmax = nullptr;   // pinned
@@ -150,6 +155,8 @@ struct swpc_ctx {
 // helpers shared by the translation units
 namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
+int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
+void snap_free(swpc_ctx *c);
 int cuda_check(swpc_ctx *c, cudaError_t e, const char *what);
 template <typename T>
 int dalloc(swpc_ctx *c, T **p, size_t n) {

@@ -97,6 +97,16 @@ class Params:
     sw_wav_stress: bool = False
     sw_wav_strain: bool = False
     abc_type: str = "pml"
+    # snapshots (m_snap.f90:105-127): enabled planes as "<section>_<quantity>"
+    # names (sections yz xz xy fs ob, quantities ps v u), e.g. {"xz_v", "fs_u"}
+    snaps: set = field(default_factory=set)
+    z0_xy: float | None = None
+    x0_yz: float | None = None
+    y0_xz: float | None = None
+    idec: int = 1
+    jdec: int = 1
+    kdec: int = 1
+    ntdec_s: int = 10
     layers: list[Layer] = field(default_factory=list)
     sources: list[Source] = field(default_factory=list)
     stations: list[Station] = field(default_factory=list)
@@ -117,6 +127,16 @@ class Params:
             raise ValueError("nm must be 0..3")
         if self.stftype not in ("kupper", "boxcar", "triangle", "herrmann", "cosine", "scosine", "texp"):
             raise ValueError(f"unknown stftype {self.stftype!r}")
+
+
+SNAP_SECTIONS = ("yz", "xz", "xy", "fs", "ob")
+SNAP_QUANTITIES = ("ps", "v", "u")
+
+
+def snap_plane(name: str) -> int:
+    """Plane id 3*section + quantity of a "<section>_<quantity>" name."""
+    sec, q = name.split("_")
+    return 3 * SNAP_SECTIONS.index(sec) + SNAP_QUANTITIES.index(q)
 
 
 _COMMENT = re.compile(r"!!.*$")
@@ -172,6 +192,14 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
             args[key] = _conv(kv[key], typ)
         elif strict and key not in ("xbeg", "ybeg", "zbeg"):
             raise KeyError(f"parameter {key} missing in strict mode")
+    for key in ("z0_xy", "x0_yz", "y0_xz"):
+        if key in kv:
+            args[key] = _conv(kv[key], float)
+    for key in ("idec", "jdec", "kdec", "ntdec_s"):
+        if key in kv:
+            args[key] = _conv(kv[key], int)
+    args["snaps"] = {f"{sec}_{q}" for sec in SNAP_SECTIONS for q in SNAP_QUANTITIES
+                     if _conv(kv.get(f"{sec}_{q}%sw", ".false."), bool)}
     p = Params(**args)
     base = Path(path).parent
     if kv.get("vmodel_type", "lhm") == "lhm" and "fn_lhm" in kv:

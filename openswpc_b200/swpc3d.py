@@ -242,6 +242,10 @@ class Swpc3D:
             check(self.ctx, self.lib.swpc_wav_setup(self.ctx, self.nst, iptr(self.ist), iptr(self.jst),
                                                     iptr(self.kst), p.ntdec_w, what, self.M0, self.UC))
         self.what = what
+        # snap__setup (m_snap.f90:95-322)
+        self.snap_nframes = 0
+        if p.snaps:
+            self.snap__setup()
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -291,6 +295,54 @@ class Swpc3D:
 
     def wav__store(self, it: int):
         check(self.ctx, self.lib.swpc_wav_store(self.ctx, it))
+
+    def snap__setup(self):
+        """Enable the snapshot planes named in ``p.snaps`` with the
+        reference's defaults for the section positions (m_snap.f90:118-120)."""
+        from .params import snap_plane
+
+        p = self.p
+        xend = f32(p.xbeg) + f32(p.nx) * f32(p.dx)
+        yend = f32(p.ybeg) + f32(p.ny) * f32(p.dy)
+        zend = f32(p.zbeg) + f32(p.nz) * f32(p.dz)
+        z0 = f32(p.z0_xy) if p.z0_xy is not None else max(min(f32(10.0), zend), f32(p.zbeg))
+        x0 = f32(p.x0_yz) if p.x0_yz is not None else max(min(f32(0.0), xend), f32(p.xbeg))
+        y0 = f32(p.y0_xz) if p.y0_xz is not None else max(min(f32(0.0), yend), f32(p.ybeg))
+        lib = self.lib
+        planes = 0
+        for name in p.snaps:
+            planes |= 1 << snap_plane(name)
+        d = _lib.SnapDesc(planes, p.idec, p.jdec, p.kdec, p.ntdec_s, lib.swpc_x2i(float(x0), p.xbeg, p.dx),
+                          lib.swpc_x2i(float(y0), p.ybeg, p.dy), lib.swpc_x2i(float(z0), p.zbeg, p.dz),
+                          float(f32(self.M0)), float(f32(self.UC)))
+        check(self.ctx, lib.swpc_snap_setup(self.ctx, C.byref(d)))
+        self.snap_desc = d
+        self.snap_nframes = (p.nt - 1) // p.ntdec_s + 1
+
+    def snap__write(self, it: int):
+        check(self.ctx, self.lib.swpc_snap_write(self.ctx, it))
+
+    def snapshots(self, name: str) -> np.ndarray:
+        """Frames of one plane ("xz_v", "fs_ps", ...): (nframes, nvar, n2, n1)."""
+        from .params import snap_plane
+
+        plane = snap_plane(name)
+        nv, n1, n2, nf = (C.c_int() for _ in range(4))
+        check(self.ctx, self.lib.swpc_snap_dims(self.ctx, plane, C.byref(nv), C.byref(n1), C.byref(n2),
+                                                C.byref(nf)))
+        out = np.zeros((nf.value, nv.value, n2.value, n1.value), np.float32)
+        check(self.ctx, self.lib.swpc_snap_fetch(self.ctx, plane, fptr(out)))
+        return out
+
+    def snapshot_max(self, name: str) -> np.ndarray:
+        """Running maxima of "fs_v", "fs_u", "ob_v" or "ob_u": (3, nys, nxs)
+        = vertical, horizontal, vector."""
+        which = {"fs_v": 0, "fs_u": 1, "ob_v": 2, "ob_u": 3}[name]
+        nv, n1, n2, nf = (C.c_int() for _ in range(4))
+        check(self.ctx, self.lib.swpc_snap_dims(self.ctx, 9, C.byref(nv), C.byref(n1), C.byref(n2), C.byref(nf)))
+        out = np.zeros((3, n2.value, n1.value), np.float32)
+        check(self.ctx, self.lib.swpc_snap_fetch_max(self.ctx, which, fptr(out)))
+        return out
 
     def kernel__vmax(self) -> np.ndarray:
         out = np.zeros(3, np.float32)

@@ -78,6 +78,11 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_sdr2moment": (None, [f, f, f, _FP]),
         "o3d_visco_set_relaxtime": (None, [i, _FP, f, f]),
         "o3d_visco_constq_zeta": (f, [i, f, f, _FP]),
+        "o3d_snap_setup": (i, [vp, i, i, i, i, i, f, f, f]),
+        "o3d_snap_write": (None, [vp, i]),
+        "o3d_snap_dims": (None, [vp, _IP]),
+        "o3d_snap_frames": (vp, [vp, i]),
+        "o3d_snap_max": (vp, [vp, i]),
     }
     for name in ("o3d_update_stress", "o3d_absorb_update_stress", "o3d_update_vel", "o3d_absorb_update_vel",
                  "o3d_comm_stress", "o3d_comm_vel"):
@@ -265,6 +270,39 @@ class Oracle3D:
         ptr = self.lib.o3d_ptr(self.o, fid)
         v = np.ascontiguousarray(values, cur.dtype).reshape(cur.shape)
         C.memmove(ptr, v.ctypes.data, v.nbytes)
+
+    # -- snapshots (m_snap.f90) --------------------------------------------
+    def snap_setup(self, planes: int, idec: int, jdec: int, kdec: int, ntdec_s: int, x0_yz: float, y0_xz: float,
+                   z0_xy: float) -> int:
+        """snap__setup for the planes whose bit (3*section + quantity) is set;
+        sections yz xz xy fs ob, quantities ps v u.  Returns the frame count."""
+        return self.lib.o3d_snap_setup(self.o, planes, idec, jdec, kdec, ntdec_s, x0_yz, y0_xz, z0_xy)
+
+    def snap_dims(self) -> dict:
+        out = np.zeros(7, np.int32)
+        self.lib.o3d_snap_dims(self.o, out.ctypes.data_as(_IP))
+        return dict(zip(("nxs", "nys", "nzs", "nframes", "i0_yz", "j0_xz", "k0_xy"), (int(v) for v in out)))
+
+    def snap_frames(self, plane: int) -> np.ndarray:
+        """(nframes, nvar, n2, n1) frames of one plane."""
+        d = self.snap_dims()
+        sec, q = divmod(plane, 3)
+        nv = 4 if q == 0 else 3
+        n1, n2 = {0: (d["nys"], d["nzs"]), 1: (d["nxs"], d["nzs"])}.get(sec, (d["nxs"], d["nys"]))
+        ptr = self.lib.o3d_snap_frames(self.o, plane)
+        n = d["nframes"] * nv * n1 * n2
+        buf = (C.c_float * n).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float32).reshape(d["nframes"], nv, n2, n1).copy()
+
+    def snap_max(self, which: int) -> np.ndarray:
+        """Running maxima (3, nys, nxs): 0 fs v, 1 fs u, 2 ob v, 3 ob u."""
+        d = self.snap_dims()
+        ptr = self.lib.o3d_snap_max(self.o, which)
+        buf = (C.c_float * (3 * d["nxs"] * d["nys"])).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float32).reshape(3, d["nys"], d["nxs"]).copy()
+
+    def snap_write(self, it: int):
+        self.lib.o3d_snap_write(self.o, it)
 
     # -- stepping -----------------------------------------------------------
     def step(self, it: int):

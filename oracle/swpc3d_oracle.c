@@ -103,6 +103,14 @@ typedef struct o3d {
     float *wav_vel, *wav_disp, *wav_stress, *wav_strain;   /* (ntw, ncmp, nst) */
     SPR *ux, *uy, *uz, *exx, *eyy, *ezz, *eyz, *exz, *exy;
     MPR r40x, r40y, r40z, r41x, r41y, r41z;                /* m_wav.f90:130-135 */
+    /* snapshots (m_snap.f90:30-90); plane = 3 * section + quantity with
+     * sections yz xz xy fs ob and quantities ps v u */
+    int snp_planes, idec, jdec, kdec, ntdec_s, i0_yz, j0_xz, k0_xy;
+    int nxs, nys, nzs, is0, is1, js0, js1, ks0, ks1, nframes;
+    MPR sr20x, sr20y, sr20z;
+    float *snp[15];             /* frames (nframes, nvar, n2, n1) */
+    float *sbuf[15];            /* current buffer (nvar, n2, n1): the `save` buf of each wbuf_* */
+    float *maxv[4];             /* max_fs_v, max_fs_u, max_ob_v, max_ob_u (3, nys, nxs) */
     int threads;
 } o3d;
 
@@ -363,6 +371,8 @@ void o3d_destroy(o3d *o) {
                   o->kst, o->wav_vel, o->wav_disp, o->wav_stress, o->wav_strain, o->ux, o->uy, o->uz,
                   o->exx, o->eyy, o->ezz, o->eyz, o->exz, o->exy};
     for (size_t n = 0; n < sizeof(ps) / sizeof(ps[0]); n++) free(ps[n]);
+    for (int q = 0; q < 15; q++) { free(o->snp[q]); free(o->sbuf[q]); }
+    for (int q = 0; q < 4; q++) free(o->maxv[q]);
     free(o);
 }
 
@@ -1273,9 +1283,158 @@ void o3d_vmax(o3d *o, float *out) {
     out[0] = xm; out[1] = ym; out[2] = zm;
 }
 
+/* ------------------------------------------------------------------------ */
+/* snapshots: snap__setup (m_snap.f90:95-322) and the wbuf_* routines of     */
+/* snap__write (m_snap.f90:911-2185) for a single MPI node; the file output  */
+/* is replaced by frames kept in memory                                      */
+/* ------------------------------------------------------------------------ */
+static void snap_dims(const o3d *o, int plane, int *nvar, int *n1, int *n2) {
+    int sec = plane / 3, q = plane % 3;
+    *nvar = q == 0 ? 4 : 3;
+    if (sec == 0) { *n1 = o->nys; *n2 = o->nzs; }
+    else if (sec == 1) { *n1 = o->nxs; *n2 = o->nzs; }
+    else { *n1 = o->nxs; *n2 = o->nys; }
+}
+
+int o3d_snap_setup(o3d *o, int planes, int idec, int jdec, int kdec, int ntdec_s, float x0_yz, float y0_xz,
+                   float z0_xy) {
+    o->snp_planes = planes; o->idec = idec; o->jdec = jdec; o->kdec = kdec; o->ntdec_s = ntdec_s;
+    /* m_snap.f90:128-131 */
+    o->nxs = (o->nx + idec / 2) / idec;
+    o->nys = (o->ny + jdec / 2) / jdec;
+    o->nzs = (o->nz + kdec / 2) / kdec;
+    /* m_snap.f90:149-154 */
+    o->is0 = (int)ceilf((float)(o->ibeg + idec / 2) / (float)idec);
+    o->is1 = (int)floorf((float)(o->iend + idec / 2) / (float)idec);
+    o->js0 = (int)ceilf((float)(o->jbeg + jdec / 2) / (float)jdec);
+    o->js1 = (int)floorf((float)(o->jend + jdec / 2) / (float)jdec);
+    o->ks0 = (int)ceilf((float)(o->kbeg + kdec / 2) / (float)kdec);
+    o->ks1 = (int)floorf((float)(o->kend + kdec / 2) / (float)kdec);
+    /* m_snap.f90:157-159 */
+    o->k0_xy = o3d_x2i(z0_xy, o->zbeg, (float)o->dz);
+    o->i0_yz = o3d_x2i(x0_yz, o->xbeg, (float)o->dx);
+    o->j0_xz = o3d_x2i(y0_xz, o->ybeg, (float)o->dy);
+    /* m_snap.f90:311-313 */
+    o->sr20x = (MPR)1.0 / o->dx;
+    o->sr20y = (MPR)1.0 / o->dy;
+    o->sr20z = (MPR)1.0 / o->dz;
+    o->nframes = (o->nt - 1) / ntdec_s + 1;
+    for (int p = 0; p < 15; p++) {
+        if (!(planes >> p & 1)) continue;
+        int nv, n1, n2;
+        snap_dims(o, p, &nv, &n1, &n2);
+        o->snp[p] = (float *)zalloc(sizeof(float) * (size_t)o->nframes * nv * n1 * n2);
+        o->sbuf[p] = (float *)zalloc(sizeof(float) * (size_t)nv * n1 * n2);
+    }
+    for (int q = 0; q < 4; q++) o->maxv[q] = (float *)zalloc(sizeof(float) * 3 * (size_t)o->nxs * o->nys);
+    return o->nframes;
+}
+
+/* grid cell of snapshot sample (a, b) of a section (m_snap.f90 wbuf_*) */
+static void snap_cell(const o3d *o, int sec, int a, int b, int *k, int *i, int *j) {
+    switch (sec) {
+    case 0: *i = o->i0_yz; *j = a * o->jdec - o->jdec / 2; *k = b * o->kdec - o->kdec / 2; break;
+    case 1: *i = a * o->idec - o->idec / 2; *j = o->j0_xz; *k = b * o->kdec - o->kdec / 2; break;
+    case 2: *i = a * o->idec - o->idec / 2; *j = b * o->jdec - o->jdec / 2; *k = o->k0_xy; break;
+    case 3: *i = a * o->idec - o->idec / 2; *j = b * o->jdec - o->jdec / 2; *k = A2(o->kfs, *i, *j) + 1; break;
+    default: *i = a * o->idec - o->idec / 2; *j = b * o->jdec - o->jdec / 2; *k = A2(o->kob, *i, *j) + 1; break;
+    }
+}
+
+static float fmax_f(float a, float b) { return a > b ? a : b; }
+
+/* one wbuf_<section>_<quantity> call (m_snap.f90:973-2185) */
+static void snap_plane(o3d *o, int p, int it) {
+    const int sec = p / 3, q = p % 3;
+    int nv, n1, n2;
+    snap_dims(o, p, &nv, &n1, &n2);
+    const long ns = (long)n1 * n2;
+    const int a0 = sec == 0 ? o->js0 : o->is0, a1 = sec == 0 ? o->js1 : o->is1;
+    const int b0 = sec <= 1 ? o->ks0 : o->js0, b1 = sec <= 1 ? o->ks1 : o->js1;
+    const int snap_step = ((it - 1) % o->ntdec_s == 0) || (it > o->nt);
+    const int every_step = q == 2 || sec >= 3;   /* u planes and fs/ob v feed running sums / maxima */
+    float *buf = o->sbuf[p];
+    const float UC = o->UC, M0 = o->M0;
+    const float eps = 1.1920929e-07f;            /* epsilon(1.0) */
+    MPR *Vx = o->Vx, *Vy = o->Vy, *Vz = o->Vz;
+    if (q == 0 && !snap_step) return;
+    if (q == 1 && !snap_step && !(sec >= 3)) return;
+    if (q == 1 && sec == 0) memset(buf, 0, sizeof(float) * 3 * ns);   /* wbuf_yz_v: buf = 0.0 */
+    for (int b = b0; b <= b1; b++)
+        for (int a = a0; a <= a1; a++) {
+            int k, i, j;
+            snap_cell(o, sec, a, b, &k, &i, &j);
+            long e = (long)(b - 1) * n1 + (a - 1);
+            if (q == 0) {
+                const MPR r20x = o->sr20x, r20y = o->sr20y, r20z = o->sr20z;
+                SPR div = (SPR)((A3(Vx, k, i, j) - A3(Vx, k, i - 1, j)) * r20x
+                              + (A3(Vy, k, i, j) - A3(Vy, k, i, j - 1)) * r20y
+                              + (A3(Vz, k, i, j) - A3(Vz, k - 1, i, j)) * r20z);
+                SPR rot_x = (SPR)((A3(Vz, k, i, j + 1) - A3(Vz, k, i, j)) * r20y
+                                - (A3(Vy, k + 1, i, j) - A3(Vy, k, i, j)) * r20z);
+                SPR rot_y = (SPR)((A3(Vx, k + 1, i, j) - A3(Vx, k, i, j)) * r20z
+                                - (A3(Vz, k, i + 1, j) - A3(Vz, k, i, j)) * r20x);
+                SPR rot_z = (SPR)((A3(Vy, k, i + 1, j) - A3(Vy, k, i, j)) * r20x
+                                - (A3(Vx, k, i, j + 1) - A3(Vx, k, i, j)) * r20y);
+                SPR lam = A3(o->lam, k, i, j), muyz = A3(o->muyz, k, i, j);
+                SPR muxz = A3(o->muxz, k, i, j), muxy = A3(o->muxy, k, i, j);
+                div = div * lam / (SPR)fabs(lam + (SPR)eps);
+                rot_x = rot_x * muyz / (SPR)fabs(muyz + (SPR)eps);
+                rot_y = rot_y * muxz / (SPR)fabs(muxz + (SPR)eps);
+                rot_z = rot_z * muxy / (SPR)fabs(muxy + (SPR)eps);
+                buf[0 * ns + e] = (float)(div * UC * M0 * 1e-3f);
+                buf[1 * ns + e] = (float)(rot_x * UC * M0 * 1e-3f);
+                buf[2 * ns + e] = (float)(rot_y * UC * M0 * 1e-3f);
+                buf[3 * ns + e] = (float)(rot_z * UC * M0 * 1e-3f);
+            } else if (q == 1) {
+                buf[0 * ns + e] = (float)(A3(Vx, k, i, j) * (MPR)UC * (MPR)M0);
+                buf[1 * ns + e] = (float)(A3(Vy, k, i, j) * (MPR)UC * (MPR)M0);
+                buf[2 * ns + e] = (float)(A3(Vz, k, i, j) * (MPR)UC * (MPR)M0);
+            } else {
+                const MPR dt = (MPR)o->dt;
+                buf[0 * ns + e] = (float)((MPR)buf[0 * ns + e] + A3(Vx, k, i, j) * (MPR)UC * (MPR)M0 * dt);
+                buf[1 * ns + e] = (float)((MPR)buf[1 * ns + e] + A3(Vy, k, i, j) * (MPR)UC * (MPR)M0 * dt);
+                buf[2 * ns + e] = (float)((MPR)buf[2 * ns + e] + A3(Vz, k, i, j) * (MPR)UC * (MPR)M0 * dt);
+            }
+        }
+    if (sec >= 3 && q >= 1) {
+        /* running maxima of wbuf_fs_v / _ob_v / _fs_u / _ob_u (m_snap.f90:1691-1703) */
+        float *mx = o->maxv[(sec - 3) * 2 + (q - 1)];
+        for (int b = b0; b <= b1; b++)
+            for (int a = a0; a <= a1; a++) {
+                long e = (long)(b - 1) * n1 + (a - 1);
+                float b1v = buf[e], b2v = buf[ns + e], b3v = buf[2 * ns + e];
+                mx[e] = fmax_f(mx[e], fabsf(b3v));
+                mx[ns + e] = fmax_f(mx[ns + e], sqrtf(b1v * b1v + b2v * b2v));
+                mx[2 * ns + e] = sqrtf(mx[e] * mx[e] + mx[ns + e] * mx[ns + e]);
+            }
+    }
+    (void)every_step;
+    if (snap_step && it <= o->nt) {
+        long f = (it - 1) / o->ntdec_s;
+        memcpy(o->snp[p] + f * nv * ns, buf, sizeof(float) * nv * ns);
+    }
+}
+
+/* snap__write (m_snap.f90:911-939): the reference's call order */
+void o3d_snap_write(o3d *o, int it) {
+    static const int order[15] = {3, 6, 9, 12, 0, 1, 4, 7, 10, 13, 2, 5, 8, 11, 14};
+    if (!o->snp_planes) return;
+    for (int n = 0; n < 15; n++)
+        if (o->snp_planes >> order[n] & 1) snap_plane(o, order[n], it);
+}
+
+void o3d_snap_dims(const o3d *o, int *out) {
+    out[0] = o->nxs; out[1] = o->nys; out[2] = o->nzs; out[3] = o->nframes;
+    out[4] = o->i0_yz; out[5] = o->j0_xz; out[6] = o->k0_xy;
+}
+float *o3d_snap_frames(o3d *o, int plane) { return (plane >= 0 && plane < 15) ? o->snp[plane] : 0; }
+float *o3d_snap_max(o3d *o, int which) { return (which >= 0 && which < 4) ? o->maxv[which] : 0; }
+
 /* one pass of the main.f90:125-144 loop body (report__progress excluded) */
 void o3d_step(o3d *o, int it) {
     o3d_wav_store(o, it);
+    o3d_snap_write(o, it);
     o3d_update_stress(o);
     o3d_absorb_update_stress(o);
     o3d_stressglut(o, it);
