@@ -175,15 +175,16 @@ extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes 
 
 extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj) {
     if (!c) return SWPC_ERR_ARG;
-    if (kernel < 0 || kernel > 3 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
-        (kernel < 2 && 32 * bi * bj > 256))
-        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..3, minb 1..4, 32*bi*bj <= 256)");
+    if (kernel < 0 || kernel > 4 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
+        ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
+        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..4, minb 1..4, 32*bi*bj <= 256)");
     invalidate_graph(c);
     switch (kernel) {
     case 0: c->stress_march = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
-    case 1: c->vel_march = false; c->vel_minb = minb; c->vbi = bi; c->vbj = bj; break;
+    case 1: c->vel_march = false; c->vel_vec = false; c->vel_minb = minb; c->vbi = bi; c->vbj = bj; break;
     case 2: c->stress_march = true; c->stress_mminb = minb; c->stress_jc = bj; break;
-    default: c->vel_march = true; c->vel_mminb = minb; c->vel_jc = bj; break;
+    case 3: c->vel_march = true; c->vel_vec = false; c->vel_mminb = minb; c->vel_jc = bj; break;
+    default: c->vel_march = false; c->vel_vec = true; c->vel_vminb = minb; c->vel_vbi = bi; c->vel_vbj = bj; break;
     }
     return SWPC_OK;
 }
@@ -712,7 +713,8 @@ static int launch_vel(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
-    if (c->vel_march) launch_vel3d_march(a, c->vel_mminb, c->vel_jc, c->stream);
+    if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);
+    else if (c->vel_march) launch_vel3d_march(a, c->vel_mminb, c->vel_jc, c->stream);
     else launch_vel3d(a, c->vel_minb, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "vel3d launch");
 }

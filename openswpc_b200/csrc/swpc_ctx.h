@@ -148,6 +148,9 @@ struct swpc_ctx {
     // 2.5D marching variants (32 x 8 plane tile walking jc planes along j)
     bool stress_march = false, vel_march = false;
     int stress_jc = 8, vel_jc = 8, stress_mminb = 2, vel_mminb = 2;
+    // velocity kernel with four consecutive k per thread (swpc3d_vec.cu)
+    bool vel_vec = false;
+    int vel_vminb = 2, vel_vbi = 2, vel_vbj = 2;
 
     long long bytes = 0;
 };

@@ -85,6 +85,7 @@ void launch_vel3d(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream
 void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st);
 void launch_stress3d_march(const Str3Args &a, int nm, int minb, int jc, cudaStream_t st);
 void launch_vel3d_march(const Vel3Args &a, int minb, int jc, cudaStream_t st);
+void launch_vel3d_vec(const Vel3Args &a, int minb, dim3 block, cudaStream_t st);
 void launch_inject(const InjArgs &a, cudaStream_t st);
 void launch_inject_multi(const InjArgs *list, int nlist, int max_n, const int *d_it, int it, cudaStream_t st);
 void launch_wav3d(const Wav3Args &a, cudaStream_t st);

@@ -264,9 +264,12 @@ def test_larger_grid_against_oracle_few_steps():
 
 
 @pytest.mark.parametrize("variant", [(0, 2, 2, 1, 1, 4, 2, 2), (0, 1, 4, 2, 1, 3, 8, 1), (2, 2, 1, 16, 3, 2, 1, 7),
-                                     (2, 1, 1, 64, 3, 1, 1, 3)])
+                                     (2, 1, 1, 64, 3, 1, 1, 3), (0, 2, 2, 1, 4, 2, 2, 2), (0, 2, 2, 1, 4, 1, 4, 1),
+                                     (0, 2, 2, 1, 4, 3, 1, 2)])
 def test_launch_variants_are_bitwise_identical(variant):
-    """Flat and marching kernels, any block shape or chunk length: same bits."""
+    """Flat, marching and four-cells-per-thread kernels, any block shape or
+    chunk length: same bits.  nz = 70 with na = 8 puts the interior/absorber
+    boundary inside a group of four and ends the column mid-group."""
     ks, ms, bis, bjs, kv, mv, biv, bjv = variant
     p = small3d(nx=44, ny=38, nz=70, na=8, nt=25)
     g0 = Swpc3D(p)
