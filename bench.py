@@ -85,6 +85,198 @@ def make_params(name: str):
                   ntdec_r=50)
 
 
+# 2D P-SV algorithmic bytes per cell-update (FP32, nm = 3): velocity phase 2 V read+write, 3 S, rho; stress
+# phase 2 V, 3 S read+write, 9 R read+write, lam, mu, taup, taus (interior); PML: 34 floats
+B_PSV_INT, B_PSV_PML = 38 * 4, 34 * 4
+
+
+def make_c2a_models(n: int = 64, seed: int = 20260203):
+    """The batched-ensemble workload: n seeded P-SV models of uneven size
+    (nx in [256, 2048], nz in [128, 1024]), dx = 0.1 km, dt = 0.005 s,
+    nt = 3000, 3-6 layers with vs 1.5-4.5 km/s (increasing with depth),
+    vp/vs 1.7-1.9, rho from Gardner's law (rho = 1.741 vp^0.25), Q = 50 vs
+    (Qp = 2 Qs), nm = 3, one explosion (mxx = mzz = 1) with a Kupper wavelet
+    of T = 0.5 s, 16 surface stations."""
+    from openswpc_b200.params import Layer, Params, Source, Station
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nx = int(rng.integers(256, 2049))
+        nz = int(rng.integers(128, 1025))
+        dx = 0.1
+        nl = int(rng.integers(3, 7))
+        tops = [0.0] + sorted(float(v) for v in rng.uniform(0.3, 0.8 * nz * dx, nl - 1))
+        vs = np.sort(rng.uniform(1.5, 4.5, nl))
+        vp = vs * rng.uniform(1.7, 1.9, nl)
+        layers = [Layer(tops[l], float(1.741 * vp[l] ** 0.25), float(vp[l]), float(vs[l]), float(100 * vs[l]),
+                        float(50 * vs[l])) for l in range(nl)]
+        xb = -(nx // 2) * dx
+        na = 20
+        src = [Source(float(rng.uniform(xb + (na + 10) * dx, -xb - (na + 10) * dx)), 0.0,
+                      float(rng.uniform(0.5, 0.5 * (nz - na) * dx)), 0.0, 0.5, mo=1e15, mxx=1.0, myy=1.0, mzz=1.0)]
+        st = [Station(float(xb + (na + 2 + (nx - 2 * na - 4) * (q + 0.5) / 16) * dx), 0.0, 0.0, f"s{q:02d}", "fsb")
+              for q in range(16)]
+        out.append(Params(nx=nx, ny=1, nz=nz, nt=3000, dx=dx, dy=dx, dz=dx, dt=0.005, na=na, nm=3, xbeg=xb,
+                          ybeg=0.0, zbeg=-3 * dx, fq_min=0.05, fq_max=4.0, layers=layers, sources=src, stations=st,
+                          ntdec_w=5, ntdec_r=100))
+    return out
+
+
+def c2a_cells(ps):
+    n_int = sum((p.nx - 2 * p.na) * (p.nz - p.na) for p in ps)
+    return n_int, sum(p.nx * p.nz for p in ps) - n_int
+
+
+def bench_c2a(args, world, rank, local):
+    """Batched 2D P-SV ensemble (one persistent launch per half step, CUDA
+    graph) against the plain per-model loop on the same GPU."""
+    ps_all = make_c2a_models()
+    ps = [p for m, p in enumerate(ps_all) if m % world == rank]   # members shard across GPUs
+    wl = {"workload": "batched ensemble of 64 uneven 2D P-SV models (nx 256-2048, nz 128-1024, nm=3, PML 20)",
+          "models": len(ps_all), "cells": sum(p.nx * p.nz for p in ps_all),
+          "l2": "inputs larger than L2 (all members resident, several GB)", "parallelism": f"members/{world} GPUs"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle.oracle import Oracle2D
+
+        p = ps_all[0]
+        o = Oracle2D(p, "psv")
+        for it in range(1, args.warmup + 1):
+            o.step(it)
+        t0 = time.perf_counter()
+        n = 0
+        for it in range(args.warmup + 1, args.warmup + 1 + args.steps):
+            o.step(it)
+            n += 1
+            if time.perf_counter() - t0 > args.cpu_budget and n >= 2:
+                break
+        dt = time.perf_counter() - t0
+        v = p.nx * p.nz * n / dt / 1e9
+        line = {"impl": "reference", "metric": "Gcell-updates/s (2D P-SV visco, FP32, batched ensemble)", "value": v,
+                "unit": UNIT, "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
+                "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": wl,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                 "sample": f"2D oracle f32, one thread, model 0 ({p.nx}x{p.nz}), {n} steps"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from openswpc_b200 import _lib
+    from openswpc_b200.swpc2d import Batch2D, Swpc2D
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    runs = [Swpc2D(p, "psv", device=local) for p in ps]
+    lib = _lib.load()
+    batch = Batch2D(runs)
+    used, ti, ri, bps = batch.autotune(1, reps=2)
+    it0 = 1 + used
+    batch.run(it0, args.warmup)
+    it0 += args.warmup
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms_batch = batch.time_steps(it0, args.steps)
+    it0 += args.steps
+    ms_batch = max_over_ranks(ms_batch)
+    # the plain per-model loop: each member alone, its own CUDA graph, one after another
+    ms_loop = 0.0
+    for r in runs:
+        check = _lib.check
+        check(r.ctx, lib.swpc_run(r.ctx, it0, args.warmup))
+        ms = C.c_float()
+        check(r.ctx, lib.swpc_time_steps(r.ctx, it0 + args.warmup, args.steps, C.byref(ms)))
+        ms_loop += ms.value
+    ms_loop = max_over_ranks(ms_loop)
+    # the same loop through per-step C-ABI calls (no graph), as a driver calling swpc_step would
+    ms_calls = 0.0
+    it1 = it0 + args.warmup + args.steps
+    for r in runs:
+        st = torch.cuda.ExternalStream(lib.swpc_stream(r.ctx), device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _lib.check(r.ctx, lib.swpc_sync(r.ctx))
+        e0.record(st)
+        for n in range(args.steps):
+            _lib.check(r.ctx, lib.swpc_step(r.ctx, it1 + n))
+        e1.record(st)
+        e1.synchronize()
+        ms_calls += e0.elapsed_time(e1)
+    ms_calls = max_over_ranks(ms_calls)
+    cells = wl["cells"]
+    n_int, n_pml = c2a_cells(ps_all)
+    value = cells * args.steps / (ms_batch / 1e3) / 1e9
+    loop_value = cells * args.steps / (ms_loop / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    bytes_step = n_int * B_PSV_INT + n_pml * B_PSV_PML
+    ach = bytes_step * args.steps / (ms_batch / 1e3) / 1e9
+
+    # end to end through the C ABI: media from host memory, per-step batch calls, traces back
+    t0 = time.perf_counter()
+    for r in runs:
+        _lib.check(r.ctx, lib.swpc_upload_medium(r.ctx, C.byref(r.medium.view())))
+    it = 1
+    for n in range(args.steps):
+        rc = lib.swpc_batch_step(batch.b, it)
+        if rc:
+            raise RuntimeError(lib.swpc_batch_last_error(batch.b).decode())
+        it += 1
+    lib.swpc_batch_sync(batch.b)
+    h2d = 0
+    d2h = 0
+    for r in runs:
+        w = r.waveforms()
+        d2h += w.nbytes
+        m = r.medium
+        h2d += sum(getattr(m, f).nbytes for f in ("rho", "lam", "mu", "taup", "taus"))
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e_val = cells * args.steps / t_e2e / 1e9
+    line = {"metric": "Gcell-updates/s (2D P-SV visco, FP32, batched ensemble)", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered models)", "config": wl,
+            "plain_loop": {"value": loop_value, "unit": UNIT, "ms_per_step": ms_loop / args.steps,
+                           "what": "each member alone, its own CUDA graph, members one after another"},
+            "plain_loop_calls": {"value": cells * args.steps / (ms_calls / 1e3) / 1e9, "unit": UNIT,
+                                 "ms_per_step": ms_calls / args.steps,
+                                 "what": "each member alone through per-step swpc_step calls, one after another"},
+            "batched_over_loop": ms_loop / ms_batch,
+            "batched_over_loop_calls": ms_calls / ms_batch,
+            "autotune": {"threads_i": ti, "rows_per_thread": ri, "blocks_per_sm": bps, "steps_used": used},
+            "roofline": {"bound": "hbm", "kernel": "psv_stress_kernel + psv_vel_kernel (whole batched step)",
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": bytes_step},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps,
+                    "what": "media upload from host memory + per-step batch calls + trace download, wall clock"},
+            "gpu_launches": args.steps * 4, "clocks": clk.summary()}
+    batch.close()
+    for r in runs:
+        r.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def cell_counts(p):
     ni, nj, nk = p.nx - 2 * p.na, p.ny - 2 * p.na, p.nz - p.na
     n_int = ni * nj * nk
@@ -199,7 +391,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a"])
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -211,6 +403,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "c2a":
+        return bench_c2a(args, world, rank, local)
     p = make_params(args.workload)
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.lower().split("x"))

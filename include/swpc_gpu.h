@@ -310,6 +310,19 @@ int swpc_batch_step(swpc_batch *b, int it);
 int swpc_batch_run(swpc_batch *b, int it0, int nsteps);
 int swpc_batch_sync(swpc_batch *b);
 int swpc_batch_time_steps(swpc_batch *b, int it0, int nsteps, float *ms);
+/* Autotuner of the batched launch shape: tiles of 32 (k) x (ti*ri) (i)
+ * cells, a block of 32 x ti threads with ri rows per thread, a persistent
+ * grid of 148 x bps blocks (bps = 0: one block per tile).  It advances the batch by real time steps from
+ * it0 -- every candidate shape runs `reps` steps timed with CUDA events --
+ * and keeps the fastest shape; the results do not depend on the shape, so
+ * these are ordinary steps of the run.  *used = steps taken (it0 ..
+ * it0 + *used - 1); *best_ti, *best_ri, *best_bps (may be NULL) = the pick.
+ * No counterpart in the reference. */
+int swpc_batch_autotune(swpc_batch *b, int it0, int reps, int *used, int *best_ti, int *best_ri, int *best_bps);
+/* Sets the launch shape directly (ti threads in i per block, 32*ti <= 256;
+ * ri rows per thread; bps blocks per SM of the persistent grid, 0 = one block
+ * per tile). */
+int swpc_batch_set_shape(swpc_batch *b, int ti, int ri, int bps);
 const char *swpc_batch_last_error(const swpc_batch *b);
 int swpc_batch_destroy(swpc_batch *b);
 

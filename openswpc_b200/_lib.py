@@ -43,7 +43,8 @@ EXPORTS = [
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
-    "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps",
+    "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
+    "swpc_batch_set_shape",
     "swpc_batch_last_error", "swpc_batch_destroy",
 ]
 
@@ -158,6 +159,8 @@ def load():
         "swpc_batch_run": (i, [vp, i, i]),
         "swpc_batch_sync": (i, [vp]),
         "swpc_batch_time_steps": (i, [vp, i, i, _FP]),
+        "swpc_batch_autotune": (i, [vp, i, i, _IP, _IP, _IP, _IP]),
+        "swpc_batch_set_shape": (i, [vp, i, i, i]),
         "swpc_batch_last_error": (C.c_char_p, [vp]),
         "swpc_batch_destroy": (i, [vp]),
     }

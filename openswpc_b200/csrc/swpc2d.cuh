@@ -43,9 +43,19 @@ struct Wav2Args {
     float M0, UC, dt;
 };
 
+// Launch shape of the tile kernels: tiles of 32 (k) x (ti * ri) (i) cells,
+// one block of 32 x ti threads per tile with ri rows per thread, and a
+// persistent grid of 148 x blocks_per_sm blocks (0: one block per tile).
+// The results do not depend on the shape.
+struct TileShape {
+    int ti, ri, blocks_per_sm;
+};
+constexpr TileShape kDefaultTiles{4, 4, 0};
+
 void launch_stress2d(int kind, int nm, const Model2D *models, const Tile2D *tiles, int ntiles, int mask,
-                     cudaStream_t st);
-void launch_vel2d(int kind, const Model2D *models, const Tile2D *tiles, int ntiles, int mask, cudaStream_t st);
+                     TileShape ts, cudaStream_t st);
+void launch_vel2d(int kind, const Model2D *models, const Tile2D *tiles, int ntiles, int mask, TileShape ts,
+                  cudaStream_t st);
 void launch_wav2d(const Wav2Args *list, int nlist, int max_nst, int it, const int *d_it, cudaStream_t st);
 void launch_vmax2d(const float *V0, const float *V1, const int *kob, int Kp, int i0, int i1, unsigned int *out,
                    cudaStream_t st);

@@ -53,9 +53,9 @@ int create_2d(swpc_ctx *c) {
     if (!rc) rc = dalloc(c, &c->d_wav2d, 1);
     c->nm2d_aux = psv ? 8 : 4;
     if (rc) return rc;
-    // tile list: 32 (k) x 4 (i)
+    // tile list: 32 (k) x (ti * ri) (i)
     std::vector<Tile2D> tiles;
-    for (int i0 = 1; i0 <= g.nx; i0 += 4)
+    for (int i0 = 1; i0 <= g.nx; i0 += kDefaultTiles.ti * kDefaultTiles.ri)
         for (int k0 = 1; k0 <= g.nz; k0 += 32) tiles.push_back(Tile2D{0, k0, i0, 0});
     c->ntiles2d = (int)tiles.size();
     RC(dalloc(c, &c->d_tiles2d, tiles.size()));
@@ -172,12 +172,14 @@ Model2D model_of(const swpc_ctx *c) {
 
 int update_stress_2d(swpc_ctx *c, int mask) {
     launch_stress2d(c->kind, c->d.nm, c->d_model2d, c->d_tiles2d, c->ntiles2d, (c->d.na > 0) ? mask : (mask & 1),
+                    kDefaultTiles,
                     c->stream);
     return cuda_check(c, cudaGetLastError(), "stress2d launch");
 }
 
 int update_vel_2d(swpc_ctx *c, int mask) {
-    launch_vel2d(c->kind, c->d_model2d, c->d_tiles2d, c->ntiles2d, (c->d.na > 0) ? mask : (mask & 1), c->stream);
+    launch_vel2d(c->kind, c->d_model2d, c->d_tiles2d, c->ntiles2d, (c->d.na > 0) ? mask : (mask & 1), kDefaultTiles,
+                 c->stream);
     return cuda_check(c, cudaGetLastError(), "vel2d launch");
 }
 
@@ -240,6 +242,8 @@ struct swpc_batch {
     Model2D *d_models = nullptr;
     Tile2D *d_tiles = nullptr;
     int ntiles = 0;
+    TileShape shape = kDefaultTiles;
+    bool tuned = false;
     Wav2Args *d_wav = nullptr;
     int max_nst = 0;
     InjArgs *d_inj = nullptr;
@@ -274,11 +278,36 @@ extern "C" int swpc_batch_destroy(swpc_batch *b) {
     return SWPC_OK;
 }
 
+#define RCB(call)            \
+    do {                     \
+        int _rc = (call);    \
+        if (_rc) return _rc; \
+    } while (0)
+
 #define BCK(call)                                                                                            \
     do {                                                                                                     \
         cudaError_t _e = (call);                                                                             \
         if (_e != cudaSuccess) return berr(b, SWPC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorName(_e)); \
     } while (0)
+
+// tile list of every member for tiles of 32 (k) x (ts.ti * ts.ri) (i)
+static int set_tiles(swpc_batch *b, TileShape ts) {
+    std::vector<Tile2D> tiles;
+    for (int q = 0; q < (int)b->members.size(); q++) {
+        const swpc_ctx *c = b->members[q];
+        for (int i0 = 1; i0 <= c->g.nx; i0 += ts.ti * ts.ri)
+            for (int k0 = 1; k0 <= c->g.nz; k0 += 32) tiles.push_back(Tile2D{q, k0, i0, 0});
+    }
+    if (b->d_tiles && (int)tiles.size() > b->ntiles) {
+        BCK(cudaFree(b->d_tiles));
+        b->d_tiles = nullptr;
+    }
+    if (!b->d_tiles) BCK(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile2D)));
+    BCK(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice));
+    b->ntiles = (int)tiles.size();
+    b->shape = ts;
+    return SWPC_OK;
+}
 
 extern "C" int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **out) {
     if (!members || n < 1 || !out) return SWPC_ERR_ARG;
@@ -300,26 +329,24 @@ extern "C" int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **o
     BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     for (auto *c : b->members) BCK(cudaStreamSynchronize(c->stream));
     std::vector<Model2D> models;
-    std::vector<Tile2D> tiles;
     std::vector<Wav2Args> wavs;
     std::vector<InjArgs> injs;
     for (int q = 0; q < n; q++) {
         swpc_ctx *c = b->members[q];
         models.push_back(model_of(c));
-        for (int i0 = 1; i0 <= c->g.nx; i0 += 4)
-            for (int k0 = 1; k0 <= c->g.nz; k0 += 32) tiles.push_back(Tile2D{q, k0, i0, 0});
         if (c->nst > 0 && c->wav_what) {
             wavs.push_back(wav_of(c));
             b->max_nst = std::max(b->max_nst, c->nst);
         }
     }
-    b->ntiles = (int)tiles.size();
     BCK(cudaMalloc(&b->d_models, models.size() * sizeof(Model2D)));
-    BCK(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile2D)));
+    {
+        int rc = set_tiles(b, kDefaultTiles);
+        if (rc) return rc;
+    }
     BCK(cudaMalloc(&b->d_wav, std::max<size_t>(wavs.size(), 1) * sizeof(Wav2Args)));
     BCK(cudaMalloc(&b->d_it, sizeof(int)));
     BCK(cudaMemcpy(b->d_models, models.data(), models.size() * sizeof(Model2D), cudaMemcpyHostToDevice));
-    BCK(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice));
     if (!wavs.empty()) BCK(cudaMemcpy(b->d_wav, wavs.data(), wavs.size() * sizeof(Wav2Args), cudaMemcpyHostToDevice));
     b->max_nst = wavs.empty() ? 0 : b->max_nst;
     // injection: stress glut lists then body-force lists of every member
@@ -345,16 +372,16 @@ static int batch_step(swpc_batch *b, int it, const int *d_it) {
     }
     const int mask_all = 3;
     launch_wav2d(b->d_wav, nwav, b->max_nst, it, d_it, b->stream);
-    launch_stress2d(b->kind, b->nm, b->d_models, b->d_tiles, b->ntiles, mask_all, b->stream);
+    launch_stress2d(b->kind, b->nm, b->d_models, b->d_tiles, b->ntiles, mask_all, b->shape, b->stream);
     launch_inject_multi(b->d_inj, b->ninj, max_inj_n, d_it, it, b->stream);
     if (b->kind == SWPC_KIND_PSV && b->psv_bf_split) {
         // P-SV applies body forces between the interior and absorber velocity
         // updates (src/swpc_psv/main.f90:106-110)
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 1, b->stream);
+        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 1, b->shape, b->stream);
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 2, b->stream);
+        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 2, b->shape, b->stream);
     } else {
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, mask_all, b->stream);
+        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, mask_all, b->shape, b->stream);
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
     }
     BCK(cudaGetLastError());
@@ -393,6 +420,61 @@ extern "C" int swpc_batch_run(swpc_batch *b, int it0, int nsteps) {
 extern "C" int swpc_batch_sync(swpc_batch *b) {
     if (!b) return SWPC_ERR_ARG;
     BCK(cudaStreamSynchronize(b->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_batch_set_shape(swpc_batch *b, int ti, int ri, int bps) {
+    if (!b) return SWPC_ERR_ARG;
+    if (ti < 1 || ri < 1 || bps < 0 || 32 * ti > 256 || ri > 64 || bps > 64)
+        return berr(b, SWPC_ERR_ARG, "tile shape out of range (32*ti <= 256, 1 <= ri <= 64, 0 <= bps <= 64)");
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (b->graph) {
+        BCK(cudaGraphExecDestroy(b->graph));
+        b->graph = nullptr;
+    }
+    return set_tiles(b, TileShape{ti, ri, bps});
+}
+
+extern "C" int swpc_batch_autotune(swpc_batch *b, int it0, int reps, int *used, int *best_ti, int *best_ri,
+                                   int *best_bps) {
+    static const TileShape cand[] = {{4, 4, 0}, {4, 2, 0}, {4, 8, 0}, {2, 8, 0}, {2, 4, 0},
+                                     {8, 4, 0}, {8, 2, 0}, {4, 1, 16}};
+    const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
+    if (!b || !used || reps < 1) return SWPC_ERR_ARG;
+    if (it0 < 1 || it0 + ncand * reps - 1 > b->nt) return berr(b, SWPC_ERR_ARG, "not enough time steps left to tune");
+    BCK(cudaSetDevice(b->device));
+    if (b->graph) {
+        BCK(cudaGraphExecDestroy(b->graph));
+        b->graph = nullptr;
+    }
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    float best = 0.f;
+    TileShape pick = kDefaultTiles;
+    int it = it0, rc = SWPC_OK;
+    for (int n = 0; n < ncand && !rc; n++) {
+        rc = set_tiles(b, cand[n]);
+        if (rc) break;
+        cudaStreamSynchronize(b->stream);
+        cudaEventRecord(e0, b->stream);
+        for (int r = 0; r < reps && !rc; r++) rc = batch_step(b, it++, nullptr);
+        cudaEventRecord(e1, b->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = berr(b, SWPC_ERR_CUDA, "autotune step failed"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (n == 0 || ms < best) { best = ms; pick = cand[n]; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    RCB(set_tiles(b, pick));
+    b->tuned = true;
+    *used = it - it0;
+    if (best_ti) *best_ti = pick.ti;
+    if (best_ri) *best_ri = pick.ri;
+    if (best_bps) *best_bps = pick.blocks_per_sm;
     return SWPC_OK;
 }
 

@@ -258,6 +258,15 @@ class Batch2D:
         self._check(self.lib.swpc_batch_time_steps(self.b, it0, nsteps, C.byref(ms)))
         return ms.value
 
+    def autotune(self, it0: int, reps: int = 2) -> tuple[int, int, int, int]:
+        """Pick the launch shape while advancing steps it0 ..; returns
+        (steps used, threads in i per block, rows per thread, blocks per SM)."""
+        used, ti, ri, bps = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.swpc_batch_autotune(self.b, it0, reps, C.byref(used), C.byref(ti), C.byref(ri),
+                                                 C.byref(bps)))
+        self._check(self.lib.swpc_batch_sync(self.b))
+        return used.value, ti.value, ri.value, bps.value
+
     def close(self):
         if self.b:
             self.lib.swpc_batch_destroy(self.b)

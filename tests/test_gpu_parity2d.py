@@ -113,3 +113,23 @@ def test_batched_ensemble_equals_independent_runs(kind):
     o.run(1, 50)
     assert same_bits(runs[2].waveforms(), o.waveforms())
     batch.close()
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_batch_autotune_steps_are_ordinary_steps(kind):
+    """The autotuner advances the run with every candidate launch shape; the
+    result equals independent runs bit for bit."""
+    sizes = [(200, 40), (64, 120), (150, 77)]
+    ps = [small2d(kind, nx=nx, nz=nz, na=8, nt=40, seed=10 + s) for s, (nx, nz) in enumerate(sizes)]
+    runs = [Swpc2D(p, kind) for p in ps]
+    batch = Batch2D(runs)
+    used, ti, ri, bps = batch.autotune(1, reps=2)
+    assert used == 16 and ti in (2, 4, 8) and ri in (1, 2, 4, 8) and bps >= 0
+    batch.run(1 + used, 40 - used)
+    for r, p in zip(runs, ps):
+        a = Swpc2D(p, kind)
+        a.run(1, 40)
+        assert same_bits(r.waveforms(), a.waveforms())
+        for fid in r.field_ids.values():
+            assert same_bits(r.download(fid), a.download(fid))
+    batch.close()
