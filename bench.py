@@ -45,6 +45,9 @@ UNIT = "Gcell-updates/s"
 # once per phase that needs it and written once
 B_STRESS_INT, B_STRESS_PML = 58 * 4, 38 * 4
 B_VEL_INT, B_VEL_PML = 15 * 4, 33 * 4
+# the same per storage form of S and R: (stress int, stress PML, vel int, vel PML); BF16 R saves 36 x 2 B of the
+# interior stress phase, FP16 S + R also 12 x 2 B of stress and 6 x 2 B of velocity accesses per cell
+BYTES = {"f32": (232, 152, 60, 132), "bf16r": (160, 152, 60, 132), "f16sr": (136, 128, 48, 120)}
 FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic of one launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the c1 mix scaled
 # down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
@@ -385,6 +388,42 @@ def cpu_reference(p, xi, steps: int, warmup: int, threads: int, budget_s: float 
     return cells * n / dt / 1e9, n, cells, dt
 
 
+def accuracy_sample(p, precision: str, device: int, steps: int = 200):
+    """rel-L2 error of one storage form against the all-double oracle on a
+    128 x 128 x 64 sample of the workload (same spacing, medium statistics,
+    one source, 16 surface stations), after `steps` steps."""
+    from oracle.oracle import Oracle3D
+    from openswpc_b200 import _lib
+    from openswpc_b200.params import Params, Station
+    from openswpc_b200.swpc3d import Swpc3D
+
+    q = Params(**{**p.__dict__})
+    q.nx, q.ny, q.nz, q.na = 128, 128, 64, 16
+    q.nt = steps
+    q.xbeg, q.ybeg = -64 * q.dx, -64 * q.dy
+    src = q.sources[0]
+    q.sources = [type(src)(**{**src.__dict__, "x": 0.0, "y": 0.0, "z": min(src.z, 0.35 * q.nz * q.dz)})]
+    rng = np.random.default_rng(11)
+    q.stations = [Station(float(rng.uniform(-40, 40) * q.dx), float(rng.uniform(-40, 40) * q.dy), 0.0, f"a{n}", "fsb")
+                  for n in range(16)]
+    q.ntdec_r = 25
+    xi = rmed(q, seed=9, device="cpu")
+    o = Oracle3D(q, xi, variant="f64", threads=os.cpu_count() or 1)
+    o.run(1, steps)
+    g = Swpc3D(q, xi, device=device, precision=precision)
+    g.run(1, steps)
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    out = {"sample": f"128x128x64, {steps} steps, vs f64 oracle", "traces_v": rel(g.waveforms(_lib.WAV_V), o.waveforms("v"))}
+    out["final_v"] = rel(np.stack([g.download(n) for n in range(3)]), np.stack([o.array(nm) for nm in ("Vx", "Vy", "Vz")]))
+    g.close()
+    o.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,6 +433,10 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a"])
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
+    ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16sr"],
+                    help="storage of stress and memory variables (arithmetic is FP32)")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="add the rel-L2 error against the f64 oracle on a 128x128x64 sample of the workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
     args = ap.parse_args()
@@ -475,12 +518,13 @@ def main():
     xi = rmed(p, device=f"cuda:{device}")
     med = Medium(p, xi)
     torch.cuda.empty_cache()
-    sim = Swpc3D(p, device=device, medium=med)
+    sim = Swpc3D(p, device=device, medium=med, precision=args.precision)
     lib = sim.lib
     ctx = sim.ctx
 
     # ---- device throughput: CUDA-graph replays of the whole step ----------
     sim.run(1, args.warmup)
+    sim.rescale()   # FP16 storage: centre the array scales (no-op otherwise)
     sim.sync()
     barrier()
     torch.cuda.synchronize(device)
@@ -513,8 +557,9 @@ def main():
     stream.synchronize()
     t_stress = np.mean([ev[n][0].elapsed_time(ev[n][1]) for n in range(nk)])
     t_vel = np.mean([ev[n][2].elapsed_time(ev[n][3]) for n in range(nk)])
-    b_stress = n_int * B_STRESS_INT + n_pml * B_STRESS_PML
-    b_vel = n_int * B_VEL_INT + n_pml * B_VEL_PML
+    bsi, bsp, bvi, bvp = BYTES[args.precision]
+    b_stress = n_int * bsi + n_pml * bsp
+    b_vel = n_int * bvi + n_pml * bvp
     peak, peak_kind = hbm_peak()
     ach_stress = b_stress / (t_stress / 1e3) / 1e9
     ach_vel = b_vel / (t_vel / 1e3) / 1e9
@@ -558,7 +603,9 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered + von Karman medium)",
+            "vs_baseline": None, "dtype": "f32",
+            "storage": {"f32": "S, R FP32", "bf16r": "R BF16", "f16sr": "S, R FP16 (power-of-two scales)"}[args.precision],
+            "data": "synthetic (seeded layered + von Karman medium)",
             "config": wl,
             "roofline": {"bound": "hbm", "kernel": "stress3d_kernel (fused interior + PML stress update)",
                          "achieved": ach_stress, "peak": peak, "unit": "GB/s", "frac": ach_stress / peak,
@@ -578,6 +625,8 @@ def main():
             "gpu_launches": args.steps * (3 + 1 + 1),
             "clocks": clk.summary()}
     sim.close()
+    if rank == 0 and args.accuracy:
+        line["accuracy"] = accuracy_sample(p, args.precision, device)
     if rank == 0 and not args.no_cpu_baseline:
         v, n, sc, dt = cpu_reference(p, xi, 1000, 1, os.cpu_count() or 1, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",

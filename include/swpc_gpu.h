@@ -94,7 +94,17 @@ typedef struct swpc_desc {
     float dt;        /* time step [s]                                             */
     float tbeg;      /* start time [s]                                            */
     int device;      /* CUDA device ordinal                                       */
+    int precision;   /* SWPC_PREC_*: storage of stress and memory variables (3D)  */
 } swpc_desc;
+
+/* Storage precision of the 3D stress (S) and memory-variable (R) arrays; the
+ * arithmetic is FP32 in every form.  F32 is the reference's MP = SP build;
+ * BF16_R stores R in BF16; F16_SR stores S and R in FP16 with one
+ * power-of-two scale per array (see swpc_rescale).  Reduced-precision forms
+ * run the one-cell-per-thread kernels (swpc_set_launch kernels 0 and 1). */
+#define SWPC_PREC_F32 0
+#define SWPC_PREC_BF16_R 1
+#define SWPC_PREC_F16_SR 2
 
 /* Medium and integer maps as produced by medium__setup
  * (src/swpc_3d/m_medium.f90:36-467).  Float fields are 3D Fortran arrays
@@ -278,6 +288,15 @@ int swpc_download_field(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i
 int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
 /* Memory-variable and PML-auxiliary fields are defined only on their
  * regions; outside them download writes 0 and upload ignores the input. */
+
+/* SWPC_PREC_F16_SR only (a no-op otherwise): re-centre the power-of-two
+ * scale of every FP16 stress and memory-variable array so that its largest
+ * stored magnitude lies in [2^10, 2^11) whenever it has left [2^6, 2^12);
+ * that leaves 32x headroom below the FP16 overflow for growth until the next
+ * call.  Scaling by a power of two is exact.  Call it between steps, e.g.
+ * with every progress report; *changed (may be NULL) = arrays rescaled.
+ * Blocks.  No counterpart in the reference. */
+int swpc_rescale(swpc_ctx *ctx, int *changed);
 
 /* Device bytes held by the context. */
 long long swpc_device_bytes(const swpc_ctx *ctx);

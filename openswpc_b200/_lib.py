@@ -20,6 +20,8 @@ SWPC_ERR_STATE = 3
 SWPC_ERR_DIVERGED = 4
 SWPC_ERR_NOMEM = 5
 SWPC_ERR_LIMIT = 6
+PREC_F32, PREC_BF16_R, PREC_F16_SR = 0, 1, 2
+PRECISIONS = {"f32": PREC_F32, "bf16r": PREC_BF16_R, "f16sr": PREC_F16_SR}
 SWPC_NOALLOC_MAX_NY = 16384
 
 KIND_3D, KIND_PSV, KIND_SH = 3, 2, 1
@@ -39,7 +41,7 @@ EXPORTS = [
     "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
-    "swpc_download_field", "swpc_upload_field", "swpc_device_bytes", "swpc_set_launch",
+    "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
@@ -58,7 +60,7 @@ class SwpcError(RuntimeError):
 class Desc(C.Structure):
     _fields_ = [("kind", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("na", C.c_int),
                 ("nm", C.c_int), ("nt", C.c_int), ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
-                ("dt", C.c_float), ("tbeg", C.c_float), ("device", C.c_int)]
+                ("dt", C.c_float), ("tbeg", C.c_float), ("device", C.c_int), ("precision", C.c_int)]
 
 
 _FP = C.POINTER(C.c_float)
@@ -139,6 +141,7 @@ def load():
         "swpc_snap_fetch_max": (i, [vp, i, _FP]),
         "swpc_download_field": (i, [vp, i, _FP, i, i]),
         "swpc_upload_field": (i, [vp, i, _FP, i, i]),
+        "swpc_rescale": (i, [vp, _IP]),
         "swpc_device_bytes": (C.c_longlong, [vp]),
         "swpc_set_launch": (i, [vp, i, i, i, i]),
         "swpc_x2i": (i, [f, f, f]),

@@ -1,6 +1,9 @@
 // swpc3d_cell.cuh -- per-cell device routines shared by the 3D kernels.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "swpc_ctx.h"
 #include "swpc_kernels.cuh"
 
@@ -12,6 +15,43 @@ namespace swpc {
 __device__ __forceinline__ float lds(const float *p) { return __ldcs(p); }
 __device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
 
+// Storage precision of the stress (S) and memory-variable (R) arrays; the
+// arithmetic is FP32 in every form.
+//   PREC_F32   : S and R in FP32 (the reference's MP = SP build)
+//   PREC_BF16_R: R stored in BF16
+//   PREC_F16_SR: S and R stored in FP16, each array with its own power-of-two
+//                scale: value = stored * s, stored = value * (1 / s) (exact)
+enum { PREC_F32 = 0, PREC_BF16_R = 1, PREC_F16_SR = 2 };
+
+template <int PREC>
+__device__ __forceinline__ float ldS(const float *p, long long e, float s) {
+    if constexpr (PREC == PREC_F16_SR) return __half2float(__ldcs(reinterpret_cast<const __half *>(p) + e)) * s;
+    else return __ldcs(p + e);
+}
+template <int PREC>
+__device__ __forceinline__ float ldgS(const float *p, long long e, float s) {
+    if constexpr (PREC == PREC_F16_SR) return __half2float(__ldg(reinterpret_cast<const __half *>(p) + e)) * s;
+    else return __ldg(p + e);
+}
+template <int PREC>
+__device__ __forceinline__ void stS(float *p, long long e, float v, float is) {
+    if constexpr (PREC == PREC_F16_SR) __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
+    else __stcs(p + e, v);
+}
+template <int PREC>
+__device__ __forceinline__ float ldR(const float *p, long long e, float s) {
+    if constexpr (PREC == PREC_F16_SR) return __half2float(__ldcs(reinterpret_cast<const __half *>(p) + e)) * s;
+    else if constexpr (PREC == PREC_BF16_R)
+        return __bfloat162float(__ldcs(reinterpret_cast<const __nv_bfloat16 *>(p) + e));
+    else return __ldcs(p + e);
+}
+template <int PREC>
+__device__ __forceinline__ void stR(float *p, long long e, float v, float is) {
+    if constexpr (PREC == PREC_F16_SR) __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
+    else if constexpr (PREC == PREC_BF16_R) __stcs(reinterpret_cast<__nv_bfloat16 *>(p) + e, __float2bfloat16_rn(v));
+    else __stcs(p + e, v);
+}
+
 // ---------------------------------------------------------------------------
 // velocity: kernel__update_vel (m_kernel.f90:75-140) +
 //           absorb_p__update_vel (m_absorb_p.f90:248-309)
@@ -20,6 +60,7 @@ __device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
 // issued before its first store: the arrays never alias, and with every
 // operand in flight at once the update is limited by HBM bandwidth instead of
 // by load latency.
+template <int PREC>
 __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j) {
     const Geo g = a.g;
     const long long col = col_index(g, i, j);
@@ -41,18 +82,18 @@ __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j)
         if (!(a.mask & 1)) return;
         const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
         const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
-        const float xx0 = __ldg(&Sxx[e]), xxp = __ldg(&Sxx[e + PI]), xxp2 = __ldg(&Sxx[e + 2 * PI]), xxm = __ldg(&Sxx[e - PI]);
-        const float yy0 = __ldg(&Syy[e]), yyp = __ldg(&Syy[e + PJ]), yyp2 = __ldg(&Syy[e + 2 * PJ]), yym = __ldg(&Syy[e - PJ]);
-        const float zz0 = __ldg(&Szz[e]), zzp = __ldg(&Szz[e + 1]), zzp2 = __ldg(&Szz[e + 2]), zzm = __ldg(&Szz[e - 1]);
-        const float xy0 = __ldg(&Sxy[e]);
-        const float xyjm = __ldg(&Sxy[e - PJ]), xyjp = __ldg(&Sxy[e + PJ]), xyjm2 = __ldg(&Sxy[e - 2 * PJ]);
-        const float xyim = __ldg(&Sxy[e - PI]), xyip = __ldg(&Sxy[e + PI]), xyim2 = __ldg(&Sxy[e - 2 * PI]);
-        const float xz0 = __ldg(&Sxz[e]);
-        const float xzkm = __ldg(&Sxz[e - 1]), xzkp = __ldg(&Sxz[e + 1]), xzkm2 = __ldg(&Sxz[e - 2]);
-        const float xzim = __ldg(&Sxz[e - PI]), xzip = __ldg(&Sxz[e + PI]), xzim2 = __ldg(&Sxz[e - 2 * PI]);
-        const float yz0 = __ldg(&Syz[e]);
-        const float yzkm = __ldg(&Syz[e - 1]), yzkp = __ldg(&Syz[e + 1]), yzkm2 = __ldg(&Syz[e - 2]);
-        const float yzjm = __ldg(&Syz[e - PJ]), yzjp = __ldg(&Syz[e + PJ]), yzjm2 = __ldg(&Syz[e - 2 * PJ]);
+        const float xx0 = ldgS<PREC>(Sxx, e, a.sS[0]), xxp = ldgS<PREC>(Sxx, e + PI, a.sS[0]), xxp2 = ldgS<PREC>(Sxx, e + 2 * PI, a.sS[0]), xxm = ldgS<PREC>(Sxx, e - PI, a.sS[0]);
+        const float yy0 = ldgS<PREC>(Syy, e, a.sS[1]), yyp = ldgS<PREC>(Syy, e + PJ, a.sS[1]), yyp2 = ldgS<PREC>(Syy, e + 2 * PJ, a.sS[1]), yym = ldgS<PREC>(Syy, e - PJ, a.sS[1]);
+        const float zz0 = ldgS<PREC>(Szz, e, a.sS[2]), zzp = ldgS<PREC>(Szz, e + 1, a.sS[2]), zzp2 = ldgS<PREC>(Szz, e + 2, a.sS[2]), zzm = ldgS<PREC>(Szz, e - 1, a.sS[2]);
+        const float xy0 = ldgS<PREC>(Sxy, e, a.sS[5]);
+        const float xyjm = ldgS<PREC>(Sxy, e - PJ, a.sS[5]), xyjp = ldgS<PREC>(Sxy, e + PJ, a.sS[5]), xyjm2 = ldgS<PREC>(Sxy, e - 2 * PJ, a.sS[5]);
+        const float xyim = ldgS<PREC>(Sxy, e - PI, a.sS[5]), xyip = ldgS<PREC>(Sxy, e + PI, a.sS[5]), xyim2 = ldgS<PREC>(Sxy, e - 2 * PI, a.sS[5]);
+        const float xz0 = ldgS<PREC>(Sxz, e, a.sS[4]);
+        const float xzkm = ldgS<PREC>(Sxz, e - 1, a.sS[4]), xzkp = ldgS<PREC>(Sxz, e + 1, a.sS[4]), xzkm2 = ldgS<PREC>(Sxz, e - 2, a.sS[4]);
+        const float xzim = ldgS<PREC>(Sxz, e - PI, a.sS[4]), xzip = ldgS<PREC>(Sxz, e + PI, a.sS[4]), xzim2 = ldgS<PREC>(Sxz, e - 2 * PI, a.sS[4]);
+        const float yz0 = ldgS<PREC>(Syz, e, a.sS[3]);
+        const float yzkm = ldgS<PREC>(Syz, e - 1, a.sS[3]), yzkp = ldgS<PREC>(Syz, e + 1, a.sS[3]), yzkm2 = ldgS<PREC>(Syz, e - 2, a.sS[3]);
+        const float yzjm = ldgS<PREC>(Syz, e - PJ, a.sS[3]), yzjp = ldgS<PREC>(Syz, e + PJ, a.sS[3]), yzjm2 = ldgS<PREC>(Syz, e - 2 * PJ, a.sS[3]);
         const int4 bd = __ldg(&a.band[col]);
         const int p1 = (k - bd.x) * (bd.y - k);
         const int p2 = (k - bd.z) * (bd.w - k);
@@ -94,12 +135,12 @@ __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j)
     const float vxSxz = lds(&axSxz[q]), vySyz = lds(&aySyz[q]), vzSzz = lds(&azSzz[q]);
     const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
     const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
-    const float xx0 = __ldg(&Sxx[e]), xxp = __ldg(&Sxx[e + PI]);
-    const float yy0 = __ldg(&Syy[e]), yyp = __ldg(&Syy[e + PJ]);
-    const float zz0 = __ldg(&Szz[e]), zzp = __ldg(&Szz[e + 1]);
-    const float yz0 = __ldg(&Syz[e]), yzjm = __ldg(&Syz[e - PJ]), yzkm = __ldg(&Syz[e - 1]);
-    const float xz0 = __ldg(&Sxz[e]), xzim = __ldg(&Sxz[e - PI]), xzkm = __ldg(&Sxz[e - 1]);
-    const float xy0 = __ldg(&Sxy[e]), xyim = __ldg(&Sxy[e - PI]), xyjm = __ldg(&Sxy[e - PJ]);
+    const float xx0 = ldgS<PREC>(Sxx, e, a.sS[0]), xxp = ldgS<PREC>(Sxx, e + PI, a.sS[0]);
+    const float yy0 = ldgS<PREC>(Syy, e, a.sS[1]), yyp = ldgS<PREC>(Syy, e + PJ, a.sS[1]);
+    const float zz0 = ldgS<PREC>(Szz, e, a.sS[2]), zzp = ldgS<PREC>(Szz, e + 1, a.sS[2]);
+    const float yz0 = ldgS<PREC>(Syz, e, a.sS[3]), yzjm = ldgS<PREC>(Syz, e - PJ, a.sS[3]), yzkm = ldgS<PREC>(Syz, e - 1, a.sS[3]);
+    const float xz0 = ldgS<PREC>(Sxz, e, a.sS[4]), xzim = ldgS<PREC>(Sxz, e - PI, a.sS[4]), xzkm = ldgS<PREC>(Sxz, e - 1, a.sS[4]);
+    const float xy0 = ldgS<PREC>(Sxy, e, a.sS[5]), xyim = ldgS<PREC>(Sxy, e - PI, a.sS[5]), xyjm = ldgS<PREC>(Sxy, e - PJ, a.sS[5]);
     const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
     const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
     const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);

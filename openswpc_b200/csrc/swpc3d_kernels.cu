@@ -15,6 +15,7 @@
 //
 // Thread mapping: a warp owns 32 consecutive k of one (i, j) column (one
 // coalesced 128-byte row per field); block = 32 x BI x BJ columns.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "swpc_ctx.h"
@@ -26,21 +27,21 @@ namespace swpc {
 // ---------------------------------------------------------------------------
 // velocity: one thread per cell (vel_cell in swpc3d_cell.cuh)
 // ---------------------------------------------------------------------------
-template <int MINB>
+template <int MINB, int PREC>
 __global__ void __launch_bounds__(256, MINB) vel3d_kernel(const Vel3Args a) {
     const Geo g = a.g;
     const int k = 1 + blockIdx.x * 32 + threadIdx.x;
     const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int j = 1 + blockIdx.z * blockDim.z + threadIdx.z;
     if (k > g.nz || i > g.nx || j > g.ny) return;
-    vel_cell(a, k, i, j);
+    vel_cell<PREC>(a, k, i, j);
 }
 
 // ---------------------------------------------------------------------------
 // stress: kernel__update_stress (m_kernel.f90:142-326) +
 //         absorb_p__update_stress (m_absorb_p.f90:424-503)
 // ---------------------------------------------------------------------------
-template <int NM, int MINB>
+template <int NM, int MINB, int PREC>
 __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const Geo g = a.g;
     const int k = 1 + blockIdx.x * 32 + threadIdx.x;
@@ -69,9 +70,9 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
 #pragma unroll
         for (int c = 0; c < 6; c++)
 #pragma unroll
-            for (int m = 0; m < NM; m++) r[c][m] = lds(&a.R[c * 3 + m][e]);
-        const float sxx = lds(&Sxx[e]), syy = lds(&Syy[e]), szz = lds(&Szz[e]);
-        const float syz = lds(&Syz[e]), sxz = lds(&Sxz[e]), sxy = lds(&Sxy[e]);
+            for (int m = 0; m < NM; m++) r[c][m] = ldR<PREC>(a.R[c * 3 + m], e, a.sR[c * 3 + m]);
+        const float sxx = ldS<PREC>(Sxx, e, a.sS[0]), syy = ldS<PREC>(Syy, e, a.sS[1]), szz = ldS<PREC>(Szz, e, a.sS[2]);
+        const float syz = ldS<PREC>(Syz, e, a.sS[3]), sxz = ldS<PREC>(Sxz, e, a.sS[4]), sxy = ldS<PREC>(Sxy, e, a.sS[5]);
         const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
         const float taup1 = lds(&a.taup[e]), taus1 = lds(&a.taus[e]);
         const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
@@ -115,9 +116,9 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
         }
         const float taup_plus1 = 1 + taup1 * (1 + a.d2);
         const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-        sts(&Sxx[e], sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt);
-        sts(&Syy[e], syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt);
-        sts(&Szz[e], szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt);
+        stS<PREC>(Sxx, e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, a.iS[0]);
+        stS<PREC>(Syy, e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, a.iS[1]);
+        stS<PREC>(Szz, e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, a.iS[2]);
 
         // shear components (m_kernel.f90:282-311)
         const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
@@ -136,13 +137,13 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
             Rxz_n = Rxz_n + a.d1[m] * r[4][m];
             Rxy_n = Rxy_n + a.d1[m] * r[5][m];
         }
-        sts(&Syz[e], syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt);
-        sts(&Sxz[e], sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt);
-        sts(&Sxy[e], sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt);
+        stS<PREC>(Syz, e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, a.iS[3]);
+        stS<PREC>(Sxz, e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, a.iS[4]);
+        stS<PREC>(Sxy, e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, a.iS[5]);
 #pragma unroll
         for (int c = 0; c < 6; c++)
 #pragma unroll
-            for (int m = 0; m < NM; m++) sts(&a.R[c * 3 + m][e], r[c][m]);
+            for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m], e, r[c][m], a.iR[c * 3 + m]);
         return;
     }
 
@@ -162,8 +163,8 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const float vaxVx = lds(&axVx[q]), vayVy = lds(&ayVy[q]), vazVz = lds(&azVz[q]);
     const float vayVx = lds(&ayVx[q]), vazVx = lds(&azVx[q]), vaxVy = lds(&axVy[q]);
     const float vazVy = lds(&azVy[q]), vaxVz = lds(&axVz[q]), vayVz = lds(&ayVz[q]);
-    const float sxx = lds(&Sxx[e]), syy = lds(&Syy[e]), szz = lds(&Szz[e]);
-    const float syz = lds(&Syz[e]), sxz = lds(&Sxz[e]), sxy = lds(&Sxy[e]);
+    const float sxx = ldS<PREC>(Sxx, e, a.sS[0]), syy = ldS<PREC>(Syy, e, a.sS[1]), szz = ldS<PREC>(Szz, e, a.sS[2]);
+    const float syz = ldS<PREC>(Syz, e, a.sS[3]), sxz = ldS<PREC>(Sxz, e, a.sS[4]), sxy = ldS<PREC>(Sxy, e, a.sS[5]);
     const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
     const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
     const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
@@ -184,9 +185,9 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
     const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
     const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
-    sts(&Sxx[e], sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt);
-    sts(&Syy[e], syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt);
-    sts(&Szz[e], szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt);
+    stS<PREC>(Sxx, e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, a.iS[0]);
+    stS<PREC>(Syy, e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, a.iS[1]);
+    stS<PREC>(Szz, e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, a.iS[2]);
     sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
     sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
     sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
@@ -197,9 +198,9 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const float dyVz = (vzjp - vz0) * r20y;
     const float dzVx = (vxkp - vx0) * r20z;
     const float dzVy = (vykp - vy0) * r20z;
-    sts(&Syz[e], syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt);
-    sts(&Sxz[e], sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt);
-    sts(&Sxy[e], sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt);
+    stS<PREC>(Syz, e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, a.iS[3]);
+    stS<PREC>(Sxz, e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, a.iS[4]);
+    stS<PREC>(Sxy, e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, a.iS[5]);
     sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
     sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
     sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
@@ -210,31 +211,47 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
 
 // MINB (minimum resident blocks per SM) trades registers for occupancy; the
 // launch table picks it per kernel (swpc_set_launch)
-void launch_vel3d(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st) {
+template <int PREC>
+static void vel_minb(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st) {
     switch (minb) {
-    case 1: vel3d_kernel<1><<<grid, block, 0, st>>>(a); break;
-    case 2: vel3d_kernel<2><<<grid, block, 0, st>>>(a); break;
-    case 3: vel3d_kernel<3><<<grid, block, 0, st>>>(a); break;
-    default: vel3d_kernel<4><<<grid, block, 0, st>>>(a); break;
+    case 1: vel3d_kernel<1, PREC><<<grid, block, 0, st>>>(a); break;
+    case 2: vel3d_kernel<2, PREC><<<grid, block, 0, st>>>(a); break;
+    case 3: vel3d_kernel<3, PREC><<<grid, block, 0, st>>>(a); break;
+    default: vel3d_kernel<4, PREC><<<grid, block, 0, st>>>(a); break;
     }
 }
 
-template <int NM>
+void launch_vel3d(const Vel3Args &a, int minb, int prec, dim3 grid, dim3 block, cudaStream_t st) {
+    // S is read in FP16 only by the PREC_F16_SR form; the others share the FP32 kernel
+    if (prec == PREC_F16_SR) vel_minb<PREC_F16_SR>(a, minb, grid, block, st);
+    else vel_minb<PREC_F32>(a, minb, grid, block, st);
+}
+
+template <int NM, int PREC>
 static void stress_minb(const Str3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st) {
     switch (minb) {
-    case 1: stress3d_kernel<NM, 1><<<grid, block, 0, st>>>(a); break;
-    case 2: stress3d_kernel<NM, 2><<<grid, block, 0, st>>>(a); break;
-    case 3: stress3d_kernel<NM, 3><<<grid, block, 0, st>>>(a); break;
-    default: stress3d_kernel<NM, 4><<<grid, block, 0, st>>>(a); break;
+    case 1: stress3d_kernel<NM, 1, PREC><<<grid, block, 0, st>>>(a); break;
+    case 2: stress3d_kernel<NM, 2, PREC><<<grid, block, 0, st>>>(a); break;
+    case 3: stress3d_kernel<NM, 3, PREC><<<grid, block, 0, st>>>(a); break;
+    default: stress3d_kernel<NM, 4, PREC><<<grid, block, 0, st>>>(a); break;
     }
 }
 
-void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st) {
+template <int PREC>
+static void stress_nm(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st) {
     switch (nm) {
-    case 0: stress_minb<0>(a, minb, grid, block, st); break;
-    case 1: stress_minb<1>(a, minb, grid, block, st); break;
-    case 2: stress_minb<2>(a, minb, grid, block, st); break;
-    default: stress_minb<3>(a, minb, grid, block, st); break;
+    case 0: stress_minb<0, PREC>(a, minb, grid, block, st); break;
+    case 1: stress_minb<1, PREC>(a, minb, grid, block, st); break;
+    case 2: stress_minb<2, PREC>(a, minb, grid, block, st); break;
+    default: stress_minb<3, PREC>(a, minb, grid, block, st); break;
+    }
+}
+
+void launch_stress3d(const Str3Args &a, int nm, int minb, int prec, dim3 grid, dim3 block, cudaStream_t st) {
+    switch (prec) {
+    case PREC_BF16_R: stress_nm<PREC_BF16_R>(a, nm, minb, grid, block, st); break;
+    case PREC_F16_SR: stress_nm<PREC_F16_SR>(a, nm, minb, grid, block, st); break;
+    default: stress_nm<PREC_F32>(a, nm, minb, grid, block, st); break;
     }
 }
 
@@ -244,9 +261,23 @@ void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block,
 // Entries are applied in list order; when no two entries touch the same
 // cell the host marks the list parallel and each entry gets a thread.
 // ---------------------------------------------------------------------------
+// S -= coef * sdrop / div on an FP16 stress array (SWPC_PREC_F16_SR)
+__device__ __forceinline__ void glut_half(const InjArgs &a, const InjEntry &en, float sdrop, int div) {
+    __half *h = reinterpret_cast<__half *>(a.fields[en.field]);
+    const int c = en.field - SWPC_F_SXX;
+    const float v = __half2float(h[en.cell]) * a.sS[c];
+    const float w = div == 1 ? v - en.coef * sdrop : v - en.coef * sdrop / div;
+    h[en.cell] = __float2half_rn(w * a.iS[c]);
+}
+
 __device__ __forceinline__ void apply_entry(const InjArgs &a, const InjEntry &en, int it) {
     float *f = a.fields[en.field];
     const float st = a.stime[(long long)(it - 1) * a.nsrc + en.src];
+    if (a.s_half && en.field >= SWPC_F_SXX && en.mode <= INJ_GLUT2) {
+        const float sdrop = a.mo[en.src] * st * a.dt_dxyz;
+        glut_half(a, en, sdrop, en.mode == INJ_GLUT ? 1 : (en.mode == INJ_GLUT4 ? 4 : 2));
+        return;
+    }
     switch (en.mode) {
     case INJ_GLUT: {        // S -= m * sdrop, sdrop = mo * stime * dt_dxyz
         const float sdrop = a.mo[en.src] * st * a.dt_dxyz;
@@ -410,6 +441,21 @@ __global__ void wav3d_kernel(const Wav3Args a) {
     }
     if (a.what & SWPC_WAV_STRESS) {
         float *w = a.wav_s + (long long)n * 6 * ntw + (itw - 1);
+        if (a.s_half) {
+            // FP16 stress arrays: the same expressions on the scaled values
+            auto S = [&](const float *p, int c, long long q) {
+                return __half2float(reinterpret_cast<const __half *>(p)[q]) * a.sS[c];
+            };
+            w[0 * ntw] = S(a.Sxx, 0, e) * M0 * UC * 1e6f;
+            w[1 * ntw] = S(a.Syy, 1, e) * M0 * UC * 1e6f;
+            w[2 * ntw] = S(a.Szz, 2, e) * M0 * UC * 1e6f;
+            w[3 * ntw] = (S(a.Syz, 3, e) + S(a.Syz, 3, e - PJ) + S(a.Syz, 3, e - 1) + S(a.Syz, 3, e - 1 - PJ)) / 4.0f
+                         * M0 * UC * 1e6f;
+            w[4 * ntw] = (S(a.Sxz, 4, e) + S(a.Sxz, 4, e - PI) + S(a.Sxz, 4, e - 1) + S(a.Sxz, 4, e - 1 - PI)) / 4.0f
+                         * M0 * UC * 1e6f;
+            w[5 * ntw] = (S(a.Sxy, 5, e) + S(a.Sxy, 5, e - PJ) + S(a.Sxy, 5, e - PI) + S(a.Sxy, 5, e - PI - PJ)) / 4.0f
+                         * M0 * UC * 1e6f;
+        } else {
         const float *Sxx = a.Sxx, *Syy = a.Syy, *Szz = a.Szz, *Syz = a.Syz, *Sxz = a.Sxz, *Sxy = a.Sxy;
         w[0 * ntw] = Sxx[e] * M0 * UC * 1e6f;
         w[1 * ntw] = Syy[e] * M0 * UC * 1e6f;
@@ -417,6 +463,7 @@ __global__ void wav3d_kernel(const Wav3Args a) {
         w[3 * ntw] = (Syz[e] + Syz[e - PJ] + Syz[e - 1] + Syz[e - 1 - PJ]) / 4.0f * M0 * UC * 1e6f;
         w[4 * ntw] = (Sxz[e] + Sxz[e - PI] + Sxz[e - 1] + Sxz[e - 1 - PI]) / 4.0f * M0 * UC * 1e6f;
         w[5 * ntw] = (Sxy[e] + Sxy[e - PJ] + Sxy[e - PI] + Sxy[e - PI - PJ]) / 4.0f * M0 * UC * 1e6f;
+        }
     }
     if (a.what & SWPC_WAV_STRAIN) {
         float *w = a.wav_e + (long long)n * 6 * ntw + (itw - 1);

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(256, MINB) vel3d_vec_kernel(const Vel3Args a) 
 #pragma unroll 1
     for (int c = 0; c < 4; c++) {
         const int k = k0 + c;
-        if (k <= g.nz) vel_cell(a, k, i, j);
+        if (k <= g.nz) vel_cell<PREC_F32>(a, k, i, j);
     }
 }
 

@@ -96,6 +96,10 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     if (d->na < 0 || 2 * d->na >= d->nx || d->na >= d->nz || (d->kind == SWPC_KIND_3D && 2 * d->na >= d->ny))
         return fail(set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid"));
     if (d->nt < 1) return fail(set_err(c, SWPC_ERR_ARG, "nt must be positive"));
+    if (d->precision < SWPC_PREC_F32 || d->precision > SWPC_PREC_F16_SR ||
+        (d->kind != SWPC_KIND_3D && d->precision != SWPC_PREC_F32))
+        return fail(set_err(c, SWPC_ERR_ARG, "precision must be SWPC_PREC_F32/BF16_R/F16_SR (3D) or SWPC_PREC_F32"));
+    c->prec = d->precision;
     if (!(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0) || (d->kind == SWPC_KIND_3D && !(d->dy > 0)))
         return fail(set_err(c, SWPC_ERR_ARG, "dx, dy, dz, dt must be positive"));
     {
@@ -122,9 +126,12 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     int rc = 0;
     if (is3d(c)) {
         for (int q = 0; q < 3 && !rc; q++) rc = dalloc(c, &c->V[q], g.ncell);
-        for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, &c->S[q], g.ncell);
+        // 2-byte storage (FP16 / BF16) takes half the floats
+        const long long nS = c->prec == SWPC_PREC_F16_SR ? (g.ncell + 1) / 2 : g.ncell;
+        const long long nR = c->prec != SWPC_PREC_F32 ? (g.ncell + 1) / 2 : g.ncell;
+        for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, &c->S[q], nS);
         for (int comp = 0; comp < 6 && !rc; comp++)
-            for (int m = 0; m < d->nm && !rc; m++) rc = dalloc(c, &c->R[comp * 3 + m], g.ncell);
+            for (int m = 0; m < d->nm && !rc; m++) rc = dalloc(c, &c->R[comp * 3 + m], nR);
         for (int q = 1; q < 11 && !rc; q++) rc = dalloc(c, &c->med[q], g.ncell);
         const long long ncol = (long long)g.Ip * g.Jp;
         if (!rc) rc = dalloc(c, &c->band, ncol);
@@ -178,6 +185,8 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
     if (kernel < 0 || kernel > 4 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
         ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
         return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..4, minb 1..4, 32*bi*bj <= 256)");
+    if (kernel >= 2 && c->prec != SWPC_PREC_F32)
+        return set_err(c, SWPC_ERR_ARG, "reduced-precision storage runs the kernels 0 and 1 only");
     invalidate_graph(c);
     switch (kernel) {
     case 0: c->stress_march = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
@@ -689,10 +698,13 @@ static int launch_stress(swpc_ctx *c, int mask) {
     a.d2 = c->d2;
     a.dt = c->d.dt;
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
+    for (int q = 0; q < 6; q++) { a.sS[q] = ldexpf(1.0f, c->eS[q]); a.iS[q] = ldexpf(1.0f, -c->eS[q]); }
+    for (int q = 0; q < 18; q++) { a.sR[q] = ldexpf(1.0f, c->eR[q]); a.iR[q] = ldexpf(1.0f, -c->eR[q]); }
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
-    if (c->stress_march) launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
-    else launch_stress3d(a, c->d.nm, c->stress_minb, grid, block, c->stream);
+    if (c->stress_march && c->prec == SWPC_PREC_F32)
+        launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
+    else launch_stress3d(a, c->d.nm, c->stress_minb, c->prec, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "stress3d launch");
 }
 
@@ -713,15 +725,19 @@ static int launch_vel(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0) ? mask : (mask & 1);
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
-    if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);
+    for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
+    if (c->prec != SWPC_PREC_F32) launch_vel3d(a, c->vel_minb, c->prec, grid, block, c->stream);
+    else if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);
     else if (c->vel_march) launch_vel3d_march(a, c->vel_mminb, c->vel_jc, c->stream);
-    else launch_vel3d(a, c->vel_minb, grid, block, c->stream);
+    else launch_vel3d(a, c->vel_minb, SWPC_PREC_F32, grid, block, c->stream);
     return cuda_check(c, cudaGetLastError(), "vel3d launch");
 }
 
 static void fill_inj_fields(swpc_ctx *c, InjArgs &a) {
     for (int q = 0; q < 3; q++) a.fields[q] = c->V[q];
     for (int q = 0; q < 6; q++) a.fields[3 + q] = c->S[q];
+    a.s_half = c->prec == SWPC_PREC_F16_SR;
+    for (int q = 0; q < 6; q++) { a.sS[q] = ldexpf(1.0f, c->eS[q]); a.iS[q] = ldexpf(1.0f, -c->eS[q]); }
     if (is3d(c)) { a.bfields[0] = c->med[5]; a.bfields[1] = c->med[6]; a.bfields[2] = c->med[7]; }
     else { a.bfields[0] = c->med[0]; a.bfields[1] = c->med[0]; a.bfields[2] = c->med[0]; }
 }
@@ -786,6 +802,8 @@ static int launch_wav(swpc_ctx *c, int it, const int *d_it) {
     a.wav_v = c->wav[0]; a.wav_u = c->wav[1]; a.wav_s = c->wav[2]; a.wav_e = c->wav[3];
     a.M0 = c->M0; a.UC = c->UC; a.dt = c->d.dt;
     memcpy(a.r40, c->r40, sizeof(a.r40)); memcpy(a.r41, c->r41, sizeof(a.r41));
+    a.s_half = c->prec == SWPC_PREC_F16_SR;
+    for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
     // outside sampling steps the kernel only integrates u / strain
     if (!d_it && (it - 1) % c->ntdec_w != 0 && !(c->wav_what & (SWPC_WAV_U | SWPC_WAV_STRAIN))) return SWPC_OK;
     launch_wav3d(a, c->stream);
@@ -987,6 +1005,15 @@ extern "C" int swpc_download_field(swpc_ctx *c, int field, float *out, int ld_k,
     if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) return aux_transfer(c, field - SWPC_F_AUX, out, nullptr, ld_k, ld_i);
     float *p = field_ptr(c, field);
     if (!p) return set_err(c, SWPC_ERR_ARG, "unknown or unallocated field id");
+    if (field_storage(c, field) != 0) {
+        // reduced-precision storage: widen to FP32 on the device first
+        float *tmp = nullptr;
+        int rc = prec_to_f32(c, field, p, &tmp);
+        if (!rc) rc = copy_box(c, tmp, nullptr, out, ld_k, ld_i);
+        cudaStreamSynchronize(c->stream);
+        if (tmp) cudaFree(tmp);
+        return rc;
+    }
     return copy_box(c, p, nullptr, out, ld_k, ld_i);
 }
 
@@ -997,5 +1024,15 @@ extern "C" int swpc_upload_field(swpc_ctx *c, int field, const float *in, int ld
     if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) return aux_transfer(c, field - SWPC_F_AUX, nullptr, in, ld_k, ld_i);
     float *p = field_ptr(c, field);
     if (!p) return set_err(c, SWPC_ERR_ARG, "unknown or unallocated field id");
+    if (field_storage(c, field) != 0) {
+        // reduced-precision storage: round the FP32 upload on the device
+        float *tmp = nullptr;
+        int rc = prec_to_f32(c, field, p, &tmp);   // keeps the cells outside the box
+        if (!rc) rc = copy_box(c, tmp, in, nullptr, ld_k, ld_i);
+        if (!rc) rc = prec_from_f32(c, field, tmp, p);
+        cudaStreamSynchronize(c->stream);
+        if (tmp) cudaFree(tmp);
+        return rc;
+    }
     return copy_box(c, p, in, nullptr, ld_k, ld_i);
 }

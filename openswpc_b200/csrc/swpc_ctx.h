@@ -62,6 +62,9 @@ struct swpc_ctx {
     int kind;
     swpc::Geo g;
     swpc_desc d;
+    int prec = SWPC_PREC_F32;   // storage of S and R (3D)
+    int eS[6] = {0, 0, 0, 0, 0, 0};   // FP16 scale exponents: value = stored * 2^e
+    int eR[18] = {0};
     int device;
     cudaStream_t stream;
     std::string err;
@@ -160,6 +163,10 @@ namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
 int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
+int field_storage(const swpc_ctx *c, int field);   // swpc_prec.cu
+float field_scale(const swpc_ctx *c, int field);
+int prec_to_f32(swpc_ctx *c, int field, const float *stored, float **tmp);
+int prec_from_f32(swpc_ctx *c, int field, const float *tmp, float *stored);
 int cuda_check(swpc_ctx *c, cudaError_t e, const char *what);
 template <typename T>
 int dalloc(swpc_ctx *c, T **p, size_t n) {

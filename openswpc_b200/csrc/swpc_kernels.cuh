@@ -23,6 +23,7 @@ struct Vel3Args {
     float r20[3];
     float dt;
     int mask;       // bit 0: interior cells, bit 1: absorber cells
+    float sS[6];    // stored -> value scale of the FP16 stress arrays (PREC_F16_SR)
 };
 
 struct Str3Args {
@@ -41,6 +42,8 @@ struct Str3Args {
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     float dt;
     int mask;
+    float sS[6], iS[6];     // FP16 stress scales (value = stored * sS, stored = value * iS)
+    float sR[18], iR[18];   // FP16 memory-variable scales
 };
 
 struct InjArgs {
@@ -57,6 +60,8 @@ struct InjArgs {
     float *fields[9];    // V (0..2) and S (3..8) by SWPC_F_* id
     const float *bfields[3];
     const long long *rho_cell;   // (nsrc) density cell of 2D body forces
+    int s_half;          // S stored in FP16 (SWPC_PREC_F16_SR)
+    float sS[6], iS[6];  // its scales: value = stored * sS
 };
 
 struct Wav3Args {
@@ -71,6 +76,8 @@ struct Wav3Args {
     float *wav_v, *wav_u, *wav_s, *wav_e;
     float M0, UC, dt;
     float r40[3], r41[3];
+    int s_half;          // S stored in FP16 (SWPC_PREC_F16_SR)
+    float sS[6];
 };
 
 struct VmaxArgs {
@@ -81,8 +88,8 @@ struct VmaxArgs {
     unsigned int *out;
 };
 
-void launch_vel3d(const Vel3Args &a, int minb, dim3 grid, dim3 block, cudaStream_t st);
-void launch_stress3d(const Str3Args &a, int nm, int minb, dim3 grid, dim3 block, cudaStream_t st);
+void launch_vel3d(const Vel3Args &a, int minb, int prec, dim3 grid, dim3 block, cudaStream_t st);
+void launch_stress3d(const Str3Args &a, int nm, int minb, int prec, dim3 grid, dim3 block, cudaStream_t st);
 void launch_stress3d_march(const Str3Args &a, int nm, int minb, int jc, cudaStream_t st);
 void launch_vel3d_march(const Vel3Args &a, int minb, int jc, cudaStream_t st);
 void launch_vel3d_vec(const Vel3Args &a, int minb, dim3 block, cudaStream_t st);

@@ -182,13 +182,20 @@ class Medium:
 class Swpc3D:
     """One 3D run on one GPU (the single-node case of the reference)."""
 
-    def __init__(self, p: Params, xi: np.ndarray | None = None, device: int = 0, medium: Medium | None = None):
+    def __init__(self, p: Params, xi: np.ndarray | None = None, device: int = 0, medium: Medium | None = None,
+                 precision: str = "f32"):
+        """``precision`` is the storage of stress and memory variables:
+        "f32" (the reference's MP = SP build), "bf16r" (memory variables in
+        BF16) or "f16sr" (stress and memory variables in FP16 with per-array
+        power-of-two scales); the arithmetic is FP32 in every form."""
         p.check()
         self.p = p
+        self.precision = precision
         self.lib = _lib.load()
         self.medium = medium if medium is not None else Medium(p, xi)
         m = self.medium
-        desc = _lib.Desc(_lib.KIND_3D, p.nx, p.ny, p.nz, p.na, p.nm, p.nt, p.dx, p.dy, p.dz, p.dt, p.tbeg, device)
+        desc = _lib.Desc(_lib.KIND_3D, p.nx, p.ny, p.nz, p.na, p.nm, p.nt, p.dx, p.dy, p.dz, p.dt, p.tbeg, device,
+                         _lib.PRECISIONS[precision])
         ctx = C.c_void_p()
         rc = self.lib.swpc_create(C.byref(desc), C.byref(ctx))
         self.ctx = ctx
@@ -366,6 +373,8 @@ class Swpc3D:
         it = it0
         while it <= last:
             if it % p.ntdec_r == 0:
+                if self.precision == "f16sr":
+                    self.rescale()
                 vm = self.kernel__vmax()
                 va = vm * f32(self.UC) * f32(self.M0)
                 reports.append((it, va))
@@ -382,6 +391,13 @@ class Swpc3D:
         ms = C.c_float()
         check(self.ctx, self.lib.swpc_time_steps(self.ctx, it0, nsteps, C.byref(ms)))
         return ms.value
+
+    def rescale(self) -> int:
+        """Re-centre the FP16 array scales (precision "f16sr"); returns the
+        number of arrays rescaled."""
+        n = C.c_int()
+        check(self.ctx, self.lib.swpc_rescale(self.ctx, C.byref(n)))
+        return n.value
 
     def sync(self):
         check(self.ctx, self.lib.swpc_sync(self.ctx))

@@ -1,0 +1,87 @@
+"""Reduced-precision storage forms of the 3D step (BF16 memory variables;
+FP16 stress and memory variables with per-array power-of-two scales).  The
+arithmetic stays FP32, so each form is checked against the FP32 form and
+against the all-double oracle with a stated tolerance, and the error is
+recorded."""
+import numpy as np
+import pytest
+
+from openswpc_b200 import _lib
+from openswpc_b200.swpc3d import Swpc3D
+from oracle.oracle import Oracle3D
+from tests.models import small3d, vonkarman_xi
+
+pytestmark = pytest.mark.gpu
+
+# rel-L2 bars of the reduced forms against the f64 oracle after 80 steps:
+# BF16 keeps 8 significand bits (2^-9 relative rounding) for R, FP16 keeps 11
+# (2^-12) for S and R; both stay far below 1e-2 on this case
+TOL = {"f32": 1e-5, "bf16r": 1e-2, "f16sr": 1e-2}
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def reference():
+    p = small3d(nt=80, sw_wav_stress=True)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    o = Oracle3D(p, xi, variant="f64")
+    o.run(1, p.nt)
+    return p, xi, o
+
+
+@pytest.mark.parametrize("form", ["f32", "bf16r", "f16sr"])
+def test_precision_form_error_against_f64(form, reference, record_property):
+    p, xi, o = reference
+    g = Swpc3D(p, xi, precision=form)
+    g.run(1, p.nt)
+    errs = {"traces_v": rel_l2(g.waveforms(_lib.WAV_V), o.waveforms("v")),
+            "traces_stress": rel_l2(g.waveforms(_lib.WAV_STRESS), o.waveforms("stress"))}
+    for n, name in enumerate(("Vx", "Vy", "Vz")):
+        errs[name] = rel_l2(g.download(n), o.array(name))
+    for k, v in errs.items():
+        record_property(f"{form}_rel_l2_vs_f64_{k}", v)
+    print(form, "rel-L2 against the f64 oracle:", errs)
+    assert all(v < TOL[form] for v in errs.values()), errs
+    if form != "f32":
+        # the reduced form differs from FP32 (it really stores fewer bits)
+        f = Swpc3D(p, xi)
+        f.run(1, p.nt)
+        assert rel_l2(g.download(0), f.download(0)) > 0
+
+
+def test_reduced_storage_roundtrip_and_rescale():
+    """Upload/download through FP16 storage rounds to FP16; rescaling by a
+    power of two keeps the stored values."""
+    p = small3d(nt=40)
+    g = Swpc3D(p, precision="f16sr")
+    g.run(1, 30)
+    before = [g.download(_lib.F_SXX + c) for c in range(6)]
+    r_before = g.download(_lib.F_R + 0)
+    n = g.rescale()
+    assert n > 0   # fresh arrays start at scale 1; the run moved them out of the window
+    after = [g.download(_lib.F_SXX + c) for c in range(6)]
+    for a, b in zip(before, after):
+        big = np.abs(a).max()
+        assert big > 0
+        # exact unless a value fell into the FP16 subnormal range
+        assert np.abs(a - b).max() <= big * 2.0 ** -20
+    assert np.abs(g.download(_lib.F_R + 0) - r_before).max() <= np.abs(r_before).max() * 2.0 ** -20
+    assert g.rescale() == 0   # now centred
+    # the run continues correctly after a rescale: same as without it
+    h = Swpc3D(p, precision="f16sr")
+    h.run(1, 30)
+    g.run(31, 10)
+    h.run(31, 10)
+    assert rel_l2(g.download(0), h.download(0)) < 1e-2
+    # upload of FP32 values rounds them to FP16 on the device
+    # values of the field's own magnitude, so that they fit its current scale
+    x = (np.random.default_rng(3).standard_normal(before[0].shape) * np.abs(before[0]).max()).astype(np.float32)
+    g.upload(_lib.F_SXX, x)
+    y = g.download(_lib.F_SXX)
+    inner = (slice(3, -3), slice(3, -3), slice(3, -3))
+    assert np.abs(y[inner] - x[inner]).max() <= np.abs(x).max() * 2.0 ** -10
