@@ -225,6 +225,31 @@ int swpc_vmax(swpc_ctx *ctx, float out[3]);
 int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const int *kob, int nx, int ny, int nz,
                       int na, int ld_k, int ld_i, float uc, void *stream, float out[3]);
 
+/* ---- adjoint and gradient (3D, FP32 storage) ---------------------------- */
+
+/* Discrete adjoint of the step: the exact transpose of update_stress +
+ * update_vel (interior, memory variables, ADE-CFS PML, free-surface band).
+ * No counterpart in the reference.  The adjoint state uses the field ids of
+ * swpc_upload_field (V, S, R, PML auxiliaries).
+ *   swpc_adj_reset        zero the adjoint state and the gradients
+ *   swpc_adj_step_linear  adjoint <- (one step)^T adjoint, sources off
+ *   swpc_adj_upload / _download  adjoint fields in the Fortran memory box
+ * swpc_gradient: misfit = 0.5 sum (v_syn - v_obs)^2 over the velocity traces
+ * (obs laid out as swpc_wav_fetch's SWPC_WAV_V buffer) of a run from rest over
+ * steps 1..nt, and its gradient with respect to the medium arrays of the
+ * kernel region.  It runs the forward with a checkpoint every `ckpt` steps,
+ * then per segment recomputes the forward from the checkpoint and steps the
+ * adjoint back through it, accumulating the gradient in FP64.  Device memory:
+ * nt/ckpt checkpoints of the state plus ckpt+1 copies of V and S.
+ * swpc_gradient_fetch: which = 0 lam, 1 mu, 2 muyz, 3 muxz, 4 muxy, 5 bx,
+ * 6 by, 7 bz; out = double array over the memory box. */
+int swpc_adj_reset(swpc_ctx *ctx);
+int swpc_adj_step_linear(swpc_ctx *ctx);
+int swpc_adj_upload(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
+int swpc_adj_download(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
+int swpc_gradient(swpc_ctx *ctx, const float *obs, int ckpt, double *misfit);
+int swpc_gradient_fetch(swpc_ctx *ctx, int which, double *out, int ld_k, int ld_i);
+
 /* ---- snapshots (3D) ------------------------------------------------------ */
 
 /* Snapshot planes of snap__setup (src/swpc_3d/m_snap.f90:95-322): a plane is

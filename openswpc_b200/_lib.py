@@ -41,6 +41,8 @@ EXPORTS = [
     "swpc_source_bodyforce", "swpc_green_source", "swpc_comm_stress", "swpc_comm_vel", "swpc_wav_store",
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
+    "swpc_adj_reset", "swpc_adj_step_linear", "swpc_adj_upload", "swpc_adj_download", "swpc_gradient",
+    "swpc_gradient_fetch",
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
@@ -142,6 +144,12 @@ def load():
         "swpc_download_field": (i, [vp, i, _FP, i, i]),
         "swpc_upload_field": (i, [vp, i, _FP, i, i]),
         "swpc_rescale": (i, [vp, _IP]),
+        "swpc_adj_reset": (i, [vp]),
+        "swpc_adj_step_linear": (i, [vp]),
+        "swpc_adj_upload": (i, [vp, i, _FP, i, i]),
+        "swpc_adj_download": (i, [vp, i, _FP, i, i]),
+        "swpc_gradient": (i, [vp, _FP, i, C.POINTER(C.c_double)]),
+        "swpc_gradient_fetch": (i, [vp, i, C.POINTER(C.c_double), i, i]),
         "swpc_device_bytes": (C.c_longlong, [vp]),
         "swpc_set_launch": (i, [vp, i, i, i, i]),
         "swpc_x2i": (i, [f, f, f]),

@@ -1,0 +1,709 @@
+// swpc_adjoint.cu -- discrete adjoint of the 3D viscoelastic step and the
+// gradient of an L2 velocity-waveform misfit with respect to the medium.
+//
+// The forward step (kernel__update_stress + absorb_p__update_stress, then
+// kernel__update_vel + absorb_p__update_vel; src/swpc_3d/m_kernel.f90:75-326,
+// src/swpc_3d/m_absorb_p.f90:126-505) is linear in the wavefield state
+// (V, S, R, PML auxiliaries).  This file applies its exact transpose, in the
+// reverse order, as two kinds of passes per half step:
+//   weights: per cell, the adjoint of that cell's own update -- memory
+//            variables and PML auxiliaries in place, and for each of the
+//            nine (field, axis) difference operators the two weights that
+//            multiply the 4th-order coefficient pair (2nd-order difference
+//            r20 and zero in absorber cells);
+//   gather:  per cell, the transposed stencil: every neighbour that read this
+//            cell adds its weight with the sign of the difference.
+// Receiver residuals enter as sources at the transposed recorder cells
+// (wav__store, src/swpc_3d/m_wav.f90:530-535).  The gradient imaging
+// condition pairs the adjoint with the forward derivatives of the same step
+// and accumulates in FP64; it is formed on the interior kernel region, whose
+// cells are the model parameters (absorber cells copy the medium of the
+// interior edge and are not parameters).  swpc_gradient runs the forward with
+// checkpoints every `ckpt` steps, then per segment recomputes the forward
+// from its checkpoint, keeping V and S of every step, and steps the adjoint
+// back through it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "swpc_ctx.h"
+#include "swpc_kernels.cuh"
+
+namespace swpc {
+int graph_invalidate(swpc_ctx *c);
+int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i);
+int aux_transfer_ptr(swpc_ctx *c, float *dev, float *out, const float *in, int ld_k, int ld_i);
+}  // namespace swpc
+
+using namespace swpc;
+
+// adjoint state of a context
+struct swpc_adj_state {
+    float *lV[3] = {}, *lS[6] = {}, *lR[18] = {}, *laux[18] = {};
+    float *w40[9] = {}, *w41[9] = {};    // difference-operator weights
+    double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz
+    float *res = nullptr;                // receiver residuals (nst, 3, ntw)
+    int ckpt = 0, nseg = 0;
+    float *ckpool = nullptr;             // checkpoints: V S R aux per segment
+    float *slots = nullptr;              // V and S after each step of a segment
+    size_t ck_floats = 0;
+    long long bytes = 0;
+};
+
+namespace {
+
+constexpr int kThreadsK = 32;
+
+struct AdjVelArgs {
+    Geo g;
+    int ibk, iek, jbk, jek, kek;
+    const float *lV[3];
+    const float *b[3];
+    const int4 *band;
+    const int2 *pmlcol;
+    float *laS[9];               // adjoint of the velocity-phase PML auxiliaries
+    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
+    float e40[3][2], e41[3][2], r20[3], dt;
+    float *w40[9], *w41[9];
+    const float *S[6];           // forward S after the stress update (gradient)
+    double *gb[3];               // gradient of bx, by, bz (null: none)
+};
+
+struct AdjStrArgs {
+    Geo g;
+    int ibk, iek, jbk, jek, kek, nm;
+    const float *lS[6];
+    float *lR[18];
+    const float *lam, *mu, *taup, *taus, *muyz, *muxz, *muxy;
+    const int4 *band;
+    const int2 *pmlcol;
+    float *laV[9];               // adjoint of the stress-phase PML auxiliaries
+    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
+    float e40[3][2], e41[3][2], r20[3], dt;
+    float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
+    float *w40[9], *w41[9];
+    const float *V[3];           // forward V before the stress update (gradient)
+    double *gm[5];               // gradient of lam, mu, muyz, muxz, muxy (null: none)
+};
+
+struct GatherArgs {
+    Geo g;
+    float *dst[6];
+    const float *w40[9], *w41[9];
+};
+
+__device__ __forceinline__ bool cell_of(const Geo &g, int &k, int &i, int &j) {
+    k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+    i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    j = 1 + blockIdx.z * blockDim.z + threadIdx.z;
+    return k <= g.nz && i <= g.nx && j <= g.ny;
+}
+
+// axis of the difference operator of stress-phase pair q (x 0, y 1, z 2)
+__device__ __forceinline__ int qaxis(int q) { return (q == 0 || q == 3 || q == 5) ? 0 : (q == 1 || q == 4 || q == 7) ? 1 : 2; }
+
+__device__ __forceinline__ int band_sign(const int4 bd, int k) {
+    const int p1 = (k - bd.x) * (bd.y - k);
+    const int p2 = (k - bd.z) * (bd.w - k);
+    return ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// transpose of the velocity update: weights
+// pairs p: 0 (Vx,Sxx,x) 1 (Vx,Sxy,y) 2 (Vx,Sxz,z) 3 (Vy,Sxy,x) 4 (Vy,Syy,y)
+//          5 (Vy,Syz,z) 6 (Vz,Sxz,x) 7 (Vz,Syz,y) 8 (Vz,Szz,z)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const float dt = a.dt;
+    const float l[3] = {a.lV[0][e], a.lV[1][e], a.lV[2][e]};
+    const float u[3] = {a.b[0][e] * dt * l[0], a.b[1][e] * dt * l[1], a.b[2][e] * dt * l[2]};
+    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
+        const int s = band_sign(__ldg(&a.band[col]), k);
+#pragma unroll
+        for (int p = 0; p < 9; p++) {
+            const int c = p / 3, ax = p % 3;
+            a.w40[p][e] = a.e40[ax][s] * u[c];
+            a.w41[p][e] = a.e41[ax][s] * u[c];
+        }
+        if (a.gb[0]) {
+            // d(Vx)/d(bx) = d3Sx3 * dt on the forward S after the stress update
+            const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+            const float *Sxx = a.S[0], *Syy = a.S[1], *Szz = a.S[2], *Syz = a.S[3], *Sxz = a.S[4], *Sxy = a.S[5];
+            const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
+            const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+            const float d3Sx3 = (Sxx[e + PI] - Sxx[e]) * re40x - (Sxx[e + 2 * PI] - Sxx[e - PI]) * re41x
+                              + (Sxy[e] - Sxy[e - PJ]) * re40y - (Sxy[e + PJ] - Sxy[e - 2 * PJ]) * re41y
+                              + (Sxz[e] - Sxz[e - 1]) * re40z - (Sxz[e + 1] - Sxz[e - 2]) * re41z;
+            const float d3Sy3 = (Sxy[e] - Sxy[e - PI]) * re40x - (Sxy[e + PI] - Sxy[e - 2 * PI]) * re41x
+                              + (Syy[e + PJ] - Syy[e]) * re40y - (Syy[e + 2 * PJ] - Syy[e - PJ]) * re41y
+                              + (Syz[e] - Syz[e - 1]) * re40z - (Syz[e + 1] - Syz[e - 2]) * re41z;
+            const float d3Sz3 = (Sxz[e] - Sxz[e - PI]) * re40x - (Sxz[e + PI] - Sxz[e - 2 * PI]) * re41x
+                              + (Syz[e] - Syz[e - PJ]) * re40y - (Syz[e + PJ] - Syz[e - 2 * PJ]) * re41y
+                              + (Szz[e + 1] - Szz[e]) * re40z - (Szz[e + 2] - Szz[e - 1]) * re41z;
+            a.gb[0][e] += (double)l[0] * d3Sx3 * dt;
+            a.gb[1][e] += (double)l[1] * d3Sy3 * dt;
+            a.gb[2][e] += (double)l[2] * d3Sz3 * dt;
+        }
+        return;
+    }
+    // absorber cell: V += b * (g.x * D + g.y * aux_old) * dt, aux = g.z * aux + g.w * D * dt
+    const int2 pc = __ldg(&a.pmlcol[col]);
+    const long long q = (long long)pc.y + (k - pc.x);
+    const float4 gp[9] = {__ldg(&a.gxe[i - 1]), __ldg(&a.gyc[j - 1]), __ldg(&a.gzc[k - 1]),
+                          __ldg(&a.gxc[i - 1]), __ldg(&a.gye[j - 1]), __ldg(&a.gzc[k - 1]),
+                          __ldg(&a.gxc[i - 1]), __ldg(&a.gyc[j - 1]), __ldg(&a.gze[k - 1])};
+#pragma unroll
+    for (int p = 0; p < 9; p++) {
+        const int c = p / 3, ax = p % 3;
+        const float la = a.laS[p][q];
+        const float lD = u[c] * gp[p].x + gp[p].w * dt * la;
+        a.laS[p][q] = gp[p].z * la + u[c] * gp[p].y;
+        a.w40[p][e] = a.r20[ax] * lD;
+        a.w41[p][e] = 0.0f;
+    }
+}
+
+// transpose of a forward difference (f[e+P] - f[e]) * A40 - (f[e+2P] - f[e-P]) * A41
+__device__ __forceinline__ float tfwd(const float *w40, const float *w41, long long f, long long P) {
+    return w40[f - P] - w40[f] - w41[f - 2 * P] + w41[f + P];
+}
+// transpose of a backward difference (f[e] - f[e-P]) * A40 - (f[e+P] - f[e-2P]) * A41
+__device__ __forceinline__ float tbwd(const float *w40, const float *w41, long long f, long long P) {
+    return w40[f] - w40[f + P] - w41[f - P] + w41[f + 2 * P];
+}
+
+// lambda_S += D_S^T weights (dst = lS: xx yy zz yz xz xy)
+__global__ void __launch_bounds__(128) adj_vel_gather_kernel(const GatherArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long f = cell_index(g, k, i, j);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    a.dst[0][f] += tfwd(a.w40[0], a.w41[0], f, PI);
+    a.dst[1][f] += tfwd(a.w40[4], a.w41[4], f, PJ);
+    a.dst[2][f] += tfwd(a.w40[8], a.w41[8], f, 1);
+    a.dst[3][f] += tbwd(a.w40[5], a.w41[5], f, 1) + tbwd(a.w40[7], a.w41[7], f, PJ);
+    a.dst[4][f] += tbwd(a.w40[2], a.w41[2], f, 1) + tbwd(a.w40[6], a.w41[6], f, PI);
+    a.dst[5][f] += tbwd(a.w40[1], a.w41[1], f, PJ) + tbwd(a.w40[3], a.w41[3], f, PI);
+}
+
+// ---------------------------------------------------------------------------
+// transpose of the stress update: weights
+// pairs q: 0 (Vx,x,bwd) 1 (Vy,y,bwd) 2 (Vz,z,bwd) 3 (Vy,x,fwd) 4 (Vx,y,fwd)
+//          5 (Vz,x,fwd) 6 (Vx,z,fwd) 7 (Vz,y,fwd) 8 (Vy,z,fwd)
+// ---------------------------------------------------------------------------
+template <int NM>
+__global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const float dt = a.dt;
+    float al[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) al[c] = a.lS[c][e] * dt;
+    const float mu = a.mu[e], lam = a.lam[e];
+    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
+        const int s = band_sign(__ldg(&a.band[col]), k);
+        const float taup1 = a.taup[e], taus1 = a.taus[e];
+        const float muc[3] = {a.muyz[e], a.muxz[e], a.muxy[e]};
+        const float mu2 = 2 * mu;
+        const float lam2mu = lam + mu2;
+        const float taup_plus1 = 1 + taup1 * (1 + a.d2);
+        const float taus_plus1 = 1 + taus1 * (1 + a.d2);
+        // memory variables: R' = c1 R - c2 F dt; S' = S + (G + sum d1 R') dt
+        float lF[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            lF[c] = 0.0f;
+#pragma unroll
+            for (int m = 0; m < NM; m++) {
+                const float L = a.lR[c * 3 + m][e] + a.d1[m] * al[c];
+                a.lR[c * 3 + m][e] = a.c1[m] * L;
+                lF[c] = lF[c] + L * (-a.c2[m] * dt);
+            }
+        }
+        // normal: G_c = lam2mu taup+ d3v3 - mu2 taus+ X_c, F_c likewise with taup, taus
+        float ld3 = 0.0f, lX[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            ld3 = ld3 + lam2mu * taup_plus1 * al[c] + lam2mu * taup1 * lF[c];
+            lX[c] = -(mu2 * taus_plus1 * al[c] + mu2 * taus1 * lF[c]);
+        }
+        float ld[9];
+        ld[0] = ld3 + lX[1] + lX[2];   // dxVx appears in X_yy and X_zz
+        ld[1] = ld3 + lX[0] + lX[2];
+        ld[2] = ld3 + lX[0] + lX[1];
+        // shear: G = mu_c taus+ D, F = mu_c taus D (c = yz xz xy)
+        const float lyz = muc[0] * taus_plus1 * al[3] + muc[0] * taus1 * lF[3];
+        const float lxz = muc[1] * taus_plus1 * al[4] + muc[1] * taus1 * lF[4];
+        const float lxy = muc[2] * taus_plus1 * al[5] + muc[2] * taus1 * lF[5];
+        ld[3] = lxy; ld[4] = lxy; ld[5] = lxz; ld[6] = lxz; ld[7] = lyz; ld[8] = lyz;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            a.w40[q][e] = a.e40[qaxis(q)][s] * ld[q];
+            a.w41[q][e] = a.e41[qaxis(q)][s] * ld[q];
+        }
+        if (a.gm[0]) {
+            // forward strain rates on V before the stress update
+            const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+            const float *Vx = a.V[0], *Vy = a.V[1], *Vz = a.V[2];
+            const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
+            const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+            const float dxVx = (Vx[e] - Vx[e - PI]) * re40x - (Vx[e + PI] - Vx[e - 2 * PI]) * re41x;
+            const float dyVy = (Vy[e] - Vy[e - PJ]) * re40y - (Vy[e + PJ] - Vy[e - 2 * PJ]) * re41y;
+            const float dzVz = (Vz[e] - Vz[e - 1]) * re40z - (Vz[e + 1] - Vz[e - 2]) * re41z;
+            const float sxy = (Vy[e + PI] - Vy[e]) * re40x - (Vy[e + 2 * PI] - Vy[e - PI]) * re41x
+                            + (Vx[e + PJ] - Vx[e]) * re40y - (Vx[e + 2 * PJ] - Vx[e - PJ]) * re41y;
+            const float sxz = (Vz[e + PI] - Vz[e]) * re40x - (Vz[e + 2 * PI] - Vz[e - PI]) * re41x
+                            + (Vx[e + 1] - Vx[e]) * re40z - (Vx[e + 2] - Vx[e - 1]) * re41z;
+            const float syz = (Vz[e + PJ] - Vz[e]) * re40y - (Vz[e + 2 * PJ] - Vz[e - PJ]) * re41y
+                            + (Vy[e + 1] - Vy[e]) * re40z - (Vy[e + 2] - Vy[e - 1]) * re41z;
+            const double d3 = (double)dxVx + dyVy + dzVz;
+            const double X[3] = {(double)dyVy + dzVz, (double)dxVx + dzVz, (double)dxVx + dyVy};
+            double glam = 0.0, gmu = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                glam += (double)al[c] * taup_plus1 * d3 + (double)lF[c] * taup1 * d3;
+                gmu += (double)al[c] * (2.0 * taup_plus1 * d3 - 2.0 * taus_plus1 * X[c])
+                     + (double)lF[c] * (2.0 * taup1 * d3 - 2.0 * taus1 * X[c]);
+            }
+            a.gm[0][e] += glam;
+            a.gm[1][e] += gmu;
+            a.gm[2][e] += ((double)al[3] * taus_plus1 + (double)lF[3] * taus1) * syz;
+            a.gm[3][e] += ((double)al[4] * taus_plus1 + (double)lF[4] * taus1) * sxz;
+            a.gm[4][e] += ((double)al[5] * taus_plus1 + (double)lF[5] * taus1) * sxy;
+        }
+        return;
+    }
+    // absorber cell (m_absorb_p.f90:445-491)
+    const int2 pc = __ldg(&a.pmlcol[col]);
+    const long long q = (long long)pc.y + (k - pc.x);
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float lam2mu_R = lam + 2 * mu;
+    const float lam_R = lam2mu_R - 2 * mu;
+    const float lA[3] = {lam2mu_R * al[0] + lam_R * (al[1] + al[2]), lam2mu_R * al[1] + lam_R * (al[0] + al[2]),
+                         lam2mu_R * al[2] + lam_R * (al[0] + al[1])};
+    float ld[9];
+    // normal: D_ade = g.x D + g.y aux, aux' = g.z aux + g.w D dt (aux axVx ayVy azVz = laV 0 4 8)
+    {
+        const float4 gg[3] = {gxc, gyc, gzc};
+        const int ia[3] = {0, 4, 8};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float la = a.laV[ia[c]][q];
+            ld[c] = gg[c].x * lA[c] + gg[c].w * dt * la;
+            a.laV[ia[c]][q] = gg[c].z * la + gg[c].y * lA[c];
+        }
+    }
+    // shear: S' = S + mu_c (g1.x D1 + g2.x D2 + g1.y aux1 + g2.y aux2) dt
+    {
+        const float byz = a.muyz[e] * dt * a.lS[3][e];
+        const float bxz = a.muxz[e] * dt * a.lS[4][e];
+        const float bxy = a.muxy[e] * dt * a.lS[5][e];
+        // (q, profile, aux index, beta): 3 dxVy gxe axVy; 4 dyVx gye ayVx; 5 dxVz gxe axVz;
+        // 6 dzVx gze azVx; 7 dyVz gye ayVz; 8 dzVy gze azVy
+        const float4 gg[6] = {gxe, gye, gxe, gze, gye, gze};
+        const int ia[6] = {3, 1, 6, 2, 7, 5};
+        const float bb[6] = {bxy, bxy, bxz, bxz, byz, byz};
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            const float la = a.laV[ia[n]][q];
+            ld[3 + n] = gg[n].x * bb[n] + gg[n].w * dt * la;
+            a.laV[ia[n]][q] = gg[n].z * la + gg[n].y * bb[n];
+        }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 9; qq++) {
+        a.w40[qq][e] = a.r20[qaxis(qq)] * ld[qq];
+        a.w41[qq][e] = 0.0f;
+    }
+}
+
+// lambda_V += D_V^T weights (dst = lV: x y z)
+__global__ void __launch_bounds__(128) adj_stress_gather_kernel(const GatherArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long f = cell_index(g, k, i, j);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    a.dst[0][f] += tbwd(a.w40[0], a.w41[0], f, PI) + tfwd(a.w40[4], a.w41[4], f, PJ) + tfwd(a.w40[6], a.w41[6], f, 1);
+    a.dst[1][f] += tbwd(a.w40[1], a.w41[1], f, PJ) + tfwd(a.w40[3], a.w41[3], f, PI) + tfwd(a.w40[8], a.w41[8], f, 1);
+    a.dst[2][f] += tbwd(a.w40[2], a.w41[2], f, 1) + tfwd(a.w40[5], a.w41[5], f, PI) + tfwd(a.w40[7], a.w41[7], f, PJ);
+}
+
+// transpose of the velocity recorder (m_wav.f90:530-535): residuals as sources
+__global__ void adj_source_kernel(Geo g, const int *st, int nst, int ntw, int itw, const float *res, float scale,
+                                  float *lVx, float *lVy, float *lVz) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nst) return;
+    const int i = st[3 * n], j = st[3 * n + 1], k = st[3 * n + 2];
+    const long long e = cell_index(g, k, i, j);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    const float rx = res[((long long)n * 3 + 0) * ntw + itw - 1] * scale;
+    const float ry = res[((long long)n * 3 + 1) * ntw + itw - 1] * scale;
+    const float rz = res[((long long)n * 3 + 2) * ntw + itw - 1] * scale;
+    atomicAdd(&lVx[e], rx);
+    atomicAdd(&lVx[e - PI], rx);
+    atomicAdd(&lVy[e], ry);
+    atomicAdd(&lVy[e - PJ], ry);
+    atomicAdd(&lVz[e], -rz);
+    atomicAdd(&lVz[e - 1], -rz);
+}
+
+__global__ void zero_double_kernel(double *p, long long n) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        p[q] = 0.0;
+}
+
+dim3 cell_grid(const Geo &g, dim3 block) {
+    return dim3((g.nz + kThreadsK - 1) / kThreadsK, (g.nx + block.y - 1) / block.y, (g.ny + block.z - 1) / block.z);
+}
+
+int err(swpc_ctx *c, int code, const char *m) { return set_err(c, code, m); }
+
+}  // namespace
+
+#define ACK(call)                                            \
+    do {                                                     \
+        int _rc = cuda_check(c, (call), #call);              \
+        if (_rc) return _rc;                                 \
+    } while (0)
+
+static int adj_alloc(swpc_ctx *c) {
+    if (c->adj) return SWPC_OK;
+    auto *s = new swpc_adj_state();
+    c->adj = s;
+    const long long n = c->g.ncell;
+    for (int q = 0; q < 3; q++) { int rc = dalloc(c, &s->lV[q], n); if (rc) return rc; }
+    for (int q = 0; q < 6; q++) { int rc = dalloc(c, &s->lS[q], n); if (rc) return rc; }
+    for (int comp = 0; comp < 6; comp++)
+        for (int m = 0; m < c->d.nm; m++) {
+            int rc = dalloc(c, &s->lR[comp * 3 + m], n);
+            if (rc) return rc;
+        }
+    if (c->npml > 0)
+        for (int q = 0; q < 18; q++) { int rc = dalloc(c, &s->laux[q], c->npml); if (rc) return rc; }
+    for (int q = 0; q < 9; q++) {
+        int rc = dalloc(c, &s->w40[q], n);
+        if (!rc) rc = dalloc(c, &s->w41[q], n);
+        if (rc) return rc;
+    }
+    for (int q = 0; q < 8; q++) { int rc = dalloc(c, &s->grad[q], n); if (rc) return rc; }
+    return SWPC_OK;
+}
+
+namespace swpc {
+void adj_free(swpc_ctx *c) {
+    swpc_adj_state *s = c->adj;
+    if (!s) return;
+    for (auto p : s->lV) if (p) cudaFree(p);
+    for (auto p : s->lS) if (p) cudaFree(p);
+    for (auto p : s->lR) if (p) cudaFree(p);
+    for (auto p : s->laux) if (p) cudaFree(p);
+    for (auto p : s->w40) if (p) cudaFree(p);
+    for (auto p : s->w41) if (p) cudaFree(p);
+    for (auto p : s->grad) if (p) cudaFree(p);
+    if (s->res) cudaFree(s->res);
+    if (s->ckpool) cudaFree(s->ckpool);
+    if (s->slots) cudaFree(s->slots);
+    delete s;
+    c->adj = nullptr;
+}
+}  // namespace swpc
+
+static int adj_ready(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "the adjoint is implemented for the 3D solver");
+    if (c->prec != SWPC_PREC_F32) return err(c, SWPC_ERR_ARG, "the adjoint needs FP32 storage");
+    if (!c->medium_ready || !c->kernel_ready || (c->d.na > 0 && !c->absorb_ready))
+        return err(c, SWPC_ERR_STATE, "medium, kernel and absorber setup must precede the adjoint");
+    ACK(cudaSetDevice(c->device));
+    return adj_alloc(c);
+}
+
+// one transposed step: vel^T then stress^T; with gradient when S_after / V_before are given
+static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const *V_before) {
+    swpc_adj_state *s = c->adj;
+    const dim3 block(kThreadsK, 2, 2);
+    const dim3 grid = cell_grid(c->g, block);
+    const bool grad = S_after != nullptr;
+    {
+        AdjVelArgs a;
+        memset(&a, 0, sizeof(a));
+        a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
+        for (int q = 0; q < 3; q++) { a.lV[q] = s->lV[q]; a.b[q] = c->med[5 + q]; }
+        a.band = c->band; a.pmlcol = c->pmlcol;
+        for (int q = 0; q < 9; q++) a.laS[q] = s->laux[9 + q];
+        a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+        memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+        a.dt = c->d.dt;
+        for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
+        if (grad) {
+            for (int q = 0; q < 6; q++) a.S[q] = S_after[q];
+            for (int q = 0; q < 3; q++) a.gb[q] = s->grad[5 + q];
+        }
+        adj_vel_weights_kernel<<<grid, block, 0, c->stream>>>(a);
+        ACK(cudaGetLastError());
+        GatherArgs ga;
+        ga.g = c->g;
+        for (int q = 0; q < 6; q++) ga.dst[q] = s->lS[q];
+        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
+        adj_vel_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
+        ACK(cudaGetLastError());
+    }
+    {
+        AdjStrArgs a;
+        memset(&a, 0, sizeof(a));
+        a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek; a.nm = c->d.nm;
+        for (int q = 0; q < 6; q++) a.lS[q] = s->lS[q];
+        for (int q = 0; q < 18; q++) a.lR[q] = s->lR[q];
+        a.lam = c->med[1]; a.mu = c->med[2]; a.taup = c->med[3]; a.taus = c->med[4];
+        a.muyz = c->med[8]; a.muxz = c->med[9]; a.muxy = c->med[10];
+        a.band = c->band; a.pmlcol = c->pmlcol;
+        for (int q = 0; q < 9; q++) a.laV[q] = s->laux[q];
+        a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+        memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+        a.dt = c->d.dt;
+        memcpy(a.c1, c->c1, sizeof(a.c1)); memcpy(a.c2, c->c2, sizeof(a.c2)); memcpy(a.d1, c->d1, sizeof(a.d1));
+        a.d2 = c->d2;
+        for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
+        if (grad) {
+            for (int q = 0; q < 3; q++) a.V[q] = V_before[q];
+            for (int q = 0; q < 5; q++) a.gm[q] = s->grad[q];
+        }
+        switch (c->d.nm) {
+        case 0: adj_stress_weights_kernel<0><<<grid, block, 0, c->stream>>>(a); break;
+        case 1: adj_stress_weights_kernel<1><<<grid, block, 0, c->stream>>>(a); break;
+        case 2: adj_stress_weights_kernel<2><<<grid, block, 0, c->stream>>>(a); break;
+        default: adj_stress_weights_kernel<3><<<grid, block, 0, c->stream>>>(a); break;
+        }
+        ACK(cudaGetLastError());
+        GatherArgs ga;
+        ga.g = c->g;
+        for (int q = 0; q < 3; q++) ga.dst[q] = s->lV[q];
+        for (int q = 3; q < 6; q++) ga.dst[q] = nullptr;
+        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
+        adj_stress_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
+        ACK(cudaGetLastError());
+    }
+    return SWPC_OK;
+}
+
+static int adj_source(swpc_ctx *c, int it) {
+    swpc_adj_state *s = c->adj;
+    if (!s->res || c->nst <= 0 || !(c->wav_what & SWPC_WAV_V)) return SWPC_OK;
+    if ((it - 1) % c->ntdec_w != 0) return SWPC_OK;
+    const int itw = (it - 1) / c->ntdec_w + 1;
+    if (itw > c->ntw) return SWPC_OK;
+    // d(trace)/dV = 0.5 M0 UC 1e9 per cell of the two-cell average
+    const float scale = 0.5f * c->M0 * c->UC * 1e9f;
+    adj_source_kernel<<<(c->nst + 127) / 128, 128, 0, c->stream>>>(c->g, c->st_ijk, c->nst, c->ntw, itw, s->res, scale,
+                                                                    s->lV[0], s->lV[1], s->lV[2]);
+    return cuda_check(c, cudaGetLastError(), "adj_source_kernel");
+}
+
+static int zero_adjoint(swpc_ctx *c) {
+    swpc_adj_state *s = c->adj;
+    const size_t n = sizeof(float) * c->g.ncell;
+    for (auto p : s->lV) if (p) ACK(cudaMemsetAsync(p, 0, n, c->stream));
+    for (auto p : s->lS) if (p) ACK(cudaMemsetAsync(p, 0, n, c->stream));
+    for (auto p : s->lR) if (p) ACK(cudaMemsetAsync(p, 0, n, c->stream));
+    for (auto p : s->laux) if (p) ACK(cudaMemsetAsync(p, 0, sizeof(float) * c->npml, c->stream));
+    for (auto p : s->grad) {
+        zero_double_kernel<<<148 * 4, 256, 0, c->stream>>>(p, c->g.ncell);
+        ACK(cudaGetLastError());
+    }
+    return SWPC_OK;
+}
+
+// the adjoint array of a field id (V, S, R, PML auxiliaries)
+static float *adj_field(swpc_ctx *c, int field, bool *compact) {
+    swpc_adj_state *s = c->adj;
+    *compact = false;
+    if (field >= SWPC_F_VX && field <= SWPC_F_VZ) return s->lV[field - SWPC_F_VX];
+    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return s->lS[field - SWPC_F_SXX];
+    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return s->lR[field - SWPC_F_R];
+    if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) { *compact = true; return s->laux[field - SWPC_F_AUX]; }
+    return nullptr;
+}
+
+extern "C" int swpc_adj_reset(swpc_ctx *c) {
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    rc = zero_adjoint(c);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
+extern "C" int swpc_adj_step_linear(swpc_ctx *c) {
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    rc = adj_step(c, nullptr, nullptr);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
+extern "C" int swpc_adj_download(swpc_ctx *c, int field, float *out, int ld_k, int ld_i) {
+    if (!out) return SWPC_ERR_ARG;
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    bool compact;
+    float *p = adj_field(c, field, &compact);
+    if (!p) return err(c, SWPC_ERR_ARG, "unknown or unallocated adjoint field");
+    ACK(cudaStreamSynchronize(c->stream));
+    return compact ? aux_transfer_ptr(c, p, out, nullptr, ld_k, ld_i) : copy_box(c, p, nullptr, out, ld_k, ld_i);
+}
+
+extern "C" int swpc_adj_upload(swpc_ctx *c, int field, const float *in, int ld_k, int ld_i) {
+    if (!in) return SWPC_ERR_ARG;
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    bool compact;
+    float *p = adj_field(c, field, &compact);
+    if (!p) return err(c, SWPC_ERR_ARG, "unknown or unallocated adjoint field");
+    ACK(cudaStreamSynchronize(c->stream));
+    return compact ? aux_transfer_ptr(c, p, nullptr, in, ld_k, ld_i) : copy_box(c, p, in, nullptr, ld_k, ld_i);
+}
+
+// ---------------------------------------------------------------------------
+// checkpointed gradient
+// ---------------------------------------------------------------------------
+static std::vector<float *> state_arrays(swpc_ctx *c, std::vector<size_t> *sizes) {
+    std::vector<float *> v;
+    for (int q = 0; q < 3; q++) { v.push_back(c->V[q]); sizes->push_back(c->g.ncell); }
+    for (int q = 0; q < 6; q++) { v.push_back(c->S[q]); sizes->push_back(c->g.ncell); }
+    for (int q = 0; q < 18; q++)
+        if (c->R[q]) { v.push_back(c->R[q]); sizes->push_back(c->g.ncell); }
+    if (c->npml > 0)
+        for (int q = 0; q < 18; q++) { v.push_back(c->aux[q]); sizes->push_back(c->npml); }
+    return v;
+}
+
+static int copy_state(swpc_ctx *c, float *ck, bool save) {
+    std::vector<size_t> sz;
+    auto arr = state_arrays(c, &sz);
+    size_t off = 0;
+    for (size_t n = 0; n < arr.size(); n++) {
+        if (save) ACK(cudaMemcpyAsync(ck + off, arr[n], sz[n] * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        else ACK(cudaMemcpyAsync(arr[n], ck + off, sz[n] * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        off += sz[n];
+    }
+    return SWPC_OK;
+}
+
+static int save_slot(swpc_ctx *c, int slot) {
+    const size_t n = c->g.ncell;
+    float *base = c->adj->slots + (size_t)slot * 9 * n;
+    for (int q = 0; q < 3; q++) ACK(cudaMemcpyAsync(base + q * n, c->V[q], n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    for (int q = 0; q < 6; q++)
+        ACK(cudaMemcpyAsync(base + (3 + q) * n, c->S[q], n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    return SWPC_OK;
+}
+
+static int zero_state(swpc_ctx *c) {
+    std::vector<size_t> sz;
+    auto arr = state_arrays(c, &sz);
+    for (size_t n = 0; n < arr.size(); n++) ACK(cudaMemsetAsync(arr[n], 0, sz[n] * sizeof(float), c->stream));
+    if (c->uacc) ACK(cudaMemsetAsync(c->uacc, 0, 3 * sizeof(float) * std::max(c->nst, 1), c->stream));
+    if (c->eacc) ACK(cudaMemsetAsync(c->eacc, 0, 6 * sizeof(float) * std::max(c->nst, 1), c->stream));
+    return SWPC_OK;
+}
+
+extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *misfit) {
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    if (!obs || !misfit || ckpt < 1) return err(c, SWPC_ERR_ARG, "observed traces, misfit and ckpt >= 1 required");
+    if (c->nst <= 0 || !(c->wav_what & SWPC_WAV_V)) return err(c, SWPC_ERR_STATE, "velocity recorder not set up");
+    swpc_adj_state *s = c->adj;
+    const int nt = c->d.nt;
+    const int nseg = (nt + ckpt - 1) / ckpt;
+    std::vector<size_t> sz;
+    state_arrays(c, &sz);
+    size_t ckf = 0;
+    for (size_t v : sz) ckf += v;
+    const size_t need_ck = ckf * nseg, need_slots = (size_t)9 * c->g.ncell * (ckpt + 1);
+    if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf) {
+        if (s->ckpool) cudaFree(s->ckpool);
+        if (s->slots) cudaFree(s->slots);
+        s->ckpool = s->slots = nullptr;
+        if (cudaMalloc((void **)&s->ckpool, need_ck * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&s->slots, need_slots * sizeof(float)) != cudaSuccess)
+            return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints (raise ckpt or shrink the grid)");
+        s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf;
+    }
+    const size_t nres = (size_t)c->nst * 3 * c->ntw;
+    if (!s->res) ACK(cudaMalloc((void **)&s->res, nres * sizeof(float)));
+    // 1. forward from rest with a checkpoint before every segment
+    rc = zero_state(c);
+    if (rc) return rc;
+    for (int g = 0; g < nseg; g++) {
+        const int it0 = g * ckpt + 1, n = std::min(ckpt, nt - it0 + 1);
+        rc = copy_state(c, s->ckpool + (size_t)g * ckf, true);
+        if (rc) return rc;
+        rc = swpc_run(c, it0, n);
+        if (rc) return rc;
+    }
+    // 2. residuals and misfit
+    std::vector<float> syn(nres);
+    ACK(cudaMemcpyAsync(syn.data(), c->wav[0], nres * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    ACK(cudaStreamSynchronize(c->stream));
+    double J = 0.0;
+    for (size_t q = 0; q < nres; q++) {
+        syn[q] = syn[q] - obs[q];
+        J += 0.5 * (double)syn[q] * (double)syn[q];
+    }
+    *misfit = J;
+    ACK(cudaMemcpyAsync(s->res, syn.data(), nres * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    // 3. adjoint, segment by segment from the last
+    rc = zero_adjoint(c);
+    if (rc) return rc;
+    const size_t n = c->g.ncell;
+    for (int g = nseg - 1; g >= 0; g--) {
+        const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt);
+        rc = copy_state(c, s->ckpool + (size_t)g * ckf, false);
+        if (!rc) rc = save_slot(c, 0);
+        for (int it = it0; it <= it1 && !rc; it++) {
+            rc = swpc_step(c, it);
+            if (!rc) rc = save_slot(c, it - it0 + 1);
+        }
+        for (int it = it1; it >= it0 && !rc; it--) {
+            const float *base_a = s->slots + (size_t)(it - it0 + 1) * 9 * n;
+            const float *base_b = s->slots + (size_t)(it - it0) * 9 * n;
+            const float *Sa[6], *Vb[3];
+            for (int q = 0; q < 6; q++) Sa[q] = base_a + (3 + q) * n;
+            for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
+            rc = adj_step(c, Sa, Vb);
+            if (!rc) rc = adj_source(c, it);
+        }
+        if (rc) return rc;
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
+extern "C" int swpc_gradient_fetch(swpc_ctx *c, int which, double *out, int ld_k, int ld_i) {
+    if (!c || !out || which < 0 || which > 7) return SWPC_ERR_ARG;
+    if (!c->adj) return err(c, SWPC_ERR_STATE, "swpc_gradient not called");
+    const Geo &g = c->g;
+    if (ld_k < g.nz + 6 || ld_i < g.nx + 6) return err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    std::vector<double> h((size_t)g.ncell);
+    ACK(cudaSetDevice(c->device));
+    ACK(cudaMemcpyAsync(h.data(), c->adj->grad[which], g.ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ACK(cudaStreamSynchronize(c->stream));
+    for (int j = -2; j <= g.ny + 3; j++)
+        for (int i = -2; i <= g.nx + 3; i++)
+            for (int k = -2; k <= g.nz + 3; k++)
+                out[((long long)(j + 2) * ld_i + (i + 2)) * ld_k + (k + 2)] = h[cell_index(g, k, i, j)];
+    return SWPC_OK;
+}

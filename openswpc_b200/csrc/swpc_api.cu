@@ -156,6 +156,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     invalidate_graph(c);
     snap_free(c);
+    adj_free(c);
     if (!is3d(c)) destroy_2d(c);
     void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
                   c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
@@ -950,14 +951,23 @@ static float *field_ptr(swpc_ctx *c, int field) {
     return nullptr;
 }
 
+namespace swpc {
+// PML auxiliary array `dev` (compact per column) <-> Fortran memory box
+int aux_transfer_ptr(swpc_ctx *c, float *dev, float *out, const float *in, int ld_k, int ld_i);
+}
+
 static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_k, int ld_i) {
     if (!c->absorb_ready || !c->aux[q]) return set_err(c, SWPC_ERR_STATE, "swpc_absorb_setup not called");
+    return aux_transfer_ptr(c, c->aux[q], out, in, ld_k, ld_i);
+}
+
+int swpc::aux_transfer_ptr(swpc_ctx *c, float *dev, float *out, const float *in, int ld_k, int ld_i) {
     const Geo &g = c->g;
     if (!is3d(c)) {
         std::vector<float> buf((size_t)std::max<long long>(c->npml, 1));
         std::vector<int2> pc(g.Ip);
         CK(cudaMemcpyAsync(pc.data(), c->pmlcol, pc.size() * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(buf.data(), c->aux[q], c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(buf.data(), dev, c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         for (int i = -2; i <= g.nx + 3; i++) {
             const long long h = (long long)(i + 2) * ld_k;
@@ -969,7 +979,7 @@ static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_
             }
         }
         if (in) {
-            CK(cudaMemcpyAsync(c->aux[q], buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(dev, buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
             CK(cudaStreamSynchronize(c->stream));
         }
         return SWPC_OK;
@@ -978,7 +988,7 @@ static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_
     std::vector<int2> pc((size_t)g.Ip * g.Jp);
     CK(cudaMemcpyAsync(pc.data(), c->pmlcol, pc.size() * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
     if (in == nullptr || true)
-        CK(cudaMemcpyAsync(buf.data(), c->aux[q], c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(buf.data(), dev, c->npml * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (int j = -2; j <= g.ny + 3; j++)
         for (int i = -2; i <= g.nx + 3; i++) {
@@ -992,7 +1002,7 @@ static int aux_transfer(swpc_ctx *c, int q, float *out, const float *in, int ld_
             }
         }
     if (in) {
-        CK(cudaMemcpyAsync(c->aux[q], buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(dev, buf.data(), c->npml * sizeof(float), cudaMemcpyHostToDevice, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     }
     return SWPC_OK;

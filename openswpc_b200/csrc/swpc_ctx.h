@@ -57,6 +57,7 @@ struct Wav2Args;
 }  // namespace swpc
 
 struct swpc_snap_state;
+struct swpc_adj_state;
 
 struct swpc_ctx {
     int kind;
@@ -126,6 +127,8 @@ struct swpc_ctx {
 
     // snapshot planes (swpc_snap.cu)
     swpc_snap_state *snp = nullptr;
+    // adjoint state and checkpoints (swpc_adjoint.cu)
+    swpc_adj_state *adj = nullptr;
 
     // vmax
     unsigned int *vmax_buf = nullptr;
@@ -163,6 +166,7 @@ namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
 int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
+void adj_free(swpc_ctx *c);   // swpc_adjoint.cu
 int field_storage(const swpc_ctx *c, int field);   // swpc_prec.cu
 float field_scale(const swpc_ctx *c, int field);
 int prec_to_f32(swpc_ctx *c, int field, const float *stored, float **tmp);
