@@ -280,6 +280,263 @@ def bench_c2a(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def make_c2b(nmem: int = 32):
+    """The reciprocity batch: 384 x 384 x 192 cells of the four-layer medium
+    at dx = 0.5 km, dt = 0.02 s, nt = 1000, nm = 3, PML 20; 32 single forces
+    (x, y, z in turn) at seeded surface stations, Kupper T = 2 s; the members
+    record at 16 seeded surface stations."""
+    from openswpc_b200.params import Layer, Params, Station
+
+    layers = [Layer(0.0, 2.7, 5.5, 3.2, 300, 150), Layer(5.0, 2.8, 6.0, 3.5, 500, 250),
+              Layer(18.0, 2.9, 6.7, 3.9, 600, 300), Layer(30.0, 3.3, 7.8, 4.5, 1000, 500)]
+    nx, ny, nz, dx, na = 384, 384, 192, 0.5, 20
+    rng = np.random.default_rng(20241204)
+    xb, yb = -nx // 2 * dx, -ny // 2 * dx
+    pick = lambda lo, hi: float(rng.uniform(lo + (na + 4) * dx, lo + (hi - na - 4) * dx))
+    st = [Station(pick(xb, nx), pick(yb, ny), 0.0, f"r{n:02d}", "fsb") for n in range(16)]
+    fst = [Station(pick(xb, nx), pick(yb, ny), 0.0, f"f{n:02d}", "fsb") for n in range(nmem)]
+    p = Params(nx=nx, ny=ny, nz=nz, nt=1000, dx=dx, dy=dx, dz=dx, dt=0.02, na=na, nm=3, xbeg=xb, ybeg=yb,
+               zbeg=-3 * dx, fq_min=0.05, fq_max=2.0, layers=layers, sources=[], stations=fst + st, ntdec_w=1,
+               ntdec_r=100, green_mode=True, green_trise=2.0, green_station=0, green_cmp="z")
+    forces = [(fst[m], "xyz"[m % 3]) for m in range(nmem)]
+    return p, forces, st
+
+
+def bench_c2b(args, world, rank, local):
+    """32 single-force reciprocity sources over one shared 3D medium, batched
+    in one launch per half step, against the plain per-source loop."""
+    nmem = 32
+    wl = {"workload": "reciprocity batch: 32 single forces over one shared 384x384x192 grid (four-layer medium, "
+                      "nm=3, PML 20, 16 stations)", "nx": 384, "ny": 384, "nz": 192, "members": nmem,
+          "l2": "inputs larger than L2 (32 wavefields resident, ~130 GB)", "parallelism": f"members/{world} GPUs"}
+    metric = "Gcell-updates/s (3D visco, FP32, reciprocity batch)"
+    p, forces, st = make_c2b(nmem)
+    forces = [f for m, f in enumerate(forces) if m % world == rank]   # members shard across GPUs
+    cells = p.nx * p.ny * p.nz
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        q = Params_copy(p)
+        q.green_mode = False
+        from openswpc_b200.params import dc_source
+        q.sources = [dc_source(0.0, 0.0, 10.0, 0.0, 2.0, 1e16, 30, 60, 90)]
+        v, n, sample_cells, dt = cpu_reference(q, None, args.steps, args.warmup, threads, budget_s=args.cpu_budget)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
+                "warmup": args.warmup, "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": wl,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"oracle f32, one source per run as the reference runs it, one step per "
+                                           f"timed step over the centre 256x256x{p.nz} column block"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    from openswpc_b200 import _lib
+    from openswpc_b200.swpc3d import ForceBatch3D, Swpc3D
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    base = Swpc3D(p, device=local)
+    base.record(st)
+    lib = base.lib
+    # the plain per-source loop: one green-mode run (its own CUDA graph) per source, one after another; every
+    # source costs the same on this grid, so the loop time is nmem x one source's time
+    _lib.check(base.ctx, lib.swpc_run(base.ctx, 1, args.warmup))
+    ms1 = C.c_float()
+    _lib.check(base.ctx, lib.swpc_time_steps(base.ctx, 1 + args.warmup, args.steps, C.byref(ms1)))
+    ms_loop = max_over_ranks(ms1.value * len(forces))
+    fb = ForceBatch3D(base, forces)
+    used, strip = fb.autotune(1, reps=2)
+    it0 = 1 + used
+    fb.run(it0, args.warmup)
+    it0 += args.warmup
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms_batch = fb.time_steps(it0, args.steps)
+    it0 += args.steps
+    ms_batch = max_over_ranks(ms_batch)
+    n_int, n_pml = cell_counts(p)
+    # algorithmic bytes: per member the 3D step without its medium reads (292 - 40 interior, 284 - 32 PML),
+    # plus the medium once per step for all members
+    b_mem = n_int * (B_STRESS_INT + B_VEL_INT - 40) + n_pml * (B_STRESS_PML + B_VEL_PML - 32)
+    b_step = len(forces) * b_mem + n_int * 40 + n_pml * 32
+    peak, peak_kind = hbm_peak()
+    ach = b_step / (ms_batch / args.steps / 1e3) / 1e9
+    value = cells * nmem * args.steps / (ms_batch / 1e3) / 1e9
+    # end to end through the public API: per-step batch calls, every member's traces back to the host
+    t0 = time.perf_counter()
+    for n in range(args.steps):
+        fb.step(it0 + n)
+    tr = [fb.waveforms(m) for m in range(len(forces))]
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    d2h = sum(t.nbytes for t in tr)
+    line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_batch / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered medium)",
+            "config": wl,
+            "what": "value counts cells x members per step",
+            "plain_loop": {"value": cells * nmem * args.steps / (ms_loop / 1e3) / 1e9, "unit": UNIT,
+                           "ms_per_step": ms_loop / args.steps,
+                           "what": "one green-mode run per source, its own CUDA graph, sources one after another"},
+            "batched_over_loop": ms_loop / ms_batch,
+            "autotune": {"strip_cells": strip, "steps_used": used},
+            "roofline": {"bound": "hbm", "kernel": "stress3d_batch_kernel + vel3d_batch_kernel (whole batched step)",
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes_per_step": b_step},
+            "e2e": {"value": cells * len(forces) * world * args.steps / t_e2e / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h / args.steps,
+                    "what": "per-step batch calls + every member's traces downloaded, wall clock"},
+            "gpu_launches": args.steps * 5, "clocks": clk.summary()}
+    fb.close()
+    base.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def Params_copy(p):
+    from openswpc_b200.params import Params
+
+    return Params(**{**p.__dict__})
+
+
+def make_c3():
+    """The adjoint-gradient workload: 256 x 256 x 128 cells, dx = 0.25 km,
+    dt = 0.01 s, nt = 2000, nm = 3, PML 20; the four-layer background, one
+    double couple at 8 km depth, 64 seeded surface stations.  Returns the
+    parameters, the starting model (vp, vs, rho, qp, qs) and the true vs:
+    the background with a seeded Gaussian blob of -8 % (radius 3 km)."""
+    from openswpc_b200.params import Layer, Params, Station, dc_source
+    from openswpc_b200.swpc3d import lhm_model
+
+    layers = [Layer(0.0, 2.7, 5.5, 3.2, 300, 150), Layer(5.0, 2.8, 6.0, 3.5, 500, 250),
+              Layer(18.0, 2.9, 6.7, 3.9, 600, 300), Layer(30.0, 3.3, 7.8, 4.5, 1000, 500)]
+    nx, ny, nz, dx, na = 256, 256, 128, 0.25, 20
+    rng = np.random.default_rng(20241205)
+    xb, yb = -nx // 2 * dx, -ny // 2 * dx
+    st = [Station(float(rng.uniform(xb + (na + 2) * dx, xb + (nx - na - 2) * dx)),
+                  float(rng.uniform(yb + (na + 2) * dx, yb + (ny - na - 2) * dx)), 0.0, f"s{n:02d}", "fsb")
+          for n in range(64)]
+    p = Params(nx=nx, ny=ny, nz=nz, nt=2000, dx=dx, dy=dx, dz=dx, dt=0.01, na=na, nm=3, xbeg=xb, ybeg=yb,
+               zbeg=-3 * dx, fq_min=0.05, fq_max=2.0, layers=layers,
+               sources=[dc_source(0.0, 0.0, 8.0, 0.0, 2.0, 1e16, 30, 60, 90)], stations=st, ntdec_w=1,
+               ntdec_r=100)
+    vp, vs, rho, qp, qs = lhm_model(p)
+    # blob centre: seeded in the middle third of the domain, 4-12 km deep
+    cx, cy = (float(rng.uniform(-nx / 6, nx / 6) * dx) for _ in range(2))
+    cz = float(rng.uniform(4.0, 12.0))
+    z = p.zbeg + (np.arange(-2, nz + 4) - 0.5) * dx
+    y = p.ybeg + (np.arange(-2, ny + 4) - 0.5) * dx
+    x = p.xbeg + (np.arange(-2, nx + 4) - 0.5) * dx
+    r2 = (y[:, None, None] - cy) ** 2 + (x[None, :, None] - cx) ** 2 + (z[None, None, :] - cz) ** 2
+    vs_true = (vs * (1.0 - 0.08 * np.exp(-r2 / (2 * 3.0 ** 2)))).astype(np.float32)
+    return p, (vp, vs, rho, qp, qs), vs_true
+
+
+def bench_c3(args, world, rank, local):
+    """Checkpointed adjoint gradient of the L2 velocity misfit with respect to
+    per-cell vp, vs, rho, against one plain forward run of the same model."""
+    wl = {"workload": "adjoint gradient 256x256x128, nt=2000 (nm=3, PML 20, 1 double couple, 64 stations, "
+                      "checkpoint every 50 steps)", "nx": 256, "ny": 256, "nz": 128, "nt": 2000, "ckpt": 50,
+          "l2": "inputs larger than L2 (wavefield, checkpoints and adjoint state resident, tens of GB)",
+          "parallelism": f"replicas x{world}"}
+    metric = "Gcell-updates/s (3D visco adjoint gradient, FP32 + FP64 accumulation)"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint or gradient path"}),
+              flush=True)
+        return
+    import torch
+    from openswpc_b200 import _lib
+    from openswpc_b200.adjoint import Misfit3D, waveform_misfit
+    from openswpc_b200.swpc3d import Medium, Swpc3D
+
+    p, (vp, vs, rho, qp, qs), vs_true = make_c3()
+    cells = p.nx * p.ny * p.nz
+    true = Swpc3D(p, device=local, medium=Medium.from_model(p, vp, vs_true, rho, qp, qs))
+    _lib.check(true.ctx, true.lib.swpc_run(true.ctx, 1, p.nt))
+    obs = true.waveforms(_lib.WAV_V)
+    true.close()
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, device=local, ckpt=50)
+    s = prob.solver
+    lib, ctx = s.lib, s.ctx
+    stream = torch.cuda.ExternalStream(lib.swpc_stream(ctx), device=local)
+    J = C.c_double()
+    obsf = np.ascontiguousarray(obs, np.float32)
+
+    def t_forward():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _lib.check(ctx, lib.swpc_reset_state(ctx))
+        e0.record(stream)
+        _lib.check(ctx, lib.swpc_run(ctx, 1, p.nt))
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def t_gradient():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _lib.check(ctx, lib.swpc_sync(ctx))
+        e0.record(stream)
+        _lib.check(ctx, lib.swpc_gradient(ctx, _lib.fptr(obsf), 50, C.byref(J)))
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        t_gradient()
+    t_forward()
+    with ClockSampler(local) as clk:
+        ms_fwd = [t_forward() for _ in range(args.steps)]
+        ms_grad = [t_gradient() for _ in range(args.steps)]
+    fwd, grad = float(np.mean(ms_fwd)), float(np.mean(ms_grad))
+    # end to end through the public API: CPU tensors in, autograd gradient out
+    tv = [torch.tensor(a, requires_grad=True) for a in (vp, vs, rho)]
+    t0 = time.perf_counter()
+    Jt = waveform_misfit(*tv, prob)
+    Jt.backward()
+    t_e2e = time.perf_counter() - t0
+    h2d = sum(a.nbytes for a in (vp, vs, rho)) * 2 + obsf.nbytes
+    d2h = sum(t.grad.numel() * 8 for t in tv) + obsf.nbytes
+    line = {"metric": metric, "value": cells * p.nt / (grad / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": grad, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + "
+            "Gaussian vs blob)", "config": wl,
+            "what": "one step = one gradient evaluation (forward with checkpoints, per-segment recompute, "
+                    "adjoint); value counts cells x nt per gradient",
+            "misfit": J.value,
+            "forward_ms": fwd, "forward_gcells": cells * p.nt / (fwd / 1e3) / 1e9,
+            "gradient_over_forward": grad / fwd,
+            "e2e": {"value": cells * p.nt / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "what": "waveform_misfit(vp, vs, rho) + backward from CPU tensors: medium setup on the host, "
+                            "upload, gradient, chain rule, gradients back, wall clock"},
+            # per gradient: forward and recompute steps (wav, stress, injection, velocity, step counter), the
+            # adjoint steps (two weight and two gather kernels, residual injection), zeroing of 8 gradients
+            "gpu_launches": args.steps * (p.nt * (5 + 4 + 5) + 8), "clocks": clk.summary()}
+    prob.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def cell_counts(p):
     ni, nj, nk = p.nx - 2 * p.na, p.ny - 2 * p.na, p.nz - p.na
     n_int = ni * nj * nk
@@ -430,7 +687,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3"])
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16sr"],
@@ -448,6 +705,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "c2a":
         return bench_c2a(args, world, rank, local)
+    if args.workload == "c3":
+        return bench_c3(args, world, rank, local)
+    if args.workload == "c2b":
+        return bench_c2b(args, world, rank, local)
     p = make_params(args.workload)
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.lower().split("x"))

@@ -244,11 +244,71 @@ int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const i
  * swpc_gradient_fetch: which = 0 lam, 1 mu, 2 muyz, 3 muxz, 4 muxy, 5 bx,
  * 6 by, 7 bz; out = double array over the memory box. */
 int swpc_adj_reset(swpc_ctx *ctx);
+/* Zero the forward state (V, S, R, PML auxiliaries, displacement and strain
+ * accumulators) for another run from rest on the same context.  No
+ * counterpart in the reference, which allocates zeroed arrays once per run
+ * (m_kernel.f90:354-378, m_absorb_p.f90:96-116). */
+int swpc_reset_state(swpc_ctx *ctx);
 int swpc_adj_step_linear(swpc_ctx *ctx);
 int swpc_adj_upload(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
 int swpc_adj_download(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
 int swpc_gradient(swpc_ctx *ctx, const float *obs, int ckpt, double *misfit);
 int swpc_gradient_fetch(swpc_ctx *ctx, int which, double *out, int ld_k, int ld_i);
+/* The gradient of the last swpc_gradient with respect to per-cell vp, vs and
+ * rho with Q held fixed: the chain rule through vmodel_lhm's moduli
+ * (src/swpc_3d/m_vmodel_lhm.f90:158-160), relaxed_medium
+ * (m_medium.f90:234-274) and averaged_medium's buoyancies and 4-point
+ * harmonic rigidities (m_medium.f90:432-465), in FP64 on the device.  No
+ * counterpart in the reference.  vp, vs, rho: the model the medium was set up
+ * from, over the memory box (host arrays, leading extents ld_k, ld_i);
+ * outputs likewise.  The parameters are the cells of the kernel region:
+ * absorber cells copy the medium of the region's edge (m_medium.f90:124-190)
+ * and their medium is held fixed, so a cell within one cell of the absorber
+ * lacks the terms of averaged entries that fall in the absorber. */
+int swpc_gradient_model(swpc_ctx *ctx, const float *vp, const float *vs, const float *rho, int ld_k, int ld_i,
+                        double *gvp, double *gvs, double *grho);
+
+/* ---- reciprocity batch (3D) ---------------------------------------------- */
+
+/* nmem independent wavefields over the medium of one context, each driven by
+ * its own single force as green__source drives a green-mode run
+ * (src/swpc_3d/m_green.f90:597-632; green__setup :146-154).  No counterpart
+ * in the reference, which runs one force per job.  Each member is bitwise
+ * the run a context in green mode gives for its force: the step is
+ * main.f90:125-144 (wav__store, stress, velocity, green__source), every half
+ * step one launch for all members, with the medium of each cell tile read
+ * from HBM once for all members.
+ *   swpc_fbatch_create        needs medium, kernel and absorber setup on ctx;
+ *                             members record at ctx's stations
+ *                             (swpc_wav_setup) into their own buffers; the
+ *                             batch allocates nmem copies of V, S, R and the
+ *                             PML auxiliaries (zero-filled)
+ *   swpc_fbatch_green_source  the force of member m (≙ green__setup): unit
+ *                             force along cmp ('x','y','z') at cell
+ *                             (ksrc, isrc, jsrc), Kupper etc. time function
+ *                             from green_tbeg / green_trise
+ *   swpc_fbatch_step / _run   one step / nsteps graph replays of all members
+ *   swpc_fbatch_set_strip     i-strip width in cells of the launch order
+ *                             (0 = from the L2 size); _autotune times the
+ *                             candidates over steps it0.. and keeps the best
+ *   swpc_fbatch_wav_fetch     traces of member m, layout of swpc_wav_fetch
+ *   swpc_fbatch_download_field  V, S or R of member m in the memory box
+ * The batch borrows ctx (which must outlive it); ctx's own state and sources
+ * are untouched. */
+typedef struct swpc_fbatch swpc_fbatch;
+int swpc_fbatch_create(swpc_ctx *ctx, int nmem, swpc_fbatch **out);
+int swpc_fbatch_destroy(swpc_fbatch *b);
+int swpc_fbatch_green_source(swpc_fbatch *b, int member, int isrc, int jsrc, int ksrc, char cmp, float green_tbeg,
+                             float green_trise, int stftype);
+int swpc_fbatch_set_strip(swpc_fbatch *b, int strip_cells);
+int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *steps_used, int *strip);
+int swpc_fbatch_step(swpc_fbatch *b, int it);
+int swpc_fbatch_run(swpc_fbatch *b, int it0, int nsteps);
+int swpc_fbatch_time_steps(swpc_fbatch *b, int it0, int nsteps, float *ms);
+int swpc_fbatch_sync(swpc_fbatch *b);
+int swpc_fbatch_wav_fetch(swpc_fbatch *b, int member, int what, float *out);
+int swpc_fbatch_download_field(swpc_fbatch *b, int member, int field, float *out, int ld_k, int ld_i);
+long long swpc_fbatch_device_bytes(const swpc_fbatch *b);
 
 /* ---- snapshots (3D) ------------------------------------------------------ */
 

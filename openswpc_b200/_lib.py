@@ -42,13 +42,16 @@ EXPORTS = [
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
     "swpc_adj_reset", "swpc_adj_step_linear", "swpc_adj_upload", "swpc_adj_download", "swpc_gradient",
-    "swpc_gradient_fetch",
+    "swpc_gradient_fetch", "swpc_gradient_model", "swpc_reset_state",
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape",
+    "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
+    "swpc_fbatch_autotune", "swpc_fbatch_step", "swpc_fbatch_run", "swpc_fbatch_time_steps", "swpc_fbatch_sync",
+    "swpc_fbatch_wav_fetch", "swpc_fbatch_download_field", "swpc_fbatch_device_bytes",
     "swpc_batch_last_error", "swpc_batch_destroy",
 ]
 
@@ -145,11 +148,14 @@ def load():
         "swpc_upload_field": (i, [vp, i, _FP, i, i]),
         "swpc_rescale": (i, [vp, _IP]),
         "swpc_adj_reset": (i, [vp]),
+        "swpc_reset_state": (i, [vp]),
         "swpc_adj_step_linear": (i, [vp]),
         "swpc_adj_upload": (i, [vp, i, _FP, i, i]),
         "swpc_adj_download": (i, [vp, i, _FP, i, i]),
         "swpc_gradient": (i, [vp, _FP, i, C.POINTER(C.c_double)]),
         "swpc_gradient_fetch": (i, [vp, i, C.POINTER(C.c_double), i, i]),
+        "swpc_gradient_model": (i, [vp, _FP, _FP, _FP, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]),
         "swpc_device_bytes": (C.c_longlong, [vp]),
         "swpc_set_launch": (i, [vp, i, i, i, i]),
         "swpc_x2i": (i, [f, f, f]),
@@ -174,6 +180,18 @@ def load():
         "swpc_batch_set_shape": (i, [vp, i, i, i]),
         "swpc_batch_last_error": (C.c_char_p, [vp]),
         "swpc_batch_destroy": (i, [vp]),
+        "swpc_fbatch_create": (i, [vp, i, C.POINTER(vp)]),
+        "swpc_fbatch_destroy": (i, [vp]),
+        "swpc_fbatch_green_source": (i, [vp, i, i, i, i, C.c_char, f, f, i]),
+        "swpc_fbatch_set_strip": (i, [vp, i]),
+        "swpc_fbatch_autotune": (i, [vp, i, i, _IP, _IP]),
+        "swpc_fbatch_step": (i, [vp, i]),
+        "swpc_fbatch_run": (i, [vp, i, i]),
+        "swpc_fbatch_time_steps": (i, [vp, i, i, _FP]),
+        "swpc_fbatch_sync": (i, [vp]),
+        "swpc_fbatch_wav_fetch": (i, [vp, i, i, _FP]),
+        "swpc_fbatch_download_field": (i, [vp, i, i, _FP, i, i]),
+        "swpc_fbatch_device_bytes": (C.c_longlong, [vp]),
     }
     for name in ("swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
                  "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_comm_stress",

@@ -1,0 +1,117 @@
+"""Misfit gradient of the 3D viscoelastic run behind ``torch.autograd``.
+
+The misfit is J = 0.5 * sum (v_syn - v_obs)^2 over the three-component
+velocity traces that wav__store records (src/swpc_3d/m_wav.f90:530-535) of a
+run from rest over steps 1..nt.  Its gradient with respect to per-cell vp, vs
+and rho (Q held fixed) comes from the library's discrete adjoint of the step
+(``swpc_gradient``: checkpointed forward, recompute per segment, transposed
+step, FP64 accumulation) and the chain rule of ``swpc_gradient_model``.  Both
+run on the GPU; this module only moves the model in and the gradient out.
+
+The parameters are the cells of the kernel region: absorber cells copy the
+medium of the region's edge (m_medium.f90:124-190) whatever the tensors hold
+there, and their medium is held fixed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, fptr
+from .params import Params
+from .swpc3d import Medium, Swpc3D
+
+
+class Misfit3D:
+    """A 3D run with its sources, stations and Q fixed, evaluated for any
+    per-cell (vp, vs, rho) against observed velocity traces ``obs`` of shape
+    (nst, 3, ntw), the layout of ``Swpc3D.waveforms``."""
+
+    def __init__(self, p: Params, vp, vs, rho, qp, qs, obs: np.ndarray, device: int = 0, ckpt: int = 50):
+        self.p = p
+        self.qp = np.ascontiguousarray(qp, np.float32)
+        self.qs = np.ascontiguousarray(qs, np.float32)
+        self.ckpt = int(ckpt)
+        m = Medium.from_model(p, vp, vs, rho, self.qp, self.qs)
+        self.solver = Swpc3D(p, device=device, medium=m)
+        self.obs = np.ascontiguousarray(obs, np.float32)
+        if self.obs.shape != (self.solver.nst, 3, self.ntw):
+            raise ValueError(f"observed traces must have shape {(self.solver.nst, 3, self.ntw)}")
+
+    @property
+    def ntw(self) -> int:
+        return (self.p.nt - 1) // self.p.ntdec_w + 1
+
+    def close(self):
+        self.solver.close()
+
+    def _set_model(self, vp, vs, rho) -> Medium:
+        s = self.solver
+        m = Medium.from_model(self.p, vp, vs, rho, self.qp, self.qs)
+        check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view())))
+        s.medium = m
+        return m
+
+    def misfit(self, vp, vs, rho) -> float:
+        """J of one forward run (no adjoint)."""
+        s = self.solver
+        self._set_model(vp, vs, rho)
+        check(s.ctx, s.lib.swpc_reset_state(s.ctx))
+        check(s.ctx, s.lib.swpc_run(s.ctx, 1, self.p.nt))
+        r = s.waveforms(_lib.WAV_V).astype(np.float64) - self.obs
+        return 0.5 * float(np.sum(r * r))
+
+    def gradient(self, vp, vs, rho):
+        """(J, dJ/dvp, dJ/dvs, dJ/drho); the gradients are float64 arrays
+        over the memory box."""
+        s, p = self.solver, self.p
+        self._set_model(vp, vs, rho)
+        J = C.c_double()
+        check(s.ctx, s.lib.swpc_gradient(s.ctx, fptr(self.obs), self.ckpt, C.byref(J)))
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        f = lambda a: np.ascontiguousarray(a, np.float32).reshape(shape)
+        out = [np.zeros(shape, np.float64) for _ in range(3)]
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        check(s.ctx, s.lib.swpc_gradient_model(s.ctx, fptr(f(vp)), fptr(f(vs)), fptr(f(rho)), p.nz + 6, p.nx + 6,
+                                               dp(out[0]), dp(out[1]), dp(out[2])))
+        return J.value, out[0], out[1], out[2]
+
+
+def _host(t: torch.Tensor) -> np.ndarray:
+    return t.detach().to("cpu", torch.float32).contiguous().numpy()
+
+
+class WaveformMisfit(torch.autograd.Function):
+    """J(vp, vs, rho) of a :class:`Misfit3D` problem as an autograd node.
+
+    ``forward`` runs the forward and, when any input needs a gradient, the
+    checkpointed adjoint in the same call (the adjoint needs the residuals of
+    the whole forward, so both run together); ``backward`` scales the stored
+    gradient by the incoming one.  J is returned as a float64 scalar tensor on
+    the device of ``vp``."""
+
+    @staticmethod
+    def forward(ctx, vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor, problem: Misfit3D):
+        args = (_host(vp), _host(vs), _host(rho))
+        if any(ctx.needs_input_grad[:3]):
+            J, gvp, gvs, grho = problem.gradient(*args)
+            ctx.save_for_backward(*(torch.from_numpy(g).to(t.device) for g, t in ((gvp, vp), (gvs, vs),
+                                                                                  (grho, rho))))
+            ctx.dtypes = (vp.dtype, vs.dtype, rho.dtype)
+        else:
+            J = problem.misfit(*args)
+        return torch.tensor(J, dtype=torch.float64, device=vp.device)
+
+    @staticmethod
+    def backward(ctx, gJ: torch.Tensor):
+        gvp, gvs, grho = ctx.saved_tensors
+        out = [(gJ * g).to(dt) for g, dt in zip((gvp, gvs, grho), ctx.dtypes)]
+        return out[0], out[1], out[2], None
+
+
+def waveform_misfit(vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor, problem: Misfit3D) -> torch.Tensor:
+    """J = 0.5 sum (v_syn - v_obs)^2, differentiable in vp, vs and rho."""
+    return WaveformMisfit.apply(vp, vs, rho, problem)

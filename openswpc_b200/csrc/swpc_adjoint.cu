@@ -367,6 +367,79 @@ __global__ void zero_double_kernel(double *p, long long n) {
         p[q] = 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// chain rule from the medium arrays to per-cell vp, vs, rho (Q fixed)
+//
+// The medium of a cell follows from its vp, vs, rho as vmodel_lhm, then
+// relaxed_medium and averaged_medium compute it (m_vmodel_lhm.f90:158-160,
+// m_medium.f90:234-274, 432-465):
+//   mu  = rho vs^2 / chi_s^2,   lam + 2 mu = rho vp^2 / chi_p^2,
+// with chi fixed by Q, so d mu/d vs = 2 mu/vs, d mu/d rho = mu/rho and the
+// same for lam + 2 mu; b_x(e) = 2/(rho(e) + rho(e+i)) (d/d rho = -b^2/2 for
+// both cells); mu_xz(e) = 4 abcd/(abc + abd + acd + bcd + eps) over the four
+// cells (e, e+k, e+i, e+k+i), and likewise mu_xy (i, j) and mu_yz (k, j).
+// ---------------------------------------------------------------------------
+struct ModelGradArgs {
+    Geo g;
+    const double *gm[8];           // lam mu muyz muxz muxy bx by bz
+    const float *lam, *mu, *b[3];  // relaxed medium, buoyancies
+    const float *vp, *vs, *rho;    // the model (device layout)
+    double *out[3];                // d misfit / d vp, vs, rho
+};
+
+// sum over the four entries of a 4-point harmonic mean that contain cell e
+// (entry E averages E, E+o1, E+o2, E+o1+o2) of g(E) * d mean(E) / d mu(e)
+__device__ double hmean_adjoint(const double *gf, const float *mu, long long e, long long o1, long long o2) {
+    const long long offs[4] = {0, o1, o2, o1 + o2};
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const long long E = e - offs[q];
+        const double gE = gf[E];
+        if (gE == 0.0) continue;
+        double m[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) m[r] = (double)mu[E + offs[r]];
+        // the three values other than the one at e (position q)
+        double o[3];
+        int n = 0;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            if (r != q) o[n++] = m[r];
+        const double x = m[q];
+        const double p3 = o[0] * o[1] * o[2];
+        const double s2 = o[0] * o[1] + o[0] * o[2] + o[1] * o[2];
+        const double D = x * s2 + p3 + (double)1.1920929e-07f;
+        const double N = 4.0 * x * p3;
+        acc += gE * (4.0 * p3 * D - N * s2) / (D * D);
+    }
+    return acc;
+}
+
+__global__ void __launch_bounds__(128) model_grad_kernel(const ModelGradArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long e = cell_index(g, k, i, j);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    const double glam = a.gm[0][e];
+    const double gmu = a.gm[1][e] + hmean_adjoint(a.gm[2], a.mu, e, 1, PJ) + hmean_adjoint(a.gm[3], a.mu, e, 1, PI) +
+                       hmean_adjoint(a.gm[4], a.mu, e, PI, PJ);
+    double grho = 0.0;
+    const long long boff[3] = {PI, PJ, 1};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const double b0 = a.b[q][e], b1 = a.b[q][e - boff[q]];
+        grho += a.gm[5 + q][e] * (-0.5 * b0 * b0) + a.gm[5 + q][e - boff[q]] * (-0.5 * b1 * b1);
+    }
+    const double lam = a.lam[e], mu = a.mu[e];
+    const double vp = a.vp[e], vs = a.vs[e], rho = a.rho[e];
+    const double m2 = lam + 2.0 * mu;
+    a.out[0][e] = vp > 0.0 ? glam * 2.0 * m2 / vp : 0.0;
+    a.out[1][e] = vs > 0.0 ? (gmu - 2.0 * glam) * 2.0 * mu / vs : 0.0;
+    a.out[2][e] = grho + (rho > 0.0 ? (glam * lam + gmu * mu) / rho : 0.0);
+}
+
 dim3 cell_grid(const Geo &g, dim3 block) {
     return dim3((g.nz + kThreadsK - 1) / kThreadsK, (g.nx + block.y - 1) / block.y, (g.ny + block.z - 1) / block.z);
 }
@@ -621,6 +694,15 @@ static int zero_state(swpc_ctx *c) {
     return SWPC_OK;
 }
 
+extern "C" int swpc_reset_state(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "swpc_reset_state is implemented for the 3D solver");
+    ACK(cudaSetDevice(c->device));
+    int rc = zero_state(c);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
 extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *misfit) {
     int rc = adj_ready(c);
     if (rc) return rc;
@@ -692,18 +774,62 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
 
-extern "C" int swpc_gradient_fetch(swpc_ctx *c, int which, double *out, int ld_k, int ld_i) {
-    if (!c || !out || which < 0 || which > 7) return SWPC_ERR_ARG;
-    if (!c->adj) return err(c, SWPC_ERR_STATE, "swpc_gradient not called");
+// device double array -> host memory box
+static int fetch_double(swpc_ctx *c, const double *dev, double *out, int ld_k, int ld_i) {
     const Geo &g = c->g;
-    if (ld_k < g.nz + 6 || ld_i < g.nx + 6) return err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
     std::vector<double> h((size_t)g.ncell);
-    ACK(cudaSetDevice(c->device));
-    ACK(cudaMemcpyAsync(h.data(), c->adj->grad[which], g.ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ACK(cudaMemcpyAsync(h.data(), dev, g.ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     ACK(cudaStreamSynchronize(c->stream));
     for (int j = -2; j <= g.ny + 3; j++)
         for (int i = -2; i <= g.nx + 3; i++)
             for (int k = -2; k <= g.nz + 3; k++)
                 out[((long long)(j + 2) * ld_i + (i + 2)) * ld_k + (k + 2)] = h[cell_index(g, k, i, j)];
     return SWPC_OK;
+}
+
+extern "C" int swpc_gradient_fetch(swpc_ctx *c, int which, double *out, int ld_k, int ld_i) {
+    if (!c || !out || which < 0 || which > 7) return SWPC_ERR_ARG;
+    if (!c->adj) return err(c, SWPC_ERR_STATE, "swpc_gradient not called");
+    const Geo &g = c->g;
+    if (ld_k < g.nz + 6 || ld_i < g.nx + 6) return err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    ACK(cudaSetDevice(c->device));
+    return fetch_double(c, c->adj->grad[which], out, ld_k, ld_i);
+}
+
+extern "C" int swpc_gradient_model(swpc_ctx *c, const float *vp, const float *vs, const float *rho, int ld_k,
+                                   int ld_i, double *gvp, double *gvs, double *grho) {
+    if (!c || !vp || !vs || !rho || !gvp || !gvs || !grho) return SWPC_ERR_ARG;
+    if (!c->adj) return err(c, SWPC_ERR_STATE, "swpc_gradient not called");
+    const Geo &g = c->g;
+    if (ld_k < g.nz + 6 || ld_i < g.nx + 6) return err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    ACK(cudaSetDevice(c->device));
+    float *dm[3] = {};
+    double *dg[3] = {};
+    int rc = SWPC_OK;
+    const float *hm[3] = {vp, vs, rho};
+    for (int q = 0; q < 3 && !rc; q++) {
+        rc = dalloc(c, &dm[q], g.ncell);
+        if (!rc) rc = dalloc(c, &dg[q], g.ncell);
+        if (!rc) rc = copy_box(c, dm[q], hm[q], nullptr, ld_k, ld_i);
+    }
+    if (!rc) {
+        ModelGradArgs a;
+        a.g = g;
+        for (int q = 0; q < 8; q++) a.gm[q] = c->adj->grad[q];
+        a.lam = c->med[1]; a.mu = c->med[2];
+        for (int q = 0; q < 3; q++) a.b[q] = c->med[5 + q];
+        a.vp = dm[0]; a.vs = dm[1]; a.rho = dm[2];
+        for (int q = 0; q < 3; q++) a.out[q] = dg[q];
+        const dim3 block(kThreadsK, 2, 2);
+        model_grad_kernel<<<cell_grid(g, block), block, 0, c->stream>>>(a);
+        rc = cuda_check(c, cudaGetLastError(), "model_grad_kernel");
+    }
+    double *ho[3] = {gvp, gvs, grho};
+    for (int q = 0; q < 3 && !rc; q++) rc = fetch_double(c, dg[q], ho[q], ld_k, ld_i);
+    cudaStreamSynchronize(c->stream);
+    for (int q = 0; q < 3; q++) {
+        if (dm[q]) { cudaFree(dm[q]); c->bytes -= (long long)g.ncell * sizeof(float); }
+        if (dg[q]) { cudaFree(dg[q]); c->bytes -= (long long)g.ncell * sizeof(double); }
+    }
+    return rc;
 }

@@ -444,7 +444,8 @@ static void add_entry(const swpc_ctx *c, std::vector<InjEntry> &v, int field, in
     v.push_back(e);
 }
 
-static int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half) {
+namespace swpc {
+int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half) {
     const int nt = c->d.nt;
     std::vector<float> t((size_t)nt * std::max(nsrc, 1), 0.f);
     for (int it = 1; it <= nt; it++) {
@@ -458,6 +459,22 @@ static int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, 
     CK(cudaStreamSynchronize(c->stream));
     return SWPC_OK;
 }
+
+// the six velocity cells of green__source (m_green.f90:615-627) for a unit
+// force along cmp at (ksrc, isrc, jsrc); false when a cell is outside the box
+bool green_entries(const swpc_ctx *c, int isrc, int jsrc, int ksrc, char cmp, std::vector<InjEntry> &v) {
+    // m_green.f90:146-154
+    const float f1[3] = {cmp == 'x' ? 1.0f : 0.0f, cmp == 'y' ? 1.0f : 0.0f, cmp == 'z' ? 1.0f : 0.0f};
+    bool bad = false;
+    add_entry(c, v, SWPC_F_VX, ksrc, isrc, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
+    add_entry(c, v, SWPC_F_VX, ksrc, isrc - 1, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
+    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc, 0, f1[1], INJ_GREEN, 1, &bad);
+    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc - 1, 0, f1[1], INJ_GREEN, 1, &bad);
+    add_entry(c, v, SWPC_F_VZ, ksrc, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
+    add_entry(c, v, SWPC_F_VZ, ksrc - 1, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
+    return !bad;
+}
+}  // namespace swpc
 
 extern "C" int swpc_source_setup(swpc_ctx *c, int nsrc, const int *isrc, const int *jsrc, const int *ksrc,
                                  const float *srcprm, const float *mo, const float *m6, int stftype) {
@@ -581,17 +598,9 @@ extern "C" int swpc_green_setup(swpc_ctx *c, int isrc, int jsrc, int ksrc, char 
     if (cmp != 'x' && cmp != 'y' && cmp != 'z') return set_err(c, SWPC_ERR_ARG, "green_cmp must be x, y or z");
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
-    // m_green.f90:146-154
-    const float f1[3] = {cmp == 'x' ? 1.0f : 0.0f, cmp == 'y' ? 1.0f : 0.0f, cmp == 'z' ? 1.0f : 0.0f};
     std::vector<InjEntry> v;
-    bool bad = false;
-    add_entry(c, v, SWPC_F_VX, ksrc, isrc, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
-    add_entry(c, v, SWPC_F_VX, ksrc, isrc - 1, jsrc, 0, f1[0], INJ_GREEN, 0, &bad);
-    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc, 0, f1[1], INJ_GREEN, 1, &bad);
-    add_entry(c, v, SWPC_F_VY, ksrc, isrc, jsrc - 1, 0, f1[1], INJ_GREEN, 1, &bad);
-    add_entry(c, v, SWPC_F_VZ, ksrc, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
-    add_entry(c, v, SWPC_F_VZ, ksrc - 1, isrc, jsrc, 0, f1[2], INJ_GREEN, 2, &bad);
-    if (bad) return set_err(c, SWPC_ERR_ARG, "green source cell outside the memory box");
+    if (!green_entries(c, isrc, jsrc, ksrc, cmp, v))
+        return set_err(c, SWPC_ERR_ARG, "green source cell outside the memory box");
     bool serial;
     RC(build_list(c, v, &c->inj_green, &c->ninj_green, &serial));
     const float prm[2] = {green_tbeg, green_trise};

@@ -126,6 +126,29 @@ def station_grid(p: Params, kfs: np.ndarray, kob: np.ndarray):
     return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
 
 
+def lhm_model(p: Params, xi: np.ndarray | None = None):
+    """Per-cell (vp, vs, rho, qp, qs) of the layered model, with the lhm_rmed
+    perturbation when ``xi`` is given, over the memory box (vmodel_lhm,
+    m_vmodel_lhm.f90:21-169).  The velocities are recovered from the moduli
+    the vmodel forms (vs = sqrt(mu/rho), vp = sqrt((lam+2mu)/rho))."""
+    lib = _lib.load()
+    g = grid_struct(p)
+    shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+    rho, lam, mu, qp, qs = (np.zeros(shape, np.float32) for _ in range(5))
+    L = p.layers
+    arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
+    if xi is not None:
+        xi = np.ascontiguousarray(xi, np.float32)
+    rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+                             fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, fptr(xi), p.rhomin,
+                             fptr(rho), fptr(lam), fptr(mu), fptr(qp), fptr(qs))
+    if rc:
+        raise ValueError("vmodel_lhm failed")
+    vs = np.sqrt(mu / rho).astype(np.float32)
+    vp = np.sqrt((lam + 2 * mu) / rho).astype(np.float32)
+    return vp, vs, rho, qp, qs
+
+
 class Medium:
     """Host copy of the medium after medium__setup (m_medium.f90:36-467)."""
 
@@ -154,6 +177,33 @@ class Medium:
                                  fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs))
         if rc:
             raise ValueError("vmodel_lhm failed")
+        self._setup(p)
+
+    @classmethod
+    def from_model(cls, p: Params, vp: np.ndarray, vs: np.ndarray, rho: np.ndarray, qp: np.ndarray,
+                   qs: np.ndarray) -> "Medium":
+        """The medium of per-cell vp, vs, rho, Qp, Qs over the memory box
+        (shape (ny+6, nx+6, nz+6), k fastest): the moduli as vmodel_lhm forms
+        them (m_vmodel_lhm.f90:158-160, in FP32 with its operation order),
+        then medium__setup."""
+        self = cls.__new__(cls)
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        f = lambda a: np.ascontiguousarray(a, np.float32).reshape(shape)
+        vp, vs, rho = f(vp), f(vs), f(rho)
+        self.rho = rho.copy()
+        self.mu = rho * vs * vs
+        self.lam = rho * (vp * vp - 2 * vs * vs)
+        self.qp, self.qs = f(qp).copy(), f(qs).copy()
+        for name in self.FIELDS[3:]:
+            setattr(self, name, np.zeros(shape, np.float32))
+        for name in self.MAPS:
+            setattr(self, name, np.zeros(shape[:2], np.int32))
+        self._setup(p)
+        return self
+
+    def _setup(self, p: Params):
+        lib = _lib.load()
+        g = grid_struct(p)
         self.ts = np.zeros(3, np.float32)
         scal = np.zeros(3, np.float32)
         rc = lib.swpc_setup_medium(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
@@ -415,6 +465,18 @@ class Swpc3D:
         assert a.shape == (p.ny + 6, p.nx + 6, p.nz + 6)
         check(self.ctx, self.lib.swpc_upload_field(self.ctx, field, fptr(a), p.nz + 6, p.nx + 6))
 
+    def record(self, stations=None, what: int = _lib.WAV_V):
+        """wav__setup (m_wav.f90:76-142) at ``stations`` (default: the
+        parameter file's), also in green mode, where the reference records
+        no traces; the traces are scaled by this run's M0 and UC."""
+        p = self.p
+        q = Params(**{**p.__dict__, "stations": list(p.stations if stations is None else stations)})
+        self.ist, self.jst, self.kst = station_grid(q, self.medium.kfs, self.medium.kob)
+        self.nst = len(self.ist)
+        check(self.ctx, self.lib.swpc_wav_setup(self.ctx, self.nst, iptr(self.ist), iptr(self.jst), iptr(self.kst),
+                                                p.ntdec_w, what, self.M0, self.UC))
+        self.what = what
+
     def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
         """wav buffer in the reference layout wav(ntw, ncmp, nst), returned as a
         numpy array of shape (nst, ncmp, ntw)."""
@@ -428,3 +490,81 @@ class Swpc3D:
 
     def device_bytes(self) -> int:
         return int(self.lib.swpc_device_bytes(self.ctx))
+
+
+class ForceBatch3D:
+    """Reciprocity batch: one independent wavefield per single force over the
+    medium of ``base`` (a 3D run set up in green mode, whose absorber
+    profiles and recorder the members share).  ``forces`` lists (station,
+    cmp): each member is driven like a green-mode run (green__source,
+    m_green.f90:597-632) with a unit force along cmp ('x', 'y', 'z') at the
+    station's grid cell and the base's green_trise / stftype.  All members
+    advance with one launch per half step."""
+
+    def __init__(self, base: Swpc3D, forces):
+        self.base = base
+        self.lib = base.lib
+        p = base.p
+        b = C.c_void_p()
+        check(base.ctx, self.lib.swpc_fbatch_create(base.ctx, len(forces), C.byref(b)))
+        self.b = b
+        self.n = len(forces)
+        stf = _lib.STF_CODES[p.stftype]
+        self.cells = []
+        for m, (st, cmp) in enumerate(forces):
+            i, j, k = station_grid(Params(**{**p.__dict__, "stations": [st]}), base.medium.kfs, base.medium.kob)
+            if len(i) != 1:
+                raise ValueError(f"force {m}: station outside the domain")
+            self.cells.append((int(i[0]), int(j[0]), int(k[0])))
+            check(base.ctx, self.lib.swpc_fbatch_green_source(b, m, int(i[0]), int(j[0]), int(k[0]),
+                                                              cmp.encode()[0:1], 0.0, p.green_trise, stf))
+
+    def close(self):
+        if self.b:
+            self.lib.swpc_fbatch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, it: int):
+        check(self.base.ctx, self.lib.swpc_fbatch_step(self.b, it))
+
+    def run(self, it0: int, nsteps: int):
+        check(self.base.ctx, self.lib.swpc_fbatch_run(self.b, it0, nsteps))
+        check(self.base.ctx, self.lib.swpc_fbatch_sync(self.b))
+
+    def time_steps(self, it0: int, nsteps: int) -> float:
+        ms = C.c_float()
+        check(self.base.ctx, self.lib.swpc_fbatch_time_steps(self.b, it0, nsteps, C.byref(ms)))
+        return ms.value
+
+    def set_strip(self, cells: int):
+        check(self.base.ctx, self.lib.swpc_fbatch_set_strip(self.b, cells))
+
+    def autotune(self, it0: int, reps: int = 2):
+        """Times the i-strip widths over steps it0..; returns (steps used, strip)."""
+        used, strip = C.c_int(), C.c_int()
+        check(self.base.ctx, self.lib.swpc_fbatch_autotune(self.b, it0, reps, C.byref(used), C.byref(strip)))
+        return used.value, strip.value
+
+    def waveforms(self, member: int, what: int = _lib.WAV_V) -> np.ndarray:
+        base = self.base
+        ncmp = 3 if what in (_lib.WAV_V, _lib.WAV_U) else 6
+        ntw = (base.p.nt - 1) // base.p.ntdec_w + 1
+        out = np.zeros((base.nst, ncmp, ntw), np.float32)
+        check(base.ctx, self.lib.swpc_fbatch_wav_fetch(self.b, member, what, fptr(out)))
+        return out
+
+    def download(self, member: int, field: int) -> np.ndarray:
+        p = self.base.p
+        out = np.zeros((p.ny + 6, p.nx + 6, p.nz + 6), np.float32)
+        check(self.base.ctx, self.lib.swpc_fbatch_download_field(self.b, member, field, fptr(out), p.nz + 6,
+                                                                 p.nx + 6))
+        return out
+
+    def device_bytes(self) -> int:
+        return int(self.lib.swpc_fbatch_device_bytes(self.b))

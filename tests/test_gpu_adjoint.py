@@ -161,3 +161,115 @@ def test_gradient_matches_finite_differences():
     print("misfit", J0, "gradient vs central differences:",
           [(r[0], float(r[2]), float(r[3]), abs(float(r[2]) / float(r[3]) - 1)) for r in rows])
     assert not bad, bad
+
+
+def model_case(nt=70):
+    """Observed data from a model with a slow Gaussian vs blob; the starting
+    model is the layered + random background (both per-cell vp, vs, rho)."""
+    from openswpc_b200.swpc3d import Medium, lhm_model
+    p = small3d(nx=40, ny=36, nz=32, na=8, nt=nt)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    vp, vs, rho, qp, qs = lhm_model(p, xi)
+    jj, ii, kk = np.meshgrid(np.arange(p.ny + 6), np.arange(p.nx + 6), np.arange(p.nz + 6), indexing="ij")
+    blob = np.exp(-((jj - 21.0) ** 2 + (ii - 23.0) ** 2 + (kk - 19.0) ** 2) / (2 * 3.0 ** 2))
+    vs_true = (vs * (1.0 - 0.08 * blob)).astype(np.float32)
+    true = Swpc3D(p, medium=Medium.from_model(p, vp, vs_true, rho, qp, qs))
+    true.run(1, p.nt)
+    obs = true.waveforms(_lib.WAV_V)
+    true.close()
+    return p, (vp, vs, rho, qp, qs), obs
+
+
+def oracle_misfit_double_traces(p, medium, obs, stations, scale):
+    """Misfit of the all-double oracle with its velocity traces formed in
+    double from its FP64 velocity fields (the oracle's own trace buffer is
+    FP32, as wav__store's is, and its rounding would swamp the misfit change
+    of a 1e-3 perturbation of a weakly sensitive cell).  The traces follow
+    wav__store (m_wav.f90:530-535): the two-cell averages of V at the start
+    of each step, times M0 UC 1e9, Vz positive up."""
+    ist, jst, kst = (np.asarray(a) + 2 for a in stations)
+    o = Oracle3D(p, variant="f64", threads=os.cpu_count() or 1, medium=medium)
+    syn = np.zeros((len(ist), 3, p.nt))
+    for it in range(1, p.nt + 1):
+        vx, vy, vz = o.array("Vx"), o.array("Vy"), o.array("Vz")
+        syn[:, 0, it - 1] = (vx[jst, ist, kst] + vx[jst, ist - 1, kst]) / 2 * scale
+        syn[:, 1, it - 1] = (vy[jst, ist, kst] + vy[jst - 1, ist, kst]) / 2 * scale
+        syn[:, 2, it - 1] = -(vz[jst, ist, kst] + vz[jst, ist, kst - 1]) / 2 * scale
+        o.step(it)
+    o.close()
+    r = syn - obs
+    return 0.5 * float(np.sum(r * r))
+
+
+def seeded_cells(p, n, seed=11):
+    """n distinct seeded cells of the solid kernel region, two or more cells
+    inside its edges (whose medium also feeds the absorber)."""
+    rng = np.random.default_rng(seed)
+    cells = set()
+    while len(cells) < n:
+        j = int(rng.integers(p.na + 3, p.ny - p.na - 1))
+        i = int(rng.integers(p.na + 3, p.nx - p.na - 1))
+        k = int(rng.integers(6, p.nz - p.na - 1))
+        cells.add((j + 2, i + 2, k + 2))   # memory-box array index of cell (k, i, j)
+    return sorted(cells)
+
+
+def test_model_gradient_matches_finite_differences_on_20_seeded_cells():
+    """dJ/dvp, dJ/dvs, dJ/drho on 20 seeded cells against central differences
+    (h = 1e-3 relative) of the all-double oracle's misfit, the medium
+    re-derived from the perturbed model each time."""
+    from openswpc_b200.adjoint import Misfit3D
+    from openswpc_b200.swpc3d import Medium
+    p, (vp, vs, rho, qp, qs), obs = model_case()
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, ckpt=16)
+    J, gvp, gvs, grho = prob.gradient(vp, vs, rho)
+    assert abs(J - prob.misfit(vp, vs, rho)) <= 1e-6 * J
+    sv = prob.solver
+    stations = (sv.ist, sv.jst, sv.kst)
+    scale = float(np.float32(sv.M0)) * float(np.float32(sv.UC)) * 1e9
+    prob.close()
+    model = {"vp": vp, "vs": vs, "rho": rho}
+    grads = {"vp": gvp, "vs": gvs, "rho": grho}
+    rows = []
+    for idx in seeded_cells(p, 20):
+        for name in ("vp", "vs", "rho"):
+            arr = model[name]
+            v0 = float(arr[idx])
+            h = 1e-3 * abs(v0)
+            Js = []
+            for sgn in (1.0, -1.0):
+                arr[idx] = np.float32(v0 + sgn * h)
+                m = Medium.from_model(p, vp, vs, rho, qp, qs)
+                Js.append(oracle_misfit_double_traces(p, m, obs, stations, scale))
+            arr[idx] = np.float32(v0)
+            step = (float(np.float32(v0 + h)) - v0) + (v0 - float(np.float32(v0 - h)))
+            rows.append((name, idx, float(grads[name][idx]), (Js[0] - Js[1]) / step))
+    # FD_TOL relative to each cell's own derivative; a cell whose derivative
+    # is below 1 % of the largest of its parameter is held to FD_TOL of 1 %
+    # of that largest value (the FD noise floor of the FP32 medium setup)
+    scale = {n: max(abs(r[3]) for r in rows if r[0] == n) for n in model}
+    bad = [r for r in rows if abs(r[2] - r[3]) > FD_TOL * max(abs(r[3]), 1e-2 * scale[r[0]])]
+    worst = max(abs(r[2] - r[3]) / max(abs(r[3]), 1e-2 * scale[r[0]]) for r in rows)
+    print(f"misfit {J:.6e}; worst relative gradient error over 60 checks {worst:.2e}")
+    assert not bad, bad
+
+
+def test_waveform_misfit_autograd():
+    """torch.autograd through WaveformMisfit gives the library's gradient and
+    the forward misfit; without grad the forward alone runs."""
+    import torch
+    from openswpc_b200.adjoint import Misfit3D, waveform_misfit
+    p, (vp, vs, rho, qp, qs), obs = model_case(nt=40)
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, ckpt=8)
+    tv = [torch.tensor(a, requires_grad=True) for a in (vp, vs, rho)]
+    J = waveform_misfit(*tv, prob)
+    (2.0 * J).backward()
+    J_ref, gvp, gvs, grho = prob.gradient(vp, vs, rho)
+    assert abs(float(J) - J_ref) <= 1e-12 * J_ref
+    for t, g in zip(tv, (gvp, gvs, grho)):
+        assert t.grad.dtype == torch.float32
+        np.testing.assert_allclose(t.grad.numpy(), (2.0 * g).astype(np.float32), rtol=1e-6, atol=0)
+    with torch.no_grad():
+        J2 = waveform_misfit(*[t.detach() for t in tv], prob)
+    assert abs(float(J2) - J_ref) <= 1e-6 * J_ref
+    prob.close()
