@@ -51,8 +51,10 @@ BYTES = {"f32": (232, 152, 60, 132), "bf16r": (160, 152, 60, 132), "f16sr": (136
 FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic of one launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the c1 mix scaled
 # down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
-# algorithmic bytes; profiles/stress3d_kernel_256x256x128_na8.md and profiles/vel3d_kernel_256x256x128_na8.md
-TRAFFIC_PER_ALGORITHMIC = {"stress": 1.988e9 / 1.828028416e9, "vel": 0.652e9 / 0.609632256e9}
+# algorithmic bytes, for the default (TMA-staged) kernels; profiles/stress3d_tma_kernel_256x256x128_na8.md and
+# profiles/vel3d_tma_kernel_256x256x128_na8.md
+TRAFFIC_PER_ALGORITHMIC = {"stress": (1.250347e9 + 0.715447e9) / 1.828028416e9,
+                           "vel": (0.509357e9 + 0.124435e9) / 0.609632256e9}
 
 
 def make_params(name: str):
@@ -868,15 +870,17 @@ def main():
             "storage": {"f32": "S, R FP32", "bf16r": "R BF16", "f16sr": "S, R FP16 (power-of-two scales)"}[args.precision],
             "data": "synthetic (seeded layered + von Karman medium)",
             "config": wl,
-            "roofline": {"bound": "hbm", "kernel": "stress3d_kernel (fused interior + PML stress update)",
+            "roofline": {"bound": "hbm", "kernel": "stress3d_tma_kernel (TMA-staged fused interior + PML stress update)"
+                         if args.precision == "f32" else "stress3d_kernel (fused interior + PML stress update)",
                          "achieved": ach_stress, "peak": peak, "unit": "GB/s", "frac": ach_stress / peak,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
-                         "traffic": b_stress * TRAFFIC_PER_ALGORITHMIC["stress"],
+                         "traffic": b_stress * TRAFFIC_PER_ALGORITHMIC["stress"] if args.precision == "f32" else None,
                          "traffic_source": "ncu DRAM bytes of the 1/64-scale case times 64 (same interior/PML mix)",
                          "algorithmic_bytes_per_launch": b_stress, "launch_ms": t_stress},
-            "roofline_vel": {"kernel": "vel3d_kernel", "achieved": ach_vel, "frac": ach_vel / peak,
-                             "traffic": b_vel * TRAFFIC_PER_ALGORITHMIC["vel"],
+            "roofline_vel": {"kernel": "vel3d_tma_kernel" if args.precision == "f32" else "vel3d_kernel",
+                             "achieved": ach_vel, "frac": ach_vel / peak,
+                             "traffic": b_vel * TRAFFIC_PER_ALGORITHMIC["vel"] if args.precision == "f32" else None,
                              "algorithmic_bytes_per_launch": b_vel, "launch_ms": t_vel},
             "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
                               "algorithmic_bytes_per_step": b_stress + b_vel},

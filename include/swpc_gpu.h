@@ -392,6 +392,14 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * velocity kernels (a 32 x 8 (k, i) tile walking bj planes along j; bi is
  * ignored).  minb = minimum resident blocks per SM the variant is compiled
  * for (1..4; fewer blocks leave more registers for operands in flight).
+ * kernel 4 selects the velocity kernel with four k per thread.  kernel 5 / 6
+ * select the TMA-staged stress / velocity kernels (FP32 3D contexts): a CTA
+ * per tile of kt (k) x bi (i) x bj (j) cells whose operands arrive in shared
+ * memory by bulk tensor copies; here minb selects kt (1: 32, 2: 64), and the
+ * compiled tiles are stress (32,4,4) (32,2,4) (32,4,2) (64,4,2) (64,2,2)
+ * (64,2,4) (64,4,1), velocity (32,4,2) (32,4,4) (32,2,2) (64,4,2) (64,2,2)
+ * (64,4,1) (64,2,4) (64,4,4).  FP32 3D contexts start with kernels 5 (32,4,4)
+ * and 6 (32,4,2); the other forms start with kernels 0 and 1.
  * The defaults come from sweeps on B200.  No counterpart in the reference
  * (its OpenMP/OpenACC schedules are fixed at compile time); results are
  * bitwise independent of the variant. */

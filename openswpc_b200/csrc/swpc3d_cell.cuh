@@ -52,6 +52,172 @@ __device__ __forceinline__ void stR(float *p, long long e, float v, float is) {
     else __stcs(p + e, v);
 }
 
+// 2nd-order band of the free surface / ocean bottom (m_kernel.f90:103-108):
+// isign = sign(1, max(...)) = +1 -> index 1 of the coefficient pairs
+__device__ __forceinline__ int band_sign_of(const int4 *band, long long col, int k) {
+    const int4 bd = __ldg(&band[col]);
+    const int p1 = (k - bd.x) * (bd.y - k);
+    const int p2 = (k - bd.z) * (bd.w - k);
+    return ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;
+}
+
+// Operands of the interior updates.  The one-cell kernels read them from
+// global memory (GVelOps, GStrOps); the staged kernels (swpc3d_tma.cu) from
+// the tiles that TMA copied to shared memory.  s(f, dk, di, dj) is stress
+// component f (xx yy zz yz xz xy) at (k+dk, i+di, j+dj), v(c, ...) velocity
+// component c (x y z).
+template <int PREC>
+struct GVelOps {
+    const Vel3Args &a;
+    long long e, PI, PJ;
+    const float *S[6];
+    const float *V[3];
+    __device__ __forceinline__ float v(int c) const { return lds(&V[c][e]); }
+    __device__ __forceinline__ float b(int c) const { return lds(&(c == 0 ? a.bx : c == 1 ? a.by : a.bz)[e]); }
+    __device__ __forceinline__ float s(int f, int dk, int di, int dj) const {
+        return ldgS<PREC>(S[f], e + dk + di * PI + dj * PJ, a.sS[f]);
+    }
+};
+
+// kernel__update_vel (m_kernel.f90:103-125) for one interior cell
+template <int PREC, class Ops>
+__device__ __forceinline__ void vel_interior(const Vel3Args &a, const Ops &o, int s, float *Vx, float *Vy, float *Vz,
+                                             long long e) {
+    const float dt = a.dt;
+    const float vx = o.v(0), vy = o.v(1), vz = o.v(2);
+    const float bx = o.b(0), by = o.b(1), bz = o.b(2);
+    const float xx0 = o.s(0, 0, 0, 0), xxp = o.s(0, 0, 1, 0), xxp2 = o.s(0, 0, 2, 0), xxm = o.s(0, 0, -1, 0);
+    const float yy0 = o.s(1, 0, 0, 0), yyp = o.s(1, 0, 0, 1), yyp2 = o.s(1, 0, 0, 2), yym = o.s(1, 0, 0, -1);
+    const float zz0 = o.s(2, 0, 0, 0), zzp = o.s(2, 1, 0, 0), zzp2 = o.s(2, 2, 0, 0), zzm = o.s(2, -1, 0, 0);
+    const float xy0 = o.s(5, 0, 0, 0);
+    const float xyjm = o.s(5, 0, 0, -1), xyjp = o.s(5, 0, 0, 1), xyjm2 = o.s(5, 0, 0, -2);
+    const float xyim = o.s(5, 0, -1, 0), xyip = o.s(5, 0, 1, 0), xyim2 = o.s(5, 0, -2, 0);
+    const float xz0 = o.s(4, 0, 0, 0);
+    const float xzkm = o.s(4, -1, 0, 0), xzkp = o.s(4, 1, 0, 0), xzkm2 = o.s(4, -2, 0, 0);
+    const float xzim = o.s(4, 0, -1, 0), xzip = o.s(4, 0, 1, 0), xzim2 = o.s(4, 0, -2, 0);
+    const float yz0 = o.s(3, 0, 0, 0);
+    const float yzkm = o.s(3, -1, 0, 0), yzkp = o.s(3, 1, 0, 0), yzkm2 = o.s(3, -2, 0, 0);
+    const float yzjm = o.s(3, 0, 0, -1), yzjp = o.s(3, 0, 0, 1), yzjm2 = o.s(3, 0, 0, -2);
+    const float re40x = a.e40[0][s], re41x = a.e41[0][s];
+    const float re40y = a.e40[1][s], re41y = a.e41[1][s];
+    const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+
+    const float d3Sx3 = (xxp - xx0) * re40x - (xxp2 - xxm) * re41x
+                      + (xy0 - xyjm) * re40y - (xyjp - xyjm2) * re41y
+                      + (xz0 - xzkm) * re40z - (xzkp - xzkm2) * re41z;
+    const float d3Sy3 = (xy0 - xyim) * re40x - (xyip - xyim2) * re41x
+                      + (yyp - yy0) * re40y - (yyp2 - yym) * re41y
+                      + (yz0 - yzkm) * re40z - (yzkp - yzkm2) * re41z;
+    const float d3Sz3 = (xz0 - xzim) * re40x - (xzip - xzim2) * re41x
+                      + (yz0 - yzjm) * re40y - (yzjp - yzjm2) * re41y
+                      + (zzp - zz0) * re40z - (zzp2 - zzm) * re41z;
+    sts(&Vx[e], vx + bx * d3Sx3 * dt);
+    sts(&Vy[e], vy + by * d3Sy3 * dt);
+    sts(&Vz[e], vz + bz * d3Sz3 * dt);
+}
+
+template <int NM, int PREC>
+struct GStrOps {
+    const Str3Args &a;
+    long long e, PI, PJ, so;
+    const float *V[3];
+    const float *S[6];
+    __device__ __forceinline__ float v(int c, int dk, int di, int dj) const {
+        return __ldg(&V[c][e + dk + di * PI + dj * PJ]);
+    }
+    __device__ __forceinline__ float sown(int f) const { return ldS<PREC>(S[f], e, a.sS[f]); }
+    __device__ __forceinline__ float r(int q) const { return ldR<PREC>(a.R[q] + so, e, a.sR[q]); }
+    // 0 mu, 1 lam, 2 taup, 3 taus, 4 muyz, 5 muxz, 6 muxy
+    __device__ __forceinline__ float med(int m) const {
+        const float *p = m == 0 ? a.mu : m == 1 ? a.lam : m == 2 ? a.taup : m == 3 ? a.taus
+                       : m == 4 ? a.muyz : m == 5 ? a.muxz : a.muxy;
+        return lds(&p[e]);
+    }
+};
+
+// kernel__update_stress (m_kernel.f90:176-321) for one interior cell: every
+// operand first (see vel_cell), then the normal and shear components and the
+// memory variables, stored at e of the given arrays
+template <int NM, int PREC, class Ops>
+__device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o, int s, float *const (&S)[6],
+                                                long long e, long long so) {
+    const float dt = a.dt;
+    float r[6][NM > 0 ? NM : 1];
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+#pragma unroll
+        for (int m = 0; m < NM; m++) r[c][m] = o.r(c * 3 + m);
+    const float sxx = o.sown(0), syy = o.sown(1), szz = o.sown(2);
+    const float syz = o.sown(3), sxz = o.sown(4), sxy = o.sown(5);
+    const float mu = o.med(0), lam = o.med(1);
+    const float taup1 = o.med(2), taus1 = o.med(3);
+    const float muyz = o.med(4), muxz = o.med(5), muxy = o.med(6);
+    const float vx0 = o.v(0, 0, 0, 0), vy0 = o.v(1, 0, 0, 0), vz0 = o.v(2, 0, 0, 0);
+    const float vxim = o.v(0, 0, -1, 0), vxip = o.v(0, 0, 1, 0), vxim2 = o.v(0, 0, -2, 0);
+    const float vxjp = o.v(0, 0, 0, 1), vxjp2 = o.v(0, 0, 0, 2), vxjm = o.v(0, 0, 0, -1);
+    const float vxkp = o.v(0, 1, 0, 0), vxkp2 = o.v(0, 2, 0, 0), vxkm = o.v(0, -1, 0, 0);
+    const float vyjm = o.v(1, 0, 0, -1), vyjp = o.v(1, 0, 0, 1), vyjm2 = o.v(1, 0, 0, -2);
+    const float vyip = o.v(1, 0, 1, 0), vyip2 = o.v(1, 0, 2, 0), vyim = o.v(1, 0, -1, 0);
+    const float vykp = o.v(1, 1, 0, 0), vykp2 = o.v(1, 2, 0, 0), vykm = o.v(1, -1, 0, 0);
+    const float vzkm = o.v(2, -1, 0, 0), vzkp = o.v(2, 1, 0, 0), vzkm2 = o.v(2, -2, 0, 0);
+    const float vzip = o.v(2, 0, 1, 0), vzip2 = o.v(2, 0, 2, 0), vzim = o.v(2, 0, -1, 0);
+    const float vzjp = o.v(2, 0, 0, 1), vzjp2 = o.v(2, 0, 0, 2), vzjm = o.v(2, 0, 0, -1);
+    const float re40x = a.e40[0][s], re41x = a.e41[0][s];
+    const float re40y = a.e40[1][s], re41y = a.e41[1][s];
+    const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+
+    // normal components (m_kernel.f90:195-235)
+    const float dxVx = (vx0 - vxim) * re40x - (vxip - vxim2) * re41x;
+    const float dyVy = (vy0 - vyjm) * re40y - (vyjp - vyjm2) * re41y;
+    const float dzVz = (vz0 - vzkm) * re40z - (vzkp - vzkm2) * re41z;
+    const float mu2 = 2 * mu;
+    const float lam2mu = lam + mu2;
+    const float d3v3 = dxVx + dyVy + dzVz;
+    const float dyVy_dzVz = dyVy + dzVz;
+    const float dxVx_dzVz = dxVx + dzVz;
+    const float dxVx_dyVy = dxVx + dyVy;
+    float Rxx_n = 0.0f, Ryy_n = 0.0f, Rzz_n = 0.0f;
+#pragma unroll
+    for (int m = 0; m < NM; m++) {
+        r[0][m] = a.c1[m] * r[0][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dyVy_dzVz) * dt;
+        r[1][m] = a.c1[m] * r[1][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dzVz) * dt;
+        r[2][m] = a.c1[m] * r[2][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dyVy) * dt;
+        Rxx_n = Rxx_n + a.d1[m] * r[0][m];
+        Ryy_n = Ryy_n + a.d1[m] * r[1][m];
+        Rzz_n = Rzz_n + a.d1[m] * r[2][m];
+    }
+    const float taup_plus1 = 1 + taup1 * (1 + a.d2);
+    const float taus_plus1 = 1 + taus1 * (1 + a.d2);
+    stS<PREC>(S[0], e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, a.iS[0]);
+    stS<PREC>(S[1], e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, a.iS[1]);
+    stS<PREC>(S[2], e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, a.iS[2]);
+
+    // shear components (m_kernel.f90:282-311)
+    const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
+                          + (vxjp - vx0) * re40y - (vxjp2 - vxjm) * re41y;
+    const float dxVz_dzVx = (vzip - vz0) * re40x - (vzip2 - vzim) * re41x
+                          + (vxkp - vx0) * re40z - (vxkp2 - vxkm) * re41z;
+    const float dyVz_dzVy = (vzjp - vz0) * re40y - (vzjp2 - vzjm) * re41y
+                          + (vykp - vy0) * re40z - (vykp2 - vykm) * re41z;
+    float Ryz_n = 0.0f, Rxz_n = 0.0f, Rxy_n = 0.0f;
+#pragma unroll
+    for (int m = 0; m < NM; m++) {
+        r[3][m] = a.c1[m] * r[3][m] - a.c2[m] * muyz * taus1 * dyVz_dzVy * dt;
+        r[4][m] = a.c1[m] * r[4][m] - a.c2[m] * muxz * taus1 * dxVz_dzVx * dt;
+        r[5][m] = a.c1[m] * r[5][m] - a.c2[m] * muxy * taus1 * dxVy_dyVx * dt;
+        Ryz_n = Ryz_n + a.d1[m] * r[3][m];
+        Rxz_n = Rxz_n + a.d1[m] * r[4][m];
+        Rxy_n = Rxy_n + a.d1[m] * r[5][m];
+    }
+    stS<PREC>(S[3], e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, a.iS[3]);
+    stS<PREC>(S[4], e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, a.iS[4]);
+    stS<PREC>(S[5], e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, a.iS[5]);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+#pragma unroll
+        for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], a.iR[c * 3 + m]);
+}
+
 // ---------------------------------------------------------------------------
 // velocity: kernel__update_vel (m_kernel.f90:75-140) +
 //           absorb_p__update_vel (m_absorb_p.f90:248-309)
@@ -82,40 +248,8 @@ __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j,
 
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         if (!(a.mask & 1)) return;
-        const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
-        const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
-        const float xx0 = ldgS<PREC>(Sxx, e, a.sS[0]), xxp = ldgS<PREC>(Sxx, e + PI, a.sS[0]), xxp2 = ldgS<PREC>(Sxx, e + 2 * PI, a.sS[0]), xxm = ldgS<PREC>(Sxx, e - PI, a.sS[0]);
-        const float yy0 = ldgS<PREC>(Syy, e, a.sS[1]), yyp = ldgS<PREC>(Syy, e + PJ, a.sS[1]), yyp2 = ldgS<PREC>(Syy, e + 2 * PJ, a.sS[1]), yym = ldgS<PREC>(Syy, e - PJ, a.sS[1]);
-        const float zz0 = ldgS<PREC>(Szz, e, a.sS[2]), zzp = ldgS<PREC>(Szz, e + 1, a.sS[2]), zzp2 = ldgS<PREC>(Szz, e + 2, a.sS[2]), zzm = ldgS<PREC>(Szz, e - 1, a.sS[2]);
-        const float xy0 = ldgS<PREC>(Sxy, e, a.sS[5]);
-        const float xyjm = ldgS<PREC>(Sxy, e - PJ, a.sS[5]), xyjp = ldgS<PREC>(Sxy, e + PJ, a.sS[5]), xyjm2 = ldgS<PREC>(Sxy, e - 2 * PJ, a.sS[5]);
-        const float xyim = ldgS<PREC>(Sxy, e - PI, a.sS[5]), xyip = ldgS<PREC>(Sxy, e + PI, a.sS[5]), xyim2 = ldgS<PREC>(Sxy, e - 2 * PI, a.sS[5]);
-        const float xz0 = ldgS<PREC>(Sxz, e, a.sS[4]);
-        const float xzkm = ldgS<PREC>(Sxz, e - 1, a.sS[4]), xzkp = ldgS<PREC>(Sxz, e + 1, a.sS[4]), xzkm2 = ldgS<PREC>(Sxz, e - 2, a.sS[4]);
-        const float xzim = ldgS<PREC>(Sxz, e - PI, a.sS[4]), xzip = ldgS<PREC>(Sxz, e + PI, a.sS[4]), xzim2 = ldgS<PREC>(Sxz, e - 2 * PI, a.sS[4]);
-        const float yz0 = ldgS<PREC>(Syz, e, a.sS[3]);
-        const float yzkm = ldgS<PREC>(Syz, e - 1, a.sS[3]), yzkp = ldgS<PREC>(Syz, e + 1, a.sS[3]), yzkm2 = ldgS<PREC>(Syz, e - 2, a.sS[3]);
-        const float yzjm = ldgS<PREC>(Syz, e - PJ, a.sS[3]), yzjp = ldgS<PREC>(Syz, e + PJ, a.sS[3]), yzjm2 = ldgS<PREC>(Syz, e - 2 * PJ, a.sS[3]);
-        const int4 bd = __ldg(&a.band[col]);
-        const int p1 = (k - bd.x) * (bd.y - k);
-        const int p2 = (k - bd.z) * (bd.w - k);
-        const int s = ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;   // isign = +1 -> 2nd-order band
-        const float re40x = a.e40[0][s], re41x = a.e41[0][s];
-        const float re40y = a.e40[1][s], re41y = a.e41[1][s];
-        const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-
-        const float d3Sx3 = (xxp - xx0) * re40x - (xxp2 - xxm) * re41x
-                          + (xy0 - xyjm) * re40y - (xyjp - xyjm2) * re41y
-                          + (xz0 - xzkm) * re40z - (xzkp - xzkm2) * re41z;
-        const float d3Sy3 = (xy0 - xyim) * re40x - (xyip - xyim2) * re41x
-                          + (yyp - yy0) * re40y - (yyp2 - yym) * re41y
-                          + (yz0 - yzkm) * re40z - (yzkp - yzkm2) * re41z;
-        const float d3Sz3 = (xz0 - xzim) * re40x - (xzip - xzim2) * re41x
-                          + (yz0 - yzjm) * re40y - (yzjp - yzjm2) * re41y
-                          + (zzp - zz0) * re40z - (zzp2 - zzm) * re41z;
-        sts(&Vx[e], vx + bx * d3Sx3 * dt);
-        sts(&Vy[e], vy + by * d3Sy3 * dt);
-        sts(&Vz[e], vz + bz * d3Sz3 * dt);
+        const GVelOps<PREC> o{a, e, PI, PJ, {Sxx, Syy, Szz, Syz, Sxz, Sxy}, {Vx, Vy, Vz}};
+        vel_interior<PREC>(a, o, band_sign_of(a.band, col, k), Vx, Vy, Vz, e);
         return;
     }
 
@@ -204,85 +338,9 @@ __device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int
 
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         if (!(a.mask & 1)) return;
-        // every operand of the cell first (see the velocity kernel)
-        float r[6][NM > 0 ? NM : 1];
-#pragma unroll
-        for (int c = 0; c < 6; c++)
-#pragma unroll
-            for (int m = 0; m < NM; m++) r[c][m] = ldR<PREC>(a.R[c * 3 + m] + so, e, a.sR[c * 3 + m]);
-        const float sxx = ldS<PREC>(Sxx, e, a.sS[0]), syy = ldS<PREC>(Syy, e, a.sS[1]), szz = ldS<PREC>(Szz, e, a.sS[2]);
-        const float syz = ldS<PREC>(Syz, e, a.sS[3]), sxz = ldS<PREC>(Sxz, e, a.sS[4]), sxy = ldS<PREC>(Sxy, e, a.sS[5]);
-        const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
-        const float taup1 = lds(&a.taup[e]), taus1 = lds(&a.taus[e]);
-        const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
-        const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
-        const float vxim = __ldg(&Vx[e - PI]), vxip = __ldg(&Vx[e + PI]), vxim2 = __ldg(&Vx[e - 2 * PI]);
-        const float vxjp = __ldg(&Vx[e + PJ]), vxjp2 = __ldg(&Vx[e + 2 * PJ]), vxjm = __ldg(&Vx[e - PJ]);
-        const float vxkp = __ldg(&Vx[e + 1]), vxkp2 = __ldg(&Vx[e + 2]), vxkm = __ldg(&Vx[e - 1]);
-        const float vyjm = __ldg(&Vy[e - PJ]), vyjp = __ldg(&Vy[e + PJ]), vyjm2 = __ldg(&Vy[e - 2 * PJ]);
-        const float vyip = __ldg(&Vy[e + PI]), vyip2 = __ldg(&Vy[e + 2 * PI]), vyim = __ldg(&Vy[e - PI]);
-        const float vykp = __ldg(&Vy[e + 1]), vykp2 = __ldg(&Vy[e + 2]), vykm = __ldg(&Vy[e - 1]);
-        const float vzkm = __ldg(&Vz[e - 1]), vzkp = __ldg(&Vz[e + 1]), vzkm2 = __ldg(&Vz[e - 2]);
-        const float vzip = __ldg(&Vz[e + PI]), vzip2 = __ldg(&Vz[e + 2 * PI]), vzim = __ldg(&Vz[e - PI]);
-        const float vzjp = __ldg(&Vz[e + PJ]), vzjp2 = __ldg(&Vz[e + 2 * PJ]), vzjm = __ldg(&Vz[e - PJ]);
-        const int4 bd = __ldg(&a.band[col]);
-        const int p1 = (k - bd.x) * (bd.y - k);
-        const int p2 = (k - bd.z) * (bd.w - k);
-        const int s = ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;
-        const float re40x = a.e40[0][s], re41x = a.e41[0][s];
-        const float re40y = a.e40[1][s], re41y = a.e41[1][s];
-        const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-
-        // normal components (m_kernel.f90:195-235)
-        const float dxVx = (vx0 - vxim) * re40x - (vxip - vxim2) * re41x;
-        const float dyVy = (vy0 - vyjm) * re40y - (vyjp - vyjm2) * re41y;
-        const float dzVz = (vz0 - vzkm) * re40z - (vzkp - vzkm2) * re41z;
-        const float mu2 = 2 * mu;
-        const float lam2mu = lam + mu2;
-        const float d3v3 = dxVx + dyVy + dzVz;
-        const float dyVy_dzVz = dyVy + dzVz;
-        const float dxVx_dzVz = dxVx + dzVz;
-        const float dxVx_dyVy = dxVx + dyVy;
-        float Rxx_n = 0.0f, Ryy_n = 0.0f, Rzz_n = 0.0f;
-#pragma unroll
-        for (int m = 0; m < NM; m++) {
-            r[0][m] = a.c1[m] * r[0][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dyVy_dzVz) * dt;
-            r[1][m] = a.c1[m] * r[1][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dzVz) * dt;
-            r[2][m] = a.c1[m] * r[2][m] - a.c2[m] * (lam2mu * taup1 * d3v3 - mu2 * taus1 * dxVx_dyVy) * dt;
-            Rxx_n = Rxx_n + a.d1[m] * r[0][m];
-            Ryy_n = Ryy_n + a.d1[m] * r[1][m];
-            Rzz_n = Rzz_n + a.d1[m] * r[2][m];
-        }
-        const float taup_plus1 = 1 + taup1 * (1 + a.d2);
-        const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-        stS<PREC>(Sxx, e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, a.iS[0]);
-        stS<PREC>(Syy, e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, a.iS[1]);
-        stS<PREC>(Szz, e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, a.iS[2]);
-
-        // shear components (m_kernel.f90:282-311)
-        const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
-                              + (vxjp - vx0) * re40y - (vxjp2 - vxjm) * re41y;
-        const float dxVz_dzVx = (vzip - vz0) * re40x - (vzip2 - vzim) * re41x
-                              + (vxkp - vx0) * re40z - (vxkp2 - vxkm) * re41z;
-        const float dyVz_dzVy = (vzjp - vz0) * re40y - (vzjp2 - vzjm) * re41y
-                              + (vykp - vy0) * re40z - (vykp2 - vykm) * re41z;
-        float Ryz_n = 0.0f, Rxz_n = 0.0f, Rxy_n = 0.0f;
-#pragma unroll
-        for (int m = 0; m < NM; m++) {
-            r[3][m] = a.c1[m] * r[3][m] - a.c2[m] * muyz * taus1 * dyVz_dzVy * dt;
-            r[4][m] = a.c1[m] * r[4][m] - a.c2[m] * muxz * taus1 * dxVz_dzVx * dt;
-            r[5][m] = a.c1[m] * r[5][m] - a.c2[m] * muxy * taus1 * dxVy_dyVx * dt;
-            Ryz_n = Ryz_n + a.d1[m] * r[3][m];
-            Rxz_n = Rxz_n + a.d1[m] * r[4][m];
-            Rxy_n = Rxy_n + a.d1[m] * r[5][m];
-        }
-        stS<PREC>(Syz, e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, a.iS[3]);
-        stS<PREC>(Sxz, e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, a.iS[4]);
-        stS<PREC>(Sxy, e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, a.iS[5]);
-#pragma unroll
-        for (int c = 0; c < 6; c++)
-#pragma unroll
-            for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], a.iR[c * 3 + m]);
+        const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}};
+        float *const Sp[6] = {Sxx, Syy, Szz, Syz, Sxz, Sxy};
+        stress_interior<NM, PREC>(a, o, band_sign_of(a.band, col, k), Sp, e, so);
         return;
     }
 

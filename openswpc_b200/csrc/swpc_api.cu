@@ -18,6 +18,7 @@
 #include "swpc_ctx.h"
 #include "swpc_host.h"
 #include "swpc_kernels.cuh"
+#include "swpc_tma.h"
 
 using namespace swpc;
 
@@ -124,7 +125,31 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     g.Jp = d->kind == SWPC_KIND_3D ? ny + 6 : 1;
     g.ncell = (long long)g.Kp * g.Ip * g.Jp;
     int rc = 0;
-    if (is3d(c)) {
+    if (is3d(c) && c->prec == SWPC_PREC_F32) {
+        // one slab: 0-2 V, 3-8 S, 9-15 lam mu taup taus muyz muxz muxy, R, bx by bz
+        const int nf = 3 + 6 + 7 + 6 * d->nm + 3;
+        rc = dalloc(c, &c->slab, (size_t)nf * g.ncell);
+        if (!rc) {
+            auto F = [&](int f) { return c->slab + (size_t)f * g.ncell; };
+            for (int q = 0; q < 3; q++) c->V[q] = F(q);
+            for (int q = 0; q < 6; q++) c->S[q] = F(3 + q);
+            const int mq[7] = {1, 2, 3, 4, 8, 9, 10};
+            for (int q = 0; q < 7; q++) c->med[mq[q]] = F(9 + q);
+            for (int comp = 0; comp < 6; comp++)
+                for (int m = 0; m < d->nm; m++) c->R[comp * 3 + m] = F(16 + comp * d->nm + m);
+            for (int q = 0; q < 3; q++) c->med[5 + q] = F(16 + 6 * d->nm + q);
+            c->slab_nf = nf;
+            // the TMA-staged kernels are the default launch of FP32 3D contexts
+            c->stress_tma = true;
+            c->vel_tma = true;
+        }
+        const long long ncol = (long long)g.Ip * g.Jp;
+        if (!rc) rc = dalloc(c, &c->band, ncol);
+        if (!rc) rc = dalloc(c, &c->pmlcol, ncol);
+        if (!rc) rc = dalloc(c, &c->kob, ncol);
+        if (!rc) rc = dalloc(c, &c->kfs, ncol);
+        if (!rc) rc = dalloc(c, &c->d_err, 1);
+    } else if (is3d(c)) {
         for (int q = 0; q < 3 && !rc; q++) rc = dalloc(c, &c->V[q], g.ncell);
         // 2-byte storage (FP16 / BF16) takes half the floats
         const long long nS = c->prec == SWPC_PREC_F16_SR ? (g.ncell + 1) / 2 : g.ncell;
@@ -158,6 +183,16 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     snap_free(c);
     adj_free(c);
     if (!is3d(c)) destroy_2d(c);
+    if (c->slab) {
+        // the slab holds V, S, R and the 3D medium fields
+        cudaFree(c->slab);
+        for (auto &p : c->V) p = nullptr;
+        for (auto &p : c->S) p = nullptr;
+        for (auto &p : c->R) p = nullptr;
+        for (auto &p : c->med) p = nullptr;
+    }
+    if (c->d_err) cudaFree(c->d_err);
+    delete static_cast<TmaMaps *>(c->tmaps);
     void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
                   c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
                   c->wav[1], c->wav[2], c->wav[3], c->uacc, c->eacc, c->vmax_buf, c->d_it};
@@ -183,18 +218,34 @@ extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes 
 
 extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj) {
     if (!c) return SWPC_ERR_ARG;
-    if (kernel < 0 || kernel > 4 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
+    if (kernel < 0 || kernel > 6 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
         ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
-        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..4, minb 1..4, 32*bi*bj <= 256)");
+        return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..6, minb 1..4, 32*bi*bj <= 256)");
     if (kernel >= 2 && c->prec != SWPC_PREC_F32)
         return set_err(c, SWPC_ERR_ARG, "reduced-precision storage runs the kernels 0 and 1 only");
+    // staged kernels: minb selects the tile's k extent (1: 32 cells, 2: 64 cells)
+    if (kernel >= 5 && (!is3d(c) || !c->slab || minb > 2 ||
+                        !(kernel == 5 ? tma_shape_ok(32 * minb, bi, bj) : tma_vel_shape_ok(32 * minb, bi, bj))))
+        return set_err(c, SWPC_ERR_ARG, "staged kernels: 3D FP32 only, with a compiled tile shape (kt, bi, bj)");
     invalidate_graph(c);
     switch (kernel) {
-    case 0: c->stress_march = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
-    case 1: c->vel_march = false; c->vel_vec = false; c->vel_minb = minb; c->vbi = bi; c->vbj = bj; break;
-    case 2: c->stress_march = true; c->stress_mminb = minb; c->stress_jc = bj; break;
-    case 3: c->vel_march = true; c->vel_vec = false; c->vel_mminb = minb; c->vel_jc = bj; break;
-    default: c->vel_march = false; c->vel_vec = true; c->vel_vminb = minb; c->vel_vbi = bi; c->vel_vbj = bj; break;
+    case 0: c->stress_march = false; c->stress_tma = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
+    case 1:
+        c->vel_march = false; c->vel_vec = false; c->vel_tma = false; c->vel_minb = minb; c->vbi = bi; c->vbj = bj;
+        break;
+    case 2: c->stress_march = true; c->stress_tma = false; c->stress_mminb = minb; c->stress_jc = bj; break;
+    case 3: c->vel_march = true; c->vel_vec = false; c->vel_tma = false; c->vel_mminb = minb; c->vel_jc = bj; break;
+    case 4:
+        c->vel_march = false; c->vel_vec = true; c->vel_tma = false; c->vel_vminb = minb; c->vel_vbi = bi;
+        c->vel_vbj = bj;
+        break;
+    case 5:
+        c->stress_march = false; c->stress_tma = true; c->stress_tkt = 32 * minb; c->stress_tbi = bi; c->stress_tbj = bj;
+        break;
+    default:
+        c->vel_march = false; c->vel_vec = false; c->vel_tma = true; c->vel_tkt = 32 * minb; c->vel_tbi = bi;
+        c->vel_tbj = bj;
+        break;
     }
     return SWPC_OK;
 }
@@ -202,6 +253,11 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
 extern "C" int swpc_sync(swpc_ctx *c) {
     if (!c) return SWPC_ERR_ARG;
     CK(cudaStreamSynchronize(c->stream));
+    if (c->d_err) {
+        int h = 0;
+        CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) return set_err(c, SWPC_ERR_CUDA, "a staged tile copy did not complete (TMA wait timed out)");
+    }
     return SWPC_OK;
 }
 
@@ -689,6 +745,29 @@ static void fill_geo_common(const swpc_ctx *c, Geo &g, int &ibk, int &iek, int &
     g = c->g; ibk = c->ibk; iek = c->iek; jbk = c->jbk; jek = c->jek; kek = c->kek;
 }
 
+// tensor maps of the staged kernels for the selected tile shapes
+static int tma_ready(swpc_ctx *c) {
+    const int key[6] = {c->stress_tkt, c->stress_tbi, c->stress_tbj, c->vel_tkt, c->vel_tbi, c->vel_tbj};
+    if (c->tmaps && std::equal(key, key + 6, c->tma_key)) return SWPC_OK;
+    if (!c->tmaps) c->tmaps = new TmaMaps();
+    TmaMaps &m = *static_cast<TmaMaps *>(c->tmaps);
+    if (!tma_encode_stress(m, c->slab, c->g, c->slab_nf, c->d.nm, key[0], key[1], key[2]) ||
+        !tma_encode_vel(m, c->slab, c->g, c->slab_nf, key[3], key[4], key[5]))
+        return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the field slab");
+    std::copy(key, key + 6, c->tma_key);
+    return SWPC_OK;
+}
+
+static TmaTiles tma_tiles(const swpc_ctx *c, int kt, int bi, int bj) {
+    TmaTiles t;
+    t.nkt = (c->g.nz + kt - 1) / kt;
+    t.nit = (c->g.nx + bi - 1) / bi;
+    t.njt = (c->g.ny + bj - 1) / bj;
+    t.b_field = 16 + 6 * c->d.nm;
+    t.err = c->d_err;
+    return t;
+}
+
 static int launch_stress(swpc_ctx *c, int mask) {
     RC(check_ready(c));
     if (!is3d(c)) return update_stress_2d(c, mask);
@@ -712,6 +791,12 @@ static int launch_stress(swpc_ctx *c, int mask) {
     for (int q = 0; q < 18; q++) { a.sR[q] = ldexpf(1.0f, c->eR[q]); a.iR[q] = ldexpf(1.0f, -c->eR[q]); }
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
+    if (c->stress_tma && c->slab) {
+        RC(tma_ready(c));
+        const TmaTiles t = tma_tiles(c, c->stress_tkt, c->stress_tbi, c->stress_tbj);
+        return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tkt,
+                                                 c->stress_tbi, c->stress_tbj, c->stream), "stress3d_tma launch");
+    }
     if (c->stress_march && c->prec == SWPC_PREC_F32)
         launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
     else launch_stress3d(a, c->d.nm, c->stress_minb, c->prec, grid, block, c->stream);
@@ -736,6 +821,12 @@ static int launch_vel(swpc_ctx *c, int mask) {
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
     for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
+    if (c->vel_tma && c->slab) {
+        RC(tma_ready(c));
+        const TmaTiles t = tma_tiles(c, c->vel_tkt, c->vel_tbi, c->vel_tbj);
+        return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tkt, c->vel_tbi,
+                                              c->vel_tbj, c->stream), "vel3d_tma launch");
+    }
     if (c->prec != SWPC_PREC_F32) launch_vel3d(a, c->vel_minb, c->prec, grid, block, c->stream);
     else if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);
     else if (c->vel_march) launch_vel3d_march(a, c->vel_mminb, c->vel_jc, c->stream);

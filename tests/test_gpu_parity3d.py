@@ -265,10 +265,12 @@ def test_larger_grid_against_oracle_few_steps():
 
 @pytest.mark.parametrize("variant", [(0, 2, 2, 1, 1, 4, 2, 2), (0, 1, 4, 2, 1, 3, 8, 1), (2, 2, 1, 16, 3, 2, 1, 7),
                                      (2, 1, 1, 64, 3, 1, 1, 3), (0, 2, 2, 1, 4, 2, 2, 2), (0, 2, 2, 1, 4, 1, 4, 1),
-                                     (0, 2, 2, 1, 4, 3, 1, 2)])
+                                     (0, 2, 2, 1, 4, 3, 1, 2), (5, 1, 4, 2, 6, 1, 4, 2), (5, 1, 2, 4, 6, 1, 4, 4),
+                                     (5, 1, 4, 4, 6, 1, 2, 2), (5, 2, 4, 2, 6, 2, 4, 2), (5, 2, 2, 2, 6, 2, 2, 2),
+                                     (5, 2, 2, 4, 6, 2, 4, 1), (5, 2, 4, 1, 6, 2, 2, 4), (5, 2, 4, 2, 6, 2, 4, 4)])
 def test_launch_variants_are_bitwise_identical(variant):
-    """Flat, marching and four-cells-per-thread kernels, any block shape or
-    chunk length: same bits.  nz = 70 with na = 8 puts the interior/absorber
+    """Flat, marching, four-cells-per-thread and TMA-staged kernels (5, 6),
+    any block shape, chunk length or tile: same bits.  nz = 70 with na = 8 puts the interior/absorber
     boundary inside a group of four and ends the column mid-group."""
     ks, ms, bis, bjs, kv, mv, biv, bjv = variant
     p = small3d(nx=44, ny=38, nz=70, na=8, nt=25)
@@ -282,3 +284,18 @@ def test_launch_variants_are_bitwise_identical(variant):
         assert same_bits(g0.download(n), g1.download(n)), n
     for q in range(18):
         assert same_bits(g0.download(_lib.F_AUX + q), g1.download(_lib.F_AUX + q)), q
+
+
+@pytest.mark.parametrize("nm", [0, 1, 2])
+def test_staged_kernels_with_fewer_memory_variables(nm):
+    """The staged kernels read R from a slab box whose width follows nm."""
+    p = small3d(nx=40, ny=36, nz=40, na=8, nt=20, nm=nm)
+    g0 = Swpc3D(p)
+    g1 = Swpc3D(p)
+    _lib.check(g1.ctx, g1.lib.swpc_set_launch(g1.ctx, 5, 1, 4, 2))
+    _lib.check(g1.ctx, g1.lib.swpc_set_launch(g1.ctx, 6, 1, 4, 4))
+    g0.run(1, p.nt)
+    g1.run(1, p.nt)
+    fields = list(range(9)) + [_lib.F_R + 3 * c + m for c in range(6) for m in range(nm)]
+    for n in fields:
+        assert same_bits(g0.download(n), g1.download(n)), n
