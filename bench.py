@@ -397,8 +397,9 @@ def bench_c2b(args, world, rank, local):
                            "ms_per_step": ms_loop / args.steps,
                            "what": "one green-mode run per source, its own CUDA graph, sources one after another"},
             "batched_over_loop": ms_loop / ms_batch,
-            "autotune": {"strip_cells": strip, "steps_used": used},
-            "roofline": {"bound": "hbm", "kernel": "stress3d_batch_kernel + vel3d_batch_kernel (whole batched step)",
+            "autotune": {"launch": fb.launch(), "steps_used": used},
+            "roofline": {"bound": "hbm", "kernel": "stress3d_tma_kernel + vel3d_tma_kernel, members grouped per CTA "
+                                                     "(whole batched step)",
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
                          "traffic": None, "algorithmic_bytes_per_step": b_step},
             "e2e": {"value": cells * len(forces) * world * args.steps / t_e2e / 1e9, "unit": UNIT,

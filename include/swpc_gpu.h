@@ -288,19 +288,33 @@ int swpc_gradient_model(swpc_ctx *ctx, const float *vp, const float *vs, const f
  *                             (ksrc, isrc, jsrc), Kupper etc. time function
  *                             from green_tbeg / green_trise
  *   swpc_fbatch_step / _run   one step / nsteps graph replays of all members
- *   swpc_fbatch_set_strip     i-strip width in cells of the launch order
- *                             (0 = from the L2 size); _autotune times the
- *                             candidates over steps it0.. and keeps the best
+ *   swpc_fbatch_set_strip     i-strip width in cells of the flat launch
+ *                             order (0 = from the L2 size); _autotune times
+ *                             the candidates over steps it0.. and keeps the
+ *                             best (see swpc_fbatch_set_launch)
  *   swpc_fbatch_wav_fetch     traces of member m, layout of swpc_wav_fetch
  *   swpc_fbatch_download_field  V, S or R of member m in the memory box
- * The batch borrows ctx (which must outlive it); ctx's own state and sources
- * are untouched. */
+ * The batch borrows ctx, which must outlive it: swpc_destroy refuses a
+ * context that still has batches (SWPC_ERR_STATE); ctx's own state and
+ * sources are untouched. */
 typedef struct swpc_fbatch swpc_fbatch;
 int swpc_fbatch_create(swpc_ctx *ctx, int nmem, swpc_fbatch **out);
 int swpc_fbatch_destroy(swpc_fbatch *b);
 int swpc_fbatch_green_source(swpc_fbatch *b, int member, int isrc, int jsrc, int ksrc, char cmp, float green_tbeg,
                              float green_trise, int stftype);
 int swpc_fbatch_set_strip(swpc_fbatch *b, int strip_cells);
+/* Launch form of the batch: kernel 0 = the flat one-cell kernels in strip
+ * order (swpc_fbatch_set_strip); kernel 5 / 6 = the TMA-staged stress /
+ * velocity kernels with tile (bi, bj) and mpc members per CTA, whose CTAs copy
+ * the medium of a tile once for the mpc members (FP32 contexts; the default,
+ * stress (4,2) and velocity (4,2) with 2 members per CTA).  Compiled stress
+ * (bi, bj, mpc): (4,4,1) (2,4,1) (4,2,1) (4,2,2) (2,4,2) (2,2,2) (2,2,4)
+ * (4,1,4); velocity: (4,2,1) (4,4,1) (2,2,1) (4,2,2) (2,2,2) (4,1,2) (2,2,4)
+ * (4,1,4).  swpc_fbatch_autotune tunes the form in use (strip widths, or
+ * the staged shapes of stress then velocity); swpc_fbatch_get_launch writes
+ * {staged, strip, stress bi, bj, mpc, velocity bi, bj, mpc} to out[8]. */
+int swpc_fbatch_set_launch(swpc_fbatch *b, int kernel, int mpc, int bi, int bj);
+int swpc_fbatch_get_launch(const swpc_fbatch *b, int *out);
 int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *steps_used, int *strip);
 int swpc_fbatch_step(swpc_fbatch *b, int it);
 int swpc_fbatch_run(swpc_fbatch *b, int it0, int nsteps);

@@ -51,7 +51,8 @@ EXPORTS = [
     "swpc_batch_set_shape",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
     "swpc_fbatch_autotune", "swpc_fbatch_step", "swpc_fbatch_run", "swpc_fbatch_time_steps", "swpc_fbatch_sync",
-    "swpc_fbatch_wav_fetch", "swpc_fbatch_download_field", "swpc_fbatch_device_bytes",
+    "swpc_fbatch_wav_fetch", "swpc_fbatch_download_field", "swpc_fbatch_device_bytes", "swpc_fbatch_set_launch",
+    "swpc_fbatch_get_launch",
     "swpc_batch_last_error", "swpc_batch_destroy",
 ]
 
@@ -192,6 +193,8 @@ def load():
         "swpc_fbatch_wav_fetch": (i, [vp, i, i, _FP]),
         "swpc_fbatch_download_field": (i, [vp, i, i, _FP, i, i]),
         "swpc_fbatch_device_bytes": (C.c_longlong, [vp]),
+        "swpc_fbatch_set_launch": (i, [vp, i, i, i, i]),
+        "swpc_fbatch_get_launch": (i, [vp, _IP]),
     }
     for name in ("swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
                  "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_comm_stress",

@@ -126,17 +126,17 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     g.ncell = (long long)g.Kp * g.Ip * g.Jp;
     int rc = 0;
     if (is3d(c) && c->prec == SWPC_PREC_F32) {
-        // one slab: 0-2 V, 3-8 S, 9-15 lam mu taup taus muyz muxz muxy, R, bx by bz
-        const int nf = 3 + 6 + 7 + 6 * d->nm + 3;
+        // one slab: 0-2 V, 3-8 S, R (6 nm), lam mu taup taus muyz muxz muxy, bx by bz
+        const int nf = 3 + 6 + 6 * d->nm + 7 + 3;
         rc = dalloc(c, &c->slab, (size_t)nf * g.ncell);
         if (!rc) {
             auto F = [&](int f) { return c->slab + (size_t)f * g.ncell; };
             for (int q = 0; q < 3; q++) c->V[q] = F(q);
             for (int q = 0; q < 6; q++) c->S[q] = F(3 + q);
-            const int mq[7] = {1, 2, 3, 4, 8, 9, 10};
-            for (int q = 0; q < 7; q++) c->med[mq[q]] = F(9 + q);
             for (int comp = 0; comp < 6; comp++)
-                for (int m = 0; m < d->nm; m++) c->R[comp * 3 + m] = F(16 + comp * d->nm + m);
+                for (int m = 0; m < d->nm; m++) c->R[comp * 3 + m] = F(9 + comp * d->nm + m);
+            const int mq[7] = {1, 2, 3, 4, 8, 9, 10};
+            for (int q = 0; q < 7; q++) c->med[mq[q]] = F(9 + 6 * d->nm + q);
             for (int q = 0; q < 3; q++) c->med[5 + q] = F(16 + 6 * d->nm + q);
             c->slab_nf = nf;
             // the TMA-staged kernels are the default launch of FP32 3D contexts
@@ -177,6 +177,7 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
 
 extern "C" int swpc_destroy(swpc_ctx *c) {
     if (!c) return SWPC_OK;
+    if (c->nfbatch > 0) return set_err(c, SWPC_ERR_STATE, "destroy the reciprocity batches over this context first");
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     invalidate_graph(c);
@@ -223,10 +224,10 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
         return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..6, minb 1..4, 32*bi*bj <= 256)");
     if (kernel >= 2 && c->prec != SWPC_PREC_F32)
         return set_err(c, SWPC_ERR_ARG, "reduced-precision storage runs the kernels 0 and 1 only");
-    // staged kernels: minb selects the tile's k extent (1: 32 cells, 2: 64 cells)
-    if (kernel >= 5 && (!is3d(c) || !c->slab || minb > 2 ||
-                        !(kernel == 5 ? tma_shape_ok(32 * minb, bi, bj) : tma_vel_shape_ok(32 * minb, bi, bj))))
-        return set_err(c, SWPC_ERR_ARG, "staged kernels: 3D FP32 only, with a compiled tile shape (kt, bi, bj)");
+    // staged kernels: minb is unused (pass 1); the tile must be compiled
+    if (kernel >= 5 && (!is3d(c) || !c->slab || minb != 1 ||
+                        !(kernel == 5 ? tma_shape_ok(bi, bj, 1) : tma_vel_shape_ok(bi, bj, 1))))
+        return set_err(c, SWPC_ERR_ARG, "staged kernels: 3D FP32 only, minb 1, with a compiled tile (bi, bj)");
     invalidate_graph(c);
     switch (kernel) {
     case 0: c->stress_march = false; c->stress_tma = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
@@ -239,12 +240,9 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
         c->vel_march = false; c->vel_vec = true; c->vel_tma = false; c->vel_vminb = minb; c->vel_vbi = bi;
         c->vel_vbj = bj;
         break;
-    case 5:
-        c->stress_march = false; c->stress_tma = true; c->stress_tkt = 32 * minb; c->stress_tbi = bi; c->stress_tbj = bj;
-        break;
+    case 5: c->stress_march = false; c->stress_tma = true; c->stress_tbi = bi; c->stress_tbj = bj; break;
     default:
-        c->vel_march = false; c->vel_vec = false; c->vel_tma = true; c->vel_tkt = 32 * minb; c->vel_tbi = bi;
-        c->vel_tbj = bj;
+        c->vel_march = false; c->vel_vec = false; c->vel_tma = true; c->vel_tbi = bi; c->vel_tbj = bj;
         break;
     }
     return SWPC_OK;
@@ -747,26 +745,38 @@ static void fill_geo_common(const swpc_ctx *c, Geo &g, int &ibk, int &iek, int &
 
 // tensor maps of the staged kernels for the selected tile shapes
 static int tma_ready(swpc_ctx *c) {
-    const int key[6] = {c->stress_tkt, c->stress_tbi, c->stress_tbj, c->vel_tkt, c->vel_tbi, c->vel_tbj};
-    if (c->tmaps && std::equal(key, key + 6, c->tma_key)) return SWPC_OK;
+    const int key[4] = {c->stress_tbi, c->stress_tbj, c->vel_tbi, c->vel_tbj};
+    if (c->tmaps && std::equal(key, key + 4, c->tma_key)) return SWPC_OK;
     if (!c->tmaps) c->tmaps = new TmaMaps();
     TmaMaps &m = *static_cast<TmaMaps *>(c->tmaps);
-    if (!tma_encode_stress(m, c->slab, c->g, c->slab_nf, c->d.nm, key[0], key[1], key[2]) ||
-        !tma_encode_vel(m, c->slab, c->g, c->slab_nf, key[3], key[4], key[5]))
+    const TmaSlabs s{c->slab, c->slab_nf, c->slab, c->slab_nf};
+    if (!tma_encode_stress(m, s, c->g, c->d.nm, key[0], key[1]) || !tma_encode_vel(m, s, c->g, key[2], key[3]))
         return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the field slab");
-    std::copy(key, key + 6, c->tma_key);
+    std::copy(key, key + 4, c->tma_key);
     return SWPC_OK;
 }
 
-static TmaTiles tma_tiles(const swpc_ctx *c, int kt, int bi, int bj) {
+namespace swpc {
+// tiles of a staged launch over the whole grid for nmem members grouped by
+// mpc; the medium fields come from the context's slab
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc) {
     TmaTiles t;
-    t.nkt = (c->g.nz + kt - 1) / kt;
+    t.nkt = (c->g.nz + 31) / 32;
     t.nit = (c->g.nx + bi - 1) / bi;
     t.njt = (c->g.ny + bj - 1) / bj;
-    t.b_field = 16 + 6 * c->d.nm;
+    t.nmem = nmem;
+    t.mgroups = (nmem + mpc - 1) / mpc;
+    t.f_v = 0;
+    t.f_state = 3;
+    t.f_member = 0;
+    t.f_med = 9 + 6 * c->d.nm;
+    t.f_b = 16 + 6 * c->d.nm;
+    t.so = 0;
+    t.ao = 0;
     t.err = c->d_err;
     return t;
 }
+}  // namespace swpc
 
 static int launch_stress(swpc_ctx *c, int mask) {
     RC(check_ready(c));
@@ -793,9 +803,9 @@ static int launch_stress(swpc_ctx *c, int mask) {
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
     if (c->stress_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->stress_tkt, c->stress_tbi, c->stress_tbj);
-        return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tkt,
-                                                 c->stress_tbi, c->stress_tbj, c->stream), "stress3d_tma launch");
+        const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1);
+        return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tbi,
+                                                 c->stress_tbj, 1, c->stream), "stress3d_tma launch");
     }
     if (c->stress_march && c->prec == SWPC_PREC_F32)
         launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
@@ -823,9 +833,9 @@ static int launch_vel(swpc_ctx *c, int mask) {
     for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
     if (c->vel_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->vel_tkt, c->vel_tbi, c->vel_tbj);
-        return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tkt, c->vel_tbi,
-                                              c->vel_tbj, c->stream), "vel3d_tma launch");
+        const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1);
+        return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tbi, c->vel_tbj, 1,
+                                              c->stream), "vel3d_tma launch");
     }
     if (c->prec != SWPC_PREC_F32) launch_vel3d(a, c->vel_minb, c->prec, grid, block, c->stream);
     else if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);

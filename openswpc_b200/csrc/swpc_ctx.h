@@ -157,19 +157,20 @@ struct swpc_ctx {
     // velocity kernel with four consecutive k per thread (swpc3d_vec.cu)
     bool vel_vec = false;
     int vel_vminb = 2, vel_vbi = 2, vel_vbj = 2;
-    // TMA-staged kernels (swpc3d_tma.cu): tile kt x bi x bj; tensor maps over
+    // TMA-staged kernels (swpc3d_tma.cu): tile 32 x bi x bj; tensor maps over
     // the field slab, encoded for the shapes in tma_key
     bool stress_tma = false, vel_tma = false;
-    int stress_tkt = 32, stress_tbi = 4, stress_tbj = 4, vel_tkt = 32, vel_tbi = 4, vel_tbj = 2;
+    int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 2;
     void *tmaps = nullptr;        // swpc::TmaMaps
-    int tma_key[6] = {-1, -1, -1, -1, -1, -1};
+    int tma_key[4] = {-1, -1, -1, -1};
     int *d_err = nullptr;         // device error word of the staged kernels
 
-    // 3D FP32 storage: V, S, stress medium, R and buoyancies in one allocation
-    // (field order 0-2 V, 3-8 S, 9-15 lam mu taup taus muyz muxz muxy, 16.. R
-    // component-major, then bx by bz), so that one tensor map covers them
+    // 3D FP32 storage: V, S, R and the medium in one allocation (field order
+    // 0-2 V, 3-8 S, 9.. R component-major, then lam mu taup taus muyz muxz
+    // muxy and bx by bz), so that tensor maps cover them
     float *slab = nullptr;
     int slab_nf = 0;
+    int nfbatch = 0;   // reciprocity batches that borrow this context (swpc_fbatch.cu)
 
     long long bytes = 0;
 };

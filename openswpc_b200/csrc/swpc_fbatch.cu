@@ -12,11 +12,16 @@
 // HBM once and served from L2 to the other members.  The tile order walks
 // i-strips of `strip` cells along j (strip by strip), which keeps the
 // velocity / stress planes that the j-stencil re-reads resident in L2 even
-// with all members in flight.
+// with all members in flight.  That is the flat form; by default the batch
+// runs the TMA-staged kernels of swpc3d_tma.cu, whose CTAs copy the medium of a
+// tile once and then the boxes of a group of members (members per CTA and
+// tile chosen by swpc_fbatch_set_launch / swpc_fbatch_autotune).
 //
-// Layout: each state field (V, S, R, PML auxiliaries) is one array of nmem
-// member copies, member m at offset m * stride (stride = the context's cell
-// count, or its compact PML cell count for the auxiliaries).
+// Layout: one slab of nmem member blocks, each block the member's V, S and R
+// (nfs = 9 + 6 nm fields of the context's cell count, the order of the
+// context's slab), so member m's copy of a field sits at m * stride (stride =
+// nfs cells); the PML auxiliaries are one array per auxiliary with the
+// members at m * astride (the context's compact PML cell count).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,11 +31,13 @@
 #include "swpc_ctx.h"
 #include "swpc_kernels.cuh"
 #include "swpc3d_cell.cuh"
+#include "swpc_tma.h"
 
 namespace swpc {
 int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half);
 bool green_entries(const swpc_ctx *c, int isrc, int jsrc, int ksrc, char cmp, std::vector<InjEntry> &v);
 int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i);
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc);
 }  // namespace swpc
 
 using namespace swpc;
@@ -39,7 +46,9 @@ struct swpc_fbatch {
     swpc_ctx *c = nullptr;
     int nmem = 0;
     long long stride = 0, astride = 0;
-    float *V[3] = {}, *S[6] = {}, *R[18] = {}, *aux[18] = {};
+    float *slab = nullptr;
+    int nfs = 0;
+    float *V[3] = {}, *S[6] = {}, *R[18] = {}, *aux[18] = {};   // member 0 (V, S, R inside the slab)
     float *wav[4] = {};            // per kind: nmem blocks of (nst, ncmp, ntw)
     float *uacc = nullptr, *eacc = nullptr;
     // green sources: entries tagged with their member, forces per member
@@ -51,7 +60,11 @@ struct swpc_fbatch {
     int ninj = 0;
     float *stf = nullptr;          // (nt, nmem)
     bool src_dirty = true;
-    int strip = 0;                 // i-strip width in cells (0: automatic)
+    int strip = 0;                 // i-strip width in cells (0: automatic), flat kernels
+    bool staged = false;           // TMA-staged kernels (FP32 contexts with a field slab)
+    int sbi = 4, sbj = 2, smpc = 2, vbi = 4, vbj = 2, vmpc = 2;   // staged tiles and members per CTA
+    void *tmaps = nullptr;         // swpc::TmaMaps over the batch slab and the context's medium
+    int tma_key[4] = {-1, -1, -1, -1};
     int *d_it = nullptr;
     cudaGraphExec_t graph = nullptr;
     long long bytes = 0;
@@ -169,10 +182,9 @@ static int falloc(swpc_fbatch *b, T **p, size_t n) {
 
 static void fb_free(swpc_fbatch *b) {
     auto f = [](void *p) { if (p) cudaFree(p); };
-    for (auto p : b->V) f(p);
-    for (auto p : b->S) f(p);
-    for (auto p : b->R) f(p);
+    f(b->slab);
     for (auto p : b->aux) f(p);
+    delete static_cast<TmaMaps *>(b->tmaps);
     for (auto p : b->wav) f(p);
     f(b->uacc); f(b->eacc); f(b->inj); f(b->inj_mem); f(b->stf); f(b->d_it);
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -192,14 +204,18 @@ extern "C" int swpc_fbatch_create(swpc_ctx *c, int nmem, swpc_fbatch **out) {
     auto *b = new swpc_fbatch();
     b->c = c;
     b->nmem = nmem;
-    b->stride = c->g.ncell;
+    b->nfs = 9 + 6 * c->d.nm;
+    b->stride = (long long)b->nfs * c->g.ncell;
     b->astride = c->npml;
-    const size_t n = (size_t)c->g.ncell * nmem;
-    int rc = SWPC_OK;
-    for (int q = 0; q < 3 && !rc; q++) rc = falloc(b, &b->V[q], n);
-    for (int q = 0; q < 6 && !rc; q++) rc = falloc(b, &b->S[q], n);
-    for (int comp = 0; comp < 6 && !rc; comp++)
-        for (int m = 0; m < c->d.nm && !rc; m++) rc = falloc(b, &b->R[comp * 3 + m], n);
+    int rc = falloc(b, &b->slab, (size_t)b->stride * nmem);
+    if (!rc) {
+        auto F = [&](int f) { return b->slab + (size_t)f * c->g.ncell; };
+        for (int q = 0; q < 3; q++) b->V[q] = F(q);
+        for (int q = 0; q < 6; q++) b->S[q] = F(3 + q);
+        for (int comp = 0; comp < 6; comp++)
+            for (int m = 0; m < c->d.nm; m++) b->R[comp * 3 + m] = F(9 + comp * c->d.nm + m);
+        b->staged = c->slab != nullptr;
+    }
     if (c->npml > 0)
         for (int q = 0; q < 18 && !rc; q++) rc = falloc(b, &b->aux[q], (size_t)c->npml * nmem);
     const int nst = std::max(c->nst, 1);
@@ -214,6 +230,7 @@ extern "C" int swpc_fbatch_create(swpc_ctx *c, int nmem, swpc_fbatch **out) {
         delete b;
         return rc;
     }
+    c->nfbatch++;
     b->h_inj.assign(nmem, {});
     b->h_prm.assign(2 * (size_t)nmem, 0.f);
     b->h_stf.assign(nmem, -1);
@@ -225,6 +242,7 @@ extern "C" int swpc_fbatch_destroy(swpc_fbatch *b) {
     if (!b) return SWPC_OK;
     cudaSetDevice(b->c->device);
     cudaStreamSynchronize(b->c->stream);
+    b->c->nfbatch--;
     fb_free(b);
     delete b;
     return SWPC_OK;
@@ -243,6 +261,24 @@ extern "C" int swpc_fbatch_green_source(swpc_fbatch *b, int member, int isrc, in
     b->h_prm[2 * member + 1] = green_trise;
     b->h_stf[member] = stftype;
     b->src_dirty = true;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    return SWPC_OK;
+}
+
+extern "C" int swpc_fbatch_set_launch(swpc_fbatch *b, int kernel, int mpc, int bi, int bj) {
+    if (!b) return SWPC_ERR_ARG;
+    if (kernel == 0) {
+        b->staged = false;
+    } else if (kernel == 5 || kernel == 6) {
+        if (!b->c->slab) return ferr(b, SWPC_ERR_ARG, "staged kernels need an FP32 context");
+        if (!(kernel == 5 ? tma_shape_ok(bi, bj, mpc) : tma_vel_shape_ok(bi, bj, mpc)))
+            return ferr(b, SWPC_ERR_ARG, "no compiled staged kernel for this tile and member count");
+        b->staged = true;
+        if (kernel == 5) { b->sbi = bi; b->sbj = bj; b->smpc = mpc; }
+        else { b->vbi = bi; b->vbj = bj; b->vmpc = mpc; }
+    } else {
+        return ferr(b, SWPC_ERR_ARG, "kernel must be 0 (flat), 5 (staged stress) or 6 (staged velocity)");
+    }
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
     return SWPC_OK;
 }
@@ -311,6 +347,29 @@ static BatchGrid batch_grid(const swpc_fbatch *b, int bi, int bj) {
     return bg;
 }
 
+// tensor maps of the staged kernels: member state over the batch slab, the
+// medium over the context's slab
+static int fb_tma_ready(swpc_fbatch *b) {
+    const int key[4] = {b->sbi, b->sbj, b->vbi, b->vbj};
+    if (b->tmaps && std::equal(key, key + 4, b->tma_key)) return SWPC_OK;
+    if (!b->tmaps) b->tmaps = new TmaMaps();
+    TmaMaps &m = *static_cast<TmaMaps *>(b->tmaps);
+    swpc_ctx *c = b->c;
+    const TmaSlabs s{b->slab, (long long)b->nfs * b->nmem, c->slab, c->slab_nf};
+    if (!tma_encode_stress(m, s, c->g, c->d.nm, key[0], key[1]) || !tma_encode_vel(m, s, c->g, key[2], key[3]))
+        return ferr(b, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the batch slab");
+    std::copy(key, key + 4, b->tma_key);
+    return SWPC_OK;
+}
+
+static TmaTiles fb_tiles(const swpc_fbatch *b, int bi, int bj, int mpc) {
+    TmaTiles t = tma_tiles(b->c, bi, bj, b->nmem, mpc);
+    t.f_member = b->nfs;
+    t.so = b->stride;
+    t.ao = b->astride;
+    return t;
+}
+
 static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
     swpc_ctx *c = b->c;
     const Geo &g = c->g;
@@ -354,6 +413,12 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         a.mask = mask;
         for (int q = 0; q < 6; q++) { a.sS[q] = 1.0f; a.iS[q] = 1.0f; }
         for (int q = 0; q < 18; q++) { a.sR[q] = 1.0f; a.iR[q] = 1.0f; }
+        if (b->staged) {
+            FRC(fb_tma_ready(b));
+            const TmaTiles t = fb_tiles(b, b->sbi, b->sbj, b->smpc);
+            FCK(launch_stress3d_tma(*static_cast<TmaMaps *>(b->tmaps), a, t, c->d.nm, b->sbi, b->sbj, b->smpc,
+                                    c->stream));
+        } else {
         const BatchGrid bg = batch_grid(b, c->bi, c->bj);
         const long long nblk = (long long)bg.nmem * bg.nkb * bg.nib * bg.njb;
         if (nblk > 0x7fffffffLL) return ferr(b, SWPC_ERR_LIMIT, "batch grid above 2^31-1 blocks");
@@ -365,6 +430,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         default: stress3d_batch_kernel<3><<<(unsigned)nblk, block, 0, c->stream>>>(a, bg); break;
         }
         FCK(cudaGetLastError());
+        }
     }
     // velocity (kernel__update_vel + absorb_p__update_vel)
     {
@@ -381,11 +447,17 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         a.dt = c->d.dt;
         a.mask = mask;
         for (int q = 0; q < 6; q++) a.sS[q] = 1.0f;
-        const BatchGrid bg = batch_grid(b, c->vbi, c->vbj);
-        const long long nblk = (long long)bg.nmem * bg.nkb * bg.nib * bg.njb;
-        if (nblk > 0x7fffffffLL) return ferr(b, SWPC_ERR_LIMIT, "batch grid above 2^31-1 blocks");
-        vel3d_batch_kernel<<<(unsigned)nblk, dim3(32, c->vbi, c->vbj), 0, c->stream>>>(a, bg);
-        FCK(cudaGetLastError());
+        if (b->staged) {
+            FRC(fb_tma_ready(b));
+            const TmaTiles t = fb_tiles(b, b->vbi, b->vbj, b->vmpc);
+            FCK(launch_vel3d_tma(*static_cast<TmaMaps *>(b->tmaps), a, t, b->vbi, b->vbj, b->vmpc, c->stream));
+        } else {
+            const BatchGrid bg = batch_grid(b, c->vbi, c->vbj);
+            const long long nblk = (long long)bg.nmem * bg.nkb * bg.nib * bg.njb;
+            if (nblk > 0x7fffffffLL) return ferr(b, SWPC_ERR_LIMIT, "batch grid above 2^31-1 blocks");
+            vel3d_batch_kernel<<<(unsigned)nblk, dim3(32, c->vbi, c->vbj), 0, c->stream>>>(a, bg);
+            FCK(cudaGetLastError());
+        }
     }
     // green__source of every member
     if (b->ninj > 0) {
@@ -456,28 +528,63 @@ extern "C" int swpc_fbatch_time_steps(swpc_fbatch *b, int it0, int nsteps, float
     return rc;
 }
 
+// time `reps` steps of the current launch after one untimed replay of the
+// (re)built graph; advances *it by 2 reps
+static int fb_time(swpc_fbatch *b, int *it, int reps, float *ms) {
+    FRC(swpc_fbatch_run(b, *it, reps));
+    *it += reps;
+    FRC(swpc_fbatch_time_steps(b, *it, reps, ms));
+    *it += reps;
+    return SWPC_OK;
+}
+
 extern "C" int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *steps_used, int *strip_out) {
     if (!b || reps < 1) return SWPC_ERR_ARG;
-    const int nx = b->c->g.nx;
-    std::vector<int> cand = {32, 64, 128, 256, 512};
-    cand.erase(std::remove_if(cand.begin(), cand.end(), [&](int w) { return w > nx; }), cand.end());
-    cand.push_back(nx);
-    int best = cand[0], it = it0, used = 0;
-    float best_ms = 1e30f;
-    for (int w : cand) {
-        if (it + 2 * reps - 1 > b->c->d.nt) break;
-        FRC(swpc_fbatch_set_strip(b, w));
-        FRC(swpc_fbatch_run(b, it, reps));   // first replay after (re)instantiation
-        it += reps;
-        float ms = 0.f;
-        FRC(swpc_fbatch_time_steps(b, it, reps, &ms));
-        it += reps;
-        used += 2 * reps;
-        if (ms < best_ms) { best_ms = ms; best = w; }
+    int it = it0;
+    const int nt = b->c->d.nt;
+    if (b->staged) {
+        // staged kernels: members per CTA and tile of the stress kernel, then of the velocity kernel
+        const int sc[][3] = {{4, 2, 2}, {4, 4, 1}, {2, 4, 2}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
+        const int vc[][3] = {{4, 2, 2}, {4, 2, 1}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
+        for (int kernel = 5; kernel <= 6; kernel++) {
+            const int(*cand)[3] = kernel == 5 ? sc : vc;
+            int best = 0;
+            float best_ms = 1e30f;
+            for (int q = 0; q < 6; q++) {
+                if (it + 2 * reps - 1 > nt) break;
+                FRC(swpc_fbatch_set_launch(b, kernel, cand[q][2], cand[q][0], cand[q][1]));
+                float ms = 0.f;
+                FRC(fb_time(b, &it, reps, &ms));
+                if (ms < best_ms) { best_ms = ms; best = q; }
+            }
+            FRC(swpc_fbatch_set_launch(b, kernel, cand[best][2], cand[best][0], cand[best][1]));
+        }
+        if (strip_out) *strip_out = 0;
+    } else {
+        const int nx = b->c->g.nx;
+        std::vector<int> cand = {32, 64, 128, 256, 512};
+        cand.erase(std::remove_if(cand.begin(), cand.end(), [&](int w) { return w > nx; }), cand.end());
+        cand.push_back(nx);
+        int best = cand[0];
+        float best_ms = 1e30f;
+        for (int w : cand) {
+            if (it + 2 * reps - 1 > nt) break;
+            FRC(swpc_fbatch_set_strip(b, w));
+            float ms = 0.f;
+            FRC(fb_time(b, &it, reps, &ms));
+            if (ms < best_ms) { best_ms = ms; best = w; }
+        }
+        FRC(swpc_fbatch_set_strip(b, best));
+        if (strip_out) *strip_out = best;
     }
-    FRC(swpc_fbatch_set_strip(b, best));
-    if (steps_used) *steps_used = used;
-    if (strip_out) *strip_out = best;
+    if (steps_used) *steps_used = it - it0;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_fbatch_get_launch(const swpc_fbatch *b, int *out) {
+    if (!b || !out) return SWPC_ERR_ARG;
+    const int v[8] = {b->staged ? 1 : 0, b->strip, b->sbi, b->sbj, b->smpc, b->vbi, b->vbj, b->vmpc};
+    std::copy(v, v + 8, out);
     return SWPC_OK;
 }
 

@@ -7,29 +7,49 @@
 
 namespace swpc {
 
-// tile grid of a staged launch: tiles of kt (k) x bi (i) x bj (j) cells
+// A staged launch: tiles of 32 (k) x bi (i) x bj (j) cells, and per tile the
+// member groups of a batch (a single run is one member).  Field coordinates
+// refer to the state slab (per member: V, S, R) and the medium slab.
 struct TmaTiles {
     int nkt, nit, njt;
-    int b_field;   // slab index of bx (velocity kernel)
-    int *err;      // raised when a tile copy does not complete
+    int nmem, mgroups;   // members, groups of members per CTA
+    int f_v;             // state slab: Vx of member 0 (S follows at f_v + 3)
+    int f_state;         // state slab: Sxx of member 0 (S, then R)
+    int f_member;        // state slab: field stride between members
+    int f_med;           // medium slab: lam (lam mu taup taus muyz muxz muxy)
+    int f_b;             // medium slab: bx (bx by bz)
+    long long so, ao;    // offset between members of the state arrays and of the PML auxiliaries
+    int *err;            // raised when a tile copy does not complete
+};
+
+// the slabs the tensor maps cover
+struct TmaSlabs {
+    float *state;
+    long long nf_state;
+    float *med;
+    long long nf_med;
 };
 
 // host copies of the tensor maps (CUtensorMap, 128 bytes, 64-byte aligned)
 struct alignas(64) TmaMaps {
-    unsigned char str[128];    // stress: S, medium, R of the tile
-    unsigned char v3h[128];    // stress: V with halo
-    unsigned char own3[128];   // velocity: V (and bx by bz) of the tile
+    unsigned char state[128];   // stress: S and R of a member
+    unsigned char med[128];     // stress: the seven medium fields of the stress update
+    unsigned char vh[128];      // stress: V of a member with halo
+    unsigned char own3[128];    // velocity: V of a member
+    unsigned char b3[128];      // velocity: bx by bz
     unsigned char va[128], vb[128], vc[128], vf[128], ve[128], vd[128];   // velocity: Sxx Syy Szz Syz Sxz Sxy
 };
 
-// tile shapes (kt = cells along k: 32 or 64; bi x bj columns) with compiled kernels
-bool tma_shape_ok(int kt, int bi, int bj);       // stress tiles
-bool tma_vel_shape_ok(int kt, int bi, int bj);   // velocity tiles
-bool tma_encode_stress(TmaMaps &m, float *slab, const Geo &g, int nf, int nm, int kt, int bi, int bj);
-bool tma_encode_vel(TmaMaps &m, float *slab, const Geo &g, int nf, int kt, int bi, int bj);
-cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, int nm, int kt, int bi, int bj,
+// compiled tiles (bi, bj) and members per CTA: stress (4,4,1) (2,4,1) (4,2,1)
+// (4,2,2) (2,4,2) (2,2,2) (2,2,4) (4,1,4); velocity (4,2,1) (4,4,1) (2,2,1)
+// (4,2,2) (2,2,2) (4,1,2) (2,2,4) (4,1,4)
+bool tma_shape_ok(int bi, int bj, int mpc);
+bool tma_vel_shape_ok(int bi, int bj, int mpc);
+bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj);
+bool tma_encode_vel(TmaMaps &m, const TmaSlabs &s, const Geo &g, int bi, int bj);
+cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, int nm, int bi, int bj, int mpc,
                                 cudaStream_t st);
-cudaError_t launch_vel3d_tma(const TmaMaps &m, const Vel3Args &a, const TmaTiles &t, int kt, int bi, int bj,
+cudaError_t launch_vel3d_tma(const TmaMaps &m, const Vel3Args &a, const TmaTiles &t, int bi, int bj, int mpc,
                              cudaStream_t st);
 
 }  // namespace swpc

@@ -16,6 +16,7 @@ that is a C-ordered array of shape ``(ny+6, nx+6, nz+6)`` indexed
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -306,6 +307,12 @@ class Swpc3D:
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
+        # batches borrow the context: they go first
+        for ref in getattr(self, "_dependents", []):
+            dep = ref()
+            if dep is not None:
+                dep.close()
+        self._dependents = []
         if self.ctx:
             self.lib.swpc_destroy(self.ctx)
             self.ctx = None
@@ -508,6 +515,9 @@ class ForceBatch3D:
         b = C.c_void_p()
         check(base.ctx, self.lib.swpc_fbatch_create(base.ctx, len(forces), C.byref(b)))
         self.b = b
+        if not hasattr(base, "_dependents"):
+            base._dependents = []
+        base._dependents.append(weakref.ref(self))
         self.n = len(forces)
         stf = _lib.STF_CODES[p.stftype]
         self.cells = []
@@ -545,8 +555,20 @@ class ForceBatch3D:
     def set_strip(self, cells: int):
         check(self.base.ctx, self.lib.swpc_fbatch_set_strip(self.b, cells))
 
+    def set_launch(self, kernel: int, mpc: int = 1, bi: int = 4, bj: int = 2):
+        """kernel 0: flat kernels; 5 / 6: staged stress / velocity kernels with
+        tile (bi, bj) and mpc members per CTA."""
+        check(self.base.ctx, self.lib.swpc_fbatch_set_launch(self.b, kernel, mpc, bi, bj))
+
+    def launch(self) -> dict:
+        out = np.zeros(8, np.int32)
+        check(self.base.ctx, self.lib.swpc_fbatch_get_launch(self.b, iptr(out)))
+        return {"staged": bool(out[0]), "strip": int(out[1]), "stress": tuple(int(v) for v in out[2:5]),
+                "velocity": tuple(int(v) for v in out[5:8])}
+
     def autotune(self, it0: int, reps: int = 2):
-        """Times the i-strip widths over steps it0..; returns (steps used, strip)."""
+        """Tunes the launch form in use (strip widths, or the staged shapes)
+        over steps it0..; returns (steps used, strip)."""
         used, strip = C.c_int(), C.c_int()
         check(self.base.ctx, self.lib.swpc_fbatch_autotune(self.b, it0, reps, C.byref(used), C.byref(strip)))
         return used.value, strip.value

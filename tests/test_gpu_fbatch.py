@@ -30,14 +30,27 @@ def single(p, xi, station, cmp):
     return g
 
 
-@pytest.mark.parametrize("strip", [0, 8])
-def test_members_equal_single_green_runs(strip):
+# launch forms: flat kernels with two strip widths; staged kernels with 1, 2
+# and 4 members per CTA (5 members: the last group is partial)
+LAUNCHES = [("flat", 0), ("flat", 8), ("staged", (4, 4, 1, 4, 2, 1)), ("staged", (4, 2, 2, 4, 2, 2)),
+            ("staged", (2, 2, 4, 2, 2, 4)), ("staged", (4, 1, 4, 4, 1, 4)), ("staged", (2, 4, 2, 2, 2, 2))]
+
+
+@pytest.mark.parametrize("launch", LAUNCHES)
+def test_members_equal_single_green_runs(launch):
     p = green_params()
     xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
     base = Swpc3D(p, xi)
     base.record(p.stations)
     fb = ForceBatch3D(base, [(p.stations[s], c) for s, c in FORCES])
-    fb.set_strip(strip)
+    kind, arg = launch
+    if kind == "flat":
+        fb.set_launch(0)
+        fb.set_strip(arg)
+    else:
+        sbi, sbj, smpc, vbi, vbj, vmpc = arg
+        fb.set_launch(5, smpc, sbi, sbj)
+        fb.set_launch(6, vmpc, vbi, vbj)
     fb.run(1, p.nt)
     fields = list(range(9)) + [_lib.F_R + 3 * c + m for c in range(6) for m in range(p.nm)]
     for m, (s, c) in enumerate(FORCES):
@@ -74,12 +87,17 @@ def test_per_call_steps_equal_graph_replays():
 
 
 def test_autotune_keeps_results_and_bad_member_is_rejected():
-    p = green_params(nt=40)
+    p = green_params(nt=80)
     base = Swpc3D(p)
     base.record(p.stations)
     fb = ForceBatch3D(base, [(p.stations[0], "z"), (p.stations[1], "x")])
-    used, strip = fb.autotune(1, reps=2)
-    assert used > 0 and strip >= 8
+    used, _ = fb.autotune(1, reps=2)
+    assert 0 < used <= 48 and fb.launch()["staged"]
+    fb.set_launch(0)
+    used2, strip = fb.autotune(1 + used, reps=2)
+    assert used2 > 0 and strip >= 8
+    # a context that still has a batch is not destroyed
+    assert base.lib.swpc_destroy(base.ctx) == _lib.SWPC_ERR_STATE
     with pytest.raises(_lib.SwpcError):
         _lib.check(base.ctx, fb.lib.swpc_fbatch_green_source(fb.b, 2, 10, 10, 5, b"z", 0.0, 1.0, 0))
     fb.close()

@@ -266,8 +266,7 @@ def test_larger_grid_against_oracle_few_steps():
 @pytest.mark.parametrize("variant", [(0, 2, 2, 1, 1, 4, 2, 2), (0, 1, 4, 2, 1, 3, 8, 1), (2, 2, 1, 16, 3, 2, 1, 7),
                                      (2, 1, 1, 64, 3, 1, 1, 3), (0, 2, 2, 1, 4, 2, 2, 2), (0, 2, 2, 1, 4, 1, 4, 1),
                                      (0, 2, 2, 1, 4, 3, 1, 2), (5, 1, 4, 2, 6, 1, 4, 2), (5, 1, 2, 4, 6, 1, 4, 4),
-                                     (5, 1, 4, 4, 6, 1, 2, 2), (5, 2, 4, 2, 6, 2, 4, 2), (5, 2, 2, 2, 6, 2, 2, 2),
-                                     (5, 2, 2, 4, 6, 2, 4, 1), (5, 2, 4, 1, 6, 2, 2, 4), (5, 2, 4, 2, 6, 2, 4, 4)])
+                                     (5, 1, 4, 4, 6, 1, 2, 2)])
 def test_launch_variants_are_bitwise_identical(variant):
     """Flat, marching, four-cells-per-thread and TMA-staged kernels (5, 6),
     any block shape, chunk length or tile: same bits.  nz = 70 with na = 8 puts the interior/absorber
