@@ -39,6 +39,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from openswpc_b200 import replicas  # noqa: E402  (rank logic; no CUDA at import)
+
 METRIC = "Gcell-updates/s (3D visco, FP32)"
 UNIT = "Gcell-updates/s"
 # algorithmic bytes per cell-update (FP32 storage, nm = 3): each array read
@@ -137,7 +139,7 @@ def bench_c2a(args, world, rank, local):
     """Batched 2D P-SV ensemble (one persistent launch per half step, CUDA
     graph) against the plain per-model loop on the same GPU."""
     ps_all = make_c2a_models()
-    ps = [p for m, p in enumerate(ps_all) if m % world == rank]   # members shard across GPUs
+    ps = replicas.shard(ps_all, world, rank)   # members shard across GPUs
     wl = {"workload": "batched ensemble of 64 uneven 2D P-SV models (nx 256-2048, nz 128-1024, nm=3, PML 20)",
           "models": len(ps_all), "cells": sum(p.nx * p.nz for p in ps_all),
           "l2": "inputs larger than L2 (all members resident, several GB)", "parallelism": f"members/{world} GPUs"}
@@ -173,21 +175,10 @@ def bench_c2a(args, world, rank, local):
     from openswpc_b200 import _lib
     from openswpc_b200.swpc2d import Batch2D, Swpc2D
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        from datetime import timedelta
+    ranks = replicas.init("nccl") if world > 1 else replicas.Ranks(1, 0, local)
+    dist = ranks.dist
 
-        dist = dist_mod
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     runs = [Swpc2D(p, "psv", device=local) for p in ps]
     lib = _lib.load()
@@ -275,9 +266,7 @@ def bench_c2a(args, world, rank, local):
     batch.close()
     for r in runs:
         r.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -313,7 +302,7 @@ def bench_c2b(args, world, rank, local):
           "l2": "inputs larger than L2 (32 wavefields resident, ~130 GB)", "parallelism": f"members/{world} GPUs"}
     metric = "Gcell-updates/s (3D visco, FP32, reciprocity batch)"
     p, forces, st = make_c2b(nmem)
-    forces = [f for m, f in enumerate(forces) if m % world == rank]   # members shard across GPUs
+    forces = replicas.shard(forces, world, rank)   # members shard across GPUs
     cells = p.nx * p.ny * p.nz
     if args.impl == "reference":
         if rank != 0:
@@ -337,21 +326,10 @@ def bench_c2b(args, world, rank, local):
     from openswpc_b200 import _lib
     from openswpc_b200.swpc3d import ForceBatch3D, Swpc3D
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        from datetime import timedelta
+    ranks = replicas.init("nccl") if world > 1 else replicas.Ranks(1, 0, local)
+    dist = ranks.dist
 
-        dist = dist_mod
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     base = Swpc3D(p, device=local)
     base.record(st)
@@ -408,9 +386,7 @@ def bench_c2b(args, world, rank, local):
             "gpu_launches": args.steps * 5, "clocks": clk.summary()}
     fb.close()
     base.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -758,25 +734,14 @@ def main():
     from openswpc_b200 import _lib
     from openswpc_b200.swpc3d import Medium, Swpc3D
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        from datetime import timedelta
-
-        dist = dist_mod
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    ranks = replicas.init("nccl") if world > 1 else replicas.Ranks(1, 0, local)
+    dist = ranks.dist
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     device = local
     xi = rmed(p, device=f"cuda:{device}")
@@ -801,7 +766,7 @@ def main():
     barrier()
     ms_total = max_over_ranks(ms_total)
     ms_step = ms_total / args.steps
-    value = cells * args.steps * world / (ms_total / 1e3) / 1e9
+    value = replicas.throughput(cells, args.steps, world, ms_total)
 
     # ---- per-kernel times for the roofline (CUDA events on the ctx stream) --
     stream = torch.cuda.ExternalStream(lib.swpc_stream(ctx), device=device)
@@ -898,9 +863,7 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"oracle f32 on the centre 256x256x{p.nz} column block, {n} steps "
                                           f"after 1 warm-up ({dt:.1f} s)"}
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
