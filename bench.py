@@ -397,26 +397,31 @@ def Params_copy(p):
     return Params(**{**p.__dict__})
 
 
-def make_c3():
+def make_c3(grid=None, nt=2000):
     """The adjoint-gradient workload: 256 x 256 x 128 cells, dx = 0.25 km,
     dt = 0.01 s, nt = 2000, nm = 3, PML 20; the four-layer background, one
     double couple at 8 km depth, 64 seeded surface stations.  Returns the
     parameters, the starting model (vp, vs, rho, qp, qs) and the true vs:
-    the background with a seeded Gaussian blob of -8 % (radius 3 km)."""
+    the background with a seeded Gaussian blob of -8 % (radius 3 km).
+    `grid` (nx, ny, nz) and `nt` shrink the case for profiling runs (the
+    source and the stations stay inside the smaller grid)."""
     from openswpc_b200.params import Layer, Params, Station, dc_source
     from openswpc_b200.swpc3d import lhm_model
 
     layers = [Layer(0.0, 2.7, 5.5, 3.2, 300, 150), Layer(5.0, 2.8, 6.0, 3.5, 500, 250),
               Layer(18.0, 2.9, 6.7, 3.9, 600, 300), Layer(30.0, 3.3, 7.8, 4.5, 1000, 500)]
     nx, ny, nz, dx, na = 256, 256, 128, 0.25, 20
+    if grid is not None:
+        nx, ny, nz = grid
     rng = np.random.default_rng(20241205)
     xb, yb = -nx // 2 * dx, -ny // 2 * dx
     st = [Station(float(rng.uniform(xb + (na + 2) * dx, xb + (nx - na - 2) * dx)),
                   float(rng.uniform(yb + (na + 2) * dx, yb + (ny - na - 2) * dx)), 0.0, f"s{n:02d}", "fsb")
           for n in range(64)]
-    p = Params(nx=nx, ny=ny, nz=nz, nt=2000, dx=dx, dy=dx, dz=dx, dt=0.01, na=na, nm=3, xbeg=xb, ybeg=yb,
+    zsrc = min(8.0, 0.5 * (nz - na) * dx)
+    p = Params(nx=nx, ny=ny, nz=nz, nt=nt, dx=dx, dy=dx, dz=dx, dt=0.01, na=na, nm=3, xbeg=xb, ybeg=yb,
                zbeg=-3 * dx, fq_min=0.05, fq_max=2.0, layers=layers,
-               sources=[dc_source(0.0, 0.0, 8.0, 0.0, 2.0, 1e16, 30, 60, 90)], stations=st, ntdec_w=1,
+               sources=[dc_source(0.0, 0.0, zsrc, 0.0, 2.0, 1e16, 30, 60, 90)], stations=st, ntdec_w=1,
                ntdec_r=100)
     vp, vs, rho, qp, qs = lhm_model(p)
     # blob centre: seeded in the middle third of the domain, 4-12 km deep
@@ -433,8 +438,12 @@ def make_c3():
 def bench_c3(args, world, rank, local):
     """Checkpointed adjoint gradient of the L2 velocity misfit with respect to
     per-cell vp, vs, rho, against one plain forward run of the same model."""
-    wl = {"workload": "adjoint gradient 256x256x128, nt=2000 (nm=3, PML 20, 1 double couple, 64 stations, "
-                      "checkpoint every 50 steps)", "nx": 256, "ny": 256, "nz": 128, "nt": 2000, "ckpt": 50,
+    grid = tuple(int(v) for v in args.grid.lower().split("x")) if args.grid else (256, 256, 128)
+    nt = args.nt or 2000
+    ckpt = min(50, nt)
+    wl = {"workload": f"adjoint gradient {grid[0]}x{grid[1]}x{grid[2]}, nt={nt} (nm=3, PML 20, 1 double couple, "
+                      f"64 stations, checkpoint every {ckpt} steps)", "nx": grid[0], "ny": grid[1], "nz": grid[2],
+          "nt": nt, "ckpt": ckpt,
           "l2": "inputs larger than L2 (wavefield, checkpoints and adjoint state resident, tens of GB)",
           "parallelism": f"replicas x{world}"}
     metric = "Gcell-updates/s (3D visco adjoint gradient, FP32 + FP64 accumulation)"
@@ -449,13 +458,13 @@ def bench_c3(args, world, rank, local):
     from openswpc_b200.adjoint import Misfit3D, waveform_misfit
     from openswpc_b200.swpc3d import Medium, Swpc3D
 
-    p, (vp, vs, rho, qp, qs), vs_true = make_c3()
+    p, (vp, vs, rho, qp, qs), vs_true = make_c3(grid, nt)
     cells = p.nx * p.ny * p.nz
     true = Swpc3D(p, device=local, medium=Medium.from_model(p, vp, vs_true, rho, qp, qs))
     _lib.check(true.ctx, true.lib.swpc_run(true.ctx, 1, p.nt))
     obs = true.waveforms(_lib.WAV_V)
     true.close()
-    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, device=local, ckpt=50)
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, device=local, ckpt=ckpt)
     s = prob.solver
     lib, ctx = s.lib, s.ctx
     stream = torch.cuda.ExternalStream(lib.swpc_stream(ctx), device=local)
@@ -475,7 +484,7 @@ def bench_c3(args, world, rank, local):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         _lib.check(ctx, lib.swpc_sync(ctx))
         e0.record(stream)
-        _lib.check(ctx, lib.swpc_gradient(ctx, _lib.fptr(obsf), 50, C.byref(J)))
+        _lib.check(ctx, lib.swpc_gradient(ctx, _lib.fptr(obsf), ckpt, C.byref(J)))
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1)
@@ -669,6 +678,7 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3"])
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
+    ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (c3 profiling runs)")
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16sr"],
                     help="storage of stress and memory variables (arithmetic is FP32)")
     ap.add_argument("--accuracy", action="store_true",

@@ -218,6 +218,148 @@ __device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o,
         for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], a.iR[c * 3 + m]);
 }
 
+// absorb_p__update_vel (m_absorb_p.f90:248-309) for one absorber cell: the
+// auxiliaries (compact, per absorber column) from global memory, the other
+// operands through the accessor
+// The nine auxiliaries of an absorber cell (compact, per absorber column:
+// m_absorb_p.f90:96-116), loaded ahead of the rest of the cell's operands.
+struct Aux9 {
+    long long q;   // index of the cell in the compact arrays (without the member offset)
+    float v[9];
+};
+__device__ __forceinline__ Aux9 aux_load(float *const *aux, long long ao, const int2 *pmlcol, const Geo &g, int k,
+                                         int i, int j) {
+    Aux9 r;
+    const int2 pc = __ldg(&pmlcol[col_index(g, i, j)]);
+    r.q = (long long)pc.y + (k - pc.x);
+#pragma unroll
+    for (int n = 0; n < 9; n++) r.v[n] = lds(&aux[n][ao + r.q]);
+    return r;
+}
+
+template <int PREC, class Ops>
+__device__ __forceinline__ void vel_absorber(const Vel3Args &a, const Ops &o, const Aux9 &x, int k, int i, int j,
+                                             long long e, long long ao, float *Vx, float *Vy, float *Vz) {
+    const float dt = a.dt;
+    const long long q = x.q;
+    float *__restrict__ axSxx = a.aS[0] + ao;
+    float *__restrict__ aySxy = a.aS[1] + ao;
+    float *__restrict__ azSxz = a.aS[2] + ao;
+    float *__restrict__ axSxy = a.aS[3] + ao;
+    float *__restrict__ aySyy = a.aS[4] + ao;
+    float *__restrict__ azSyz = a.aS[5] + ao;
+    float *__restrict__ axSxz = a.aS[6] + ao;
+    float *__restrict__ aySyz = a.aS[7] + ao;
+    float *__restrict__ azSzz = a.aS[8] + ao;
+    const float vxSxx = x.v[0], vySxy = x.v[1], vzSxz = x.v[2];
+    const float vxSxy = x.v[3], vySyy = x.v[4], vzSyz = x.v[5];
+    const float vxSxz = x.v[6], vySyz = x.v[7], vzSzz = x.v[8];
+    const float vx = o.v(0), vy = o.v(1), vz = o.v(2);
+    const float bx = o.b(0), by = o.b(1), bz = o.b(2);
+    const float xx0 = o.s(0, 0, 0, 0), xxp = o.s(0, 0, 1, 0);
+    const float yy0 = o.s(1, 0, 0, 0), yyp = o.s(1, 0, 0, 1);
+    const float zz0 = o.s(2, 0, 0, 0), zzp = o.s(2, 1, 0, 0);
+    const float yz0 = o.s(3, 0, 0, 0), yzjm = o.s(3, 0, 0, -1), yzkm = o.s(3, -1, 0, 0);
+    const float xz0 = o.s(4, 0, 0, 0), xzim = o.s(4, 0, -1, 0), xzkm = o.s(4, -1, 0, 0);
+    const float xy0 = o.s(5, 0, 0, 0), xyim = o.s(5, 0, -1, 0), xyjm = o.s(5, 0, 0, -1);
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+    const float dxSxx = (xxp - xx0) * r20x;
+    const float dySyy = (yyp - yy0) * r20y;
+    const float dzSzz = (zzp - zz0) * r20z;
+    const float dySyz = (yz0 - yzjm) * r20y;
+    const float dzSyz = (yz0 - yzkm) * r20z;
+    const float dxSxz = (xz0 - xzim) * r20x;
+    const float dzSxz = (xz0 - xzkm) * r20z;
+    const float dxSxy = (xy0 - xyim) * r20x;
+    const float dySxy = (xy0 - xyjm) * r20y;
+
+    sts(&Vx[e], vx + bx * (gxe.x * dxSxx + gyc.x * dySxy + gzc.x * dzSxz
+                           + gxe.y * vxSxx + gyc.y * vySxy + gzc.y * vzSxz) * dt);
+    sts(&Vy[e], vy + by * (gxc.x * dxSxy + gye.x * dySyy + gzc.x * dzSyz
+                           + gxc.y * vxSxy + gye.y * vySyy + gzc.y * vzSyz) * dt);
+    sts(&Vz[e], vz + bz * (gxc.x * dxSxz + gyc.x * dySyz + gze.x * dzSzz
+                           + gxc.y * vxSxz + gyc.y * vySyz + gze.y * vzSzz) * dt);
+
+    sts(&axSxx[q], gxe.z * vxSxx + gxe.w * dxSxx * dt);
+    sts(&aySxy[q], gyc.z * vySxy + gyc.w * dySxy * dt);
+    sts(&azSxz[q], gzc.z * vzSxz + gzc.w * dzSxz * dt);
+    sts(&axSxy[q], gxc.z * vxSxy + gxc.w * dxSxy * dt);
+    sts(&aySyy[q], gye.z * vySyy + gye.w * dySyy * dt);
+    sts(&azSyz[q], gzc.z * vzSyz + gzc.w * dzSyz * dt);
+    sts(&axSxz[q], gxc.z * vxSxz + gxc.w * dxSxz * dt);
+    sts(&aySyz[q], gyc.z * vySyz + gyc.w * dySyz * dt);
+    sts(&azSzz[q], gze.z * vzSzz + gze.w * dzSzz * dt);
+}
+
+// absorb_p__update_stress (m_absorb_p.f90:445-491) for one absorber cell: the
+// auxiliaries from global memory, the other operands through the accessor
+template <int PREC, class Ops>
+__device__ __forceinline__ void stress_absorber(const Str3Args &a, const Ops &o, const Aux9 &x, int k, int i, int j,
+                                                long long e, long long ao, float *const (&S)[6]) {
+    const float dt = a.dt;
+    const long long q = x.q;
+    float *__restrict__ axVx = a.aV[0] + ao;
+    float *__restrict__ ayVx = a.aV[1] + ao;
+    float *__restrict__ azVx = a.aV[2] + ao;
+    float *__restrict__ axVy = a.aV[3] + ao;
+    float *__restrict__ ayVy = a.aV[4] + ao;
+    float *__restrict__ azVy = a.aV[5] + ao;
+    float *__restrict__ axVz = a.aV[6] + ao;
+    float *__restrict__ ayVz = a.aV[7] + ao;
+    float *__restrict__ azVz = a.aV[8] + ao;
+    // aux order of a.aV: axVx ayVx azVx axVy ayVy azVy axVz ayVz azVz
+    const float vaxVx = x.v[0], vayVy = x.v[4], vazVz = x.v[8];
+    const float vayVx = x.v[1], vazVx = x.v[2], vaxVy = x.v[3];
+    const float vazVy = x.v[5], vaxVz = x.v[6], vayVz = x.v[7];
+    const float sxx = o.sown(0), syy = o.sown(1), szz = o.sown(2);
+    const float syz = o.sown(3), sxz = o.sown(4), sxy = o.sown(5);
+    const float mu = o.med(0), lam = o.med(1);
+    const float muyz = o.med(4), muxz = o.med(5), muxy = o.med(6);
+    const float vx0 = o.v(0, 0, 0, 0), vy0 = o.v(1, 0, 0, 0), vz0 = o.v(2, 0, 0, 0);
+    const float vxim = o.v(0, 0, -1, 0), vyjm = o.v(1, 0, 0, -1), vzkm = o.v(2, -1, 0, 0);
+    const float vyip = o.v(1, 0, 1, 0), vzip = o.v(2, 0, 1, 0);
+    const float vxjp = o.v(0, 0, 0, 1), vzjp = o.v(2, 0, 0, 1);
+    const float vxkp = o.v(0, 1, 0, 0), vykp = o.v(1, 1, 0, 0);
+    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
+    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
+    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
+    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
+
+    const float dxVx = (vx0 - vxim) * r20x;
+    const float dyVy = (vy0 - vyjm) * r20y;
+    const float dzVz = (vz0 - vzkm) * r20z;
+    const float lam2mu_R = (lam + 2 * mu);
+    const float lam_R = lam2mu_R - 2 * mu;
+    const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
+    const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
+    const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
+    stS<PREC>(S[0], e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, a.iS[0]);
+    stS<PREC>(S[1], e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, a.iS[1]);
+    stS<PREC>(S[2], e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, a.iS[2]);
+    sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
+    sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
+    sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
+
+    const float dxVy = (vyip - vy0) * r20x;
+    const float dxVz = (vzip - vz0) * r20x;
+    const float dyVx = (vxjp - vx0) * r20y;
+    const float dyVz = (vzjp - vz0) * r20y;
+    const float dzVx = (vxkp - vx0) * r20z;
+    const float dzVy = (vykp - vy0) * r20z;
+    stS<PREC>(S[3], e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, a.iS[3]);
+    stS<PREC>(S[4], e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, a.iS[4]);
+    stS<PREC>(S[5], e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, a.iS[5]);
+    sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
+    sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
+    sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
+    sts(&azVy[q], gze.z * vazVy + gze.w * dzVy * dt);
+    sts(&axVz[q], gxe.z * vaxVz + gxe.w * dxVz * dt);
+    sts(&ayVz[q], gye.z * vayVz + gye.w * dyVz * dt);
+}
+
 // ---------------------------------------------------------------------------
 // velocity: kernel__update_vel (m_kernel.f90:75-140) +
 //           absorb_p__update_vel (m_absorb_p.f90:248-309)
@@ -255,61 +397,10 @@ __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j,
 
     // absorber cell: k >= kbeg_a(i, j) holds for every cell outside the kernel box
     if (!(a.mask & 2)) return;
-    const int2 pc = __ldg(&a.pmlcol[col]);
-    const long long q = (long long)pc.y + (k - pc.x);
-    float *__restrict__ axSxx = a.aS[0] + ao;
-    float *__restrict__ aySxy = a.aS[1] + ao;
-    float *__restrict__ azSxz = a.aS[2] + ao;
-    float *__restrict__ axSxy = a.aS[3] + ao;
-    float *__restrict__ aySyy = a.aS[4] + ao;
-    float *__restrict__ azSyz = a.aS[5] + ao;
-    float *__restrict__ axSxz = a.aS[6] + ao;
-    float *__restrict__ aySyz = a.aS[7] + ao;
-    float *__restrict__ azSzz = a.aS[8] + ao;
-    const float vxSxx = lds(&axSxx[q]), vySxy = lds(&aySxy[q]), vzSxz = lds(&azSxz[q]);
-    const float vxSxy = lds(&axSxy[q]), vySyy = lds(&aySyy[q]), vzSyz = lds(&azSyz[q]);
-    const float vxSxz = lds(&axSxz[q]), vySyz = lds(&aySyz[q]), vzSzz = lds(&azSzz[q]);
-    const float vx = lds(&Vx[e]), vy = lds(&Vy[e]), vz = lds(&Vz[e]);
-    const float bx = lds(&a.bx[e]), by = lds(&a.by[e]), bz = lds(&a.bz[e]);
-    const float xx0 = ldgS<PREC>(Sxx, e, a.sS[0]), xxp = ldgS<PREC>(Sxx, e + PI, a.sS[0]);
-    const float yy0 = ldgS<PREC>(Syy, e, a.sS[1]), yyp = ldgS<PREC>(Syy, e + PJ, a.sS[1]);
-    const float zz0 = ldgS<PREC>(Szz, e, a.sS[2]), zzp = ldgS<PREC>(Szz, e + 1, a.sS[2]);
-    const float yz0 = ldgS<PREC>(Syz, e, a.sS[3]), yzjm = ldgS<PREC>(Syz, e - PJ, a.sS[3]), yzkm = ldgS<PREC>(Syz, e - 1, a.sS[3]);
-    const float xz0 = ldgS<PREC>(Sxz, e, a.sS[4]), xzim = ldgS<PREC>(Sxz, e - PI, a.sS[4]), xzkm = ldgS<PREC>(Sxz, e - 1, a.sS[4]);
-    const float xy0 = ldgS<PREC>(Sxy, e, a.sS[5]), xyim = ldgS<PREC>(Sxy, e - PI, a.sS[5]), xyjm = ldgS<PREC>(Sxy, e - PJ, a.sS[5]);
-    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
-    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
-    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
-    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
-    const float dxSxx = (xxp - xx0) * r20x;
-    const float dySyy = (yyp - yy0) * r20y;
-    const float dzSzz = (zzp - zz0) * r20z;
-    const float dySyz = (yz0 - yzjm) * r20y;
-    const float dzSyz = (yz0 - yzkm) * r20z;
-    const float dxSxz = (xz0 - xzim) * r20x;
-    const float dzSxz = (xz0 - xzkm) * r20z;
-    const float dxSxy = (xy0 - xyim) * r20x;
-    const float dySxy = (xy0 - xyjm) * r20y;
-
-    sts(&Vx[e], vx + bx * (gxe.x * dxSxx + gyc.x * dySxy + gzc.x * dzSxz
-                           + gxe.y * vxSxx + gyc.y * vySxy + gzc.y * vzSxz) * dt);
-    sts(&Vy[e], vy + by * (gxc.x * dxSxy + gye.x * dySyy + gzc.x * dzSyz
-                           + gxc.y * vxSxy + gye.y * vySyy + gzc.y * vzSyz) * dt);
-    sts(&Vz[e], vz + bz * (gxc.x * dxSxz + gyc.x * dySyz + gze.x * dzSzz
-                           + gxc.y * vxSxz + gyc.y * vySyz + gze.y * vzSzz) * dt);
-
-    sts(&axSxx[q], gxe.z * vxSxx + gxe.w * dxSxx * dt);
-    sts(&aySxy[q], gyc.z * vySxy + gyc.w * dySxy * dt);
-    sts(&azSxz[q], gzc.z * vzSxz + gzc.w * dzSxz * dt);
-    sts(&axSxy[q], gxc.z * vxSxy + gxc.w * dxSxy * dt);
-    sts(&aySyy[q], gye.z * vySyy + gye.w * dySyy * dt);
-    sts(&azSyz[q], gzc.z * vzSyz + gzc.w * dzSyz * dt);
-    sts(&axSxz[q], gxc.z * vxSxz + gxc.w * dxSxz * dt);
-    sts(&aySyz[q], gyc.z * vySyz + gyc.w * dySyz * dt);
-    sts(&azSzz[q], gze.z * vzSzz + gze.w * dzSzz * dt);
+    const Aux9 x = aux_load(a.aS, ao, a.pmlcol, g, k, i, j);
+    const GVelOps<PREC> o{a, e, PI, PJ, {Sxx, Syy, Szz, Syz, Sxz, Sxy}, {Vx, Vy, Vz}};
+    vel_absorber<PREC>(a, o, x, k, i, j, e, ao, Vx, Vy, Vz);
 }
-
-
 
 // ---------------------------------------------------------------------------
 // stress: kernel__update_stress (m_kernel.f90:142-326) +
@@ -346,64 +437,10 @@ __device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int
 
     // absorber cell (m_absorb_p.f90:445-491)
     if (!(a.mask & 2)) return;
-    const int2 pc = __ldg(&a.pmlcol[col]);
-    const long long q = (long long)pc.y + (k - pc.x);
-    float *__restrict__ axVx = a.aV[0] + ao;
-    float *__restrict__ ayVx = a.aV[1] + ao;
-    float *__restrict__ azVx = a.aV[2] + ao;
-    float *__restrict__ axVy = a.aV[3] + ao;
-    float *__restrict__ ayVy = a.aV[4] + ao;
-    float *__restrict__ azVy = a.aV[5] + ao;
-    float *__restrict__ axVz = a.aV[6] + ao;
-    float *__restrict__ ayVz = a.aV[7] + ao;
-    float *__restrict__ azVz = a.aV[8] + ao;
-    const float vaxVx = lds(&axVx[q]), vayVy = lds(&ayVy[q]), vazVz = lds(&azVz[q]);
-    const float vayVx = lds(&ayVx[q]), vazVx = lds(&azVx[q]), vaxVy = lds(&axVy[q]);
-    const float vazVy = lds(&azVy[q]), vaxVz = lds(&axVz[q]), vayVz = lds(&ayVz[q]);
-    const float sxx = ldS<PREC>(Sxx, e, a.sS[0]), syy = ldS<PREC>(Syy, e, a.sS[1]), szz = ldS<PREC>(Szz, e, a.sS[2]);
-    const float syz = ldS<PREC>(Syz, e, a.sS[3]), sxz = ldS<PREC>(Sxz, e, a.sS[4]), sxy = ldS<PREC>(Sxy, e, a.sS[5]);
-    const float mu = lds(&a.mu[e]), lam = lds(&a.lam[e]);
-    const float muyz = lds(&a.muyz[e]), muxz = lds(&a.muxz[e]), muxy = lds(&a.muxy[e]);
-    const float vx0 = __ldg(&Vx[e]), vy0 = __ldg(&Vy[e]), vz0 = __ldg(&Vz[e]);
-    const float vxim = __ldg(&Vx[e - PI]), vyjm = __ldg(&Vy[e - PJ]), vzkm = __ldg(&Vz[e - 1]);
-    const float vyip = __ldg(&Vy[e + PI]), vzip = __ldg(&Vz[e + PI]);
-    const float vxjp = __ldg(&Vx[e + PJ]), vzjp = __ldg(&Vz[e + PJ]);
-    const float vxkp = __ldg(&Vx[e + 1]), vykp = __ldg(&Vy[e + 1]);
-    const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
-    const float4 gyc = __ldg(&a.gyc[j - 1]), gye = __ldg(&a.gye[j - 1]);
-    const float4 gzc = __ldg(&a.gzc[k - 1]), gze = __ldg(&a.gze[k - 1]);
-    const float r20x = a.r20[0], r20y = a.r20[1], r20z = a.r20[2];
-
-    const float dxVx = (vx0 - vxim) * r20x;
-    const float dyVy = (vy0 - vyjm) * r20y;
-    const float dzVz = (vz0 - vzkm) * r20z;
-    const float lam2mu_R = (lam + 2 * mu);
-    const float lam_R = lam2mu_R - 2 * mu;
-    const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
-    const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
-    const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
-    stS<PREC>(Sxx, e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, a.iS[0]);
-    stS<PREC>(Syy, e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, a.iS[1]);
-    stS<PREC>(Szz, e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, a.iS[2]);
-    sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
-    sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
-    sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
-
-    const float dxVy = (vyip - vy0) * r20x;
-    const float dxVz = (vzip - vz0) * r20x;
-    const float dyVx = (vxjp - vx0) * r20y;
-    const float dyVz = (vzjp - vz0) * r20y;
-    const float dzVx = (vxkp - vx0) * r20z;
-    const float dzVy = (vykp - vy0) * r20z;
-    stS<PREC>(Syz, e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, a.iS[3]);
-    stS<PREC>(Sxz, e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, a.iS[4]);
-    stS<PREC>(Sxy, e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, a.iS[5]);
-    sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
-    sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
-    sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
-    sts(&azVy[q], gze.z * vazVy + gze.w * dzVy * dt);
-    sts(&axVz[q], gxe.z * vaxVz + gxe.w * dxVz * dt);
-    sts(&ayVz[q], gye.z * vayVz + gye.w * dyVz * dt);
+    const Aux9 x = aux_load(a.aV, ao, a.pmlcol, g, k, i, j);
+    const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}};
+    float *const Sp[6] = {Sxx, Syy, Szz, Syz, Sxz, Sxy};
+    stress_absorber<PREC>(a, o, x, k, i, j, e, ao, Sp);
 }
 
 // ---------------------------------------------------------------------------

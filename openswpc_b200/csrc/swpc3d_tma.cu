@@ -15,9 +15,10 @@
 // per SM keep well over a hundred KB per SM in flight without holding
 // registers.  Each thread then updates its cell from shared memory with the
 // arithmetic of the one-cell kernels (stress_interior / vel_interior, the same
-// expression order), so the results are bitwise identical.  Absorber cells of
-// a tile take the one-cell path (stress_cell / vel_cell); tiles without
-// interior cells copy nothing.  The tensor boxes may reach past the grid at
+// expression order), so the results are bitwise identical.  Absorber cells
+// read the tile too (stress_absorber / vel_absorber); only their compact PML
+// auxiliaries come from global memory.  A stress tile without interior cells
+// copies S without R.  The tensor boxes may reach past the grid at
 // its edges: TMA fills those elements with zeros and they are never used.
 //
 // A CTA serves M members that share the medium (M = 1 for a single run; the
@@ -137,6 +138,12 @@ __device__ __forceinline__ bool tile_has_interior(const Tile &T, int bi, int bj,
                                                   int kek) {
     return T.k0 <= kek && T.i0 <= iek && T.i0 + bi - 1 >= ibk && T.j0 <= jek && T.j0 + bj - 1 >= jbk;
 }
+// does the tile hold absorber cells (cells of the grid outside the kernel region)?
+__device__ __forceinline__ bool tile_has_absorber(const Tile &T, int bi, int bj, const Geo &g, int ibk, int iek,
+                                                  int jbk, int jek, int kek) {
+    const int i1 = min(T.i0 + bi - 1, g.nx), j1 = min(T.j0 + bj - 1, g.ny), k1 = min(T.k0 + KT - 1, g.nz);
+    return T.i0 < ibk || i1 > iek || T.j0 < jbk || j1 > jek || k1 > kek;
+}
 
 __host__ __device__ constexpr int up32(int n) { return (n + 31) / 32 * 32; }
 template <int SMEM_FLOATS, int THREADS>
@@ -156,11 +163,14 @@ template <int NM, int BI, int BJ, int M>
 struct StrBoxes {
     static constexpr int nMed = 7 * BJ * BI * KT;
     static constexpr int nState = (6 + 6 * NM) * BJ * BI * KT;
+    static constexpr int nS = 6 * BJ * BI * KT;   // S alone (tiles without interior cells)
     static constexpr int nV = 3 * (BJ + 4) * (BI + 4) * KB;
     static constexpr int member = up32(nState) + up32(nV);
     static constexpr int total = up32(nMed) + M * member;
     __host__ __device__ static constexpr int oMem(int mm) { return up32(nMed) + mm * member; }
-    __host__ __device__ static constexpr int bytes(int nmem) { return 4 * (nMed + nmem * (nState + nV)); }
+    __host__ __device__ static constexpr int bytes(int nmem, bool with_r) {
+        return 4 * (nMed + nmem * ((with_r ? nState : nS) + nV));
+    }
 };
 
 template <int NM, int BI, int BJ>
@@ -181,8 +191,9 @@ struct SStrOps {
 
 template <int NM, int BI, int BJ, int M>
 __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, BJ, M>::total, KT * BI * BJ>()))
-    stress3d_tma_kernel(const __grid_constant__ CUtensorMap tm_state, const __grid_constant__ CUtensorMap tm_med,
-                        const __grid_constant__ CUtensorMap tm_v, const Str3Args a, const TmaTiles t) {
+    stress3d_tma_kernel(const __grid_constant__ CUtensorMap tm_state, const __grid_constant__ CUtensorMap tm_s,
+                        const __grid_constant__ CUtensorMap tm_med, const __grid_constant__ CUtensorMap tm_v,
+                        const Str3Args a, const TmaTiles t) {
     using L = StrBoxes<NM, BI, BJ, M>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
@@ -192,40 +203,51 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
     const Tile T = tile_of<M>(t, BI, BJ);
     const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
     const bool lead = tx == 0 && ty == 0 && tz == 0;
-    const bool staged = (a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    // cells of this launch in the tile: interior ones need S, R and the medium, absorber ones S and the medium
+    const bool with_r = (a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    const bool staged =
+        with_r || ((a.mask & 2) && tile_has_absorber(T, BI, BJ, g, a.ibk, a.iek, a.jbk, a.jek, a.kek));
     bool ok = true;
     if (staged && !stage_begin(&bar, &go, t.err, lead)) ok = false;
-    else if (staged) {
-        if (lead) {
-            mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem));
-            const int x0 = T.k0 - 1 + KH;
-            tma_load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
-            for (int mm = 0; mm < T.nmem; mm++) {
-                const int fm = (T.m0 + mm) * t.f_member;
-                float *p = sm + L::oMem(mm);
-                tma_load_4d(p, &tm_state, x0, T.i0 + 2, T.j0 + 2, t.f_state + fm, &bar);
-                tma_load_4d(p + up32(L::nState), &tm_v, x0 - 4, T.i0, T.j0, t.f_v + fm, &bar);
-            }
+    else if (staged && lead) {
+        mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem, with_r));
+        const int x0 = T.k0 - 1 + KH;
+        tma_load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
+        for (int mm = 0; mm < T.nmem; mm++) {
+            const int fm = (T.m0 + mm) * t.f_member;
+            float *p = sm + L::oMem(mm);
+            tma_load_4d(p, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state + fm, &bar);
+            tma_load_4d(p + up32(L::nState), &tm_v, x0 - 4, T.i0, T.j0, t.f_v + fm, &bar);
         }
-        ok = wait_tiles(&bar, t.err);
     }
     const int k = T.k0 + tx, i = T.i0 + ty, j = T.j0 + tz;
-    if (k > g.nz || i > g.nx || j > g.ny) return;
     const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+    const bool mine = k <= g.nz && i <= g.nx && j <= g.ny && (a.mask & (interior ? 1 : 2));
+    // an absorber cell's auxiliaries travel while the tiles do (up to two members)
+    constexpr bool PRE = M <= 2;
+    Aux9 xs[PRE ? M : 1];
+    if (PRE && staged && ok && mine && !interior) {
+#pragma unroll
+        for (int mm = 0; mm < (PRE ? M : 1); mm++)
+            if (mm < T.nmem) xs[mm] = aux_load(a.aV, (long long)(T.m0 + mm) * t.ao, a.pmlcol, g, k, i, j);
+    }
+    if (staged && ok) ok = wait_tiles(&bar, t.err);
+    if (!staged || !ok || !mine) return;   // nothing of this launch here, or the copy failed
     const long long col = col_index(g, i, j);
     const long long e = col * g.Kp + (k - 1 + KH);
-#pragma unroll 1
-    for (int mm = 0; mm < T.nmem; mm++) {
+#pragma unroll
+    for (int mm = 0; mm < M; mm++) {
+        if (mm >= T.nmem) break;
         const long long so = (long long)(T.m0 + mm) * t.so, ao = (long long)(T.m0 + mm) * t.ao;
-        if (!interior) {
-            stress_cell<NM, PREC_F32>(a, k, i, j, so, ao);   // absorber cell
-            continue;
-        }
-        if (!staged || !ok) continue;   // interior cells not in this launch (mask), or the copy failed
         const float *p = sm + L::oMem(mm);
         const SStrOps<NM, BI, BJ> o{p, p + up32(L::nState), sm, tx, ty, tz};
         float *const Sp[6] = {a.Sxx + so, a.Syy + so, a.Szz + so, a.Syz + so, a.Sxz + so, a.Sxy + so};
-        stress_interior<NM, PREC_F32>(a, o, band_sign_of(a.band, col, k), Sp, e, so);
+        if (interior) {
+            stress_interior<NM, PREC_F32>(a, o, band_sign_of(a.band, col, k), Sp, e, so);
+        } else {
+            const Aux9 x = PRE ? xs[PRE ? mm : 0] : aux_load(a.aV, ao, a.pmlcol, g, k, i, j);
+            stress_absorber<PREC_F32>(a, o, x, k, i, j, e, ao, Sp);
+        }
     }
 }
 
@@ -295,46 +317,63 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
     const Tile T = tile_of<M>(t, BI, BJ);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool lead = tx == 0 && ty == 0;
-    const bool staged = (a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    const bool staged = ((a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek)) ||
+                        ((a.mask & 2) && tile_has_absorber(T, BI, BJ, g, a.ibk, a.iek, a.jbk, a.jek, a.kek));
     bool ok = true;
     if (staged && !stage_begin(&bar, &go, t.err, lead)) ok = false;
-    else if (staged) {
-        if (lead) {
-            mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem));
-            const int x0 = T.k0 - 1 + KH, ic = T.i0 + 2, jc = T.j0 + 2;
-            tma_load_4d(sm, &tm_b, x0, ic, jc, t.f_b, &bar);
-            for (int mm = 0; mm < T.nmem; mm++) {
-                const int f = t.f_v + (T.m0 + mm) * t.f_member;   // Vx of the member; S follows at f + 3
-                float *p = sm + L::oMem(mm);
-                tma_load_4d(p + L::oV, &tm_own, x0, ic, jc, f, &bar);
-                tma_load_4d(p + L::oA, &tm_a, x0, ic - 1, jc, f + 3, &bar);
-                tma_load_4d(p + L::oBy, &tm_by, x0, ic, jc - 1, f + 4, &bar);
-                tma_load_4d(p + L::oC, &tm_c, x0 - 4, ic, jc, f + 5, &bar);
-                tma_load_4d(p + L::oF, &tm_f, x0 - 4, ic, jc - 2, f + 6, &bar);
-                tma_load_4d(p + L::oE, &tm_e, x0 - 4, ic - 2, jc, f + 7, &bar);
-                tma_load_4d(p + L::oD, &tm_d, x0, ic - 2, jc - 2, f + 8, &bar);
-            }
+    else if (staged && lead) {
+        mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem));
+        const int x0 = T.k0 - 1 + KH, ic = T.i0 + 2, jc = T.j0 + 2;
+        tma_load_4d(sm, &tm_b, x0, ic, jc, t.f_b, &bar);
+        for (int mm = 0; mm < T.nmem; mm++) {
+            const int f = t.f_v + (T.m0 + mm) * t.f_member;   // Vx of the member; S follows at f + 3
+            float *p = sm + L::oMem(mm);
+            tma_load_4d(p + L::oV, &tm_own, x0, ic, jc, f, &bar);
+            tma_load_4d(p + L::oA, &tm_a, x0, ic - 1, jc, f + 3, &bar);
+            tma_load_4d(p + L::oBy, &tm_by, x0, ic, jc - 1, f + 4, &bar);
+            tma_load_4d(p + L::oC, &tm_c, x0 - 4, ic, jc, f + 5, &bar);
+            tma_load_4d(p + L::oF, &tm_f, x0 - 4, ic, jc - 2, f + 6, &bar);
+            tma_load_4d(p + L::oE, &tm_e, x0 - 4, ic - 2, jc, f + 7, &bar);
+            tma_load_4d(p + L::oD, &tm_d, x0, ic - 2, jc - 2, f + 8, &bar);
         }
-        ok = wait_tiles(&bar, t.err);
     }
     const int k = T.k0 + tx, i = T.i0 + ty;
-    if (k > g.nz || i > g.nx) return;
-#pragma unroll 1
-    for (int mm = 0; mm < T.nmem; mm++) {
+    const bool col_ok = k <= g.nz && i <= g.nx;
+    // the auxiliaries of this thread's absorber cells travel while the tiles do
+    // (up to two cells: BJ planes x M members)
+    constexpr bool PRE = BJ * M <= 2;
+    Aux9 xs[PRE ? M : 1][PRE ? BJ : 1];
+    if (PRE && staged && ok && col_ok && (a.mask & 2)) {
+#pragma unroll
+        for (int mm = 0; mm < (PRE ? M : 1); mm++)
+#pragma unroll
+            for (int jj = 0; jj < (PRE ? BJ : 1); jj++) {
+                const int j = T.j0 + jj;
+                if (mm < T.nmem && j <= g.ny && !(i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek))
+                    xs[mm][jj] = aux_load(a.aS, (long long)(T.m0 + mm) * t.ao, a.pmlcol, g, k, i, j);
+            }
+    }
+    if (staged && ok) ok = wait_tiles(&bar, t.err);
+    if (!staged || !ok || !col_ok) return;   // nothing of this launch here, or the copy failed
+#pragma unroll
+    for (int mm = 0; mm < M; mm++) {
+        if (mm >= T.nmem) break;
         const long long so = (long long)(T.m0 + mm) * t.so, ao = (long long)(T.m0 + mm) * t.ao;
-#pragma unroll 1
+#pragma unroll
         for (int jj = 0; jj < BJ; jj++) {
             const int j = T.j0 + jj;
             if (j > g.ny) break;
-            if (!(i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek)) {
-                vel_cell<PREC_F32>(a, k, i, j, so, ao);   // absorber cell
-                continue;
-            }
-            if (!staged || !ok) continue;   // interior cells not in this launch (mask), or the copy failed
+            const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+            if (!(a.mask & (interior ? 1 : 2))) continue;
             const SVelOps<BI, BJ> o{sm + L::oMem(mm), sm, tx, ty, jj};
-            const long long col = col_index(g, i, j);
-            const long long e = col * g.Kp + (k - 1 + KH);
-            vel_interior<PREC_F32>(a, o, band_sign_of(a.band, col, k), a.Vx + so, a.Vy + so, a.Vz + so, e);
+            const long long e = col_index(g, i, j) * g.Kp + (k - 1 + KH);
+            if (interior) {
+                vel_interior<PREC_F32>(a, o, band_sign_of(a.band, col_index(g, i, j), k), a.Vx + so, a.Vy + so,
+                                       a.Vz + so, e);
+            } else {
+                const Aux9 x = PRE ? xs[PRE ? mm : 0][PRE ? jj : 0] : aux_load(a.aS, ao, a.pmlcol, g, k, i, j);
+                vel_absorber<PREC_F32>(a, o, x, k, i, j, e, ao, a.Vx + so, a.Vy + so, a.Vz + so);
+            }
         }
     }
 }
@@ -358,7 +397,8 @@ cudaError_t run_stress(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, c
     cudaError_t e = smem_attr(stress3d_tma_kernel<NM, BI, BJ, M>, bytes, devices);
     if (e != cudaSuccess) return e;
     const unsigned nblk = (unsigned)((long long)t.nkt * t.nit * t.njt * t.mgroups);
-    stress3d_tma_kernel<NM, BI, BJ, M><<<nblk, dim3(KT, BI, BJ), bytes, st>>>(map(m.state), map(m.med), map(m.vh), a, t);
+    stress3d_tma_kernel<NM, BI, BJ, M><<<nblk, dim3(KT, BI, BJ), bytes, st>>>(map(m.state), map(m.s6), map(m.med),
+                                                                               map(m.vh), a, t);
     return cudaGetLastError();
 }
 
@@ -466,6 +506,7 @@ static bool encode(unsigned char *out, float *slab, const Geo &g, long long nf, 
 
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj) {
     return encode(m.state, s.state, g, s.nf_state, KT, bi, bj, 6 + 6 * nm) &&
+           encode(m.s6, s.state, g, s.nf_state, KT, bi, bj, 6) &&
            encode(m.med, s.med, g, s.nf_med, KT, bi, bj, 7) && encode(m.vh, s.state, g, s.nf_state, KB, bi + 4, bj + 4, 3);
 }
 

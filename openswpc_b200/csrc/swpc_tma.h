@@ -33,6 +33,7 @@ struct TmaSlabs {
 // host copies of the tensor maps (CUtensorMap, 128 bytes, 64-byte aligned)
 struct alignas(64) TmaMaps {
     unsigned char state[128];   // stress: S and R of a member
+    unsigned char s6[128];      // stress: S of a member (tiles without interior cells)
     unsigned char med[128];     // stress: the seven medium fields of the stress update
     unsigned char vh[128];      // stress: V of a member with halo
     unsigned char own3[128];    // velocity: V of a member
