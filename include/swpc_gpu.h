@@ -310,9 +310,12 @@ int swpc_fbatch_set_strip(swpc_fbatch *b, int strip_cells);
  * stress (4,2) and velocity (4,2) with 2 members per CTA).  Compiled stress
  * (bi, bj, mpc): (4,4,1) (2,4,1) (4,2,1) (4,2,2) (2,4,2) (2,2,2) (2,2,4)
  * (4,1,4); velocity: (4,2,1) (4,4,1) (2,2,1) (4,2,2) (2,2,2) (4,1,2) (2,2,4)
- * (4,1,4).  swpc_fbatch_autotune tunes the form in use (strip widths, or
- * the staged shapes of stress then velocity); swpc_fbatch_get_launch writes
- * {staged, strip, stress bi, bj, mpc, velocity bi, bj, mpc} to out[8]. */
+ * (4,1,4).  kernel 7 sets the staged launch order: mpc = 0 member groups
+ * fastest (the medium of a tile is re-read from L2), 1 tiles fastest (the
+ * halos of neighbouring tiles are).  swpc_fbatch_autotune tunes the form in
+ * use (strip widths, or the staged order and the shapes of stress then
+ * velocity); swpc_fbatch_get_launch writes {staged, strip, stress bi, bj,
+ * mpc, velocity bi, bj, mpc, tiles first} to out[9]. */
 int swpc_fbatch_set_launch(swpc_fbatch *b, int kernel, int mpc, int bi, int bj);
 int swpc_fbatch_get_launch(const swpc_fbatch *b, int *out);
 int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *steps_used, int *strip);

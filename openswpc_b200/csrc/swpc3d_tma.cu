@@ -122,13 +122,17 @@ __device__ __forceinline__ bool stage_begin(uint64_t *bar, int *flag, const int 
 }
 
 // tile and member group of this CTA: member group fastest, then k, i, j
+// (the medium of a tile is re-read from L2 by the groups that follow), or with
+// t.tiles_first the tiles fastest and the groups one after another (the halos
+// of neighbouring tiles are re-read from L2, as in a run of its own)
 struct Tile {
     int k0, i0, j0, m0, nmem;   // first cell, first member, members in the group
 };
 template <int M>
 __device__ __forceinline__ Tile tile_of(const TmaTiles &t, int bi, int bj) {
-    const int grp = blockIdx.x % t.mgroups;
-    const int b = blockIdx.x / t.mgroups;
+    const int ntile = t.nkt * t.nit * t.njt;
+    const int grp = t.tiles_first ? blockIdx.x / ntile : blockIdx.x % t.mgroups;
+    const int b = t.tiles_first ? blockIdx.x % ntile : blockIdx.x / t.mgroups;
     const int kt = b % t.nkt, it = (b / t.nkt) % t.nit, jt = b / (t.nkt * t.nit);
     const int m0 = grp * M;
     return Tile{1 + KT * kt, 1 + bi * it, 1 + bj * jt, m0, min(M, t.nmem - m0)};

@@ -766,6 +766,7 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc) {
     t.njt = (c->g.ny + bj - 1) / bj;
     t.nmem = nmem;
     t.mgroups = (nmem + mpc - 1) / mpc;
+    t.tiles_first = 0;
     t.f_v = 0;
     t.f_state = 3;
     t.f_member = 0;

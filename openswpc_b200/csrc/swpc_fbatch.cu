@@ -63,6 +63,7 @@ struct swpc_fbatch {
     int strip = 0;                 // i-strip width in cells (0: automatic), flat kernels
     bool staged = false;           // TMA-staged kernels (FP32 contexts with a field slab)
     int sbi = 4, sbj = 2, smpc = 2, vbi = 4, vbj = 2, vmpc = 2;   // staged tiles and members per CTA
+    int tiles_first = 0;           // staged launch order (see swpc3d_tma.cu tile_of)
     void *tmaps = nullptr;         // swpc::TmaMaps over the batch slab and the context's medium
     int tma_key[4] = {-1, -1, -1, -1};
     int *d_it = nullptr;
@@ -276,8 +277,10 @@ extern "C" int swpc_fbatch_set_launch(swpc_fbatch *b, int kernel, int mpc, int b
         b->staged = true;
         if (kernel == 5) { b->sbi = bi; b->sbj = bj; b->smpc = mpc; }
         else { b->vbi = bi; b->vbj = bj; b->vmpc = mpc; }
+    } else if (kernel == 7) {
+        b->tiles_first = mpc != 0;
     } else {
-        return ferr(b, SWPC_ERR_ARG, "kernel must be 0 (flat), 5 (staged stress) or 6 (staged velocity)");
+        return ferr(b, SWPC_ERR_ARG, "kernel must be 0 (flat), 5 (staged stress), 6 (staged velocity) or 7 (order)");
     }
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
     return SWPC_OK;
@@ -367,6 +370,7 @@ static TmaTiles fb_tiles(const swpc_fbatch *b, int bi, int bj, int mpc) {
     t.f_member = b->nfs;
     t.so = b->stride;
     t.ao = b->astride;
+    t.tiles_first = b->tiles_first;
     return t;
 }
 
@@ -544,6 +548,18 @@ extern "C" int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *step
     const int nt = b->c->d.nt;
     if (b->staged) {
         // staged kernels: members per CTA and tile of the stress kernel, then of the velocity kernel
+        // launch order with the current shapes, then the shapes
+        {
+            int best = 0;
+            float best_ms = 1e30f;
+            for (int q = 0; q < 2 && it + 2 * reps - 1 <= nt; q++) {
+                FRC(swpc_fbatch_set_launch(b, 7, q, 0, 0));
+                float ms = 0.f;
+                FRC(fb_time(b, &it, reps, &ms));
+                if (ms < best_ms) { best_ms = ms; best = q; }
+            }
+            FRC(swpc_fbatch_set_launch(b, 7, best, 0, 0));
+        }
         const int sc[][3] = {{4, 2, 2}, {4, 4, 1}, {2, 4, 2}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
         const int vc[][3] = {{4, 2, 2}, {4, 2, 1}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
         for (int kernel = 5; kernel <= 6; kernel++) {
@@ -583,8 +599,8 @@ extern "C" int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *step
 
 extern "C" int swpc_fbatch_get_launch(const swpc_fbatch *b, int *out) {
     if (!b || !out) return SWPC_ERR_ARG;
-    const int v[8] = {b->staged ? 1 : 0, b->strip, b->sbi, b->sbj, b->smpc, b->vbi, b->vbj, b->vmpc};
-    std::copy(v, v + 8, out);
+    const int v[9] = {b->staged ? 1 : 0, b->strip, b->sbi, b->sbj, b->smpc, b->vbi, b->vbj, b->vmpc, b->tiles_first};
+    std::copy(v, v + 9, out);
     return SWPC_OK;
 }
 

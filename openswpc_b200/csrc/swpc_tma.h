@@ -13,6 +13,7 @@ namespace swpc {
 struct TmaTiles {
     int nkt, nit, njt;
     int nmem, mgroups;   // members, groups of members per CTA
+    int tiles_first;     // launch order: 0 member groups fastest, 1 tiles fastest
     int f_v;             // state slab: Vx of member 0 (S follows at f_v + 3)
     int f_state;         // state slab: Sxx of member 0 (S, then R)
     int f_member;        // state slab: field stride between members

@@ -557,14 +557,15 @@ class ForceBatch3D:
 
     def set_launch(self, kernel: int, mpc: int = 1, bi: int = 4, bj: int = 2):
         """kernel 0: flat kernels; 5 / 6: staged stress / velocity kernels with
-        tile (bi, bj) and mpc members per CTA."""
+        tile (bi, bj) and mpc members per CTA; 7: staged launch order (mpc 1:
+        tiles fastest, 0: member groups fastest)."""
         check(self.base.ctx, self.lib.swpc_fbatch_set_launch(self.b, kernel, mpc, bi, bj))
 
     def launch(self) -> dict:
-        out = np.zeros(8, np.int32)
+        out = np.zeros(9, np.int32)
         check(self.base.ctx, self.lib.swpc_fbatch_get_launch(self.b, iptr(out)))
         return {"staged": bool(out[0]), "strip": int(out[1]), "stress": tuple(int(v) for v in out[2:5]),
-                "velocity": tuple(int(v) for v in out[5:8])}
+                "velocity": tuple(int(v) for v in out[5:8]), "tiles_first": bool(out[8])}
 
     def autotune(self, it0: int, reps: int = 2):
         """Tunes the launch form in use (strip widths, or the staged shapes)

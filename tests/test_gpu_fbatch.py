@@ -32,8 +32,9 @@ def single(p, xi, station, cmp):
 
 # launch forms: flat kernels with two strip widths; staged kernels with 1, 2
 # and 4 members per CTA (5 members: the last group is partial)
-LAUNCHES = [("flat", 0), ("flat", 8), ("staged", (4, 4, 1, 4, 2, 1)), ("staged", (4, 2, 2, 4, 2, 2)),
-            ("staged", (2, 2, 4, 2, 2, 4)), ("staged", (4, 1, 4, 4, 1, 4)), ("staged", (2, 4, 2, 2, 2, 2))]
+LAUNCHES = [("flat", 0), ("flat", 8), ("staged", (4, 4, 1, 4, 2, 1, 0)), ("staged", (4, 2, 2, 4, 2, 2, 0)),
+            ("staged", (2, 2, 4, 2, 2, 4, 0)), ("staged", (4, 1, 4, 4, 1, 4, 1)), ("staged", (2, 4, 2, 2, 2, 2, 1)),
+            ("staged", (4, 4, 1, 4, 2, 1, 1))]
 
 
 @pytest.mark.parametrize("launch", LAUNCHES)
@@ -48,9 +49,10 @@ def test_members_equal_single_green_runs(launch):
         fb.set_launch(0)
         fb.set_strip(arg)
     else:
-        sbi, sbj, smpc, vbi, vbj, vmpc = arg
+        sbi, sbj, smpc, vbi, vbj, vmpc, order = arg
         fb.set_launch(5, smpc, sbi, sbj)
         fb.set_launch(6, vmpc, vbi, vbj)
+        fb.set_launch(7, order)
     fb.run(1, p.nt)
     fields = list(range(9)) + [_lib.F_R + 3 * c + m for c in range(6) for m in range(p.nm)]
     for m, (s, c) in enumerate(FORCES):
@@ -92,7 +94,7 @@ def test_autotune_keeps_results_and_bad_member_is_rejected():
     base.record(p.stations)
     fb = ForceBatch3D(base, [(p.stations[0], "z"), (p.stations[1], "x")])
     used, _ = fb.autotune(1, reps=2)
-    assert 0 < used <= 48 and fb.launch()["staged"]
+    assert 0 < used <= 56 and fb.launch()["staged"]
     fb.set_launch(0)
     used2, strip = fb.autotune(1 + used, reps=2)
     assert used2 > 0 and strip >= 8
