@@ -53,8 +53,8 @@ BYTES = {"f32": (232, 152, 60, 132), "bf16r": (160, 152, 60, 132), "f16sr": (136
 FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic of one launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the c1 mix scaled
 # down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
-# algorithmic bytes, for the default (TMA-staged) kernels; profiles/stress3d_tma_kernel_256x256x128_na8.md and
-# profiles/vel3d_tma_kernel_256x256x128_na8.md
+# algorithmic bytes, for the default (TMA-staged) kernels (the ncu summaries of stress3d_tma_kernel and
+# vel3d_tma_kernel on that grid, under profiles/)
 TRAFFIC_PER_ALGORITHMIC = {"stress": (1.250347e9 + 0.715447e9) / 1.828028416e9,
                            "vel": (0.509357e9 + 0.124435e9) / 0.609632256e9}
 
@@ -95,6 +95,18 @@ def make_params(name: str):
 # 2D P-SV algorithmic bytes per cell-update (FP32, nm = 3): velocity phase 2 V read+write, 3 S, rho; stress
 # phase 2 V, 3 S read+write, 9 R read+write, lam, mu, taup, taus (interior); PML: 34 floats
 B_PSV_INT, B_PSV_PML = 38 * 4, 34 * 4
+# one adjoint step per cell (FP32 state, FP64 gradients, nm = 3), interior / absorber: velocity weights (lV, b
+# read, nine w40 + nine w41 written, S of the slot read, three b gradients read and written; absorber: nine PML
+# auxiliaries read and written instead of S and the gradients), velocity gather (18 weights read, six lS read and
+# written), stress weights (lS, seven medium fields, 18 lR read and written, 18 weights written, V of the slot, five
+# medium gradients read and written; absorber: lS, five medium fields, nine auxiliaries, 18 weights), stress gather
+# (18 weights read, three lV read and written)
+B_ADJ_INT = (12 + 12 + 72 + 24 + 48) + (72 + 48) + (24 + 28 + 144 + 72 + 12 + 80) + (72 + 24)
+B_ADJ_PML = (12 + 12 + 72 + 72) + (72 + 48) + (24 + 20 + 72 + 72) + (72 + 24)
+# V and S of every recomputed step copied into the segment's slots (read and written)
+B_SLOT = 9 * 4 * 2
+# V, S and R (27 fields) saved at each checkpoint and restored before the segment's recompute
+B_CKPT = 27 * 4 * 2 * 2
 
 
 def make_c2a_models(n: int = 64, seed: int = 20260203):
@@ -184,6 +196,9 @@ def bench_c2a(args, world, rank, local):
     lib = _lib.load()
     batch = Batch2D(runs)
     used, ti, ri, bps = batch.autotune(1, reps=2)
+    pick = batch.launch()
+    kern = " + ".join([("stress2d_tma_kernel" if pick["stress_ti"] else "tile2d_kernel (stress)"),
+                       ("vel2d_tma_kernel" if pick["vel_ti"] else "tile2d_kernel (velocity)")])
     it0 = 1 + used
     batch.run(it0, args.warmup)
     it0 += args.warmup
@@ -255,8 +270,8 @@ def bench_c2a(args, world, rank, local):
                                  "what": "each member alone through per-step swpc_step calls, one after another"},
             "batched_over_loop": ms_loop / ms_batch,
             "batched_over_loop_calls": ms_calls / ms_batch,
-            "autotune": {"threads_i": ti, "rows_per_thread": ri, "blocks_per_sm": bps, "steps_used": used},
-            "roofline": {"bound": "hbm", "kernel": "psv_stress_kernel + psv_vel_kernel (whole batched step)",
+            "autotune": {**pick, "steps_used": used},
+            "roofline": {"bound": "hbm", "kernel": f"{kern} (whole batched step)",
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": bytes_step},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
@@ -504,6 +519,16 @@ def bench_c3(args, world, rank, local):
     t_e2e = time.perf_counter() - t0
     h2d = sum(a.nbytes for a in (vp, vs, rho)) * 2 + obsf.nbytes
     d2h = sum(t.grad.numel() * 8 for t in tv) + obsf.nbytes
+    # algorithmic bytes of one gradient: forward and recompute (the 3D step each), slot copies, the adjoint step,
+    # checkpoint save and restore
+    n_int, n_pml = cell_counts(p)
+    nseg = -(-p.nt // ckpt)
+    b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
+    b_grad = (p.nt * (2 * b_fwd + (n_int + n_pml) * B_SLOT + n_int * B_ADJ_INT + n_pml * B_ADJ_PML)
+              + nseg * (n_int + n_pml) * B_CKPT)
+    peak, peak_kind = hbm_peak()
+    ach = b_grad / (grad / 1e3) / 1e9
+    ach_fwd = p.nt * b_fwd / (fwd / 1e3) / 1e9
     line = {"metric": metric, "value": cells * p.nt / (grad / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": grad, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + "
@@ -513,6 +538,14 @@ def bench_c3(args, world, rank, local):
             "misfit": J.value,
             "forward_ms": fwd, "forward_gcells": cells * p.nt / (fwd / 1e3) / 1e9,
             "gradient_over_forward": grad / fwd,
+            "algorithmic_gradient_over_forward": b_grad / (p.nt * b_fwd),
+            "roofline": {"bound": "hbm", "kernel": "whole gradient: stress3d_tma_kernel + vel3d_tma_kernel (forward "
+                                                     "and recompute), adj_*_kernel (adjoint step), slot and "
+                                                     "checkpoint copies",
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes_per_step": b_grad},
+            "roofline_forward": {"achieved": ach_fwd, "frac": ach_fwd / peak,
+                                 "algorithmic_bytes_per_step": p.nt * b_fwd},
             "e2e": {"value": cells * p.nt / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "what": "waveform_misfit(vp, vs, rho) + backward from CPU tensors: medium setup on the host, "
@@ -521,6 +554,14 @@ def bench_c3(args, world, rank, local):
             # adjoint steps (two weight and two gather kernels, residual injection), zeroing of 8 gradients
             "gpu_launches": args.steps * (p.nt * (5 + 4 + 5) + 8), "clocks": clk.summary()}
     prob.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        # the reference has no adjoint: its CPU cost of a gradient is at least its forward run, timed here
+        v, n, sc, dt = cpu_reference(p, None, 1000, 1, os.cpu_count() or 1, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"oracle f32 forward of the starting model on the centre "
+                                          f"{min(256, p.nx)}x{min(256, p.ny)}x{p.nz} column block, {n} steps after "
+                                          f"1 warm-up ({dt:.1f} s); the reference has no adjoint, so this is the "
+                                          f"forward part of a gradient only"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 

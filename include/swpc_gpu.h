@@ -411,12 +411,15 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * for (1..4; fewer blocks leave more registers for operands in flight).
  * kernel 4 selects the velocity kernel with four k per thread.  kernel 5 / 6
  * select the TMA-staged stress / velocity kernels (FP32 3D contexts): a CTA
- * per tile of kt (k) x bi (i) x bj (j) cells whose operands arrive in shared
- * memory by bulk tensor copies; here minb selects kt (1: 32, 2: 64), and the
- * compiled tiles are stress (32,4,4) (32,2,4) (32,4,2) (64,4,2) (64,2,2)
- * (64,2,4) (64,4,1), velocity (32,4,2) (32,4,4) (32,2,2) (64,4,2) (64,2,2)
- * (64,4,1) (64,2,4) (64,4,4).  FP32 3D contexts start with kernels 5 (32,4,4)
- * and 6 (32,4,2); the other forms start with kernels 0 and 1.
+ * per tile of 32 (k) x bi (i) x bj (j) cells whose operands arrive in shared
+ * memory by bulk tensor copies; minb must be 1, and the compiled tiles
+ * (bi, bj) are stress (4,4) (2,4) (4,2), velocity (4,2) (4,4) (2,2).  FP32
+ * 3D contexts start with kernels 5 (4,4) and 6 (4,2); the other 3D forms
+ * start with kernels 0 and 1.
+ * 2D contexts (P-SV, SH) take kernels 0 / 1 (the tile-walking stress /
+ * velocity kernels) and 5 / 6 (the staged ones: a CTA per 32 x 16 tile with
+ * bi = 4, 8 or 16 threads along i, minb 1, bj 1); they start with kernels
+ * 5 and 6 at bi = 8.
  * The defaults come from sweeps on B200.  No counterpart in the reference
  * (its OpenMP/OpenACC schedules are fixed at compile time); results are
  * bitwise independent of the variant. */
@@ -432,26 +435,38 @@ int swpc_set_launch(swpc_ctx *ctx, int kernel, int minb, int bi, int bj);
  * (work/auto_chengyu.py:68-110) and has no counterpart inside the solver.
  * The batch snapshots its members at creation: set every member up first.
  * Batch work runs on the batch's own stream; call swpc_batch_sync before
- * reading a member's fields or traces. */
+ * reading a member's fields or traces (it also reports a staged tile copy
+ * that did not complete, SWPC_ERR_CUDA). */
 typedef struct swpc_batch swpc_batch;
 int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **out);
 int swpc_batch_step(swpc_batch *b, int it);
 int swpc_batch_run(swpc_batch *b, int it0, int nsteps);
 int swpc_batch_sync(swpc_batch *b);
 int swpc_batch_time_steps(swpc_batch *b, int it0, int nsteps, float *ms);
-/* Autotuner of the batched launch shape: tiles of 32 (k) x (ti*ri) (i)
- * cells, a block of 32 x ti threads with ri rows per thread, a persistent
- * grid of 148 x bps blocks (bps = 0: one block per tile).  It advances the batch by real time steps from
- * it0 -- every candidate shape runs `reps` steps timed with CUDA events --
- * and keeps the fastest shape; the results do not depend on the shape, so
- * these are ordinary steps of the run.  *used = steps taken (it0 ..
- * it0 + *used - 1); *best_ti, *best_ri, *best_bps (may be NULL) = the pick.
- * No counterpart in the reference. */
+/* Autotuner of the batched launch.  Candidates: the TMA-staged kernels on
+ * tiles of 32 (k) x 16 (i) cells with 4, 8 or 16 threads along i in the
+ * stress and velocity CTAs, and the tile-walking kernels on tiles of 32 (k) x
+ * (ti*ri) (i) cells, a block of 32 x ti threads with ri rows per thread, a
+ * persistent grid of 148 x bps blocks (bps = 0: one block per tile).  It
+ * advances the batch by real time steps from it0 -- every candidate runs
+ * `reps` steps timed with CUDA events (12 candidates) -- and keeps the
+ * fastest; the results do not depend on the launch, so these are ordinary
+ * steps of the run.  *used = steps taken (it0 .. it0 + *used - 1); *best_ti,
+ * *best_ri, *best_bps (may be NULL) = the tile shape of the pick (see
+ * swpc_batch_get_launch for the whole pick).  No counterpart in the
+ * reference. */
 int swpc_batch_autotune(swpc_batch *b, int it0, int reps, int *used, int *best_ti, int *best_ri, int *best_bps);
-/* Sets the launch shape directly (ti threads in i per block, 32*ti <= 256;
+/* Sets the tile shape directly (ti threads in i per block, 32*ti <= 256;
  * ri rows per thread; bps blocks per SM of the persistent grid, 0 = one block
- * per tile). */
+ * per tile).  A shape with ti*ri != 16 selects the tile-walking kernels. */
 int swpc_batch_set_shape(swpc_batch *b, int ti, int ri, int bps);
+/* Selects the TMA-staged kernels (stress_ti / vel_ti = 4, 8 or 16 threads
+ * along i of the stress / velocity CTA) or the tile-walking kernels (0) per
+ * phase; staged kernels switch the tiles to 32 x 16.  A new batch starts
+ * with both phases staged at 8. */
+int swpc_batch_set_staged(swpc_batch *b, int stress_ti, int vel_ti);
+/* The current launch: out[5] = ti, ri, bps, stress_ti, vel_ti. */
+int swpc_batch_get_launch(const swpc_batch *b, int *out);
 const char *swpc_batch_last_error(const swpc_batch *b);
 int swpc_batch_destroy(swpc_batch *b);
 

@@ -48,7 +48,7 @@ EXPORTS = [
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
-    "swpc_batch_set_shape",
+    "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
     "swpc_fbatch_autotune", "swpc_fbatch_step", "swpc_fbatch_run", "swpc_fbatch_time_steps", "swpc_fbatch_sync",
     "swpc_fbatch_wav_fetch", "swpc_fbatch_download_field", "swpc_fbatch_device_bytes", "swpc_fbatch_set_launch",
@@ -179,6 +179,8 @@ def load():
         "swpc_batch_time_steps": (i, [vp, i, i, _FP]),
         "swpc_batch_autotune": (i, [vp, i, i, _IP, _IP, _IP, _IP]),
         "swpc_batch_set_shape": (i, [vp, i, i, i]),
+        "swpc_batch_set_staged": (i, [vp, i, i]),
+        "swpc_batch_get_launch": (i, [vp, _IP]),
         "swpc_batch_last_error": (C.c_char_p, [vp]),
         "swpc_batch_destroy": (i, [vp]),
         "swpc_fbatch_create": (i, [vp, i, C.POINTER(vp)]),

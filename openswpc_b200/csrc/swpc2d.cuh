@@ -30,9 +30,12 @@ struct Model2D {
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
 };
 
+// A tile of 32 (k) x (tile step) (i) cells of one model; flags: the tile
+// holds interior (kTileInterior) and absorber (kTileAbsorber) cells.
 struct Tile2D {
-    int model, k0, i0, pad;
+    int model, k0, i0, flags;
 };
+constexpr int kTileInterior = 1, kTileAbsorber = 2;
 
 struct Wav2Args {
     int Kp, nst, ntw, ntdec_w, what, psv;
@@ -51,6 +54,38 @@ struct TileShape {
     int ti, ri, blocks_per_sm;
 };
 constexpr TileShape kDefaultTiles{4, 4, 0};
+
+// TMA-staged kernels (swpc2d_tma.cu): tiles of 32 (k) x kTileI2D (i), one
+// CTA of 32 x ti threads per tile (ti = 4, 8 or 16), the operands of each
+// model read through its tensor maps, which travel as a kernel parameter: a
+// launch covers one model, or up to kGroup2D consecutive models of a batch
+// (their sets fill the 32 KB parameter space).  Field indices of a model's
+// slab: V at v, S at s (R follows S), lam taup taus mu rho from med.
+constexpr int kTileI2D = 16;
+constexpr int kGroup2D = 48;
+struct Fields2D {
+    int v, s, med;
+};
+// the tensor maps of one model for one phase (CUtensorMap: 128 bytes)
+struct alignas(64) MapSet2D {
+    unsigned char m[5][128];
+};
+struct Maps2D {
+    MapSet2D str, vel;
+};
+Fields2D fields2d(int kind, int nm);
+int slab_fields2d(int kind, int nm);
+bool staged2d_ti_ok(int ti);
+bool encode_maps2d(Maps2D &m, int kind, int nm, float *slab, const Geo &g);
+// one launch over the ntiles tiles from `tiles`, all of models model0 ..
+// model0 + nset - 1 (nset = 1 .. kGroup2D), whose map sets are sets[0 .. nset-1]
+cudaError_t launch_stress2d_tma(int kind, int nm, int ti, const MapSet2D *sets, int nset, int model0,
+                                const Model2D *models, const Tile2D *tiles, int ntiles, int mask, Fields2D f, int *err,
+                                cudaStream_t st);
+cudaError_t launch_vel2d_tma(int kind, int ti, const MapSet2D *sets, int nset, int model0, const Model2D *models,
+                             const Tile2D *tiles, int ntiles, int mask, Fields2D f, int *err, cudaStream_t st);
+// flags of the tile (k0, i0) of a model (tile extents 32 x ni)
+int tile2d_flags(const swpc_ctx *c, int k0, int i0, int ni);
 
 void launch_stress2d(int kind, int nm, const Model2D *models, const Tile2D *tiles, int ntiles, int mask,
                      TileShape ts, cudaStream_t st);

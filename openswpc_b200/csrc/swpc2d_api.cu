@@ -35,28 +35,60 @@ int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int
 static const int PSV_V[2] = {0, 2}, PSV_S[3] = {0, 2, 4}, PSV_R[3] = {0, 2, 4};
 static const int SH_V[1] = {1}, SH_S[2] = {3, 5}, SH_R[2] = {3, 5};
 
+// flags of the 32 x ni tile at (k0, i0): interior and absorber cells present
+int tile2d_flags(const swpc_ctx *c, int k0, int i0, int ni) {
+    const Geo &g = c->g;
+    const int i1 = std::min(i0 + ni - 1, g.nx), k1 = std::min(k0 + 31, g.nz);
+    int f = 0;
+    if (k0 <= c->kek && i0 <= c->iek && i1 >= c->ibk) f |= kTileInterior;
+    if (i0 < c->ibk || i1 > c->iek || k1 > c->kek) f |= kTileAbsorber;
+    return f;
+}
+
 int create_2d(swpc_ctx *c) {
     const Geo &g = c->g;
     const bool psv = c->kind == SWPC_KIND_PSV;
     int rc = 0;
-    const int nv = psv ? 2 : 1, ns = psv ? 3 : 2;
-    for (int q = 0; q < nv && !rc; q++) rc = dalloc(c, &c->V[psv ? PSV_V[q] : SH_V[q]], g.ncell);
-    for (int q = 0; q < ns && !rc; q++) rc = dalloc(c, &c->S[psv ? PSV_S[q] : SH_S[q]], g.ncell);
-    for (int q = 0; q < ns && !rc; q++)
-        for (int m = 0; m < c->d.nm && !rc; m++) rc = dalloc(c, &c->R[(psv ? PSV_R[q] : SH_R[q]) * 3 + m], g.ncell);
-    for (int q = 0; q < 5 && !rc; q++) rc = dalloc(c, &c->med[q], g.ncell);
+    const int nv = psv ? 2 : 1, ns = psv ? 3 : 2, nm = c->d.nm;
+    // one slab: V, S, R (component-major), then lam taup taus mu rho
+    const int nf = slab_fields2d(c->kind, nm);
+    rc = dalloc(c, &c->slab, (size_t)nf * g.ncell);
+    if (rc) return rc;
+    c->slab_nf = nf;
+    auto F = [&](int f) { return c->slab + (size_t)f * g.ncell; };
+    for (int q = 0; q < nv; q++) c->V[psv ? PSV_V[q] : SH_V[q]] = F(q);
+    for (int q = 0; q < ns; q++) c->S[psv ? PSV_S[q] : SH_S[q]] = F(nv + q);
+    for (int q = 0; q < ns; q++)
+        for (int m = 0; m < nm; m++) c->R[(psv ? PSV_R[q] : SH_R[q]) * 3 + m] = F(nv + ns + q * nm + m);
+    const int mb = fields2d(c->kind, nm).med;
+    c->med[1] = F(mb);       // lam
+    c->med[3] = F(mb + 1);   // taup
+    c->med[4] = F(mb + 2);   // taus
+    c->med[2] = F(mb + 3);   // mu
+    c->med[0] = F(mb + 4);   // rho
     if (!rc) rc = dalloc(c, &c->band, g.Ip);
     if (!rc) rc = dalloc(c, &c->pmlcol, g.Ip);
     if (!rc) rc = dalloc(c, &c->kob, g.Ip);
     if (!rc) rc = dalloc(c, &c->kfs, g.Ip);
     if (!rc) rc = dalloc(c, &c->d_model2d, 1);
     if (!rc) rc = dalloc(c, &c->d_wav2d, 1);
+    if (!rc) rc = dalloc(c, &c->d_err, 1);
     c->nm2d_aux = psv ? 8 : 4;
     if (rc) return rc;
-    // tile list: 32 (k) x (ti * ri) (i)
+    // tensor maps of the staged kernels over the slab; the staged kernels are
+    // the default launch
+    Maps2D *mp = new Maps2D();
+    memset(mp, 0, sizeof(Maps2D));
+    c->maps2d = mp;
+    if (!encode_maps2d(*mp, c->kind, nm, c->slab, g))
+        return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the 2D field slab");
+    c->stress_tma = c->vel_tma = true;
+    c->stress_tbi = c->vel_tbi = 8;
+    // tile list: 32 (k) x 16 (i)
     std::vector<Tile2D> tiles;
-    for (int i0 = 1; i0 <= g.nx; i0 += kDefaultTiles.ti * kDefaultTiles.ri)
-        for (int k0 = 1; k0 <= g.nz; k0 += 32) tiles.push_back(Tile2D{0, k0, i0, 0});
+    const int ni = kDefaultTiles.ti * kDefaultTiles.ri;
+    for (int i0 = 1; i0 <= g.nx; i0 += ni)
+        for (int k0 = 1; k0 <= g.nz; k0 += 32) tiles.push_back(Tile2D{0, k0, i0, tile2d_flags(c, k0, i0, ni)});
     c->ntiles2d = (int)tiles.size();
     RC(dalloc(c, &c->d_tiles2d, tiles.size()));
     CK(cudaMemcpyAsync(c->d_tiles2d, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, c->stream));
@@ -66,6 +98,8 @@ int create_2d(swpc_ctx *c) {
 
 void destroy_2d(swpc_ctx *c) {
     if (c->d_model2d) cudaFree(c->d_model2d);
+    delete static_cast<Maps2D *>(c->maps2d);
+    c->maps2d = nullptr;
     if (c->d_tiles2d) cudaFree(c->d_tiles2d);
     if (c->d_wav2d) cudaFree(c->d_wav2d);
     if (c->rho_cell_bf) cudaFree(c->rho_cell_bf);
@@ -171,15 +205,24 @@ Model2D model_of(const swpc_ctx *c) {
 }
 
 int update_stress_2d(swpc_ctx *c, int mask) {
-    launch_stress2d(c->kind, c->d.nm, c->d_model2d, c->d_tiles2d, c->ntiles2d, (c->d.na > 0) ? mask : (mask & 1),
-                    kDefaultTiles,
-                    c->stream);
+    const int m = (c->d.na > 0) ? mask : (mask & 1);
+    if (c->stress_tma)
+        return cuda_check(c, launch_stress2d_tma(c->kind, c->d.nm, c->stress_tbi, &static_cast<Maps2D *>(c->maps2d)->str,
+                                                 1, 0, c->d_model2d, c->d_tiles2d, c->ntiles2d, m,
+                                                 fields2d(c->kind, c->d.nm), c->d_err, c->stream),
+                          "stress2d_tma launch");
+    launch_stress2d(c->kind, c->d.nm, c->d_model2d, c->d_tiles2d, c->ntiles2d, m, kDefaultTiles, c->stream);
     return cuda_check(c, cudaGetLastError(), "stress2d launch");
 }
 
 int update_vel_2d(swpc_ctx *c, int mask) {
-    launch_vel2d(c->kind, c->d_model2d, c->d_tiles2d, c->ntiles2d, (c->d.na > 0) ? mask : (mask & 1), kDefaultTiles,
-                 c->stream);
+    const int m = (c->d.na > 0) ? mask : (mask & 1);
+    if (c->vel_tma)
+        return cuda_check(c, launch_vel2d_tma(c->kind, c->vel_tbi, &static_cast<Maps2D *>(c->maps2d)->vel, 1, 0,
+                                              c->d_model2d, c->d_tiles2d, c->ntiles2d, m, fields2d(c->kind, c->d.nm),
+                                              c->d_err, c->stream),
+                          "vel2d_tma launch");
+    launch_vel2d(c->kind, c->d_model2d, c->d_tiles2d, c->ntiles2d, m, kDefaultTiles, c->stream);
     return cuda_check(c, cudaGetLastError(), "vel2d launch");
 }
 
@@ -251,6 +294,15 @@ struct swpc_batch {
     int *d_it = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool psv_bf_split = false;
+    // TMA-staged kernels: threads along i of the stress / velocity CTAs (4, 8
+    // or 16; 0 = the tile-walking kernels); the members' tensor-map sets in
+    // member order; one staged launch per group of consecutive members
+    // (first member of each group, and the end); the first tile of every
+    // member (and the end); the error word of the staged copies
+    int sti = 8, vti = 8;
+    std::vector<MapSet2D> str_sets, vel_sets;
+    std::vector<int> group_first, tile_first;
+    int *d_err = nullptr;
     std::string err;
 };
 
@@ -272,7 +324,7 @@ extern "C" int swpc_batch_destroy(swpc_batch *b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    void *ps[] = {b->d_models, b->d_tiles, b->d_wav, b->d_inj, b->d_it};
+    void *ps[] = {b->d_models, b->d_tiles, b->d_wav, b->d_inj, b->d_it, b->d_err};
     for (void *p : ps) if (p) cudaFree(p);
     delete b;
     return SWPC_OK;
@@ -293,11 +345,15 @@ extern "C" int swpc_batch_destroy(swpc_batch *b) {
 // tile list of every member for tiles of 32 (k) x (ts.ti * ts.ri) (i)
 static int set_tiles(swpc_batch *b, TileShape ts) {
     std::vector<Tile2D> tiles;
+    b->tile_first.clear();
     for (int q = 0; q < (int)b->members.size(); q++) {
         const swpc_ctx *c = b->members[q];
-        for (int i0 = 1; i0 <= c->g.nx; i0 += ts.ti * ts.ri)
-            for (int k0 = 1; k0 <= c->g.nz; k0 += 32) tiles.push_back(Tile2D{q, k0, i0, 0});
+        b->tile_first.push_back((int)tiles.size());
+        const int ni = ts.ti * ts.ri;
+        for (int i0 = 1; i0 <= c->g.nx; i0 += ni)
+            for (int k0 = 1; k0 <= c->g.nz; k0 += 32) tiles.push_back(Tile2D{q, k0, i0, tile2d_flags(c, k0, i0, ni)});
     }
+    b->tile_first.push_back((int)tiles.size());
     if (b->d_tiles && (int)tiles.size() > b->ntiles) {
         BCK(cudaFree(b->d_tiles));
         b->d_tiles = nullptr;
@@ -306,6 +362,8 @@ static int set_tiles(swpc_batch *b, TileShape ts) {
     BCK(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice));
     b->ntiles = (int)tiles.size();
     b->shape = ts;
+    // the staged kernels work on tiles of 32 x 16
+    if (ts.ti * ts.ri != kTileI2D) b->sti = b->vti = 0;
     return SWPC_OK;
 }
 
@@ -341,6 +399,18 @@ extern "C" int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **o
     }
     BCK(cudaMalloc(&b->d_models, models.size() * sizeof(Model2D)));
     {
+        for (int q = 0; q < n; q++) {
+            if (!b->members[q]->maps2d) return berr(b, SWPC_ERR_STATE, "batch member without tensor maps");
+            b->str_sets.push_back(static_cast<const Maps2D *>(b->members[q]->maps2d)->str);
+            b->vel_sets.push_back(static_cast<const Maps2D *>(b->members[q]->maps2d)->vel);
+        }
+        // groups of consecutive members of nearly equal count, at most kGroup2D each
+        const int ng = (n + kGroup2D - 1) / kGroup2D;
+        for (int g = 0; g <= ng; g++) b->group_first.push_back((int)((long long)n * g / ng));
+        BCK(cudaMalloc(&b->d_err, sizeof(int)));
+        BCK(cudaMemset(b->d_err, 0, sizeof(int)));
+    }
+    {
         int rc = set_tiles(b, kDefaultTiles);
         if (rc) return rc;
     }
@@ -371,17 +441,49 @@ static int batch_step(swpc_batch *b, int it, const int *d_it) {
         max_inj_n = std::max(max_inj_n, std::max(c->ninj_glut, c->ninj_bf));
     }
     const int mask_all = 3;
+    const Fields2D f = fields2d(b->kind, b->nm);
+    // staged: one launch per member group over that group's tiles
+    const int ng = (int)b->group_first.size() - 1;
+    auto stress = [&](int mask) {
+        if (!b->sti) {
+            launch_stress2d(b->kind, b->nm, b->d_models, b->d_tiles, b->ntiles, mask, b->shape, b->stream);
+            return cudaGetLastError();
+        }
+        for (int g = 0; g < ng; g++) {
+            const int m0 = b->group_first[g], m1 = b->group_first[g + 1];
+            const int t0 = b->tile_first[m0], t1 = b->tile_first[m1];
+            const cudaError_t e = launch_stress2d_tma(b->kind, b->nm, b->sti, &b->str_sets[m0], m1 - m0, m0,
+                                                      b->d_models, b->d_tiles + t0, t1 - t0, mask, f, b->d_err,
+                                                      b->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    auto vel = [&](int mask) {
+        if (!b->vti) {
+            launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, mask, b->shape, b->stream);
+            return cudaGetLastError();
+        }
+        for (int g = 0; g < ng; g++) {
+            const int m0 = b->group_first[g], m1 = b->group_first[g + 1];
+            const int t0 = b->tile_first[m0], t1 = b->tile_first[m1];
+            const cudaError_t e = launch_vel2d_tma(b->kind, b->vti, &b->vel_sets[m0], m1 - m0, m0, b->d_models,
+                                                   b->d_tiles + t0, t1 - t0, mask, f, b->d_err, b->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
     launch_wav2d(b->d_wav, nwav, b->max_nst, it, d_it, b->stream);
-    launch_stress2d(b->kind, b->nm, b->d_models, b->d_tiles, b->ntiles, mask_all, b->shape, b->stream);
+    BCK(stress(mask_all));
     launch_inject_multi(b->d_inj, b->ninj, max_inj_n, d_it, it, b->stream);
     if (b->kind == SWPC_KIND_PSV && b->psv_bf_split) {
         // P-SV applies body forces between the interior and absorber velocity
         // updates (src/swpc_psv/main.f90:106-110)
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 1, b->shape, b->stream);
+        BCK(vel(1));
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, 2, b->shape, b->stream);
+        BCK(vel(2));
     } else {
-        launch_vel2d(b->kind, b->d_models, b->d_tiles, b->ntiles, mask_all, b->shape, b->stream);
+        BCK(vel(mask_all));
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
     }
     BCK(cudaGetLastError());
@@ -420,6 +522,37 @@ extern "C" int swpc_batch_run(swpc_batch *b, int it0, int nsteps) {
 extern "C" int swpc_batch_sync(swpc_batch *b) {
     if (!b) return SWPC_ERR_ARG;
     BCK(cudaStreamSynchronize(b->stream));
+    int h = 0;
+    BCK(cudaMemcpy(&h, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return berr(b, SWPC_ERR_CUDA, "a staged tile copy did not complete (TMA wait timed out)");
+    return SWPC_OK;
+}
+
+static int drop_graph(swpc_batch *b) {
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (b->graph) {
+        BCK(cudaGraphExecDestroy(b->graph));
+        b->graph = nullptr;
+    }
+    return SWPC_OK;
+}
+
+extern "C" int swpc_batch_set_staged(swpc_batch *b, int stress_ti, int vel_ti) {
+    if (!b) return SWPC_ERR_ARG;
+    if ((stress_ti && !staged2d_ti_ok(stress_ti)) || (vel_ti && !staged2d_ti_ok(vel_ti)))
+        return berr(b, SWPC_ERR_ARG, "staged kernels take 4, 8 or 16 threads along i (0: tile-walking kernels)");
+    RCB(drop_graph(b));
+    if ((stress_ti || vel_ti) && b->shape.ti * b->shape.ri != kTileI2D) RCB(set_tiles(b, kDefaultTiles));
+    b->sti = stress_ti;
+    b->vti = vel_ti;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_batch_get_launch(const swpc_batch *b, int *out) {
+    if (!b || !out) return SWPC_ERR_ARG;
+    out[0] = b->shape.ti; out[1] = b->shape.ri; out[2] = b->shape.blocks_per_sm;
+    out[3] = b->sti; out[4] = b->vti;
     return SWPC_OK;
 }
 
@@ -427,36 +560,36 @@ extern "C" int swpc_batch_set_shape(swpc_batch *b, int ti, int ri, int bps) {
     if (!b) return SWPC_ERR_ARG;
     if (ti < 1 || ri < 1 || bps < 0 || 32 * ti > 256 || ri > 64 || bps > 64)
         return berr(b, SWPC_ERR_ARG, "tile shape out of range (32*ti <= 256, 1 <= ri <= 64, 0 <= bps <= 64)");
-    BCK(cudaSetDevice(b->device));
-    BCK(cudaStreamSynchronize(b->stream));
-    if (b->graph) {
-        BCK(cudaGraphExecDestroy(b->graph));
-        b->graph = nullptr;
-    }
+    RCB(drop_graph(b));
     return set_tiles(b, TileShape{ti, ri, bps});
 }
 
 extern "C" int swpc_batch_autotune(swpc_batch *b, int it0, int reps, int *used, int *best_ti, int *best_ri,
                                    int *best_bps) {
-    static const TileShape cand[] = {{4, 4, 0}, {4, 2, 0}, {4, 8, 0}, {2, 8, 0}, {2, 4, 0},
-                                     {8, 4, 0}, {8, 2, 0}, {4, 1, 16}};
+    // candidates: staged kernels (threads along i of the stress and velocity
+    // CTAs) on 32 x 16 tiles, then tile-walking kernels of several shapes
+    struct Cand {
+        TileShape ts;
+        int sti, vti;
+    };
+    static const Cand cand[] = {{{4, 4, 0}, 8, 8},  {{4, 4, 0}, 4, 4},  {{4, 4, 0}, 16, 16}, {{4, 4, 0}, 8, 4},
+                                {{4, 4, 0}, 4, 8},  {{4, 4, 0}, 16, 8}, {{4, 4, 0}, 0, 0},   {{4, 2, 0}, 0, 0},
+                                {{4, 8, 0}, 0, 0},  {{2, 8, 0}, 0, 0},  {{8, 4, 0}, 0, 0},   {{4, 1, 16}, 0, 0}};
     const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
     if (!b || !used || reps < 1) return SWPC_ERR_ARG;
     if (it0 < 1 || it0 + ncand * reps - 1 > b->nt) return berr(b, SWPC_ERR_ARG, "not enough time steps left to tune");
-    BCK(cudaSetDevice(b->device));
-    if (b->graph) {
-        BCK(cudaGraphExecDestroy(b->graph));
-        b->graph = nullptr;
-    }
+    RCB(drop_graph(b));
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
     float best = 0.f;
-    TileShape pick = kDefaultTiles;
+    Cand pick = cand[0];
     int it = it0, rc = SWPC_OK;
     for (int n = 0; n < ncand && !rc; n++) {
-        rc = set_tiles(b, cand[n]);
+        rc = set_tiles(b, cand[n].ts);
         if (rc) break;
+        b->sti = cand[n].sti;
+        b->vti = cand[n].vti;
         cudaStreamSynchronize(b->stream);
         cudaEventRecord(e0, b->stream);
         for (int r = 0; r < reps && !rc; r++) rc = batch_step(b, it++, nullptr);
@@ -469,12 +602,14 @@ extern "C" int swpc_batch_autotune(swpc_batch *b, int it0, int reps, int *used, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    RCB(set_tiles(b, pick));
+    RCB(set_tiles(b, pick.ts));
+    b->sti = pick.sti;
+    b->vti = pick.vti;
     b->tuned = true;
     *used = it - it0;
-    if (best_ti) *best_ti = pick.ti;
-    if (best_ri) *best_ri = pick.ri;
-    if (best_bps) *best_bps = pick.blocks_per_sm;
+    if (best_ti) *best_ti = pick.ts.ti;
+    if (best_ri) *best_ri = pick.ts.ri;
+    if (best_bps) *best_bps = pick.ts.blocks_per_sm;
     return SWPC_OK;
 }
 

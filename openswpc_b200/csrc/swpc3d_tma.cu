@@ -38,88 +38,16 @@
 
 #include "swpc3d_cell.cuh"
 #include "swpc_tma.h"
+#include "swpc_tma_ptx.cuh"
 
 namespace swpc {
 
 namespace {
 
+using namespace tma;
+
 constexpr int KT = 32;                                 // cells of a tile along k
 constexpr int KB = KT + 8;                             // k extent of a halo box: k0-4 .. k0+35 (16-byte aligned start)
-constexpr unsigned long long kWaitNs = 100000000ull;   // 100 ms: a tile copy takes microseconds
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-// tiled 4D tensor copy global -> shared, completion counted on bar (no multicast)
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2, int c3,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
-        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// first 128-byte aligned address of the dynamic shared memory (TMA
-// destinations); the launches reserve 128 bytes for the shift
-__device__ __forceinline__ float *aligned128(unsigned char *p) {
-    const unsigned a = smem_u32(p);
-    return reinterpret_cast<float *>(p + ((128u - (a & 127u)) & 127u));
-}
-
-__device__ __forceinline__ unsigned long long gtime() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Bounded wait for the tile copies.  After kWaitNs the kernel raises the
-// context's error word, waits once more (bounded) for its copies in flight,
-// and the caller skips the staged cells; CTAs that start after the error
-// copy nothing (see stage_begin).
-__device__ __forceinline__ bool wait_tiles(uint64_t *bar, int *err) {
-    const unsigned long long t0 = gtime();
-    while (!mbar_try_wait(bar, 0)) {
-        if (gtime() - t0 > kWaitNs) {
-            atomicExch(err, 1);
-            const unsigned long long t1 = gtime();
-            while (!mbar_try_wait(bar, 0) && gtime() - t1 < kWaitNs) {
-            }
-            return false;
-        }
-    }
-    return true;
-}
-
-// barrier set-up of a staged CTA; false when an earlier tile copy of the
-// launch failed (nothing is copied then)
-__device__ __forceinline__ bool stage_begin(uint64_t *bar, int *flag, const int *err, bool lead) {
-    if (lead) {
-        *flag = *reinterpret_cast<const volatile int *>(err) == 0;
-        if (*flag) {
-            mbar_init(bar, 1);
-            fence_barrier_init();
-        }
-    }
-    __syncthreads();
-    return *flag != 0;
-}
 
 // tile and member group of this CTA: member group fastest, then k, i, j
 // (the medium of a tile is re-read from L2 by the groups that follow), or with
@@ -149,7 +77,6 @@ __device__ __forceinline__ bool tile_has_absorber(const Tile &T, int bi, int bj,
     return T.i0 < ibk || i1 > iek || T.j0 < jbk || j1 > jek || k1 > kek;
 }
 
-__host__ __device__ constexpr int up32(int n) { return (n + 31) / 32 * 32; }
 template <int SMEM_FLOATS, int THREADS>
 __host__ __device__ constexpr int blocks_per_sm() {
     constexpr int by_smem = (227 * 1024) / (SMEM_FLOATS * 4 + 128 + 1024);
@@ -216,12 +143,12 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
     else if (staged && lead) {
         mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem, with_r));
         const int x0 = T.k0 - 1 + KH;
-        tma_load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
+        load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
         for (int mm = 0; mm < T.nmem; mm++) {
             const int fm = (T.m0 + mm) * t.f_member;
             float *p = sm + L::oMem(mm);
-            tma_load_4d(p, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state + fm, &bar);
-            tma_load_4d(p + up32(L::nState), &tm_v, x0 - 4, T.i0, T.j0, t.f_v + fm, &bar);
+            load_4d(p, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state + fm, &bar);
+            load_4d(p + up32(L::nState), &tm_v, x0 - 4, T.i0, T.j0, t.f_v + fm, &bar);
         }
     }
     const int k = T.k0 + tx, i = T.i0 + ty, j = T.j0 + tz;
@@ -328,17 +255,17 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
     else if (staged && lead) {
         mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem));
         const int x0 = T.k0 - 1 + KH, ic = T.i0 + 2, jc = T.j0 + 2;
-        tma_load_4d(sm, &tm_b, x0, ic, jc, t.f_b, &bar);
+        load_4d(sm, &tm_b, x0, ic, jc, t.f_b, &bar);
         for (int mm = 0; mm < T.nmem; mm++) {
             const int f = t.f_v + (T.m0 + mm) * t.f_member;   // Vx of the member; S follows at f + 3
             float *p = sm + L::oMem(mm);
-            tma_load_4d(p + L::oV, &tm_own, x0, ic, jc, f, &bar);
-            tma_load_4d(p + L::oA, &tm_a, x0, ic - 1, jc, f + 3, &bar);
-            tma_load_4d(p + L::oBy, &tm_by, x0, ic, jc - 1, f + 4, &bar);
-            tma_load_4d(p + L::oC, &tm_c, x0 - 4, ic, jc, f + 5, &bar);
-            tma_load_4d(p + L::oF, &tm_f, x0 - 4, ic, jc - 2, f + 6, &bar);
-            tma_load_4d(p + L::oE, &tm_e, x0 - 4, ic - 2, jc, f + 7, &bar);
-            tma_load_4d(p + L::oD, &tm_d, x0, ic - 2, jc - 2, f + 8, &bar);
+            load_4d(p + L::oV, &tm_own, x0, ic, jc, f, &bar);
+            load_4d(p + L::oA, &tm_a, x0, ic - 1, jc, f + 3, &bar);
+            load_4d(p + L::oBy, &tm_by, x0, ic, jc - 1, f + 4, &bar);
+            load_4d(p + L::oC, &tm_c, x0 - 4, ic, jc, f + 5, &bar);
+            load_4d(p + L::oF, &tm_f, x0 - 4, ic, jc - 2, f + 6, &bar);
+            load_4d(p + L::oE, &tm_e, x0 - 4, ic - 2, jc, f + 7, &bar);
+            load_4d(p + L::oD, &tm_d, x0, ic - 2, jc - 2, f + 8, &bar);
         }
     }
     const int k = T.k0 + tx, i = T.i0 + ty;

@@ -15,6 +15,7 @@
 #include <utility>
 #include <vector>
 
+#include "swpc2d.cuh"
 #include "swpc_ctx.h"
 #include "swpc_host.h"
 #include "swpc_kernels.cuh"
@@ -219,6 +220,19 @@ extern "C" long long swpc_device_bytes(const swpc_ctx *c) { return c ? c->bytes 
 
 extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj) {
     if (!c) return SWPC_ERR_ARG;
+    if (!is3d(c)) {
+        // 2D: kernels 0 / 1 the tile-walking stress / velocity kernels, 5 / 6
+        // the staged ones with bi = 4, 8 or 16 threads along i (bj = 1)
+        if (!(kernel == 0 || kernel == 1 || kernel == 5 || kernel == 6) ||
+            (kernel >= 5 && (!staged2d_ti_ok(bi) || bj != 1 || minb != 1)))
+            return set_err(c, SWPC_ERR_ARG, "2D launch: kernel 0, 1, or 5, 6 with minb 1, bi 4/8/16, bj 1");
+        invalidate_graph(c);
+        if (kernel == 0) c->stress_tma = false;
+        else if (kernel == 1) c->vel_tma = false;
+        else if (kernel == 5) { c->stress_tma = true; c->stress_tbi = bi; }
+        else { c->vel_tma = true; c->vel_tbi = bi; }
+        return SWPC_OK;
+    }
     if (kernel < 0 || kernel > 6 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
         ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
         return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..6, minb 1..4, 32*bi*bj <= 256)");

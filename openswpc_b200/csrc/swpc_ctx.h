@@ -146,6 +146,7 @@ struct swpc_ctx {
     swpc::Wav2Args *d_wav2d = nullptr;
     int nm2d_aux = 0;
     bool desc_dirty = true;   // device descriptors must be refreshed before the next launch
+    void *maps2d = nullptr;   // tensor maps of the model (swpc::Maps2D): a kernel parameter of the staged kernels
 
     // launch shape (swpc_set_launch): block = 32 x bi x bj threads; minb =
     // minimum resident blocks per SM the kernels are compiled for
@@ -158,16 +159,18 @@ struct swpc_ctx {
     bool vel_vec = false;
     int vel_vminb = 2, vel_vbi = 2, vel_vbj = 2;
     // TMA-staged kernels (swpc3d_tma.cu): tile 32 x bi x bj; tensor maps over
-    // the field slab, encoded for the shapes in tma_key
+    // the field slab, encoded for the shapes in tma_key.  2D contexts
+    // (swpc2d_tma.cu): tiles 32 x 16 with stress_tbi / vel_tbi threads along i
     bool stress_tma = false, vel_tma = false;
     int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 2;
     void *tmaps = nullptr;        // swpc::TmaMaps
     int tma_key[4] = {-1, -1, -1, -1};
     int *d_err = nullptr;         // device error word of the staged kernels
 
-    // 3D FP32 storage: V, S, R and the medium in one allocation (field order
-    // 0-2 V, 3-8 S, 9.. R component-major, then lam mu taup taus muyz muxz
-    // muxy and bx by bz), so that tensor maps cover them
+    // FP32 storage: V, S, R and the medium in one allocation, so that tensor
+    // maps cover them.  3D field order: 0-2 V, 3-8 S, 9.. R component-major,
+    // then lam mu taup taus muyz muxz muxy and bx by bz; 2D: V, S, R, then
+    // lam taup taus mu rho
     float *slab = nullptr;
     int slab_nf = 0;
     int nfbatch = 0;   // reciprocity batches that borrow this context (swpc_fbatch.cu)

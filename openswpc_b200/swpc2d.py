@@ -258,9 +258,26 @@ class Batch2D:
         self._check(self.lib.swpc_batch_time_steps(self.b, it0, nsteps, C.byref(ms)))
         return ms.value
 
+    def set_staged(self, stress_ti: int, vel_ti: int):
+        """TMA-staged kernels with stress_ti / vel_ti threads along i (4, 8,
+        16), or the tile-walking kernels (0), per phase."""
+        self._check(self.lib.swpc_batch_set_staged(self.b, stress_ti, vel_ti))
+
+    def set_shape(self, ti: int, ri: int, bps: int):
+        """Tile shape of the tile-walking kernels (ti * ri != 16 also selects
+        them for both phases)."""
+        self._check(self.lib.swpc_batch_set_shape(self.b, ti, ri, bps))
+
+    def launch(self) -> dict:
+        """The current launch: tile shape and staged threads per phase."""
+        out = (C.c_int * 5)()
+        self._check(self.lib.swpc_batch_get_launch(self.b, out))
+        return {"ti": out[0], "ri": out[1], "bps": out[2], "stress_ti": out[3], "vel_ti": out[4]}
+
     def autotune(self, it0: int, reps: int = 2) -> tuple[int, int, int, int]:
-        """Pick the launch shape while advancing steps it0 ..; returns
-        (steps used, threads in i per block, rows per thread, blocks per SM)."""
+        """Pick the launch while advancing steps it0 ..; returns (steps used,
+        threads in i per block, rows per thread, blocks per SM) of the tile
+        shape (launch() gives the whole pick)."""
         used, ti, ri, bps = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.swpc_batch_autotune(self.b, it0, reps, C.byref(used), C.byref(ti), C.byref(ri),
                                                  C.byref(bps)))

@@ -61,10 +61,24 @@ def compare(g: Swpc2D, o: Oracle2D, p):
         assert same_bits(g.download(_lib.F_AUX + q), aux_box(o, name, p)), name
 
 
+def set_launch(g: Swpc2D, stress_ti: int, vel_ti: int):
+    """Staged kernels with ti threads along i (4, 8, 16), or the tile-walking
+    kernels (0), per phase."""
+    _lib.check(g.ctx, g.lib.swpc_set_launch(g.ctx, 5 if stress_ti else 0, 1, stress_ti or 1, 1))
+    _lib.check(g.ctx, g.lib.swpc_set_launch(g.ctx, 6 if vel_ti else 1, 1, vel_ti or 1, 1))
+
+
+LAUNCHES = [(8, 8), (4, 16), (16, 4), (0, 0)]
+
+
+@pytest.mark.parametrize("launch", LAUNCHES, ids=lambda l: f"stress{l[0]}-vel{l[1]}")
 @pytest.mark.parametrize("kind", ["psv", "sh"])
-def test_2d_forward_matches_oracle(kind):
+def test_2d_forward_matches_oracle(kind, launch):
+    """Staged kernels (ti threads along i) and tile-walking kernels (0) give
+    the oracle's bits."""
     p = small2d(kind, nt=120)
     g = Swpc2D(p, kind)
+    set_launch(g, *launch)
     o = Oracle2D(p, kind)
     g.run(1, p.nt)
     o.run(1, p.nt)
@@ -76,6 +90,21 @@ def test_2d_forward_matches_oracle(kind):
     compare(g, o, p)
     vm = g.kernel__vmax()
     assert same_bits(vm, o.vmax()[:len(vm)])
+
+
+@pytest.mark.parametrize("nm", [0, 1, 2])
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_2d_staged_thick_absorber_and_fewer_memory_variables(kind, nm):
+    """A 20-cell absorber leaves tiles without interior cells (the staged
+    stress kernel copies S without R there); nm = 0..2 memory variables."""
+    p = small2d(kind, nx=104, nz=70, na=20, nt=90, nm=nm)
+    g = Swpc2D(p, kind)
+    o = Oracle2D(p, kind)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    assert np.linalg.norm(o.waveforms()) > 0
+    assert same_bits(g.waveforms(), o.waveforms())
+    compare(g, o, p)
 
 
 @pytest.mark.parametrize("kind", ["psv", "sh"])
@@ -103,6 +132,7 @@ def test_batched_ensemble_equals_independent_runs(kind):
     runs = [Swpc2D(p, kind) for p in ps]
     alone = [Swpc2D(p, kind) for p in ps]
     batch = Batch2D(runs)
+    assert batch.launch() == {"ti": 4, "ri": 4, "bps": 0, "stress_ti": 8, "vel_ti": 8}
     batch.run(1, 50)
     for r, a, p in zip(runs, alone, ps):
         a.run(1, 50)
@@ -116,6 +146,56 @@ def test_batched_ensemble_equals_independent_runs(kind):
 
 
 @pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_batch_launch_forms_give_the_same_bits(kind):
+    """Staged kernels with every thread count, mixed with the tile-walking
+    kernels, and tile-walking shapes: all give the bits of independent runs,
+    one launch form per ten steps."""
+    sizes = [(96, 48), (40, 40), (150, 77)]
+    ps = [small2d(kind, nx=nx, nz=nz, na=8, nt=60, seed=20 + s) for s, (nx, nz) in enumerate(sizes)]
+    runs = [Swpc2D(p, kind) for p in ps]
+    batch = Batch2D(runs)
+    forms = [("staged", 4, 16), ("staged", 16, 0), ("shape", 4, 2), ("staged", 0, 8), ("shape", 8, 4),
+             ("staged", 8, 4)]
+    it = 1
+    for what, a, b in forms:
+        if what == "staged":
+            batch.set_staged(a, b)
+            assert batch.launch()["ti"] * batch.launch()["ri"] == 16
+        else:
+            batch.set_shape(a, b, 0)
+            assert batch.launch()["stress_ti"] == 0 and batch.launch()["vel_ti"] == 0
+        batch.run(it, 10)
+        it += 10
+    for r, p in zip(runs, ps):
+        a = Swpc2D(p, kind)
+        a.run(1, 60)
+        assert same_bits(r.waveforms(), a.waveforms())
+        for fid in r.field_ids.values():
+            assert same_bits(r.download(fid), a.download(fid))
+    with pytest.raises(_lib.SwpcError):
+        batch.set_staged(6, 8)
+    batch.close()
+
+
+def test_batch_of_more_members_than_one_staged_launch_takes():
+    """50 members: the staged kernels take their tensor maps as a kernel
+    parameter for at most 48 members per launch, so the batch launches two
+    member groups per phase; every member keeps the bits of its own run."""
+    ps = [small2d("psv", nx=40 + 8 * (s % 5), nz=32 + 6 * (s % 3), na=6, nt=12, seed=100 + s) for s in range(50)]
+    runs = [Swpc2D(p, "psv") for p in ps]
+    batch = Batch2D(runs)
+    batch.run(1, 12)
+    for r, p in zip(runs, ps):
+        a = Swpc2D(p, "psv")
+        a.run(1, 12)
+        assert same_bits(r.waveforms(), a.waveforms())
+        for fid in r.field_ids.values():
+            assert same_bits(r.download(fid), a.download(fid))
+        a.close()
+    batch.close()
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
 def test_batch_autotune_steps_are_ordinary_steps(kind):
     """The autotuner advances the run with every candidate launch shape; the
     result equals independent runs bit for bit."""
@@ -124,7 +204,9 @@ def test_batch_autotune_steps_are_ordinary_steps(kind):
     runs = [Swpc2D(p, kind) for p in ps]
     batch = Batch2D(runs)
     used, ti, ri, bps = batch.autotune(1, reps=2)
-    assert used == 16 and ti in (2, 4, 8) and ri in (1, 2, 4, 8) and bps >= 0
+    assert used == 24 and ti in (2, 4, 8) and ri in (1, 2, 4, 8) and bps >= 0
+    pick = batch.launch()
+    assert pick["stress_ti"] in (0, 4, 8, 16) and pick["vel_ti"] in (0, 4, 8, 16)
     batch.run(1 + used, 40 - used)
     for r, p in zip(runs, ps):
         a = Swpc2D(p, kind)
