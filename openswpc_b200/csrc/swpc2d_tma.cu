@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(32 * TI) stress2d_tma_kernel(const __grid_cons
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ Model2D sM;
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int go;
+    __shared__ unsigned long long limit;
     float *sm = aligned128(smraw);
     const Tile2D tl = tiles[blockIdx.x];
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -159,24 +159,28 @@ __global__ void __launch_bounds__(32 * TI) stress2d_tma_kernel(const __grid_cons
     const bool with_r = (mask & 1) && (tl.flags & kTileInterior);
     if (!with_r && !((mask & 2) && (tl.flags & kTileAbsorber))) return;   // nothing of this launch here
     if (lead) {
-        go = *reinterpret_cast<const volatile int *>(err) == 0;
-        if (go) {
-            mbar_init(&bar, 1);
-            fence_barrier_init();
-            const CUtensorMap *mp = set_maps(pm.set[tl.model - model0]);
-            const CUtensorMap *st = with_r ? &mp[ST_STATE] : &mp[ST_S];
-            mbar_expect_tx(&bar, L::bytes(with_r));
-            const int x0 = tl.k0 - 1 + KH, ic = tl.i0 + 2;
-            load_3d(sm + L::oState, st, x0, ic, f.s, &bar);
-            load_3d(sm + L::oMed, &mp[ST_MED], x0, ic, KIND == 0 ? f.med : f.med + 2, &bar);   // lam taup taus / taus
-            load_3d(sm + L::oMu, &mp[ST_MU], x0, ic, f.med + 3, &bar);
-            load_3d(sm + L::oV, &mp[ST_V], x0 - 4, ic - 2, f.v, &bar);
-        }
+        // the copies go out first; the error word is read while they travel
+        stage_init(&bar, L::bytes(with_r));
+        const CUtensorMap *mp = set_maps(pm.set[tl.model - model0]);
+        const int x0 = tl.k0 - 1 + KH, ic = tl.i0 + 2;
+        load_3d(sm + L::oState, with_r ? &mp[ST_STATE] : &mp[ST_S], x0, ic, f.s, &bar);
+        load_3d(sm + L::oMed, &mp[ST_MED], x0, ic, KIND == 0 ? f.med : f.med + 2, &bar);   // lam taup taus / taus
+        load_3d(sm + L::oMu, &mp[ST_MU], x0, ic, f.med + 3, &bar);
+        load_3d(sm + L::oV, &mp[ST_V], x0 - 4, ic - 2, f.v, &bar);
+        limit = wait_limit(err);
     }
     copy_model(models, tl.model, sM);
-    __syncthreads();
-    if (!go || !wait_tiles(&bar, err)) return;   // an earlier copy failed, or this one did not complete
+    __syncthreads();   // barrier initialised, wait limit and model descriptor set
     const Model2D &M = sM;
+    // the band signs of this thread's cells are read while the tiles travel
+    int sg[RI];
+#pragma unroll
+    for (int r = 0; r < RI; r++) {
+        const int k = tl.k0 + tx, i = tl.i0 + ty + r * TI;
+        const bool interior = i >= M.ibk && i <= M.iek && k <= M.kek;
+        sg[r] = (interior && k <= M.nz && (mask & 1)) ? band_sign2d(M, k, i) : -1;
+    }
+    if (!wait_tiles(&bar, err, limit)) return;   // the copy did not complete
 #pragma unroll
     for (int r = 0; r < RI; r++) {
         const int row = ty + r * TI;
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(32 * TI) stress2d_tma_kernel(const __grid_cons
         if (!(mask & (interior ? 1 : 2))) continue;
         const long long e = (long long)(i + 2) * M.Kp + (k - 1 + KH);
         const SStr2<KIND, NM> o{sm, row, tx};
-        const int s = interior ? band_sign2d(M, k, i) : -1;
+        const int s = sg[r];
         if (KIND == 0) {
             if (interior) psv_stress_interior<NM>(M, o, s, e);
             else psv_stress_absorber(M, o, k, i, e);
@@ -206,36 +210,41 @@ __global__ void __launch_bounds__(32 * TI) vel2d_tma_kernel(const __grid_constan
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ Model2D sM;
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int go;
+    __shared__ unsigned long long limit;
     float *sm = aligned128(smraw);
     const Tile2D tl = tiles[blockIdx.x];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool lead = tx == 0 && ty == 0;
     if (!((mask & 1) && (tl.flags & kTileInterior)) && !((mask & 2) && (tl.flags & kTileAbsorber))) return;
     if (lead) {
-        go = *reinterpret_cast<const volatile int *>(err) == 0;
-        if (go) {
-            mbar_init(&bar, 1);
-            fence_barrier_init();
-            const CUtensorMap *mp = set_maps(pm.set[tl.model - model0]);
-            mbar_expect_tx(&bar, L::bytes());
-            const int x0 = tl.k0 - 1 + KH, ic = tl.i0 + 2;
-            load_3d(sm + L::oOwn, &mp[VE_OWN], x0, ic, f.v, &bar);
-            load_3d(sm + L::oRho, &mp[VE_RHO], x0, ic, f.med + 4, &bar);
-            if (KIND == 0) {
-                load_3d(sm + L::oA, &mp[VE_A], x0, ic - 1, f.s, &bar);            // Sxx
-                load_3d(sm + L::oC, &mp[VE_C], x0 - 4, ic, f.s + 1, &bar);        // Szz
-                load_3d(sm + L::oE, &mp[VE_E], x0 - 4, ic - 2, f.s + 2, &bar);    // Sxz
-            } else {
-                load_3d(sm + L::oA, &mp[VE_A], x0, ic - 2, f.s + 1, &bar);        // Sxy
-                load_3d(sm + L::oC, &mp[VE_C], x0 - 4, ic, f.s, &bar);            // Syz
-            }
+        // the copies go out first; the error word is read while they travel
+        stage_init(&bar, L::bytes());
+        const CUtensorMap *mp = set_maps(pm.set[tl.model - model0]);
+        const int x0 = tl.k0 - 1 + KH, ic = tl.i0 + 2;
+        load_3d(sm + L::oOwn, &mp[VE_OWN], x0, ic, f.v, &bar);
+        load_3d(sm + L::oRho, &mp[VE_RHO], x0, ic, f.med + 4, &bar);
+        if (KIND == 0) {
+            load_3d(sm + L::oA, &mp[VE_A], x0, ic - 1, f.s, &bar);            // Sxx
+            load_3d(sm + L::oC, &mp[VE_C], x0 - 4, ic, f.s + 1, &bar);        // Szz
+            load_3d(sm + L::oE, &mp[VE_E], x0 - 4, ic - 2, f.s + 2, &bar);    // Sxz
+        } else {
+            load_3d(sm + L::oA, &mp[VE_A], x0, ic - 2, f.s + 1, &bar);        // Sxy
+            load_3d(sm + L::oC, &mp[VE_C], x0 - 4, ic, f.s, &bar);            // Syz
         }
+        limit = wait_limit(err);
     }
     copy_model(models, tl.model, sM);
-    __syncthreads();
-    if (!go || !wait_tiles(&bar, err)) return;
+    __syncthreads();   // barrier initialised, wait limit and model descriptor set
     const Model2D &M = sM;
+    // the band signs of this thread's cells are read while the tiles travel
+    int sg[RI];
+#pragma unroll
+    for (int r = 0; r < RI; r++) {
+        const int k = tl.k0 + tx, i = tl.i0 + ty + r * TI;
+        const bool interior = i >= M.ibk && i <= M.iek && k <= M.kek;
+        sg[r] = (interior && k <= M.nz && (mask & 1)) ? band_sign2d(M, k, i) : -1;
+    }
+    if (!wait_tiles(&bar, err, limit)) return;   // the copy did not complete
 #pragma unroll
     for (int r = 0; r < RI; r++) {
         const int row = ty + r * TI;
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(32 * TI) vel2d_tma_kernel(const __grid_constan
         if (!(mask & (interior ? 1 : 2))) continue;
         const long long e = (long long)(i + 2) * M.Kp + (k - 1 + KH);
         const SVel2<KIND> o{sm, row, tx};
-        const int s = interior ? band_sign2d(M, k, i) : -1;
+        const int s = sg[r];
         if (KIND == 0) psv_vel_cell(M, o, k, i, e, s);
         else sh_vel_cell(M, o, k, i, e, s);
     }

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
     using L = StrBoxes<NM, BI, BJ, M>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int go;
+    __shared__ unsigned long long limit;
     float *sm = aligned128(smraw);
     const Geo g = a.g;
     const Tile T = tile_of<M>(t, BI, BJ);
@@ -138,10 +138,10 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
     const bool with_r = (a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek);
     const bool staged =
         with_r || ((a.mask & 2) && tile_has_absorber(T, BI, BJ, g, a.ibk, a.iek, a.jbk, a.jek, a.kek));
-    bool ok = true;
-    if (staged && !stage_begin(&bar, &go, t.err, lead)) ok = false;
-    else if (staged && lead) {
-        mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem, with_r));
+    if (!staged) return;   // nothing of this launch here (uniform over the CTA)
+    if (lead) {
+        // the copies go out first; the error word is read while they travel
+        stage_init(&bar, (unsigned)L::bytes(T.nmem, with_r));
         const int x0 = T.k0 - 1 + KH;
         load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
         for (int mm = 0; mm < T.nmem; mm++) {
@@ -150,22 +150,25 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
             load_4d(p, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state + fm, &bar);
             load_4d(p + up32(L::nState), &tm_v, x0 - 4, T.i0, T.j0, t.f_v + fm, &bar);
         }
+        limit = wait_limit(t.err);
     }
     const int k = T.k0 + tx, i = T.i0 + ty, j = T.j0 + tz;
     const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
     const bool mine = k <= g.nz && i <= g.nx && j <= g.ny && (a.mask & (interior ? 1 : 2));
-    // an absorber cell's auxiliaries travel while the tiles do (up to two members)
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    // the band sign of an interior cell and the auxiliaries of an absorber
+    // cell (up to two members) are read while the tiles travel
+    const int sgn = (mine && interior) ? band_sign_of(a.band, col, k) : 0;
     constexpr bool PRE = M <= 2;
     Aux9 xs[PRE ? M : 1];
-    if (PRE && staged && ok && mine && !interior) {
+    if (PRE && mine && !interior) {
 #pragma unroll
         for (int mm = 0; mm < (PRE ? M : 1); mm++)
             if (mm < T.nmem) xs[mm] = aux_load(a.aV, (long long)(T.m0 + mm) * t.ao, a.pmlcol, g, k, i, j);
     }
-    if (staged && ok) ok = wait_tiles(&bar, t.err);
-    if (!staged || !ok || !mine) return;   // nothing of this launch here, or the copy failed
-    const long long col = col_index(g, i, j);
-    const long long e = col * g.Kp + (k - 1 + KH);
+    __syncthreads();   // barrier initialised, wait limit set
+    if (!wait_tiles(&bar, t.err, limit) || !mine) return;   // the copy failed, or no cell of this launch here
 #pragma unroll
     for (int mm = 0; mm < M; mm++) {
         if (mm >= T.nmem) break;
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(KT * BI * BJ, (blocks_per_sm<StrBoxes<NM, BI, 
         const SStrOps<NM, BI, BJ> o{p, p + up32(L::nState), sm, tx, ty, tz};
         float *const Sp[6] = {a.Sxx + so, a.Syy + so, a.Szz + so, a.Syz + so, a.Sxz + so, a.Sxy + so};
         if (interior) {
-            stress_interior<NM, PREC_F32>(a, o, band_sign_of(a.band, col, k), Sp, e, so);
+            stress_interior<NM, PREC_F32>(a, o, sgn, Sp, e, so);
         } else {
             const Aux9 x = PRE ? xs[PRE ? mm : 0] : aux_load(a.aV, ao, a.pmlcol, g, k, i, j);
             stress_absorber<PREC_F32>(a, o, x, k, i, j, e, ao, Sp);
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
     using L = VelBoxes<BI, BJ, M>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int go;
+    __shared__ unsigned long long limit;
     float *sm = aligned128(smraw);
     const Geo g = a.g;
     const Tile T = tile_of<M>(t, BI, BJ);
@@ -250,10 +253,10 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
     const bool lead = tx == 0 && ty == 0;
     const bool staged = ((a.mask & 1) && tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek)) ||
                         ((a.mask & 2) && tile_has_absorber(T, BI, BJ, g, a.ibk, a.iek, a.jbk, a.jek, a.kek));
-    bool ok = true;
-    if (staged && !stage_begin(&bar, &go, t.err, lead)) ok = false;
-    else if (staged && lead) {
-        mbar_expect_tx(&bar, (unsigned)L::bytes(T.nmem));
+    if (!staged) return;   // nothing of this launch here (uniform over the CTA)
+    if (lead) {
+        // the copies go out first; the error word is read while they travel
+        stage_init(&bar, (unsigned)L::bytes(T.nmem));
         const int x0 = T.k0 - 1 + KH, ic = T.i0 + 2, jc = T.j0 + 2;
         load_4d(sm, &tm_b, x0, ic, jc, t.f_b, &bar);
         for (int mm = 0; mm < T.nmem; mm++) {
@@ -267,14 +270,23 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
             load_4d(p + L::oE, &tm_e, x0 - 4, ic - 2, jc, f + 7, &bar);
             load_4d(p + L::oD, &tm_d, x0, ic - 2, jc - 2, f + 8, &bar);
         }
+        limit = wait_limit(t.err);
     }
     const int k = T.k0 + tx, i = T.i0 + ty;
     const bool col_ok = k <= g.nz && i <= g.nx;
-    // the auxiliaries of this thread's absorber cells travel while the tiles do
-    // (up to two cells: BJ planes x M members)
+    // read while the tiles travel: the band signs of this thread's interior
+    // cells, and the auxiliaries of its absorber cells (up to two cells: BJ
+    // planes x M members)
+    int sgn[BJ];
+#pragma unroll
+    for (int jj = 0; jj < BJ; jj++) {
+        const int j = T.j0 + jj;
+        const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+        sgn[jj] = (col_ok && interior && (a.mask & 1)) ? band_sign_of(a.band, col_index(g, i, j), k) : 0;
+    }
     constexpr bool PRE = BJ * M <= 2;
     Aux9 xs[PRE ? M : 1][PRE ? BJ : 1];
-    if (PRE && staged && ok && col_ok && (a.mask & 2)) {
+    if (PRE && col_ok && (a.mask & 2)) {
 #pragma unroll
         for (int mm = 0; mm < (PRE ? M : 1); mm++)
 #pragma unroll
@@ -284,8 +296,8 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
                     xs[mm][jj] = aux_load(a.aS, (long long)(T.m0 + mm) * t.ao, a.pmlcol, g, k, i, j);
             }
     }
-    if (staged && ok) ok = wait_tiles(&bar, t.err);
-    if (!staged || !ok || !col_ok) return;   // nothing of this launch here, or the copy failed
+    __syncthreads();   // barrier initialised, wait limit set
+    if (!wait_tiles(&bar, t.err, limit) || !col_ok) return;   // the copy failed, or no cell of this launch here
 #pragma unroll
     for (int mm = 0; mm < M; mm++) {
         if (mm >= T.nmem) break;
@@ -299,8 +311,7 @@ __global__ void __launch_bounds__(KT * BI, (blocks_per_sm<VelBoxes<BI, BJ, M>::t
             const SVelOps<BI, BJ> o{sm + L::oMem(mm), sm, tx, ty, jj};
             const long long e = col_index(g, i, j) * g.Kp + (k - 1 + KH);
             if (interior) {
-                vel_interior<PREC_F32>(a, o, band_sign_of(a.band, col_index(g, i, j), k), a.Vx + so, a.Vy + so,
-                                       a.Vz + so, e);
+                vel_interior<PREC_F32>(a, o, sgn[jj], a.Vx + so, a.Vy + so, a.Vz + so, e);
             } else {
                 const Aux9 x = PRE ? xs[PRE ? mm : 0][PRE ? jj : 0] : aux_load(a.aS, ao, a.pmlcol, g, k, i, j);
                 vel_absorber<PREC_F32>(a, o, x, k, i, j, e, ao, a.Vx + so, a.Vy + so, a.Vz + so);

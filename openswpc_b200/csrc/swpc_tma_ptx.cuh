@@ -62,36 +62,38 @@ __device__ __forceinline__ unsigned long long gtime() {
     return t;
 }
 
-// Bounded wait for the tile copies.  After kWaitNs the kernel raises the
+// Barrier set-up by the lead thread, before it issues the tile copies.  The
+// other threads touch the barrier only after the block synchronises.
+__device__ __forceinline__ void stage_init(uint64_t *bar, unsigned bytes) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+    mbar_expect_tx(bar, bytes);
+}
+
+// Wait limit of a CTA, read by the lead thread after it issued its copies
+// (the read travels with them): kWaitNs, or kWaitAfterErrNs once an earlier
+// tile copy of the launch did not complete, so that a launch whose copies
+// fail ends quickly.
+constexpr unsigned long long kWaitAfterErrNs = 1000000ull;   // 1 ms
+__device__ __forceinline__ unsigned long long wait_limit(const int *err) {
+    return *reinterpret_cast<const volatile int *>(err) == 0 ? kWaitNs : kWaitAfterErrNs;
+}
+
+// Bounded wait for the tile copies.  After `limit` ns the kernel raises the
 // error word, waits once more (bounded) for its copies in flight, and the
-// caller skips the staged cells; CTAs that start after the error copy nothing
-// (see stage_begin).
-__device__ __forceinline__ bool wait_tiles(uint64_t *bar, int *err) {
+// caller skips the staged cells.
+__device__ __forceinline__ bool wait_tiles(uint64_t *bar, int *err, unsigned long long limit) {
     const unsigned long long t0 = gtime();
     while (!mbar_try_wait(bar, 0)) {
-        if (gtime() - t0 > kWaitNs) {
+        if (gtime() - t0 > limit) {
             atomicExch(err, 1);
             const unsigned long long t1 = gtime();
-            while (!mbar_try_wait(bar, 0) && gtime() - t1 < kWaitNs) {
+            while (!mbar_try_wait(bar, 0) && gtime() - t1 < limit) {
             }
             return false;
         }
     }
     return true;
-}
-
-// barrier set-up of a staged CTA; false when an earlier tile copy of the
-// launch failed (nothing is copied then)
-__device__ __forceinline__ bool stage_begin(uint64_t *bar, int *flag, const int *err, bool lead) {
-    if (lead) {
-        *flag = *reinterpret_cast<const volatile int *>(err) == 0;
-        if (*flag) {
-            mbar_init(bar, 1);
-            fence_barrier_init();
-        }
-    }
-    __syncthreads();
-    return *flag != 0;
 }
 
 __host__ __device__ constexpr int up32(int n) { return (n + 31) / 32 * 32; }
