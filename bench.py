@@ -55,8 +55,8 @@ FALLBACK_HBM_GBS = 6650.0
 # down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
 # algorithmic bytes, for the default (TMA-staged) kernels (the ncu summaries of stress3d_tma_kernel and
 # vel3d_tma_kernel on that grid, under profiles/)
-TRAFFIC_PER_ALGORITHMIC = {"stress": (1.250347e9 + 0.715447e9) / 1.828028416e9,
-                           "vel": (0.509357e9 + 0.124435e9) / 0.609632256e9}
+TRAFFIC_PER_ALGORITHMIC = {"stress": (1.261579e9 + 0.708133e9) / 1.828028416e9,
+                           "vel": (0.511189e9 + 0.124598e9) / 0.609632256e9}
 
 
 def make_params(name: str):
