@@ -889,15 +889,16 @@ def main():
             "storage": {"f32": "S, R FP32", "bf16r": "R BF16", "f16sr": "S, R FP16 (power-of-two scales)"}[args.precision],
             "data": "synthetic (seeded layered + von Karman medium)",
             "config": wl,
-            "roofline": {"bound": "hbm", "kernel": "stress3d_tma_kernel (TMA-staged fused interior + PML stress update)"
-                         if args.precision == "f32" else "stress3d_kernel (fused interior + PML stress update)",
+            "roofline": {"bound": "hbm", "kernel": "stress3d_tma_kernel (TMA-staged fused interior + PML stress update"
+                                                     + ("" if args.precision == "f32" else
+                                                        f", {args.precision} storage tiles") + ")",
                          "achieved": ach_stress, "peak": peak, "unit": "GB/s", "frac": ach_stress / peak,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "traffic": b_stress * TRAFFIC_PER_ALGORITHMIC["stress"] if args.precision == "f32" else None,
                          "traffic_source": "ncu DRAM bytes of the 1/64-scale case times 64 (same interior/PML mix)",
                          "algorithmic_bytes_per_launch": b_stress, "launch_ms": t_stress},
-            "roofline_vel": {"kernel": "vel3d_tma_kernel" if args.precision == "f32" else "vel3d_kernel",
+            "roofline_vel": {"kernel": "vel3d_tma_kernel" + (" (FP16 stress tiles)" if args.precision == "f16sr" else ""),
                              "achieved": ach_vel, "frac": ach_vel / peak,
                              "traffic": b_vel * TRAFFIC_PER_ALGORITHMIC["vel"] if args.precision == "f32" else None,
                              "algorithmic_bytes_per_launch": b_vel, "launch_ms": t_vel},

@@ -151,19 +151,38 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
         if (!rc) rc = dalloc(c, &c->kfs, ncol);
         if (!rc) rc = dalloc(c, &c->d_err, 1);
     } else if (is3d(c)) {
-        for (int q = 0; q < 3 && !rc; q++) rc = dalloc(c, &c->V[q], g.ncell);
-        // 2-byte storage (FP16 / BF16) takes half the floats
-        const long long nS = c->prec == SWPC_PREC_F16_SR ? (g.ncell + 1) / 2 : g.ncell;
-        const long long nR = c->prec != SWPC_PREC_F32 ? (g.ncell + 1) / 2 : g.ncell;
-        for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, &c->S[q], nS);
-        for (int comp = 0; comp < 6 && !rc; comp++)
-            for (int m = 0; m < d->nm && !rc; m++) rc = dalloc(c, &c->R[comp * 3 + m], nR);
-        for (int q = 1; q < 11 && !rc; q++) rc = dalloc(c, &c->med[q], g.ncell);
+        // reduced-precision storage: the FP32 fields in one slab (V, then S
+        // for BF16_R, then lam mu taup taus muyz muxz muxy and bx by bz) and
+        // the 2-byte fields in a second (S for F16_SR, then R component-major)
+        const bool h_s = c->prec == SWPC_PREC_F16_SR;
+        const int nf = 3 + (h_s ? 0 : 6) + 7 + 3;
+        const int nh = (h_s ? 6 : 0) + 6 * d->nm;
+        rc = dalloc(c, &c->slab, (size_t)nf * g.ncell);
+        // g.ncell is even (Kp is a multiple of 8), so every 2-byte field starts on a 4-byte boundary
+        if (!rc) rc = dalloc(c, &c->hslab, (size_t)std::max(nh, 1) * g.ncell);
+        if (!rc) {
+            auto F = [&](int f) { return c->slab + (size_t)f * g.ncell; };
+            auto H = [&](int f) { return reinterpret_cast<float *>(c->hslab + (size_t)f * g.ncell); };
+            for (int q = 0; q < 3; q++) c->V[q] = F(q);
+            for (int q = 0; q < 6; q++) c->S[q] = h_s ? H(q) : F(3 + q);
+            for (int comp = 0; comp < 6; comp++)
+                for (int m = 0; m < d->nm; m++) c->R[comp * 3 + m] = H((h_s ? 6 : 0) + comp * d->nm + m);
+            const int mb = h_s ? 3 : 9;
+            const int mq[7] = {1, 2, 3, 4, 8, 9, 10};
+            for (int q = 0; q < 7; q++) c->med[mq[q]] = F(mb + q);
+            for (int q = 0; q < 3; q++) c->med[5 + q] = F(mb + 7 + q);
+            c->slab_nf = nf;
+            c->hslab_nf = nh;
+            // the staged kernels are the default launch
+            c->stress_tma = true;
+            c->vel_tma = true;
+        }
         const long long ncol = (long long)g.Ip * g.Jp;
         if (!rc) rc = dalloc(c, &c->band, ncol);
         if (!rc) rc = dalloc(c, &c->pmlcol, ncol);
         if (!rc) rc = dalloc(c, &c->kob, ncol);
         if (!rc) rc = dalloc(c, &c->kfs, ncol);
+        if (!rc) rc = dalloc(c, &c->d_err, 1);
     } else {
         rc = create_2d(c);
     }
@@ -186,8 +205,9 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     adj_free(c);
     if (!is3d(c)) destroy_2d(c);
     if (c->slab) {
-        // the slab holds V, S, R and the 3D medium fields
+        // the slabs hold V, S, R and the medium fields
         cudaFree(c->slab);
+        if (c->hslab) cudaFree(c->hslab);
         for (auto &p : c->V) p = nullptr;
         for (auto &p : c->S) p = nullptr;
         for (auto &p : c->R) p = nullptr;
@@ -236,12 +256,12 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
     if (kernel < 0 || kernel > 6 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
         ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
         return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..6, minb 1..4, 32*bi*bj <= 256)");
-    if (kernel >= 2 && c->prec != SWPC_PREC_F32)
-        return set_err(c, SWPC_ERR_ARG, "reduced-precision storage runs the kernels 0 and 1 only");
+    if (kernel >= 2 && kernel <= 4 && c->prec != SWPC_PREC_F32)
+        return set_err(c, SWPC_ERR_ARG, "reduced-precision storage runs the kernels 0, 1, 5 and 6 only");
     // staged kernels: minb is unused (pass 1); the tile must be compiled
-    if (kernel >= 5 && (!is3d(c) || !c->slab || minb != 1 ||
-                        !(kernel == 5 ? tma_shape_ok(bi, bj, 1) : tma_vel_shape_ok(bi, bj, 1))))
-        return set_err(c, SWPC_ERR_ARG, "staged kernels: 3D FP32 only, minb 1, with a compiled tile (bi, bj)");
+    if (kernel >= 5 && (!c->slab || minb != 1 ||
+                        !(kernel == 5 ? tma_shape_ok(bi, bj, 1, c->prec) : tma_vel_shape_ok(bi, bj, 1, c->prec))))
+        return set_err(c, SWPC_ERR_ARG, "staged kernels: minb 1 and a compiled tile (bi, bj)");
     invalidate_graph(c);
     switch (kernel) {
     case 0: c->stress_march = false; c->stress_tma = false; c->stress_minb = minb; c->bi = bi; c->bj = bj; break;
@@ -763,8 +783,9 @@ static int tma_ready(swpc_ctx *c) {
     if (c->tmaps && std::equal(key, key + 4, c->tma_key)) return SWPC_OK;
     if (!c->tmaps) c->tmaps = new TmaMaps();
     TmaMaps &m = *static_cast<TmaMaps *>(c->tmaps);
-    const TmaSlabs s{c->slab, c->slab_nf, c->slab, c->slab_nf};
-    if (!tma_encode_stress(m, s, c->g, c->d.nm, key[0], key[1]) || !tma_encode_vel(m, s, c->g, key[2], key[3]))
+    const TmaSlabs s{c->slab, c->slab_nf, c->slab, c->slab_nf, c->hslab, c->hslab_nf};
+    if (!tma_encode_stress(m, s, c->g, c->d.nm, key[0], key[1], c->prec) ||
+        !tma_encode_vel(m, s, c->g, key[2], key[3], c->prec))
         return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the field slab");
     std::copy(key, key + 4, c->tma_key);
     return SWPC_OK;
@@ -781,11 +802,14 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc) {
     t.nmem = nmem;
     t.mgroups = (nmem + mpc - 1) / mpc;
     t.tiles_first = 0;
+    // slab field order: FP32 V S R medium b; BF16_R V S medium b (R in the
+    // 2-byte slab); F16_SR V medium b (S and R in the 2-byte slab)
     t.f_v = 0;
     t.f_state = 3;
     t.f_member = 0;
-    t.f_med = 9 + 6 * c->d.nm;
-    t.f_b = 16 + 6 * c->d.nm;
+    t.f_med = c->prec == SWPC_PREC_F32 ? 9 + 6 * c->d.nm : c->prec == SWPC_PREC_BF16_R ? 9 : 3;
+    t.f_b = t.f_med + 7;
+    t.f_h = 0;
     t.so = 0;
     t.ao = 0;
     t.err = c->d_err;
@@ -820,7 +844,7 @@ static int launch_stress(swpc_ctx *c, int mask) {
         RC(tma_ready(c));
         const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1);
         return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tbi,
-                                                 c->stress_tbj, 1, c->stream), "stress3d_tma launch");
+                                                 c->stress_tbj, 1, c->stream, c->prec), "stress3d_tma launch");
     }
     if (c->stress_march && c->prec == SWPC_PREC_F32)
         launch_stress3d_march(a, c->d.nm, c->stress_mminb, c->stress_jc, c->stream);
@@ -850,7 +874,7 @@ static int launch_vel(swpc_ctx *c, int mask) {
         RC(tma_ready(c));
         const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1);
         return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tbi, c->vel_tbj, 1,
-                                              c->stream), "vel3d_tma launch");
+                                              c->stream, c->prec), "vel3d_tma launch");
     }
     if (c->prec != SWPC_PREC_F32) launch_vel3d(a, c->vel_minb, c->prec, grid, block, c->stream);
     else if (c->vel_vec) launch_vel3d_vec(a, c->vel_vminb, dim3(32, c->vel_vbi, c->vel_vbj), c->stream);

@@ -173,6 +173,10 @@ struct swpc_ctx {
     // lam taup taus mu rho
     float *slab = nullptr;
     int slab_nf = 0;
+    // reduced-precision 3D storage: the 2-byte fields (S for F16_SR, then R
+    // component-major) in a second slab of ncell-element fields
+    unsigned short *hslab = nullptr;
+    int hslab_nf = 0;
     int nfbatch = 0;   // reciprocity batches that borrow this context (swpc_fbatch.cu)
 
     long long bytes = 0;

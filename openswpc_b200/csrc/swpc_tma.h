@@ -19,6 +19,7 @@ struct TmaTiles {
     int f_member;        // state slab: field stride between members
     int f_med;           // medium slab: lam (lam mu taup taus muyz muxz muxy)
     int f_b;             // medium slab: bx (bx by bz)
+    int f_h;             // 2-byte slab of a reduced storage form: S (F16_SR) or R (BF16_R)
     long long so, ao;    // offset between members of the state arrays and of the PML auxiliaries
     int *err;            // raised when a tile copy does not complete
 };
@@ -29,12 +30,14 @@ struct TmaSlabs {
     long long nf_state;
     float *med;
     long long nf_med;
+    void *half;           // reduced storage forms: the 2-byte fields (S for F16_SR, then R)
+    long long nf_half;
 };
 
 // host copies of the tensor maps (CUtensorMap, 128 bytes, 64-byte aligned)
 struct alignas(64) TmaMaps {
-    unsigned char state[128];   // stress: S and R of a member
-    unsigned char s6[128];      // stress: S of a member (tiles without interior cells)
+    unsigned char state[128];   // stress: S and R of a member (BF16_R: R; F16_SR: S and R in FP16)
+    unsigned char s6[128];      // stress: S of a member (tiles without interior cells; F16_SR: FP16)
     unsigned char med[128];     // stress: the seven medium fields of the stress update
     unsigned char vh[128];      // stress: V of a member with halo
     unsigned char own3[128];    // velocity: V of a member
@@ -44,14 +47,16 @@ struct alignas(64) TmaMaps {
 
 // compiled tiles (bi, bj) and members per CTA: stress (4,4,1) (2,4,1) (4,2,1)
 // (4,2,2) (2,4,2) (2,2,2) (2,2,4) (4,1,4); velocity (4,2,1) (4,4,1) (2,2,1)
-// (4,2,2) (2,2,2) (4,1,2) (2,2,4) (4,1,4)
-bool tma_shape_ok(int bi, int bj, int mpc);
-bool tma_vel_shape_ok(int bi, int bj, int mpc);
-bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj);
-bool tma_encode_vel(TmaMaps &m, const TmaSlabs &s, const Geo &g, int bi, int bj);
+// (4,2,2) (2,2,2) (4,1,2) (2,2,4) (4,1,4).  The reduced storage forms (prec
+// PREC_BF16_R / PREC_F16_SR of swpc3d_cell.cuh) run stress (4,4,1) and
+// velocity (4,2,1).
+bool tma_shape_ok(int bi, int bj, int mpc, int prec = 0);
+bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec = 0);
+bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec = 0);
+bool tma_encode_vel(TmaMaps &m, const TmaSlabs &s, const Geo &g, int bi, int bj, int prec = 0);
 cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, int nm, int bi, int bj, int mpc,
-                                cudaStream_t st);
+                                cudaStream_t st, int prec = 0);
 cudaError_t launch_vel3d_tma(const TmaMaps &m, const Vel3Args &a, const TmaTiles &t, int bi, int bj, int mpc,
-                             cudaStream_t st);
+                             cudaStream_t st, int prec = 0);
 
 }  // namespace swpc

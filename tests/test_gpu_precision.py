@@ -85,3 +85,30 @@ def test_reduced_storage_roundtrip_and_rescale():
     y = g.download(_lib.F_SXX)
     inner = (slice(3, -3), slice(3, -3), slice(3, -3))
     assert np.abs(y[inner] - x[inner]).max() <= np.abs(x).max() * 2.0 ** -10
+
+
+@pytest.mark.parametrize("nm,grid", [(3, (40, 36, 32)), (1, (42, 38, 45)), (0, (42, 38, 45)), (2, (40, 36, 32))])
+@pytest.mark.parametrize("form", ["bf16r", "f16sr"])
+def test_staged_reduced_forms_equal_the_flat_kernels(form, nm, grid):
+    """The TMA-staged kernels of the reduced storage forms (2-byte tiles of S
+    and R) give the bits of the one-cell kernels of the same form: traces,
+    wavefield, memory variables and PML auxiliaries; tiles partial in k, i
+    and j, and tiles without interior cells, included."""
+    nx, ny, nz = grid
+    p = small3d(nx=nx, ny=ny, nz=nz, nt=50, nm=nm, sw_wav_stress=True)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    staged = Swpc3D(p, xi, precision=form)   # the default launch
+    flat = Swpc3D(p, xi, precision=form)
+    _lib.check(flat.ctx, flat.lib.swpc_set_launch(flat.ctx, 0, 2, 2, 1))
+    _lib.check(flat.ctx, flat.lib.swpc_set_launch(flat.ctx, 1, 4, 2, 2))
+    staged.run(1, p.nt)
+    flat.run(1, p.nt)
+    for what in (_lib.WAV_V, _lib.WAV_STRESS):
+        a, b = staged.waveforms(what), flat.waveforms(what)
+        assert np.linalg.norm(b) > 0
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+    fields = list(range(9)) + [_lib.F_R + 3 * c + m for c in range(6) for m in range(nm)] + \
+        [_lib.F_AUX + q for q in range(18)]
+    for fid in fields:
+        a, b = staged.download(fid), flat.download(fid)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), fid
