@@ -100,8 +100,9 @@ typedef struct swpc_desc {
 /* Storage precision of the 3D stress (S) and memory-variable (R) arrays; the
  * arithmetic is FP32 in every form.  F32 is the reference's MP = SP build;
  * BF16_R stores R in BF16; F16_SR stores S and R in FP16 with one
- * power-of-two scale per array (see swpc_rescale).  Reduced-precision forms
- * run the one-cell-per-thread kernels (swpc_set_launch kernels 0 and 1). */
+ * power-of-two scale per array (see swpc_rescale).  Every form runs the
+ * TMA-staged kernels by default (swpc_set_launch kernels 5 and 6); the
+ * one-cell-per-thread kernels 0 and 1 stay selectable. */
 #define SWPC_PREC_F32 0
 #define SWPC_PREC_BF16_R 1
 #define SWPC_PREC_F16_SR 2
@@ -413,9 +414,14 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * select the TMA-staged stress / velocity kernels (FP32 3D contexts): a CTA
  * per tile of 32 (k) x bi (i) x bj (j) cells whose operands arrive in shared
  * memory by bulk tensor copies; minb must be 1, and the compiled tiles
- * (bi, bj) are stress (4,4) (2,4) (4,2), velocity (4,2) (4,4) (2,2).  FP32
- * 3D contexts start with kernels 5 (4,4) and 6 (4,2); the other 3D forms
- * start with kernels 0 and 1.
+ * (bi, bj) are stress (4,4) (2,4) (4,2), velocity (4,4) (4,2) (2,2); the
+ * reduced storage forms (BF16_R, F16_SR) compile stress (4,4) and velocity
+ * (4,4).  3D contexts start with kernels 5 (4,4) and 6 (4,4).
+ * kernel 7 (3D) sets the launch order of the staged kernels: tiles run k
+ * fastest, then over (i, j) in blocks of bi consecutive j tiles (j fastest
+ * within a block), so that a tile's j-halo is still in L2; bi = 1 runs i then
+ * j, bi = 0 (the default) takes 16 when a j plane of tiles outgrows half of
+ * the L2 and 1 otherwise.
  * 2D contexts (P-SV, SH) take kernels 0 / 1 (the tile-walking stress /
  * velocity kernels) and 5 / 6 (the staged ones: a CTA per 32 x 16 tile with
  * bi = 4, 8 or 16 threads along i, minb 1, bj 1); they start with kernels

@@ -57,11 +57,19 @@ struct Tile {
     int k0, i0, j0, m0, nmem;   // first cell, first member, members in the group
 };
 template <int M>
+// Within a member group the tiles run k fastest, then over (i, j) in blocks
+// of t.jblock consecutive j tiles: j fastest inside a block, then i, then the
+// next block.  The j halo of a tile (V for the stress update, the shear and
+// Syy boxes for the velocity update) then comes from tiles launched a few
+// CTAs earlier, still in L2, instead of a j plane of tiles earlier.
 __device__ __forceinline__ Tile tile_of(const TmaTiles &t, int bi, int bj) {
     const int ntile = t.nkt * t.nit * t.njt;
     const int grp = t.tiles_first ? blockIdx.x / ntile : blockIdx.x % t.mgroups;
     const int b = t.tiles_first ? blockIdx.x % ntile : blockIdx.x / t.mgroups;
-    const int kt = b % t.nkt, it = (b / t.nkt) % t.nit, jt = b / (t.nkt * t.nit);
+    const int kt = b % t.nkt, r = b / t.nkt;
+    const int jb = t.jblock, blk = r / (t.nit * jb), rem = r - blk * t.nit * jb;
+    const int nb = min(jb, t.njt - blk * jb);   // j tiles in this block (the last one may be short)
+    const int it = rem / nb, jt = blk * jb + rem % nb;
     const int m0 = grp * M;
     return Tile{1 + KT * kt, 1 + bi * it, 1 + bj * jt, m0, min(M, t.nmem - m0)};
 }
@@ -419,7 +427,7 @@ cudaError_t stress_nm(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, in
 // compiled (bi, bj, members per CTA); the reduced storage forms run the first
 // (default) shape of each list with one member
 constexpr int kStressShapes[][3] = {{4, 4, 1}, {2, 4, 1}, {4, 2, 1}, {4, 2, 2}, {2, 4, 2}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
-constexpr int kVelShapes[][3] = {{4, 2, 1}, {4, 4, 1}, {2, 2, 1}, {4, 2, 2}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
+constexpr int kVelShapes[][3] = {{4, 4, 1}, {4, 2, 1}, {2, 2, 1}, {4, 2, 2}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
 
 }  // namespace
 
@@ -458,7 +466,7 @@ cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTi
 cudaError_t launch_vel3d_tma(const TmaMaps &m, const Vel3Args &a, const TmaTiles &t, int bi, int bj, int mpc,
                              cudaStream_t st, int prec) {
     // BF16_R keeps S in FP32: its velocity update is the FP32 one
-    if (prec == PREC_F16_SR) return run_vel<4, 2, 1, PREC_F16_SR>(m, a, t, st);
+    if (prec == PREC_F16_SR) return run_vel<4, 4, 1, PREC_F16_SR>(m, a, t, st);
     if (mpc == 4) {
         if (bi == 4 && bj == 1) return run_vel<4, 1, 4, PREC_F32>(m, a, t, st);
         return run_vel<2, 2, 4, PREC_F32>(m, a, t, st);

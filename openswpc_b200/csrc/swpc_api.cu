@@ -253,6 +253,13 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
         else { c->vel_tma = true; c->vel_tbi = bi; }
         return SWPC_OK;
     }
+    if (kernel == 7) {
+        // launch order of the staged kernels: blocks of bi j tiles (0: chosen by size)
+        if (bi < 0 || bi > 1024) return set_err(c, SWPC_ERR_ARG, "kernel 7: bi = j tiles per block, 0..1024");
+        invalidate_graph(c);
+        c->tile_jblock = bi;
+        return SWPC_OK;
+    }
     if (kernel < 0 || kernel > 6 || minb < 1 || minb > 4 || bi < 1 || bj < 1 ||
         ((kernel < 2 || kernel == 4) && 32 * bi * bj > 256))
         return set_err(c, SWPC_ERR_ARG, "launch shape out of range (kernel 0..6, minb 1..4, 32*bi*bj <= 256)");
@@ -794,7 +801,7 @@ static int tma_ready(swpc_ctx *c) {
 namespace swpc {
 // tiles of a staged launch over the whole grid for nmem members grouped by
 // mpc; the medium fields come from the context's slab
-TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc) {
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields) {
     TmaTiles t;
     t.nkt = (c->g.nz + 31) / 32;
     t.nit = (c->g.nx + bi - 1) / bi;
@@ -802,6 +809,11 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc) {
     t.nmem = nmem;
     t.mgroups = (nmem + mpc - 1) / mpc;
     t.tiles_first = 0;
+    // launch order: blocks of j tiles once a j plane of tiles (the fields the
+    // kernel reads over bj planes, every member) outgrows half of the L2
+    const double plane = (double)nfields * nmem * c->g.Kp * c->g.Ip * bj * 4.0;
+    const int jb = c->tile_jblock > 0 ? c->tile_jblock : (plane > 64e6 ? 16 : 1);
+    t.jblock = std::max(1, std::min(jb, t.njt));
     // slab field order: FP32 V S R medium b; BF16_R V S medium b (R in the
     // 2-byte slab); F16_SR V medium b (S and R in the 2-byte slab)
     t.f_v = 0;
@@ -842,7 +854,7 @@ static int launch_stress(swpc_ctx *c, int mask) {
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
     if (c->stress_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1);
+        const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1, kStressFields(c));
         return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tbi,
                                                  c->stress_tbj, 1, c->stream, c->prec), "stress3d_tma launch");
     }
@@ -872,7 +884,7 @@ static int launch_vel(swpc_ctx *c, int mask) {
     for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
     if (c->vel_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1);
+        const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1, kVelFields);
         return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tbi, c->vel_tbj, 1,
                                               c->stream, c->prec), "vel3d_tma launch");
     }

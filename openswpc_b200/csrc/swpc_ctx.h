@@ -162,7 +162,8 @@ struct swpc_ctx {
     // the field slab, encoded for the shapes in tma_key.  2D contexts
     // (swpc2d_tma.cu): tiles 32 x 16 with stress_tbi / vel_tbi threads along i
     bool stress_tma = false, vel_tma = false;
-    int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 2;
+    int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 4;
+    int tile_jblock = 0;          // j tiles per block of the staged launch order (0: by size, see tma_tiles)
     void *tmaps = nullptr;        // swpc::TmaMaps
     int tma_key[4] = {-1, -1, -1, -1};
     int *d_err = nullptr;         // device error word of the staged kernels

@@ -37,7 +37,7 @@ namespace swpc {
 int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half);
 bool green_entries(const swpc_ctx *c, int isrc, int jsrc, int ksrc, char cmp, std::vector<InjEntry> &v);
 int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i);
-TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc);
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields);
 }  // namespace swpc
 
 using namespace swpc;
@@ -365,8 +365,8 @@ static int fb_tma_ready(swpc_fbatch *b) {
     return SWPC_OK;
 }
 
-static TmaTiles fb_tiles(const swpc_fbatch *b, int bi, int bj, int mpc) {
-    TmaTiles t = tma_tiles(b->c, bi, bj, b->nmem, mpc);
+static TmaTiles fb_tiles(const swpc_fbatch *b, int bi, int bj, int mpc, int nfields) {
+    TmaTiles t = tma_tiles(b->c, bi, bj, b->nmem, mpc, nfields);
     t.f_member = b->nfs;
     t.so = b->stride;
     t.ao = b->astride;
@@ -419,7 +419,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         for (int q = 0; q < 18; q++) { a.sR[q] = 1.0f; a.iR[q] = 1.0f; }
         if (b->staged) {
             FRC(fb_tma_ready(b));
-            const TmaTiles t = fb_tiles(b, b->sbi, b->sbj, b->smpc);
+            const TmaTiles t = fb_tiles(b, b->sbi, b->sbj, b->smpc, kStressFields(b->c));
             FCK(launch_stress3d_tma(*static_cast<TmaMaps *>(b->tmaps), a, t, c->d.nm, b->sbi, b->sbj, b->smpc,
                                     c->stream));
         } else {
@@ -453,7 +453,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         for (int q = 0; q < 6; q++) a.sS[q] = 1.0f;
         if (b->staged) {
             FRC(fb_tma_ready(b));
-            const TmaTiles t = fb_tiles(b, b->vbi, b->vbj, b->vmpc);
+            const TmaTiles t = fb_tiles(b, b->vbi, b->vbj, b->vmpc, kVelFields);
             FCK(launch_vel3d_tma(*static_cast<TmaMaps *>(b->tmaps), a, t, b->vbi, b->vbj, b->vmpc, c->stream));
         } else {
             const BatchGrid bg = batch_grid(b, c->vbi, c->vbj);

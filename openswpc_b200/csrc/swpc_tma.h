@@ -14,6 +14,7 @@ struct TmaTiles {
     int nkt, nit, njt;
     int nmem, mgroups;   // members, groups of members per CTA
     int tiles_first;     // launch order: 0 member groups fastest, 1 tiles fastest
+    int jblock;          // tiles of a group: k fastest, then blocks of jblock j tiles (j, then i)
     int f_v;             // state slab: Vx of member 0 (S follows at f_v + 3)
     int f_state;         // state slab: Sxx of member 0 (S, then R)
     int f_member;        // state slab: field stride between members
@@ -23,6 +24,11 @@ struct TmaTiles {
     long long so, ao;    // offset between members of the state arrays and of the PML auxiliaries
     int *err;            // raised when a tile copy does not complete
 };
+
+// fields a staged stress / velocity update reads over its tile (member state
+// and medium): S, R, V, lam mu taup taus muyz muxz muxy, bx by bz / V, S, bx by bz
+inline int kStressFields(const swpc_ctx *c) { return 16 + 6 * c->d.nm; }
+constexpr int kVelFields = 12;
 
 // the slabs the tensor maps cover
 struct TmaSlabs {
@@ -46,10 +52,10 @@ struct alignas(64) TmaMaps {
 };
 
 // compiled tiles (bi, bj) and members per CTA: stress (4,4,1) (2,4,1) (4,2,1)
-// (4,2,2) (2,4,2) (2,2,2) (2,2,4) (4,1,4); velocity (4,2,1) (4,4,1) (2,2,1)
+// (4,2,2) (2,4,2) (2,2,2) (2,2,4) (4,1,4); velocity (4,4,1) (4,2,1) (2,2,1)
 // (4,2,2) (2,2,2) (4,1,2) (2,2,4) (4,1,4).  The reduced storage forms (prec
 // PREC_BF16_R / PREC_F16_SR of swpc3d_cell.cuh) run stress (4,4,1) and
-// velocity (4,2,1).
+// velocity (4,4,1).
 bool tma_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec = 0);

@@ -285,6 +285,25 @@ def test_launch_variants_are_bitwise_identical(variant):
         assert same_bits(g0.download(_lib.F_AUX + q), g1.download(_lib.F_AUX + q)), q
 
 
+@pytest.mark.parametrize("jblock", [1, 3, 5, 0])
+def test_staged_launch_order_is_bitwise_identical(jblock):
+    """Blocks of jblock j tiles in the staged launch order (a short last
+    block for 3 of the 10 j tiles; 0 = the size-dependent default) against
+    the flat kernels."""
+    p = small3d(nx=44, ny=38, nz=70, na=8, nt=25)
+    g0 = Swpc3D(p)
+    g1 = Swpc3D(p)
+    _lib.check(g0.ctx, g0.lib.swpc_set_launch(g0.ctx, 0, 2, 2, 1))
+    _lib.check(g0.ctx, g0.lib.swpc_set_launch(g0.ctx, 1, 4, 2, 2))
+    _lib.check(g1.ctx, g1.lib.swpc_set_launch(g1.ctx, 7, 1, jblock, 1))
+    g0.run(1, p.nt)
+    g1.run(1, p.nt)
+    for n in range(9):
+        assert same_bits(g0.download(n), g1.download(n)), n
+    for q in range(18):
+        assert same_bits(g0.download(_lib.F_AUX + q), g1.download(_lib.F_AUX + q)), q
+
+
 @pytest.mark.parametrize("nm", [0, 1, 2])
 def test_staged_kernels_with_fewer_memory_variables(nm):
     """The staged kernels read R from a slab box whose width follows nm."""
