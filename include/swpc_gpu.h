@@ -422,6 +422,9 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * within a block), so that a tile's j-halo is still in L2; bi = 1 runs i then
  * j, bi = 0 (the default) takes 16 when a j plane of tiles outgrows half of
  * the L2 and 1 otherwise.
+ * kernel 8 (3D) selects the stress-phase weights kernel of the adjoint step
+ * (swpc_adj_*, swpc_gradient): bi = 1 the TMA-staged kernel (default), 0 the
+ * one-cell-per-thread kernel.
  * 2D contexts (P-SV, SH) take kernels 0 / 1 (the tile-walking stress /
  * velocity kernels) and 5 / 6 (the staged ones: a CTA per 32 x 16 tile with
  * bi = 4, 8 or 16 threads along i, minb 1, bj 1); they start with kernels

@@ -39,59 +39,13 @@
 #include "swpc3d_cell.cuh"
 #include "swpc_tma.h"
 #include "swpc_tma_ptx.cuh"
+#include "swpc_tma_tile.cuh"
 
 namespace swpc {
 
 namespace {
 
 using namespace tma;
-
-constexpr int KT = 32;                                 // cells of a tile along k
-constexpr int KB = KT + 8;                             // k extent of a halo box: k0-4 .. k0+35 (16-byte aligned start)
-
-// tile and member group of this CTA: member group fastest, then k, i, j
-// (the medium of a tile is re-read from L2 by the groups that follow), or with
-// t.tiles_first the tiles fastest and the groups one after another (the halos
-// of neighbouring tiles are re-read from L2, as in a run of its own)
-struct Tile {
-    int k0, i0, j0, m0, nmem;   // first cell, first member, members in the group
-};
-template <int M>
-// Within a member group the tiles run k fastest, then over (i, j) in blocks
-// of t.jblock consecutive j tiles: j fastest inside a block, then i, then the
-// next block.  The j halo of a tile (V for the stress update, the shear and
-// Syy boxes for the velocity update) then comes from tiles launched a few
-// CTAs earlier, still in L2, instead of a j plane of tiles earlier.
-__device__ __forceinline__ Tile tile_of(const TmaTiles &t, int bi, int bj) {
-    const int ntile = t.nkt * t.nit * t.njt;
-    const int grp = t.tiles_first ? blockIdx.x / ntile : blockIdx.x % t.mgroups;
-    const int b = t.tiles_first ? blockIdx.x % ntile : blockIdx.x / t.mgroups;
-    const int kt = b % t.nkt, r = b / t.nkt;
-    const int jb = t.jblock, blk = r / (t.nit * jb), rem = r - blk * t.nit * jb;
-    const int nb = min(jb, t.njt - blk * jb);   // j tiles in this block (the last one may be short)
-    const int it = rem / nb, jt = blk * jb + rem % nb;
-    const int m0 = grp * M;
-    return Tile{1 + KT * kt, 1 + bi * it, 1 + bj * jt, m0, min(M, t.nmem - m0)};
-}
-
-__device__ __forceinline__ bool tile_has_interior(const Tile &T, int bi, int bj, int ibk, int iek, int jbk, int jek,
-                                                  int kek) {
-    return T.k0 <= kek && T.i0 <= iek && T.i0 + bi - 1 >= ibk && T.j0 <= jek && T.j0 + bj - 1 >= jbk;
-}
-// does the tile hold absorber cells (cells of the grid outside the kernel region)?
-__device__ __forceinline__ bool tile_has_absorber(const Tile &T, int bi, int bj, const Geo &g, int ibk, int iek,
-                                                  int jbk, int jek, int kek) {
-    const int i1 = min(T.i0 + bi - 1, g.nx), j1 = min(T.j0 + bj - 1, g.ny), k1 = min(T.k0 + KT - 1, g.nz);
-    return T.i0 < ibk || i1 > iek || T.j0 < jbk || j1 > jek || k1 > kek;
-}
-
-template <int SMEM_FLOATS, int THREADS>
-__host__ __device__ constexpr int blocks_per_sm() {
-    constexpr int by_smem = (227 * 1024) / (SMEM_FLOATS * 4 + 128 + 1024);
-    constexpr int by_threads = 1024 / THREADS;   // at least 64 registers a thread
-    constexpr int n = by_smem < by_threads ? by_smem : by_threads;
-    return n < 1 ? 1 : n;
-}
 
 // ---------------------------------------------------------------------------
 // stress
@@ -511,6 +465,11 @@ static bool encode(unsigned char *out, void *slab, const Geo &g, long long nf, u
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+bool tma_encode_box(unsigned char *out, float *slab, const Geo &g, long long nf, unsigned bk, unsigned bi, unsigned bj,
+                    unsigned bf) {
+    return encode(out, slab, g, nf, bk, bi, bj, bf);
 }
 
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec) {

@@ -31,6 +31,9 @@
 
 #include "swpc_ctx.h"
 #include "swpc_kernels.cuh"
+#include "swpc_tma.h"
+#include "swpc_tma_ptx.cuh"
+#include "swpc_tma_tile.cuh"
 
 namespace swpc {
 int graph_invalidate(swpc_ctx *c);
@@ -43,6 +46,9 @@ using namespace swpc;
 // adjoint state of a context
 struct swpc_adj_state {
     float *lV[3] = {}, *lS[6] = {}, *lR[18] = {}, *laux[18] = {};
+    float *slab = nullptr;               // lV, lS, lR in the forward slab's field order (V, S, R)
+    int slab_nf = 0;
+    swpc::TmaMaps *maps = nullptr;       // staged stress-phase weights: state, s6 (adjoint slab), med, vh (slots)
     float *w40[9] = {}, *w41[9] = {};    // difference-operator weights
     double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
@@ -111,22 +117,48 @@ __device__ __forceinline__ int band_sign(const int4 bd, int k) {
     return ((p1 > p2 ? p1 : p2) >= 0) ? 1 : 0;
 }
 
+// tiles of the staged adjoint kernels: 32 x 4 x 4 cells, one thread per cell
+namespace adjt {
+using namespace tma;
+constexpr int BI = 4, BJ = 4, NT = KT * BI * BJ;
+}  // namespace adjt
+
 // ---------------------------------------------------------------------------
 // transpose of the velocity update: weights
 // pairs p: 0 (Vx,Sxx,x) 1 (Vx,Sxy,y) 2 (Vx,Sxz,z) 3 (Vy,Sxy,x) 4 (Vy,Syy,y)
 //          5 (Vy,Syz,z) 6 (Vz,Sxz,x) 7 (Vz,Syz,y) 8 (Vz,Szz,z)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a) {
-    const Geo g = a.g;
-    int k, i, j;
-    if (!cell_of(g, k, i, j)) return;
-    const long long col = col_index(g, i, j);
-    const long long e = col * g.Kp + (k - 1 + KH);
+// Operands of one cell: lV(c) the adjoint velocity, b(c) the buoyancy,
+// S(f, dk, di, dj) the forward stress after the stress update (f: xx yy zz
+// yz xz xy).
+struct GAdjVelOps {
+    const AdjVelArgs &a;
+    long long e, PI, PJ;
+    __device__ __forceinline__ float lV(int c) const { return a.lV[c][e]; }
+    __device__ __forceinline__ float b(int c) const { return a.b[c][e]; }
+    __device__ __forceinline__ float S(int f, int dk, int di, int dj) const {
+        return a.S[f][e + dk + di * PI + dj * PJ];
+    }
+};
+
+struct Gb3 {
+    double v[3];
+};
+__device__ __forceinline__ Gb3 gb_load(const AdjVelArgs &a, long long e) {
+    Gb3 g;
+#pragma unroll
+    for (int q = 0; q < 3; q++) g.v[q] = a.gb[q][e];
+    return g;
+}
+
+// interior (s >= 0: band sign) or absorber (s < 0) cell
+template <class O>
+__device__ __forceinline__ void adj_vel_cell(const AdjVelArgs &a, const O &o, long long col, int k, int i, int j,
+                                             long long e, int s, const Gb3 &g0) {
     const float dt = a.dt;
-    const float l[3] = {a.lV[0][e], a.lV[1][e], a.lV[2][e]};
-    const float u[3] = {a.b[0][e] * dt * l[0], a.b[1][e] * dt * l[1], a.b[2][e] * dt * l[2]};
-    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
-        const int s = band_sign(__ldg(&a.band[col]), k);
+    const float l[3] = {o.lV(0), o.lV(1), o.lV(2)};
+    const float u[3] = {o.b(0) * dt * l[0], o.b(1) * dt * l[1], o.b(2) * dt * l[2]};
+    if (s >= 0) {
 #pragma unroll
         for (int p = 0; p < 9; p++) {
             const int c = p / 3, ax = p % 3;
@@ -135,22 +167,20 @@ __global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a
         }
         if (a.gb[0]) {
             // d(Vx)/d(bx) = d3Sx3 * dt on the forward S after the stress update
-            const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
-            const float *Sxx = a.S[0], *Syy = a.S[1], *Szz = a.S[2], *Syz = a.S[3], *Sxz = a.S[4], *Sxy = a.S[5];
             const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
             const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-            const float d3Sx3 = (Sxx[e + PI] - Sxx[e]) * re40x - (Sxx[e + 2 * PI] - Sxx[e - PI]) * re41x
-                              + (Sxy[e] - Sxy[e - PJ]) * re40y - (Sxy[e + PJ] - Sxy[e - 2 * PJ]) * re41y
-                              + (Sxz[e] - Sxz[e - 1]) * re40z - (Sxz[e + 1] - Sxz[e - 2]) * re41z;
-            const float d3Sy3 = (Sxy[e] - Sxy[e - PI]) * re40x - (Sxy[e + PI] - Sxy[e - 2 * PI]) * re41x
-                              + (Syy[e + PJ] - Syy[e]) * re40y - (Syy[e + 2 * PJ] - Syy[e - PJ]) * re41y
-                              + (Syz[e] - Syz[e - 1]) * re40z - (Syz[e + 1] - Syz[e - 2]) * re41z;
-            const float d3Sz3 = (Sxz[e] - Sxz[e - PI]) * re40x - (Sxz[e + PI] - Sxz[e - 2 * PI]) * re41x
-                              + (Syz[e] - Syz[e - PJ]) * re40y - (Syz[e + PJ] - Syz[e - 2 * PJ]) * re41y
-                              + (Szz[e + 1] - Szz[e]) * re40z - (Szz[e + 2] - Szz[e - 1]) * re41z;
-            a.gb[0][e] += (double)l[0] * d3Sx3 * dt;
-            a.gb[1][e] += (double)l[1] * d3Sy3 * dt;
-            a.gb[2][e] += (double)l[2] * d3Sz3 * dt;
+            const float d3Sx3 = (o.S(0, 0, 1, 0) - o.S(0, 0, 0, 0)) * re40x - (o.S(0, 0, 2, 0) - o.S(0, 0, -1, 0)) * re41x
+                              + (o.S(5, 0, 0, 0) - o.S(5, 0, 0, -1)) * re40y - (o.S(5, 0, 0, 1) - o.S(5, 0, 0, -2)) * re41y
+                              + (o.S(4, 0, 0, 0) - o.S(4, -1, 0, 0)) * re40z - (o.S(4, 1, 0, 0) - o.S(4, -2, 0, 0)) * re41z;
+            const float d3Sy3 = (o.S(5, 0, 0, 0) - o.S(5, 0, -1, 0)) * re40x - (o.S(5, 0, 1, 0) - o.S(5, 0, -2, 0)) * re41x
+                              + (o.S(1, 0, 0, 1) - o.S(1, 0, 0, 0)) * re40y - (o.S(1, 0, 0, 2) - o.S(1, 0, 0, -1)) * re41y
+                              + (o.S(3, 0, 0, 0) - o.S(3, -1, 0, 0)) * re40z - (o.S(3, 1, 0, 0) - o.S(3, -2, 0, 0)) * re41z;
+            const float d3Sz3 = (o.S(4, 0, 0, 0) - o.S(4, 0, -1, 0)) * re40x - (o.S(4, 0, 1, 0) - o.S(4, 0, -2, 0)) * re41x
+                              + (o.S(3, 0, 0, 0) - o.S(3, 0, 0, -1)) * re40y - (o.S(3, 0, 0, 1) - o.S(3, 0, 0, -2)) * re41y
+                              + (o.S(2, 1, 0, 0) - o.S(2, 0, 0, 0)) * re40z - (o.S(2, 2, 0, 0) - o.S(2, -1, 0, 0)) * re41z;
+            a.gb[0][e] = g0.v[0] + (double)l[0] * d3Sx3 * dt;
+            a.gb[1][e] = g0.v[1] + (double)l[1] * d3Sy3 * dt;
+            a.gb[2][e] = g0.v[2] + (double)l[2] * d3Sz3 * dt;
         }
         return;
     }
@@ -169,6 +199,19 @@ __global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a
         a.w40[p][e] = a.r20[ax] * lD;
         a.w41[p][e] = 0.0f;
     }
+}
+
+__global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const GAdjVelOps o{a, e, (long long)g.Kp, (long long)g.Kp * g.Ip};
+    const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+    const int s = interior ? band_sign(__ldg(&a.band[col]), k) : -1;
+    const Gb3 g0 = (interior && a.gb[0]) ? gb_load(a, e) : Gb3{};
+    adj_vel_cell(a, o, col, k, i, j, e, s, g0);
 }
 
 // transpose of a forward difference (f[e+P] - f[e]) * A40 - (f[e+2P] - f[e-P]) * A41
@@ -200,92 +243,125 @@ __global__ void __launch_bounds__(128) adj_vel_gather_kernel(const GatherArgs a)
 // pairs q: 0 (Vx,x,bwd) 1 (Vy,y,bwd) 2 (Vz,z,bwd) 3 (Vy,x,fwd) 4 (Vx,y,fwd)
 //          5 (Vz,x,fwd) 6 (Vx,z,fwd) 7 (Vz,y,fwd) 8 (Vy,z,fwd)
 // ---------------------------------------------------------------------------
-template <int NM>
-__global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArgs a) {
-    const Geo g = a.g;
-    int k, i, j;
-    if (!cell_of(g, k, i, j)) return;
-    const long long col = col_index(g, i, j);
-    const long long e = col * g.Kp + (k - 1 + KH);
+// Operands of one cell: lS(c) the adjoint stress, lR(q) the adjoint memory
+// variable q = component * 3 + m, med(m) the medium (0 mu, 1 lam, 2 taup,
+// 3 taus, 4 muyz, 5 muxz, 6 muxy), V(c, dk, di, dj) the forward velocity
+// before the stress update.  The one-cell kernel reads them from global
+// memory, the staged kernel from the tiles TMA copied to shared memory.
+struct GAdjStrOps {
+    const AdjStrArgs &a;
+    long long e, PI, PJ;
+    __device__ __forceinline__ float lS(int c) const { return a.lS[c][e]; }
+    __device__ __forceinline__ float lR(int q) const { return a.lR[q][e]; }
+    __device__ __forceinline__ float med(int m) const {
+        const float *p = m == 0 ? a.mu : m == 1 ? a.lam : m == 2 ? a.taup : m == 3 ? a.taus
+                       : m == 4 ? a.muyz : m == 5 ? a.muxz : a.muxy;
+        return p[e];
+    }
+    __device__ __forceinline__ float V(int c, int dk, int di, int dj) const {
+        return a.V[c][e + dk + di * PI + dj * PJ];
+    }
+};
+
+// the five imaging accumulators of a cell before this step (read early by
+// the staged kernel)
+struct Gm5 {
+    double v[5];
+};
+__device__ __forceinline__ Gm5 gm_load(const AdjStrArgs &a, long long e) {
+    Gm5 g;
+#pragma unroll
+    for (int q = 0; q < 5; q++) g.v[q] = a.gm[q][e];
+    return g;
+}
+
+// interior cell (s: band sign)
+template <int NM, class O>
+__device__ __forceinline__ void adj_stress_interior(const AdjStrArgs &a, const O &o, int s, long long e, const Gm5 &g0) {
     const float dt = a.dt;
     float al[6];
 #pragma unroll
-    for (int c = 0; c < 6; c++) al[c] = a.lS[c][e] * dt;
-    const float mu = a.mu[e], lam = a.lam[e];
-    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
-        const int s = band_sign(__ldg(&a.band[col]), k);
-        const float taup1 = a.taup[e], taus1 = a.taus[e];
-        const float muc[3] = {a.muyz[e], a.muxz[e], a.muxy[e]};
-        const float mu2 = 2 * mu;
-        const float lam2mu = lam + mu2;
-        const float taup_plus1 = 1 + taup1 * (1 + a.d2);
-        const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-        // memory variables: R' = c1 R - c2 F dt; S' = S + (G + sum d1 R') dt
-        float lF[6];
+    for (int c = 0; c < 6; c++) al[c] = o.lS(c) * dt;
+    const float mu = o.med(0), lam = o.med(1);
+    const float taup1 = o.med(2), taus1 = o.med(3);
+    const float muc[3] = {o.med(4), o.med(5), o.med(6)};
+    const float mu2 = 2 * mu;
+    const float lam2mu = lam + mu2;
+    const float taup_plus1 = 1 + taup1 * (1 + a.d2);
+    const float taus_plus1 = 1 + taus1 * (1 + a.d2);
+    // memory variables: R' = c1 R - c2 F dt; S' = S + (G + sum d1 R') dt
+    float lF[6];
 #pragma unroll
-        for (int c = 0; c < 6; c++) {
-            lF[c] = 0.0f;
+    for (int c = 0; c < 6; c++) {
+        lF[c] = 0.0f;
 #pragma unroll
-            for (int m = 0; m < NM; m++) {
-                const float L = a.lR[c * 3 + m][e] + a.d1[m] * al[c];
-                a.lR[c * 3 + m][e] = a.c1[m] * L;
-                lF[c] = lF[c] + L * (-a.c2[m] * dt);
-            }
+        for (int m = 0; m < NM; m++) {
+            const float L = o.lR(c * 3 + m) + a.d1[m] * al[c];
+            a.lR[c * 3 + m][e] = a.c1[m] * L;
+            lF[c] = lF[c] + L * (-a.c2[m] * dt);
         }
-        // normal: G_c = lam2mu taup+ d3v3 - mu2 taus+ X_c, F_c likewise with taup, taus
-        float ld3 = 0.0f, lX[3];
+    }
+    // normal: G_c = lam2mu taup+ d3v3 - mu2 taus+ X_c, F_c likewise with taup, taus
+    float ld3 = 0.0f, lX[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        ld3 = ld3 + lam2mu * taup_plus1 * al[c] + lam2mu * taup1 * lF[c];
+        lX[c] = -(mu2 * taus_plus1 * al[c] + mu2 * taus1 * lF[c]);
+    }
+    float ld[9];
+    ld[0] = ld3 + lX[1] + lX[2];   // dxVx appears in X_yy and X_zz
+    ld[1] = ld3 + lX[0] + lX[2];
+    ld[2] = ld3 + lX[0] + lX[1];
+    // shear: G = mu_c taus+ D, F = mu_c taus D (c = yz xz xy)
+    const float lyz = muc[0] * taus_plus1 * al[3] + muc[0] * taus1 * lF[3];
+    const float lxz = muc[1] * taus_plus1 * al[4] + muc[1] * taus1 * lF[4];
+    const float lxy = muc[2] * taus_plus1 * al[5] + muc[2] * taus1 * lF[5];
+    ld[3] = lxy; ld[4] = lxy; ld[5] = lxz; ld[6] = lxz; ld[7] = lyz; ld[8] = lyz;
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        a.w40[q][e] = a.e40[qaxis(q)][s] * ld[q];
+        a.w41[q][e] = a.e41[qaxis(q)][s] * ld[q];
+    }
+    if (a.gm[0]) {
+        // forward strain rates on V before the stress update
+        const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
+        const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+        const float vx0 = o.V(0, 0, 0, 0), vy0 = o.V(1, 0, 0, 0), vz0 = o.V(2, 0, 0, 0);
+        const float dxVx = (vx0 - o.V(0, 0, -1, 0)) * re40x - (o.V(0, 0, 1, 0) - o.V(0, 0, -2, 0)) * re41x;
+        const float dyVy = (vy0 - o.V(1, 0, 0, -1)) * re40y - (o.V(1, 0, 0, 1) - o.V(1, 0, 0, -2)) * re41y;
+        const float dzVz = (vz0 - o.V(2, -1, 0, 0)) * re40z - (o.V(2, 1, 0, 0) - o.V(2, -2, 0, 0)) * re41z;
+        const float sxy = (o.V(1, 0, 1, 0) - vy0) * re40x - (o.V(1, 0, 2, 0) - o.V(1, 0, -1, 0)) * re41x
+                        + (o.V(0, 0, 0, 1) - vx0) * re40y - (o.V(0, 0, 0, 2) - o.V(0, 0, 0, -1)) * re41y;
+        const float sxz = (o.V(2, 0, 1, 0) - vz0) * re40x - (o.V(2, 0, 2, 0) - o.V(2, 0, -1, 0)) * re41x
+                        + (o.V(0, 1, 0, 0) - vx0) * re40z - (o.V(0, 2, 0, 0) - o.V(0, -1, 0, 0)) * re41z;
+        const float syz = (o.V(2, 0, 0, 1) - vz0) * re40y - (o.V(2, 0, 0, 2) - o.V(2, 0, 0, -1)) * re41y
+                        + (o.V(1, 1, 0, 0) - vy0) * re40z - (o.V(1, 2, 0, 0) - o.V(1, -1, 0, 0)) * re41z;
+        const double d3 = (double)dxVx + dyVy + dzVz;
+        const double X[3] = {(double)dyVy + dzVz, (double)dxVx + dzVz, (double)dxVx + dyVy};
+        double glam = 0.0, gmu = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            ld3 = ld3 + lam2mu * taup_plus1 * al[c] + lam2mu * taup1 * lF[c];
-            lX[c] = -(mu2 * taus_plus1 * al[c] + mu2 * taus1 * lF[c]);
+            glam += (double)al[c] * taup_plus1 * d3 + (double)lF[c] * taup1 * d3;
+            gmu += (double)al[c] * (2.0 * taup_plus1 * d3 - 2.0 * taus_plus1 * X[c])
+                 + (double)lF[c] * (2.0 * taup1 * d3 - 2.0 * taus1 * X[c]);
         }
-        float ld[9];
-        ld[0] = ld3 + lX[1] + lX[2];   // dxVx appears in X_yy and X_zz
-        ld[1] = ld3 + lX[0] + lX[2];
-        ld[2] = ld3 + lX[0] + lX[1];
-        // shear: G = mu_c taus+ D, F = mu_c taus D (c = yz xz xy)
-        const float lyz = muc[0] * taus_plus1 * al[3] + muc[0] * taus1 * lF[3];
-        const float lxz = muc[1] * taus_plus1 * al[4] + muc[1] * taus1 * lF[4];
-        const float lxy = muc[2] * taus_plus1 * al[5] + muc[2] * taus1 * lF[5];
-        ld[3] = lxy; ld[4] = lxy; ld[5] = lxz; ld[6] = lxz; ld[7] = lyz; ld[8] = lyz;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-            a.w40[q][e] = a.e40[qaxis(q)][s] * ld[q];
-            a.w41[q][e] = a.e41[qaxis(q)][s] * ld[q];
-        }
-        if (a.gm[0]) {
-            // forward strain rates on V before the stress update
-            const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
-            const float *Vx = a.V[0], *Vy = a.V[1], *Vz = a.V[2];
-            const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
-            const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-            const float dxVx = (Vx[e] - Vx[e - PI]) * re40x - (Vx[e + PI] - Vx[e - 2 * PI]) * re41x;
-            const float dyVy = (Vy[e] - Vy[e - PJ]) * re40y - (Vy[e + PJ] - Vy[e - 2 * PJ]) * re41y;
-            const float dzVz = (Vz[e] - Vz[e - 1]) * re40z - (Vz[e + 1] - Vz[e - 2]) * re41z;
-            const float sxy = (Vy[e + PI] - Vy[e]) * re40x - (Vy[e + 2 * PI] - Vy[e - PI]) * re41x
-                            + (Vx[e + PJ] - Vx[e]) * re40y - (Vx[e + 2 * PJ] - Vx[e - PJ]) * re41y;
-            const float sxz = (Vz[e + PI] - Vz[e]) * re40x - (Vz[e + 2 * PI] - Vz[e - PI]) * re41x
-                            + (Vx[e + 1] - Vx[e]) * re40z - (Vx[e + 2] - Vx[e - 1]) * re41z;
-            const float syz = (Vz[e + PJ] - Vz[e]) * re40y - (Vz[e + 2 * PJ] - Vz[e - PJ]) * re41y
-                            + (Vy[e + 1] - Vy[e]) * re40z - (Vy[e + 2] - Vy[e - 1]) * re41z;
-            const double d3 = (double)dxVx + dyVy + dzVz;
-            const double X[3] = {(double)dyVy + dzVz, (double)dxVx + dzVz, (double)dxVx + dyVy};
-            double glam = 0.0, gmu = 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                glam += (double)al[c] * taup_plus1 * d3 + (double)lF[c] * taup1 * d3;
-                gmu += (double)al[c] * (2.0 * taup_plus1 * d3 - 2.0 * taus_plus1 * X[c])
-                     + (double)lF[c] * (2.0 * taup1 * d3 - 2.0 * taus1 * X[c]);
-            }
-            a.gm[0][e] += glam;
-            a.gm[1][e] += gmu;
-            a.gm[2][e] += ((double)al[3] * taus_plus1 + (double)lF[3] * taus1) * syz;
-            a.gm[3][e] += ((double)al[4] * taus_plus1 + (double)lF[4] * taus1) * sxz;
-            a.gm[4][e] += ((double)al[5] * taus_plus1 + (double)lF[5] * taus1) * sxy;
-        }
-        return;
+        a.gm[0][e] = g0.v[0] + glam;
+        a.gm[1][e] = g0.v[1] + gmu;
+        a.gm[2][e] = g0.v[2] + ((double)al[3] * taus_plus1 + (double)lF[3] * taus1) * syz;
+        a.gm[3][e] = g0.v[3] + ((double)al[4] * taus_plus1 + (double)lF[4] * taus1) * sxz;
+        a.gm[4][e] = g0.v[4] + ((double)al[5] * taus_plus1 + (double)lF[5] * taus1) * sxy;
     }
-    // absorber cell (m_absorb_p.f90:445-491)
+}
+
+// absorber cell (m_absorb_p.f90:445-491)
+template <class O>
+__device__ __forceinline__ void adj_stress_absorber(const AdjStrArgs &a, const O &o, long long col, int k, int i,
+                                                    int j, long long e) {
+    const float dt = a.dt;
+    float al[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) al[c] = o.lS(c) * dt;
+    const float mu = o.med(0), lam = o.med(1);
     const int2 pc = __ldg(&a.pmlcol[col]);
     const long long q = (long long)pc.y + (k - pc.x);
     const float4 gxc = __ldg(&a.gxc[i - 1]), gxe = __ldg(&a.gxe[i - 1]);
@@ -309,9 +385,9 @@ __global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArg
     }
     // shear: S' = S + mu_c (g1.x D1 + g2.x D2 + g1.y aux1 + g2.y aux2) dt
     {
-        const float byz = a.muyz[e] * dt * a.lS[3][e];
-        const float bxz = a.muxz[e] * dt * a.lS[4][e];
-        const float bxy = a.muxy[e] * dt * a.lS[5][e];
+        const float byz = o.med(4) * dt * o.lS(3);
+        const float bxz = o.med(5) * dt * o.lS(4);
+        const float bxy = o.med(6) * dt * o.lS(5);
         // (q, profile, aux index, beta): 3 dxVy gxe axVy; 4 dyVx gye ayVx; 5 dxVz gxe axVz;
         // 6 dzVx gze azVx; 7 dyVz gye ayVz; 8 dzVy gze azVy
         const float4 gg[6] = {gxe, gye, gxe, gze, gye, gze};
@@ -329,6 +405,92 @@ __global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArg
         a.w40[qq][e] = a.r20[qaxis(qq)] * ld[qq];
         a.w41[qq][e] = 0.0f;
     }
+}
+
+template <int NM>
+__global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const GAdjStrOps o{a, e, (long long)g.Kp, (long long)g.Kp * g.Ip};
+    if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
+        const Gm5 g0 = a.gm[0] ? gm_load(a, e) : Gm5{};
+        adj_stress_interior<NM>(a, o, band_sign(__ldg(&a.band[col]), k), e, g0);
+    } else {
+        adj_stress_absorber(a, o, col, k, i, j, e);
+    }
+}
+
+// The staged form (see swpc3d_tma.cu for the design): a CTA per tile of
+// 32 x 4 x 4 cells whose medium (the context's slab), adjoint S and R (the
+// adjoint slab, S alone in tiles without interior cells) and, for the
+// gradient, the forward V with its halo (one slot of the recompute) arrive
+// by bulk tensor copies; the imaging accumulators and band signs are read
+// while the copies travel.
+namespace adjt {
+template <int NM>
+struct Boxes {
+    static constexpr int n = NT;
+    static constexpr int nMed = 7 * n, nState = (6 + 6 * NM) * n, nV = 3 * (BJ + 4) * (BI + 4) * KB;
+    static constexpr int oState = up32(nMed), oV = oState + up32(nState), total = oV + up32(nV);
+    __host__ __device__ static constexpr unsigned bytes(bool with_r, bool grad) {
+        return 4u * (unsigned)(nMed + (with_r ? nState : 6 * n) + (grad ? nV : 0));
+    }
+};
+template <int NM>
+struct SOps {
+    const float *sm;
+    int tx, ty, tz;
+    using L = Boxes<NM>;
+    __device__ __forceinline__ int at(int f) const { return ((f * BJ + tz) * BI + ty) * KT + tx; }
+    __device__ __forceinline__ float lS(int c) const { return sm[L::oState + at(c)]; }
+    __device__ __forceinline__ float lR(int q) const { return sm[L::oState + at(6 + (q / 3) * NM + q % 3)]; }
+    // medium box: lam mu taup taus muyz muxz muxy
+    __device__ __forceinline__ float med(int m) const { return sm[at(m == 0 ? 1 : m == 1 ? 0 : m)]; }
+    __device__ __forceinline__ float V(int c, int dk, int di, int dj) const {
+        return sm[L::oV + ((c * (BJ + 4) + tz + 2 + dj) * (BI + 4) + ty + 2 + di) * KB + tx + 4 + dk];
+    }
+};
+}  // namespace adjt
+
+template <int NM, bool GRAD>
+__global__ void __launch_bounds__(adjt::NT, (tma::blocks_per_sm<adjt::Boxes<NM>::total, adjt::NT>()))
+    adj_stress_tma_kernel(const __grid_constant__ CUtensorMap tm_state, const __grid_constant__ CUtensorMap tm_s,
+                          const __grid_constant__ CUtensorMap tm_med, const __grid_constant__ CUtensorMap tm_v,
+                          const AdjStrArgs a, const TmaTiles t, int fv) {
+    using namespace adjt;
+    using L = Boxes<NM>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ unsigned long long limit;
+    float *sm = aligned128(smraw);
+    const Geo g = a.g;
+    const Tile T = tile_of<1>(t, BI, BJ);
+    const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+    const bool with_r = tile_has_interior(T, BI, BJ, a.ibk, a.iek, a.jbk, a.jek, a.kek);
+    if (tx == 0 && ty == 0 && tz == 0) {
+        // the copies go out first; the error word is read while they travel
+        stage_init(&bar, L::bytes(with_r, GRAD));
+        const int x0 = T.k0 - 1 + KH;
+        load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
+        load_4d(sm + L::oState, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state, &bar);
+        if (GRAD) load_4d(sm + L::oV, &tm_v, x0 - 4, T.i0, T.j0, fv, &bar);
+        limit = wait_limit(t.err);
+    }
+    const int k = T.k0 + tx, i = T.i0 + ty, j = T.j0 + tz;
+    const bool mine = k <= g.nz && i <= g.nx && j <= g.ny;
+    const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const int sgn = (mine && interior) ? band_sign(__ldg(&a.band[col]), k) : 0;
+    const Gm5 g0 = (GRAD && mine && interior) ? gm_load(a, e) : Gm5{};
+    __syncthreads();   // barrier initialised, wait limit set
+    if (!wait_tiles(&bar, t.err, limit) || !mine) return;   // the copy failed, or no cell here
+    const SOps<NM> o{sm, tx, ty, tz};
+    if (interior) adj_stress_interior<NM>(a, o, sgn, e, g0);
+    else adj_stress_absorber(a, o, col, k, i, j, e);
 }
 
 // lambda_V += D_V^T weights (dst = lV: x y z)
@@ -459,13 +621,20 @@ static int adj_alloc(swpc_ctx *c) {
     auto *s = new swpc_adj_state();
     c->adj = s;
     const long long n = c->g.ncell;
-    for (int q = 0; q < 3; q++) { int rc = dalloc(c, &s->lV[q], n); if (rc) return rc; }
-    for (int q = 0; q < 6; q++) { int rc = dalloc(c, &s->lS[q], n); if (rc) return rc; }
+    // adjoint state slab: 0-2 lV, 3-8 lS, 9.. lR (component-major), as the forward slab
+    s->slab_nf = 9 + 6 * c->d.nm;
+    {
+        int rc = dalloc(c, &s->slab, (size_t)s->slab_nf * n);
+        if (rc) return rc;
+    }
+    for (int q = 0; q < 3; q++) s->lV[q] = s->slab + (size_t)q * n;
+    for (int q = 0; q < 6; q++) s->lS[q] = s->slab + (size_t)(3 + q) * n;
     for (int comp = 0; comp < 6; comp++)
-        for (int m = 0; m < c->d.nm; m++) {
-            int rc = dalloc(c, &s->lR[comp * 3 + m], n);
-            if (rc) return rc;
-        }
+        for (int m = 0; m < c->d.nm; m++) s->lR[comp * 3 + m] = s->slab + (size_t)(9 + comp * c->d.nm + m) * n;
+    s->maps = new TmaMaps();
+    const TmaSlabs sl{s->slab, s->slab_nf, c->slab, c->slab_nf, nullptr, 0};
+    if (!tma_encode_stress(*s->maps, sl, c->g, c->d.nm, adjt::BI, adjt::BJ))
+        return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint slab");
     if (c->npml > 0)
         for (int q = 0; q < 18; q++) { int rc = dalloc(c, &s->laux[q], c->npml); if (rc) return rc; }
     for (int q = 0; q < 9; q++) {
@@ -481,9 +650,8 @@ namespace swpc {
 void adj_free(swpc_ctx *c) {
     swpc_adj_state *s = c->adj;
     if (!s) return;
-    for (auto p : s->lV) if (p) cudaFree(p);
-    for (auto p : s->lS) if (p) cudaFree(p);
-    for (auto p : s->lR) if (p) cudaFree(p);
+    if (s->slab) cudaFree(s->slab);   // lV, lS, lR
+    delete s->maps;
     for (auto p : s->laux) if (p) cudaFree(p);
     for (auto p : s->w40) if (p) cudaFree(p);
     for (auto p : s->w41) if (p) cudaFree(p);
@@ -506,8 +674,37 @@ static int adj_ready(swpc_ctx *c) {
     return adj_alloc(c);
 }
 
-// one transposed step: vel^T then stress^T; with gradient when S_after / V_before are given
-static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const *V_before) {
+// staged stress-phase weights over the whole grid; fv: field of the forward V
+// in the slots buffer (gradient), or -1
+template <int NM>
+static cudaError_t adj_stress_tma(const swpc_adj_state *s, const AdjStrArgs &a, const TmaTiles &t, int fv,
+                                  cudaStream_t st) {
+    constexpr int bytes = adjt::Boxes<NM>::total * 4 + 128;
+    static unsigned long long devices = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(devices >> dev & 1ull)) {
+        cudaError_t e0 = cudaFuncSetAttribute(adj_stress_tma_kernel<NM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e0 == cudaSuccess)
+            e0 = cudaFuncSetAttribute(adj_stress_tma_kernel<NM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e0 != cudaSuccess) return e0;
+        devices |= 1ull << dev;
+    }
+    const TmaMaps &m = *s->maps;
+    auto map = [](const unsigned char *p) -> const CUtensorMap & { return *reinterpret_cast<const CUtensorMap *>(p); };
+    const unsigned nblk = (unsigned)((long long)t.nkt * t.nit * t.njt);
+    const dim3 block(tma::KT, adjt::BI, adjt::BJ);
+    if (fv >= 0)
+        adj_stress_tma_kernel<NM, true><<<nblk, block, bytes, st>>>(map(m.state), map(m.s6), map(m.med), map(m.vh), a, t, fv);
+    else
+        adj_stress_tma_kernel<NM, false><<<nblk, block, bytes, st>>>(map(m.state), map(m.s6), map(m.med), map(m.vh), a, t, 0);
+    return cudaGetLastError();
+}
+
+// one transposed step: vel^T then stress^T; with gradient when S_after /
+// V_before are given (for the staged stress-phase weights, V_before is field
+// fv of the slots buffer)
+static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const *V_before, int fv) {
     swpc_adj_state *s = c->adj;
     const dim3 block(kThreadsK, 2, 2);
     const dim3 grid = cell_grid(c->g, block);
@@ -527,6 +724,8 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
             for (int q = 0; q < 6; q++) a.S[q] = S_after[q];
             for (int q = 0; q < 3; q++) a.gb[q] = s->grad[5 + q];
         }
+        // one cell per thread: the kernel is bound by its 18 weight stores, and
+        // staging its few loads (a TMA-staged form was tried) made it slower
         adj_vel_weights_kernel<<<grid, block, 0, c->stream>>>(a);
         ACK(cudaGetLastError());
         GatherArgs ga;
@@ -556,13 +755,24 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
             for (int q = 0; q < 3; q++) a.V[q] = V_before[q];
             for (int q = 0; q < 5; q++) a.gm[q] = s->grad[q];
         }
-        switch (c->d.nm) {
-        case 0: adj_stress_weights_kernel<0><<<grid, block, 0, c->stream>>>(a); break;
-        case 1: adj_stress_weights_kernel<1><<<grid, block, 0, c->stream>>>(a); break;
-        case 2: adj_stress_weights_kernel<2><<<grid, block, 0, c->stream>>>(a); break;
-        default: adj_stress_weights_kernel<3><<<grid, block, 0, c->stream>>>(a); break;
+        if (c->adj_tma && (!grad || fv >= 0)) {
+            const TmaTiles t = tma_tiles(c, adjt::BI, adjt::BJ, 1, 1, kStressFields(c));
+            const int f = grad ? fv : -1;
+            switch (c->d.nm) {
+            case 0: ACK(adj_stress_tma<0>(s, a, t, f, c->stream)); break;
+            case 1: ACK(adj_stress_tma<1>(s, a, t, f, c->stream)); break;
+            case 2: ACK(adj_stress_tma<2>(s, a, t, f, c->stream)); break;
+            default: ACK(adj_stress_tma<3>(s, a, t, f, c->stream)); break;
+            }
+        } else {
+            switch (c->d.nm) {
+            case 0: adj_stress_weights_kernel<0><<<grid, block, 0, c->stream>>>(a); break;
+            case 1: adj_stress_weights_kernel<1><<<grid, block, 0, c->stream>>>(a); break;
+            case 2: adj_stress_weights_kernel<2><<<grid, block, 0, c->stream>>>(a); break;
+            default: adj_stress_weights_kernel<3><<<grid, block, 0, c->stream>>>(a); break;
+            }
+            ACK(cudaGetLastError());
         }
-        ACK(cudaGetLastError());
         GatherArgs ga;
         ga.g = c->g;
         for (int q = 0; q < 3; q++) ga.dst[q] = s->lV[q];
@@ -623,7 +833,7 @@ extern "C" int swpc_adj_reset(swpc_ctx *c) {
 extern "C" int swpc_adj_step_linear(swpc_ctx *c) {
     int rc = adj_ready(c);
     if (rc) return rc;
-    rc = adj_step(c, nullptr, nullptr);
+    rc = adj_step(c, nullptr, nullptr, -1);
     if (rc) return rc;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
@@ -724,6 +934,9 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             cudaMalloc((void **)&s->slots, need_slots * sizeof(float)) != cudaSuccess)
             return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints (raise ckpt or shrink the grid)");
         s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf;
+        // the staged stress-phase weights read the forward V of a slot with its halo
+        if (!tma_encode_box(s->maps->vh, s->slots, c->g, 9LL * (ckpt + 1), tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
+            return err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the recompute slots");
     }
     const size_t nres = (size_t)c->nst * 3 * c->ntw;
     if (!s->res) ACK(cudaMalloc((void **)&s->res, nres * sizeof(float)));
@@ -766,7 +979,7 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             const float *Sa[6], *Vb[3];
             for (int q = 0; q < 6; q++) Sa[q] = base_a + (3 + q) * n;
             for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
-            rc = adj_step(c, Sa, Vb);
+            rc = adj_step(c, Sa, Vb, (it - it0) * 9);
             if (!rc) rc = adj_source(c, it);
         }
         if (rc) return rc;

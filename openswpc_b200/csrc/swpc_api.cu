@@ -253,6 +253,12 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
         else { c->vel_tma = true; c->vel_tbi = bi; }
         return SWPC_OK;
     }
+    if (kernel == 8) {
+        // adjoint stress-phase weights: bi = 1 staged, 0 one cell per thread
+        if (!is3d(c) || (bi != 0 && bi != 1)) return set_err(c, SWPC_ERR_ARG, "kernel 8 (3D): bi = 0 or 1");
+        c->adj_tma = bi == 1;
+        return SWPC_OK;
+    }
     if (kernel == 7) {
         // launch order of the staged kernels: blocks of bi j tiles (0: chosen by size)
         if (bi < 0 || bi > 1024) return set_err(c, SWPC_ERR_ARG, "kernel 7: bi = j tiles per block, 0..1024");

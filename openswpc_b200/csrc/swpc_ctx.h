@@ -163,6 +163,7 @@ struct swpc_ctx {
     // (swpc2d_tma.cu): tiles 32 x 16 with stress_tbi / vel_tbi threads along i
     bool stress_tma = false, vel_tma = false;
     int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 4;
+    bool adj_tma = true;          // staged stress-phase adjoint weights (swpc_adjoint.cu)
     int tile_jblock = 0;          // j tiles per block of the staged launch order (0: by size, see tma_tiles)
     void *tmaps = nullptr;        // swpc::TmaMaps
     int tma_key[4] = {-1, -1, -1, -1};

@@ -37,7 +37,6 @@ namespace swpc {
 int stime_table(swpc_ctx *c, float **dst, int nsrc, const float *srcprm, int stftype, bool half);
 bool green_entries(const swpc_ctx *c, int isrc, int jsrc, int ksrc, char cmp, std::vector<InjEntry> &v);
 int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i);
-TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields);
 }  // namespace swpc
 
 using namespace swpc;
@@ -561,7 +560,7 @@ extern "C" int swpc_fbatch_autotune(swpc_fbatch *b, int it0, int reps, int *step
             FRC(swpc_fbatch_set_launch(b, 7, best, 0, 0));
         }
         const int sc[][3] = {{4, 2, 2}, {4, 4, 1}, {2, 4, 2}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
-        const int vc[][3] = {{4, 2, 2}, {4, 2, 1}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
+        const int vc[][3] = {{4, 2, 2}, {4, 4, 1}, {4, 2, 1}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
         for (int kernel = 5; kernel <= 6; kernel++) {
             const int(*cand)[3] = kernel == 5 ? sc : vc;
             int best = 0;

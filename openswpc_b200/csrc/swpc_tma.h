@@ -25,6 +25,11 @@ struct TmaTiles {
     int *err;            // raised when a tile copy does not complete
 };
 
+// tiles of a staged launch over a context's grid for nmem members grouped
+// by mpc; nfields = the fields the kernel reads over its tile per member
+// (chooses the launch order); the field indices follow the context's slab
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields);
+
 // fields a staged stress / velocity update reads over its tile (member state
 // and medium): S, R, V, lam mu taup taus muyz muxz muxy, bx by bz / V, S, bx by bz
 inline int kStressFields(const swpc_ctx *c) { return 16 + 6 * c->d.nm; }
@@ -59,6 +64,9 @@ struct alignas(64) TmaMaps {
 bool tma_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec = 0);
+// one FP32 map (k, i, j, field) over a slab of nf fields with box (bk, bi, bj, bf)
+bool tma_encode_box(unsigned char *out, float *slab, const Geo &g, long long nf, unsigned bk, unsigned bi, unsigned bj,
+                    unsigned bf);
 bool tma_encode_vel(TmaMaps &m, const TmaSlabs &s, const Geo &g, int bi, int bj, int prec = 0);
 cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, int nm, int bi, int bj, int mpc,
                                 cudaStream_t st, int prec = 0);

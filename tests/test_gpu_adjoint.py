@@ -43,12 +43,16 @@ def fields(p):
     return out
 
 
+@pytest.mark.parametrize("staged", [1, 0])
 @pytest.mark.parametrize("nm", [3, 1])
-def test_adjoint_dot_product(nm):
+def test_adjoint_dot_product(nm, staged):
+    """staged: the TMA-staged stress-phase weights (1, the default) or the
+    one-cell-per-thread kernel (0)."""
     p = small3d(nx=36, ny=30, nz=28, na=6, nt=10, nm=nm)
     xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
     g = Swpc3D(p, xi)
     lib, ctx = g.lib, g.ctx
+    check(ctx, lib.swpc_set_launch(ctx, 8, 1, staged, 1))
     rng = np.random.default_rng(42)
     dom, ker = domain_mask(p), kernel_mask(p)
     shape = dom.shape
@@ -98,6 +102,41 @@ def misfit_case():
     obs = true.waveforms(_lib.WAV_V)
     true.close()
     return p, xi, obs
+
+
+def test_staged_adjoint_weights_give_the_bits_of_the_one_cell_kernel():
+    """The gradient (misfit, the eight medium gradients, the final adjoint
+    state) with the staged stress-phase weights equals, bit for bit, the
+    gradient with the one-cell-per-thread kernel."""
+    p, xi, obs = misfit_case()
+    obsf = np.ascontiguousarray(obs, np.float32)
+    shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+    runs = []
+    for staged in (1, 0):
+        g = Swpc3D(p, xi)
+        check(g.ctx, g.lib.swpc_set_launch(g.ctx, 8, 1, staged, 1))
+        J = C.c_double()
+        check(g.ctx, g.lib.swpc_gradient(g.ctx, fptr(obsf), 16, C.byref(J)))
+        grads = []
+        for w in range(8):
+            out = np.zeros(shape, np.float64)
+            check(g.ctx, g.lib.swpc_gradient_fetch(g.ctx, w, out.ctypes.data_as(C.POINTER(C.c_double)), p.nz + 6,
+                                                   p.nx + 6))
+            grads.append(out)
+        adj = []
+        for fid, _ in fields(p):
+            b = np.zeros(shape, np.float32)
+            check(g.ctx, g.lib.swpc_adj_download(g.ctx, fid, fptr(b), p.nz + 6, p.nx + 6))
+            adj.append(b)
+        runs.append((J.value, grads, adj))
+        g.close()
+    (J1, g1, a1), (J0, g0, a0) = runs
+    assert J1 == J0
+    assert any(np.abs(x).max() > 0 for x in g1)
+    for w, (x, y) in enumerate(zip(g1, g0)):
+        assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), w
+    for (fid, _), x, y in zip(fields(p), a1, a0):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), fid
 
 
 def forward_misfit(g, p, obs):
