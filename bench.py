@@ -56,7 +56,7 @@ FALLBACK_HBM_GBS = 6650.0
 # algorithmic bytes, for the default (TMA-staged) kernels (the ncu summaries of stress3d_tma_kernel and
 # vel3d_tma_kernel on that grid, under profiles/)
 TRAFFIC_PER_ALGORITHMIC = {"stress": (1.261579e9 + 0.708133e9) / 1.828028416e9,
-                           "vel": (0.511189e9 + 0.124598e9) / 0.609632256e9}
+                           "vel": (0.510744e9 + 0.124089e9) / 0.609632256e9}
 
 
 def make_params(name: str):
