@@ -415,8 +415,9 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * per tile of 32 (k) x bi (i) x bj (j) cells whose operands arrive in shared
  * memory by bulk tensor copies; minb must be 1, and the compiled tiles
  * (bi, bj) are stress (4,4) (2,4) (4,2), velocity (4,4) (4,2) (2,2); the
- * reduced storage forms (BF16_R, F16_SR) compile stress (4,4) and velocity
- * (4,4).  3D contexts start with kernels 5 (4,4) and 6 (4,4).
+ * reduced storage forms (BF16_R, F16_SR) compile (4,4) and (4,2) for both.
+ * 3D contexts start with kernels 5 (4,4) and 6 (4,4); the reduced storage
+ * forms with kernel 5 on (4,2).
  * kernel 7 (3D) sets the launch order of the staged kernels: tiles run k
  * fastest, then over (i, j) in blocks of bi consecutive j tiles (j fastest
  * within a block), so that a tile's j-halo is still in L2; bi = 1 runs i then

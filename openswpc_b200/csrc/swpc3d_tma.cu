@@ -378,22 +378,22 @@ cudaError_t stress_nm(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, in
     }
 }
 
-// compiled (bi, bj, members per CTA); the reduced storage forms run the first
-// (default) shape of each list with one member
+// compiled (bi, bj, members per CTA); the reduced storage forms run (4, 4) and
+// (4, 2) with one member
 constexpr int kStressShapes[][3] = {{4, 4, 1}, {2, 4, 1}, {4, 2, 1}, {4, 2, 2}, {2, 4, 2}, {2, 2, 2}, {2, 2, 4}, {4, 1, 4}};
 constexpr int kVelShapes[][3] = {{4, 4, 1}, {4, 2, 1}, {2, 2, 1}, {4, 2, 2}, {2, 2, 2}, {4, 1, 2}, {2, 2, 4}, {4, 1, 4}};
 
 }  // namespace
 
 bool tma_shape_ok(int bi, int bj, int mpc, int prec) {
-    if (prec != PREC_F32) return bi == kStressShapes[0][0] && bj == kStressShapes[0][1] && mpc == 1;
+    if (prec != PREC_F32) return bi == 4 && (bj == 4 || bj == 2) && mpc == 1;
     for (auto &v : kStressShapes)
         if (v[0] == bi && v[1] == bj && v[2] == mpc) return true;
     return false;
 }
 
 bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec) {
-    if (prec != PREC_F32) return bi == kVelShapes[0][0] && bj == kVelShapes[0][1] && mpc == 1;
+    if (prec != PREC_F32) return bi == 4 && (bj == 4 || bj == 2) && mpc == 1;
     for (auto &v : kVelShapes)
         if (v[0] == bi && v[1] == bj && v[2] == mpc) return true;
     return false;
@@ -401,8 +401,10 @@ bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec) {
 
 cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTiles &t, int nm, int bi, int bj, int mpc,
                                 cudaStream_t st, int prec) {
-    if (prec == PREC_BF16_R) return stress_nm<4, 4, 1, PREC_BF16_R>(m, a, t, nm, st);
-    if (prec == PREC_F16_SR) return stress_nm<4, 4, 1, PREC_F16_SR>(m, a, t, nm, st);
+    if (prec == PREC_BF16_R)
+        return bj == 2 ? stress_nm<4, 2, 1, PREC_BF16_R>(m, a, t, nm, st) : stress_nm<4, 4, 1, PREC_BF16_R>(m, a, t, nm, st);
+    if (prec == PREC_F16_SR)
+        return bj == 2 ? stress_nm<4, 2, 1, PREC_F16_SR>(m, a, t, nm, st) : stress_nm<4, 4, 1, PREC_F16_SR>(m, a, t, nm, st);
     if (mpc == 4) {
         if (bi == 4 && bj == 1) return stress_nm<4, 1, 4>(m, a, t, nm, st);
         return stress_nm<2, 2, 4>(m, a, t, nm, st);
@@ -420,7 +422,8 @@ cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTi
 cudaError_t launch_vel3d_tma(const TmaMaps &m, const Vel3Args &a, const TmaTiles &t, int bi, int bj, int mpc,
                              cudaStream_t st, int prec) {
     // BF16_R keeps S in FP32: its velocity update is the FP32 one
-    if (prec == PREC_F16_SR) return run_vel<4, 4, 1, PREC_F16_SR>(m, a, t, st);
+    if (prec == PREC_F16_SR)
+        return bj == 2 ? run_vel<4, 2, 1, PREC_F16_SR>(m, a, t, st) : run_vel<4, 4, 1, PREC_F16_SR>(m, a, t, st);
     if (mpc == 4) {
         if (bi == 4 && bj == 1) return run_vel<4, 1, 4, PREC_F32>(m, a, t, st);
         return run_vel<2, 2, 4, PREC_F32>(m, a, t, st);

@@ -756,7 +756,7 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
             for (int q = 0; q < 5; q++) a.gm[q] = s->grad[q];
         }
         if (c->adj_tma && (!grad || fv >= 0)) {
-            const TmaTiles t = tma_tiles(c, adjt::BI, adjt::BJ, 1, 1, kStressFields(c));
+            const TmaTiles t = tma_tiles(c, adjt::BI, adjt::BJ, 1, 1, kStressFields(c), 1);
             const int f = grad ? fv : -1;
             switch (c->d.nm) {
             case 0: ACK(adj_stress_tma<0>(s, a, t, f, c->stream)); break;

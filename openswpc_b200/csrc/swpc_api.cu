@@ -173,9 +173,12 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
             for (int q = 0; q < 3; q++) c->med[5 + q] = F(mb + 7 + q);
             c->slab_nf = nf;
             c->hslab_nf = nh;
-            // the staged kernels are the default launch
+            // the staged kernels are the default launch; the 2-byte forms move
+            // fewer bytes a tile, and their stress update runs faster on 4 x 2
+            // tiles (more CTAs, hence more tiles in flight, per SM)
             c->stress_tma = true;
             c->vel_tma = true;
+            c->stress_tbj = 2;
         }
         const long long ncol = (long long)g.Ip * g.Jp;
         if (!rc) rc = dalloc(c, &c->band, ncol);
@@ -807,7 +810,7 @@ static int tma_ready(swpc_ctx *c) {
 namespace swpc {
 // tiles of a staged launch over the whole grid for nmem members grouped by
 // mpc; the medium fields come from the context's slab
-TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields) {
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields, int live) {
     TmaTiles t;
     t.nkt = (c->g.nz + 31) / 32;
     t.nit = (c->g.nx + bi - 1) / bi;
@@ -816,8 +819,9 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfi
     t.mgroups = (nmem + mpc - 1) / mpc;
     t.tiles_first = 0;
     // launch order: blocks of j tiles once a j plane of tiles (the fields the
-    // kernel reads over bj planes, every member) outgrows half of the L2
-    const double plane = (double)nfields * nmem * c->g.Kp * c->g.Ip * bj * 4.0;
+    // kernel reads over bj planes, for the members whose tiles interleave in
+    // the launch order) outgrows half of the L2
+    const double plane = (double)nfields * live * c->g.Kp * c->g.Ip * bj * 4.0;
     const int jb = c->tile_jblock > 0 ? c->tile_jblock : (plane > 64e6 ? 16 : 1);
     t.jblock = std::max(1, std::min(jb, t.njt));
     // slab field order: FP32 V S R medium b; BF16_R V S medium b (R in the
@@ -860,7 +864,7 @@ static int launch_stress(swpc_ctx *c, int mask) {
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
     if (c->stress_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1, kStressFields(c));
+        const TmaTiles t = tma_tiles(c, c->stress_tbi, c->stress_tbj, 1, 1, kStressFields(c), 1);
         return cuda_check(c, launch_stress3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->d.nm, c->stress_tbi,
                                                  c->stress_tbj, 1, c->stream, c->prec), "stress3d_tma launch");
     }
@@ -890,7 +894,7 @@ static int launch_vel(swpc_ctx *c, int mask) {
     for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
     if (c->vel_tma && c->slab) {
         RC(tma_ready(c));
-        const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1, kVelFields);
+        const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1, kVelFields, 1);
         return cuda_check(c, launch_vel3d_tma(*static_cast<TmaMaps *>(c->tmaps), a, t, c->vel_tbi, c->vel_tbj, 1,
                                               c->stream, c->prec), "vel3d_tma launch");
     }

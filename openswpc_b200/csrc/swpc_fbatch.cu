@@ -365,7 +365,8 @@ static int fb_tma_ready(swpc_fbatch *b) {
 }
 
 static TmaTiles fb_tiles(const swpc_fbatch *b, int bi, int bj, int mpc, int nfields) {
-    TmaTiles t = tma_tiles(b->c, bi, bj, b->nmem, mpc, nfields);
+    // tiles fastest: one member group's tiles run at a time; else all groups of a tile
+    TmaTiles t = tma_tiles(b->c, bi, bj, b->nmem, mpc, nfields, b->tiles_first ? mpc : b->nmem);
     t.f_member = b->nfs;
     t.so = b->stride;
     t.ao = b->astride;

@@ -26,9 +26,10 @@ struct TmaTiles {
 };
 
 // tiles of a staged launch over a context's grid for nmem members grouped
-// by mpc; nfields = the fields the kernel reads over its tile per member
-// (chooses the launch order); the field indices follow the context's slab
-TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields);
+// by mpc; nfields = the fields the kernel reads over its tile per member and
+// live = the members whose tiles interleave in the launch order (both choose
+// the j-block length); the field indices follow the context's slab
+TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfields, int live);
 
 // fields a staged stress / velocity update reads over its tile (member state
 // and medium): S, R, V, lam mu taup taus muyz muxz muxy, bx by bz / V, S, bx by bz
@@ -59,8 +60,7 @@ struct alignas(64) TmaMaps {
 // compiled tiles (bi, bj) and members per CTA: stress (4,4,1) (2,4,1) (4,2,1)
 // (4,2,2) (2,4,2) (2,2,2) (2,2,4) (4,1,4); velocity (4,4,1) (4,2,1) (2,2,1)
 // (4,2,2) (2,2,2) (4,1,2) (2,2,4) (4,1,4).  The reduced storage forms (prec
-// PREC_BF16_R / PREC_F16_SR of swpc3d_cell.cuh) run stress (4,4,1) and
-// velocity (4,4,1).
+// PREC_BF16_R / PREC_F16_SR of swpc3d_cell.cuh) run (4,4,1) and (4,2,1).
 bool tma_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_vel_shape_ok(int bi, int bj, int mpc, int prec = 0);
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec = 0);

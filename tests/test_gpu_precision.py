@@ -112,3 +112,25 @@ def test_staged_reduced_forms_equal_the_flat_kernels(form, nm, grid):
     for fid in fields:
         a, b = staged.download(fid), flat.download(fid)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), fid
+
+
+@pytest.mark.parametrize("form", ["bf16r", "f16sr"])
+def test_reduced_forms_on_every_compiled_staged_tile(form):
+    """The reduced forms compile stress and velocity tiles (4, 4) and (4, 2):
+    each combination gives the bits of the flat kernels."""
+    p = small3d(nx=42, ny=38, nz=45, nt=30, nm=3, sw_wav_stress=True)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    flat = Swpc3D(p, xi, precision=form)
+    _lib.check(flat.ctx, flat.lib.swpc_set_launch(flat.ctx, 0, 2, 2, 1))
+    _lib.check(flat.ctx, flat.lib.swpc_set_launch(flat.ctx, 1, 4, 2, 2))
+    flat.run(1, p.nt)
+    ref = [flat.download(fid) for fid in range(9)]
+    for sbj, vbj in ((4, 2), (2, 4), (4, 4), (2, 2)):
+        g = Swpc3D(p, xi, precision=form)
+        _lib.check(g.ctx, g.lib.swpc_set_launch(g.ctx, 5, 1, 4, sbj))
+        _lib.check(g.ctx, g.lib.swpc_set_launch(g.ctx, 6, 1, 4, vbj))
+        g.run(1, p.nt)
+        for fid in range(9):
+            a = g.download(fid)
+            assert np.array_equal(a.view(np.uint32), ref[fid].view(np.uint32)), (sbj, vbj, fid)
+        g.close()
