@@ -7,7 +7,8 @@
  * argument-less Fortran module procedures acting on module-global arrays;
  * here every routine takes an opaque context that owns the device copies of
  * those arrays.  A Fortran caller keeps one `type(c_ptr)` per run and binds
- * each entry point with ISO_C_BINDING.
+ * each entry point with ISO_C_BINDING: one interface block per function,
+ * bind(C) with the C name, scalars by value, arrays by reference.
  *
  * Conventions
  *   - every function returns an int status: 0 = OK, otherwise an
