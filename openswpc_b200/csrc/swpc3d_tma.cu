@@ -21,16 +21,22 @@
 // copies S without R.  The tensor boxes may reach past the grid at
 // its edges: TMA fills those elements with zeros and they are never used.
 //
+// The lead thread issues the copies first and only then reads the launch's
+// error word, while the copies travel; the other threads meanwhile read the
+// band signs and the absorber auxiliaries of their cells.  The tile wait is
+// bounded (swpc_tma_ptx.cuh).
+//
 // A CTA serves M members that share the medium (M = 1 for a single run; the
 // reciprocity batch, swpc_fbatch.cu, groups its members): the medium box is
 // copied once and each member's boxes follow, so the medium crosses HBM once
-// per M member updates.  Consecutive CTAs take consecutive member groups of
-// the same tile.
+// per M member updates.  The launch order of tiles and member groups is
+// tile_of's (swpc_tma_tile.cuh).
 //
 // Field order of the state slab (per member): 0-2 V, 3-8 S, 9.. R
 // (component-major, nm per component).  Medium slab: lam mu taup taus muyz
 // muxz muxy, then bx by bz, from field f_med (the context's slab holds both,
-// see swpc_create).
+// see swpc_create).  The reduced storage forms keep S (F16_SR) and R in a
+// second slab of 2-byte fields (template parameter PREC).
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
