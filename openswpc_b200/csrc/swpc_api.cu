@@ -217,6 +217,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
         for (auto &p : c->med) p = nullptr;
     }
     if (c->d_err) cudaFree(c->d_err);
+    if (c->stage) cudaFree(c->stage);
     delete static_cast<TmaMaps *>(c->tmaps);
     void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
                   c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
@@ -316,26 +317,63 @@ namespace swpc {
 
 // host (k, i, j) Fortran array over k in [-2, nz+3+], i in [-2, nx+3+], j in
 // [-2, ny+3+] with leading extents ld_k, ld_i  <->  device column layout.
+// chunk of nj planes of the host box (rows of ld_k k values, ld_i rows a
+// plane) in the staging buffer -> the device columns of planes j0 ..
+__global__ void repack_box_kernel(const float *__restrict__ stage, float *__restrict__ dev, int nkb, int nib, int nj,
+                                  int ld_k, int ld_i, int Kp, int Ip, int j0, int koff) {
+    const long long n = (long long)nkb * nib * nj;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int kk = (int)(q % nkb);
+        const long long r = q / nkb;
+        const int ii = (int)(r % nib), jj = (int)(r / nib);
+        dev[((long long)(j0 + jj) * Ip + ii) * Kp + koff + kk] = stage[((long long)jj * ld_i + ii) * ld_k + kk];
+    }
+}
+
 int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i) {
     const Geo &g = c->g;
     const int nkb = g.nz + 6;             // k = -2 .. nz+3
     const int nib = g.nx + 6;             // i = -2 .. nx+3
     const int njb = is3d(c) ? g.ny + 6 : 1;
     if (ld_k < nkb || ld_i < nib) return set_err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
-    const size_t dpitch = (size_t)g.Kp * sizeof(float);
-    const size_t hpitch = (size_t)ld_k * sizeof(float);
-    const size_t width = (size_t)nkb * sizeof(float);
     const int koff = -2 - 1 + KH;         // device offset of k = -2 within a column
-    for (int jj = 0; jj < njb; jj++) {
-        float *dcol = dev + ((long long)jj * g.Ip) * g.Kp + koff;
-        const long long hoff = (long long)jj * ld_i * ld_k;
-        cudaError_t e;
-        if (host_in)
-            e = cudaMemcpy2DAsync(dcol, dpitch, host_in + hoff, hpitch, width, nib, cudaMemcpyHostToDevice, c->stream);
-        else
-            e = cudaMemcpy2DAsync(host_out + hoff, hpitch, dcol, dpitch, width, nib, cudaMemcpyDeviceToHost, c->stream);
-        if (e != cudaSuccess) return cuda_check(c, e, "cudaMemcpy2DAsync");
+    const long long plane = (long long)ld_i * ld_k;   // floats of a host plane
+    if (host_in && plane * njb >= (1LL << 22)) {
+        // a large upload: contiguous chunks of host planes at full link speed
+        // into a staging buffer, each repacked into the device columns on the
+        // device (the strided copy of 2 KB rows is several times slower)
+        const int nj = (int)std::max<long long>(1, std::min<long long>(njb, (16LL << 20) / plane));
+        if (c->stage_floats < plane * nj) {
+            if (c->stage) cudaFree(c->stage);
+            c->stage = nullptr;
+            c->stage_floats = 0;
+            if (cudaMalloc((void **)&c->stage, plane * nj * sizeof(float)) != cudaSuccess)
+                return set_err(c, SWPC_ERR_NOMEM, "no room for the upload staging buffer");
+            c->stage_floats = plane * nj;
+        }
+        for (int j0 = 0; j0 < njb; j0 += nj) {
+            const int n = std::min(nj, njb - j0);
+            CK(cudaMemcpyAsync(c->stage, host_in + (long long)j0 * plane, (size_t)(plane * n) * sizeof(float),
+                               cudaMemcpyHostToDevice, c->stream));
+            repack_box_kernel<<<148 * 8, 256, 0, c->stream>>>(c->stage, dev, nkb, nib, n, ld_k, ld_i, g.Kp, g.Ip, j0,
+                                                             koff);
+            CK(cudaGetLastError());
+        }
+        return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     }
+    // one pitched 3D copy for the whole box: rows of nkb k values, nib rows
+    // (i) a plane, njb planes (j); the host box has row pitch ld_k and ld_i
+    // rows a plane, the device Kp and Ip
+    cudaMemcpy3DParms q = {};
+    const cudaPitchedPtr hp = make_cudaPitchedPtr(const_cast<float *>(host_in ? host_in : host_out),
+                                                  (size_t)ld_k * sizeof(float), (size_t)nkb, (size_t)ld_i);
+    const cudaPitchedPtr dp = make_cudaPitchedPtr(dev + koff, (size_t)g.Kp * sizeof(float), (size_t)nkb, (size_t)g.Ip);
+    q.srcPtr = host_in ? hp : dp;
+    q.dstPtr = host_in ? dp : hp;
+    q.extent = make_cudaExtent((size_t)nkb * sizeof(float), (size_t)nib, (size_t)njb);
+    q.kind = host_in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    const cudaError_t e = cudaMemcpy3DAsync(&q, c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cudaMemcpy3DAsync");
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
 

@@ -174,6 +174,8 @@ struct swpc_ctx {
     // then lam mu taup taus muyz muxz muxy and bx by bz; 2D: V, S, R, then
     // lam taup taus mu rho
     float *slab = nullptr;
+    float *stage = nullptr;       // staging buffer of host uploads (copy_box), allocated on first use
+    long long stage_floats = 0;
     int slab_nf = 0;
     // reduced-precision 3D storage: the 2-byte fields (S for F16_SR, then R
     // component-major) in a second slab of ncell-element fields

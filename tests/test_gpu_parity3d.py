@@ -251,6 +251,26 @@ def test_vmax_and_divergence_detection():
     assert e.value.code == _lib.SWPC_ERR_DIVERGED
 
 
+def test_large_box_uploads_through_the_staging_buffer():
+    """Boxes of 2^22 floats and more travel to the device in contiguous
+    chunks of planes through a staging buffer and are repacked there (174
+    planes: a full chunk and a short one).  The medium upload of the run and
+    a field upload both take that path: the run matches the oracle bitwise,
+    and a random field comes back unchanged."""
+    p = small3d(nx=168, ny=168, nz=140, na=10, nt=4)
+    assert (p.nx + 6) * (p.ny + 6) * (p.nz + 6) >= 1 << 22
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    g = Swpc3D(p, xi)
+    o = Oracle3D(p, xi, threads=8)
+    for it in range(1, p.nt + 1):
+        g.step(it)
+        o.step(it)
+    compare_state(g, o, p, what="v")
+    x = np.random.default_rng(8).standard_normal((p.ny + 6, p.nx + 6, p.nz + 6)).astype(np.float32)
+    g.upload(_lib.F_VY, x)
+    assert same_bits(g.download(_lib.F_VY), x)
+
+
 def test_larger_grid_against_oracle_few_steps():
     """A grid whose planes exceed one warp row in every direction (k spans
     several 32-cell chunks, absorber/interior boundaries fall mid-warp)."""
