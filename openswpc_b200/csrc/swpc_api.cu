@@ -338,10 +338,11 @@ int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int
     if (ld_k < nkb || ld_i < nib) return set_err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
     const int koff = -2 - 1 + KH;         // device offset of k = -2 within a column
     const long long plane = (long long)ld_i * ld_k;   // floats of a host plane
-    if (host_in && plane * njb >= (1LL << 22)) {
-        // a large upload: contiguous chunks of host planes at full link speed
-        // into a staging buffer, each repacked into the device columns on the
-        // device (the strided copy of 2 KB rows is several times slower)
+    if (host_in && plane * njb >= (1LL << 16)) {
+        // an upload of 256 KB or more: contiguous chunks of host planes at full
+        // link speed into a staging buffer (at most 16 MB), each repacked into
+        // the device columns on the device (the strided copy of short rows is
+        // several times slower)
         const int nj = (int)std::max<long long>(1, std::min<long long>(njb, (16LL << 20) / plane));
         if (c->stage_floats < plane * nj) {
             if (c->stage) cudaFree(c->stage);

@@ -252,9 +252,9 @@ def test_vmax_and_divergence_detection():
 
 
 def test_large_box_uploads_through_the_staging_buffer():
-    """Boxes of 2^22 floats and more travel to the device in contiguous
-    chunks of planes through a staging buffer and are repacked there (174
-    planes: a full chunk and a short one).  The medium upload of the run and
+    """Boxes of 2^16 floats and more travel to the device in contiguous
+    chunks of planes (16 MB) through a staging buffer and are repacked there
+    (174 planes here: a full chunk and a short one).  The medium upload of the run and
     a field upload both take that path: the run matches the oracle bitwise,
     and a random field comes back unchanged."""
     p = small3d(nx=168, ny=168, nz=140, na=10, nt=4)
