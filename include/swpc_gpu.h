@@ -387,7 +387,11 @@ int swpc_time_steps(swpc_ctx *ctx, int it0, int nsteps, float *ms);
 /* wav buffers in the reference layout wav_*(ntw, ncmp, nst) (m_wav.f90:37-38). */
 int swpc_wav_fetch(swpc_ctx *ctx, int what, float *out);
 int swpc_wav_dims(const swpc_ctx *ctx, int *ntw, int *nst);
-/* One field in the Fortran memory-box layout (ld_k, ld_i as above). */
+/* One field in the Fortran memory-box layout (ld_k, ld_i as above).  Uploads
+ * of a box of 256 KB or more (here and in swpc_upload_medium) travel in
+ * contiguous chunks of planes through a staging buffer of the context (about
+ * 16 MB, allocated by the first such upload and kept until swpc_destroy;
+ * counted by swpc_device_bytes); pinned host memory makes them fastest. */
 int swpc_download_field(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
 int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
 /* Memory-variable and PML-auxiliary fields are defined only on their

@@ -346,11 +346,13 @@ int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int
         const int nj = (int)std::max<long long>(1, std::min<long long>(njb, (16LL << 20) / plane));
         if (c->stage_floats < plane * nj) {
             if (c->stage) cudaFree(c->stage);
+            c->bytes -= c->stage_floats * (long long)sizeof(float);
             c->stage = nullptr;
             c->stage_floats = 0;
             if (cudaMalloc((void **)&c->stage, plane * nj * sizeof(float)) != cudaSuccess)
                 return set_err(c, SWPC_ERR_NOMEM, "no room for the upload staging buffer");
             c->stage_floats = plane * nj;
+            c->bytes += c->stage_floats * (long long)sizeof(float);
         }
         for (int j0 = 0; j0 < njb; j0 += nj) {
             const int n = std::min(nj, njb - j0);
