@@ -95,6 +95,9 @@ def make_params(name: str):
 # 2D P-SV algorithmic bytes per cell-update (FP32, nm = 3): velocity phase 2 V read+write, 3 S, rho; stress
 # phase 2 V, 3 S read+write, 9 R read+write, lam, mu, taup, taus (interior); PML: 34 floats
 B_PSV_INT, B_PSV_PML = 38 * 4, 34 * 4
+# DRAM traffic of the staged 2D kernels over their algorithmic bytes, measured by ncu on the first 16 c2A models
+# (stress 0.941 + 0.546 GB, velocity 0.328 + 0.087 GB against 1.481 + 0.430 GB; the 2D batch summary under profiles/)
+TRAFFIC_PER_ALGORITHMIC_2D = (0.941275 + 0.545625 + 0.328020 + 0.086632) / (1.4813472 + 0.429801472)
 # one adjoint step per cell (FP32 state, FP64 gradients, nm = 3), interior / absorber: velocity weights (lV, b
 # read, nine w40 + nine w41 written, S of the slot read, three b gradients read and written; absorber: nine PML
 # auxiliaries read and written instead of S and the gradients), velocity gather (18 weights read, six lS read and
@@ -274,7 +277,12 @@ def bench_c2a(args, world, rank, local):
             "autotune": {**pick, "steps_used": used},
             "roofline": {"bound": "hbm", "kernel": f"{kern} (whole batched step)",
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": bytes_step},
+                         "peak_kind": peak_kind,
+                         "traffic": bytes_step * TRAFFIC_PER_ALGORITHMIC_2D if pick["stress_ti"] and pick["vel_ti"]
+                         else None,
+                         "traffic_source": "ncu DRAM bytes of both staged kernels on the first 16 models, as a ratio "
+                                           "to their algorithmic bytes, times this step's algorithmic bytes",
+                         "algorithmic_bytes_per_step": bytes_step},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "what": "media upload from host memory + per-step batch calls + trace download, wall clock"},
