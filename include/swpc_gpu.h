@@ -73,6 +73,10 @@ extern "C" {
  * axVx ayVx azVx axVy ayVy azVy axVz ayVz azVz
  * axSxx aySxy azSxz axSxy aySyy azSyz axSxz aySyz azSzz */
 #define SWPC_F_AUX 40
+/* 3D medium arrays, swpc_download_field only: SWPC_F_MED + q, q = 1..10 in
+ * the field order of the medium view: lam mu taup taus bx by bz muyz muxz
+ * muxy (rho is not kept) */
+#define SWPC_F_MED 60
 
 /* wave-field recorder components (m_wav.f90:31-34) */
 #define SWPC_WAV_V 1
@@ -140,7 +144,10 @@ int swpc_sync(swpc_ctx *ctx);
 /* ---- setup ------------------------------------------------------------- */
 
 /* Copies the medium and maps to HBM (the `!$acc enter data copyin` of
- * main.f90:97-119). */
+ * main.f90:97-119).  3D: with rho given and bx, by, bz, muyz, muxz, muxy all
+ * NULL, the six averaged fields are formed in HBM from rho and mu as
+ * averaged_medium (m_medium.f90:432-465) forms them, bitwise equal to the
+ * fields of swpc_setup_medium; the host then sends 5 arrays instead of 10. */
 int swpc_upload_medium(swpc_ctx *ctx, const swpc_medium_view *m);
 
 /* kernel__setup (src/swpc_3d/m_kernel.f90:30-73): FD coefficients from dx,

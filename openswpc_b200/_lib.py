@@ -30,6 +30,7 @@ STF_CODES = {"kupper": 0, "boxcar": 1, "triangle": 2, "herrmann": 3, "cosine": 4
 F_VX, F_VY, F_VZ, F_SXX, F_SYY, F_SZZ, F_SYZ, F_SXZ, F_SXY = range(9)
 F_R = 10
 F_AUX = 40
+F_MED = 60
 WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 
 # every symbol the headers in include/ declare

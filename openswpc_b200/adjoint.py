@@ -51,7 +51,7 @@ class Misfit3D:
     def _set_model(self, vp, vs, rho) -> Medium:
         s = self.solver
         m = Medium.from_model(self.p, vp, vs, rho, self.qp, self.qs)
-        check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view())))
+        check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view(average_on_device=True))))
         s.medium = m
         return m
 

@@ -380,6 +380,54 @@ int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
 
+// 4 a b c d / (a b c + a b d + a c d + b c d + epsilon(1.0)), every product and
+// sum rounded left to right without contraction, as the host restatement of
+// averaged_medium (m_medium.f90:451-459) evaluates it
+__device__ __forceinline__ float harmonic4(float a, float b, float c, float d) {
+    const float num = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(4.0f, a), b), c), d);
+    float den = __fmul_rn(__fmul_rn(a, b), c);
+    den = __fadd_rn(den, __fmul_rn(__fmul_rn(a, b), d));
+    den = __fadd_rn(den, __fmul_rn(__fmul_rn(a, c), d));
+    den = __fadd_rn(den, __fmul_rn(__fmul_rn(b, c), d));
+    den = __fadd_rn(den, 1.1920929e-07f);
+    return __fdiv_rn(num, den);
+}
+
+// averaged_medium (m_medium.f90:432-465) over the memory box, on the device:
+// buoyancies 2 / (rho + rho') at the velocity points and 4-point harmonic
+// means of mu at the shear-stress points for k, i, j in [1, n], zero on the
+// rest of the box.  The host sends rho into the muyz array; pass 0 forms bx,
+// by, bz, muxz, muxy from it and mu, then pass 1 forms muyz over it.
+__global__ void average_medium_kernel(Geo g, const float *rho, const float *__restrict__ mu, float *bx, float *by,
+                                      float *bz, float *muyz, float *muxz, float *muxy, int pass) {
+    const int nkb = g.nz + 6, nib = g.nx + 6;
+    const long long n = (long long)nkb * nib * (g.ny + 6);
+    const long long pk = 1, pi = g.Kp, pj = (long long)g.Ip * g.Kp;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q % nkb) - 2;
+        const long long r = q / nkb;
+        const int i = (int)(r % nib) - 2, j = (int)(r / nib) - 2;
+        const long long e = cell_index(g, k, i, j);
+        const bool in = k >= 1 && k <= g.nz && i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+        const float nnn = in ? mu[e] : 0.0f;
+        const float pnn = in ? mu[e + pk] : 0.0f, npn = in ? mu[e + pi] : 0.0f, nnp = in ? mu[e + pj] : 0.0f;
+        if (pass == 0) {
+            float vx = 0.0f, vy = 0.0f, vz = 0.0f, vxz = 0.0f, vxy = 0.0f;
+            if (in) {
+                const float r0 = rho[e];
+                vx = __fdiv_rn(2.0f, __fadd_rn(r0, rho[e + pi]));
+                vy = __fdiv_rn(2.0f, __fadd_rn(r0, rho[e + pj]));
+                vz = __fdiv_rn(2.0f, __fadd_rn(r0, rho[e + pk]));
+                vxz = harmonic4(nnn, pnn, npn, mu[e + pk + pi]);
+                vxy = harmonic4(nnn, npn, nnp, mu[e + pi + pj]);
+            }
+            bx[e] = vx; by[e] = vy; bz[e] = vz; muxz[e] = vxz; muxy[e] = vxy;
+        } else {
+            muyz[e] = in ? harmonic4(nnn, pnn, nnp, mu[e + pk + pj]) : 0.0f;
+        }
+    }
+}
+
 }  // namespace swpc
 
 // ---------------------------------------------------------------------------
@@ -392,9 +440,20 @@ extern "C" int swpc_upload_medium(swpc_ctx *c, const swpc_medium_view *m) {
     if (!is3d(c)) return upload_medium_2d(c, m);
     const Geo &g = c->g;
     const float *src[11] = {m->rho, m->lam, m->mu, m->taup, m->taus, m->bx, m->by, m->bz, m->muyz, m->muxz, m->muxy};
-    for (int q = 1; q < 11; q++) {
+    // rho without the six averaged fields: form them in HBM (half the bytes
+    // over the host link)
+    const bool average = m->rho && !m->bx && !m->by && !m->bz && !m->muyz && !m->muxz && !m->muxy;
+    for (int q = 1; q < (average ? 5 : 11); q++) {
         if (!src[q]) return set_err(c, SWPC_ERR_ARG, "medium field missing");
         RC(copy_box(c, c->med[q], src[q], nullptr, m->ld_k, m->ld_i));
+    }
+    if (average) {
+        RC(copy_box(c, c->med[8], m->rho, nullptr, m->ld_k, m->ld_i));
+        for (int pass = 0; pass < 2; pass++) {
+            average_medium_kernel<<<148 * 8, 256, 0, c->stream>>>(g, c->med[8], c->med[2], c->med[5], c->med[6],
+                                                                 c->med[7], c->med[8], c->med[9], c->med[10], pass);
+            CK(cudaGetLastError());
+        }
     }
     if (!m->kfs || !m->kob || !m->kfs_top || !m->kfs_bot || !m->kob_top || !m->kob_bot || !m->kbeg_a)
         return set_err(c, SWPC_ERR_ARG, "integer map missing");
@@ -1225,6 +1284,10 @@ extern "C" int swpc_download_field(swpc_ctx *c, int field, float *out, int ld_k,
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     if (field >= SWPC_F_AUX && field < SWPC_F_AUX + 18) return aux_transfer(c, field - SWPC_F_AUX, out, nullptr, ld_k, ld_i);
+    if (field > SWPC_F_MED && field <= SWPC_F_MED + 10) {
+        if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "medium field ids address the 3D medium");
+        return copy_box(c, c->med[field - SWPC_F_MED], nullptr, out, ld_k, ld_i);
+    }
     float *p = field_ptr(c, field);
     if (!p) return set_err(c, SWPC_ERR_ARG, "unknown or unallocated field id");
     if (field_storage(c, field) != 0) {

@@ -218,9 +218,12 @@ class Medium:
         self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
         lib.swpc_kbeg_a(C.byref(g), iptr(self.kbeg_a))
 
-    def view(self) -> _lib.MediumView:
+    def view(self, average_on_device: bool = False) -> _lib.MediumView:
+        """The C view of the medium.  With ``average_on_device`` the six
+        averaged fields (bx, by, bz, muyz, muxz, muxy) are left out and
+        swpc_upload_medium forms them in HBM from rho and mu."""
         v = _lib.MediumView()
-        for name in self.FIELDS:
+        for name in self.FIELDS[:5] if average_on_device else self.FIELDS:
             setattr(v, name, fptr(getattr(self, name)))
         for name in self.MAPS:
             setattr(v, name, iptr(getattr(self, name)))
@@ -234,11 +237,13 @@ class Swpc3D:
     """One 3D run on one GPU (the single-node case of the reference)."""
 
     def __init__(self, p: Params, xi: np.ndarray | None = None, device: int = 0, medium: Medium | None = None,
-                 precision: str = "f32"):
+                 precision: str = "f32", average_on_device: bool = False):
         """``precision`` is the storage of stress and memory variables:
         "f32" (the reference's MP = SP build), "bf16r" (memory variables in
         BF16) or "f16sr" (stress and memory variables in FP16 with per-array
-        power-of-two scales); the arithmetic is FP32 in every form."""
+        power-of-two scales); the arithmetic is FP32 in every form.  With
+        ``average_on_device`` the upload sends rho instead of the six averaged
+        fields, which the library forms in HBM (same bits)."""
         p.check()
         self.p = p
         self.precision = precision
@@ -256,7 +261,7 @@ class Swpc3D:
             self.ctx = None
             raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_create failed")
         self._keep = []
-        check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view())))
+        check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view(average_on_device))))
         check(self.ctx, self.lib.swpc_kernel_setup(self.ctx, fptr(m.ts)))
         # source__setup (m_source.f90) or green__setup (m_green.f90)
         self.src = source_grid(p)

@@ -271,6 +271,28 @@ def test_large_box_uploads_through_the_staging_buffer():
     assert same_bits(g.download(_lib.F_VY), x)
 
 
+def test_averaged_medium_formed_on_the_device():
+    """With rho given and the six averaged fields left out, swpc_upload_medium
+    forms bx, by, bz, muyz, muxz, muxy in HBM (averaged_medium,
+    m_medium.f90:432-465): bitwise equal to the host fields over the whole
+    memory box, on a perturbed medium with air cells (harmonic means over zero
+    rigidity) that is large enough for the chunked upload; runs on either
+    medium agree bitwise."""
+    p = small3d(nx=90, ny=80, nz=60, na=10, nt=6)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    g0 = Swpc3D(p, xi)
+    m = g0.medium
+    assert float(m.mu.min()) == 0.0 and float(m.mu.max()) > 0.0
+    g1 = Swpc3D(p, medium=m, average_on_device=True)
+    for q, name in enumerate(m.FIELDS[1:], start=1):
+        assert same_bits(g1.download(_lib.F_MED + q), getattr(m, name)), name
+    for it in range(1, p.nt + 1):
+        g0.step(it)
+        g1.step(it)
+    for f in list(range(_lib.F_VX, _lib.F_SXY + 1)) + [_lib.F_R, _lib.F_R + 17]:
+        assert same_bits(g0.download(f), g1.download(f)), f
+
+
 def test_larger_grid_against_oracle_few_steps():
     """A grid whose planes exceed one warp row in every direction (k spans
     several 32-cell chunks, absorber/interior boundaries fall mid-warp)."""
