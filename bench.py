@@ -243,7 +243,18 @@ def bench_c2a(args, world, rank, local):
     bytes_step = n_int * B_PSV_INT + n_pml * B_PSV_PML
     ach = bytes_step * args.steps / (ms_batch / 1e3) / 1e9
 
-    # end to end through the C ABI: media from host memory, per-step batch calls, traces back
+    # end to end through the C ABI: media from pinned host memory, per-step batch calls, traces back
+    pinned = []
+    for r in runs:
+        for name in r.medium.FIELDS:
+            a = getattr(r.medium, name)
+            t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+            t.numpy()[...] = a
+            pinned.append(t)
+            setattr(r.medium, name, t.numpy())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(local)
     t0 = time.perf_counter()
     for r in runs:
         _lib.check(r.ctx, lib.swpc_upload_medium(r.ctx, C.byref(r.medium.view())))
@@ -285,7 +296,8 @@ def bench_c2a(args, world, rank, local):
                          "algorithmic_bytes_per_step": bytes_step},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
-                    "what": "media upload from host memory + per-step batch calls + trace download, wall clock"},
+                    "what": "media upload from pinned host memory + per-step batch calls + trace download, "
+                            "wall clock"},
             "gpu_launches": args.steps * 4, "clocks": clk.summary()}
     batch.close()
     for r in runs:
@@ -383,13 +395,28 @@ def bench_c2b(args, world, rank, local):
     peak, peak_kind = hbm_peak()
     ach = b_step / (ms_batch / args.steps / 1e3) / 1e9
     value = cells * nmem * args.steps / (ms_batch / 1e3) / 1e9
-    # end to end through the public API: per-step batch calls, every member's traces back to the host
+    # end to end through the public API: the shared medium from pinned host memory (the averaged arrays formed
+    # on the device), per-step batch calls, every member's traces back to the host
+    med = base.medium
+    pinned = []
+    for name in med.FIELDS[:5]:
+        a = getattr(med, name)
+        t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        t.numpy()[...] = a
+        pinned.append(t)
+        setattr(med, name, t.numpy())
+    view = med.view(average_on_device=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(local)
     t0 = time.perf_counter()
+    _lib.check(base.ctx, lib.swpc_upload_medium(base.ctx, C.byref(view)))
     for n in range(args.steps):
         fb.step(it0 + n)
     tr = [fb.waveforms(m) for m in range(len(forces))]
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     d2h = sum(t.nbytes for t in tr)
+    h2d = sum(t.numel() * 4 for t in pinned)
     line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_batch / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered medium)",
@@ -405,8 +432,9 @@ def bench_c2b(args, world, rank, local):
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
                          "traffic": None, "algorithmic_bytes_per_step": b_step},
             "e2e": {"value": cells * len(forces) * world * args.steps / t_e2e / 1e9, "unit": UNIT,
-                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h / args.steps,
-                    "what": "per-step batch calls + every member's traces downloaded, wall clock"},
+                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                    "what": "shared medium from pinned host memory (5 arrays; the 6 averaged ones formed on the "
+                            "device) + per-step batch calls + every member's traces downloaded, wall clock"},
             "gpu_launches": args.steps * 5, "clocks": clk.summary()}
     fb.close()
     base.close()
@@ -793,7 +821,7 @@ def main():
 
     import torch
     from openswpc_b200 import _lib
-    from openswpc_b200.swpc3d import Medium, Swpc3D
+    from openswpc_b200.swpc3d import DeviceMedium, Medium, Swpc3D
 
     ranks = replicas.init("nccl") if world > 1 else replicas.Ranks(1, 0, local)
     dist = ranks.dist
@@ -856,9 +884,14 @@ def main():
     ach_step = (b_stress + b_vel) / (ms_step / 1e3) / 1e9
 
     # ---- end to end through the C ABI with host buffers ---------------------
-    # medium upload from pinned host memory (rho, lam, mu, taup, taus; the
-    # averaged fields formed on the device) + per-routine C-ABI calls per step
-    # (vmax report every ntdec_r) + trace download, all inside the timed region
+    # the medium from host memory, the per-routine C-ABI calls of every step
+    # (vmax report every ntdec_r) and the trace download, all inside the timed
+    # region.  Headline: the layer table and the pinned perturbation xi, with
+    # vmodel_lhm and medium__setup run on the device (DeviceMedium).  Beside
+    # it: the host-built medium from pinned memory (rho, lam, mu, taup, taus;
+    # the averaged fields formed on the device).
+    xi_h = torch.empty(xi.shape, dtype=torch.float32, pin_memory=True)
+    xi_h.numpy()[...] = xi
     pinned = {}
     for name in Medium.FIELDS[:5]:
         a = getattr(med, name)
@@ -871,26 +904,30 @@ def main():
     lib.swpc_wav_dims(ctx, C.byref(ntw), C.byref(nst))
     tr = torch.empty((nst.value, 3, ntw.value), dtype=torch.float32, pin_memory=True)
     vm = (C.c_float * 3)()
-    barrier()
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    _lib.check(ctx, lib.swpc_upload_medium(ctx, C.byref(view)))
-    it = 1
-    for n in range(args.steps):
-        if it % p.ntdec_r == 0:
-            _lib.check(ctx, lib.swpc_vmax(ctx, vm))
-        _lib.check(ctx, lib.swpc_wav_store(ctx, it))
-        _lib.check(ctx, lib.swpc_update_stress(ctx))
-        _lib.check(ctx, lib.swpc_source_stressglut(ctx, it))
-        _lib.check(ctx, lib.swpc_update_vel(ctx))
-        it += 1
-    _lib.check(ctx, lib.swpc_wav_fetch(ctx, _lib.WAV_V, tr.numpy().ctypes.data_as(C.POINTER(C.c_float))))
-    _lib.check(ctx, lib.swpc_sync(ctx))
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
-    e2e_val = cells * args.steps * world / t_e2e / 1e9
-    med_bytes = sum(v.nbytes for v in pinned.values())
-    h2d = med_bytes / args.steps
+
+    def e2e_run(load_medium):
+        barrier()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        load_medium()
+        it = 1
+        for n in range(args.steps):
+            if it % p.ntdec_r == 0:
+                _lib.check(ctx, lib.swpc_vmax(ctx, vm))
+            _lib.check(ctx, lib.swpc_wav_store(ctx, it))
+            _lib.check(ctx, lib.swpc_update_stress(ctx))
+            _lib.check(ctx, lib.swpc_source_stressglut(ctx, it))
+            _lib.check(ctx, lib.swpc_update_vel(ctx))
+            it += 1
+        _lib.check(ctx, lib.swpc_wav_fetch(ctx, _lib.WAV_V, tr.numpy().ctypes.data_as(C.POINTER(C.c_float))))
+        _lib.check(ctx, lib.swpc_sync(ctx))
+        return cells * args.steps * world / max_over_ranks(time.perf_counter() - t0) / 1e9
+
+    e2e_host_val = e2e_run(lambda: _lib.check(ctx, lib.swpc_upload_medium(ctx, C.byref(view))))
+    e2e_val = e2e_run(lambda: DeviceMedium(lib, ctx, p, xi_h.numpy()))
     d2h = (tr.numel() * 4 + 12 * (args.steps // p.ntdec_r)) / args.steps
+    h2d = (xi_h.numel() * 4 + 24 * len(p.layers)) / args.steps
+    h2d_host = sum(v.nbytes for v in pinned.values()) / args.steps
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -914,9 +951,13 @@ def main():
             "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
                               "algorithmic_bytes_per_step": b_stress + b_vel},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "what": "medium upload from pinned host memory (5 arrays; the 6 averaged ones formed on "
-                            "the device) + per-routine C-ABI step calls + vmax reports + trace download, "
-                            "wall clock, max over ranks"},
+                    "what": "layer table + random perturbation xi from pinned host memory, vmodel_lhm and "
+                            "medium__setup on the device, per-routine C-ABI step calls, vmax reports, trace "
+                            "download; wall clock, max over ranks"},
+            "e2e_host_medium": {"value": e2e_host_val, "unit": UNIT, "h2d_bytes_per_step": h2d_host,
+                                "d2h_bytes_per_step": d2h,
+                                "what": "the host-built medium from pinned memory (5 arrays; the 6 averaged ones "
+                                        "formed on the device), then the same calls"},
             "gpu_launches": args.steps * (3 + 1 + 1),
             "clocks": clk.summary()}
     sim.close()

@@ -150,6 +150,33 @@ int swpc_sync(swpc_ctx *ctx);
  * fields of swpc_setup_medium; the host then sends 5 arrays instead of 10. */
 int swpc_upload_medium(swpc_ctx *ctx, const swpc_medium_view *m);
 
+/* ---- medium built on the device (3D) ------------------------------------
+ * The alternative to the host setup + swpc_upload_medium: the per-cell model
+ * and medium__setup (src/swpc_3d/m_medium.f90:36-467) run in HBM, bitwise
+ * equal to swpc_vmodel_lhm + swpc_setup_medium (swpc_setup.h) on the same
+ * inputs, and the context ends in the state swpc_upload_medium leaves.
+ *
+ * Step 1, one of:
+ *   swpc_vmodel_lhm_device: vmodel_lhm (m_vmodel_lhm.f90:21-169) from the
+ *     layer table; with xi != NULL the lhm_rmed perturbation
+ *     (m_vmodel_lhm_rmed.f90:187-195, vcheck m_fdtool.f90:15-48).  xi is a
+ *     host or a device array over the memory box (leading extents ld_k,
+ *     ld_i); zbeg is the top of the grid (m_global.f90 zbeg).
+ *   swpc_vmodel_upload: rho, lam, mu, qp, qs of any host-side model.
+ * Step 2, swpc_medium_setup_device: absorber homogenisation, tau method,
+ *   relaxed moduli, surface detection, velocity range and averaged medium.
+ *   Returns ts(1:nm) and scal = {zeta, vmin, vmax} as swpc_setup_medium does,
+ *   and, where the pointers are not NULL, the integer maps over
+ *   (-2:nx+3, -2:ny+3) with leading extent ld_i2 (kbeg_a as swpc_kbeg_a). */
+int swpc_vmodel_lhm_device(swpc_ctx *ctx, int nlayer, const float *depth, const float *rho0, const float *vp0,
+                           const float *vs0, const float *qp0, const float *qs0, float vcut, float rhomin, float zbeg,
+                           const float *xi, int ld_k, int ld_i);
+int swpc_vmodel_upload(swpc_ctx *ctx, const float *rho, const float *lam, const float *mu, const float *qp,
+                       const float *qs, int ld_k, int ld_i);
+int swpc_medium_setup_device(swpc_ctx *ctx, float fq_min, float fq_max, float fq_ref, float *ts, float *scal,
+                             int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, int *kbeg_a,
+                             int ld_i2);
+
 /* kernel__setup (src/swpc_3d/m_kernel.f90:30-73): FD coefficients from dx,
  * dy, dz and the Zener coefficients c1, c2, d1, d2 from ts(1:nm) and dt,
  * computed in single precision with the reference's expression order. */

@@ -36,6 +36,7 @@ WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 # every symbol the headers in include/ declare
 EXPORTS = [
     "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
+    "swpc_vmodel_lhm_device", "swpc_vmodel_upload", "swpc_medium_setup_device",
     "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
@@ -128,6 +129,9 @@ def load():
         "swpc_stream": (vp, [vp]),
         "swpc_sync": (i, [vp]),
         "swpc_upload_medium": (i, [vp, C.POINTER(MediumView)]),
+        "swpc_vmodel_lhm_device": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i]),
+        "swpc_vmodel_upload": (i, [vp, _FP, _FP, _FP, _FP, _FP, i, i]),
+        "swpc_medium_setup_device": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i]),
         "swpc_kernel_setup": (i, [vp, _FP]),
         "swpc_absorb_setup": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "swpc_source_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, _FP, i]),

@@ -428,6 +428,25 @@ __global__ void average_medium_kernel(Geo g, const float *rho, const float *__re
     }
 }
 
+int copy_box_from_device(swpc_ctx *c, float *dev, const float *src, int ld_k, int ld_i) {
+    const Geo &g = c->g;
+    const int nkb = g.nz + 6, nib = g.nx + 6, njb = is3d(c) ? g.ny + 6 : 1;
+    if (ld_k < nkb || ld_i < nib) return set_err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    repack_box_kernel<<<148 * 8, 256, 0, c->stream>>>(src, dev, nkb, nib, njb, ld_k, ld_i, g.Kp, g.Ip, 0,
+                                                     -2 - 1 + KH);
+    CK(cudaGetLastError());
+    return SWPC_OK;
+}
+
+int average_medium(swpc_ctx *c) {
+    for (int pass = 0; pass < 2; pass++) {
+        average_medium_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, c->med[8], c->med[2], c->med[5], c->med[6],
+                                                             c->med[7], c->med[8], c->med[9], c->med[10], pass);
+        CK(cudaGetLastError());
+    }
+    return SWPC_OK;
+}
+
 }  // namespace swpc
 
 // ---------------------------------------------------------------------------
@@ -449,11 +468,7 @@ extern "C" int swpc_upload_medium(swpc_ctx *c, const swpc_medium_view *m) {
     }
     if (average) {
         RC(copy_box(c, c->med[8], m->rho, nullptr, m->ld_k, m->ld_i));
-        for (int pass = 0; pass < 2; pass++) {
-            average_medium_kernel<<<148 * 8, 256, 0, c->stream>>>(g, c->med[8], c->med[2], c->med[5], c->med[6],
-                                                                 c->med[7], c->med[8], c->med[9], c->med[10], pass);
-            CK(cudaGetLastError());
-        }
+        RC(average_medium(c));
     }
     if (!m->kfs || !m->kob || !m->kfs_top || !m->kfs_bot || !m->kob_top || !m->kob_bot || !m->kbeg_a)
         return set_err(c, SWPC_ERR_ARG, "integer map missing");

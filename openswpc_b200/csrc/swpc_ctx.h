@@ -95,6 +95,7 @@ struct swpc_ctx {
     // coefficients
     bool kernel_ready = false;
     bool medium_ready = false;
+    bool vmodel_ready = false;   // a per-cell model waits in the medium arrays (swpc_medium.cu)
     float e40[3][2], e41[3][2];   // [axis][0: 4th order (isign=-1), 1: 2nd order band]
     float r20[3];
     float c1[swpc::NM_MAX], c2[swpc::NM_MAX], d1[swpc::NM_MAX], d2;
@@ -197,6 +198,12 @@ float field_scale(const swpc_ctx *c, int field);
 int prec_to_f32(swpc_ctx *c, int field, const float *stored, float **tmp);
 int prec_from_f32(swpc_ctx *c, int field, const float *tmp, float *stored);
 int cuda_check(swpc_ctx *c, cudaError_t e, const char *what);
+// host Fortran box (leading extents ld_k, ld_i) <-> device columns (swpc_api.cu)
+int copy_box(swpc_ctx *c, float *dev, const float *host_in, float *host_out, int ld_k, int ld_i);
+// the same from a device array in the Fortran box layout, on the context stream
+int copy_box_from_device(swpc_ctx *c, float *dev, const float *src, int ld_k, int ld_i);
+// averaged_medium on the device from rho (held in the muyz array) and mu (swpc_api.cu)
+int average_medium(swpc_ctx *c);
 template <typename T>
 int dalloc(swpc_ctx *c, T **p, size_t n) {
     if (n == 0) n = 1;

@@ -37,6 +37,35 @@ Box make_box(const swpc_grid *g) {
 
 namespace swpc {
 
+void relaxed_cc(int nm, const float *ts, float fq_ref, float *ccr_out, float *cci_out) {
+    const float omega = (float)(2 * kPi * (double)fq_ref);
+    float ccr = 0.0f, cci = 0.0f;
+    for (int m = 0; m < nm; m++) {
+        const double a = (double)omega * (double)ts[m];
+        const double den = 1.0 + a * a;
+        ccr = ccr + (float)(-(a * a) / den);
+        cci = cci + (float)(a / den);
+    }
+    *ccr_out = ccr / nm;
+    *cci_out = cci / nm;
+}
+
+void lhm_layers(const swpc_grid *g, int nlayer, const float *depth, const float *rho0_in, const float *vp0_in,
+                const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut, float *r0, float *p0,
+                float *s0, float *qa, float *qb, float *vmax_r) {
+    for (int l = 0; l < nlayer; l++) {
+        r0[l] = rho0_in[l]; p0[l] = vp0_in[l]; s0[l] = vs0_in[l]; qa[l] = qp0_in[l]; qb[l] = qs0_in[l];
+    }
+    // velocity cut-off (m_vmodel_lhm.f90:93-101)
+    for (int l = nlayer - 2; l >= 0; l--)
+        if ((p0[l] < vcut || s0[l] < vcut) && (p0[l] > 0 && s0[l] > 0)) {
+            p0[l] = p0[l + 1]; s0[l] = s0[l + 1]; r0[l] = r0[l + 1]; qa[l] = qa[l + 1]; qb[l] = qb[l + 1];
+        }
+    // velocity bounds of lhm_rmed (m_vmodel_lhm_rmed.f90:95-98)
+    const float dh = 1.0f / sqrtf(1.0f / (g->dx * g->dx) + 1.0f / (g->dy * g->dy) + 1.0f / (g->dz * g->dz));
+    *vmax_r = 6.0f / 7.0f * dh / g->dt;
+}
+
 float momentrate(float t, int stftype, float ts, float tr) {
     switch (stftype) {
     case SWPC_STF_BOXCAR:
@@ -178,16 +207,10 @@ int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const fl
                     const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut, const float *xi,
                     float rhomin, float *rho, float *lam, float *mu, float *qp, float *qs) {
     if (nlayer < 1) return SWPC_ERR_ARG;
-    std::vector<float> r0(rho0_in, rho0_in + nlayer), p0(vp0_in, vp0_in + nlayer), s0(vs0_in, vs0_in + nlayer);
-    std::vector<float> qa(qp0_in, qp0_in + nlayer), qb(qs0_in, qs0_in + nlayer);
-    // velocity cut-off (m_vmodel_lhm.f90:93-101)
-    for (int l = nlayer - 2; l >= 0; l--)
-        if ((p0[l] < vcut || s0[l] < vcut) && (p0[l] > 0 && s0[l] > 0)) {
-            p0[l] = p0[l + 1]; s0[l] = s0[l + 1]; r0[l] = r0[l + 1]; qa[l] = qa[l + 1]; qb[l] = qb[l + 1];
-        }
-    // velocity bounds of lhm_rmed (m_vmodel_lhm_rmed.f90:95-98)
-    const float dh = 1.0f / sqrtf(1.0f / (g->dx * g->dx) + 1.0f / (g->dy * g->dy) + 1.0f / (g->dz * g->dz));
-    const float vmax_r = 6.0f / 7.0f * dh / g->dt;
+    std::vector<float> r0(nlayer), p0(nlayer), s0(nlayer), qa(nlayer), qb(nlayer);
+    float vmax_r;
+    swpc::lhm_layers(g, nlayer, depth, rho0_in, vp0_in, vs0_in, qp0_in, qs0_in, vcut, r0.data(), p0.data(),
+                     s0.data(), qa.data(), qb.data(), &vmax_r);
     const Box b = make_box(g);
     const int jlo = g->ny > 1 ? -2 : 0, jhi = g->ny > 1 ? g->ny + 3 : 0;
 #pragma omp parallel for schedule(static)
@@ -271,16 +294,8 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
     // relaxed_medium (m_medium.f90:234-274): chi = 1 / Re(1/sqrt(1 - cc*tau)),
     // cc = mean over m of (i w ts)/(1 - i w ts)
     if (nm > 0) {
-        const float omega = (float)(2 * kPi * (double)fq_ref);
-        float ccr = 0.0f, cci = 0.0f;
-        for (int m = 0; m < nm; m++) {
-            const double a = (double)omega * (double)ts[m];
-            const double den = 1.0 + a * a;
-            ccr = ccr + (float)(-(a * a) / den);
-            cci = cci + (float)(a / den);
-        }
-        ccr = ccr / nm;
-        cci = cci / nm;
+        float ccr, cci;
+        swpc::relaxed_cc(nm, ts, fq_ref, &ccr, &cci);
 #pragma omp parallel for schedule(static)
         for (long e = 0; e < n3; e++) {
             const float rb2 = mu[e];

@@ -233,23 +233,65 @@ class Medium:
         return v
 
 
+class DeviceMedium:
+    """The medium built in HBM (swpc_vmodel_lhm_device, then
+    swpc_medium_setup_device): vmodel_lhm with the lhm_rmed perturbation
+    ``xi`` and medium__setup (m_medium.f90:36-467) run on the device, bitwise
+    equal to ``Medium``; the fields stay there and the integer maps, the
+    relaxation times and the velocity range come back.  ``xi`` is None, a
+    host array or a CUDA tensor of shape (ny+6, nx+6, nz+6)."""
+
+    MAPS = Medium.MAPS
+
+    def __init__(self, lib, ctx, p: Params, xi=None):
+        L = p.layers
+        if not L:
+            raise ValueError("a layered (lhm) velocity model is required")
+        arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        xp = None
+        if xi is not None:
+            if hasattr(xi, "data_ptr") and getattr(xi, "is_cuda", False):
+                import torch
+
+                assert tuple(xi.shape) == shape and xi.dtype == torch.float32 and xi.is_contiguous()
+                xp = C.cast(C.c_void_p(xi.data_ptr()), _lib._FP)
+            else:
+                xi = np.ascontiguousarray(xi, np.float32)
+                assert xi.shape == shape
+                xp = fptr(xi)
+        check(ctx, lib.swpc_vmodel_lhm_device(ctx, len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+                                              fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, p.rhomin,
+                                              p.zbeg, xp, p.nz + 6, p.nx + 6))
+        for name in self.MAPS:
+            setattr(self, name, np.zeros(shape[:2], np.int32))
+        self.ts = np.zeros(3, np.float32)
+        scal = np.zeros(3, np.float32)
+        check(ctx, lib.swpc_medium_setup_device(ctx, p.fq_min, p.fq_max, p.fq_ref, fptr(self.ts), fptr(scal),
+                                                *(iptr(getattr(self, n)) for n in self.MAPS), p.nx + 6))
+        self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
+
+
 class Swpc3D:
     """One 3D run on one GPU (the single-node case of the reference)."""
 
     def __init__(self, p: Params, xi: np.ndarray | None = None, device: int = 0, medium: Medium | None = None,
-                 precision: str = "f32", average_on_device: bool = False):
+                 precision: str = "f32", average_on_device: bool = False, medium_on_device: bool = False):
         """``precision`` is the storage of stress and memory variables:
         "f32" (the reference's MP = SP build), "bf16r" (memory variables in
         BF16) or "f16sr" (stress and memory variables in FP16 with per-array
         power-of-two scales); the arithmetic is FP32 in every form.  With
         ``average_on_device`` the upload sends rho instead of the six averaged
-        fields, which the library forms in HBM (same bits)."""
+        fields, which the library forms in HBM (same bits); with
+        ``medium_on_device`` the whole medium is built in HBM from the layers
+        and ``xi`` (``DeviceMedium``, same bits)."""
         p.check()
         self.p = p
         self.precision = precision
         self.lib = _lib.load()
-        self.medium = medium if medium is not None else Medium(p, xi)
-        m = self.medium
+        if not medium_on_device:
+            self.medium = medium if medium is not None else Medium(p, xi)
+        m = self.medium if not medium_on_device else None
         desc = _lib.Desc(_lib.KIND_3D, p.nx, p.ny, p.nz, p.na, p.nm, p.nt, p.dx, p.dy, p.dz, p.dt, p.tbeg, device,
                          _lib.PRECISIONS[precision])
         ctx = C.c_void_p()
@@ -261,7 +303,10 @@ class Swpc3D:
             self.ctx = None
             raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_create failed")
         self._keep = []
-        check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view(average_on_device))))
+        if medium_on_device:
+            m = self.medium = DeviceMedium(self.lib, self.ctx, p, xi)
+        else:
+            check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view(average_on_device))))
         check(self.ctx, self.lib.swpc_kernel_setup(self.ctx, fptr(m.ts)))
         # source__setup (m_source.f90) or green__setup (m_green.f90)
         self.src = source_grid(p)
