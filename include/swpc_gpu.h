@@ -189,6 +189,16 @@ int swpc_kernel_setup(swpc_ctx *ctx, const float *ts);
 int swpc_absorb_setup(swpc_ctx *ctx, const float *gxc, const float *gxe, const float *gyc, const float *gye,
                       const float *gzc, const float *gze);
 
+/* absorb_c__setup (src/swpc_3d/m_absorb_c.f90:27-103), abc_type = 'cerjan',
+ * in place of swpc_absorb_setup: the sponge factors at cell centres (_c) and
+ * +d/2 boundaries (_b), n values per axis (swpc_cerjan_profiles).  The
+ * interior update then covers the whole domain (m_global.f90:349-378) and
+ * the absorber updates multiply by the factors (m_absorb_c.f90:105-198).
+ * 3D with FP32 storage; the adjoint and the reciprocity batch refuse such
+ * a context. */
+int swpc_absorb_setup_cerjan(swpc_ctx *ctx, const float *gx_c, const float *gx_b, const float *gy_c,
+                             const float *gy_b, const float *gz_c, const float *gz_b);
+
 /* source__setup (src/swpc_3d/m_source.f90:41-313) after grid assignment and
  * normalisation: nsrc sources at grid (isrc, jsrc, ksrc), srcprm(2, nsrc) =
  * (start time, rise time), mo(nsrc) already divided by M0, m6(6, nsrc) =

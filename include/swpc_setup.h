@@ -83,6 +83,13 @@ int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float f
 void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gxe, float *gyc, float *gye, float *gzc,
                            float *gze);
 
+/* absorb_c__setup (src/swpc_3d/m_absorb_c.f90:27-103): the Cerjan sponge
+ * factors at cell centres (_c) and +d/2 boundaries (_b), n values per axis
+ * indexed [i-1]; the free surface (k <= na) is undamped.  For the 2D codes
+ * gy_c and gy_b may be NULL. */
+void swpc_cerjan_profiles(const swpc_grid *g, float *gx_c, float *gx_b, float *gy_c, float *gy_b, float *gz_c,
+                          float *gz_b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,7 @@ WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 # every symbol the headers in include/ declare
 EXPORTS = [
     "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
-    "swpc_vmodel_lhm_device", "swpc_vmodel_upload", "swpc_medium_setup_device",
+    "swpc_vmodel_lhm_device", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_absorb_setup_cerjan",
     "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
@@ -48,7 +48,7 @@ EXPORTS = [
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
-    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d",
+    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
@@ -134,6 +134,8 @@ def load():
         "swpc_medium_setup_device": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i]),
         "swpc_kernel_setup": (i, [vp, _FP]),
         "swpc_absorb_setup": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "swpc_absorb_setup_cerjan": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "swpc_cerjan_profiles": (None, [C.POINTER(Grid), _FP, _FP, _FP, _FP, _FP, _FP]),
         "swpc_source_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, _FP, i]),
         "swpc_bodyforce_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, i]),
         "swpc_green_setup": (i, [vp, i, i, i, C.c_char, f, f, i]),

@@ -218,6 +218,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     }
     if (c->d_err) cudaFree(c->d_err);
     if (c->stage) cudaFree(c->stage);
+    if (c->cj) cudaFree(c->cj);
     delete static_cast<TmaMaps *>(c->tmaps);
     void *ps[] = {c->V[0], c->V[1], c->V[2], c->band, c->pmlcol, c->kob, c->kfs, c->inj_glut, c->inj_bf,
                   c->stime_glut, c->mo_glut, c->stime_bf, c->inj_green, c->stf_green, c->st_ijk, c->wav[0],
@@ -488,7 +489,7 @@ extern "C" int swpc_upload_medium(swpc_ctx *c, const swpc_medium_view *m) {
         }
     // the fused kernels assume kbeg_a = 1 on side columns and kend_k + 1 under
     // the interior box (m_global.f90:336-345); reject anything else.
-    for (int j = 1; j <= g.ny; j++)
+    for (int j = 1; j <= g.ny && c->abc == 0; j++)
         for (int i = 1; i <= g.nx; i++) {
             const bool inner = i >= c->ibk && i <= c->iek && j >= c->jbk && j <= c->jek;
             const int want = inner ? c->kek + 1 : 1;
@@ -559,6 +560,7 @@ extern "C" int swpc_absorb_setup(swpc_ctx *c, const float *gxc, const float *gxe
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
     if (!c->medium_ready) return set_err(c, SWPC_ERR_STATE, "swpc_upload_medium must precede swpc_absorb_setup");
+    if (c->abc != 0) return set_err(c, SWPC_ERR_STATE, "the context runs the Cerjan sponge (abc_type = 'cerjan')");
     if (!is3d(c)) return absorb_setup_2d(c, gxc, gxe, gzc, gze);
     const Geo &g = c->g;
     RC(upload_profile(c, &c->gx[0], gxc, g.nx));
@@ -591,6 +593,77 @@ extern "C" int swpc_absorb_setup(swpc_ctx *c, const float *gxc, const float *gxe
     CK(cudaStreamSynchronize(c->stream));
     c->absorb_ready = true;
     return SWPC_OK;
+}
+
+// absorb_c__setup (src/swpc_3d/m_absorb_c.f90:27-103) with the kernel region
+// of abc_type = 'cerjan' (m_global.f90:349-378: the whole domain, so the
+// interior update covers every cell and no PML cell remains)
+extern "C" int swpc_absorb_setup_cerjan(swpc_ctx *c, const float *gx_c, const float *gx_b, const float *gy_c,
+                                        const float *gy_b, const float *gz_c, const float *gz_b) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "the Cerjan sponge is implemented for the 3D code");
+    if (c->prec != SWPC_PREC_F32) return set_err(c, SWPC_ERR_ARG, "the Cerjan sponge runs with FP32 storage");
+    if (c->abc == 0 && c->absorb_ready)
+        return set_err(c, SWPC_ERR_STATE, "the context already runs the PML (abc_type = 'pml')");
+    if (!gx_c || !gx_b || !gy_c || !gy_b || !gz_c || !gz_b) return set_err(c, SWPC_ERR_ARG, "sponge profile missing");
+    CK(cudaSetDevice(c->device));
+    invalidate_graph(c);
+    const Geo &g = c->g;
+    const size_t n = 2 * (size_t)(g.nx + g.ny + g.nz);
+    if (!c->cj) RC(dalloc(c, &c->cj, n));
+    std::vector<float> h(n);
+    std::copy(gx_c, gx_c + g.nx, h.begin());
+    std::copy(gx_b, gx_b + g.nx, h.begin() + g.nx);
+    std::copy(gy_c, gy_c + g.ny, h.begin() + 2 * g.nx);
+    std::copy(gy_b, gy_b + g.ny, h.begin() + 2 * g.nx + g.ny);
+    std::copy(gz_c, gz_c + g.nz, h.begin() + 2 * (g.nx + g.ny));
+    std::copy(gz_b, gz_b + g.nz, h.begin() + 2 * (g.nx + g.ny) + g.nz);
+    CK(cudaMemcpyAsync(c->cj, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->abc = 1;
+    c->ibk = 1; c->iek = g.nx; c->jbk = 1; c->jek = g.ny; c->kbk = 1; c->kek = g.nz;
+    c->absorb_ready = true;
+    return SWPC_OK;
+}
+
+// absorb_c__update_stress / absorb_c__update_vel (m_absorb_c.f90:105-198):
+// each field times the factors of its staggered position, after the
+// interior update.  Cells whose factors are all 1 (inside the sponge-free
+// box) are skipped: a product with 1 leaves the bits unchanged.
+__global__ void cerjan3d_kernel(Geo g, int na, int phase, const float *__restrict__ cj, float *f0, float *f1,
+                                float *f2, float *f3, float *f4, float *f5) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const float *gxc = cj, *gxb = cj + nx, *gyc = cj + 2 * nx, *gyb = gyc + ny, *gzc = gyc + 2 * ny, *gzb = gzc + nz;
+    const long long n = (long long)nz * nx * ny;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = 1 + (int)(q % nz);
+        const long long r = q / nz;
+        const int i = 1 + (int)(r % nx), j = 1 + (int)(r / nx);
+        if (i > na && i <= nx - na && j > na && j <= ny - na && k <= nz - na) continue;
+        const long long e = cell_index(g, k, i, j);
+        const float xc = gxc[i - 1], xb = gxb[i - 1], yc = gyc[j - 1], yb = gyb[j - 1], zc = gzc[k - 1], zb = gzb[k - 1];
+        if (phase == 0) {
+            const float gcc = __fmul_rn(__fmul_rn(xc, yc), zc);
+            f0[e] = __fmul_rn(f0[e], gcc);
+            f1[e] = __fmul_rn(f1[e], gcc);
+            f2[e] = __fmul_rn(f2[e], gcc);
+            f3[e] = __fmul_rn(__fmul_rn(__fmul_rn(f3[e], xc), yb), zb);
+            f4[e] = __fmul_rn(__fmul_rn(__fmul_rn(f4[e], xb), yc), zb);
+            f5[e] = __fmul_rn(__fmul_rn(__fmul_rn(f5[e], xb), yb), zc);
+        } else {
+            f0[e] = __fmul_rn(__fmul_rn(__fmul_rn(f0[e], xb), yc), zc);
+            f1[e] = __fmul_rn(__fmul_rn(__fmul_rn(f1[e], xc), yb), zc);
+            f2[e] = __fmul_rn(__fmul_rn(__fmul_rn(f2[e], xc), yc), zb);
+        }
+    }
+}
+
+static int launch_cerjan(swpc_ctx *c, int phase) {
+    float *const *f = phase == 0 ? c->S : c->V;
+    cerjan3d_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, c->d.na, phase, c->cj, f[0], f[1], f[2],
+                                                     phase == 0 ? f[3] : nullptr, phase == 0 ? f[4] : nullptr,
+                                                     phase == 0 ? f[5] : nullptr);
+    return cuda_check(c, cudaGetLastError(), "cerjan3d launch");
 }
 
 // ---------------------------------------------------------------------------
@@ -954,9 +1027,23 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfi
 }
 }  // namespace swpc
 
+static int launch_stress_kernel(swpc_ctx *c, int mask);
+static int launch_vel_kernel(swpc_ctx *c, int mask);
+
 static int launch_stress(swpc_ctx *c, int mask) {
     RC(check_ready(c));
     if (!is3d(c)) return update_stress_2d(c, mask);
+    if (c->abc == 1) {
+        // Cerjan: the interior update over the whole domain, then the sponge
+        // (absorb__update_stress's dispatch, m_absorb.f90:43-58)
+        if (mask & 1) RC(launch_stress_kernel(c, 1));
+        if (mask & 2) RC(launch_cerjan(c, 0));
+        return SWPC_OK;
+    }
+    return launch_stress_kernel(c, mask);
+}
+
+static int launch_stress_kernel(swpc_ctx *c, int mask) {
     Str3Args a;
     memset(&a, 0, sizeof(a));
     fill_geo_common(c, a.g, a.ibk, a.iek, a.jbk, a.jek, a.kek);
@@ -972,7 +1059,7 @@ static int launch_stress(swpc_ctx *c, int mask) {
     memcpy(a.c1, c->c1, sizeof(a.c1)); memcpy(a.c2, c->c2, sizeof(a.c2)); memcpy(a.d1, c->d1, sizeof(a.d1));
     a.d2 = c->d2;
     a.dt = c->d.dt;
-    a.mask = (c->d.na > 0) ? mask : (mask & 1);
+    a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     for (int q = 0; q < 6; q++) { a.sS[q] = ldexpf(1.0f, c->eS[q]); a.iS[q] = ldexpf(1.0f, -c->eS[q]); }
     for (int q = 0; q < 18; q++) { a.sR[q] = ldexpf(1.0f, c->eR[q]); a.iR[q] = ldexpf(1.0f, -c->eR[q]); }
     dim3 block(32, c->bi, c->bj);
@@ -992,6 +1079,16 @@ static int launch_stress(swpc_ctx *c, int mask) {
 static int launch_vel(swpc_ctx *c, int mask) {
     RC(check_ready(c));
     if (!is3d(c)) return update_vel_2d(c, mask);
+    if (c->abc == 1) {
+        // Cerjan (absorb__update_vel's dispatch, m_absorb.f90:60-75)
+        if (mask & 1) RC(launch_vel_kernel(c, 1));
+        if (mask & 2) RC(launch_cerjan(c, 1));
+        return SWPC_OK;
+    }
+    return launch_vel_kernel(c, mask);
+}
+
+static int launch_vel_kernel(swpc_ctx *c, int mask) {
     Vel3Args a;
     memset(&a, 0, sizeof(a));
     fill_geo_common(c, a.g, a.ibk, a.iek, a.jbk, a.jek, a.kek);
@@ -1003,7 +1100,7 @@ static int launch_vel(swpc_ctx *c, int mask) {
     a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
     memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
     a.dt = c->d.dt;
-    a.mask = (c->d.na > 0) ? mask : (mask & 1);
+    a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
     for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);

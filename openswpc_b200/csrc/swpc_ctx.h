@@ -84,6 +84,9 @@ struct swpc_ctx {
     int *kob = nullptr, *kfs = nullptr;   // per column
     std::vector<int> h_kbeg_a;            // host copy (columns, device indexing)
 
+    // absorber: 0 ADE-CFS PML, 1 Cerjan sponge (abc_type, m_absorb.f90:25-75)
+    int abc = 0;
+    float *cj = nullptr;   // Cerjan factors: gx_c gx_b (nx) gy_c gy_b (ny) gz_c gz_b (nz)
     // PML
     bool absorb_ready = false;
     long long npml = 0;

@@ -509,4 +509,37 @@ void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gx
     }
 }
 
+// one axis of absorb_c__setup (src/swpc_3d/m_absorb_c.f90:48-85): inside
+// the na cells at the low end (when `low`) and at the high end, exp(-alpha
+// (1 - x/L)^2) with x the distance from the edge at the cell centre (c) and
+// at its +d/2 boundary (b); 1 elsewhere
+static void cerjan_axis(int n, int na, float d, bool low, float *gc, float *gb) {
+    const float alpha = 0.09f;
+    const float L = na * d;
+    for (int i = 1; i <= n; i++) {
+        float c = 1.0f, b = 1.0f;
+        if (low && i <= na) {
+            const float x = swpc_i2x(i, 0.0f, d);
+            const float uc = 1.0f - x / L, ub = 1.0f - (x + d / 2) / L;
+            c = expf(-alpha * (uc * uc));
+            b = expf(-alpha * (ub * ub));
+        } else if (i >= n - na + 1) {
+            const float x = swpc_i2x(i, n * d, -d);
+            const float uc = 1.0f - (x + d / 2) / L, ub = 1.0f - x / L;
+            c = expf(-alpha * (uc * uc));
+            b = expf(-alpha * (ub * ub));
+        }
+        gc[i - 1] = c;
+        gb[i - 1] = b;
+    }
+}
+
+void swpc_cerjan_profiles(const swpc_grid *g, float *gx_c, float *gx_b, float *gy_c, float *gy_b, float *gz_c,
+                          float *gz_b) {
+    cerjan_axis(g->nx, g->na, g->dx, true, gx_c, gx_b);
+    if (gy_c && gy_b) cerjan_axis(g->ny, g->na, g->dy, true, gy_c, gy_b);
+    // the free surface side (k <= na) is not damped (m_absorb_c.f90:73-80)
+    cerjan_axis(g->nz, g->na, g->dz, false, gz_c, gz_b);
+}
+
 }  // extern "C"

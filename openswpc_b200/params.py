@@ -121,8 +121,8 @@ class Params:
             self.zbeg = float(np.float32(-30) * np.float32(self.dz))
 
     def check(self) -> None:
-        if self.abc_type != "pml":
-            raise ValueError("only abc_type = 'pml' is supported (the Cerjan sponge is not implemented)")
+        if self.abc_type not in ("pml", "cerjan"):
+            raise ValueError("abc_type must be 'pml' or 'cerjan'")
         if self.nm not in (0, 1, 2, 3):
             raise ValueError("nm must be 0..3")
         if self.stftype not in ("kupper", "boxcar", "triangle", "herrmann", "cosine", "scosine", "texp"):

@@ -81,6 +81,8 @@ class Swpc2D:
 
     def __init__(self, p: Params, kind: str = "psv", device: int = 0):
         p.check()
+        if p.abc_type != "pml":
+            raise ValueError("the 2D codes run with the PML (abc_type = 'pml')")
         self.p, self.kind = p, kind
         lib = self.lib = _lib.load()
         m = self.medium = Medium2D(p)

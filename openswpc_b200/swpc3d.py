@@ -331,15 +331,25 @@ class Swpc3D:
             check(self.ctx, self.lib.swpc_source_setup(self.ctx, len(s.isrc), iptr(s.isrc), iptr(s.jsrc),
                                                        iptr(s.ksrc), fptr(s.srcprm), fptr(s.mo), fptr(s.m6), stf))
             self.fcut = s.fcut
-        # absorb_p__setup with fcut from the source setup (m_absorb_p.f90:528)
         g = grid_struct(p)
-        self.gprof = {n: np.zeros((p.nx if n[1] == "x" else p.ny if n[1] == "y" else p.nz, 4), np.float32)
-                      for n in ("gxc", "gxe", "gyc", "gye", "gzc", "gze")}
-        gp = self.gprof
-        self.lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]),
-                                       fptr(gp["gyc"]), fptr(gp["gye"]), fptr(gp["gzc"]), fptr(gp["gze"]))
-        check(self.ctx, self.lib.swpc_absorb_setup(self.ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), fptr(gp["gyc"]),
-                                                   fptr(gp["gye"]), fptr(gp["gzc"]), fptr(gp["gze"])))
+        if p.abc_type == "cerjan":
+            # absorb__setup's dispatch (m_absorb.f90:25-41): absorb_c__setup
+            n = {"x": p.nx, "y": p.ny, "z": p.nz}
+            self.cprof = {a + t: np.zeros(n[a[1]], np.float32) for a in ("gx", "gy", "gz") for t in ("_c", "_b")}
+            cp = self.cprof
+            names = ("gx_c", "gx_b", "gy_c", "gy_b", "gz_c", "gz_b")
+            self.lib.swpc_cerjan_profiles(C.byref(g), *(fptr(cp[k]) for k in names))
+            check(self.ctx, self.lib.swpc_absorb_setup_cerjan(self.ctx, *(fptr(cp[k]) for k in names)))
+        else:
+            # absorb_p__setup with fcut from the source setup (m_absorb_p.f90:528)
+            self.gprof = {n: np.zeros((p.nx if n[1] == "x" else p.ny if n[1] == "y" else p.nz, 4), np.float32)
+                          for n in ("gxc", "gxe", "gyc", "gye", "gzc", "gze")}
+            gp = self.gprof
+            self.lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]),
+                                           fptr(gp["gyc"]), fptr(gp["gye"]), fptr(gp["gzc"]), fptr(gp["gze"]))
+            check(self.ctx, self.lib.swpc_absorb_setup(self.ctx, fptr(gp["gxc"]), fptr(gp["gxe"]),
+                                                       fptr(gp["gyc"]), fptr(gp["gye"]), fptr(gp["gzc"]),
+                                                       fptr(gp["gze"])))
         # wav__setup (m_wav.f90:76-142); off in green mode
         self.nst = 0
         what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u) | (_lib.WAV_STRESS * p.sw_wav_stress) | \

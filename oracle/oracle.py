@@ -37,6 +37,10 @@ AUX_NAMES = ["axVx", "ayVx", "azVx", "axVy", "ayVy", "azVy", "axVz", "ayVz", "az
              "axSxx", "aySxy", "azSxz", "axSxy", "aySyy", "azSyz", "axSxz", "aySyz", "azSzz"]
 for _n, _a in enumerate(AUX_NAMES):
     FIELD_IDS[_a] = 60 + _n
+# Cerjan sponge factors (n values per axis)
+CERJAN_NAMES = ["gx_c", "gx_b", "gy_c", "gy_b", "gz_c", "gz_b"]
+for _n, _a in enumerate(CERJAN_NAMES):
+    FIELD_IDS[_a] = 110 + _n
 
 
 def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
@@ -61,6 +65,7 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_set_maps": (None, [vp, _IP, _IP, _IP, _IP, _IP, _IP]),
         "o3d_kernel_setup": (None, [vp]),
         "o3d_absorb_setup": (None, [vp, f]),
+        "o3d_cerjan_setup": (None, [vp]),
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
@@ -156,7 +161,12 @@ class Oracle3D:
                                              _f(m6), _f(f3), stf)
         sc = self.scalars()
         fcut = sc["fcut"] if not p.green_mode else float(np.float32(1.0) / np.float32(p.green_trise))
-        lib.o3d_absorb_setup(self.o, fcut)
+        if getattr(p, "abc_type", "pml") == "cerjan":
+            # absorb__setup's dispatch (m_absorb.f90:25-41): the sponge, and
+            # the kernel region over the whole domain
+            lib.o3d_cerjan_setup(self.o)
+        else:
+            lib.o3d_absorb_setup(self.o, fcut)
         if profiles is not None:
             lib.o3d_set_profiles(self.o, *[_f(profiles[k]) for k in ("gxc", "gxe", "gyc", "gye", "gzc", "gze")])
         if p.green_mode:
@@ -246,6 +256,8 @@ class Oracle3D:
             dt, shape = np.int32, (d["nj"], d["ni"])
         elif fid in range(60, 78):
             dt, shape = self.spr, (p.ny, p.nx, d["nka"])
+        elif fid in range(110, 116):
+            dt, shape = self.spr, ((p.nx, p.nx, p.ny, p.ny, p.nz, p.nz)[fid - 110],)
         else:
             raise KeyError(name)
         n = int(np.prod(shape))

@@ -86,6 +86,9 @@ typedef struct o3d {
     SPR *axSxx, *aySxy, *azSxz, *axSxy, *aySyy, *azSyz, *axSxz, *aySyz, *azSzz;
     MPR r20x, r20y, r20z;
     int kbeg_min;
+    /* Cerjan sponge (m_absorb_c.f90:19-20), indexed [i - 1] */
+    int cerjan;
+    SPR *cgx_c, *cgx_b, *cgy_c, *cgy_b, *cgz_c, *cgz_b;
     long nka;                   /* PML aux k extent */
     /* sources (m_source.f90:26-36) */
     int bf_mode, stftype, nsrc;
@@ -369,7 +372,8 @@ void o3d_destroy(o3d *o) {
                   o->aySyy, o->azSyz, o->axSxz, o->aySyz, o->azSzz, o->isrc, o->jsrc, o->ksrc, o->srcprm,
                   o->mo, o->mxx, o->myy, o->mzz, o->myz, o->mxz, o->mxy, o->fx, o->fy, o->fz, o->ist, o->jst,
                   o->kst, o->wav_vel, o->wav_disp, o->wav_stress, o->wav_strain, o->ux, o->uy, o->uz,
-                  o->exx, o->eyy, o->ezz, o->eyz, o->exz, o->exy};
+                  o->exx, o->eyy, o->ezz, o->eyz, o->exz, o->exy, o->cgx_c, o->cgx_b, o->cgy_c, o->cgy_b,
+                  o->cgz_c, o->cgz_b};
     for (size_t n = 0; n < sizeof(ps) / sizeof(ps[0]); n++) free(ps[n]);
     for (int q = 0; q < 15; q++) { free(o->snp[q]); free(o->sbuf[q]); }
     for (int q = 0; q < 4; q++) free(o->maxv[q]);
@@ -852,9 +856,93 @@ void o3d_update_stress(o3d *o) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* absorb_p__update_vel: m_absorb_p.f90:126-311 (pw_mode off)               */
+/* absorb_c__setup: m_absorb_c.f90:27-103, with the kernel region of          */
+/* abc_type = 'cerjan' (m_global.f90:349-378: the whole domain)              */
+/* ------------------------------------------------------------------------ */
+static void cerjan_axis(SPR *gc, SPR *gb, int n, int na, float d, int low) {
+    const float alpha = 0.09f;
+    const float L = na * d;
+    for (int i = 1; i <= n; i++) {
+        float c = 1.0f, b = 1.0f;
+        if (low && i <= na) {
+            /* m_absorb_c.f90:56-58 */
+            const float x = o3d_i2x(i, 0.0f, d);
+            const float yc = 1.0f - x / L, yb = 1.0f - (x + d / 2) / L;
+            c = expf(-alpha * (yc * yc));
+            b = expf(-alpha * (yb * yb));
+        } else if (i >= n - na + 1) {
+            /* m_absorb_c.f90:59-61 */
+            const float x = o3d_i2x(i, n * d, -d);
+            const float yc = 1.0f - (x + d / 2) / L, yb = 1.0f - x / L;
+            c = expf(-alpha * (yc * yc));
+            b = expf(-alpha * (yb * yb));
+        }
+        gc[i - 1] = c;
+        gb[i - 1] = b;
+    }
+}
+
+void o3d_cerjan_setup(o3d *o) {
+    o->cerjan = 1;
+    o->cgx_c = (SPR *)zalloc(sizeof(SPR) * o->nx); o->cgx_b = (SPR *)zalloc(sizeof(SPR) * o->nx);
+    o->cgy_c = (SPR *)zalloc(sizeof(SPR) * o->ny); o->cgy_b = (SPR *)zalloc(sizeof(SPR) * o->ny);
+    o->cgz_c = (SPR *)zalloc(sizeof(SPR) * o->nz); o->cgz_b = (SPR *)zalloc(sizeof(SPR) * o->nz);
+    cerjan_axis(o->cgx_c, o->cgx_b, o->nx, o->na, (float)o->dx, 1);
+    cerjan_axis(o->cgy_c, o->cgy_b, o->ny, o->na, (float)o->dy, 1);
+    cerjan_axis(o->cgz_c, o->cgz_b, o->nz, o->na, (float)o->dz, 0);   /* free surface undamped (:73-80) */
+    o->ibeg_k = o->ibeg; o->iend_k = o->iend; o->jbeg_k = o->jbeg; o->jend_k = o->jend;
+    o->kbeg_k = o->kbeg; o->kend_k = o->kend;
+    o->nkk = o->kend_k - o->kbeg_k + 1;
+    o->nik = o->iend_k - o->ibeg_k + 1;
+    o->njk = o->jend_k - o->jbeg_k + 1;
+    const long nr = (long)o->nm * o->nkk * o->nik * o->njk;
+    SPR **R[6] = {&o->Rxx, &o->Ryy, &o->Rzz, &o->Ryz, &o->Rxz, &o->Rxy};
+    for (int q = 0; q < 6; q++) {
+        free(*R[q]);
+        *R[q] = (SPR *)zalloc(sizeof(SPR) * (size_t)nr);
+    }
+}
+
+/* absorb_c__update_stress: m_absorb_c.f90:105-167 */
+static void cerjan_update_stress(o3d *o) {
+#pragma omp parallel for schedule(dynamic) num_threads(o->threads)
+    for (int j = o->jbeg; j <= o->jend; j++)
+        for (int i = o->ibeg; i <= o->iend; i++)
+            for (int k = o->kbeg; k <= o->kend_k; k++) {
+                const SPR gxc = o->cgx_c[i - 1], gxb = o->cgx_b[i - 1], gyc = o->cgy_c[j - 1], gyb = o->cgy_b[j - 1];
+                const SPR gzc = o->cgz_c[k - 1], gzb = o->cgz_b[k - 1];
+                const SPR gcc = gxc * gyc * gzc;
+                A3(o->Sxx, k, i, j) = A3(o->Sxx, k, i, j) * gcc;
+                A3(o->Syy, k, i, j) = A3(o->Syy, k, i, j) * gcc;
+                A3(o->Szz, k, i, j) = A3(o->Szz, k, i, j) * gcc;
+                A3(o->Syz, k, i, j) = A3(o->Syz, k, i, j) * gxc * gyb * gzb;
+                A3(o->Sxz, k, i, j) = A3(o->Sxz, k, i, j) * gxb * gyc * gzb;
+                A3(o->Sxy, k, i, j) = A3(o->Sxy, k, i, j) * gxb * gyb * gzc;
+            }
+}
+
+/* absorb_c__update_vel: m_absorb_c.f90:169-198 */
+static void cerjan_update_vel(o3d *o) {
+#pragma omp parallel for schedule(dynamic) num_threads(o->threads)
+    for (int j = o->jbeg; j <= o->jend; j++)
+        for (int i = o->ibeg; i <= o->iend; i++)
+            for (int k = o->kbeg; k <= o->kend; k++) {
+                const SPR gxc = o->cgx_c[i - 1], gxb = o->cgx_b[i - 1], gyc = o->cgy_c[j - 1], gyb = o->cgy_b[j - 1];
+                const SPR gzc = o->cgz_c[k - 1], gzb = o->cgz_b[k - 1];
+                A3(o->Vx, k, i, j) = A3(o->Vx, k, i, j) * gxb * gyc * gzc;
+                A3(o->Vy, k, i, j) = A3(o->Vy, k, i, j) * gxc * gyb * gzc;
+                A3(o->Vz, k, i, j) = A3(o->Vz, k, i, j) * gxc * gyc * gzb;
+            }
+}
+
+/* absorb_p__update_vel: m_absorb_p.f90:126-311 (pw_mode off); the dispatch
+ * of absorb__update_vel (m_absorb.f90:60-75) picks the sponge instead */
 /* ------------------------------------------------------------------------ */
 void o3d_absorb_update_vel(o3d *o) {
+    if (o->cerjan) {
+        cerjan_update_vel(o);
+        return;
+    }
     const float dt = o->dt;
     MPR *Sxx = o->Sxx, *Syy = o->Syy, *Szz = o->Szz, *Syz = o->Syz, *Sxz = o->Sxz, *Sxy = o->Sxy;
 #pragma omp parallel for schedule(dynamic) num_threads(o->threads)
@@ -890,9 +978,15 @@ void o3d_absorb_update_vel(o3d *o) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* absorb_p__update_stress: m_absorb_p.f90:313-505 (pw_mode off)            */
+/* absorb_p__update_stress: m_absorb_p.f90:313-505 (pw_mode off); the
+ * dispatch of absorb__update_stress (m_absorb.f90:43-58) picks the sponge
+ * instead */
 /* ------------------------------------------------------------------------ */
 void o3d_absorb_update_stress(o3d *o) {
+    if (o->cerjan) {
+        cerjan_update_stress(o);
+        return;
+    }
     const float dt = o->dt;
     MPR *Vx = o->Vx, *Vy = o->Vy, *Vz = o->Vz;
 #pragma omp parallel for schedule(dynamic) num_threads(o->threads)
@@ -1496,6 +1590,8 @@ void *o3d_ptr(o3d *o, int id) {
     case 93: return o->wav_strain;
     case 95: return o->ist; case 96: return o->jst; case 97: return o->kst;
     case 98: return o->isrc; case 99: return o->jsrc; case 100: return o->ksrc;
+    case 110: return o->cgx_c; case 111: return o->cgx_b; case 112: return o->cgy_c;
+    case 113: return o->cgy_b; case 114: return o->cgz_c; case 115: return o->cgz_b;
     default: return 0;
     }
 }

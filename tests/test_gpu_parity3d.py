@@ -71,7 +71,7 @@ def compare_state(g: Swpc3D, o: Oracle3D, p, what="all"):
                 a = g.download(_lib.F_R + 3 * c + m)
                 b = oracle_R_as_box(o, name, m, p)
                 assert same_bits(a, b), (name, m, np.abs(a - b).max())
-        if p.na > 0:
+        if p.na > 0 and p.abc_type == "pml":
             for q, name in enumerate(AUX_NAMES):
                 a = g.download(_lib.F_AUX + q)
                 b = oracle_aux_as_box(o, name, p)

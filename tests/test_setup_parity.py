@@ -203,3 +203,27 @@ def test_oracle_2d_fp32_close_to_fp64(kind):
     wa, wb = a.waveforms("v").astype(np.float64), b.waveforms("v").astype(np.float64)
     assert np.linalg.norm(wb) > 0
     assert np.linalg.norm(wa - wb) / np.linalg.norm(wb) < 1e-4
+
+
+def test_cerjan_profiles_match_oracle():
+    """swpc_cerjan_profiles (absorb_c__setup, m_absorb_c.f90:27-103) against
+    the oracle's sponge factors, bitwise; the free-surface side is 1."""
+    import ctypes as C
+
+    from openswpc_b200 import _lib
+    from openswpc_b200.swpc3d import grid_struct
+    from oracle.oracle import Oracle3D
+    from tests.models import small3d
+
+    p = small3d(nx=40, ny=36, nz=32, na=8, nt=2, abc_type="cerjan")
+    lib = _lib.load()
+    n = {"x": p.nx, "y": p.ny, "z": p.nz}
+    names = ("gx_c", "gx_b", "gy_c", "gy_b", "gz_c", "gz_b")
+    prof = {k: np.zeros(n[k[1]], np.float32) for k in names}
+    lib.swpc_cerjan_profiles(C.byref(grid_struct(p)), *(_lib.fptr(prof[k]) for k in names))
+    o = Oracle3D(p)
+    for k in names:
+        b = o.array(k)
+        assert np.array_equal(prof[k].view(np.uint32), b.astype(np.float32).view(np.uint32)), k
+    assert np.all(prof["gz_c"][:p.na] == 1.0) and prof["gz_c"][-1] < 1.0
+    assert prof["gx_c"][0] < prof["gx_c"][p.na - 1] < 1.0 and prof["gx_c"][p.na] == 1.0
