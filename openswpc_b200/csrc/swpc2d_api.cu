@@ -45,6 +45,8 @@ int tile2d_flags(const swpc_ctx *c, int k0, int i0, int ni) {
     return f;
 }
 
+int build_tiles_2d(swpc_ctx *c);
+
 int create_2d(swpc_ctx *c) {
     const Geo &g = c->g;
     const bool psv = c->kind == SWPC_KIND_PSV;
@@ -84,16 +86,90 @@ int create_2d(swpc_ctx *c) {
         return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the 2D field slab");
     c->stress_tma = c->vel_tma = true;
     c->stress_tbi = c->vel_tbi = 8;
-    // tile list: 32 (k) x 16 (i)
+    return build_tiles_2d(c);
+}
+
+// tile list: 32 (k) x 16 (i), flagged by the kernel region
+int build_tiles_2d(swpc_ctx *c) {
+    const Geo &g = c->g;
     std::vector<Tile2D> tiles;
     const int ni = kDefaultTiles.ti * kDefaultTiles.ri;
     for (int i0 = 1; i0 <= g.nx; i0 += ni)
         for (int k0 = 1; k0 <= g.nz; k0 += 32) tiles.push_back(Tile2D{0, k0, i0, tile2d_flags(c, k0, i0, ni)});
+    if (!c->d_tiles2d) RC(dalloc(c, &c->d_tiles2d, tiles.size()));
     c->ntiles2d = (int)tiles.size();
-    RC(dalloc(c, &c->d_tiles2d, tiles.size()));
     CK(cudaMemcpyAsync(c->d_tiles2d, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return SWPC_OK;
+}
+
+// absorb_c__setup of the 2D codes (src/swpc_psv/m_absorb_c.f90:27-88,
+// src/swpc_sh/m_absorb_c.f90:27-80) with the kernel region of abc_type =
+// 'cerjan' (src/swpc_psv/m_global.f90:281-303: the whole domain)
+int cerjan_setup_2d(swpc_ctx *c, const float *gx_c, const float *gx_b, const float *gz_c, const float *gz_b) {
+    const Geo &g = c->g;
+    if (!gx_c || !gx_b || !gz_c || !gz_b) return set_err(c, SWPC_ERR_ARG, "sponge profile missing");
+    const size_t n = 2 * (size_t)(g.nx + g.nz);
+    if (!c->cj) RC(dalloc(c, &c->cj, n));
+    std::vector<float> h(n);
+    std::copy(gx_c, gx_c + g.nx, h.begin());
+    std::copy(gx_b, gx_b + g.nx, h.begin() + g.nx);
+    std::copy(gz_c, gz_c + g.nz, h.begin() + 2 * g.nx);
+    std::copy(gz_b, gz_b + g.nz, h.begin() + 2 * g.nx + g.nz);
+    CK(cudaMemcpyAsync(c->cj, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    c->abc = 1;
+    c->ibk = 1; c->iek = g.nx; c->kbk = 1; c->kek = g.nz;
+    RC(build_tiles_2d(c));
+    c->desc_dirty = true;
+    c->absorb_ready = true;
+    return SWPC_OK;
+}
+
+// absorb_c__update_stress / _vel of P-SV (src/swpc_psv/m_absorb_c.f90:
+// 90-160) and SH (src/swpc_sh/m_absorb_c.f90:82-135) in the reference's
+// product order; cells with both factors 1 are skipped (same bits)
+__global__ void cerjan2d_kernel(int psv, int phase, int nx, int nz, int na, int Kp, const float *__restrict__ cj,
+                                float *f0, float *f1, float *f2) {
+    const float *gxc = cj, *gxb = cj + nx, *gzc = cj + 2 * nx, *gzb = gzc + nz;
+    const long long n = (long long)nz * nx;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = 1 + (int)(q % nz), i = 1 + (int)(q / nz);
+        if (i > na && i <= nx - na && k <= nz - na) continue;
+        const long long e = (long long)(i + 2) * Kp + (k - 1 + KH);
+        const float xc = gxc[i - 1], xb = gxb[i - 1], zc = gzc[k - 1], zb = gzb[k - 1];
+        if (psv) {
+            if (phase == 0) {
+                const float gc = __fmul_rn(xc, zc), gb = __fmul_rn(xb, zb);
+                f0[e] = __fmul_rn(f0[e], gc);
+                f1[e] = __fmul_rn(f1[e], gc);
+                f2[e] = __fmul_rn(f2[e], gb);
+            } else {
+                f0[e] = __fmul_rn(__fmul_rn(f0[e], xb), zc);
+                f1[e] = __fmul_rn(__fmul_rn(f1[e], xc), zb);
+            }
+        } else if (phase == 0) {
+            f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zb);
+            f1[e] = __fmul_rn(__fmul_rn(f1[e], xb), zc);
+        } else {
+            f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zc);
+        }
+    }
+}
+
+static int launch_cerjan2d(swpc_ctx *c, int phase) {
+    const bool psv = c->kind == SWPC_KIND_PSV;
+    float *f0, *f1 = nullptr, *f2 = nullptr;
+    if (phase == 0) {
+        f0 = psv ? c->S[0] : c->S[3];
+        f1 = psv ? c->S[2] : c->S[5];
+        f2 = psv ? c->S[4] : nullptr;
+    } else {
+        f0 = psv ? c->V[0] : c->V[1];
+        f1 = psv ? c->V[2] : nullptr;
+    }
+    cerjan2d_kernel<<<148 * 4, 256, 0, c->stream>>>(psv ? 1 : 0, phase, c->g.nx, c->g.nz, c->d.na, c->g.Kp, c->cj, f0,
+                                                     f1, f2);
+    return cuda_check(c, cudaGetLastError(), "cerjan2d launch");
 }
 
 void destroy_2d(swpc_ctx *c) {
@@ -123,7 +199,7 @@ int upload_medium_2d(swpc_ctx *c, const swpc_medium_view *m) {
         kfs[i + 2] = m->kfs[i + 2];
         c->h_kbeg_a[i + 2] = m->kbeg_a[i + 2];
     }
-    for (int i = 1; i <= g.nx; i++) {
+    for (int i = 1; i <= g.nx && c->abc == 0; i++) {
         const int want = (i >= c->ibk && i <= c->iek) ? c->kek + 1 : 1;
         if (c->h_kbeg_a[i + 2] != want)
             return set_err(c, SWPC_ERR_ARG, "kbeg_a map does not match the absorber layout (src/swpc_psv/m_global.f90:271-278)");
@@ -204,8 +280,21 @@ Model2D model_of(const swpc_ctx *c) {
     return m;
 }
 
+int update_stress_2d_kernel(swpc_ctx *c, int mask);
+int update_vel_2d_kernel(swpc_ctx *c, int mask);
+
 int update_stress_2d(swpc_ctx *c, int mask) {
-    const int m = (c->d.na > 0) ? mask : (mask & 1);
+    if (c->abc == 1) {
+        // Cerjan: the interior update over the whole domain, then the sponge
+        if (mask & 1) RC(update_stress_2d_kernel(c, 1));
+        if (mask & 2) RC(launch_cerjan2d(c, 0));
+        return SWPC_OK;
+    }
+    return update_stress_2d_kernel(c, mask);
+}
+
+int update_stress_2d_kernel(swpc_ctx *c, int mask) {
+    const int m = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     if (c->stress_tma)
         return cuda_check(c, launch_stress2d_tma(c->kind, c->d.nm, c->stress_tbi, &static_cast<Maps2D *>(c->maps2d)->str,
                                                  1, 0, c->d_model2d, c->d_tiles2d, c->ntiles2d, m,
@@ -216,7 +305,16 @@ int update_stress_2d(swpc_ctx *c, int mask) {
 }
 
 int update_vel_2d(swpc_ctx *c, int mask) {
-    const int m = (c->d.na > 0) ? mask : (mask & 1);
+    if (c->abc == 1) {
+        if (mask & 1) RC(update_vel_2d_kernel(c, 1));
+        if (mask & 2) RC(launch_cerjan2d(c, 1));
+        return SWPC_OK;
+    }
+    return update_vel_2d_kernel(c, mask);
+}
+
+int update_vel_2d_kernel(swpc_ctx *c, int mask) {
+    const int m = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     if (c->vel_tma)
         return cuda_check(c, launch_vel2d_tma(c->kind, c->vel_tbi, &static_cast<Maps2D *>(c->maps2d)->vel, 1, 0,
                                               c->d_model2d, c->d_tiles2d, c->ntiles2d, m, fields2d(c->kind, c->d.nm),
@@ -380,6 +478,7 @@ extern "C" int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **o
             return berr(b, SWPC_ERR_ARG, "batch members must share kind, nm and device");
         if (!c->medium_ready || !c->kernel_ready || (!c->absorb_ready && c->d.na > 0))
             return berr(b, SWPC_ERR_STATE, "batch member not fully set up");
+        if (c->abc != 0) return berr(b, SWPC_ERR_STATE, "batch members run with the PML");
         b->nt = std::min(b->nt, c->d.nt);
         if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) b->psv_bf_split = true;
     }

@@ -45,6 +45,7 @@ int wav_store_2d(swpc_ctx *c, int it, const int *d_it);
 int vmax_2d(swpc_ctx *c, float *out);
 void destroy_2d(swpc_ctx *c);
 int refresh_2d(swpc_ctx *c);
+int cerjan_setup_2d(swpc_ctx *c, const float *gx_c, const float *gx_b, const float *gz_c, const float *gz_b);
 
 }  // namespace swpc
 
@@ -601,13 +602,13 @@ extern "C" int swpc_absorb_setup(swpc_ctx *c, const float *gxc, const float *gxe
 extern "C" int swpc_absorb_setup_cerjan(swpc_ctx *c, const float *gx_c, const float *gx_b, const float *gy_c,
                                         const float *gy_b, const float *gz_c, const float *gz_b) {
     if (!c) return SWPC_ERR_ARG;
-    if (!is3d(c)) return set_err(c, SWPC_ERR_ARG, "the Cerjan sponge is implemented for the 3D code");
     if (c->prec != SWPC_PREC_F32) return set_err(c, SWPC_ERR_ARG, "the Cerjan sponge runs with FP32 storage");
     if (c->abc == 0 && c->absorb_ready)
         return set_err(c, SWPC_ERR_STATE, "the context already runs the PML (abc_type = 'pml')");
-    if (!gx_c || !gx_b || !gy_c || !gy_b || !gz_c || !gz_b) return set_err(c, SWPC_ERR_ARG, "sponge profile missing");
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
+    if (!is3d(c)) return cerjan_setup_2d(c, gx_c, gx_b, gz_c, gz_b);
+    if (!gx_c || !gx_b || !gy_c || !gy_b || !gz_c || !gz_b) return set_err(c, SWPC_ERR_ARG, "sponge profile missing");
     const Geo &g = c->g;
     const size_t n = 2 * (size_t)(g.nx + g.ny + g.nz);
     if (!c->cj) RC(dalloc(c, &c->cj, n));

@@ -81,8 +81,6 @@ class Swpc2D:
 
     def __init__(self, p: Params, kind: str = "psv", device: int = 0):
         p.check()
-        if p.abc_type != "pml":
-            raise ValueError("the 2D codes run with the PML (abc_type = 'pml')")
         self.p, self.kind = p, kind
         lib = self.lib = _lib.load()
         m = self.medium = Medium2D(p)
@@ -141,12 +139,23 @@ class Swpc2D:
                                              stf))
         self.M0, self.UC, self.fcut = float(M0), float(UC), float(fcut)
         g = grid2d(p)
-        self.gprof = {k: np.zeros((p.nx if k[1] == "x" else p.nz, 4), np.float32) for k in ("gxc", "gxe", "gzc", "gze")}
-        gp = self.gprof
-        lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]), None, None,
-                                  fptr(gp["gzc"]), fptr(gp["gze"]))
-        check(ctx, lib.swpc_absorb_setup(ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), None, None, fptr(gp["gzc"]),
-                                         fptr(gp["gze"])))
+        if p.abc_type == "cerjan":
+            # absorb_c__setup (src/swpc_psv/m_absorb_c.f90, src/swpc_sh/m_absorb_c.f90)
+            self.cprof = {k: np.zeros(p.nx if k[1] == "x" else p.nz, np.float32) for k in ("gx_c", "gx_b", "gz_c",
+                                                                                          "gz_b")}
+            cp = self.cprof
+            lib.swpc_cerjan_profiles(C.byref(g), fptr(cp["gx_c"]), fptr(cp["gx_b"]), None, None, fptr(cp["gz_c"]),
+                                     fptr(cp["gz_b"]))
+            check(ctx, lib.swpc_absorb_setup_cerjan(ctx, fptr(cp["gx_c"]), fptr(cp["gx_b"]), None, None,
+                                                    fptr(cp["gz_c"]), fptr(cp["gz_b"])))
+        else:
+            self.gprof = {k: np.zeros((p.nx if k[1] == "x" else p.nz, 4), np.float32)
+                          for k in ("gxc", "gxe", "gzc", "gze")}
+            gp = self.gprof
+            lib.swpc_damping_profiles(C.byref(g), float(f32(self.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]), None,
+                                      None, fptr(gp["gzc"]), fptr(gp["gze"]))
+            check(ctx, lib.swpc_absorb_setup(ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), None, None, fptr(gp["gzc"]),
+                                             fptr(gp["gze"])))
         # wav__setup / set_stinfo (src/swpc_psv/m_wav.f90:480-540)
         self.nst = 0
         what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u)

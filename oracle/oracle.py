@@ -355,6 +355,7 @@ def load2d(variant: str = "f32") -> C.CDLL:
         "o2d_medium_setup": (None, [vp, _FP, _FP, f, f, f]),
         "o2d_kernel_setup": (None, [vp]),
         "o2d_absorb_setup": (None, [vp, f]),
+        "o2d_cerjan_setup": (None, [vp]),
         "o2d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o2d_wav_setup": (i, [vp, i, _FP, _FP, _IP, i, i, i]),
         "o2d_step": (None, [vp, i]),
@@ -406,7 +407,10 @@ class Oracle2D:
         self._hold = [sx, sz, prm, mo, m6, f3]
         self.nsrc = lib.o2d_source_setup(self.o, int(p.bf_mode), n, _f(sx), _f(sz), _f(prm), _f(mo), _f(m6), _f(f3),
                                          STF[p.stftype])
-        lib.o2d_absorb_setup(self.o, self.scalars()["fcut"])
+        if getattr(p, "abc_type", "pml") == "cerjan":
+            lib.o2d_cerjan_setup(self.o)
+        else:
+            lib.o2d_absorb_setup(self.o, self.scalars()["fcut"])
         self.nst = 0
         if p.stations and (p.sw_wav_v or p.sw_wav_u):
             St = p.stations
@@ -449,6 +453,7 @@ class Oracle2D:
                ["axVy", "azVy", "axSxy", "azSyz"])
         for n, a in enumerate(aux):
             ids[a] = 60 + n
+        ids.update({"gx_c": 110, "gx_b": 111, "gz_c": 114, "gz_b": 115})
         return ids[name]
 
     def array(self, name: str) -> np.ndarray:
@@ -466,6 +471,8 @@ class Oracle2D:
             dt, shape = np.float32, (d["ni"], d["nk"])
         elif fid < 60:
             dt, shape = np.int32, (d["ni"],)
+        elif fid >= 110:
+            dt, shape = self.spr, (p.nx if fid < 114 else p.nz,)
         else:
             dt, shape = self.spr, (p.nx, d["nka"])
         n = int(np.prod(shape))

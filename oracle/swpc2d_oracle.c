@@ -61,6 +61,8 @@ typedef struct o2d {
     MPR r20x, r20z;
     int kbeg_min;
     long nka;
+    int cerjan;                  /* abc_type = 'cerjan' (m_absorb_c.f90) */
+    SPR *cgx_c, *cgx_b, *cgz_c, *cgz_b;   /* sponge factors, indexed [i - 1] */
     int bf_mode, stftype, nsrc;
     int *isrc, *ksrc;
     float *srcprm;
@@ -221,7 +223,8 @@ void o2d_destroy(o2d *o) {
                   o->kob, o->kfs_top, o->kfs_bot, o->kob_top, o->kob_bot, o->fgxc, o->fgxe, o->fgzc, o->fgze,
                   o->gxc, o->gxe, o->gzc, o->gze, o->aux[0], o->aux[1], o->aux[2], o->aux[3], o->aux[4], o->aux[5],
                   o->aux[6], o->aux[7], o->isrc, o->ksrc, o->srcprm, o->mo, o->mxx, o->mzz, o->mxz, o->myz,
-                  o->mxy, o->fx, o->fy, o->fz, o->ist, o->kst, o->wav_vel, o->wav_disp, o->ux, o->uz};
+                  o->mxy, o->fx, o->fy, o->fz, o->ist, o->kst, o->wav_vel, o->wav_disp, o->ux, o->uz,
+                  o->cgx_c, o->cgx_b, o->cgz_c, o->cgz_b};
     for (size_t n = 0; n < sizeof(ps) / sizeof(ps[0]); n++) free(ps[n]);
     free(o);
 }
@@ -492,7 +495,72 @@ static void psv_update_stress(o2d *o) {
         }
 }
 
+/* absorb_c__setup of the 2D codes (src/swpc_psv/m_absorb_c.f90:27-88,
+ * src/swpc_sh/m_absorb_c.f90:27-80) and the kernel region of abc_type =
+ * 'cerjan' (src/swpc_psv/m_global.f90:281-303: the whole domain) */
+static void cerjan_axis2d(SPR *gc, SPR *gb, int n, int na, float d, int low) {
+    const float alpha = 0.09f;
+    const float L = na * d;
+    for (int i = 1; i <= n; i++) {
+        float c = 1.0f, b = 1.0f;
+        if (low && i <= na) {
+            const float x = i2x(i, 0.0f, d);
+            const float yc = 1.0f - x / L, yb = 1.0f - (x + d / 2) / L;
+            c = expf(-alpha * (yc * yc));
+            b = expf(-alpha * (yb * yb));
+        } else if (i >= n - na + 1) {
+            const float x = i2x(i, n * d, -d);
+            const float yc = 1.0f - (x + d / 2) / L, yb = 1.0f - x / L;
+            c = expf(-alpha * (yc * yc));
+            b = expf(-alpha * (yb * yb));
+        }
+        gc[i - 1] = c;
+        gb[i - 1] = b;
+    }
+}
+
+void o2d_cerjan_setup(o2d *o) {
+    o->cerjan = 1;
+    o->cgx_c = (SPR *)zalloc(sizeof(SPR) * o->nx); o->cgx_b = (SPR *)zalloc(sizeof(SPR) * o->nx);
+    o->cgz_c = (SPR *)zalloc(sizeof(SPR) * o->nz); o->cgz_b = (SPR *)zalloc(sizeof(SPR) * o->nz);
+    cerjan_axis2d(o->cgx_c, o->cgx_b, o->nx, o->na, (float)o->dx, 1);
+    cerjan_axis2d(o->cgz_c, o->cgz_b, o->nz, o->na, (float)o->dz, 0);   /* free surface undamped */
+    o->ibeg_k = o->ibeg; o->iend_k = o->iend; o->kbeg_k = o->kbeg; o->kend_k = o->kend;
+}
+
+/* absorb_c__update_stress / _vel (src/swpc_psv/m_absorb_c.f90:90-160) */
+static void cerjan_psv(o2d *o, int stress) {
+    for (int i = o->ibeg; i <= o->iend; i++)
+        for (int k = o->kbeg; k <= o->kend; k++) {
+            const SPR xc = o->cgx_c[i - 1], xb = o->cgx_b[i - 1], zc = o->cgz_c[k - 1], zb = o->cgz_b[k - 1];
+            if (stress) {
+                const SPR gc = xc * zc, gb = xb * zb;
+                A(o->S[0], k, i) = A(o->S[0], k, i) * gc;
+                A(o->S[1], k, i) = A(o->S[1], k, i) * gc;
+                A(o->S[2], k, i) = A(o->S[2], k, i) * gb;
+            } else {
+                A(o->V[0], k, i) = A(o->V[0], k, i) * xb * zc;
+                A(o->V[1], k, i) = A(o->V[1], k, i) * xc * zb;
+            }
+        }
+}
+
+/* absorb_c__update_stress / _vel (src/swpc_sh/m_absorb_c.f90:82-135) */
+static void cerjan_sh(o2d *o, int stress) {
+    for (int i = o->ibeg; i <= o->iend; i++)
+        for (int k = o->kbeg; k <= o->kend; k++) {
+            const SPR xc = o->cgx_c[i - 1], xb = o->cgx_b[i - 1], zc = o->cgz_c[k - 1], zb = o->cgz_b[k - 1];
+            if (stress) {
+                A(o->S[0], k, i) = A(o->S[0], k, i) * xc * zb;
+                A(o->S[1], k, i) = A(o->S[1], k, i) * xb * zc;
+            } else {
+                A(o->V[0], k, i) = A(o->V[0], k, i) * xc * zc;
+            }
+        }
+}
+
 static void psv_absorb_vel(o2d *o) {
+    if (o->cerjan) { cerjan_psv(o, 0); return; }
     MPR *Vx = o->V[0], *Vz = o->V[1], *Sxx = o->S[0], *Szz = o->S[1], *Sxz = o->S[2];
     SPR *axSxx = o->aux[4], *azSxz = o->aux[5], *axSxz = o->aux[6], *azSzz = o->aux[7];
     float dt = o->dt;
@@ -517,6 +585,7 @@ static void psv_absorb_vel(o2d *o) {
 }
 
 static void psv_absorb_stress(o2d *o) {
+    if (o->cerjan) { cerjan_psv(o, 1); return; }
     MPR *Vx = o->V[0], *Vz = o->V[1];
     SPR *axVx = o->aux[0], *azVx = o->aux[1], *axVz = o->aux[2], *azVz = o->aux[3];
     float dt = o->dt;
@@ -597,6 +666,7 @@ static void sh_update_stress(o2d *o) {
 }
 
 static void sh_absorb_vel(o2d *o) {
+    if (o->cerjan) { cerjan_sh(o, 0); return; }
     MPR *Vy = o->V[0], *Syz = o->S[0], *Sxy = o->S[1];
     SPR *axSxy = o->aux[2], *azSyz = o->aux[3];
     float dt = o->dt;
@@ -614,6 +684,7 @@ static void sh_absorb_vel(o2d *o) {
 }
 
 static void sh_absorb_stress(o2d *o) {
+    if (o->cerjan) { cerjan_sh(o, 1); return; }
     MPR *Vy = o->V[0];
     SPR *axVy = o->aux[0], *azVy = o->aux[1];
     float dt = o->dt;
@@ -862,6 +933,7 @@ void *o2d_ptr(o2d *o, int id) {
     case 50: return o->kfs; case 51: return o->kob; case 52: return o->kfs_top; case 53: return o->kfs_bot;
     case 54: return o->kob_top; case 55: return o->kob_bot; case 56: return o->kbeg_a;
     case 80: return o->fgxc; case 81: return o->fgxe; case 82: return o->fgzc; case 83: return o->fgze;
+    case 110: return o->cgx_c; case 111: return o->cgx_b; case 114: return o->cgz_c; case 115: return o->cgz_b;
     case 90: return o->wav_vel; case 91: return o->wav_disp; case 95: return o->ist; case 96: return o->kst;
     case 98: return o->isrc; case 99: return o->ksrc;
     default: return 0;

@@ -11,10 +11,13 @@ import numpy as np
 import pytest
 
 from openswpc_b200 import _lib
-from openswpc_b200.adjoint import Misfit3D
-from openswpc_b200.swpc3d import ForceBatch3D, Swpc3D
-from oracle.oracle import Oracle3D
-from tests.models import small3d, vonkarman_xi
+from openswpc_b200.params import Source
+from openswpc_b200.swpc2d import Batch2D, Swpc2D
+from openswpc_b200.swpc3d import Swpc3D
+from oracle.oracle import Oracle2D, Oracle3D
+from tests.models import small2d, small3d, vonkarman_xi
+from tests.test_gpu_parity2d import compare as compare2d
+from tests.test_gpu_parity2d import set_launch as set_launch2d
 from tests.test_gpu_parity3d import compare_state, same_bits
 
 pytestmark = pytest.mark.gpu
@@ -66,3 +69,47 @@ def test_cerjan_context_refuses_pml_adjoint_and_batch():
 
     b = C.c_void_p()
     assert g.lib.swpc_fbatch_create(g.ctx, 2, C.byref(b)) == _lib.SWPC_ERR_STATE
+
+
+@pytest.mark.parametrize("launch", [(8, 8), (0, 0)], ids=["staged", "tiles"])
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_cerjan_2d_matches_oracle_bitwise(kind, launch):
+    """P-SV and SH with the sponge (src/swpc_psv/m_absorb_c.f90,
+    src/swpc_sh/m_absorb_c.f90): traces, fields, memory variables and the
+    vmax report over the whole-domain kernel region."""
+    p = small2d(kind, nt=100, abc_type="cerjan")
+    g = Swpc2D(p, kind)
+    set_launch2d(g, *launch)
+    o = Oracle2D(p, kind)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    for what, comp in ((_lib.WAV_V, "v"), (_lib.WAV_U, "u")):
+        a, b = g.waveforms(what), o.waveforms(comp)
+        assert np.linalg.norm(b) > 0, comp
+        assert same_bits(a, b), comp
+    compare2d(g, o, p)
+    vm = g.kernel__vmax()
+    assert same_bits(vm, o.vmax()[:len(vm)])
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_cerjan_2d_body_force(kind):
+    """Body forces with the sponge: P-SV applies them between the interior
+    update and the sponge, SH after the sponge, as the reference does."""
+    srcs = [Source(0.4, 0.0, 3.0, 0.0, 0.7, fx=1.0, fy=0.8, fz=-0.5),
+            Source(-13.9, 0.0, 1.0, 0.1, 0.6, fx=0.3, fy=1.0, fz=1.0)]
+    p = small2d(kind, nt=80, bf_mode=True, sources=srcs, abc_type="cerjan")
+    g = Swpc2D(p, kind)
+    o = Oracle2D(p, kind)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    assert np.linalg.norm(o.waveforms()) > 0
+    assert same_bits(g.waveforms(), o.waveforms())
+    compare2d(g, o, p)
+
+
+def test_cerjan_2d_member_refused_by_batch():
+    p = small2d("psv", nt=10, abc_type="cerjan")
+    g = Swpc2D(p, "psv")
+    with pytest.raises(Exception):
+        Batch2D([g])

@@ -227,3 +227,20 @@ def test_cerjan_profiles_match_oracle():
         assert np.array_equal(prof[k].view(np.uint32), b.astype(np.float32).view(np.uint32)), k
     assert np.all(prof["gz_c"][:p.na] == 1.0) and prof["gz_c"][-1] < 1.0
     assert prof["gx_c"][0] < prof["gx_c"][p.na - 1] < 1.0 and prof["gx_c"][p.na] == 1.0
+
+
+def test_cerjan_profiles_2d_match_oracle():
+    """The 2D sponge factors (gy omitted) against the 2D oracle, bitwise."""
+    from openswpc_b200 import _lib
+    from openswpc_b200.swpc2d import grid2d
+    from oracle.oracle import Oracle2D
+    from tests.models import small2d
+
+    p = small2d("psv", nt=2, abc_type="cerjan")
+    lib = _lib.load()
+    prof = {k: np.zeros(p.nx if k[1] == "x" else p.nz, np.float32) for k in ("gx_c", "gx_b", "gz_c", "gz_b")}
+    lib.swpc_cerjan_profiles(C.byref(grid2d(p)), _lib.fptr(prof["gx_c"]), _lib.fptr(prof["gx_b"]), None, None,
+                             _lib.fptr(prof["gz_c"]), _lib.fptr(prof["gz_b"]))
+    o = Oracle2D(p, "psv")
+    for k, v in prof.items():
+        assert np.array_equal(v.view(np.uint32), o.array(k).astype(np.float32).view(np.uint32)), k
