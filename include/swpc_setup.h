@@ -65,6 +65,12 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
                       const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by, float *bz,
                       float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
                       int *kob_top, int *kob_bot, float *ts, float *scal);
+/* The same with the input-file switch stabilize_pml (m_medium.f90:219-222,
+ * stabilize_absorber :276-340) applied before the averaged medium. */
+int swpc_setup_medium_opt(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                          float *mu, const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by,
+                          float *bz, float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top,
+                          int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal, int stabilize_pml);
 
 /* medium__setup of the 2D codes after the vmodel (src/swpc_psv/m_medium.f90:124-281,
  * src/swpc_sh/m_medium.f90): absorber homogenisation in x and at the bottom,

@@ -253,6 +253,69 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
                       const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by, float *bz,
                       float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
                       int *kob_top, int *kob_bot, float *ts, float *scal) {
+    return swpc_setup_medium_opt(g, fq_min, fq_max, fq_ref, rho, lam, mu, qp, qs, taup, taus, bx, by, bz, muyz, muxz,
+                                 muxy, kfs, kob, kfs_top, kfs_bot, kob_top, kob_bot, ts, scal, 0);
+}
+
+// stabilize_absorber (m_medium.f90:276-340): in each column around the
+// absorber, thin low-velocity layers (at most 20 cells) take the medium of
+// the cell above, then shear velocities below 0.4 vmax are raised to it
+// with vp = sqrt(3) vs
+static void stabilize_absorber(const swpc_grid *g, const Box &b, float *rho, float *lam, float *mu, float *taup,
+                               float *taus, float vmax) {
+    const float vmin_pml = vmax * 0.4f;
+    const int lv_thick = 20;
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    std::vector<int> ka((size_t)b.ni * b.nj);
+    swpc_kbeg_a(g, ka.data());
+    auto kstart = [&](int i, int j) {
+        int m = 1 << 30;
+        for (int jj = j - 2; jj <= j + 2; jj++)
+            for (int ii = i - 2; ii <= i + 2; ii++) m = std::min(m, ka[b.col(ii, jj)]);
+        return m;
+    };
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= ny + 1; j++)
+        for (int i = 0; i <= nx + 1; i++) {
+            int k = kstart(i, j);
+            while (k <= nz) {
+                const long e = b.idx(k, i, j), u = b.idx(k - 1, i, j);
+                if (lam[e] < lam[u] || mu[e] < mu[u]) {
+                    int k2 = k + 1;
+                    for (; k2 <= nz; k2++) {
+                        const long e2 = b.idx(k2, i, j), u2 = b.idx(k2 - 1, i, j);
+                        if (lam[e2] > lam[u2] || mu[e2] > mu[u2]) break;
+                    }
+                    if (k2 - k <= lv_thick) {
+                        rho[e] = rho[u]; lam[e] = lam[u]; mu[e] = mu[u]; taup[e] = taup[u]; taus[e] = taus[u];
+                        k = k2 - 1;
+                    }
+                }
+                k++;
+            }
+        }
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= ny + 1; j++)
+        for (int i = 0; i <= nx + 1; i++)
+            for (int k = kstart(i, j); k <= nz; k++) {
+                const long e = b.idx(k, i, j);
+                float vp = sqrtf((lam[e] + 2 * mu[e]) / rho[e]);
+                float vs = sqrtf(mu[e] / rho[e]);
+                if (vs < kEps) continue;   // ocean and air
+                const float gamma = sqrtf(3.0f);
+                if (vs < vmin_pml) {
+                    vs = vmin_pml;
+                    vp = vs * gamma;
+                    lam[e] = rho[e] * (vp * vp - 2 * (vs * vs));
+                    mu[e] = rho[e] * (vs * vs);
+                }
+            }
+}
+
+int swpc_setup_medium_opt(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                          float *mu, const float *qp, const float *qs, float *taup, float *taus, float *bx, float *by,
+                          float *bz, float *muyz, float *muxz, float *muxy, int *kfs, int *kob, int *kfs_top,
+                          int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal, int stabilize_pml) {
     if (g->ny <= 1) return SWPC_ERR_ARG;
     const Box b = make_box(g);
     const int nx = g->nx, ny = g->ny, nz = g->nz, na = g->na, nm = g->nm;
@@ -354,6 +417,8 @@ int swpc_setup_medium(const swpc_grid *g, float fq_min, float fq_max, float fq_r
                 if (vs < kEps) continue;
                 vmin1 = std::min(vmin1, vs);
             }
+    // stabilize_pml (m_medium.f90:219-222)
+    if (stabilize_pml) stabilize_absorber(g, b, rho, lam, mu, taup, taus, vmax1);
     // averaged_medium (m_medium.f90:432-465)
     memset(bx, 0, sizeof(float) * n3); memset(by, 0, sizeof(float) * n3); memset(bz, 0, sizeof(float) * n3);
     memset(muyz, 0, sizeof(float) * n3); memset(muxz, 0, sizeof(float) * n3); memset(muxy, 0, sizeof(float) * n3);

@@ -97,6 +97,7 @@ class Params:
     sw_wav_stress: bool = False
     sw_wav_strain: bool = False
     abc_type: str = "pml"
+    stabilize_pml: bool = False   # m_medium.f90:219-222 (3D)
     # snapshots (m_snap.f90:105-127): enabled planes as "<section>_<quantity>"
     # names (sections yz xz xy fs ob, quantities ps v u), e.g. {"xz_v", "fs_u"}
     snaps: set = field(default_factory=set)
@@ -185,7 +186,8 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
              "dt": float, "na": int, "xbeg": float, "ybeg": float, "zbeg": float, "tbeg": float, "fq_min": float,
              "fq_max": float, "fq_ref": float, "vcut": float, "rhomin": float, "stftype": str, "bf_mode": bool,
              "green_mode": bool, "green_cmp": str, "green_trise": float, "ntdec_r": int, "ntdec_w": int,
-             "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str}
+             "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str,
+             "stabilize_pml": bool}
     args = {}
     for key, typ in types.items():
         if key in kv:

@@ -207,12 +207,12 @@ class Medium:
         g = grid_struct(p)
         self.ts = np.zeros(3, np.float32)
         scal = np.zeros(3, np.float32)
-        rc = lib.swpc_setup_medium(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
-                                   fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup), fptr(self.taus),
-                                   fptr(self.bx), fptr(self.by), fptr(self.bz), fptr(self.muyz), fptr(self.muxz),
-                                   fptr(self.muxy), iptr(self.kfs), iptr(self.kob), iptr(self.kfs_top),
-                                   iptr(self.kfs_bot), iptr(self.kob_top), iptr(self.kob_bot), fptr(self.ts),
-                                   fptr(scal))
+        rc = lib.swpc_setup_medium_opt(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
+                                       fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup), fptr(self.taus),
+                                       fptr(self.bx), fptr(self.by), fptr(self.bz), fptr(self.muyz),
+                                       fptr(self.muxz), fptr(self.muxy), iptr(self.kfs), iptr(self.kob),
+                                       iptr(self.kfs_top), iptr(self.kfs_bot), iptr(self.kob_top),
+                                       iptr(self.kob_bot), fptr(self.ts), fptr(scal), int(p.stabilize_pml))
         if rc:
             raise ValueError("medium setup failed")
         self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
@@ -247,6 +247,8 @@ class DeviceMedium:
         L = p.layers
         if not L:
             raise ValueError("a layered (lhm) velocity model is required")
+        if p.stabilize_pml:
+            raise ValueError("stabilize_pml is applied by the host setup (Medium), not on the device")
         arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
         shape = (p.ny + 6, p.nx + 6, p.nz + 6)
         xp = None

@@ -66,6 +66,7 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_kernel_setup": (None, [vp]),
         "o3d_absorb_setup": (None, [vp, f]),
         "o3d_cerjan_setup": (None, [vp]),
+        "o3d_set_stabilize": (None, [vp, i]),
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
@@ -132,6 +133,7 @@ class Oracle3D:
             xi_c = None if xi is None else np.ascontiguousarray(xi, np.float32)
             lib.o3d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
                                _f(arr("qp")), _f(arr("qs")), p.vcut, _f(xi_c), p.rhomin, _f(qp), _f(qs))
+            lib.o3d_set_stabilize(self.o, int(getattr(p, "stabilize_pml", False)))
             lib.o3d_medium_setup(self.o, _f(qp), _f(qs), p.fq_min, p.fq_max, p.fq_ref)
         else:
             # externally prepared medium (e.g. to isolate the time step)

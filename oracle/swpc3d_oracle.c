@@ -89,6 +89,7 @@ typedef struct o3d {
     /* Cerjan sponge (m_absorb_c.f90:19-20), indexed [i - 1] */
     int cerjan;
     SPR *cgx_c, *cgx_b, *cgy_c, *cgy_b, *cgz_c, *cgz_b;
+    int stabilize_pml;          /* input-file switch (m_medium.f90:219) */
     long nka;                   /* PML aux k extent */
     /* sources (m_source.f90:26-36) */
     int bf_mode, stftype, nsrc;
@@ -582,6 +583,45 @@ void o3d_medium_setup(o3d *o, const float *qp, const float *qs, float fq_min, fl
             }
     o->vmax = vmax1;
     o->vmin = vmin1;
+    /* stabilize_absorber: m_medium.f90:219-222, 276-340 */
+    if (o->stabilize_pml) {
+        const float vmin_pml = vmax1 * 0.4f;
+        for (int j = o->jbeg - 1; j <= o->jend + 1; j++)
+            for (int i = o->ibeg - 1; i <= o->iend + 1; i++) {
+                int k0 = 1 << 30;
+                for (int jj = j - 2; jj <= j + 2; jj++)
+                    for (int ii = i - 2; ii <= i + 2; ii++)
+                        if (A2(o->kbeg_a, ii, jj) < k0) k0 = A2(o->kbeg_a, ii, jj);
+                int k = k0;
+                while (k <= o->kend) {
+                    long e = IDX3(o, k, i, j), u = IDX3(o, k - 1, i, j);
+                    if (lam[e] < lam[u] || mu[e] < mu[u]) {
+                        int k2;
+                        for (k2 = k + 1; k2 <= o->kend; k2++)
+                            if (A3(lam, k2, i, j) > A3(lam, k2 - 1, i, j) || A3(mu, k2, i, j) > A3(mu, k2 - 1, i, j))
+                                break;
+                        if (k2 - k <= 20) {
+                            rho[e] = rho[u]; lam[e] = lam[u]; mu[e] = mu[u]; taup[e] = taup[u]; taus[e] = taus[u];
+                            k = k2 - 1;
+                        }
+                    }
+                    k = k + 1;
+                }
+                for (k = k0; k <= o->kend; k++) {
+                    long e = IDX3(o, k, i, j);
+                    float vp = sqrtf((lam[e] + 2 * mu[e]) / rho[e]);
+                    float vs = sqrtf(mu[e] / rho[e]);
+                    if (vs < epsl) continue;
+                    float gamma = sqrtf(3.0f);
+                    if (vs < vmin_pml) {
+                        vs = vmin_pml;
+                        vp = vs * gamma;
+                        lam[e] = rho[e] * (vp * vp - 2 * (vs * vs));
+                        mu[e] = rho[e] * (vs * vs);
+                    }
+                }
+            }
+    }
     /* averaged_medium: m_medium.f90:432-465 */
     for (int j = o->jbeg; j <= o->jend; j++)
         for (int i = o->ibeg; i <= o->iend; i++)
@@ -881,6 +921,8 @@ static void cerjan_axis(SPR *gc, SPR *gb, int n, int na, float d, int low) {
         gb[i - 1] = b;
     }
 }
+
+void o3d_set_stabilize(o3d *o, int on) { o->stabilize_pml = on; }
 
 void o3d_cerjan_setup(o3d *o) {
     o->cerjan = 1;

@@ -359,3 +359,20 @@ def test_staged_kernels_with_fewer_memory_variables(nm):
     fields = list(range(9)) + [_lib.F_R + 3 * c + m for c in range(6) for m in range(nm)]
     for n in fields:
         assert same_bits(g0.download(n), g1.download(n)), n
+
+
+def test_stabilized_medium_run_matches_oracle():
+    """A run on a medium set up with stabilize_pml (a thin low-velocity layer
+    in the absorber) equals the oracle bitwise."""
+    from openswpc_b200.params import Layer
+    from tests.models import LAYERS
+
+    layers = [Layer(0.0, 2.2, 2.4, 1.2, 100, 50), Layer(1.0, 2.7, 5.5, 3.2, 300, 150),
+              Layer(3.0, 2.4, 3.0, 1.6, 100, 50), Layer(4.0, 2.7, 5.5, 3.2, 300, 150)] + LAYERS[1:]
+    p = small3d(nx=40, ny=36, nz=32, na=8, nt=30, layers=layers, stabilize_pml=True)
+    g = Swpc3D(p)
+    o = Oracle3D(p, threads=4)
+    g.run(1, p.nt)
+    o.run(1, p.nt)
+    assert same_bits(g.waveforms(), o.waveforms("v"))
+    compare_state(g, o, p)

@@ -244,3 +244,26 @@ def test_cerjan_profiles_2d_match_oracle():
     o = Oracle2D(p, "psv")
     for k, v in prof.items():
         assert np.array_equal(v.view(np.uint32), o.array(k).astype(np.float32).view(np.uint32)), k
+
+
+def test_stabilize_pml_matches_oracle():
+    """stabilize_pml (m_medium.f90:219-222, stabilize_absorber :276-340): a
+    thin low-velocity layer inside the absorber takes the medium above it and
+    slow cells are raised to 0.4 vmax, bitwise as the oracle; the interior
+    away from the absorber is untouched."""
+    from openswpc_b200.swpc3d import Medium
+    from tests.models import LAYERS, small3d
+
+    # a 1 km low-velocity layer at 3 km depth, and a slow top layer
+    layers = [Layer(0.0, 2.2, 2.4, 1.2, 100, 50), Layer(1.0, 2.7, 5.5, 3.2, 300, 150),
+              Layer(3.0, 2.4, 3.0, 1.6, 100, 50), Layer(4.0, 2.7, 5.5, 3.2, 300, 150)] + LAYERS[1:]
+    p = small3d(nx=40, ny=36, nz=32, na=8, nt=2, layers=layers, stabilize_pml=True)
+    q = small3d(nx=40, ny=36, nz=32, na=8, nt=2, layers=layers)
+    m, m0 = Medium(p), Medium(q)
+    o = Oracle3D(p)
+    for name in ("lam", "mu", "taup", "taus", "bx", "by", "bz", "muyz", "muxz", "muxy"):
+        b = o.array(name).astype(np.float32)
+        assert np.array_equal(getattr(m, name).view(np.uint32), b.view(np.uint32)), name
+    assert not np.array_equal(m.mu, m0.mu)                     # the switch acted
+    c = (slice(14, 26), slice(14, 30), slice(3, 20))           # columns away from the absorber
+    assert np.array_equal(m.mu[c], m0.mu[c])
