@@ -127,31 +127,36 @@ int cerjan_setup_2d(swpc_ctx *c, const float *gx_c, const float *gx_b, const flo
 
 // absorb_c__update_stress / _vel of P-SV (src/swpc_psv/m_absorb_c.f90:
 // 90-160) and SH (src/swpc_sh/m_absorb_c.f90:82-135) in the reference's
-// product order; cells with both factors 1 are skipped (same bits)
+// product order; cells with both factors 1 are not visited (same bits)
 __global__ void cerjan2d_kernel(int psv, int phase, int nx, int nz, int na, int Kp, const float *__restrict__ cj,
                                 float *f0, float *f1, float *f2) {
     const float *gxc = cj, *gxb = cj + nx, *gzc = cj + 2 * nx, *gzb = gzc + nz;
-    const long long n = (long long)nz * nx;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int k = 1 + (int)(q % nz), i = 1 + (int)(q / nz);
-        if (i > na && i <= nx - na && k <= nz - na) continue;
-        const long long e = (long long)(i + 2) * Kp + (k - 1 + KH);
-        const float xc = gxc[i - 1], xb = gxb[i - 1], zc = gzc[k - 1], zb = gzb[k - 1];
-        if (psv) {
-            if (phase == 0) {
-                const float gc = __fmul_rn(xc, zc), gb = __fmul_rn(xb, zb);
-                f0[e] = __fmul_rn(f0[e], gc);
-                f1[e] = __fmul_rn(f1[e], gc);
-                f2[e] = __fmul_rn(f2[e], gb);
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    // one warp per column, lanes along k: every k of the side columns, the
+    // bottom na cells of the others
+    for (int i = 1 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i <= nx; i += nw) {
+        const bool side = i <= na || i > nx - na;
+        const float xc = gxc[i - 1], xb = gxb[i - 1];
+        for (int k = (side ? 1 : nz - na + 1) + lane; k <= nz; k += 32) {
+            const long long e = (long long)(i + 2) * Kp + (k - 1 + KH);
+            const float zc = gzc[k - 1], zb = gzb[k - 1];
+            if (psv) {
+                if (phase == 0) {
+                    const float gc = __fmul_rn(xc, zc), gb = __fmul_rn(xb, zb);
+                    f0[e] = __fmul_rn(f0[e], gc);
+                    f1[e] = __fmul_rn(f1[e], gc);
+                    f2[e] = __fmul_rn(f2[e], gb);
+                } else {
+                    f0[e] = __fmul_rn(__fmul_rn(f0[e], xb), zc);
+                    f1[e] = __fmul_rn(__fmul_rn(f1[e], xc), zb);
+                }
+            } else if (phase == 0) {
+                f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zb);
+                f1[e] = __fmul_rn(__fmul_rn(f1[e], xb), zc);
             } else {
-                f0[e] = __fmul_rn(__fmul_rn(f0[e], xb), zc);
-                f1[e] = __fmul_rn(__fmul_rn(f1[e], xc), zb);
+                f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zc);
             }
-        } else if (phase == 0) {
-            f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zb);
-            f1[e] = __fmul_rn(__fmul_rn(f1[e], xb), zc);
-        } else {
-            f0[e] = __fmul_rn(__fmul_rn(f0[e], xc), zc);
         }
     }
 }

@@ -629,32 +629,37 @@ extern "C" int swpc_absorb_setup_cerjan(swpc_ctx *c, const float *gx_c, const fl
 
 // absorb_c__update_stress / absorb_c__update_vel (m_absorb_c.f90:105-198):
 // each field times the factors of its staggered position, after the
-// interior update.  Cells whose factors are all 1 (inside the sponge-free
-// box) are skipped: a product with 1 leaves the bits unchanged.
+// interior update.  Only the sponge is visited, one warp per column with
+// lanes along k: every k of the side columns, the bottom na cells of the
+// others.  The cells skipped have all factors 1, and a product with 1
+// leaves the bits unchanged.
 __global__ void cerjan3d_kernel(Geo g, int na, int phase, const float *__restrict__ cj, float *f0, float *f1,
                                 float *f2, float *f3, float *f4, float *f5) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const float *gxc = cj, *gxb = cj + nx, *gyc = cj + 2 * nx, *gyb = gyc + ny, *gzc = gyc + 2 * ny, *gzb = gzc + nz;
-    const long long n = (long long)nz * nx * ny;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int k = 1 + (int)(q % nz);
-        const long long r = q / nz;
-        const int i = 1 + (int)(r % nx), j = 1 + (int)(r / nx);
-        if (i > na && i <= nx - na && j > na && j <= ny - na && k <= nz - na) continue;
-        const long long e = cell_index(g, k, i, j);
-        const float xc = gxc[i - 1], xb = gxb[i - 1], yc = gyc[j - 1], yb = gyb[j - 1], zc = gzc[k - 1], zb = gzb[k - 1];
-        if (phase == 0) {
-            const float gcc = __fmul_rn(__fmul_rn(xc, yc), zc);
-            f0[e] = __fmul_rn(f0[e], gcc);
-            f1[e] = __fmul_rn(f1[e], gcc);
-            f2[e] = __fmul_rn(f2[e], gcc);
-            f3[e] = __fmul_rn(__fmul_rn(__fmul_rn(f3[e], xc), yb), zb);
-            f4[e] = __fmul_rn(__fmul_rn(__fmul_rn(f4[e], xb), yc), zb);
-            f5[e] = __fmul_rn(__fmul_rn(__fmul_rn(f5[e], xb), yb), zc);
-        } else {
-            f0[e] = __fmul_rn(__fmul_rn(__fmul_rn(f0[e], xb), yc), zc);
-            f1[e] = __fmul_rn(__fmul_rn(__fmul_rn(f1[e], xc), yb), zc);
-            f2[e] = __fmul_rn(__fmul_rn(__fmul_rn(f2[e], xc), yc), zb);
+    const int lane = threadIdx.x & 31;
+    const long long ncol = (long long)nx * ny;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < ncol; w += nw) {
+        const int i = 1 + (int)(w % nx), j = 1 + (int)(w / nx);
+        const bool side = i <= na || i > nx - na || j <= na || j > ny - na;
+        const float xc = gxc[i - 1], xb = gxb[i - 1], yc = gyc[j - 1], yb = gyb[j - 1];
+        for (int k = (side ? 1 : nz - na + 1) + lane; k <= nz; k += 32) {
+            const long long e = cell_index(g, k, i, j);
+            const float zc = gzc[k - 1], zb = gzb[k - 1];
+            if (phase == 0) {
+                const float gcc = __fmul_rn(__fmul_rn(xc, yc), zc);
+                f0[e] = __fmul_rn(f0[e], gcc);
+                f1[e] = __fmul_rn(f1[e], gcc);
+                f2[e] = __fmul_rn(f2[e], gcc);
+                f3[e] = __fmul_rn(__fmul_rn(__fmul_rn(f3[e], xc), yb), zb);
+                f4[e] = __fmul_rn(__fmul_rn(__fmul_rn(f4[e], xb), yc), zb);
+                f5[e] = __fmul_rn(__fmul_rn(__fmul_rn(f5[e], xb), yb), zc);
+            } else {
+                f0[e] = __fmul_rn(__fmul_rn(__fmul_rn(f0[e], xb), yc), zc);
+                f1[e] = __fmul_rn(__fmul_rn(__fmul_rn(f1[e], xc), yb), zc);
+                f2[e] = __fmul_rn(__fmul_rn(__fmul_rn(f2[e], xc), yc), zb);
+            }
         }
     }
 }
