@@ -219,6 +219,22 @@ int swpc_bodyforce_setup(swpc_ctx *ctx, int nsrc, const int *isrc, const int *js
 int swpc_green_setup(swpc_ctx *ctx, int isrc, int jsrc, int ksrc, char cmp, float green_tbeg, float green_trise,
                      int stftype);
 
+/* green__store (src/swpc_3d/m_green.f90:389-534): the reciprocity Green's
+ * functions at ng grid points (ig, jg, kg in 1..n; the cells of the green
+ * table after green__setup's grid assignment).  Each step integrates the
+ * nine velocity derivatives (and with bforce the velocities) and every
+ * ntdec_w steps samples them into gf(ntw, ncmp*ng), ncmp = 6 (mxx myy mzz
+ * myz mxz mxy) or 9 (+ fx fy fz), in the reference's units.  The reference
+ * never calls green__store from its main loop; swpc_step and swpc_run call
+ * it beside wav__store once this setup has run, and swpc_green_store runs
+ * it alone.  swpc_green_fetch copies gf out (column-major, as the reference
+ * holds it; green__export's sign flip for green_cmp = 'z' stays with the
+ * caller).  FP32 storage. */
+int swpc_green_store_setup(swpc_ctx *ctx, int ng, const int *ig, const int *jg, const int *kg, int bforce,
+                           int ntdec_w);
+int swpc_green_store(swpc_ctx *ctx, int it);
+int swpc_green_fetch(swpc_ctx *ctx, float *gf);
+
 /* wav__setup / set_stinfo (src/swpc_3d/m_wav.f90:76-142, 144-274): station
  * cells, decimation, and output scaling M0, UC; what = OR of SWPC_WAV_*. */
 int swpc_wav_setup(swpc_ctx *ctx, int nst, const int *ist, const int *jst, const int *kst, int ntdec_w,

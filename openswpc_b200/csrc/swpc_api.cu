@@ -207,6 +207,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
     invalidate_graph(c);
     snap_free(c);
     adj_free(c);
+    green_free(c);
     if (!is3d(c)) destroy_2d(c);
     if (c->slab) {
         // the slabs hold V, S, R and the medium fields
@@ -1225,6 +1226,7 @@ extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(
 // by the caller between steps)
 static int step_body(swpc_ctx *c, int it, const int *d_it) {
     RC(launch_wav(c, it, d_it));
+    RC(green_store_launch(c, it, d_it));
     RC(snap_launch(c, it, d_it));
     RC(launch_stress(c, 3));
     RC(launch_glut(c, it, d_it));

@@ -133,6 +133,12 @@ struct swpc_ctx {
     swpc_snap_state *snp = nullptr;
     // adjoint state and checkpoints (swpc_adjoint.cu)
     swpc_adj_state *adj = nullptr;
+    // green__store points (swpc_green.cu): ng grid points, accumulated
+    // displacement derivatives (and displacements) and the sampled output
+    int ng = 0, ng_cmp = 0, ng_ntw = 0, ng_ntdec = 1;
+    int *g_ijk = nullptr;     // (3, ng)
+    float *g_acc = nullptr;   // (12, ng): dxUx dxUy dxUz dyUx dyUy dyUz dzUx dzUy dzUz ux uy uz
+    float *g_out = nullptr;   // gf(ntw, ncmp*ng), column-major as the reference
 
     // vmax
     unsigned int *vmax_buf = nullptr;
@@ -196,6 +202,8 @@ int set_err(swpc_ctx *c, int code, const std::string &msg);
 int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
 void adj_free(swpc_ctx *c);   // swpc_adjoint.cu
+int green_store_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_green.cu
+void green_free(swpc_ctx *c);
 int field_storage(const swpc_ctx *c, int field);   // swpc_prec.cu
 float field_scale(const swpc_ctx *c, int field);
 int prec_to_f32(swpc_ctx *c, int field, const float *stored, float **tmp);

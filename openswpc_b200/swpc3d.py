@@ -522,6 +522,22 @@ class Swpc3D:
         check(self.ctx, self.lib.swpc_sync(self.ctx))
 
     # -- data ---------------------------------------------------------------
+    def green_store_setup(self, ig, jg, kg, bforce: bool = False, ntdec_w: int = 1):
+        """green__store (m_green.f90:389-534) at the grid cells (ig, jg, kg):
+        reciprocity Green's functions sampled every ntdec_w steps."""
+        ip = lambda a: np.ascontiguousarray(a, np.int32)
+        self._green = (ip(ig), ip(jg), ip(kg), 9 if bforce else 6, (self.p.nt - 1) // ntdec_w + 1)
+        g = self._green
+        check(self.ctx, self.lib.swpc_green_store_setup(self.ctx, len(g[0]), *(iptr(a) for a in g[:3]),
+                                                        int(bforce), ntdec_w))
+
+    def green_functions(self) -> np.ndarray:
+        """gf(ntw, ncmp*ng) (column-major, as the reference) as (ncmp*ng, ntw)."""
+        ig, _, _, ncmp, ntw = self._green
+        out = np.zeros((ncmp * len(ig), ntw), np.float32)
+        check(self.ctx, self.lib.swpc_green_fetch(self.ctx, fptr(out)))
+        return out
+
     def download(self, field: int) -> np.ndarray:
         p = self.p
         out = np.zeros((p.ny + 6, p.nx + 6, p.nz + 6), np.float32)

@@ -67,6 +67,7 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_absorb_setup": (None, [vp, f]),
         "o3d_cerjan_setup": (None, [vp]),
         "o3d_set_stabilize": (None, [vp, i]),
+        "o3d_green_store_setup": (None, [vp, i, _IP, _IP, _IP, i, i]),
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
@@ -265,6 +266,22 @@ class Oracle3D:
         n = int(np.prod(shape))
         buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
         return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+    def green_store_setup(self, ig, jg, kg, bforce: bool = False, ntdec_w: int = 1):
+        """green__store (m_green.f90:389-534) at the given grid cells; o3d_step
+        then calls it beside wav__store."""
+        ip = lambda a: np.ascontiguousarray(a, np.int32)
+        self._green = (ip(ig), ip(jg), ip(kg), 9 if bforce else 6, (self.p.nt - 1) // ntdec_w + 1)
+        g = self._green
+        self.lib.o3d_green_store_setup(self.o, len(g[0]), *(a.ctypes.data_as(_IP) for a in g[:3]), int(bforce),
+                                       ntdec_w)
+
+    def green_functions(self) -> np.ndarray:
+        """gf(ntw, ncmp*ng) as the reference holds it, returned as (ncmp*ng, ntw)."""
+        ig, _, _, ncmp, ntw = self._green
+        n = ncmp * len(ig) * ntw
+        buf = (C.c_float * n).from_address(self.lib.o3d_ptr(self.o, 120))
+        return np.frombuffer(buf, dtype=np.float32).reshape(ncmp * len(ig), ntw).copy()
 
     def waveforms(self, comp: str = "v") -> np.ndarray:
         d = self.dims()

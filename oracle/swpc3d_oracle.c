@@ -90,6 +90,11 @@ typedef struct o3d {
     int cerjan;
     SPR *cgx_c, *cgx_b, *cgy_c, *cgy_b, *cgz_c, *cgz_b;
     int stabilize_pml;          /* input-file switch (m_medium.f90:219) */
+    /* green__store (m_green.f90:389-534) */
+    int ng, ng_cmp, ng_ntw, ng_ntdec;
+    int *gi, *gj, *gk;
+    float *gacc;                /* (12, ng) */
+    float *gf;                  /* gf(ntw, ncmp*ng), column-major */
     long nka;                   /* PML aux k extent */
     /* sources (m_source.f90:26-36) */
     int bf_mode, stftype, nsrc;
@@ -374,7 +379,7 @@ void o3d_destroy(o3d *o) {
                   o->mo, o->mxx, o->myy, o->mzz, o->myz, o->mxz, o->mxy, o->fx, o->fy, o->fz, o->ist, o->jst,
                   o->kst, o->wav_vel, o->wav_disp, o->wav_stress, o->wav_strain, o->ux, o->uy, o->uz,
                   o->exx, o->eyy, o->ezz, o->eyz, o->exz, o->exy, o->cgx_c, o->cgx_b, o->cgy_c, o->cgy_b,
-                  o->cgz_c, o->cgz_b};
+                  o->cgz_c, o->cgz_b, o->gi, o->gj, o->gk, o->gacc, o->gf};
     for (size_t n = 0; n < sizeof(ps) / sizeof(ps[0]); n++) free(ps[n]);
     for (int q = 0; q < 15; q++) { free(o->snp[q]); free(o->sbuf[q]); }
     for (int q = 0; q < 4; q++) free(o->maxv[q]);
@@ -1568,8 +1573,82 @@ float *o3d_snap_frames(o3d *o, int plane) { return (plane >= 0 && plane < 15) ? 
 float *o3d_snap_max(o3d *o, int which) { return (which >= 0 && which < 4) ? o->maxv[which] : 0; }
 
 /* one pass of the main.f90:125-144 loop body (report__progress excluded) */
+/* green__store: m_green.f90:389-534 (green table points given as grid cells) */
+void o3d_green_store_setup(o3d *o, int ng, const int *ig, const int *jg, const int *kg, int bforce, int ntdec) {
+    o->ng = ng;
+    o->ng_cmp = bforce ? 9 : 6;
+    o->ng_ntdec = ntdec;
+    o->ng_ntw = (o->nt - 1) / ntdec + 1;
+    o->gi = (int *)zalloc(sizeof(int) * ng); o->gj = (int *)zalloc(sizeof(int) * ng); o->gk = (int *)zalloc(sizeof(int) * ng);
+    for (int n = 0; n < ng; n++) { o->gi[n] = ig[n]; o->gj[n] = jg[n]; o->gk[n] = kg[n]; }
+    o->gacc = (float *)zalloc(sizeof(float) * 12 * (size_t)ng);
+    o->gf = (float *)zalloc(sizeof(float) * (size_t)o->ng_ntw * o->ng_cmp * ng);
+}
+
+void o3d_green_store(o3d *o, int it) {
+    if (o->ng <= 0) return;
+    const MPR r40x = (MPR)(9.0 / 8.0) / o->dx, r40y = (MPR)(9.0 / 8.0) / o->dy, r40z = (MPR)(9.0 / 8.0) / o->dz;
+    const MPR r41x = (MPR)(1.0 / 24.0) / o->dx, r41y = (MPR)(1.0 / 24.0) / o->dy, r41z = (MPR)(1.0 / 24.0) / o->dz;
+    const float dt = o->dt;
+    MPR *Vx = o->Vx, *Vy = o->Vy, *Vz = o->Vz;
+    const int ng = o->ng;
+#define V_(f, k, i, j) A3(f, k, i, j)
+#define DF(f, k, i, j, dk, di, dj, r0, r1)                                                                 \
+    ((V_(f, (k) + (dk), (i) + (di), (j) + (dj)) - V_(f, k, i, j)) * (r0) -                                 \
+     (V_(f, (k) + 2 * (dk), (i) + 2 * (di), (j) + 2 * (dj)) - V_(f, (k) - (dk), (i) - (di), (j) - (dj))) * (r1))
+#define DB(f, k, i, j, dk, di, dj, r0, r1)                                                                 \
+    ((V_(f, k, i, j) - V_(f, (k) - (dk), (i) - (di), (j) - (dj))) * (r0) -                                 \
+     (V_(f, (k) + (dk), (i) + (di), (j) + (dj)) - V_(f, (k) - 2 * (dk), (i) - 2 * (di), (j) - 2 * (dj))) * (r1))
+    for (int n = 0; n < ng; n++) {
+        const int ii = o->gi[n], jj = o->gj[n], kk = o->gk[n];
+        MPR dxVx = DB(Vx, kk, ii, jj, 0, 1, 0, r40x, r41x);
+        MPR dyVy = DB(Vy, kk, ii, jj, 0, 0, 1, r40y, r41y);
+        MPR dzVz = DB(Vz, kk, ii, jj, 1, 0, 0, r40z, r41z);
+        MPR dxVy = (DF(Vy, kk, ii, jj, 0, 1, 0, r40x, r41x) + DF(Vy, kk, ii, jj - 1, 0, 1, 0, r40x, r41x) +
+                    DB(Vy, kk, ii, jj, 0, 1, 0, r40x, r41x) + DB(Vy, kk, ii, jj - 1, 0, 1, 0, r40x, r41x)) * 0.25f;
+        MPR dxVz = (DF(Vz, kk, ii, jj, 0, 1, 0, r40x, r41x) + DF(Vz, kk - 1, ii, jj, 0, 1, 0, r40x, r41x) +
+                    DB(Vz, kk, ii, jj, 0, 1, 0, r40x, r41x) + DB(Vz, kk - 1, ii, jj, 0, 1, 0, r40x, r41x)) * 0.25f;
+        MPR dyVx = (DF(Vx, kk, ii, jj, 0, 0, 1, r40y, r41y) + DF(Vx, kk, ii - 1, jj, 0, 0, 1, r40y, r41y) +
+                    DB(Vx, kk, ii, jj, 0, 0, 1, r40y, r41y) + DB(Vx, kk, ii - 1, jj, 0, 0, 1, r40y, r41y)) * 0.25f;
+        MPR dyVz = (DF(Vz, kk, ii, jj, 0, 0, 1, r40y, r41y) + DF(Vz, kk - 1, ii, jj, 0, 0, 1, r40y, r41y) +
+                    DB(Vz, kk, ii, jj, 0, 0, 1, r40y, r41y) + DB(Vz, kk - 1, ii, jj, 0, 0, 1, r40y, r41y)) * 0.25f;
+        MPR dzVx = (DF(Vx, kk, ii, jj, 1, 0, 0, r40z, r41z) + DF(Vx, kk, ii - 1, jj, 1, 0, 0, r40z, r41z) +
+                    DB(Vx, kk, ii, jj, 1, 0, 0, r40z, r41z) + DB(Vx, kk, ii - 1, jj, 1, 0, 0, r40z, r41z)) * 0.25f;
+        MPR dzVy = (DF(Vy, kk, ii, jj, 1, 0, 0, r40z, r41z) + DF(Vy, kk, ii, jj - 1, 1, 0, 0, r40z, r41z) +
+                    DB(Vy, kk, ii, jj, 1, 0, 0, r40z, r41z) + DB(Vy, kk, ii, jj - 1, 1, 0, 0, r40z, r41z)) * 0.25f;
+        const MPR d[9] = {dxVx, dxVy, dxVz, dyVx, dyVy, dyVz, dzVx, dzVy, dzVz};
+        for (int q = 0; q < 9; q++) o->gacc[q * ng + n] = o->gacc[q * ng + n] + (float)(d[q] * dt);
+        if (o->ng_cmp == 9) {
+            o->gacc[9 * ng + n] = o->gacc[9 * ng + n] + 0.5f * (float)(V_(Vx, kk, ii, jj) + V_(Vx, kk, ii - 1, jj)) * dt;
+            o->gacc[10 * ng + n] = o->gacc[10 * ng + n] + 0.5f * (float)(V_(Vy, kk, ii, jj) + V_(Vy, kk, ii, jj - 1)) * dt;
+            o->gacc[11 * ng + n] = o->gacc[11 * ng + n] + 0.5f * (float)(V_(Vz, kk, ii, jj) + V_(Vz, kk - 1, ii, jj)) * dt;
+        }
+    }
+#undef DF
+#undef DB
+#undef V_
+    if ((it - 1) % o->ng_ntdec != 0) return;
+    const int itw = (it - 1) / o->ng_ntdec + 1;
+    if (itw > o->ng_ntw) return;
+    const float uc = 1e-15f, ub = 1e-12f;   /* UC_DERIV, UC_BF (m_green.f90:31-32) */
+    for (int n = 0; n < ng; n++) {
+        const float *u = o->gacc;
+        float *g = o->gf + (size_t)n * o->ng_cmp * o->ng_ntw + (itw - 1);
+        const long w = o->ng_ntw;
+        g[0 * w] = u[0 * ng + n] * uc * 1e9f;
+        g[1 * w] = u[4 * ng + n] * uc * 1e9f;
+        g[2 * w] = u[8 * ng + n] * uc * 1e9f;
+        g[3 * w] = (u[5 * ng + n] + u[7 * ng + n]) * uc * 1e9f;
+        g[4 * w] = (u[2 * ng + n] + u[6 * ng + n]) * uc * 1e9f;
+        g[5 * w] = (u[1 * ng + n] + u[3 * ng + n]) * uc * 1e9f;
+        if (o->ng_cmp == 9)
+            for (int q = 0; q < 3; q++) g[(6 + q) * w] = u[(9 + q) * ng + n] * ub * 1e9f;
+    }
+}
+
 void o3d_step(o3d *o, int it) {
     o3d_wav_store(o, it);
+    o3d_green_store(o, it);
     o3d_snap_write(o, it);
     o3d_update_stress(o);
     o3d_absorb_update_stress(o);
@@ -1632,6 +1711,7 @@ void *o3d_ptr(o3d *o, int id) {
     case 93: return o->wav_strain;
     case 95: return o->ist; case 96: return o->jst; case 97: return o->kst;
     case 98: return o->isrc; case 99: return o->jsrc; case 100: return o->ksrc;
+    case 120: return o->gf;
     case 110: return o->cgx_c; case 111: return o->cgx_b; case 112: return o->cgy_c;
     case 113: return o->cgy_b; case 114: return o->cgz_c; case 115: return o->cgz_b;
     default: return 0;
