@@ -388,6 +388,9 @@ int swpc_fbatch_time_steps(swpc_fbatch *b, int it0, int nsteps, float *ms);
 int swpc_fbatch_sync(swpc_fbatch *b);
 int swpc_fbatch_wav_fetch(swpc_fbatch *b, int member, int what, float *out);
 int swpc_fbatch_download_field(swpc_fbatch *b, int member, int field, float *out, int ld_k, int ld_i);
+/* green__store of one member: the context's green table (set up before
+ * swpc_fbatch_create) is recorded for every member; gf as swpc_green_fetch. */
+int swpc_fbatch_green_fetch(swpc_fbatch *b, int member, float *gf);
 long long swpc_fbatch_device_bytes(const swpc_fbatch *b);
 
 /* ---- snapshots (3D) ------------------------------------------------------ */

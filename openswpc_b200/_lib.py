@@ -37,7 +37,7 @@ WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 EXPORTS = [
     "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
     "swpc_vmodel_lhm_device", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_absorb_setup_cerjan",
-    "swpc_green_store_setup", "swpc_green_store", "swpc_green_fetch",
+    "swpc_green_store_setup", "swpc_green_store", "swpc_green_fetch", "swpc_fbatch_green_fetch",
     "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
     "swpc_absorb_update_vel", "swpc_update_stress", "swpc_update_vel", "swpc_source_stressglut",
@@ -140,6 +140,7 @@ def load():
         "swpc_green_store_setup": (i, [vp, i, _IP, _IP, _IP, i, i]),
         "swpc_green_store": (i, [vp, i]),
         "swpc_green_fetch": (i, [vp, _FP]),
+        "swpc_fbatch_green_fetch": (i, [vp, i, _FP]),
         "swpc_cerjan_profiles": (None, [C.POINTER(Grid), _FP, _FP, _FP, _FP, _FP, _FP]),
         "swpc_source_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, _FP, i]),
         "swpc_bodyforce_setup": (i, [vp, i, _IP, _IP, _IP, _FP, _FP, i]),

@@ -203,6 +203,10 @@ int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
 void adj_free(swpc_ctx *c);   // swpc_adjoint.cu
 int green_store_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_green.cu
+// the same for nmem wavefields at V[q] + m * vstride (reciprocity batch), with
+// per-member accumulators (12 ng each) and outputs (ntw ncmp ng each)
+int green_store_members(swpc_ctx *c, float *const *V, long long vstride, int nmem, float *acc, float *out, int it,
+                        const int *d_it);
 void green_free(swpc_ctx *c);
 int field_storage(const swpc_ctx *c, int field);   // swpc_prec.cu
 float field_scale(const swpc_ctx *c, int field);

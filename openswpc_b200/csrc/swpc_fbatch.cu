@@ -50,6 +50,9 @@ struct swpc_fbatch {
     float *V[3] = {}, *S[6] = {}, *R[18] = {}, *aux[18] = {};   // member 0 (V, S, R inside the slab)
     float *wav[4] = {};            // per kind: nmem blocks of (nst, ncmp, ntw)
     float *uacc = nullptr, *eacc = nullptr;
+    // green__store of every member at the context's green table (when set up)
+    float *g_acc = nullptr, *g_out = nullptr;
+    int g_ng = 0;
     // green sources: entries tagged with their member, forces per member
     std::vector<std::vector<InjEntry>> h_inj;
     std::vector<float> h_prm;      // (2, nmem) tbeg, trise
@@ -186,7 +189,7 @@ static void fb_free(swpc_fbatch *b) {
     for (auto p : b->aux) f(p);
     delete static_cast<TmaMaps *>(b->tmaps);
     for (auto p : b->wav) f(p);
-    f(b->uacc); f(b->eacc); f(b->inj); f(b->inj_mem); f(b->stf); f(b->d_it);
+    f(b->uacc); f(b->eacc); f(b->inj); f(b->inj_mem); f(b->stf); f(b->d_it); f(b->g_acc); f(b->g_out);
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->c) b->c->bytes -= b->bytes;
 }
@@ -225,6 +228,12 @@ extern "C" int swpc_fbatch_create(swpc_ctx *c, int nmem, swpc_fbatch **out) {
     if (!rc) rc = falloc(b, &b->uacc, (size_t)3 * nst * nmem);
     if (!rc) rc = falloc(b, &b->eacc, (size_t)6 * nst * nmem);
     if (!rc) rc = falloc(b, &b->d_it, 1);
+    if (!rc && c->ng > 0) {
+        // green__store for every member at the context's green table
+        b->g_ng = c->ng;
+        rc = falloc(b, &b->g_acc, (size_t)12 * c->ng * nmem);
+        if (!rc) rc = falloc(b, &b->g_out, (size_t)c->ng_ntw * c->ng_cmp * c->ng * nmem);
+    }
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     if (rc) {
         fb_free(b);
@@ -396,6 +405,11 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
             wav3d_batch_kernel<<<dim3((c->nst + 127) / 128, b->nmem), 128, 0, c->stream>>>(a, b->stride, 3, 6);
             FCK(cudaGetLastError());
         }
+    }
+    // green__store beside wav__store, as the context's step
+    if (b->g_ng > 0) {
+        if (c->ng != b->g_ng) return ferr(b, SWPC_ERR_STATE, "the context's green table changed after the batch");
+        FRC(green_store_members(c, b->V, b->stride, b->nmem, b->g_acc, b->g_out, it, d_it));
     }
     const int mask = c->d.na > 0 ? 3 : 1;
     // stress (kernel__update_stress + absorb_p__update_stress)
@@ -637,6 +651,18 @@ extern "C" int swpc_fbatch_download_field(swpc_fbatch *b, int member, int field,
     FCK(cudaSetDevice(b->c->device));
     FCK(cudaStreamSynchronize(b->c->stream));
     return copy_box(b->c, base + b->stride * member, nullptr, out, ld_k, ld_i);
+}
+
+extern "C" int swpc_fbatch_green_fetch(swpc_fbatch *b, int member, float *out) {
+    if (!b || !out) return SWPC_ERR_ARG;
+    swpc_ctx *c = b->c;
+    if (member < 0 || member >= b->nmem) return ferr(b, SWPC_ERR_ARG, "member index out of range");
+    if (b->g_ng <= 0) return ferr(b, SWPC_ERR_STATE, "the context had no green table when the batch was created");
+    FCK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->ng_ntw * c->ng_cmp * b->g_ng;
+    FCK(cudaMemcpyAsync(out, b->g_out + n * member, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    FCK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
 }
 
 extern "C" long long swpc_fbatch_device_bytes(const swpc_fbatch *b) { return b ? b->bytes : 0; }

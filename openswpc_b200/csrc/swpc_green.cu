@@ -35,6 +35,7 @@ struct GreenArgs {
     int ng, ncmp, ntw, ntdec, it;
     const int *d_it;
     float r40[3], r41[3], dt;
+    long long vstride;   // field offset of member blockIdx.y (reciprocity batch; 0 for a context)
 };
 
 // (f(+0) - f(-1)) * r40 - (f(+1) - f(-2)) * r41 along stride P from e
@@ -57,7 +58,9 @@ __global__ void green_store_kernel(const GreenArgs a) {
     const Geo &g = a.g;
     const long long PK = 1, PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
     const long long e = cell_index(g, a.ijk[3 * n + 2], a.ijk[3 * n], a.ijk[3 * n + 1]);
-    const float *Vx = a.Vx, *Vy = a.Vy, *Vz = a.Vz;
+    const long long mo = (long long)blockIdx.y * a.vstride;
+    const float *Vx = a.Vx + mo, *Vy = a.Vy + mo, *Vz = a.Vz + mo;
+    float *const acc = a.acc + (long long)blockIdx.y * 12 * a.ng;
     const float rx0 = a.r40[0], rx1 = a.r41[0], ry0 = a.r40[1], ry1 = a.r41[1], rz0 = a.r40[2], rz1 = a.r41[2];
     // m_green.f90:449-487
     const float dxVx = dbwd(Vx, e, PI, rx0, rx1);
@@ -80,16 +83,16 @@ __global__ void green_store_kernel(const GreenArgs a) {
     const int ng = a.ng;
 #pragma unroll
     for (int q = 0; q < 9; q++) {
-        u[q] = __fadd_rn(a.acc[q * ng + n], __fmul_rn(d[q], a.dt));
-        a.acc[q * ng + n] = u[q];
+        u[q] = __fadd_rn(acc[q * ng + n], __fmul_rn(d[q], a.dt));
+        acc[q * ng + n] = u[q];
     }
     if (a.ncmp == 9) {
         // m_green.f90:499-503
         const float v3[3] = {__fadd_rn(Vx[e], Vx[e - PI]), __fadd_rn(Vy[e], Vy[e - PJ]), __fadd_rn(Vz[e], Vz[e - PK])};
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            u[9 + q] = __fadd_rn(a.acc[(9 + q) * ng + n], __fmul_rn(__fmul_rn(0.5f, v3[q]), a.dt));
-            a.acc[(9 + q) * ng + n] = u[9 + q];
+            u[9 + q] = __fadd_rn(acc[(9 + q) * ng + n], __fmul_rn(__fmul_rn(0.5f, v3[q]), a.dt));
+            acc[(9 + q) * ng + n] = u[9 + q];
         }
     }
     if ((it - 1) % a.ntdec != 0) return;
@@ -98,7 +101,7 @@ __global__ void green_store_kernel(const GreenArgs a) {
     // m_green.f90:506-526; column (n-1)*ncmp + j of gf(ntw, ncmp*ng)
     const float uc = 1e-15f, ub = 1e-12f;
     const float g6[6] = {u[0], u[4], u[8], __fadd_rn(u[5], u[7]), __fadd_rn(u[2], u[6]), __fadd_rn(u[1], u[3])};
-    float *o = a.out + (long long)n * a.ncmp * a.ntw + (itw - 1);
+    float *o = a.out + ((long long)blockIdx.y * a.ng + n) * a.ncmp * a.ntw + (itw - 1);
 #pragma unroll
     for (int j = 0; j < 6; j++) o[(long long)j * a.ntw] = __fmul_rn(__fmul_rn(g6[j], uc), 1e9f);
     if (a.ncmp == 9)
@@ -109,17 +112,23 @@ __global__ void green_store_kernel(const GreenArgs a) {
 
 namespace swpc {
 
-int green_store_launch(swpc_ctx *c, int it, const int *d_it) {
+int green_store_members(swpc_ctx *c, float *const *V, long long vstride, int nmem, float *acc, float *out, int it,
+                        const int *d_it) {
     if (c->ng <= 0) return SWPC_OK;
     GreenArgs a;
     a.g = c->g;
-    a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
-    a.ijk = c->g_ijk; a.acc = c->g_acc; a.out = c->g_out;
+    a.Vx = V[0]; a.Vy = V[1]; a.Vz = V[2];
+    a.ijk = c->g_ijk; a.acc = acc; a.out = out;
     a.ng = c->ng; a.ncmp = c->ng_cmp; a.ntw = c->ng_ntw; a.ntdec = c->ng_ntdec; a.it = it; a.d_it = d_it;
     for (int q = 0; q < 3; q++) { a.r40[q] = c->r40[q]; a.r41[q] = c->r41[q]; }
     a.dt = c->d.dt;
-    green_store_kernel<<<(c->ng + 127) / 128, 128, 0, c->stream>>>(a);
+    a.vstride = vstride;
+    green_store_kernel<<<dim3((c->ng + 127) / 128, nmem), 128, 0, c->stream>>>(a);
     return cuda_check(c, cudaGetLastError(), "green_store launch");
+}
+
+int green_store_launch(swpc_ctx *c, int it, const int *d_it) {
+    return green_store_members(c, c->V, 0, 1, c->g_acc, c->g_out, it, d_it);
 }
 
 void green_free(swpc_ctx *c) {

@@ -660,6 +660,14 @@ class ForceBatch3D:
         check(base.ctx, self.lib.swpc_fbatch_wav_fetch(self.b, member, what, fptr(out)))
         return out
 
+    def green_functions(self, member: int) -> np.ndarray:
+        """green__store of one member at the base context's green table
+        (``Swpc3D.green_store_setup`` before the batch), as (ncmp*ng, ntw)."""
+        ig, _, _, ncmp, ntw = self.base._green
+        out = np.zeros((ncmp * len(ig), ntw), np.float32)
+        check(self.base.ctx, self.lib.swpc_fbatch_green_fetch(self.b, member, fptr(out)))
+        return out
+
     def download(self, member: int, field: int) -> np.ndarray:
         p = self.base.p
         out = np.zeros((p.ny + 6, p.nx + 6, p.nz + 6), np.float32)

@@ -6,7 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from openswpc_b200.swpc3d import Swpc3D
+from openswpc_b200.swpc3d import ForceBatch3D, Swpc3D, station_grid
 from oracle.oracle import Oracle3D
 from tests.models import small3d, vonkarman_xi
 from tests.test_gpu_parity3d import same_bits
@@ -53,3 +53,31 @@ def test_green_store_per_step_calls_equal_graph():
     for it in range(1, p.nt + 1):
         g1.step(it)
     assert same_bits(g0.green_functions(), g1.green_functions())
+
+
+def test_reciprocity_batch_members_store_their_green_functions():
+    """Every member of a reciprocity batch records green__store at the
+    context's green table, bitwise as a green-mode run of its own force."""
+    p = small3d(nx=44, ny=40, nz=32, na=8, nt=30, green_mode=True, green_trise=1.2, green_cmp="x",
+                green_station=0, sources=[])
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    ig, jg, kg = green_table(p, n=16, seed=7)
+    base = Swpc3D(p, xi)
+    # and the cells right below the force stations, which the waves reach at once
+    si, sj, sk = station_grid(p, base.medium.kfs, base.medium.kob)
+    ig, jg, kg = np.r_[ig, si], np.r_[jg, sj], np.r_[kg, np.minimum(sk + 1, p.nz)]
+    base.green_store_setup(ig, jg, kg, bforce=True, ntdec_w=2)
+    forces = [(0, "x"), (2, "z"), (3, "y")]
+    fb = ForceBatch3D(base, [(p.stations[s], c) for s, c in forces])
+    fb.run(1, p.nt)
+    for m, (s, c) in enumerate(forces):
+        q = small3d(nx=44, ny=40, nz=32, na=8, nt=30, green_mode=True, green_trise=1.2, green_cmp=c,
+                    green_station=s, sources=[])
+        g = Swpc3D(q, xi)
+        g.green_store_setup(ig, jg, kg, bforce=True, ntdec_w=2)
+        g.run(1, q.nt)
+        a, b = fb.green_functions(m), g.green_functions()
+        assert np.abs(b).max() > 0
+        assert same_bits(a, b), f"member {m}"
+        g.close()
+    fb.close()
