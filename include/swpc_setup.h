@@ -83,6 +83,12 @@ int swpc_setup_medium_opt(const swpc_grid *g, float fq_min, float fq_max, float 
 int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
                          float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs, int *kob,
                          int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal);
+/* The same with stabilize_pml (src/swpc_psv/m_medium.f90:175-178, 309-365)
+ * applied last. */
+int swpc_setup_medium_2d_opt(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                             float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs,
+                             int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts,
+                             float *scal, int stabilize_pml);
 
 /* damping_profile (src/swpc_3d/m_absorb_p.f90:507-547) for the six profiles
  * of absorb_p__setup (:79-93); each output is g(4, n). */

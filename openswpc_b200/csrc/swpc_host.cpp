@@ -468,6 +468,14 @@ static float visco_chi(int nm, const float *ts, float tau, float f) {
 int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
                          float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs, int *kob,
                          int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts, float *scal) {
+    return swpc_setup_medium_2d_opt(g, fq_min, fq_max, fq_ref, rho, lam, mu, qp, qs, taup, taus, kfs, kob, kfs_top,
+                                    kfs_bot, kob_top, kob_bot, ts, scal, 0);
+}
+
+int swpc_setup_medium_2d_opt(const swpc_grid *g, float fq_min, float fq_max, float fq_ref, float *rho, float *lam,
+                             float *mu, const float *qp, const float *qs, float *taup, float *taus, int *kfs,
+                             int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, float *ts,
+                             float *scal, int stabilize_pml) {
     const int nx = g->nx, nz = g->nz, na = g->na, nm = g->nm;
     const long nk = nz + 6, ni = nx + 6;
     auto id = [&](int k, int i) { return (long)(i + 2) * nk + (k + 2); };
@@ -527,6 +535,48 @@ int swpc_setup_medium_2d(const swpc_grid *g, float fq_min, float fq_max, float f
             vmin1 = std::min(vmin1, vs);
         }
     scal[0] = zeta; scal[1] = vmin1; scal[2] = vmax1;
+    if (stabilize_pml) {
+        // stabilize_absorber of the 2D codes (src/swpc_psv/m_medium.f90:309-365,
+        // src/swpc_sh/m_medium.f90:301-357): unlike the 3D routine, a thin
+        // low-velocity layer takes the medium above it over its whole thickness
+        std::vector<int> ka((size_t)ni);
+        swpc_kbeg_a(g, ka.data());
+        const float vmin_pml = vmax1 * 0.4f;
+        for (int i = 0; i <= nx + 1; i++) {
+            int k0 = 1 << 30;
+            for (int ii = i - 2; ii <= i + 2; ii++) k0 = std::min(k0, ka[ii + 2]);
+            int k = k0;
+            while (k <= nz) {
+                if (lam[id(k, i)] < lam[id(k - 1, i)] || mu[id(k, i)] < mu[id(k - 1, i)]) {
+                    int k2 = k + 1;
+                    for (; k2 <= nz; k2++)
+                        if (lam[id(k2, i)] > lam[id(k2 - 1, i)] || mu[id(k2, i)] > mu[id(k2 - 1, i)]) break;
+                    if (k2 - k <= 20) {
+                        const long u = id(k - 1, i);
+                        for (int kk = k; kk <= k2 - 1; kk++) {
+                            const long e = id(kk, i);
+                            rho[e] = rho[u]; lam[e] = lam[u]; mu[e] = mu[u]; taup[e] = taup[u]; taus[e] = taus[u];
+                        }
+                        k = k2 - 1;
+                    }
+                }
+                k++;
+            }
+            for (k = k0; k <= nz; k++) {
+                const long e = id(k, i);
+                float vp = sqrtf((lam[e] + 2 * mu[e]) / rho[e]);
+                float vs = sqrtf(mu[e] / rho[e]);
+                if (vs < kEps) continue;
+                const float gamma = sqrtf(3.0f);
+                if (vs < vmin_pml) {
+                    vs = vmin_pml;
+                    vp = vs * gamma;
+                    lam[e] = rho[e] * (vp * vp - 2 * (vs * vs));
+                    mu[e] = rho[e] * (vs * vs);
+                }
+            }
+        }
+    }
     return SWPC_OK;
 }
 

@@ -54,11 +54,11 @@ class Medium2D:
             raise ValueError("vmodel_lhm failed")
         self.ts = np.zeros(3, np.float32)
         scal = np.zeros(3, np.float32)
-        rc = lib.swpc_setup_medium_2d(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
-                                      fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup),
-                                      fptr(self.taus), iptr(self.kfs), iptr(self.kob), iptr(self.kfs_top),
-                                      iptr(self.kfs_bot), iptr(self.kob_top), iptr(self.kob_bot), fptr(self.ts),
-                                      fptr(scal))
+        rc = lib.swpc_setup_medium_2d_opt(C.byref(g), p.fq_min, p.fq_max, p.fq_ref, fptr(self.rho), fptr(self.lam),
+                                          fptr(self.mu), fptr(self.qp), fptr(self.qs), fptr(self.taup),
+                                          fptr(self.taus), iptr(self.kfs), iptr(self.kob), iptr(self.kfs_top),
+                                          iptr(self.kfs_bot), iptr(self.kob_top), iptr(self.kob_bot),
+                                          fptr(self.ts), fptr(scal), int(p.stabilize_pml))
         if rc:
             raise ValueError("2D medium setup failed")
         self.zeta, self.vmin, self.vmax = (float(x) for x in scal)

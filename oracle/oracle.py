@@ -375,6 +375,7 @@ def load2d(variant: str = "f32") -> C.CDLL:
         "o2d_kernel_setup": (None, [vp]),
         "o2d_absorb_setup": (None, [vp, f]),
         "o2d_cerjan_setup": (None, [vp]),
+        "o2d_set_stabilize": (None, [vp, i]),
         "o2d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o2d_wav_setup": (i, [vp, i, _FP, _FP, _IP, i, i, i]),
         "o2d_step": (None, [vp, i]),
@@ -413,6 +414,7 @@ class Oracle2D:
         qs = np.zeros(shape, np.float32)
         lib.o2d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
                            _f(arr("qp")), _f(arr("qs")), p.vcut, None, p.rhomin, _f(qp), _f(qs))
+        lib.o2d_set_stabilize(self.o, int(getattr(p, "stabilize_pml", False)))
         lib.o2d_medium_setup(self.o, _f(qp), _f(qs), p.fq_min, p.fq_max, p.fq_ref)
         lib.o2d_kernel_setup(self.o)
         S = p.sources

@@ -62,6 +62,7 @@ typedef struct o2d {
     int kbeg_min;
     long nka;
     int cerjan;                  /* abc_type = 'cerjan' (m_absorb_c.f90) */
+    int stabilize_pml;           /* input-file switch (src/swpc_psv/m_medium.f90:175) */
     SPR *cgx_c, *cgx_b, *cgz_c, *cgz_b;   /* sponge factors, indexed [i - 1] */
     int bf_mode, stftype, nsrc;
     int *isrc, *ksrc;
@@ -346,6 +347,44 @@ void o2d_medium_setup(o2d *o, const float *qp, const float *qs, float fq_min, fl
             if (vs < vmin1) vmin1 = vs;
         }
     o->vmax = vmax1; o->vmin = vmin1;
+    /* stabilize_absorber: src/swpc_psv/m_medium.f90:175-178, 309-365 */
+    if (o->stabilize_pml) {
+        const float vmin_pml = vmax1 * 0.4f;
+        for (int i = o->ibeg - 1; i <= o->iend + 1; i++) {
+            int k0 = 1 << 30;
+            for (int ii = i - 2; ii <= i + 2; ii++)
+                if (o->kbeg_a[IM(o, ii)] < k0) k0 = o->kbeg_a[IM(o, ii)];
+            int k = k0;
+            while (k <= o->kend) {
+                if (A(lam, k, i) < A(lam, k - 1, i) || A(mu, k, i) < A(mu, k - 1, i)) {
+                    int k2;
+                    for (k2 = k + 1; k2 <= o->kend; k2++)
+                        if (A(lam, k2, i) > A(lam, k2 - 1, i) || A(mu, k2, i) > A(mu, k2 - 1, i)) break;
+                    if (k2 - k <= 20) {
+                        for (int kk = k; kk <= k2 - 1; kk++) {
+                            A(rho, kk, i) = A(rho, k - 1, i); A(lam, kk, i) = A(lam, k - 1, i);
+                            A(mu, kk, i) = A(mu, k - 1, i); A(taup, kk, i) = A(taup, k - 1, i);
+                            A(taus, kk, i) = A(taus, k - 1, i);
+                        }
+                        k = k2 - 1;
+                    }
+                }
+                k = k + 1;
+            }
+            for (k = k0; k <= o->kend; k++) {
+                float vp = sqrtf((A(lam, k, i) + 2 * A(mu, k, i)) / A(rho, k, i));
+                float vs = sqrtf(A(mu, k, i) / A(rho, k, i));
+                if (vs < EPSL) continue;
+                float gamma = sqrtf(3.0f);
+                if (vs < vmin_pml) {
+                    vs = vmin_pml;
+                    vp = vs * gamma;
+                    A(lam, k, i) = A(rho, k, i) * (vp * vp - 2 * (vs * vs));
+                    A(mu, k, i) = A(rho, k, i) * (vs * vs);
+                }
+            }
+        }
+    }
     for (long e = 0; e < n2; e++) {
         o->rho[e] = (SPR)rho[e]; o->lam[e] = (SPR)lam[e]; o->mu[e] = (SPR)mu[e];
         o->taup[e] = (SPR)taup[e]; o->taus[e] = (SPR)taus[e];
@@ -518,6 +557,8 @@ static void cerjan_axis2d(SPR *gc, SPR *gb, int n, int na, float d, int low) {
         gb[i - 1] = b;
     }
 }
+
+void o2d_set_stabilize(o2d *o, int on) { o->stabilize_pml = on; }
 
 void o2d_cerjan_setup(o2d *o) {
     o->cerjan = 1;

@@ -267,3 +267,23 @@ def test_stabilize_pml_matches_oracle():
     assert not np.array_equal(m.mu, m0.mu)                     # the switch acted
     c = (slice(14, 26), slice(14, 30), slice(3, 20))           # columns away from the absorber
     assert np.array_equal(m.mu[c], m0.mu[c])
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_stabilize_pml_2d_matches_oracle(kind):
+    """The 2D stabilize_absorber (src/swpc_psv/m_medium.f90:309-365), which
+    fills the whole thin low-velocity layer, bitwise as the oracle."""
+    from openswpc_b200.swpc2d import Medium2D
+    from oracle.oracle import Oracle2D
+    from tests.models import LAYERS, small2d
+
+    layers = [Layer(0.0, 2.2, 2.4, 1.2, 100, 50), Layer(1.0, 2.7, 5.5, 3.2, 300, 150),
+              Layer(3.0, 2.4, 3.0, 1.6, 100, 50), Layer(4.0, 2.7, 5.5, 3.2, 300, 150)] + LAYERS[1:]
+    p = small2d(kind, nt=2, layers=layers, stabilize_pml=True)
+    q = small2d(kind, nt=2, layers=layers)
+    m, m0 = Medium2D(p), Medium2D(q)
+    o = Oracle2D(p, kind)
+    for name in ("rho", "lam", "mu", "taup", "taus"):
+        b = o.array(name).astype(np.float32)
+        assert np.array_equal(getattr(m, name).view(np.uint32), b.view(np.uint32)), name
+    assert not np.array_equal(m.mu, m0.mu)
