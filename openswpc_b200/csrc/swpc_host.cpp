@@ -498,15 +498,26 @@ int swpc_setup_medium_2d_opt(const swpc_grid *g, float fq_min, float fq_max, flo
     }
     if (nm > 0)
 #pragma omp parallel for schedule(static)
-        for (int i = -2; i <= nx + 3; i++)
+        for (int i = -2; i <= nx + 3; i++) {
+            // chi is a function of tau alone, and a column holds runs of equal
+            // tau (layers): reuse the last value of each (same bits)
+            float ls = 0.0f, lp = 0.0f, cs = 0.0f, cp = 0.0f;
+            bool hs = false, hp = false;
             for (int k = -2; k <= nz + 3; k++) {
                 const long e = id(k, i);
                 const float rb2 = mu[e], ra2 = lam[e] + 2 * mu[e];
-                const float cm = visco_chi(nm, ts, taus[e], fq_ref);
+                if (!hs || memcmp(&ls, &taus[e], sizeof(float)) != 0) {
+                    ls = taus[e]; cs = visco_chi(nm, ts, ls, fq_ref); hs = true;
+                }
+                const float cm = cs;
                 mu[e] = rb2 / (cm * cm);
-                const float cl = visco_chi(nm, ts, taup[e], fq_ref);
+                if (!hp || memcmp(&lp, &taup[e], sizeof(float)) != 0) {
+                    lp = taup[e]; cp = visco_chi(nm, ts, lp, fq_ref); hp = true;
+                }
+                const float cl = cp;
                 lam[e] = ra2 / (cl * cl) - 2 * mu[e];
             }
+        }
     for (int i = -2; i <= nx + 3; i++) { kfs[i + 2] = 0; kob[i + 2] = 0; kfs_top[i + 2] = kfs_bot[i + 2] = kob_top[i + 2] = kob_bot[i + 2] = 0; }
     for (int i = 0; i <= nx + 2; i++)
         for (int k = 1; k <= nz - 1; k++) {
