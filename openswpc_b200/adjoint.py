@@ -25,6 +25,17 @@ from .params import Params
 from .swpc3d import Medium, Swpc3D
 
 
+class _MediumMaps:
+    """Integer maps, relaxation times and velocity range of a medium built in
+    HBM (what the host keeps of it)."""
+
+    def __init__(self, p: Params):
+        for n in Medium.MAPS:
+            setattr(self, n, np.zeros((p.ny + 6, p.nx + 6), np.int32))
+        self.ts = np.zeros(3, np.float32)
+        self.scal = np.zeros(3, np.float32)
+
+
 class Misfit3D:
     """A 3D run with its sources, stations and Q fixed, evaluated for any
     per-cell (vp, vs, rho) against observed velocity traces ``obs`` of shape
@@ -48,10 +59,27 @@ class Misfit3D:
     def close(self):
         self.solver.close()
 
-    def _set_model(self, vp, vs, rho) -> Medium:
-        s = self.solver
-        m = Medium.from_model(self.p, vp, vs, rho, self.qp, self.qs)
-        check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view(average_on_device=True))))
+    def _set_model(self, vp, vs, rho):
+        """The medium of per-cell vp, vs, rho: the moduli formed as
+        vmodel_lhm forms them (m_vmodel_lhm.f90:158-160, FP32), then
+        medium__setup in HBM (swpc_vmodel_upload, swpc_medium_setup_device;
+        bitwise the host setup of ``Medium.from_model``)."""
+        s, p = self.solver, self.p
+        if p.stabilize_pml:
+            m = Medium.from_model(p, vp, vs, rho, self.qp, self.qs)
+            check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view(average_on_device=True))))
+            s.medium = m
+            return m
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        f = lambda a: np.ascontiguousarray(a, np.float32).reshape(shape)
+        vp, vs, rho = f(vp), f(vs), f(rho)
+        mu = rho * vs * vs
+        lam = rho * (vp * vp - 2 * vs * vs)
+        check(s.ctx, s.lib.swpc_vmodel_upload(s.ctx, fptr(rho), fptr(lam), fptr(mu), fptr(self.qp), fptr(self.qs),
+                                              p.nz + 6, p.nx + 6))
+        m = _MediumMaps(p)
+        check(s.ctx, s.lib.swpc_medium_setup_device(s.ctx, p.fq_min, p.fq_max, p.fq_ref, fptr(m.ts), fptr(m.scal),
+                                                    *(_lib.iptr(getattr(m, n)) for n in Medium.MAPS), p.nx + 6))
         s.medium = m
         return m
 
