@@ -139,6 +139,7 @@ struct swpc_ctx {
     int *g_ijk = nullptr;     // (3, ng)
     float *g_acc = nullptr;   // (12, ng): dxUx dxUy dxUz dyUx dyUy dyUz dzUx dzUy dzUz ux uy uz
     float *g_out = nullptr;   // gf(ntw, ncmp*ng), column-major as the reference
+    long long g_bytes = 0;    // device bytes of the three arrays (counted in `bytes`)
 
     // vmax
     unsigned int *vmax_buf = nullptr;

@@ -136,6 +136,8 @@ void green_free(swpc_ctx *c) {
     if (c->g_acc) cudaFree(c->g_acc);
     if (c->g_out) cudaFree(c->g_out);
     c->g_ijk = nullptr; c->g_acc = nullptr; c->g_out = nullptr;
+    c->bytes -= c->g_bytes;
+    c->g_bytes = 0;
     c->ng = 0;
 }
 
@@ -165,9 +167,11 @@ extern "C" int swpc_green_store_setup(swpc_ctx *c, int ng, const int *ig, const 
     if (ng == 0) return SWPC_OK;
     const int ncmp = bforce ? 9 : 6;
     const int ntw = (c->d.nt - 1) / ntdec_w + 1;   // m_green.f90 ntw as m_wav.f90
+    const long long before = c->bytes;
     int rc = dalloc(c, &c->g_ijk, 3 * (size_t)ng);
     if (!rc) rc = dalloc(c, &c->g_acc, 12 * (size_t)ng);
     if (!rc) rc = dalloc(c, &c->g_out, (size_t)ntw * ncmp * ng);
+    c->g_bytes = c->bytes - before;
     if (!rc) rc = cuda_check(c, cudaMemcpyAsync(c->g_ijk, ijk.data(), 3 * (size_t)ng * sizeof(int),
                                                 cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");

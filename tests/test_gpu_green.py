@@ -81,3 +81,17 @@ def test_reciprocity_batch_members_store_their_green_functions():
         assert same_bits(a, b), f"member {m}"
         g.close()
     fb.close()
+
+
+def test_green_store_device_bytes_are_returned_on_reset():
+    """A second setup frees the first table's arrays: swpc_device_bytes comes
+    back to its value before the first setup when the table is cleared."""
+    p = small3d(nt=10, green_mode=True, green_cmp="z", green_trise=1.0, green_station=0, sources=[])
+    g = Swpc3D(p)
+    b0 = g.lib.swpc_device_bytes(g.ctx)
+    ig, jg, kg = green_table(p, n=8)
+    g.green_store_setup(ig, jg, kg, bforce=True)
+    g.green_store_setup(ig, jg, kg)
+    assert g.lib.swpc_device_bytes(g.ctx) > b0
+    g.green_store_setup([], [], [])
+    assert g.lib.swpc_device_bytes(g.ctx) == b0
