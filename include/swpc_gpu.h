@@ -195,8 +195,9 @@ int swpc_absorb_setup(swpc_ctx *ctx, const float *gxc, const float *gxe, const f
  * interior update then covers the whole domain (m_global.f90:349-378) and
  * the absorber updates multiply by the factors (m_absorb_c.f90:105-198).
  * FP32 storage.  The 2D codes pass gy_c = gy_b = NULL
- * (src/swpc_psv/m_absorb_c.f90, src/swpc_sh/m_absorb_c.f90).  The adjoint,
- * the reciprocity batch and the 2D batch refuse such a context. */
+ * (src/swpc_psv/m_absorb_c.f90, src/swpc_sh/m_absorb_c.f90); a 2D batch
+ * applies the sponge of such members after each batched update.  The adjoint
+ * and the reciprocity batch refuse such a context. */
 int swpc_absorb_setup_cerjan(swpc_ctx *ctx, const float *gx_c, const float *gx_b, const float *gy_c,
                              const float *gy_b, const float *gz_c, const float *gz_b);
 

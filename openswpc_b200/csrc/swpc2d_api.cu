@@ -161,7 +161,7 @@ __global__ void cerjan2d_kernel(int psv, int phase, int nx, int nz, int na, int 
     }
 }
 
-static int launch_cerjan2d(swpc_ctx *c, int phase) {
+static int launch_cerjan2d(swpc_ctx *c, int phase, cudaStream_t stream) {
     const bool psv = c->kind == SWPC_KIND_PSV;
     float *f0, *f1 = nullptr, *f2 = nullptr;
     if (phase == 0) {
@@ -172,8 +172,8 @@ static int launch_cerjan2d(swpc_ctx *c, int phase) {
         f0 = psv ? c->V[0] : c->V[1];
         f1 = psv ? c->V[2] : nullptr;
     }
-    cerjan2d_kernel<<<148 * 4, 256, 0, c->stream>>>(psv ? 1 : 0, phase, c->g.nx, c->g.nz, c->d.na, c->g.Kp, c->cj, f0,
-                                                     f1, f2);
+    cerjan2d_kernel<<<148 * 4, 256, 0, stream>>>(psv ? 1 : 0, phase, c->g.nx, c->g.nz, c->d.na, c->g.Kp, c->cj, f0,
+                                                  f1, f2);
     return cuda_check(c, cudaGetLastError(), "cerjan2d launch");
 }
 
@@ -292,7 +292,7 @@ int update_stress_2d(swpc_ctx *c, int mask) {
     if (c->abc == 1) {
         // Cerjan: the interior update over the whole domain, then the sponge
         if (mask & 1) RC(update_stress_2d_kernel(c, 1));
-        if (mask & 2) RC(launch_cerjan2d(c, 0));
+        if (mask & 2) RC(launch_cerjan2d(c, 0, c->stream));
         return SWPC_OK;
     }
     return update_stress_2d_kernel(c, mask);
@@ -312,7 +312,7 @@ int update_stress_2d_kernel(swpc_ctx *c, int mask) {
 int update_vel_2d(swpc_ctx *c, int mask) {
     if (c->abc == 1) {
         if (mask & 1) RC(update_vel_2d_kernel(c, 1));
-        if (mask & 2) RC(launch_cerjan2d(c, 1));
+        if (mask & 2) RC(launch_cerjan2d(c, 1, c->stream));
         return SWPC_OK;
     }
     return update_vel_2d_kernel(c, mask);
@@ -483,7 +483,6 @@ extern "C" int swpc_batch_create(swpc_ctx *const *members, int n, swpc_batch **o
             return berr(b, SWPC_ERR_ARG, "batch members must share kind, nm and device");
         if (!c->medium_ready || !c->kernel_ready || (!c->absorb_ready && c->d.na > 0))
             return berr(b, SWPC_ERR_STATE, "batch member not fully set up");
-        if (c->abc != 0) return berr(b, SWPC_ERR_STATE, "batch members run with the PML");
         b->nt = std::min(b->nt, c->d.nt);
         if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) b->psv_bf_split = true;
     }
@@ -577,8 +576,19 @@ static int batch_step(swpc_batch *b, int it, const int *d_it) {
         }
         return cudaSuccess;
     };
+    // the Cerjan sponge of the members that run it (absorb__update_*), after
+    // the batched update of the phase; their tiles hold no PML cells
+    auto sponge = [&](int phase) {
+        for (auto *c : b->members)
+            if (c->abc == 1) {
+                const int rc = launch_cerjan2d(c, phase, b->stream);
+                if (rc) return rc;
+            }
+        return (int)SWPC_OK;
+    };
     launch_wav2d(b->d_wav, nwav, b->max_nst, it, d_it, b->stream);
     BCK(stress(mask_all));
+    RC(sponge(0));
     launch_inject_multi(b->d_inj, b->ninj, max_inj_n, d_it, it, b->stream);
     if (b->kind == SWPC_KIND_PSV && b->psv_bf_split) {
         // P-SV applies body forces between the interior and absorber velocity
@@ -586,8 +596,10 @@ static int batch_step(swpc_batch *b, int it, const int *d_it) {
         BCK(vel(1));
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
         BCK(vel(2));
+        RC(sponge(1));
     } else {
         BCK(vel(mask_all));
+        RC(sponge(1));
         launch_inject_multi(b->d_inj + b->ninj, b->max_inj, max_inj_n, d_it, it, b->stream);
     }
     BCK(cudaGetLastError());
