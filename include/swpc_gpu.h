@@ -281,10 +281,12 @@ int swpc_vmax(swpc_ctx *ctx, float out[3]);
  * thread's current device, and the call blocks until out[3] (host) is set.
  * Allocates nothing: its scratch is a fixed device array of the library,
  * 3 words per row j, held by every GPU that loads the library until exit, so
- * ny above SWPC_NOALLOC_MAX_NY returns SWPC_ERR_LIMIT.  The first call on a
- * device looks the array's address up; make that first call before any
- * stream capture.  All calls on a device share the array: calls that overlap
- * on the GPU (other streams or threads) race and must be serialised. */
+ * ny above SWPC_NOALLOC_MAX_NY returns SWPC_ERR_LIMIT.  Every call looks the
+ * array's device address up on the current device (nothing is cached, so a
+ * cudaDeviceReset between calls is harmless); the first call on a device may
+ * load the library's device code, so make it before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU (other
+ * streams or threads) race and must be serialised. */
 #define SWPC_NOALLOC_MAX_NY 16384
 int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const int *kob, int nx, int ny, int nz,
                       int na, int ld_k, int ld_i, float uc, void *stream, float out[3]);
@@ -304,12 +306,17 @@ int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const i
  * kernel region.  It runs the forward with a checkpoint every `ckpt` steps,
  * then per segment recomputes the forward from the checkpoint and steps the
  * adjoint back through it, accumulating the gradient in FP64.  Device memory:
- * nt/ckpt checkpoints of the state plus ckpt+1 copies of V and S.
+ * nt/ckpt checkpoints of the state plus ckpt+1 copies of V and S.  Every
+ * recorder (traces, green__store, snapshots) records the forward run once:
+ * the recompute advances the wavefield without them, so what they hold after
+ * the call equals a plain run of steps 1..nt from rest.
  * swpc_gradient_fetch: which = 0 lam, 1 mu, 2 muyz, 3 muxz, 4 muxy, 5 bx,
  * 6 by, 7 bz; out = double array over the memory box. */
 int swpc_adj_reset(swpc_ctx *ctx);
-/* Zero the forward state (V, S, R, PML auxiliaries, displacement and strain
- * accumulators) for another run from rest on the same context.  No
+/* Zero the forward state (V, S, R, PML auxiliaries) and every recorder total
+ * (displacement and strain sums of the stations, green__store's sums,
+ * snapshot frames, sums and maxima) for another run from rest on the same
+ * context.  No
  * counterpart in the reference, which allocates zeroed arrays once per run
  * (m_kernel.f90:354-378, m_absorb_p.f90:96-116). */
 int swpc_reset_state(swpc_ctx *ctx);

@@ -900,9 +900,12 @@ static int zero_state(swpc_ctx *c) {
     std::vector<size_t> sz;
     auto arr = state_arrays(c, &sz);
     for (size_t n = 0; n < arr.size(); n++) ACK(cudaMemsetAsync(arr[n], 0, sz[n] * sizeof(float), c->stream));
+    // recorder totals start from zero at it = 1 as the reference allocates them (m_wav.f90 displacement and
+    // strain sums; m_green.f90:409-425 dxUx..uz); snapshot accumulators and maxima likewise
     if (c->uacc) ACK(cudaMemsetAsync(c->uacc, 0, 3 * sizeof(float) * std::max(c->nst, 1), c->stream));
     if (c->eacc) ACK(cudaMemsetAsync(c->eacc, 0, 6 * sizeof(float) * std::max(c->nst, 1), c->stream));
-    return SWPC_OK;
+    if (c->g_acc) ACK(cudaMemsetAsync(c->g_acc, 0, 12 * sizeof(float) * std::max(c->ng, 1), c->stream));
+    return snap_clear(c);
 }
 
 extern "C" int swpc_reset_state(swpc_ctx *c) {
@@ -970,8 +973,9 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
         const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt);
         rc = copy_state(c, s->ckpool + (size_t)g * ckf, false);
         if (!rc) rc = save_slot(c, 0);
+        // the recompute advances the wavefield only: the recorders already hold these steps
         for (int it = it0; it <= it1 && !rc; it++) {
-            rc = swpc_step(c, it);
+            rc = step_state(c, it);
             if (!rc) rc = save_slot(c, it - it0 + 1);
         }
         for (int it = it1; it >= it0 && !rc; it--) {

@@ -1222,12 +1222,15 @@ extern "C" int swpc_comm_stress(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG
 extern "C" int swpc_comm_vel(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
 extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(c, it, nullptr); }
 
-// main.f90:125-144 loop body (report__progress and snap__write are driven
-// by the caller between steps)
-static int step_body(swpc_ctx *c, int it, const int *d_it) {
-    RC(launch_wav(c, it, d_it));
-    RC(green_store_launch(c, it, d_it));
-    RC(snap_launch(c, it, d_it));
+// main.f90:125-144 loop body (report__progress is driven by the caller
+// between steps); with record = false the wavefield advances without
+// wav__store, green__store and snap__write
+static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
+    if (record) {
+        RC(launch_wav(c, it, d_it));
+        RC(green_store_launch(c, it, d_it));
+        RC(snap_launch(c, it, d_it));
+    }
     RC(launch_stress(c, 3));
     RC(launch_glut(c, it, d_it));
     if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) {
@@ -1250,6 +1253,15 @@ extern "C" int swpc_step(swpc_ctx *c, int it) {
     PREP(c);
     return step_body(c, it, nullptr);
 }
+
+namespace swpc {
+int step_state(swpc_ctx *c, int it) {
+    if (!c) return SWPC_ERR_ARG;
+    if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
+    PREP(c);
+    return step_body(c, it, nullptr, false);
+}
+}  // namespace swpc
 
 static int build_graph(swpc_ctx *c) {
     if (c->graph_exec) return SWPC_OK;

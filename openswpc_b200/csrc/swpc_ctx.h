@@ -202,6 +202,10 @@ namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
 int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
+int snap_clear(swpc_ctx *c);   // frames, displacement accumulators and maxima back to zero
+// one time step of the wavefield alone, without recorders (swpc_api.cu): the
+// recompute of a checkpointed segment must not record a step twice
+int step_state(swpc_ctx *c, int it);
 void adj_free(swpc_ctx *c);   // swpc_adjoint.cu
 int green_store_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_green.cu
 // the same for nmem wavefields at V[q] + m * vstride (reciprocity batch), with

@@ -14,7 +14,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "../../include/swpc_gpu.h"
 
@@ -23,7 +22,6 @@ namespace {
 constexpr int kMaxNy = SWPC_NOALLOC_MAX_NY;
 constexpr int kResult = 3 * kMaxNy;   // first word of the 3-word result
 constexpr int kWords = kResult + 64;  // row partials, result, padding to 256 B
-constexpr int kMaxDevices = 64;
 constexpr int kThreads = 256;
 
 // Scratch shared by every call on a device: 3 words (max |vx|, |vy|, |vz| as
@@ -34,20 +32,16 @@ constexpr int kThreads = 256;
 // cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned int vmax_scratch[kWords];
 
-std::mutex scratch_mu;
-unsigned int *scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up on
-// the first call made with that device current.
-cudaError_t scratch_for(int dev, unsigned int **out) {
-    std::lock_guard<std::mutex> lock(scratch_mu);
-    if (!scratch_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, vmax_scratch);
-        if (e != cudaSuccess) return e;
-        scratch_addr[dev] = static_cast<unsigned int *>(p);
-    }
-    *out = scratch_addr[dev];
+// Device address of the scratch array on the current device.  It is looked
+// up on every call rather than cached: after a cudaDeviceReset (or any new
+// primary context) the array lives at a new address, and a cached one would
+// send the kernels to memory that is no longer mapped.  The lookup allocates
+// nothing and costs little once the module is loaded.
+cudaError_t scratch_for(unsigned int **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, vmax_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned int *>(p);
     return cudaSuccess;
 }
 
@@ -117,11 +111,8 @@ extern "C" int swpc_vmax_noalloc(const float *vx, const float *vy, const float *
     if (!vx || !vy || !vz || !kob || !out) return SWPC_ERR_ARG;
     if (nx < 1 || ny < 1 || nz < 1 || na < 0 || ld_k < nz + 6 || ld_i < nx + 6) return SWPC_ERR_ARG;
     if (ny > kMaxNy) return SWPC_ERR_LIMIT;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return SWPC_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return SWPC_ERR_LIMIT;
     unsigned int *scratch = nullptr;
-    if (scratch_for(dev, &scratch) != cudaSuccess) return SWPC_ERR_CUDA;
+    if (scratch_for(&scratch) != cudaSuccess) return SWPC_ERR_CUDA;
 
     // range of kernel__vmax on a single node (m_kernel.f90:343-344)
     const int margin = 5;

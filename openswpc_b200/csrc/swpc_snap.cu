@@ -155,6 +155,12 @@ void snap_free(swpc_ctx *c) {
     c->snp = nullptr;
 }
 
+int snap_clear(swpc_ctx *c) {
+    if (!c->snp || !c->snp->pool) return SWPC_OK;
+    return cuda_check(c, cudaMemsetAsync(c->snp->pool, 0, c->snp->pool_floats * sizeof(float), c->stream),
+                      "cudaMemsetAsync");
+}
+
 int snap_launch(swpc_ctx *c, int it, const int *d_it) {
     swpc_snap_state *s = c->snp;
     if (!s || s->planes.empty()) return SWPC_OK;

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import os
 import re
+import warnings
 from dataclasses import dataclass, field, fields
 from pathlib import Path
 
@@ -49,6 +50,19 @@ class Source:
     fx: float = 0.0
     fy: float = 0.0
     fz: float = 0.0
+    # double couple (xym0dc / xymwdc): strike (from the map azimuth), dip and
+    # rake in degrees; the moment tensor is then formed by sdr2moment
+    # (m_fdtool.f90:307-336) by whoever consumes the source, in place of mij
+    strike: float | None = None
+    dip: float | None = None
+    rake: float | None = None
+
+    def moment(self, sdr2moment) -> tuple:
+        """(mxx, myy, mzz, myz, mxz, mxy): the given components, or for a
+        double couple the result of ``sdr2moment(strike, dip, rake)``."""
+        if self.strike is None:
+            return (self.mxx, self.myy, self.mzz, self.myz, self.mxz, self.mxy)
+        return tuple(sdr2moment(self.strike, self.dip, self.rake))
 
 
 @dataclass
@@ -98,6 +112,12 @@ class Params:
     sw_wav_strain: bool = False
     abc_type: str = "pml"
     stabilize_pml: bool = False   # m_medium.f90:219-222 (3D)
+    # source depth fitted to a boundary depth: 'asis' or 'bd0'..'bd9' (m_source.f90:99, 262-270)
+    sdep_fit: str = "asis"
+    # boundary depths bddep(i, j, 0:9) of the memory box, shape (ny+6, nx+6, 10) in 3D and (nx+6, 10) in 2D, for
+    # a velocity model that carries its own (vmodel_grd / vmodel_user); None takes vmodel_lhm's: depth(1) of
+    # the layer table at index 0 and -9999 at 1..9 (m_vmodel_lhm.f90:104, 161)
+    bddep: np.ndarray | None = None
     # snapshots (m_snap.f90:105-127): enabled planes as "<section>_<quantity>"
     # names (sections yz xz xy fs ob, quantities ps v u), e.g. {"xz_v", "fs_u"}
     snaps: set = field(default_factory=set)
@@ -122,12 +142,50 @@ class Params:
             self.zbeg = float(np.float32(-30) * np.float32(self.dz))
 
     def check(self) -> None:
+        if self.sdep_fit != "asis" and self.sdep_fit not in BD_NAMES:
+            raise ValueError("sdep_fit must be 'asis' or 'bd0'..'bd9'")
         if self.abc_type not in ("pml", "cerjan"):
             raise ValueError("abc_type must be 'pml' or 'cerjan'")
         if self.nm not in (0, 1, 2, 3):
             raise ValueError("nm must be 0..3")
         if self.stftype not in ("kupper", "boxcar", "triangle", "herrmann", "cosine", "scosine", "texp"):
             raise ValueError(f"unknown stftype {self.stftype!r}")
+
+
+NBD = 9   # boundary depths kept per column (m_global.f90:32)
+BD_NAMES = tuple(f"bd{n}" for n in range(NBD + 1))
+# station depth modes of set_stinfo (m_wav.f90:209-225): the code is 10 + n for 'bd<n>'
+ZSW_CODES = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3, **{f"bd{n}": 10 + n for n in range(NBD + 1)}}
+
+
+def zsw_code(zsw: str, name: str = "") -> int:
+    """The depth-mode code of a station; an unknown mode is taken as 'dep'
+    with a message, as set_stinfo does (m_wav.f90:224-226)."""
+    code = ZSW_CODES.get(zsw)
+    if code is None:
+        warnings.warn(f"unknown zsw type {zsw!r} in station file (station {name}). Assume 'dep'", stacklevel=2)
+        return 0
+    return code
+
+
+def sdep_index(p) -> int:
+    """The bddep index that sdep_fit selects, or -1 for 'asis'."""
+    s = getattr(p, "sdep_fit", "asis")
+    return BD_NAMES.index(s) if s in BD_NAMES else -1
+
+
+def bddep_of(p, two_d: bool = False) -> np.ndarray:
+    """bddep over the memory box: the caller's array, else vmodel_lhm's rule
+    (depth(1) of the layer table, then -9999; m_vmodel_lhm.f90:104, 161)."""
+    shape = (p.nx + 6, NBD + 1) if two_d else (p.ny + 6, p.nx + 6, NBD + 1)
+    if getattr(p, "bddep", None) is not None:
+        bd = np.ascontiguousarray(p.bddep, np.float32)
+        if bd.shape != shape:
+            raise ValueError(f"bddep must have shape {shape}, got {bd.shape}")
+        return bd
+    bd = np.full(shape, np.float32(-9999.0), np.float32)
+    bd[..., 0] = np.float32(p.layers[0].depth) if p.layers else np.float32(0.0)
+    return bd
 
 
 SNAP_SECTIONS = ("yz", "xz", "xy", "fs", "ob")
@@ -187,12 +245,12 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
              "fq_max": float, "fq_ref": float, "vcut": float, "rhomin": float, "stftype": str, "bf_mode": bool,
              "green_mode": bool, "green_cmp": str, "green_trise": float, "ntdec_r": int, "ntdec_w": int,
              "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str,
-             "stabilize_pml": bool}
+             "stabilize_pml": bool, "sdep_fit": str}
     args = {}
     for key, typ in types.items():
         if key in kv:
             args[key] = _conv(kv[key], typ)
-        elif strict and key not in ("xbeg", "ybeg", "zbeg"):
+        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit"):
             raise KeyError(f"parameter {key} missing in strict mode")
     for key in ("z0_xy", "x0_yz", "y0_xz"):
         if key in kv:
@@ -236,8 +294,6 @@ def read_lhm(path: str | Path) -> list[Layer]:
 def read_sources(path: str | Path, stf_format: str = "xym0ij", bf_mode: bool = False) -> list[Source]:
     """Source list in the xy-based formats of source__grid_moment /
     source__grid_bodyforce (m_source.f90:511-559, 740-744)."""
-    from . import _lib
-
     out = []
     for t in _data_lines(Path(path)):
         v = [float(x) for x in t[:12] if _isnum(x)]
@@ -259,15 +315,12 @@ def read_sources(path: str | Path, stf_format: str = "xym0ij", bf_mode: bool = F
 
 
 def dc_source(x, y, z, tbeg, trise, mo, strike, dip, rake, phi: float = 0.0) -> Source:
-    """Double-couple source via sdr2moment (m_fdtool.f90:307-336); strike is
-    measured from the map azimuth phi (m_source.f90:525)."""
-    from . import _lib
-    import ctypes as C
-
-    lib = _lib.load()
-    m6 = (C.c_float * 6)()
-    lib.swpc_sdr2moment(float(np.float32(strike) - np.float32(phi)), dip, rake, m6)
-    return Source(x, y, z, tbeg, trise, mo=mo, mxx=m6[0], myy=m6[1], mzz=m6[2], myz=m6[3], mxz=m6[4], mxy=m6[5])
+    """Double-couple source (xym0dc): strike is measured from the map azimuth
+    phi (m_source.f90:525).  The moment tensor is not formed here: the solver
+    forms it with its own sdr2moment (m_fdtool.f90:307-336) at source setup,
+    see :meth:`Source.moment`."""
+    return Source(x, y, z, tbeg, trise, mo=mo, strike=float(np.float32(strike) - np.float32(phi)),
+                  dip=float(dip), rake=float(rake))
 
 
 def _isnum(s: str) -> bool:

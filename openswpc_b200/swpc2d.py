@@ -19,7 +19,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, fptr, iptr
-from .params import Params
+from .params import Params, bddep_of, sdep_index, zsw_code
+from .swpc3d import SourceGrid, _sdr2moment
 
 f32 = np.float32
 KINDS = {"psv": _lib.KIND_PSV, "sh": _lib.KIND_SH}
@@ -27,6 +28,95 @@ KINDS = {"psv": _lib.KIND_PSV, "sh": _lib.KIND_SH}
 
 def grid2d(p: Params) -> _lib.Grid:
     return _lib.Grid(p.nx, 1, p.nz, p.na, p.nm, p.dx, p.dx, p.dz, p.dt, p.xbeg, 0.0, p.zbeg, p.tbeg)
+
+
+def source_grid2d(p: Params, kind: str = "psv") -> SourceGrid:
+    """source__setup of the 2D codes (src/swpc_psv/m_source.f90:150-268,
+    src/swpc_sh/m_source.f90): cut-off frequency, total moment (P-SV body
+    forces: sqrt(sum fx^2 + fz^2); SH: |sum fy|), grid assignment with the
+    node sleeve, sdep_fit, normalisation by M0.  ``jsrc`` is all zeros."""
+    lib = _lib.load()
+    srcs = p.sources
+    fcut = f32(0.0)
+    for s in srcs:
+        fcut = max(fcut, f32(1) / f32(s.trise))
+    UC = f32(1e-15)
+    if p.bf_mode:
+        acc = f32(0.0)
+        if kind == "psv":
+            for s in srcs:
+                acc = acc + (f32(s.fx) * f32(s.fx) + f32(s.fz) * f32(s.fz))
+            M0 = np.sqrt(acc, dtype=np.float32)
+        else:
+            for s in srcs:
+                acc = acc + f32(s.fy)
+            M0 = np.sqrt(acc * acc, dtype=np.float32)
+        UC = UC * f32(1000)
+    else:
+        M0 = f32(0.0)
+        for s in srcs:
+            M0 = M0 + f32(s.mo)
+    nbd = sdep_index(p)
+    bd = bddep_of(p, two_d=True) if nbd >= 0 else None
+    zend = f32(p.zbeg) + f32(p.nz) * f32(p.dz)
+    rows = []
+    for s in srcs:
+        i = lib.swpc_x2i(s.x, p.xbeg, p.dx)
+        k = lib.swpc_x2i(s.z, p.zbeg, p.dz)
+        if -1 <= i <= p.nx + 3 and -1 <= k <= p.nz + 3:
+            if bd is not None:
+                # sdep_fit = 'bd<n>' (src/swpc_psv/m_source.f90:227-236, inside FDM space :242-245)
+                sz = bd[i + 2, nbd]
+                k = lib.swpc_x2i(float(sz), p.zbeg, p.dz)
+                if not (f32(p.zbeg) <= sz <= zend):
+                    raise ValueError(f"sdep_fit={p.sdep_fit}: source depth {float(sz)} outside the model")
+            rows.append((i, k, s))
+    n = len(rows)
+    isrc = np.array([r[0] for r in rows], np.int32)
+    ksrc = np.array([r[1] for r in rows], np.int32)
+    prm = np.array([[r[2].tbeg, r[2].trise] for r in rows], np.float32).reshape(n, 2)
+    if p.bf_mode:
+        f3 = np.array([[f32(r[2].fx) / M0, f32(r[2].fy) / M0, f32(r[2].fz) / M0] for r in rows],
+                      np.float32).reshape(n, 3)
+        mo = np.zeros(n, np.float32)
+    else:
+        f3 = np.zeros((n, 3), np.float32)
+        mo = np.array([f32(r[2].mo) / M0 for r in rows], np.float32)
+    sdr = _sdr2moment(lib)
+    m6 = np.array([r[2].moment(sdr) for r in rows], np.float32).reshape(n, 6)
+    return SourceGrid(isrc, np.zeros(n, np.int32), ksrc, prm, mo, m6, f3, float(M0), float(UC), float(fcut))
+
+
+def station_grid2d(p: Params, kfs: np.ndarray, kob: np.ndarray):
+    """set_stinfo of the 2D codes (src/swpc_psv/m_wav.f90:480-540): station
+    cells (ist, kst) with depth modes dep / fsb / obb / oba / bd0-bd9; kfs
+    and kob are (nx+6,) maps."""
+    lib = _lib.load()
+    x1, xn = lib.swpc_i2x(1, p.xbeg, p.dx), lib.swpc_i2x(p.nx, p.xbeg, p.dx)
+    cells = []
+    bd = None
+    for st in p.stations:
+        xs, zs = float(f32(st.x)), float(f32(st.z))
+        i = lib.swpc_x2i(xs, p.xbeg, p.dx)
+        k = lib.swpc_x2i(zs, p.zbeg, p.dz)
+        if not (x1 < xs < xn and 1 < k < p.nz and 1 <= i <= p.nx):
+            continue
+        z = zsw_code(st.zsw, st.name)
+        if z == 1:
+            k = int(kfs[i + 2]) + 1
+        elif z == 2:
+            k = int(kob[i + 2]) + 1
+        elif z == 3:
+            k = int(kob[i + 2]) - 1
+        elif z >= 10:
+            # bd0-bd9 (src/swpc_psv/m_wav.f90:511-520)
+            if bd is None:
+                bd = bddep_of(p, two_d=True)
+            k = lib.swpc_x2i(float(bd[i + 2, z - 10]), p.zbeg, p.dz)
+        k = p.nz - 1 if k > p.nz else (2 if k < 1 else k)
+        cells.append((i, k))
+    a = np.array(cells, np.int32).reshape(-1, 2)
+    return a[:, 0].copy(), a[:, 1].copy()
 
 
 class Medium2D:
@@ -96,47 +186,16 @@ class Swpc2D:
         check(ctx, lib.swpc_upload_medium(ctx, C.byref(m.view())))
         check(ctx, lib.swpc_kernel_setup(ctx, fptr(m.ts)))
         # source__setup of the 2D codes (src/swpc_psv/m_source.f90:150-268)
-        srcs = p.sources
-        fcut = f32(0.0)
-        for s in srcs:
-            fcut = max(fcut, f32(1) / f32(s.trise))
-        UC = f32(1e-15)
-        if p.bf_mode:
-            acc = f32(0.0)
-            if kind == "psv":
-                for s in srcs:
-                    acc = acc + (f32(s.fx) * f32(s.fx) + f32(s.fz) * f32(s.fz))
-                M0 = np.sqrt(acc, dtype=np.float32)
-            else:
-                for s in srcs:
-                    acc = acc + f32(s.fy)
-                M0 = np.sqrt(acc * acc, dtype=np.float32)
-            UC = UC * f32(1000)
-        else:
-            M0 = f32(0.0)
-            for s in srcs:
-                M0 = M0 + f32(s.mo)
-        rows = []
-        for s in srcs:
-            i = lib.swpc_x2i(s.x, p.xbeg, p.dx)
-            k = lib.swpc_x2i(s.z, p.zbeg, p.dz)
-            if -1 <= i <= p.nx + 3 and -1 <= k <= p.nz + 3:
-                rows.append((i, k, s))
-        n = len(rows)
-        isrc = np.array([r[0] for r in rows], np.int32)
-        ksrc = np.array([r[1] for r in rows], np.int32)
-        prm = np.array([[r[2].tbeg, r[2].trise] for r in rows], np.float32).reshape(n, 2)
+        sg = source_grid2d(p, kind)
+        M0, UC, fcut = sg.M0, sg.UC, sg.fcut
+        n = len(sg.isrc)
         stf = _lib.STF_CODES[p.stftype]
         if p.bf_mode:
-            f3 = np.array([[f32(r[2].fx) / M0, f32(r[2].fy) / M0, f32(r[2].fz) / M0] for r in rows],
-                          np.float32).reshape(n, 3)
-            check(ctx, lib.swpc_bodyforce_setup(ctx, n, iptr(isrc), None, iptr(ksrc), fptr(prm), fptr(f3), stf))
+            check(ctx, lib.swpc_bodyforce_setup(ctx, n, iptr(sg.isrc), None, iptr(sg.ksrc), fptr(sg.srcprm),
+                                                fptr(sg.f3), stf))
         else:
-            mo = np.array([f32(r[2].mo) / M0 for r in rows], np.float32)
-            m6 = np.array([[r[2].mxx, r[2].myy, r[2].mzz, r[2].myz, r[2].mxz, r[2].mxy] for r in rows],
-                          np.float32).reshape(n, 6)
-            check(ctx, lib.swpc_source_setup(ctx, n, iptr(isrc), None, iptr(ksrc), fptr(prm), fptr(mo), fptr(m6),
-                                             stf))
+            check(ctx, lib.swpc_source_setup(ctx, n, iptr(sg.isrc), None, iptr(sg.ksrc), fptr(sg.srcprm),
+                                             fptr(sg.mo), fptr(sg.m6), stf))
         self.M0, self.UC, self.fcut = float(M0), float(UC), float(fcut)
         g = grid2d(p)
         if p.abc_type == "cerjan":
@@ -160,27 +219,8 @@ class Swpc2D:
         self.nst = 0
         what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u)
         if p.stations and what:
-            x1, xn = lib.swpc_i2x(1, p.xbeg, p.dx), lib.swpc_i2x(p.nx, p.xbeg, p.dx)
-            cells = []
-            zsw = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
-            for st in p.stations:
-                xs, zs = float(f32(st.x)), float(f32(st.z))
-                i = lib.swpc_x2i(xs, p.xbeg, p.dx)
-                k = lib.swpc_x2i(zs, p.zbeg, p.dz)
-                if not (x1 < xs < xn and 1 < k < p.nz and 1 <= i <= p.nx):
-                    continue
-                z = zsw.get(st.zsw, 0)
-                if z == 1:
-                    k = int(m.kfs[i + 2]) + 1
-                elif z == 2:
-                    k = int(m.kob[i + 2]) + 1
-                elif z == 3:
-                    k = int(m.kob[i + 2]) - 1
-                k = p.nz - 1 if k > p.nz else (2 if k < 1 else k)
-                cells.append((i, k))
-            a = np.array(cells, np.int32).reshape(-1, 2)
-            self.ist, self.kst = a[:, 0].copy(), a[:, 1].copy()
-            self.nst = len(cells)
+            self.ist, self.kst = station_grid2d(p, m.kfs, m.kob)
+            self.nst = len(self.ist)
             check(ctx, lib.swpc_wav_setup(ctx, self.nst, iptr(self.ist), None, iptr(self.kst), p.ntdec_w, what,
                                           self.M0, self.UC))
         self.what = what

@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, fptr, iptr
-from .params import Params
+from .params import Params, bddep_of, sdep_index, zsw_code
 
 f32 = np.float32
 
@@ -48,9 +48,19 @@ def grid_struct(p: Params) -> _lib.Grid:
     return _lib.Grid(p.nx, p.ny, p.nz, p.na, p.nm, p.dx, p.dy, p.dz, p.dt, p.xbeg, p.ybeg, p.zbeg, p.tbeg)
 
 
+def _sdr2moment(lib):
+    """The library's sdr2moment (m_fdtool.f90:307-336) as a Python callable."""
+    def f(strike, dip, rake):
+        m6 = (C.c_float * 6)()
+        lib.swpc_sdr2moment(strike, dip, rake, m6)
+        return tuple(m6)
+    return f
+
+
 def source_grid(p: Params) -> SourceGrid:
     """source__setup (m_source.f90:181-305): cut-off frequency, total moment,
-    grid assignment with the node sleeve, normalisation by M0."""
+    grid assignment with the node sleeve, sdep_fit, normalisation by M0.
+    Double couples get their moment tensor from sdr2moment here."""
     lib = _lib.load()
     srcs = p.sources
     fcut = f32(0.0)
@@ -67,12 +77,21 @@ def source_grid(p: Params) -> SourceGrid:
         M0 = f32(0.0)
         for s in srcs:
             M0 = M0 + f32(s.mo)
+    nbd = sdep_index(p)
+    bd = bddep_of(p) if nbd >= 0 else None
+    zend = f32(p.zbeg) + f32(p.nz) * f32(p.dz)
     rows = []
     for s in srcs:
         i = lib.swpc_x2i(s.x, p.xbeg, p.dx)
         j = lib.swpc_x2i(s.y, p.ybeg, p.dy)
         k = lib.swpc_x2i(s.z, p.zbeg, p.dz)
         if -1 <= i <= p.nx + 3 and -1 <= j <= p.ny + 3 and -1 <= k <= p.nz + 3:
+            if bd is not None:
+                # sdep_fit = 'bd<n>' (m_source.f90:262-270); FDM space must contain the depth (:276-280)
+                sz = bd[j + 2, i + 2, nbd]
+                k = lib.swpc_x2i(float(sz), p.zbeg, p.dz)
+                if not (f32(p.zbeg) <= sz <= zend):
+                    raise ValueError(f"sdep_fit={p.sdep_fit}: source depth {float(sz)} outside the model")
             rows.append((i, j, k, s))
     n = len(rows)
     isrc = np.array([r[0] for r in rows], np.int32)
@@ -85,21 +104,20 @@ def source_grid(p: Params) -> SourceGrid:
     else:
         f3 = np.zeros((n, 3), np.float32)
         mo = np.array([f32(r[3].mo) / M0 for r in rows], np.float32)
-    m6 = np.array([[r[3].mxx, r[3].myy, r[3].mzz, r[3].myz, r[3].mxz, r[3].mxy] for r in rows],
-                  np.float32).reshape(n, 6)
+    sdr = _sdr2moment(lib)
+    m6 = np.array([r[3].moment(sdr) for r in rows], np.float32).reshape(n, 6)
     return SourceGrid(isrc, jsrc, ksrc, srcprm, mo, m6, f3.reshape(n, 3), float(M0), float(UC), float(fcut))
-
-
-ZSW = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
 
 
 def station_grid(p: Params, kfs: np.ndarray, kob: np.ndarray):
     """set_stinfo (m_wav.f90:144-274) for a single node: station cells and
-    depth mode (dep / fsb / obb / oba).  kfs/kob are (ny+6, nx+6) maps."""
+    depth mode (dep / fsb / obb / oba / bd0-bd9).  kfs/kob are (ny+6, nx+6)
+    maps; the boundary depths come from ``p.bddep`` or vmodel_lhm's rule."""
     lib = _lib.load()
     out = []
     x1, xn = lib.swpc_i2x(1, p.xbeg, p.dx), lib.swpc_i2x(p.nx, p.xbeg, p.dx)
     y1, yn = lib.swpc_i2x(1, p.ybeg, p.dy), lib.swpc_i2x(p.ny, p.ybeg, p.dy)
+    bd = None
     for st in p.stations:
         xs, ys, zs = float(f32(st.x)), float(f32(st.y)), float(f32(st.z))
         i = lib.swpc_x2i(xs, p.xbeg, p.dx)
@@ -109,13 +127,17 @@ def station_grid(p: Params, kfs: np.ndarray, kob: np.ndarray):
             continue
         if not (1 <= i <= p.nx and 1 <= j <= p.ny):
             continue
-        z = ZSW.get(st.zsw, 0)
+        z = zsw_code(st.zsw, st.name)
         if z == 1:
             k = int(kfs[j + 2, i + 2]) + 1
         elif z == 2:
             k = int(kob[j + 2, i + 2]) + 1
         elif z == 3:
             k = int(kob[j + 2, i + 2]) - 1
+        elif z >= 10:
+            if bd is None:
+                bd = bddep_of(p)
+            k = lib.swpc_x2i(float(bd[j + 2, i + 2, z - 10]), p.zbeg, p.dz)
         else:
             k = lib.swpc_x2i(zs, p.zbeg, p.dz)
         if k > p.nz:

@@ -23,7 +23,25 @@ _FP = C.POINTER(C.c_float)
 _IP = C.POINTER(C.c_int)
 _cache: dict[str, C.CDLL] = {}
 
-ZSW = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3}
+# station depth modes of set_stinfo (m_wav.f90:209-225); 'bd<n>' is 10 + n, anything else is 'dep'
+ZSW = {"dep": 0, "fsb": 1, "obb": 2, "oba": 3, **{f"bd{n}": 10 + n for n in range(10)}}
+NBD = 9
+
+
+def _sdep(p) -> int:
+    """sdep_fit of the run (m_source.f90:99): -1 for 'asis', n for 'bd<n>'."""
+    s = getattr(p, "sdep_fit", "asis")
+    return int(s[2:]) if len(s) == 3 and s[:2] == "bd" and s[2].isdigit() else -1
+
+
+def _moment6(lib, s):
+    """The moment tensor of a source: its components, or for a double couple
+    (strike/dip/rake given) the oracle's own sdr2moment (m_fdtool.f90:307-336)."""
+    if getattr(s, "strike", None) is None:
+        return [s.mxx, s.myy, s.mzz, s.myz, s.mxz, s.mxy]
+    m6 = (C.c_float * 6)()
+    lib.o3d_sdr2moment(s.strike, s.dip, s.rake, m6)
+    return list(m6)
 STF = {"kupper": 0, "boxcar": 1, "triangle": 2, "herrmann": 3, "cosine": 4, "scosine": 4, "texp": 5}
 
 # field ids of o3d_ptr
@@ -32,7 +50,7 @@ FIELD_IDS = {"Vx": 0, "Vy": 1, "Vz": 2, "Sxx": 3, "Syy": 4, "Szz": 5, "Syz": 6, 
              "lam": 20, "mu": 21, "taup": 22, "taus": 23, "bx": 24, "by": 25, "bz": 26, "muyz": 27,
              "muxz": 28, "muxy": 29, "frho": 30, "flam": 31, "fmu": 32, "ftaup": 33, "ftaus": 34, "fbx": 35,
              "fby": 36, "fbz": 37, "fmuyz": 38, "fmuxz": 39, "fmuxy": 40, "kfs": 50, "kob": 51, "kfs_top": 52,
-             "kfs_bot": 53, "kob_top": 54, "kob_bot": 55, "kbeg_a": 56}
+             "kfs_bot": 53, "kob_top": 54, "kob_bot": 55, "kbeg_a": 56, "bddep": 57}
 AUX_NAMES = ["axVx", "ayVx", "azVx", "axVy", "ayVy", "azVy", "axVz", "ayVz", "azVz",
              "axSxx", "aySxy", "azSxz", "axSxy", "aySyy", "azSyz", "axSxz", "aySyz", "azSzz"]
 for _n, _a in enumerate(AUX_NAMES):
@@ -69,6 +87,8 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_set_stabilize": (None, [vp, i]),
         "o3d_green_store_setup": (None, [vp, i, _IP, _IP, _IP, i, i]),
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "o3d_set_sdep_fit": (None, [vp, i]),
+        "o3d_set_bddep": (None, [vp, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
         "o3d_wav_setup": (i, [vp, i, _FP, _FP, _FP, _IP, i, i, i, i, i, _IP, _IP, _IP]),
@@ -144,6 +164,10 @@ class Oracle3D:
             ip = lambda a: np.ascontiguousarray(a, np.int32).ctypes.data_as(_IP)
             lib.o3d_set_maps(self.o, ip(m.kfs), ip(m.kob), ip(m.kfs_top), ip(m.kfs_bot), ip(m.kob_top),
                              ip(m.kob_bot))
+        if getattr(p, "bddep", None) is not None:
+            bd = np.ascontiguousarray(p.bddep, np.float32)
+            assert bd.shape == (p.ny + 6, p.nx + 6, NBD + 1)
+            lib.o3d_set_bddep(self.o, _f(bd))
         lib.o3d_kernel_setup(self.o)
         # sources
         stf = STF[p.stftype]
@@ -157,11 +181,14 @@ class Oracle3D:
             sz = np.array([s.z for s in S], np.float32)
             prm = np.array([[s.tbeg, s.trise] for s in S], np.float32).reshape(n, 2)
             mo = np.array([s.mo for s in S], np.float32)
-            m6 = np.array([[s.mxx, s.myy, s.mzz, s.myz, s.mxz, s.mxy] for s in S], np.float32).reshape(n, 6)
+            m6 = np.array([_moment6(lib, s) for s in S], np.float32).reshape(n, 6)
             f3 = np.array([[s.fx, s.fy, s.fz] for s in S], np.float32).reshape(n, 3)
             self._hold += [sx, sy, sz, prm, mo, m6, f3]
+            lib.o3d_set_sdep_fit(self.o, _sdep(p))
             self.nsrc = lib.o3d_source_setup(self.o, int(p.bf_mode), n, _f(sx), _f(sy), _f(sz), _f(prm), _f(mo),
                                              _f(m6), _f(f3), stf)
+            if self.nsrc < 0:
+                raise ValueError("source depth outside the model after sdep_fit")
         sc = self.scalars()
         fcut = sc["fcut"] if not p.green_mode else float(np.float32(1.0) / np.float32(p.green_trise))
         if getattr(p, "abc_type", "pml") == "cerjan":
@@ -211,6 +238,9 @@ class Oracle3D:
                 k = int(kob[j + 2, i + 2]) + 1
             elif z == 3:
                 k = int(kob[j + 2, i + 2]) - 1
+            elif z >= 10:
+                bd = self.bddep()
+                k = lib.o3d_x2i(float(bd[j + 2, i + 2, z - 10]), p.zbeg, p.dz)
             out[0].append(i)
             out[1].append(j)
             out[2].append(k)
@@ -257,6 +287,8 @@ class Oracle3D:
             dt, shape = np.float32, (d["nj"], d["ni"], d["nk"])
         elif fid in range(50, 57):
             dt, shape = np.int32, (d["nj"], d["ni"])
+        elif fid == 57:
+            dt, shape = np.float32, (d["nj"], d["ni"], NBD + 1)
         elif fid in range(60, 78):
             dt, shape = self.spr, (p.ny, p.nx, d["nka"])
         elif fid in range(110, 116):
@@ -266,6 +298,10 @@ class Oracle3D:
         n = int(np.prod(shape))
         buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
         return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+    def bddep(self) -> np.ndarray:
+        """Boundary depths bddep(i, j, 0:NBD) of the memory box, shape (nj, ni, NBD + 1)."""
+        return self.array("bddep")
 
     def green_store_setup(self, ig, jg, kg, bforce: bool = False, ntdec_w: int = 1):
         """green__store (m_green.f90:389-534) at the given grid cells; o3d_step
@@ -376,6 +412,8 @@ def load2d(variant: str = "f32") -> C.CDLL:
         "o2d_absorb_setup": (None, [vp, f]),
         "o2d_cerjan_setup": (None, [vp]),
         "o2d_set_stabilize": (None, [vp, i]),
+        "o2d_set_bddep": (None, [vp, _FP]),
+        "o2d_set_sdep_fit": (None, [vp, i]),
         "o2d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o2d_wav_setup": (i, [vp, i, _FP, _FP, _IP, i, i, i]),
         "o2d_step": (None, [vp, i]),
@@ -423,11 +461,18 @@ class Oracle2D:
         sz = np.array([s.z for s in S], np.float32)
         prm = np.array([[s.tbeg, s.trise] for s in S], np.float32).reshape(n, 2)
         mo = np.array([s.mo for s in S], np.float32)
-        m6 = np.array([[s.mxx, s.myy, s.mzz, s.myz, s.mxz, s.mxy] for s in S], np.float32).reshape(n, 6)
+        m6 = np.array([_moment6(load(variant, "3d"), s) for s in S], np.float32).reshape(n, 6)
         f3 = np.array([[s.fx, s.fy, s.fz] for s in S], np.float32).reshape(n, 3)
         self._hold = [sx, sz, prm, mo, m6, f3]
+        if getattr(p, "bddep", None) is not None:
+            bd = np.ascontiguousarray(p.bddep, np.float32)
+            assert bd.shape == (p.nx + 6, NBD + 1)
+            lib.o2d_set_bddep(self.o, _f(bd))
+        lib.o2d_set_sdep_fit(self.o, _sdep(p))
         self.nsrc = lib.o2d_source_setup(self.o, int(p.bf_mode), n, _f(sx), _f(sz), _f(prm), _f(mo), _f(m6), _f(f3),
                                          STF[p.stftype])
+        if self.nsrc < 0:
+            raise ValueError("source depth outside the model after sdep_fit")
         if getattr(p, "abc_type", "pml") == "cerjan":
             lib.o2d_cerjan_setup(self.o)
         else:

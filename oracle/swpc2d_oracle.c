@@ -53,6 +53,8 @@ typedef struct o2d {
     SPR *rho, *lam, *mu, *taup, *taus;
     float ts[NM_MAX];
     int *kfs, *kob, *kfs_top, *kfs_bot, *kob_top, *kob_bot;
+    float *bddep;                /* (i, 0:NBD2) boundary depths (src/swpc_psv/m_global.f90 bddep) */
+    int sdep_fit1;               /* sdep_fit: 0 'asis', 1 + n for 'bd<n>' (src/swpc_psv/m_source.f90:85) */
     SPR c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     MPR rc40x, rc41x, rc40z, rc41z, rd40x, rd41x, rd40z, rd41z;
     float *fgxc, *fgxe, *fgzc, *fgze;
@@ -76,6 +78,7 @@ typedef struct o2d {
     int threads;
 } o2d;
 
+#define NBD2 9
 #define I2(o, k, i) ((((long)(i)) - (o)->ibeg_m) * (o)->nk + ((long)(k) - (o)->kbeg_m))
 #define IA(o, k, i) ((((long)(i)) - (o)->ibeg) * (o)->nka + ((long)(k) - (o)->kbeg_min))
 #define A(arr, k, i) (arr)[I2(o, k, i)]
@@ -214,8 +217,15 @@ o2d *o2d_create(int kind, int nx, int nz, int na, int nm, int nt, double dx, dou
     o->kfs = (int *)zalloc(sizeof(int) * o->ni); o->kob = (int *)zalloc(sizeof(int) * o->ni);
     o->kfs_top = (int *)zalloc(sizeof(int) * o->ni); o->kfs_bot = (int *)zalloc(sizeof(int) * o->ni);
     o->kob_top = (int *)zalloc(sizeof(int) * o->ni); o->kob_bot = (int *)zalloc(sizeof(int) * o->ni);
+    o->bddep = (float *)zalloc(sizeof(float) * o->ni * (NBD2 + 1));
     return o;
 }
+
+/* boundary depths of a model that carries its own; vmodel_lhm fills depth(1) and -9999 */
+void o2d_set_bddep(o2d *o, const float *bd) { memcpy(o->bddep, bd, sizeof(float) * o->ni * (NBD2 + 1)); }
+
+/* sdep_fit: -1 for 'asis', n for 'bd<n>'; set before o2d_source_setup */
+void o2d_set_sdep_fit(o2d *o, int n) { o->sdep_fit1 = (n >= 0 && n <= NBD2) ? n + 1 : 0; }
 
 void o2d_destroy(o2d *o) {
     if (!o) return;
@@ -225,7 +235,7 @@ void o2d_destroy(o2d *o) {
                   o->gxc, o->gxe, o->gzc, o->gze, o->aux[0], o->aux[1], o->aux[2], o->aux[3], o->aux[4], o->aux[5],
                   o->aux[6], o->aux[7], o->isrc, o->ksrc, o->srcprm, o->mo, o->mxx, o->mzz, o->mxz, o->myz,
                   o->mxy, o->fx, o->fy, o->fz, o->ist, o->kst, o->wav_vel, o->wav_disp, o->ux, o->uz,
-                  o->cgx_c, o->cgx_b, o->cgz_c, o->cgz_b};
+                  o->cgx_c, o->cgx_b, o->cgz_c, o->cgz_b, o->bddep};
     for (size_t n = 0; n < sizeof(ps) / sizeof(ps[0]); n++) free(ps[n]);
     free(o);
 }
@@ -242,6 +252,11 @@ void o2d_vmodel_lhm(o2d *o, int nlayer, const float *depth, const float *rho0, c
             p0[l] = p0[l + 1]; s0[l] = s0[l + 1]; r0[l] = r0[l + 1]; a0[l] = a0[l + 1]; b0[l] = b0[l + 1];
         }
     float ddx = (float)o->dx, ddz = (float)o->dz;
+    /* topography shape and dummy boundary depths (src/swpc_psv/m_vmodel_lhm.f90, as m_vmodel_lhm.f90:104, 161) */
+    for (int i = 0; i < o->ni; i++) {
+        o->bddep[i * (NBD2 + 1)] = depth[0];
+        for (int n = 1; n <= NBD2; n++) o->bddep[i * (NBD2 + 1) + n] = -9999.0f;
+    }
     float dh = 1.0f / sqrtf(1.0f / (ddx * ddx) + 1.0f / (ddz * ddz));
     float vmax_r = 6.0f / 7.0f * dh / o->dt;
     for (int i = -2; i <= o->nx + 3; i++)
@@ -808,6 +823,12 @@ int o2d_source_setup(o2d *o, int bf_mode, int n_g, const float *sx, const float 
     for (int i = 0; i < n_g; i++) {
         if (!in[i]) continue;
         o->isrc[nn] = is[i]; o->ksrc[nn] = ks[i];
+        /* sdep_fit = 'bd<n>' (src/swpc_psv/m_source.f90:227-236), inside FDM space (:242-245) */
+        if (o->sdep_fit1 > 0) {
+            float szb = o->bddep[(is[i] + 2) * (NBD2 + 1) + (o->sdep_fit1 - 1)];
+            o->ksrc[nn] = x2i(szb, o->zbeg, (float)o->dz);
+            if (!(o->zbeg <= szb && szb <= o->zend)) { free(is); free(ks); free(in); return -1; }
+        }
         o->srcprm[2 * nn] = prm[2 * i]; o->srcprm[2 * nn + 1] = prm[2 * i + 1];
         o->mo[nn] = (MPR)(bf_mode ? 0.0f : mo_g[i]);
         o->mxx[nn] = (MPR)m6[6 * i]; o->mzz[nn] = (MPR)m6[6 * i + 2]; o->myz[nn] = (MPR)m6[6 * i + 3];
@@ -879,6 +900,8 @@ int o2d_wav_setup(o2d *o, int n_g, const float *xs, const float *zs, const int *
         if (zsw[s] == 1) k = o->kfs[i + 2] + 1;
         else if (zsw[s] == 2) k = o->kob[i + 2] + 1;
         else if (zsw[s] == 3) k = o->kob[i + 2] - 1;
+        else if (zsw[s] >= 10 && zsw[s] <= 10 + NBD2)   /* bd0-bd9 (src/swpc_psv/m_wav.f90:511-520) */
+            k = x2i(o->bddep[(i + 2) * (NBD2 + 1) + (zsw[s] - 10)], o->zbeg, ddz);
         else k = x2i(zs[s], o->zbeg, ddz);
         if (k > o->kend) k = o->kend - 1;
         if (k < o->kbeg) k = o->kbeg + 1;

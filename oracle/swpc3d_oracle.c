@@ -75,6 +75,7 @@ typedef struct o3d {
     float zeta;
     int *kfs, *kob, *kfs_top, *kfs_bot, *kob_top, *kob_bot;
     float *bddep;               /* (i, j, 0:NBD) */
+    int sdep_fit1;              /* sdep_fit: 0 'asis', 1 + n for 'bd<n>' (m_source.f90:99) */
     /* kernel coefficients (m_kernel.f90:23-26) */
     SPR c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     MPR rc40x, rc41x, rc40y, rc41y, rc40z, rc41z;
@@ -1164,6 +1165,13 @@ int o3d_source_setup(o3d *o, int bf_mode, int nsrc_g, const float *sx, const flo
         if (!in[i]) continue;
         o->isrc[nn] = is[i]; o->jsrc[nn] = js[i]; o->ksrc[nn] = ks[i];
         o->srcprm[2 * nn] = srcprm[2 * i]; o->srcprm[2 * nn + 1] = srcprm[2 * i + 1];
+        /* sdep_fit = 'bd<n>': the source depth becomes the n-th boundary depth of its column
+           (m_source.f90:262-270), and FDM space must contain it (m_source.f90:276-280) */
+        if (o->sdep_fit1 > 0) {
+            float szb = o->bddep[IDX2(o, is[i], js[i]) * (NBD + 1) + (o->sdep_fit1 - 1)];
+            o->ksrc[nn] = o3d_x2i(szb, o->zbeg, (float)o->dz);
+            if (!(o->zbeg <= szb && szb <= o->zend)) { free(is); free(js); free(ks); free(in); return -1; }
+        }
         if (bf_mode) {
             o->fx[nn] = (MPR)f3[3 * i]; o->fy[nn] = (MPR)f3[3 * i + 1]; o->fz[nn] = (MPR)f3[3 * i + 2];
         } else {
@@ -1185,6 +1193,15 @@ int o3d_source_setup(o3d *o, int bf_mode, int nsrc_g, const float *sx, const flo
     /* dt_dxyz = dt / (dx * dy * dz): m_source.f90:305 */
     o->dt_dxyz = o->dt / (o->dx * o->dy * o->dz);
     return n;
+}
+
+/* sdep_fit (m_source.f90:99): -1 for 'asis', n for 'bd<n>'; set before o3d_source_setup */
+void o3d_set_sdep_fit(o3d *o, int n) { o->sdep_fit1 = (n >= 0 && n <= NBD) ? n + 1 : 0; }
+
+/* boundary depths bddep(i, j, 0:NBD) of a velocity model that carries its own (vmodel_grd / vmodel_user,
+   m_vmodel_grd.f90:258-270); vmodel_lhm fills depth(1) and -9999 (m_vmodel_lhm.f90:104, 161) */
+void o3d_set_bddep(o3d *o, const float *bd) {
+    memcpy(o->bddep, bd, sizeof(float) * o->ni * o->nj * (NBD + 1));
 }
 
 /* source__stressglut: m_source.f90:775-833 */
@@ -1682,7 +1699,7 @@ int o3d_spr_size(void) { return (int)sizeof(SPR); }
 /* field ids: 0..8 V/S (MPR), 10..15 R (SPR), 20..29 medium (SPR) lam mu taup
  * taus bx by bz muyz muxz muxy, 30.. float setup copies rho lam mu taup taus
  * bx by bz muyz muxz muxy, 50..55 int maps kfs kob kfs_top kfs_bot kob_top
- * kob_bot, 56 kbeg_a, 60..77 PML aux (SPR), 80..85 float profiles gxc gxe
+ * kob_bot, 56 kbeg_a, 57 bddep (float, (i, j, 0:NBD)), 60..77 PML aux (SPR), 80..85 float profiles gxc gxe
  * gyc gye gzc gze, 90..93 wav buffers */
 void *o3d_ptr(o3d *o, int id) {
     switch (id) {
@@ -1699,6 +1716,7 @@ void *o3d_ptr(o3d *o, int id) {
     case 38: return o->fmuyz; case 39: return o->fmuxz; case 40: return o->fmuxy;
     case 50: return o->kfs; case 51: return o->kob; case 52: return o->kfs_top; case 53: return o->kfs_bot;
     case 54: return o->kob_top; case 55: return o->kob_bot; case 56: return o->kbeg_a;
+    case 57: return o->bddep;
     case 60: return o->axVx; case 61: return o->ayVx; case 62: return o->azVx;
     case 63: return o->axVy; case 64: return o->ayVy; case 65: return o->azVy;
     case 66: return o->axVz; case 67: return o->ayVz; case 68: return o->azVz;

@@ -50,4 +50,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_example_golden.py /path/to/OpenSWPC")
+    main(Path(sys.argv[1]))

@@ -13,19 +13,29 @@ KEYS = {"impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_
         "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"}
 
 
-def run_reference(workload: str) -> dict:
-    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", workload,
+# runs bench.py in this interpreter, then lists the shared objects of the package it mapped
+_WRAP = ("import runpy, sys; sys.argv = ['bench.py'] + sys.argv[1:]; runpy.run_path('bench.py', run_name='__main__'); "
+         "print('MAPPED', sorted({l.split()[-1] for l in open('/proc/self/maps') if 'openswpc_b200' in l}))")
+
+
+def run_reference(workload: str, mapped: list | None = None) -> dict:
+    out = subprocess.run([sys.executable, "-c", _WRAP, "--impl", "reference", "--workload", workload,
                           "--steps", "3", "--warmup", "3", "--cpu-budget", "2"],
                          cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1, out.stdout[-2000:]
+    if mapped is not None:
+        mapped += eval(next(l for l in out.stdout.splitlines() if l.startswith("MAPPED"))[len("MAPPED"):])
     return json.loads(lines[0])
 
 
 @pytest.mark.parametrize("workload", ["c0", "c2a"])
 def test_reference_arm_prints_the_contract_line(workload):
-    line = run_reference(workload)
+    mapped = []
+    line = run_reference(workload, mapped)
+    # the reference arm runs the oracle alone: no library of the package is loaded
+    assert not mapped, mapped
     assert KEYS <= set(line), KEYS - set(line)
     assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] >= 1
     assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["cores"] >= 1

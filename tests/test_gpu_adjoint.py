@@ -312,3 +312,40 @@ def test_waveform_misfit_autograd():
         J2 = waveform_misfit(*[t.detach() for t in tv], prob)
     assert abs(float(J2) - J_ref) <= 1e-6 * J_ref
     prob.close()
+
+
+def _recorders(g, ig):
+    """Everything the recorders of a run hold: velocity, displacement,
+    stress and strain traces, green__store's Green's functions."""
+    out = [g.waveforms(w) for w in (_lib.WAV_V, _lib.WAV_U, _lib.WAV_STRESS, _lib.WAV_STRAIN)]
+    return out + [g.green_functions()]
+
+
+def test_recorders_after_gradient_and_reset_equal_a_plain_run():
+    """The gradient's recompute advances the wavefield without recording, and
+    swpc_reset_state clears every recorder total, so traces and Green's
+    functions after either equal those of one plain run from rest, bitwise."""
+    p = small3d(nt=40, sw_wav_u=True, sw_wav_stress=True, sw_wav_strain=True)
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    rng = np.random.default_rng(8)
+    ig, jg, kg = (rng.integers(p.na + 2, n - p.na - 2, 16) for n in (p.nx, p.ny, p.nz))
+    plain = Swpc3D(p, xi)
+    plain.green_store_setup(ig, jg, kg, bforce=True)
+    plain.run(1, p.nt)
+    ref = _recorders(plain, ig)
+    assert all(np.abs(a).max() > 0 for a in ref)
+    # a second run from rest on the same context
+    check(plain.ctx, plain.lib.swpc_reset_state(plain.ctx))
+    plain.run(1, p.nt)
+    again = _recorders(plain, ig)
+    for a, b in zip(again, ref):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    # the gradient: forward, then checkpointed recompute of every segment
+    g = Swpc3D(p, xi)
+    g.green_store_setup(ig, jg, kg, bforce=True)
+    obs = np.zeros_like(ref[0])
+    J = C.c_double()
+    check(g.ctx, g.lib.swpc_gradient(g.ctx, fptr(obs), 16, C.byref(J)))
+    after = _recorders(g, ig)
+    for a, b in zip(after, ref):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

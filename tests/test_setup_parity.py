@@ -287,3 +287,132 @@ def test_stabilize_pml_2d_matches_oracle(kind):
         b = o.array(name).astype(np.float32)
         assert np.array_equal(getattr(m, name).view(np.uint32), b.view(np.uint32)), name
     assert not np.array_equal(m.mu, m0.mu)
+
+
+def test_sdr2moment_bit_exact_against_oracle():
+    """The library's sdr2moment and the oracle's restatement agree bit for bit
+    (m_fdtool.f90:307-336), so double couples enter both runs identically."""
+    lib = _lib.load()
+    ol = oload()
+    rng = np.random.default_rng(11)
+    sdrs = [(30, 60, 90), (0, 90, 0), (360, 90, 180), (-360, -90, -180), (123.4, 45.6, -60.7)]
+    sdrs += [tuple(v) for v in np.stack([rng.uniform(-360, 360, 2000), rng.uniform(-90, 90, 2000),
+                                         rng.uniform(-180, 180, 2000)], 1).astype(np.float32)]
+    a, b = (C.c_float * 6)(), (C.c_float * 6)()
+    for sdr in sdrs:
+        lib.swpc_sdr2moment(*map(float, sdr), a)
+        ol.o3d_sdr2moment(*map(float, sdr), b)
+        assert np.array_equal(bits(np.array(a[:], np.float32)), bits(np.array(b[:], np.float32))), sdr
+
+
+def test_dc_source_moment_is_formed_by_each_side():
+    """A double couple carries strike/dip/rake; the product forms its tensor
+    at source setup and the oracle with its own sdr2moment."""
+    p = small3d(sources=[dc_source(0.3, -0.7, 6.1, 0.0, 1.0, 1e16, 30, 60, 90, phi=10.0)])
+    s = p.sources[0]
+    assert s.strike == np.float32(20.0) and s.mxx == 0.0
+    sg = source_grid(p)
+    ref = (C.c_float * 6)()
+    oload().o3d_sdr2moment(20.0, 60.0, 90.0, ref)
+    assert np.array_equal(bits(sg.m6[0]), bits(np.array(ref[:], np.float32)))
+
+
+def _bd_params(custom: bool, two_d: bool = False):
+    """Stations in every depth mode (dep fsb obb oba bd0-bd9), an unknown mode
+    among them, and optionally boundary depths of the caller's own."""
+    from tests.models import small2d
+
+    modes = ["dep", "fsb", "obb", "oba"] + [f"bd{n}" for n in range(10)]
+    rng = np.random.default_rng(21)
+    p = small2d() if two_d else small3d()
+    st = []
+    for q, z in enumerate(modes * 2):
+        x = float(rng.uniform(p.xbeg + (p.na + 2) * p.dx, p.xbeg + (p.nx - p.na - 2) * p.dx))
+        y = 0.0 if two_d else float(rng.uniform(p.ybeg + (p.na + 2) * p.dy, p.ybeg + (p.ny - p.na - 2) * p.dy))
+        st.append(Station(x, y, float(rng.uniform(0.5, 6.0)), f"b{q}", z))
+    p.stations = st
+    if custom:
+        shape = (p.nx + 6, 10) if two_d else (p.ny + 6, p.nx + 6, 10)
+        bd = rng.uniform(-1.0, 0.6 * p.nz * p.dz, shape).astype(np.float32)
+        bd[..., 9] = 99.0     # below the model: clamped to kend - 1
+        bd[..., 8] = -50.0    # above the model: clamped to kbeg + 1
+        p.bddep = bd
+    return p
+
+
+@pytest.mark.parametrize("custom", [False, True])
+def test_station_depth_modes_bit_exact(custom):
+    """set_stinfo's depth modes, bd0-bd9 included (m_wav.f90:209-236): the
+    station cells equal the oracle's, with vmodel_lhm's boundary depths
+    (depth(1), then -9999) or the caller's."""
+    p = _bd_params(custom)
+    m = Medium(p)
+    ist, jst, kst = station_grid(p, m.kfs, m.kob)
+    o = Oracle3D(p)
+    assert len(ist) == len(p.stations) == o.nst
+    assert np.array_equal(ist, o.ist) and np.array_equal(jst, o.jst) and np.array_equal(kst, o.kst)
+    # the boundary-depth stations did not all land on the 'dep' cell
+    assert len(set(kst[4:14].tolist())) > (3 if custom else 1)
+
+
+@pytest.mark.parametrize("custom", [False, True])
+def test_station_depth_modes_bit_exact_2d(custom):
+    """The same depth modes in the P-SV code (src/swpc_psv/m_wav.f90:505-532)."""
+    from openswpc_b200.swpc2d import Medium2D, station_grid2d
+    from oracle.oracle import Oracle2D
+
+    p = _bd_params(custom, two_d=True)
+    m = Medium2D(p)
+    ist, kst = station_grid2d(p, m.kfs, m.kob)
+    o = Oracle2D(p, "psv")
+    n = o.nst
+    oi = np.ctypeslib.as_array(C.cast(o.lib.o2d_ptr(o.o, 95), C.POINTER(C.c_int)), (n,))
+    ok = np.ctypeslib.as_array(C.cast(o.lib.o2d_ptr(o.o, 96), C.POINTER(C.c_int)), (n,))
+    assert len(ist) == n == len(p.stations)
+    assert np.array_equal(ist, oi) and np.array_equal(kst, ok)
+
+
+def test_unknown_station_mode_is_taken_as_dep_with_a_message():
+    p = small3d()
+    p.stations = [Station(0.3, 0.2, 2.0, "x", "bdx"), Station(0.3, 0.2, 2.0, "y", "dep")]
+    m = Medium(p)
+    with pytest.warns(UserWarning, match="Assume 'dep'"):
+        ist, jst, kst = station_grid(p, m.kfs, m.kob)
+    assert kst[0] == kst[1]
+
+
+@pytest.mark.parametrize("fit", ["bd0", "bd4"])
+def test_source_depth_fit_bit_exact(fit):
+    """sdep_fit = 'bd<n>' moves each source to its column's boundary depth
+    (m_source.f90:262-270) on both sides."""
+    from openswpc_b200.swpc2d import source_grid2d
+    from oracle.oracle import Oracle2D
+
+    p = _bd_params(True)
+    p.sdep_fit = fit
+    p.sources = [dc_source(0.3, -0.7, 6.1, 0.0, 1.0, 1e16, 30, 60, 90),
+                 Source(2.2, 1.1, 4.0, 0.2, 1.5, mo=3e15, mxx=1, myy=1, mzz=1)]
+    sg = source_grid(p)
+    o = Oracle3D(p)
+    n = o.dims()["nsrc"]
+    ks = np.ctypeslib.as_array(C.cast(o.lib.o3d_ptr(o.o, 100), C.POINTER(C.c_int)), (n,))
+    assert np.array_equal(sg.ksrc, ks)
+    assert sg.ksrc[0] == _lib.load().swpc_x2i(float(p.bddep[sg.jsrc[0] + 2, sg.isrc[0] + 2, int(fit[2])]),
+                                              p.zbeg, p.dz)
+    q = _bd_params(True, two_d=True)
+    q.sdep_fit = fit
+    sg2 = source_grid2d(q, "psv")
+    o2 = Oracle2D(q, "psv")
+    n2 = o2.nsrc
+    ks2 = np.ctypeslib.as_array(C.cast(o2.lib.o2d_ptr(o2.o, 99), C.POINTER(C.c_int)), (n2,))
+    assert np.array_equal(sg2.ksrc, ks2)
+
+
+def test_source_depth_fit_outside_the_model_is_refused():
+    """With vmodel_lhm's dummy depths (-9999) a fit to bd1 leaves FDM space,
+    which source__setup asserts against (m_source.f90:276-280)."""
+    p = small3d(sdep_fit="bd1")
+    with pytest.raises(ValueError, match="outside the model"):
+        source_grid(p)
+    with pytest.raises(ValueError, match="outside the model"):
+        Oracle3D(p)
