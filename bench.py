@@ -610,9 +610,19 @@ def cell_counts(p):
 
 
 def rmed(p, seed=5, device=None):
+    """The von Karman medium of a run (eps = 5 %, a = 5 km, kappa = 0.5), generated in HBM by the library."""
     from openswpc_b200.media import vonkarman_3d
 
     return vonkarman_3d((p.ny + 6, p.nx + 6, p.nz + 6), p.dx, p.dy, p.dz, 0.05, 5.0, 0.5, seed, device)
+
+
+def rmed_sample(p, seed=5):
+    """The same statistics over the CPU baseline's centre column block, from the oracle's restatement of the
+    generator (the reference arm runs without the library)."""
+    from oracle.rmedia import vonkarman_box
+
+    ns = min(256, p.nx)
+    return vonkarman_box((ns + 6, ns + 6, p.nz + 6), p.dx, p.dy, p.dz, 0.05, 5.0, 0.5, seed)
 
 
 def hbm_peak():
@@ -688,13 +698,15 @@ def cpu_reference(p, xi, steps: int, warmup: int, threads: int, budget_s: float 
     ns = min(256, p.nx)
     i0 = (p.nx - ns) // 2
     j0 = (p.ny - ns) // 2
+    # xi over the whole grid, or a medium of the sample block itself
+    si, sj = (0, 0) if xi is not None and xi.shape[:2] == (ns + 6, ns + 6) else (i0, j0)
     q = Params(**{**p.__dict__})
     q.nx, q.ny = ns, ns
     q.xbeg = float(np.float32(p.xbeg) + np.float32(i0) * np.float32(p.dx))
     q.ybeg = float(np.float32(p.ybeg) + np.float32(j0) * np.float32(p.dy))
     q.stations = []
     q.sources = [s for s in p.sources][:1]
-    xs = np.ascontiguousarray(xi[j0:j0 + ns + 6, i0:i0 + ns + 6, :]) if xi is not None else None
+    xs = np.ascontiguousarray(xi[sj:sj + ns + 6, si:si + ns + 6, :]) if xi is not None else None
     o = Oracle3D(q, xs, variant="f32", threads=threads)
     for it in range(1, warmup + 1):
         o.step(it)
@@ -730,7 +742,7 @@ def accuracy_sample(p, precision: str, device: int, steps: int = 200):
     q.stations = [Station(float(rng.uniform(-40, 40) * q.dx), float(rng.uniform(-40, 40) * q.dy), 0.0, f"a{n}", "fsb")
                   for n in range(16)]
     q.ntdec_r = 25
-    xi = rmed(q, seed=9, device="cpu")
+    xi = rmed(q, seed=9, device=device)
     o = Oracle3D(q, xi, variant="f64", threads=os.cpu_count() or 1)
     o.run(1, steps)
     g = Swpc3D(q, xi, device=device, precision=precision)
@@ -804,7 +816,7 @@ def main():
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        xi = rmed(p, device="cpu")
+        xi = rmed_sample(p)
         # each step = one oracle step over the bounded sample (warm-up untimed)
         v, n, sample_cells, dt = cpu_reference(p, xi, args.steps, args.warmup, threads)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,

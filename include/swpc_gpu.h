@@ -171,6 +171,11 @@ int swpc_upload_medium(swpc_ctx *ctx, const swpc_medium_view *m);
 int swpc_vmodel_lhm_device(swpc_ctx *ctx, int nlayer, const float *depth, const float *rho0, const float *vp0,
                            const float *vs0, const float *qp0, const float *qs0, float vcut, float rhomin, float zbeg,
                            const float *xi, int ld_k, int ld_i);
+/* The same with munk_profile (m_vmodel_lhm.f90:53-54): the seawater above
+ * depth(1) takes Munk's profile instead of 1.5 km/s (swpc_vmodel_lhm_opt). */
+int swpc_vmodel_lhm_device_opt(swpc_ctx *ctx, int nlayer, const float *depth, const float *rho0, const float *vp0,
+                               const float *vs0, const float *qp0, const float *qs0, float vcut, float rhomin,
+                               float zbeg, const float *xi, int ld_k, int ld_i, int munk_profile);
 int swpc_vmodel_upload(swpc_ctx *ctx, const float *rho, const float *lam, const float *mu, const float *qp,
                        const float *qs, int ld_k, int ld_i);
 int swpc_medium_setup_device(swpc_ctx *ctx, float fq_min, float fq_max, float fq_ref, float *ts, float *scal,

@@ -49,10 +49,22 @@ void swpc_kbeg_a(const swpc_grid *g, int *kbeg_a);
 /* vmodel_lhm (src/swpc_3d/m_vmodel_lhm.f90:21-169); with xi != NULL the
  * lhm_rmed perturbation (m_vmodel_lhm_rmed.f90:187-195, vcheck
  * m_fdtool.f90:15-48).  depth/rho/vp/vs/qp/qs per layer; outputs over the
- * memory box: rho, lam, mu, qp, qs.  Air above depth(1) with z < 0. */
+ * memory box: rho, lam, mu, qp, qs.  Air above depth(1) with z < 0, seawater of
+ * 1.5 km/s above depth(1) with z >= 0. */
 int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const float *rho0, const float *vp0,
                     const float *vs0, const float *qp0, const float *qs0, float vcut, const float *xi, float rhomin,
                     float *rho, float *lam, float *mu, float *qp, float *qs);
+/* The same with the input-file switch munk_profile (m_vmodel_lhm.f90:53-54):
+ * cells with 0 <= z < depth(1) are seawater (rho 1, mu 0, Q 1e6) whose
+ * P velocity is 1.5 km/s, or Munk's profile when munk_profile != 0
+ * (seawater__vel, src/shared/m_seawater.f90:36-49).  swpc_vmodel_lhm is
+ * this call with munk_profile = 0. */
+int swpc_vmodel_lhm_opt(const swpc_grid *g, int nlayer, const float *depth, const float *rho0, const float *vp0,
+                        const float *vs0, const float *qp0, const float *qs0, float vcut, const float *xi,
+                        float rhomin, float *rho, float *lam, float *mu, float *qp, float *qs, int munk_profile);
+/* seawater__vel (src/shared/m_seawater.f90:36-49): the P velocity [km/s] of
+ * seawater at depth z [km]. */
+float swpc_seawater_vel(float z, int munk_profile);
 
 /* medium__setup after the vmodel (src/swpc_3d/m_medium.f90:124-225 and its
  * contained routines): absorber homogenisation, tau-method (taup/taus from
@@ -101,6 +113,36 @@ void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gx
  * gy_c and gy_b may be NULL. */
 void swpc_cerjan_profiles(const swpc_grid *g, float *gx_c, float *gx_b, float *gy_c, float *gy_b, float *gz_c,
                           float *gz_b);
+
+/* Random media (src/shared/m_rmedia.f90): rmedia__3dgen (:176-307) for
+ * ny > 1 and rmedia__2dgen (:424-) for ny = 1, generated on the current CUDA
+ * device.  Uniform random numbers in [0, 1) over nx x ny x nz cells, their
+ * spectrum whitened and filtered by the Gaussian (ptype 1), exponential (2)
+ * or von Karman (3) power spectral density of correlation distance a, rms
+ * epsil and order kappa (rmedia__psdf_*, :530-679), DC removed, mean removed
+ * and scaled to rms epsil.  The volume is written to the device array xi over
+ * the memory box -- (-2:nz+3, -2:nx+3, -2:ny+3) with leading extents ld_k,
+ * ld_i, or (-2:nz+3, -2:nx+3) for ny = 1 -- with the cyclic wrap rdrmed__3d
+ * uses for cells outside 1..n (src/shared/m_rdrmed.f90:111-132), ready for
+ * swpc_vmodel_lhm_device or swpc_vmodel_lhm.  The random numbers are a
+ * counter-based stream of `seed` (gfortran's random_number stream of the
+ * reference cannot be reproduced), so a realisation depends on the seed
+ * alone.  Runs on `stream` (a cudaStream_t; NULL = the default stream) and
+ * blocks until xi is written; allocates about 2.1 x 4 B x nx ny nz of
+ * temporary device memory (volume, half spectrum, FFT plans) and frees it
+ * before it returns.  Returns SWPC_ERR_ARG, SWPC_ERR_NOMEM or SWPC_ERR_CUDA
+ * on failure. */
+#define SWPC_RMEDIA_GAUSS 1
+#define SWPC_RMEDIA_EXP 2
+#define SWPC_RMEDIA_VONKARMAN 3
+typedef struct swpc_rmedia_desc {
+    int ptype;
+    int nx, ny, nz;
+    float dx, dy, dz;
+    float a, epsil, kappa;
+    unsigned long long seed;
+} swpc_rmedia_desc;
+int swpc_rmedia_generate(const swpc_rmedia_desc *d, float *xi, int ld_k, int ld_i, void *stream);
 
 #ifdef __cplusplus
 }

@@ -36,7 +36,7 @@ WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 # every symbol the headers in include/ declare
 EXPORTS = [
     "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
-    "swpc_vmodel_lhm_device", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_absorb_setup_cerjan",
+    "swpc_vmodel_lhm_device", "swpc_vmodel_lhm_device_opt", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_absorb_setup_cerjan",
     "swpc_green_store_setup", "swpc_green_store", "swpc_green_fetch", "swpc_fbatch_green_fetch",
     "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
@@ -49,8 +49,8 @@ EXPORTS = [
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
-    "swpc_vmodel_lhm", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
-    "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt",
+    "swpc_vmodel_lhm", "swpc_vmodel_lhm_opt", "swpc_seawater_vel", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
+    "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt", "swpc_rmedia_generate",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
@@ -96,6 +96,13 @@ class Grid(C.Structure):
                 ("xbeg", C.c_float), ("ybeg", C.c_float), ("zbeg", C.c_float), ("tbeg", C.c_float)]
 
 
+class RmediaDesc(C.Structure):
+    """swpc_rmedia_desc of swpc_setup.h."""
+    _fields_ = [("ptype", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_float),
+                ("dy", C.c_float), ("dz", C.c_float), ("a", C.c_float), ("epsil", C.c_float), ("kappa", C.c_float),
+                ("seed", C.c_ulonglong)]
+
+
 _lib = None
 
 
@@ -132,6 +139,7 @@ def load():
         "swpc_sync": (i, [vp]),
         "swpc_upload_medium": (i, [vp, C.POINTER(MediumView)]),
         "swpc_vmodel_lhm_device": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i]),
+        "swpc_vmodel_lhm_device_opt": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i, i]),
         "swpc_vmodel_upload": (i, [vp, _FP, _FP, _FP, _FP, _FP, i, i]),
         "swpc_medium_setup_device": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i]),
         "swpc_kernel_setup": (i, [vp, _FP]),
@@ -180,6 +188,9 @@ def load():
         "swpc_kbeg_a": (None, [C.POINTER(Grid), _IP]),
         "swpc_vmodel_lhm": (i, [C.POINTER(Grid), i, _FP, _FP, _FP, _FP, _FP, _FP, f, _FP, f, _FP, _FP, _FP,
                                 _FP, _FP]),
+        "swpc_vmodel_lhm_opt": (i, [C.POINTER(Grid), i, _FP, _FP, _FP, _FP, _FP, _FP, f, _FP, f, _FP, _FP, _FP,
+                                    _FP, _FP, i]),
+        "swpc_seawater_vel": (f, [f, i]),
         "swpc_setup_medium": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP,
                                   _FP, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _FP, _FP]),
         "swpc_setup_medium_opt": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _FP,
@@ -189,6 +200,7 @@ def load():
                                      _IP, _IP, _IP, _FP, _FP]),
         "swpc_setup_medium_2d_opt": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _IP, _IP, _IP,
                                      _IP, _IP, _IP, _FP, _FP, i]),
+        "swpc_rmedia_generate": (i, [C.POINTER(RmediaDesc), _FP, i, i, vp]),
         "swpc_batch_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),
         "swpc_batch_step": (i, [vp, i]),
         "swpc_batch_run": (i, [vp, i, i]),

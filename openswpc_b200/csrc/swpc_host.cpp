@@ -203,9 +203,26 @@ static void vcheck(float &vp, float &vs, float &rho, float xi, float vmin, float
     if (rho < rhomin) rho = rhomin;
 }
 
+// seawater__vel (src/shared/m_seawater.f90:19-49): Munk's profile (eps = 0.00737) of depth z [km], or 1.5 km/s
+// without it, evaluated in double as the reference does
+float swpc_seawater_vel(float z, int munk_profile) {
+    const double eps = munk_profile ? 0.00737 : 0.0;
+    const double zc = 1300.0;
+    const double zb = 2 * ((double)z * 1000. - zc) / zc;
+    return (float)(1.5 * (1.0 + eps * (zb - 1.0 + std::exp(-zb))));
+}
+
 int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const float *rho0_in, const float *vp0_in,
                     const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut, const float *xi,
                     float rhomin, float *rho, float *lam, float *mu, float *qp, float *qs) {
+    return swpc_vmodel_lhm_opt(g, nlayer, depth, rho0_in, vp0_in, vs0_in, qp0_in, qs0_in, vcut, xi, rhomin, rho, lam,
+                               mu, qp, qs, 0);
+}
+
+int swpc_vmodel_lhm_opt(const swpc_grid *g, int nlayer, const float *depth, const float *rho0_in,
+                        const float *vp0_in, const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut,
+                        const float *xi, float rhomin, float *rho, float *lam, float *mu, float *qp, float *qs,
+                        int munk_profile) {
     if (nlayer < 1) return SWPC_ERR_ARG;
     std::vector<float> r0(nlayer), p0(nlayer), s0(nlayer), qa(nlayer), qb(nlayer);
     float vmax_r;
@@ -220,8 +237,12 @@ int swpc_vmodel_lhm(const swpc_grid *g, int nlayer, const float *depth, const fl
             for (int i = -2; i <= g->nx + 3; i++) {
                 const long e = g->ny > 1 ? b.idx(k, i, j) : ((long)(i + 2) * b.nk + (k + 2));
                 if (zs < depth[0]) {
-                    // air column (no ocean layer in this model family)
-                    rho[e] = 0.001f; mu[e] = 0.0f; lam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+                    if (zs < 0.0f) {   // air column (m_vmodel_lhm.f90:110-121)
+                        rho[e] = 0.001f; mu[e] = 0.0f; lam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+                    } else {           // seawater above depth(1) (:123-133)
+                        const float vp1 = 1.0f * swpc_seawater_vel(zs, munk_profile);
+                        rho[e] = 1.0f; mu[e] = 0.0f; lam[e] = 1.0f * vp1 * vp1; qp[e] = 1000000.0f; qs[e] = 1000000.0f;
+                    }
                     continue;
                 }
                 float rho1 = 0, vp1 = 0, vs1 = 0, qp1 = 0, qs1 = 0;

@@ -45,7 +45,8 @@ constexpr float kEpsF = 1.1920929e-07f;   // epsilon(1.0)
 // the layered model at one depth row k: the last layer l with z(k) >= depth(l)
 struct KRow {
     float r0, p0, s0, qa, qb;
-    int kind;   // 0 air (z < depth(1)), 1 layer with vcheck (vp, vs > 0), 2 layer without
+    int kind;   // 0 air (z < depth(1), z < 0), 1 layer with vcheck (vp, vs > 0), 2 layer without,
+                // 3 seawater (0 <= z < depth(1); p0 holds its lam)
 };
 
 void drop_graph(swpc_ctx *c) {
@@ -97,6 +98,10 @@ __global__ void vmodel_kernel(Geo g, const KRow *__restrict__ rows, int has_xi, 
         const KRow r = rows[k + 2];
         if (r.kind == 0) {
             rho[e] = 0.001f; mu[e] = 0.0f; lam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+            continue;
+        }
+        if (r.kind == 3) {
+            rho[e] = 1.0f; mu[e] = 0.0f; lam[e] = r.p0; qp[e] = 1000000.0f; qs[e] = 1000000.0f;
             continue;
         }
         float rho1 = r.r0, vp1 = r.p0, vs1 = r.s0;
@@ -272,6 +277,14 @@ constexpr int kGrid = 148 * 8, kBlock = 256;
 extern "C" int swpc_vmodel_lhm_device(swpc_ctx *c, int nlayer, const float *depth, const float *rho0,
                                       const float *vp0, const float *vs0, const float *qp0, const float *qs0,
                                       float vcut, float rhomin, float zbeg, const float *xi, int ld_k, int ld_i) {
+    return swpc_vmodel_lhm_device_opt(c, nlayer, depth, rho0, vp0, vs0, qp0, qs0, vcut, rhomin, zbeg, xi, ld_k, ld_i,
+                                      0);
+}
+
+extern "C" int swpc_vmodel_lhm_device_opt(swpc_ctx *c, int nlayer, const float *depth, const float *rho0,
+                                          const float *vp0, const float *vs0, const float *qp0, const float *qs0,
+                                          float vcut, float rhomin, float zbeg, const float *xi, int ld_k, int ld_i,
+                                          int munk_profile) {
     if (!c) return SWPC_ERR_ARG;
     if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the device medium setup is for the 3D code");
     if (nlayer < 1 || !depth || !rho0 || !vp0 || !vs0 || !qp0 || !qs0)
@@ -291,6 +304,10 @@ extern "C" int swpc_vmodel_lhm_device(swpc_ctx *c, int nlayer, const float *dept
     for (int k = -2; k <= g.nz + 3; k++) {
         const float zs = swpc_i2x(k, zbeg, sg.dz);
         KRow r = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0};
+        if (zs < depth[0] && !(zs < 0.0f)) {   // seawater, lam = 1.0 * vp * vp (m_vmodel_lhm.f90:123-133)
+            const float vp1 = 1.0f * swpc_seawater_vel(zs, munk_profile);
+            r = {1.0f, 1.0f * vp1 * vp1, 0.0f, 1000000.0f, 1000000.0f, 3};
+        }
         if (!(zs < depth[0])) {
             for (int l = 0; l < nlayer; l++)
                 if (zs >= depth[l]) {

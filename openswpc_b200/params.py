@@ -112,6 +112,7 @@ class Params:
     sw_wav_strain: bool = False
     abc_type: str = "pml"
     stabilize_pml: bool = False   # m_medium.f90:219-222 (3D)
+    munk_profile: bool = False    # Munk's seawater profile above depth(1) (m_vmodel_lhm.f90:53-54)
     # source depth fitted to a boundary depth: 'asis' or 'bd0'..'bd9' (m_source.f90:99, 262-270)
     sdep_fit: str = "asis"
     # boundary depths bddep(i, j, 0:9) of the memory box, shape (ny+6, nx+6, 10) in 3D and (nx+6, 10) in 2D, for
@@ -245,12 +246,12 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
              "fq_max": float, "fq_ref": float, "vcut": float, "rhomin": float, "stftype": str, "bf_mode": bool,
              "green_mode": bool, "green_cmp": str, "green_trise": float, "ntdec_r": int, "ntdec_w": int,
              "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str,
-             "stabilize_pml": bool, "sdep_fit": str}
+             "stabilize_pml": bool, "sdep_fit": str, "munk_profile": bool}
     args = {}
     for key, typ in types.items():
         if key in kv:
             args[key] = _conv(kv[key], typ)
-        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit"):
+        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit", "munk_profile"):
             raise KeyError(f"parameter {key} missing in strict mode")
     for key in ("z0_xy", "x0_yz", "y0_xz"):
         if key in kv:

@@ -137,9 +137,10 @@ class Medium2D:
             setattr(self, name, np.zeros(p.nx + 6, np.int32))
         L = p.layers
         arr = lambda a: np.array([getattr(l, a) for l in L], np.float32)
-        rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+        rc = lib.swpc_vmodel_lhm_opt(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
                                  fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, None, p.rhomin,
-                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs))
+                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs),
+                                     int(p.munk_profile))
         if rc:
             raise ValueError("vmodel_lhm failed")
         self.ts = np.zeros(3, np.float32)

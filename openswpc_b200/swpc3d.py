@@ -162,9 +162,9 @@ def lhm_model(p: Params, xi: np.ndarray | None = None):
     arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
     if xi is not None:
         xi = np.ascontiguousarray(xi, np.float32)
-    rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+    rc = lib.swpc_vmodel_lhm_opt(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
                              fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, fptr(xi), p.rhomin,
-                             fptr(rho), fptr(lam), fptr(mu), fptr(qp), fptr(qs))
+                             fptr(rho), fptr(lam), fptr(mu), fptr(qp), fptr(qs), int(p.munk_profile))
     if rc:
         raise ValueError("vmodel_lhm failed")
     vs = np.sqrt(mu / rho).astype(np.float32)
@@ -195,9 +195,10 @@ class Medium:
         if xi is not None:
             xi = np.ascontiguousarray(xi, np.float32)
             assert xi.shape == shape
-        rc = lib.swpc_vmodel_lhm(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
+        rc = lib.swpc_vmodel_lhm_opt(C.byref(g), len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
                                  fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, fptr(xi), p.rhomin,
-                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs))
+                                 fptr(self.rho), fptr(self.lam), fptr(self.mu), fptr(self.qp), fptr(self.qs),
+                                     int(p.munk_profile))
         if rc:
             raise ValueError("vmodel_lhm failed")
         self._setup(p)
@@ -284,9 +285,10 @@ class DeviceMedium:
                 xi = np.ascontiguousarray(xi, np.float32)
                 assert xi.shape == shape
                 xp = fptr(xi)
-        check(ctx, lib.swpc_vmodel_lhm_device(ctx, len(L), fptr(arr("depth")), fptr(arr("rho")), fptr(arr("vp")),
-                                              fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")), p.vcut, p.rhomin,
-                                              p.zbeg, xp, p.nz + 6, p.nx + 6))
+        check(ctx, lib.swpc_vmodel_lhm_device_opt(ctx, len(L), fptr(arr("depth")), fptr(arr("rho")),
+                                                  fptr(arr("vp")), fptr(arr("vs")), fptr(arr("qp")), fptr(arr("qs")),
+                                                  p.vcut, p.rhomin, p.zbeg, xp, p.nz + 6, p.nx + 6,
+                                                  int(p.munk_profile)))
         for name in self.MAPS:
             setattr(self, name, np.zeros(shape[:2], np.int32))
         self.ts = np.zeros(3, np.float32)

@@ -88,6 +88,8 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_green_store_setup": (None, [vp, i, _IP, _IP, _IP, i, i]),
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "o3d_set_sdep_fit": (None, [vp, i]),
+        "o3d_set_munk": (None, [vp, i]),
+        "o3d_seawater_vel": (f, [f, i]),
         "o3d_set_bddep": (None, [vp, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o3d_green_setup": (None, [vp, i, i, i, C.c_char, f, f, i]),
@@ -152,6 +154,7 @@ class Oracle3D:
             qp = np.zeros(shape, np.float32)
             qs = np.zeros(shape, np.float32)
             xi_c = None if xi is None else np.ascontiguousarray(xi, np.float32)
+            lib.o3d_set_munk(self.o, int(getattr(p, "munk_profile", False)))
             lib.o3d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
                                _f(arr("qp")), _f(arr("qs")), p.vcut, _f(xi_c), p.rhomin, _f(qp), _f(qs))
             lib.o3d_set_stabilize(self.o, int(getattr(p, "stabilize_pml", False)))
@@ -413,6 +416,7 @@ def load2d(variant: str = "f32") -> C.CDLL:
         "o2d_cerjan_setup": (None, [vp]),
         "o2d_set_stabilize": (None, [vp, i]),
         "o2d_set_bddep": (None, [vp, _FP]),
+        "o2d_set_munk": (None, [vp, i]),
         "o2d_set_sdep_fit": (None, [vp, i]),
         "o2d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, i]),
         "o2d_wav_setup": (i, [vp, i, _FP, _FP, _IP, i, i, i]),
@@ -450,6 +454,7 @@ class Oracle2D:
         arr = lambda a: np.array([getattr(l, a) for l in L], np.float32)
         qp = np.zeros(shape, np.float32)
         qs = np.zeros(shape, np.float32)
+        lib.o2d_set_munk(self.o, int(getattr(p, "munk_profile", False)))
         lib.o2d_vmodel_lhm(self.o, len(L), _f(arr("depth")), _f(arr("rho")), _f(arr("vp")), _f(arr("vs")),
                            _f(arr("qp")), _f(arr("qs")), p.vcut, None, p.rhomin, _f(qp), _f(qs))
         lib.o2d_set_stabilize(self.o, int(getattr(p, "stabilize_pml", False)))

@@ -55,6 +55,7 @@ typedef struct o2d {
     int *kfs, *kob, *kfs_top, *kfs_bot, *kob_top, *kob_bot;
     float *bddep;                /* (i, 0:NBD2) boundary depths (src/swpc_psv/m_global.f90 bddep) */
     int sdep_fit1;               /* sdep_fit: 0 'asis', 1 + n for 'bd<n>' (src/swpc_psv/m_source.f90:85) */
+    int munk;                    /* munk_profile of the ocean column */
     SPR c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     MPR rc40x, rc41x, rc40z, rc41z, rd40x, rd41x, rd40z, rd41z;
     float *fgxc, *fgxe, *fgzc, *fgze;
@@ -240,6 +241,17 @@ void o2d_destroy(o2d *o) {
     free(o);
 }
 
+/* seawater__vel (src/shared/m_seawater.f90:36-49) */
+static float o2d_seawater_vel(float z, int munk) {
+    double eps = munk ? 0.00737 : 0.0;
+    double zc = 1300.0;
+    double zb = 2 * ((double)z * 1000. - zc) / zc;
+    return (float)(1.5 * (1.0 + eps * (zb - 1.0 + exp(-zb))));
+}
+
+/* munk_profile switch; set before o2d_vmodel_lhm */
+void o2d_set_munk(o2d *o, int munk) { o->munk = munk; }
+
 /* vmodel_lhm in 2D (src/swpc_psv/m_vmodel_lhm.f90; same rule as 3D) with
  * the optional lhm_rmed perturbation (vcheck for P-SV, vcheck_sh for SH). */
 void o2d_vmodel_lhm(o2d *o, int nlayer, const float *depth, const float *rho0, const float *vp0, const float *vs0,
@@ -264,7 +276,14 @@ void o2d_vmodel_lhm(o2d *o, int nlayer, const float *depth, const float *rho0, c
             long e = I2(o, k, i);
             float zs = o->zc[k + 2];
             if (zs < depth[0]) {
-                o->frho[e] = 0.001f; o->fmu[e] = 0.0f; o->flam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+                /* air (zs < 0) or seawater: src/swpc_psv/m_vmodel_lhm.f90:102-121, lam = rho (vp^2 - 2 vs^2) */
+                if (zs < 0.0f) {
+                    o->frho[e] = 0.001f; o->fmu[e] = 0.0f; o->flam[e] = 0.0f; qp[e] = 10.0f; qs[e] = 10.0f;
+                } else {
+                    float rho1 = 1.0f, vp1 = 1.0f * o2d_seawater_vel(zs, o->munk), vs1 = 0.0f;
+                    o->frho[e] = rho1; o->fmu[e] = rho1 * vs1 * vs1; o->flam[e] = rho1 * (vp1 * vp1 - 2 * vs1 * vs1);
+                    qp[e] = 1000000.0f; qs[e] = 1000000.0f;
+                }
                 continue;
             }
             float rho1 = 0, vp1 = 0, vs1 = 0, q1 = 0, q2 = 0;

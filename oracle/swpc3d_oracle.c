@@ -76,6 +76,7 @@ typedef struct o3d {
     int *kfs, *kob, *kfs_top, *kfs_bot, *kob_top, *kob_bot;
     float *bddep;               /* (i, j, 0:NBD) */
     int sdep_fit1;              /* sdep_fit: 0 'asis', 1 + n for 'bd<n>' (m_source.f90:99) */
+    int munk;                   /* munk_profile of the ocean column (m_vmodel_lhm.f90:53-54) */
     /* kernel coefficients (m_kernel.f90:23-26) */
     SPR c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     MPR rc40x, rc41x, rc40y, rc41y, rc40z, rc41z;
@@ -392,6 +393,17 @@ void o3d_destroy(o3d *o) {
 /* m_vmodel_lhm_rmed.f90:84-227 (no ocean column, no earth flattening)      */
 /* xi: optional perturbation over the memory box (NULL = lhm)               */
 /* ------------------------------------------------------------------------ */
+/* seawater__vel: src/shared/m_seawater.f90:19-49 (Munk's profile in DP; eps = 0 gives 1.5 km/s) */
+float o3d_seawater_vel(float z, int munk) {
+    double eps = munk ? 0.00737 : 0.0;
+    double zc = 1300.0;
+    double zb = 2 * ((double)z * 1000. - zc) / zc;
+    return (float)(1.5 * (1.0 + eps * (zb - 1.0 + exp(-zb))));
+}
+
+/* munk_profile switch of the ocean column; set before o3d_vmodel_lhm */
+void o3d_set_munk(o3d *o, int munk) { o->munk = munk; }
+
 void o3d_vmodel_lhm(o3d *o, int nlayer, const float *depth, const float *rho0_in, const float *vp0_in,
                     const float *vs0_in, const float *qp0_in, const float *qs0_in, float vcut, const float *xi,
                     float rhomin, float *qp, float *qs) {
@@ -422,12 +434,18 @@ void o3d_vmodel_lhm(o3d *o, int nlayer, const float *depth, const float *rho0_in
     for (int k = o->kbeg_m; k <= o->kend_m; k++) {
         float zs = o->zc[k - o->kbeg_m];
         if (zs < depth[0]) {
-            /* air column (zs < 0); the ocean column is not modelled here */
+            /* air column (zs < 0) or seawater (0 <= zs < depth(1)): m_vmodel_lhm.f90:108-138 */
+            float vpw = 1.0f * o3d_seawater_vel(zs, o->munk);
             for (int j = o->jbeg_m; j <= o->jend_m; j++)
                 for (int i = o->ibeg_m; i <= o->iend_m; i++) {
                     long e = IDX3(o, k, i, j);
-                    o->frho[e] = 0.001f; o->fmu[e] = 0.0f; o->flam[e] = 0.0f;
-                    qp[e] = 10.0f; qs[e] = 10.0f;
+                    if (zs < 0.0f) {
+                        o->frho[e] = 0.001f; o->fmu[e] = 0.0f; o->flam[e] = 0.0f;
+                        qp[e] = 10.0f; qs[e] = 10.0f;
+                    } else {
+                        o->frho[e] = 1.0f; o->fmu[e] = 0.0f; o->flam[e] = 1.0f * vpw * vpw;
+                        qp[e] = 1000000.0f; qs[e] = 1000000.0f;
+                    }
                 }
             continue;
         }

@@ -51,7 +51,7 @@ def run_and_compare(p, g0, g1, steps):
         assert same_bits(g0.download(f), g1.download(f)), f
 
 
-@pytest.mark.parametrize("case", ["layers", "perturbed", "ocean_clipped"])
+@pytest.mark.parametrize("case", ["layers", "perturbed", "ocean_clipped", "seawater_munk"])
 def test_device_medium_equals_host_setup(case):
     """vmodel_lhm (+ lhm_rmed) and medium__setup in HBM: every field over the
     memory box, the six maps, ts, zeta and the velocity range equal the host
@@ -61,6 +61,9 @@ def test_device_medium_equals_host_setup(case):
     kw = {}
     if case == "ocean_clipped":
         kw = dict(layers=OCEAN, vcut=1.0, rhomin=2.75)
+    elif case == "seawater_munk":
+        # seawater of Munk's profile between z = 0 and depth(1) = 1.8 km (m_vmodel_lhm.f90:123-133)
+        kw = dict(layers=[Layer(1.8, 2.7, 5.5, 3.2, 300, 150)] + list(LAYERS[1:]), munk_profile=True)
     p = small3d(nx=56, ny=48, nz=44, na=8, nt=8, **kw)
     shape = (p.ny + 6, p.nx + 6, p.nz + 6)
     xi = None

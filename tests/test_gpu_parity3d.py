@@ -376,3 +376,22 @@ def test_stabilized_medium_run_matches_oracle():
     o.run(1, p.nt)
     assert same_bits(g.waveforms(), o.waveforms("v"))
     compare_state(g, o, p)
+
+
+def test_seawater_forward_run_matches_oracle():
+    """A run with seawater of Munk's profile above the first layer
+    (m_vmodel_lhm.f90:123-133): the ocean bottom lies below the free surface,
+    so the ocean-bottom stations ('obb', 'oba') and the 2nd-order bands of
+    both surfaces are exercised; traces and final state bitwise."""
+    from openswpc_b200.params import Layer
+    from tests.models import LAYERS
+
+    p = small3d(nt=60, munk_profile=True, layers=[Layer(1.8, 2.7, 5.5, 3.2, 300, 150)] + list(LAYERS[1:]))
+    g = Swpc3D(p)
+    o = Oracle3D(p)
+    assert (g.medium.kob[4:-4, 4:-4] > g.medium.kfs[4:-4, 4:-4]).all()
+    g.run(1, p.nt)
+    o.run(1, p.nt, ntdec_r=p.ntdec_r)
+    a, b = g.waveforms(_lib.WAV_V), o.waveforms("v")
+    assert np.linalg.norm(b) > 0 and same_bits(a, b)
+    compare_state(g, o, p)

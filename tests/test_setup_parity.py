@@ -416,3 +416,61 @@ def test_source_depth_fit_outside_the_model_is_refused():
         source_grid(p)
     with pytest.raises(ValueError, match="outside the model"):
         Oracle3D(p)
+
+
+def test_seawater_velocity_matches_oracle():
+    """seawater__vel (src/shared/m_seawater.f90:36-49): 1.5 km/s, or Munk's
+    profile (its minimum of 1.5 km/s at 1.3 km depth)."""
+    lib = _lib.load()
+    ol = oload()
+    for z in np.linspace(0.0, 8.0, 801, dtype=np.float32):
+        for munk in (0, 1):
+            assert np.float32(lib.swpc_seawater_vel(float(z), munk)) == np.float32(ol.o3d_seawater_vel(float(z), munk))
+    assert lib.swpc_seawater_vel(3.0, 0) == np.float32(1.5)
+    assert lib.swpc_seawater_vel(1.3, 1) == np.float32(1.5)
+    assert abs(lib.swpc_seawater_vel(0.0, 1) - 1.5 * (1 + 0.00737 * (np.exp(2.0) - 3.0))) < 1e-6
+
+
+def _ocean(q):
+    """An ocean above the layered medium: depth(1) = 1.2 km, so the cells with
+    0 <= z < 1.2 km are seawater."""
+    q.layers = [Layer(1.2, 2.7, 5.5, 3.2, 300, 150)] + list(q.layers[1:])
+    return q
+
+
+@pytest.mark.parametrize("munk", [False, True])
+def test_ocean_medium_bit_exact(munk):
+    """vmodel_lhm's seawater column (m_vmodel_lhm.f90:108-138) with and
+    without munk_profile: every medium field and integer map of the host
+    setup equals the oracle's; the ocean bottom lies below the free surface."""
+    p = _ocean(small3d(munk_profile=munk))
+    m = Medium(p)
+    o = Oracle3D(p)
+    for f in ("rho", "lam", "mu", "taup", "taus", "bx", "by", "bz", "muyz", "muxz", "muxy"):
+        assert np.array_equal(bits(getattr(m, f)), bits(o.array("f" + f))), f
+    for f in ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot"):
+        assert np.array_equal(getattr(m, f), o.array(f)), f
+    assert (m.kob[4:-4, 4:-4] > m.kfs[4:-4, 4:-4]).all()
+    # zbeg = -1.5, dz = 0.5: cells k = 4, 5 (z = 0.25, 0.75 km) are seawater, k = 6 (1.25 km) is rock; lam is
+    # the relaxed modulus of Q = 1e6, within 1e-5 of rho vp^2
+    water = m.lam[5, 5, 6:8]
+    assert (m.mu[5, 5, 6:8] == 0).all() and (m.rho[5, 5, 6:8] == 1).all() and m.mu[5, 5, 8] > 0
+    if munk:
+        assert (water > np.float32(2.25)).all() and water[0] > water[1]   # Munk's profile slows towards 1.3 km
+    else:
+        assert np.allclose(water, 2.25, rtol=1e-5, atol=0)
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_ocean_medium_2d_bit_exact(kind):
+    from openswpc_b200.swpc2d import Medium2D
+    from oracle.oracle import Oracle2D
+    from tests.models import small2d
+
+    p = _ocean(small2d(kind, munk_profile=True))
+    m = Medium2D(p)
+    o = Oracle2D(p, kind)
+    for f in ("rho", "lam", "mu", "taup", "taus"):
+        assert np.array_equal(bits(getattr(m, f)), bits(o.array("f" + f))), f
+    for f in ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot"):
+        assert np.array_equal(getattr(m, f), o.array(f)), f
