@@ -181,6 +181,12 @@ int swpc_vmodel_upload(swpc_ctx *ctx, const float *rho, const float *lam, const 
 int swpc_medium_setup_device(swpc_ctx *ctx, float fq_min, float fq_max, float fq_ref, float *ts, float *scal,
                              int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, int *kbeg_a,
                              int ld_i2);
+/* The same with the input-file switch stabilize_pml (m_medium.f90:219-222,
+ * stabilize_absorber :276-340) applied in HBM before the averaged medium, as
+ * swpc_setup_medium_opt does on the host. */
+int swpc_medium_setup_device_opt(swpc_ctx *ctx, float fq_min, float fq_max, float fq_ref, float *ts, float *scal,
+                                 int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot,
+                                 int *kbeg_a, int ld_i2, int stabilize_pml);
 
 /* kernel__setup (src/swpc_3d/m_kernel.f90:30-73): FD coefficients from dx,
  * dy, dz and the Zener coefficients c1, c2, d1, d2 from ts(1:nm) and dt,
@@ -265,6 +271,15 @@ int swpc_green_source(swpc_ctx *ctx, int it);       /* m_green.f90:597-632   */
  * for call-order fidelity. */
 int swpc_comm_stress(swpc_ctx *ctx);
 int swpc_comm_vel(swpc_ctx *ctx);
+/* Plane-wave mode (pw_mode, src/swpc_3d/m_source.f90:67-79): with on != 0
+ * the absorber updates first extrapolate the ghost planes of the four side
+ * faces from inside (V before the stress update, S before the velocity
+ * update; m_absorb_p.f90:136-243, 324-431), and swpc_comm_stress /
+ * swpc_comm_vel (and swpc_step, swpc_run) zero the ghost planes that
+ * global__comm_stress / global__comm_vel zero on a single domain.  The
+ * initial wavefield comes from swpc_pw_setup (swpc_setup.h) through
+ * swpc_upload_field.  FP32 storage and the PML only. */
+int swpc_set_pw_mode(swpc_ctx *ctx, int on);
 int swpc_wav_store(swpc_ctx *ctx, int it);          /* m_wav.f90:400-628     */
 /* kernel__vmax (m_kernel.f90:328-352): max |V| one cell below the ocean
  * bottom; blocks.  Sets SWPC_ERR_DIVERGED when max*UC > 1e5

@@ -114,6 +114,21 @@ void swpc_damping_profiles(const swpc_grid *g, float fcut, float *gxc, float *gx
 void swpc_cerjan_profiles(const swpc_grid *g, float *gx_c, float *gx_b, float *gy_c, float *gy_b, float *gz_c,
                           float *gz_b);
 
+/* pw_setup (src/swpc_3d/m_source.f90:315-465): the initial wavefield of the
+ * plane-wave mode (pw_mode = .true.) from the medium after medium__setup
+ * (rho, lam, mu over the memory box).  ps = 0 for a P wave, 1 for an S wave;
+ * the front lies at depth pw_ztop with length pw_zlen [km] along the
+ * direction of strike and dip (rake: polarisation of the S wave) [deg],
+ * shaped by the moment-rate function stftype (SWPC_STF_*).  Writes V and S
+ * over the memory box (cells whose wave speed is below epsilon(1.0) are left
+ * as they are) and the cut-off frequency fcut of the PML profiles
+ * (:443-462).  The run then has no source grid, its output moment is
+ * M0 = 1 / UC (:72-79), and swpc_set_pw_mode switches on the zero-derivative
+ * side boundary of the absorber. */
+int swpc_pw_setup(const swpc_grid *g, const float *rho, const float *lam, const float *mu, float pw_ztop,
+                  float pw_zlen, int ps, float strike, float dip, float rake, int stftype, float *vx, float *vy,
+                  float *vz, float *sxx, float *syy, float *szz, float *syz, float *sxz, float *sxy, float *fcut);
+
 /* Random media (src/shared/m_rmedia.f90): rmedia__3dgen (:176-307) for
  * ny > 1 and rmedia__2dgen (:424-) for ny = 1, generated on the current CUDA
  * device.  Uniform random numbers in [0, 1) over nx x ny x nz cells, their

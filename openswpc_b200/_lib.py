@@ -36,7 +36,7 @@ WAV_V, WAV_U, WAV_STRESS, WAV_STRAIN = 1, 2, 4, 8
 # every symbol the headers in include/ declare
 EXPORTS = [
     "swpc_create", "swpc_destroy", "swpc_last_error", "swpc_stream", "swpc_sync", "swpc_upload_medium",
-    "swpc_vmodel_lhm_device", "swpc_vmodel_lhm_device_opt", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_absorb_setup_cerjan",
+    "swpc_vmodel_lhm_device", "swpc_vmodel_lhm_device_opt", "swpc_vmodel_upload", "swpc_medium_setup_device", "swpc_medium_setup_device_opt", "swpc_absorb_setup_cerjan",
     "swpc_green_store_setup", "swpc_green_store", "swpc_green_fetch", "swpc_fbatch_green_fetch",
     "swpc_kernel_setup", "swpc_absorb_setup", "swpc_source_setup", "swpc_bodyforce_setup", "swpc_green_setup",
     "swpc_wav_setup", "swpc_kernel_update_stress", "swpc_absorb_update_stress", "swpc_kernel_update_vel",
@@ -50,7 +50,7 @@ EXPORTS = [
     # swpc_setup.h
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_vmodel_lhm_opt", "swpc_seawater_vel", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
-    "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt", "swpc_rmedia_generate",
+    "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt", "swpc_rmedia_generate", "swpc_pw_setup", "swpc_set_pw_mode",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
@@ -142,6 +142,7 @@ def load():
         "swpc_vmodel_lhm_device_opt": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i, i]),
         "swpc_vmodel_upload": (i, [vp, _FP, _FP, _FP, _FP, _FP, i, i]),
         "swpc_medium_setup_device": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i]),
+        "swpc_medium_setup_device_opt": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i, i]),
         "swpc_kernel_setup": (i, [vp, _FP]),
         "swpc_absorb_setup": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "swpc_absorb_setup_cerjan": (i, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
@@ -201,6 +202,8 @@ def load():
         "swpc_setup_medium_2d_opt": (i, [C.POINTER(Grid), f, f, f, _FP, _FP, _FP, _FP, _FP, _FP, _FP, _IP, _IP, _IP,
                                      _IP, _IP, _IP, _FP, _FP, i]),
         "swpc_rmedia_generate": (i, [C.POINTER(RmediaDesc), _FP, i, i, vp]),
+        "swpc_pw_setup": (i, [C.POINTER(Grid), _FP, _FP, _FP, f, f, i, f, f, f, i] + [_FP] * 9 + [_FP]),
+        "swpc_set_pw_mode": (i, [vp, i]),
         "swpc_batch_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),
         "swpc_batch_step": (i, [vp, i]),
         "swpc_batch_run": (i, [vp, i, i]),

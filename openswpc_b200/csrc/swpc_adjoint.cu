@@ -669,6 +669,7 @@ static int adj_ready(swpc_ctx *c) {
     if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "the adjoint is implemented for the 3D solver");
     if (c->prec != SWPC_PREC_F32) return err(c, SWPC_ERR_ARG, "the adjoint needs FP32 storage");
     if (c->abc != 0) return err(c, SWPC_ERR_STATE, "the adjoint is implemented for the PML (not the Cerjan sponge)");
+    if (c->pw_mode) return err(c, SWPC_ERR_STATE, "the adjoint is not implemented for the plane-wave mode");
     if (!c->medium_ready || !c->kernel_ready || (c->d.na > 0 && !c->absorb_ready))
         return err(c, SWPC_ERR_STATE, "medium, kernel and absorber setup must precede the adjoint");
     ACK(cudaSetDevice(c->device));

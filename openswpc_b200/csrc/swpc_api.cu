@@ -1040,6 +1040,7 @@ static int launch_vel_kernel(swpc_ctx *c, int mask);
 static int launch_stress(swpc_ctx *c, int mask) {
     RC(check_ready(c));
     if (!is3d(c)) return update_stress_2d(c, mask);
+    if (mask & 2) RC(pw_fill(c, 0));   // plane-wave side boundary before the absorber update
     if (c->abc == 1) {
         // Cerjan: the interior update over the whole domain, then the sponge
         // (absorb__update_stress's dispatch, m_absorb.f90:43-58)
@@ -1086,6 +1087,7 @@ static int launch_stress_kernel(swpc_ctx *c, int mask) {
 static int launch_vel(swpc_ctx *c, int mask) {
     RC(check_ready(c));
     if (!is3d(c)) return update_vel_2d(c, mask);
+    if (mask & 2) RC(pw_fill(c, 1));
     if (c->abc == 1) {
         // Cerjan (absorb__update_vel's dispatch, m_absorb.f90:60-75)
         if (mask & 1) RC(launch_vel_kernel(c, 1));
@@ -1218,8 +1220,19 @@ extern "C" int swpc_update_vel(swpc_ctx *c) { PREP(c); return launch_vel(c, 3); 
 extern "C" int swpc_source_stressglut(swpc_ctx *c, int it) { return c ? launch_glut(c, it, nullptr) : SWPC_ERR_ARG; }
 extern "C" int swpc_source_bodyforce(swpc_ctx *c, int it) { return c ? launch_bf(c, it, nullptr) : SWPC_ERR_ARG; }
 extern "C" int swpc_green_source(swpc_ctx *c, int it) { return c ? launch_green(c, it, nullptr) : SWPC_ERR_ARG; }
-extern "C" int swpc_comm_stress(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
-extern "C" int swpc_comm_vel(swpc_ctx *c) { return c ? SWPC_OK : SWPC_ERR_ARG; }
+// single domain: the exchange only zeroes ghost planes, which no kernel writes except in plane-wave mode
+extern "C" int swpc_comm_stress(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!c->pw_mode) return SWPC_OK;
+    PREP(c);
+    return pw_comm_zero(c, 1);
+}
+extern "C" int swpc_comm_vel(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!c->pw_mode) return SWPC_OK;
+    PREP(c);
+    return pw_comm_zero(c, 0);
+}
 extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(c, it, nullptr); }
 
 // main.f90:125-144 loop body (report__progress is driven by the caller
@@ -1233,6 +1246,7 @@ static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
     }
     RC(launch_stress(c, 3));
     RC(launch_glut(c, it, d_it));
+    RC(pw_comm_zero(c, 1));   // global__comm_stress (no-op outside plane-wave mode)
     if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) {
         // P-SV applies body forces between the interior and absorber velocity
         // updates (src/swpc_psv/main.f90:106-110)
@@ -1244,6 +1258,7 @@ static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
         RC(launch_bf(c, it, d_it));
     }
     RC(launch_green(c, it, d_it));
+    RC(pw_comm_zero(c, 0));   // global__comm_vel
     return SWPC_OK;
 }
 

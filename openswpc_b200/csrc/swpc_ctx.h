@@ -86,6 +86,8 @@ struct swpc_ctx {
 
     // absorber: 0 ADE-CFS PML, 1 Cerjan sponge (abc_type, m_absorb.f90:25-75)
     int abc = 0;
+    // plane-wave mode (pw_mode, m_source.f90:67-79): zero-derivative side boundary of the PML updates
+    int pw_mode = 0;
     float *cj = nullptr;   // Cerjan factors: gx_c gx_b (nx) gy_c gy_b (ny) gz_c gz_b (nz)
     // PML
     bool absorb_ready = false;
@@ -208,6 +210,10 @@ int snap_clear(swpc_ctx *c);   // frames, displacement accumulators and maxima b
 int step_state(swpc_ctx *c, int it);
 void adj_free(swpc_ctx *c);   // swpc_adjoint.cu
 int green_store_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_green.cu
+// plane-wave mode (swpc_pw.cu): the ghost planes of V (which = 0) or S (1) extrapolated from inside, and the
+// ghost planes global__comm_vel / global__comm_stress zero on a single domain
+int pw_fill(swpc_ctx *c, int which);
+int pw_comm_zero(swpc_ctx *c, int which);
 // the same for nmem wavefields at V[q] + m * vstride (reciprocity batch), with
 // per-member accumulators (12 ng each) and outputs (ntw ncmp ng each)
 int green_store_members(swpc_ctx *c, float *const *V, long long vstride, int nmem, float *acc, float *out, int it,

@@ -202,6 +202,7 @@ extern "C" int swpc_fbatch_create(swpc_ctx *c, int nmem, swpc_fbatch **out) {
     if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the reciprocity batch is a 3D feature");
     if (c->prec != SWPC_PREC_F32) return set_err(c, SWPC_ERR_ARG, "the reciprocity batch needs FP32 storage");
     if (c->abc != 0) return set_err(c, SWPC_ERR_STATE, "the reciprocity batch runs with the PML");
+    if (c->pw_mode) return set_err(c, SWPC_ERR_STATE, "the reciprocity batch has no plane-wave mode");
     if (!c->medium_ready || !c->kernel_ready || (c->d.na > 0 && !c->absorb_ready))
         return set_err(c, SWPC_ERR_STATE, "medium, kernel and absorber setup must precede swpc_fbatch_create");
     if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, SWPC_ERR_CUDA, "cudaSetDevice failed");

@@ -690,3 +690,72 @@ void swpc_cerjan_profiles(const swpc_grid *g, float *gx_c, float *gx_b, float *g
 }
 
 }  // extern "C"
+
+// pw_setup (src/swpc_3d/m_source.f90:315-465): the plane-wave initial condition.  Every cell of the memory box
+// whose wave speed reaches epsilon(1.0) gets the velocities and stresses of a plane P or S wave travelling along
+// the direction (strike, dip), shaped by the moment-rate function over the rotated coordinate (zeta, length
+// pw_zlen, front at depth pw_ztop); velocities are evaluated half a time step ahead on their staggered points.
+// Single precision with the reference's expression order; fcut from the wave speed at the grid centre and depth
+// pw_ztop (:443-462).
+extern "C" int swpc_pw_setup(const swpc_grid *g, const float *rho, const float *lam, const float *mu, float pw_ztop,
+                  float pw_zlen, int ps, float strike, float dip, float rake, int stftype, float *vx, float *vy,
+                  float *vz, float *sxx, float *syy, float *szz, float *syz, float *sxz, float *sxy, float *fcut) {
+    if (g->ny <= 1 || !(pw_zlen > 0.0f) || (ps != 0 && ps != 1)) return SWPC_ERR_ARG;
+    const Box b = make_box(g);
+    auto rad = [](float deg) { return (float)(kPi / 180.0 * (double)deg); };   // std__deg2rad (m_std.f90:132-139)
+    const float tf = rad(strike), td = rad(dip), tl = rad(rake);
+    const float sd = sinf(td), cd = cosf(td), sf = sinf(tf), cf = cosf(tf);
+    const float sl = sinf(tl), cl = cosf(tl), c2d = cosf(2 * td), c2f = cosf(2 * tf);
+    const float dx = g->dx, dy = g->dy, dz = g->dz;
+    auto speed = [&](long e) {
+        return ps == 0 ? sqrtf((lam[e] + 2 * mu[e]) / rho[e]) : sqrtf(mu[e] / rho[e]);
+    };
+#pragma omp parallel for schedule(static)
+    for (int j = -2; j <= g->ny + 3; j++)
+        for (int i = -2; i <= g->nx + 3; i++)
+            for (int k = -2; k <= g->nz + 3; k++) {
+                const long e = b.idx(k, i, j);
+                const float v = speed(e);
+                if (v < kEps) continue;
+                const float x0 = g->xbeg + (i - 0.5f) * dx, y0 = g->ybeg + (j - 0.5f) * dy;
+                const float z0 = g->zbeg + (k - 0.5f) * dz - pw_ztop;
+                const float x1 = x0 + dx / 2.0f, y1 = y0 + dy / 2.0f, z1 = z0 + dz / 2.0f;
+                const float ahead = g->dt / 2.0f * v;
+                auto stf = [&](float x, float y, float z, float shift) {
+                    const float zeta = sd * sf * x - sd * cf * y + cd * z;
+                    return swpc::momentrate(shift != 0.0f ? zeta + shift : zeta, stftype, 0.0f, pw_zlen);
+                };
+                const float s_ii = stf(x0, y0, z0, 0.0f);
+                const float s_vx = stf(x1, y0, z0, ahead), s_vy = stf(x0, y1, z0, ahead), s_vz = stf(x0, y0, z1, ahead);
+                const float s_yz = stf(x0, y1, z1, 0.0f), s_xz = stf(x1, y0, z1, 0.0f), s_xy = stf(x1, y1, z0, 0.0f);
+                const float la0 = lam[e], mu0 = mu[e];
+                if (ps == 0) {
+                    vx[e] = -sd * sf * s_vx;
+                    vy[e] = sd * cf * s_vy;
+                    vz[e] = -cd * s_vz;
+                    sxx[e] = -(la0 + 2 * mu0 * sd * sd * sf * sf) * s_ii / v;
+                    syy[e] = -(la0 + 2 * mu0 * sd * sd * cf * cf) * s_ii / v;
+                    szz[e] = -(la0 + 2 * mu0 * cd * cd) * s_ii / v;
+                    syz[e] = 2 * mu0 * sd * cd * cf * s_yz / v;
+                    sxz[e] = -2 * mu0 * sd * cd * sf * s_xz / v;
+                    sxy[e] = 2 * mu0 * sd * cd * sf * s_xy / v;
+                } else {
+                    const float ax = cl * cf + sl * cd * sf, ay = cl * sf - sl * cd * cf;
+                    vx[e] = ax * s_vx;
+                    vy[e] = ay * s_vy;
+                    vz[e] = -sl * sd * s_vz;
+                    sxx[e] = 2 * mu0 * sd * sf * ax * s_ii / v;
+                    syy[e] = -2 * mu0 * sd * cf * ay * s_ii / v;
+                    szz[e] = -2 * mu0 * cd * sl * sd * s_ii / v;
+                    syz[e] = mu0 * (cl * cd * sf - sl * c2d * cf) * s_yz / v;
+                    sxz[e] = mu0 * (cl * cd * cf + sl * c2d * sf) * s_xz / v;
+                    sxy[e] = -mu0 * (cl * sd * c2f + 2 * sl * sd * cd * sf * cf) * s_xy / v;
+                }
+            }
+    const float xend = g->xbeg + g->nx * dx, yend = g->ybeg + g->ny * dy;
+    const int ic = swpc_x2i((g->xbeg + xend) / 2, g->xbeg, dx), jc = swpc_x2i((g->ybeg + yend) / 2, g->ybeg, dy);
+    const int kc = swpc_x2i(pw_ztop, g->zbeg, dz);
+    if (ic < -2 || ic > g->nx + 3 || jc < -2 || jc > g->ny + 3 || kc < -2 || kc > g->nz + 3) return SWPC_ERR_ARG;
+    *fcut = speed(b.idx(kc, ic, jc)) / pw_zlen;
+    return SWPC_OK;
+}

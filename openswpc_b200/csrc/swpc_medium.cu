@@ -120,6 +120,53 @@ __global__ void vmodel_kernel(Geo g, const KRow *__restrict__ rows, int has_xi, 
     }
 }
 
+// stabilize_absorber (m_medium.f90:276-340), one thread per column i, j in
+// [0, n+1]: from the first absorber depth within two columns (kbeg_a,
+// m_global.f90:336-345) down, a low-velocity layer of at most 20 cells takes
+// the medium of the cell above it, then shear velocities below 0.4 vmax are
+// raised to it with vp = sqrt(3) vs.  The walk down a column is sequential,
+// as each cell compares with the (possibly replaced) cell above.
+__global__ void stabilize_kernel(Geo g, int na, float vmax, float *rho, float *lam, float *mu, float *taup,
+                                 float *taus) {
+    const int ni = g.nx + 2, nj = g.ny + 2;
+    const long long ncol = (long long)ni * nj;
+    const float vmin_pml = vmax * 0.4f;
+    const int lv_thick = 20;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncol; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)(q / ni);
+        // min of kbeg_a over i-2..i+2, j-2..j+2: 1 when a side absorber column is among them
+        const bool side = i - 2 <= na || g.nx - na + 1 <= i + 2 || j - 2 <= na || g.ny - na + 1 <= j + 2;
+        const int k0 = side ? 1 : g.nz - na + 1;
+        for (int k = k0; k <= g.nz; k++) {
+            const long long e = cell_index(g, k, i, j), u = cell_index(g, k - 1, i, j);
+            if (lam[e] < lam[u] || mu[e] < mu[u]) {
+                int k2 = k + 1;
+                for (; k2 <= g.nz; k2++) {
+                    const long long e2 = cell_index(g, k2, i, j), u2 = cell_index(g, k2 - 1, i, j);
+                    if (lam[e2] > lam[u2] || mu[e2] > mu[u2]) break;
+                }
+                if (k2 - k <= lv_thick) {
+                    rho[e] = rho[u]; lam[e] = lam[u]; mu[e] = mu[u]; taup[e] = taup[u]; taus[e] = taus[u];
+                    k = k2 - 1;
+                }
+            }
+        }
+        for (int k = k0; k <= g.nz; k++) {
+            const long long e = cell_index(g, k, i, j);
+            float vp = __fsqrt_rn(__fdiv_rn(__fadd_rn(lam[e], __fmul_rn(2.0f, mu[e])), rho[e]));
+            float vs = __fsqrt_rn(__fdiv_rn(mu[e], rho[e]));
+            if (vs < kEpsF) continue;   // ocean and air
+            const float gamma = __fsqrt_rn(3.0f);
+            if (vs < vmin_pml) {
+                vs = vmin_pml;
+                vp = __fmul_rn(vs, gamma);
+                lam[e] = __fmul_rn(rho[e], __fsub_rn(__fmul_rn(vp, vp), __fmul_rn(2.0f, __fmul_rn(vs, vs))));
+                mu[e] = __fmul_rn(rho[e], __fmul_rn(vs, vs));
+            }
+        }
+    }
+}
+
 // absorber homogenisation (m_medium.f90:124-190): the x sides copy column
 // na+1 / nx-na, then the y sides row na+1 / ny-na, then the bottom layer
 // nz-na.  The three passes compose to one gather from the clamped cell,
@@ -354,6 +401,13 @@ extern "C" int swpc_vmodel_upload(swpc_ctx *c, const float *rho, const float *la
 extern "C" int swpc_medium_setup_device(swpc_ctx *c, float fq_min, float fq_max, float fq_ref, float *ts,
                                         float *scal, int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top,
                                         int *kob_bot, int *kbeg_a, int ld_i2) {
+    return swpc_medium_setup_device_opt(c, fq_min, fq_max, fq_ref, ts, scal, kfs, kob, kfs_top, kfs_bot, kob_top,
+                                        kob_bot, kbeg_a, ld_i2, 0);
+}
+
+extern "C" int swpc_medium_setup_device_opt(swpc_ctx *c, float fq_min, float fq_max, float fq_ref, float *ts,
+                                            float *scal, int *kfs, int *kob, int *kfs_top, int *kfs_bot,
+                                            int *kob_top, int *kob_bot, int *kbeg_a, int ld_i2, int stabilize_pml) {
     if (!c) return SWPC_ERR_ARG;
     if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the device medium setup is for the 3D code");
     if (!c->vmodel_ready) return set_err(c, SWPC_ERR_STATE, "no model on the device (swpc_vmodel_lhm_device or swpc_vmodel_upload)");
@@ -397,6 +451,19 @@ extern "C" int swpc_medium_setup_device(swpc_ctx *c, float fq_min, float fq_max,
     }
     if (!rc) rc = cuda_check(c, cudaMemcpyAsync(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost, c->stream),
                              "cudaMemcpyAsync");
+    if (!rc && stabilize_pml) {
+        // stabilize_pml (m_medium.f90:219-222) with the velocity maximum of velocity_minmax
+        rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        float vmx = -1.0f;
+        if (mm[0] != 0u) {
+            const unsigned b = mm[0] - 1u;
+            memcpy(&vmx, &b, sizeof(float));
+        }
+        if (!rc) {
+            stabilize_kernel<<<kGrid, kBlock, 0, c->stream>>>(g, na, vmx, rho, lam, mu, taup, taus);
+            rc = cuda_check(c, cudaGetLastError(), "stabilize_kernel");
+        }
+    }
     if (!rc) rc = average_medium(c);
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     cudaFree(d_mm);

@@ -113,6 +113,14 @@ class Params:
     abc_type: str = "pml"
     stabilize_pml: bool = False   # m_medium.f90:219-222 (3D)
     munk_profile: bool = False    # Munk's seawater profile above depth(1) (m_vmodel_lhm.f90:53-54)
+    # plane-wave mode (m_source.f90:67-79, pw_setup :315-465): a plane P or S wave in place of a source grid
+    pw_mode: bool = False
+    pw_ztop: float = 1e30
+    pw_zlen: float = -1.0
+    pw_ps: str = ""
+    pw_strike: float = 0.0
+    pw_dip: float = 0.0
+    pw_rake: float = 0.0
     # source depth fitted to a boundary depth: 'asis' or 'bd0'..'bd9' (m_source.f90:99, 262-270)
     sdep_fit: str = "asis"
     # boundary depths bddep(i, j, 0:9) of the memory box, shape (ny+6, nx+6, 10) in 3D and (nx+6, 10) in 2D, for
@@ -246,12 +254,13 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
              "fq_max": float, "fq_ref": float, "vcut": float, "rhomin": float, "stftype": str, "bf_mode": bool,
              "green_mode": bool, "green_cmp": str, "green_trise": float, "ntdec_r": int, "ntdec_w": int,
              "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str,
-             "stabilize_pml": bool, "sdep_fit": str, "munk_profile": bool}
+             "stabilize_pml": bool, "sdep_fit": str, "munk_profile": bool, "pw_mode": bool, "pw_ztop": float,
+             "pw_zlen": float, "pw_ps": str, "pw_strike": float, "pw_dip": float, "pw_rake": float}
     args = {}
     for key, typ in types.items():
         if key in kv:
             args[key] = _conv(kv[key], typ)
-        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit", "munk_profile"):
+        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit", "munk_profile") and not key.startswith("pw_"):
             raise KeyError(f"parameter {key} missing in strict mode")
     for key in ("z0_xy", "x0_yz", "y0_xz"):
         if key in kv:
@@ -265,7 +274,7 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
     base = Path(path).parent
     if kv.get("vmodel_type", "lhm") == "lhm" and "fn_lhm" in kv:
         p.layers = read_lhm(_resolve(base, kv["fn_lhm"]))
-    if "fn_stf" in kv and not p.green_mode:
+    if "fn_stf" in kv and not p.green_mode and not p.pw_mode:
         p.sources = read_sources(_resolve(base, kv["fn_stf"]), kv.get("stf_format", "xym0ij"), p.bf_mode)
     if "fn_stloc" in kv:
         p.stations = read_stations(_resolve(base, kv["fn_stloc"]))

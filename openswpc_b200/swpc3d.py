@@ -270,8 +270,6 @@ class DeviceMedium:
         L = p.layers
         if not L:
             raise ValueError("a layered (lhm) velocity model is required")
-        if p.stabilize_pml:
-            raise ValueError("stabilize_pml is applied by the host setup (Medium), not on the device")
         arr = lambda attr: np.array([getattr(l, attr) for l in L], np.float32)
         shape = (p.ny + 6, p.nx + 6, p.nz + 6)
         xp = None
@@ -293,8 +291,9 @@ class DeviceMedium:
             setattr(self, name, np.zeros(shape[:2], np.int32))
         self.ts = np.zeros(3, np.float32)
         scal = np.zeros(3, np.float32)
-        check(ctx, lib.swpc_medium_setup_device(ctx, p.fq_min, p.fq_max, p.fq_ref, fptr(self.ts), fptr(scal),
-                                                *(iptr(getattr(self, n)) for n in self.MAPS), p.nx + 6))
+        check(ctx, lib.swpc_medium_setup_device_opt(ctx, p.fq_min, p.fq_max, p.fq_ref, fptr(self.ts), fptr(scal),
+                                                    *(iptr(getattr(self, n)) for n in self.MAPS), p.nx + 6,
+                                                    int(p.stabilize_pml)))
         self.zeta, self.vmin, self.vmax = (float(x) for x in scal)
 
 
@@ -335,10 +334,15 @@ class Swpc3D:
             check(self.ctx, self.lib.swpc_upload_medium(self.ctx, C.byref(m.view(average_on_device))))
         check(self.ctx, self.lib.swpc_kernel_setup(self.ctx, fptr(m.ts)))
         # source__setup (m_source.f90) or green__setup (m_green.f90)
-        self.src = source_grid(p)
+        if p.pw_mode and p.green_mode:
+            raise ValueError("pw_mode and green_mode exclude each other (m_source.f90:69)")
+        self.src = source_grid(Params(**{**p.__dict__, "sources": [], "bf_mode": False})) if p.pw_mode \
+            else source_grid(p)
         self.M0, self.UC = self.src.M0, self.src.UC
         stf = _lib.STF_CODES[p.stftype]
-        if p.green_mode:
+        if p.pw_mode:
+            self._pw_setup(p, stf)
+        elif p.green_mode:
             st = p.stations[p.green_station]
             self.M0 = 1.0
             i, j, k = station_grid(Params(**{**p.__dict__, "stations": [st]}), m.kfs, m.kob)
@@ -390,6 +394,30 @@ class Swpc3D:
         self.snap_nframes = 0
         if p.snaps:
             self.snap__setup()
+
+    def _pw_setup(self, p: Params, stf: int):
+        """pw_setup (m_source.f90:315-465): the plane-wave initial wavefield
+        from the host medium, uploaded over the memory box; no source grid,
+        M0 = 1 / UC, the PML's fcut from the wave speed at the front, and the
+        zero-derivative side boundary switched on."""
+        if not isinstance(self.medium, Medium):
+            raise ValueError("the plane-wave setup reads the host medium (Medium), not the device-built one")
+        if p.pw_ps.lower() not in ("p", "s"):
+            raise ValueError("pw_ps must be 'P' or 'S'")
+        m = self.medium
+        shape = m.rho.shape
+        f = [np.zeros(shape, np.float32) for _ in range(9)]
+        fcut = C.c_float()
+        rc = self.lib.swpc_pw_setup(C.byref(grid_struct(p)), fptr(m.rho), fptr(m.lam), fptr(m.mu), p.pw_ztop,
+                                    p.pw_zlen, 0 if p.pw_ps.lower() == "p" else 1, p.pw_strike, p.pw_dip, p.pw_rake,
+                                    stf, *(fptr(a) for a in f), C.byref(fcut))
+        if rc:
+            raise ValueError("pw_setup failed (pw_zlen > 0 and pw_ztop inside the grid are required)")
+        for q, a in enumerate(f):
+            self.upload(_lib.F_VX + q, a)
+        self.M0 = float(f32(1.0) / f32(self.UC))
+        self.fcut = float(fcut.value)
+        check(self.ctx, self.lib.swpc_set_pw_mode(self.ctx, 1))
 
     # -- lifetime ---------------------------------------------------------
     def close(self):

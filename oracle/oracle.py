@@ -89,6 +89,7 @@ def load(variant: str = "f32", kind: str = "3d") -> C.CDLL:
         "o3d_set_profiles": (None, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "o3d_set_sdep_fit": (None, [vp, i]),
         "o3d_set_munk": (None, [vp, i]),
+        "o3d_pw_setup": (None, [vp, f, f, i, f, f, f, i]),
         "o3d_seawater_vel": (f, [f, i]),
         "o3d_set_bddep": (None, [vp, _FP]),
         "o3d_source_setup": (i, [vp, i, i, _FP, _FP, _FP, _FP, _FP, _FP, _FP, i]),
@@ -174,7 +175,12 @@ class Oracle3D:
         lib.o3d_kernel_setup(self.o)
         # sources
         stf = STF[p.stftype]
-        if p.green_mode:
+        if getattr(p, "pw_mode", False):
+            # pw_setup (m_source.f90:315-465) in place of a source grid
+            lib.o3d_pw_setup(self.o, p.pw_ztop, p.pw_zlen, 0 if p.pw_ps.lower() == "p" else 1, p.pw_strike,
+                             p.pw_dip, p.pw_rake, stf)
+            self.nsrc = 0
+        elif p.green_mode:
             self.nsrc = 0
         else:
             S = p.sources

@@ -77,6 +77,7 @@ typedef struct o3d {
     float *bddep;               /* (i, j, 0:NBD) */
     int sdep_fit1;              /* sdep_fit: 0 'asis', 1 + n for 'bd<n>' (m_source.f90:99) */
     int munk;                   /* munk_profile of the ocean column (m_vmodel_lhm.f90:53-54) */
+    int pw_mode;                /* plane-wave mode (m_source.f90:67-79) */
     /* kernel coefficients (m_kernel.f90:23-26) */
     SPR c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     MPR rc40x, rc41x, rc40y, rc41y, rc40z, rc41z;
@@ -1004,10 +1005,36 @@ static void cerjan_update_vel(o3d *o) {
 /* absorb_p__update_vel: m_absorb_p.f90:126-311 (pw_mode off); the dispatch
  * of absorb__update_vel (m_absorb.f90:60-75) picks the sponge instead */
 /* ------------------------------------------------------------------------ */
+/* horizontal zero-derivative boundary of the plane-wave mode (m_absorb_p.f90:136-243, 324-431): the ghost
+   planes i = 0, nx+1 (j = jbeg..jend) and j = 0, ny+1 (i = ibeg..iend), k = 1..nz, of each field extrapolated
+   linearly from the two cells inside */
+static void pw_ghosts(o3d *o, MPR **f, int nf) {
+    for (int q = 0; q < nf; q++) {
+        MPR *a = f[q];
+        for (int j = o->jbeg; j <= o->jend; j++)
+            for (int k = 1; k <= o->nz; k++) {
+                A3(a, k, 0, j) = 2 * A3(a, k, 1, j) - A3(a, k, 2, j);
+                A3(a, k, o->nx + 1, j) = 2 * A3(a, k, o->nx, j) - A3(a, k, o->nx - 1, j);
+            }
+    }
+    for (int q = 0; q < nf; q++) {
+        MPR *a = f[q];
+        for (int i = o->ibeg; i <= o->iend; i++)
+            for (int k = 1; k <= o->nz; k++) {
+                A3(a, k, i, 0) = 2 * A3(a, k, i, 1) - A3(a, k, i, 2);
+                A3(a, k, i, o->ny + 1) = 2 * A3(a, k, i, o->ny) - A3(a, k, i, o->ny - 1);
+            }
+    }
+}
+
 void o3d_absorb_update_vel(o3d *o) {
     if (o->cerjan) {
         cerjan_update_vel(o);
         return;
+    }
+    if (o->pw_mode) {
+        MPR *f[6] = {o->Sxx, o->Syy, o->Szz, o->Syz, o->Sxz, o->Sxy};
+        pw_ghosts(o, f, 6);
     }
     const float dt = o->dt;
     MPR *Sxx = o->Sxx, *Syy = o->Syy, *Szz = o->Szz, *Syz = o->Syz, *Sxz = o->Sxz, *Sxy = o->Sxy;
@@ -1052,6 +1079,10 @@ void o3d_absorb_update_stress(o3d *o) {
     if (o->cerjan) {
         cerjan_update_stress(o);
         return;
+    }
+    if (o->pw_mode) {
+        MPR *f[3] = {o->Vx, o->Vy, o->Vz};
+        pw_ghosts(o, f, 3);
     }
     const float dt = o->dt;
     MPR *Vx = o->Vx, *Vy = o->Vy, *Vz = o->Vz;
@@ -1211,6 +1242,75 @@ int o3d_source_setup(o3d *o, int bf_mode, int nsrc_g, const float *sx, const flo
     /* dt_dxyz = dt / (dx * dy * dz): m_source.f90:305 */
     o->dt_dxyz = o->dt / (o->dx * o->dy * o->dz);
     return n;
+}
+
+/* pw_setup: m_source.f90:315-465.  The plane-wave initial condition over the memory box from the medium after
+   medium__setup (every cell whose vp -- vs for an S wave -- reaches epsilon(1.0)), the cut-off frequency at the
+   grid centre and depth pw_ztop, no source grid, and the fictitious moment M0 = 1 / UC (m_source.f90:72-79).
+   ps: 0 P wave, 1 S wave; angles in degrees. */
+void o3d_pw_setup(o3d *o, float pw_ztop, float pw_zlen, int ps, float strike, float dip, float rake, int stftype) {
+    const float d2r_strike = (float)(PI_D / 180.0 * (double)strike);
+    const float d2r_dip = (float)(PI_D / 180.0 * (double)dip);
+    const float d2r_rake = (float)(PI_D / 180.0 * (double)rake);
+    const float sd = sinf(d2r_dip), cd = cosf(d2r_dip), sf = sinf(d2r_strike), cf = cosf(d2r_strike);
+    const float sl = sinf(d2r_rake), cl = cosf(d2r_rake), c2d = cosf(2 * d2r_dip), c2f = cosf(2 * d2r_strike);
+    const float eps = 1.1920929e-07f;
+    o->pw_mode = 1;
+    o->stftype = stftype;
+    for (int j = o->jbeg_m; j <= o->jend_m; j++)
+        for (int i = o->ibeg_m; i <= o->iend_m; i++)
+            for (int k = o->kbeg_m; k <= o->kend_m; k++) {
+                const long e = IDX3(o, k, i, j);
+                const float rho = o->frho[e], la0 = o->flam[e], mu0 = o->fmu[e];
+                const float v = ps == 0 ? sqrtf((la0 + 2 * mu0) / rho) : sqrtf(mu0 / rho);
+                if (v < eps) continue;
+                const float x0 = (float)(o->xbeg + (MPR)(i - 0.5f) * o->dx);
+                const float y0 = (float)(o->ybeg + (MPR)(j - 0.5f) * o->dy);
+                const float z0 = (float)(o->zbeg + (MPR)(k - 0.5f) * o->dz - pw_ztop);
+                const float x1 = (float)(x0 + o->dx / (MPR)2);
+                const float y1 = (float)(y0 + o->dy / (MPR)2);
+                const float z1 = (float)(z0 + o->dz / (MPR)2);
+                const float hv = o->dt / 2.f * v;
+                const float s_ii = o3d_momentrate(sd * sf * x0 - sd * cf * y0 + cd * z0, stftype, 0.0f, pw_zlen);
+                const float s_vx = o3d_momentrate(sd * sf * x1 - sd * cf * y0 + cd * z0 + hv, stftype, 0.0f, pw_zlen);
+                const float s_vy = o3d_momentrate(sd * sf * x0 - sd * cf * y1 + cd * z0 + hv, stftype, 0.0f, pw_zlen);
+                const float s_vz = o3d_momentrate(sd * sf * x0 - sd * cf * y0 + cd * z1 + hv, stftype, 0.0f, pw_zlen);
+                const float s_yz = o3d_momentrate(sd * sf * x0 - sd * cf * y1 + cd * z1, stftype, 0.0f, pw_zlen);
+                const float s_xz = o3d_momentrate(sd * sf * x1 - sd * cf * y0 + cd * z1, stftype, 0.0f, pw_zlen);
+                const float s_xy = o3d_momentrate(sd * sf * x1 - sd * cf * y1 + cd * z0, stftype, 0.0f, pw_zlen);
+                if (ps == 0) {
+                    A3(o->Vx, k, i, j) = -sd * sf * s_vx;
+                    A3(o->Vy, k, i, j) = sd * cf * s_vy;
+                    A3(o->Vz, k, i, j) = -cd * s_vz;
+                    A3(o->Sxx, k, i, j) = -(la0 + 2 * mu0 * sd * sd * sf * sf) * s_ii / v;
+                    A3(o->Syy, k, i, j) = -(la0 + 2 * mu0 * sd * sd * cf * cf) * s_ii / v;
+                    A3(o->Szz, k, i, j) = -(la0 + 2 * mu0 * cd * cd) * s_ii / v;
+                    A3(o->Syz, k, i, j) = 2 * mu0 * sd * cd * cf * s_yz / v;
+                    A3(o->Sxz, k, i, j) = -2 * mu0 * sd * cd * sf * s_xz / v;
+                    A3(o->Sxy, k, i, j) = 2 * mu0 * sd * cd * sf * s_xy / v;
+                } else {
+                    A3(o->Vx, k, i, j) = (cl * cf + sl * cd * sf) * s_vx;
+                    A3(o->Vy, k, i, j) = (cl * sf - sl * cd * cf) * s_vy;
+                    A3(o->Vz, k, i, j) = -sl * sd * s_vz;
+                    A3(o->Sxx, k, i, j) = 2 * mu0 * sd * sf * (cl * cf + sl * cd * sf) * s_ii / v;
+                    A3(o->Syy, k, i, j) = -2 * mu0 * sd * cf * (cl * sf - sl * cd * cf) * s_ii / v;
+                    A3(o->Szz, k, i, j) = -2 * mu0 * cd * sl * sd * s_ii / v;
+                    A3(o->Syz, k, i, j) = mu0 * (cl * cd * sf - sl * c2d * cf) * s_yz / v;
+                    A3(o->Sxz, k, i, j) = mu0 * (cl * cd * cf + sl * c2d * sf) * s_xz / v;
+                    A3(o->Sxy, k, i, j) = -mu0 * (cl * sd * c2f + 2 * sl * sd * cd * sf * cf) * s_xy / v;
+                }
+            }
+    /* wavelength condition: m_source.f90:443-462 */
+    const int ic = o3d_x2i((o->xbeg + o->xend) / 2, o->xbeg, (float)o->dx);
+    const int jc = o3d_x2i((o->ybeg + o->yend) / 2, o->ybeg, (float)o->dy);
+    const int kc = o3d_x2i(pw_ztop, o->zbeg, (float)o->dz);
+    const long e = IDX3(o, kc, ic, jc);
+    const float rho = o->frho[e], la0 = o->flam[e], mu0 = o->fmu[e];
+    const float v = ps == 0 ? sqrtf((la0 + 2 * mu0) / rho) : sqrtf(mu0 / rho);
+    o->fcut = v / pw_zlen;
+    o->fmax = o->fcut * 2.0f;
+    o->nsrc = 0;
+    o->M0 = 1.0f / o->UC;
 }
 
 /* sdep_fit (m_source.f90:99): -1 for 'asis', n for 'bd<n>'; set before o3d_source_setup */

@@ -51,7 +51,12 @@ def run_and_compare(p, g0, g1, steps):
         assert same_bits(g0.download(f), g1.download(f)), f
 
 
-@pytest.mark.parametrize("case", ["layers", "perturbed", "ocean_clipped", "seawater_munk"])
+# a 1 km low-velocity layer at 3 km depth and a slow top layer, for stabilize_pml
+SLOW = [Layer(0.0, 2.2, 2.4, 1.2, 100, 50), Layer(1.0, 2.7, 5.5, 3.2, 300, 150),
+        Layer(3.0, 2.4, 3.0, 1.6, 100, 50), Layer(4.0, 2.7, 5.5, 3.2, 300, 150)] + LAYERS[1:]
+
+
+@pytest.mark.parametrize("case", ["layers", "perturbed", "ocean_clipped", "seawater_munk", "stabilize_pml"])
 def test_device_medium_equals_host_setup(case):
     """vmodel_lhm (+ lhm_rmed) and medium__setup in HBM: every field over the
     memory box, the six maps, ts, zeta and the velocity range equal the host
@@ -61,13 +66,16 @@ def test_device_medium_equals_host_setup(case):
     kw = {}
     if case == "ocean_clipped":
         kw = dict(layers=OCEAN, vcut=1.0, rhomin=2.75)
+    elif case == "stabilize_pml":
+        # stabilize_absorber (m_medium.f90:276-340) on the device against the host's
+        kw = dict(layers=SLOW, stabilize_pml=True)
     elif case == "seawater_munk":
         # seawater of Munk's profile between z = 0 and depth(1) = 1.8 km (m_vmodel_lhm.f90:123-133)
         kw = dict(layers=[Layer(1.8, 2.7, 5.5, 3.2, 300, 150)] + list(LAYERS[1:]), munk_profile=True)
     p = small3d(nx=56, ny=48, nz=44, na=8, nt=8, **kw)
     shape = (p.ny + 6, p.nx + 6, p.nz + 6)
     xi = None
-    if case == "perturbed":
+    if case in ("perturbed", "stabilize_pml"):
         xi = vonkarman_xi(shape)
     elif case == "ocean_clipped":
         xi = vonkarman_xi(shape, eps=0.25, seed=11)

@@ -395,3 +395,35 @@ def test_seawater_forward_run_matches_oracle():
     a, b = g.waveforms(_lib.WAV_V), o.waveforms("v")
     assert np.linalg.norm(b) > 0 and same_bits(a, b)
     compare_state(g, o, p)
+
+
+@pytest.mark.parametrize("ps", ["P", "S"])
+def test_plane_wave_run_matches_oracle(ps):
+    """Plane-wave mode (pw_setup, m_source.f90:315-465, and the zero-derivative
+    side boundary of the PML, m_absorb_p.f90:136-243, 324-431, with the ghost
+    planes the single-domain exchange zeroes): traces, final V, S, memory
+    variables and PML auxiliaries bitwise; per-routine calls equal graph
+    steps."""
+    p = small3d(nt=50, pw_mode=True, pw_ztop=8.0, pw_zlen=4.0, pw_ps=ps, pw_strike=30.0, pw_dip=20.0,
+                pw_rake=40.0, sources=[], sw_wav_stress=True)
+    g = Swpc3D(p)
+    o = Oracle3D(p)
+    g.run(1, p.nt)
+    o.run(1, p.nt, ntdec_r=p.ntdec_r)
+    for what, comp in ((_lib.WAV_V, "v"), (_lib.WAV_STRESS, "stress")):
+        a, b = g.waveforms(what), o.waveforms(comp)
+        assert np.linalg.norm(b) > 0 and same_bits(a, b), comp
+    compare_state(g, o, p)
+    h = Swpc3D(p)
+    for it in range(1, p.nt + 1):
+        h.wav__store(it)
+        h.kernel__update_stress()
+        h.absorb__update_stress()
+        h.source__stressglut(it)
+        h.global__comm_stress()
+        h.kernel__update_vel()
+        h.absorb__update_vel()
+        h.source__bodyforce(it)
+        h.global__comm_vel()
+    for n in range(9):
+        assert same_bits(h.download(n), g.download(n)), n

@@ -474,3 +474,31 @@ def test_ocean_medium_2d_bit_exact(kind):
         assert np.array_equal(bits(getattr(m, f)), bits(o.array("f" + f))), f
     for f in ("kfs", "kob", "kfs_top", "kfs_bot", "kob_top", "kob_bot"):
         assert np.array_equal(getattr(m, f), o.array(f)), f
+
+
+def _pw_params(ps):
+    """Plane-wave mode: a front at 8 km depth, 4 km long, oblique (strike 30, dip 20)."""
+    return small3d(pw_mode=True, pw_ztop=8.0, pw_zlen=4.0, pw_ps=ps, pw_strike=30.0, pw_dip=20.0, pw_rake=40.0,
+                   sources=[])
+
+
+@pytest.mark.parametrize("ps", ["P", "S"])
+def test_plane_wave_setup_bit_exact(ps):
+    """pw_setup (m_source.f90:315-465): the initial V and S over the memory
+    box and the PML's fcut equal the oracle's bit for bit."""
+    p = _pw_params(ps)
+    m = Medium(p)
+    lib = _lib.load()
+    f = [np.zeros(m.rho.shape, np.float32) for _ in range(9)]
+    fcut = C.c_float()
+    assert lib.swpc_pw_setup(C.byref(grid_struct(p)), _lib.fptr(m.rho), _lib.fptr(m.lam), _lib.fptr(m.mu),
+                             p.pw_ztop, p.pw_zlen, 0 if ps == "P" else 1, p.pw_strike, p.pw_dip, p.pw_rake,
+                             _lib.STF_CODES[p.stftype], *(_lib.fptr(a) for a in f), C.byref(fcut)) == 0
+    o = Oracle3D(p)
+    names = ["Vx", "Vy", "Vz", "Sxx", "Syy", "Szz", "Syz", "Sxz", "Sxy"]
+    for a, name in zip(f, names):
+        assert np.array_equal(bits(a), bits(o.array(name))), name
+    assert np.abs(f[2]).max() > 0 and np.abs(f[3]).max() > 0
+    sc = o.scalars()
+    assert np.float32(sc["fcut"]) == np.float32(fcut.value)
+    assert np.float32(sc["M0"]) == np.float32(1.0) / np.float32(1e-15)
