@@ -79,6 +79,10 @@ class Station:
 @dataclass
 class Params:
     title: str = "swpc3d"
+    # map projection of the grid (m_global.f90:171-173): centre longitude, latitude, azimuth of the x axis
+    clon: float = 139.7604
+    clat: float = 35.7182
+    phi: float = 0.0
     nx: int = 256
     ny: int = 256
     nz: int = 256
@@ -255,12 +259,14 @@ def params_from_ini(path: str | Path, strict: bool = False) -> Params:
              "green_mode": bool, "green_cmp": str, "green_trise": float, "ntdec_r": int, "ntdec_w": int,
              "sw_wav_v": bool, "sw_wav_u": bool, "sw_wav_stress": bool, "sw_wav_strain": bool, "abc_type": str,
              "stabilize_pml": bool, "sdep_fit": str, "munk_profile": bool, "pw_mode": bool, "pw_ztop": float,
-             "pw_zlen": float, "pw_ps": str, "pw_strike": float, "pw_dip": float, "pw_rake": float}
+             "pw_zlen": float, "pw_ps": str, "pw_strike": float, "pw_dip": float, "pw_rake": float,
+             "clon": float, "clat": float, "phi": float}
     args = {}
     for key, typ in types.items():
         if key in kv:
             args[key] = _conv(kv[key], typ)
-        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit", "munk_profile") and not key.startswith("pw_"):
+        elif strict and key not in ("xbeg", "ybeg", "zbeg", "sdep_fit", "munk_profile", "clon", "clat", "phi") \
+                and not key.startswith("pw_"):
             raise KeyError(f"parameter {key} missing in strict mode")
     for key in ("z0_xy", "x0_yz", "y0_xz"):
         if key in kv:
