@@ -49,7 +49,8 @@ B_STRESS_INT, B_STRESS_PML = 58 * 4, 38 * 4
 B_VEL_INT, B_VEL_PML = 15 * 4, 33 * 4
 # the same per storage form of S and R: (stress int, stress PML, vel int, vel PML); BF16 R saves 36 x 2 B of the
 # interior stress phase, FP16 S + R also 12 x 2 B of stress and 6 x 2 B of velocity accesses per cell
-BYTES = {"f32": (232, 152, 60, 132), "bf16r": (160, 152, 60, 132), "f16sr": (136, 128, 48, 120)}
+BYTES = {"f32": (232, 152, 60, 132), "bf16r": (160, 152, 60, 132), "f16r": (160, 152, 60, 132),
+         "f16sr": (136, 128, 48, 120)}
 FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic of one launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the c1 mix scaled
 # down by 4 per axis (256x256x128, na = 8: 1/64 of c1's interior and PML cells), divided by that launch's
@@ -759,6 +760,28 @@ def accuracy_sample(p, precision: str, device: int, steps: int = 200):
     return out
 
 
+def accuracy_full_grid(p, xi, precision: str, device: int, steps: int = 1000):
+    """rel-L2 distance of one storage form to the FP32 form on the workload's own grid after `steps` steps
+    (traces and final velocity); with the FP32 form's own error against the all-double oracle (the sample
+    above) this bounds the form's error against FP64 at full size."""
+    from openswpc_b200 import _lib
+    from openswpc_b200.swpc3d import Swpc3D
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    runs = {}
+    for form in (precision, "f32"):
+        g = Swpc3D(p, xi, device=device, precision=form)
+        g.run(1, steps)   # reports (and FP16 rescales) every ntdec_r steps
+        runs[form] = (g.waveforms(_lib.WAV_V), np.stack([g.download(n) for n in range(3)]))
+        g.close()
+    a, b = runs[precision], runs["f32"]
+    return {"grid": f"{p.nx}x{p.ny}x{p.nz}", "steps": steps, "traces_v_vs_f32": rel(a[0], b[0]),
+            "final_v_vs_f32": rel(a[1], b[1])}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -770,11 +793,14 @@ def main():
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (c3 profiling runs)")
-    ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16sr"],
+    ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16r", "f16sr"],
                     help="storage of stress and memory variables (arithmetic is FP32)")
     ap.add_argument("--accuracy", action="store_true",
                     help="add the rel-L2 error against the f64 oracle on a 128x128x64 sample of the workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="c1 on one GPU: skip the batched-ensemble, reciprocity, gradient and storage-form lines "
+                         "measured after the headline")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -944,7 +970,8 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "storage": {"f32": "S, R FP32", "bf16r": "R BF16", "f16sr": "S, R FP16 (power-of-two scales)"}[args.precision],
+            "storage": {"f32": "S, R FP32", "bf16r": "R BF16", "f16r": "R FP16 (power-of-two scales)",
+                        "f16sr": "S, R FP16 (power-of-two scales)"}[args.precision],
             "data": "synthetic (seeded layered + von Karman medium)",
             "config": wl,
             "roofline": {"bound": "hbm", "kernel": "stress3d_tma_kernel (TMA-staged fused interior + PML stress update"
@@ -975,14 +1002,67 @@ def main():
     sim.close()
     if rank == 0 and args.accuracy:
         line["accuracy"] = accuracy_sample(p, args.precision, device)
+        if args.precision != "f32":
+            torch.cuda.empty_cache()
+            line["accuracy_full_grid"] = accuracy_full_grid(p, xi, args.precision, device)
     if rank == 0 and not args.no_cpu_baseline:
         v, n, sc, dt = cpu_reference(p, xi, 1000, 1, os.cpu_count() or 1, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"oracle f32 on the centre 256x256x{p.nz} column block, {n} steps "
                                           f"after 1 warm-up ({dt:.1f} s)"}
     ranks.close()
+    if rank == 0 and world == 1 and args.workload == "c1" and args.precision == "f32" and not args.no_secondary:
+        line["secondary"] = secondary_lines()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# the other workloads, measured after the headline in the default run (one GPU): each in its own process with a
+# bounded number of steps, the whole set bounded in time; the summary keeps the figures each workload is judged on
+SECONDARY = [
+    ("c2a", ["--steps", "10", "--warmup", "3"], ("value", "ms_per_step", "batched_over_loop", "plain_loop",
+                                                  "batched_over_loop_calls", "roofline", "e2e", "clocks")),
+    ("c2b", ["--steps", "10", "--warmup", "3"], ("value", "ms_per_step", "batched_over_loop", "plain_loop",
+                                                  "roofline", "e2e", "clocks")),
+    ("c3", ["--steps", "1", "--warmup", "3", "--no-cpu-baseline"],
+     ("value", "ms_per_step", "forward_ms", "gradient_over_forward", "algorithmic_gradient_over_forward",
+      "roofline", "roofline_forward", "e2e", "clocks")),
+    ("c4", ["--steps", "10", "--warmup", "3", "--no-cpu-baseline", "--no-secondary", "--accuracy",
+            "--precision", "bf16r"], ("value", "ms_per_step", "storage", "roofline", "accuracy",
+                                      "accuracy_full_grid", "clocks")),
+    ("c4", ["--steps", "10", "--warmup", "3", "--no-cpu-baseline", "--no-secondary", "--accuracy",
+            "--precision", "f16r"], ("value", "ms_per_step", "storage", "roofline", "accuracy",
+                                     "accuracy_full_grid", "clocks")),
+    ("c4", ["--steps", "10", "--warmup", "3", "--no-cpu-baseline", "--no-secondary", "--accuracy",
+            "--precision", "f32"], ("value", "ms_per_step", "storage", "roofline", "accuracy", "clocks")),
+]
+
+
+def secondary_lines(budget_s: float = 420.0) -> dict:
+    import subprocess
+
+    out = {}
+    t0 = time.perf_counter()
+    for wl, extra, keys in SECONDARY:
+        name = wl if "--precision" not in extra else f"{wl}_{extra[extra.index('--precision') + 1]}"
+        left = budget_s - (time.perf_counter() - t0)
+        if left < 30:
+            out[name] = {"skipped": "time budget of the secondary workloads spent"}
+            continue
+        cmd = [sys.executable, str(ROOT / "bench.py"), "--workload", wl] + extra
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=left, cwd=ROOT)
+            rows = [l for l in r.stdout.splitlines() if l.startswith("{")]
+            if r.returncode != 0 or not rows:
+                out[name] = {"failed": f"exit {r.returncode}: " + (r.stderr.strip().splitlines() or [""])[-1][:300]}
+                continue
+            full = json.loads(rows[-1])
+            out[name] = {"workload": full["config"].get("workload"), "metric": full["metric"],
+                         "command": " ".join(["python", "bench.py", "--workload", wl] + extra),
+                         **{k: full[k] for k in keys if k in full}}
+        except subprocess.TimeoutExpired:
+            out[name] = {"skipped": "did not finish within the time budget"}
+    return out
 
 
 if __name__ == "__main__":

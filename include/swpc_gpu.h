@@ -111,6 +111,7 @@ typedef struct swpc_desc {
 #define SWPC_PREC_F32 0
 #define SWPC_PREC_BF16_R 1
 #define SWPC_PREC_F16_SR 2
+#define SWPC_PREC_F16_R 3
 
 /* Medium and integer maps as produced by medium__setup
  * (src/swpc_3d/m_medium.f90:36-467).  Float fields are 3D Fortran arrays

@@ -20,8 +20,8 @@ SWPC_ERR_STATE = 3
 SWPC_ERR_DIVERGED = 4
 SWPC_ERR_NOMEM = 5
 SWPC_ERR_LIMIT = 6
-PREC_F32, PREC_BF16_R, PREC_F16_SR = 0, 1, 2
-PRECISIONS = {"f32": PREC_F32, "bf16r": PREC_BF16_R, "f16sr": PREC_F16_SR}
+PREC_F32, PREC_BF16_R, PREC_F16_SR, PREC_F16_R = 0, 1, 2, 3
+PRECISIONS = {"f32": PREC_F32, "bf16r": PREC_BF16_R, "f16sr": PREC_F16_SR, "f16r": PREC_F16_R}
 SWPC_NOALLOC_MAX_NY = 16384
 
 KIND_3D, KIND_PSV, KIND_SH = 3, 2, 1

@@ -21,7 +21,11 @@ __device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
 //   PREC_BF16_R: R stored in BF16
 //   PREC_F16_SR: S and R stored in FP16, each array with its own power-of-two
 //                scale: value = stored * s, stored = value * (1 / s) (exact)
-enum { PREC_F32 = 0, PREC_BF16_R = 1, PREC_F16_SR = 2 };
+//   PREC_F16_R : R stored in FP16 with the same per-array scales, S in FP32
+enum { PREC_F32 = 0, PREC_BF16_R = 1, PREC_F16_SR = 2, PREC_F16_R = 3 };
+// the forms whose R lives in the 2-byte slab and S in the FP32 one
+template <int PREC>
+__host__ __device__ constexpr bool r_only_half() { return PREC == PREC_BF16_R || PREC == PREC_F16_R; }
 
 template <int PREC>
 __device__ __forceinline__ float ldS(const float *p, long long e, float s) {
@@ -40,14 +44,16 @@ __device__ __forceinline__ void stS(float *p, long long e, float v, float is) {
 }
 template <int PREC>
 __device__ __forceinline__ float ldR(const float *p, long long e, float s) {
-    if constexpr (PREC == PREC_F16_SR) return __half2float(__ldcs(reinterpret_cast<const __half *>(p) + e)) * s;
+    if constexpr (PREC == PREC_F16_SR || PREC == PREC_F16_R)
+        return __half2float(__ldcs(reinterpret_cast<const __half *>(p) + e)) * s;
     else if constexpr (PREC == PREC_BF16_R)
         return __bfloat162float(__ldcs(reinterpret_cast<const __nv_bfloat16 *>(p) + e));
     else return __ldcs(p + e);
 }
 template <int PREC>
 __device__ __forceinline__ void stR(float *p, long long e, float v, float is) {
-    if constexpr (PREC == PREC_F16_SR) __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
+    if constexpr (PREC == PREC_F16_SR || PREC == PREC_F16_R)
+        __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
     else if constexpr (PREC == PREC_BF16_R) __stcs(reinterpret_cast<__nv_bfloat16 *>(p) + e, __float2bfloat16_rn(v));
     else __stcs(p + e, v);
 }

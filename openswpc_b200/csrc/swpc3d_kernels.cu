@@ -93,6 +93,7 @@ void launch_stress3d(const Str3Args &a, int nm, int minb, int prec, dim3 grid, d
     switch (prec) {
     case PREC_BF16_R: stress_nm<PREC_BF16_R>(a, nm, minb, grid, block, st); break;
     case PREC_F16_SR: stress_nm<PREC_F16_SR>(a, nm, minb, grid, block, st); break;
+    case PREC_F16_R: stress_nm<PREC_F16_R>(a, nm, minb, grid, block, st); break;
     default: stress_nm<PREC_F32>(a, nm, minb, grid, block, st); break;
     }
 }

@@ -66,8 +66,8 @@ struct StrBoxes {
     static constexpr int n = BJ * BI * KT;   // cells of a tile
     static constexpr int nMed = 7 * n;
     static constexpr int nState = PREC == PREC_F32 ? (6 + 6 * NM) * n
-                                : PREC == PREC_BF16_R ? up32(6 * n) + 3 * NM * n : (3 + 3 * NM) * n;
-    static constexpr int oR = up32(6 * n);   // BF16 R box within the state region
+                                : r_only_half<PREC>() ? up32(6 * n) + 3 * NM * n : (3 + 3 * NM) * n;
+    static constexpr int oR = up32(6 * n);   // 2-byte R box within the state region (BF16_R, F16_R)
     static constexpr int nV = 3 * (BJ + 4) * (BI + 4) * KB;
     static constexpr int member = up32(nState) + up32(nV);
     static constexpr int total = up32(nMed) + M * member;
@@ -75,7 +75,7 @@ struct StrBoxes {
     // bytes a member's state copies bring (S alone in tiles without interior cells)
     __host__ __device__ static constexpr int state_bytes(bool with_r) {
         return PREC == PREC_F32 ? 4 * (with_r ? 6 + 6 * NM : 6) * n
-             : PREC == PREC_BF16_R ? 4 * 6 * n + (with_r ? 2 * 6 * NM * n : 0) : 2 * (with_r ? 6 + 6 * NM : 6) * n;
+             : r_only_half<PREC>() ? 4 * 6 * n + (with_r ? 2 * 6 * NM * n : 0) : 2 * (with_r ? 6 + 6 * NM : 6) * n;
     }
     __host__ __device__ static constexpr int bytes(int nmem, bool with_r) {
         return 4 * nMed + nmem * (state_bytes(with_r) + 4 * nV);
@@ -102,6 +102,8 @@ struct SStrOps {
         if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(6 + f)]) * a.sR[q];
         else if constexpr (PREC == PREC_BF16_R)
             return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(ss + StrBoxes<NM, BI, BJ, 1, PREC>::oR)[at(f)]);
+        else if constexpr (PREC == PREC_F16_R)
+            return __half2float(reinterpret_cast<const __half *>(ss + StrBoxes<NM, BI, BJ, 1, PREC>::oR)[at(f)]) * a.sR[q];
         else return ss[at(6 + f)];
     }
     // 0 mu, 1 lam, 2 taup, 3 taus, 4 muyz, 5 muxz, 6 muxy
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(KT * BI * BJ,
         for (int mm = 0; mm < T.nmem; mm++) {
             const int fm = (T.m0 + mm) * t.f_member;
             float *p = sm + L::oMem(mm);
-            if constexpr (PREC == PREC_BF16_R) {
+            if constexpr (r_only_half<PREC>()) {
                 load_4d(p, &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state, &bar);
                 if (with_r && NM > 0) load_4d(p + L::oR, &tm_state, x0, T.i0 + 2, T.j0 + 2, t.f_h, &bar);
             } else if constexpr (PREC == PREC_F16_SR) {
@@ -409,6 +411,8 @@ cudaError_t launch_stress3d_tma(const TmaMaps &m, const Str3Args &a, const TmaTi
                                 cudaStream_t st, int prec) {
     if (prec == PREC_BF16_R)
         return bj == 2 ? stress_nm<4, 2, 1, PREC_BF16_R>(m, a, t, nm, st) : stress_nm<4, 4, 1, PREC_BF16_R>(m, a, t, nm, st);
+    if (prec == PREC_F16_R)
+        return bj == 2 ? stress_nm<4, 2, 1, PREC_F16_R>(m, a, t, nm, st) : stress_nm<4, 4, 1, PREC_F16_R>(m, a, t, nm, st);
     if (prec == PREC_F16_SR)
         return bj == 2 ? stress_nm<4, 2, 1, PREC_F16_SR>(m, a, t, nm, st) : stress_nm<4, 4, 1, PREC_F16_SR>(m, a, t, nm, st);
     if (mpc == 4) {
@@ -484,9 +488,11 @@ bool tma_encode_box(unsigned char *out, float *slab, const Geo &g, long long nf,
 bool tma_encode_stress(TmaMaps &m, const TmaSlabs &s, const Geo &g, int nm, int bi, int bj, int prec) {
     bool ok = encode(m.med, s.med, g, s.nf_med, KT, bi, bj, 7) &&
               encode(m.vh, s.state, g, s.nf_state, KB, bi + 4, bj + 4, 3);
-    if (prec == PREC_BF16_R)   // S in the FP32 slab, R in the 2-byte slab
+    if (prec == PREC_BF16_R || prec == PREC_F16_R)   // S in the FP32 slab, R in the 2-byte slab
         return ok && encode(m.s6, s.state, g, s.nf_state, KT, bi, bj, 6) &&
-               (nm == 0 || encode(m.state, s.half, g, s.nf_half, KT, bi, bj, 6 * nm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16));
+               (nm == 0 || encode(m.state, s.half, g, s.nf_half, KT, bi, bj, 6 * nm,
+                                  prec == PREC_BF16_R ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT16));
     if (prec == PREC_F16_SR)   // S and R in the 2-byte slab
         return ok && encode(m.s6, s.half, g, s.nf_half, KT, bi, bj, 6, CU_TENSOR_MAP_DATA_TYPE_FLOAT16) &&
                encode(m.state, s.half, g, s.nf_half, KT, bi, bj, 6 + 6 * nm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16);

@@ -99,9 +99,10 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     if (d->na < 0 || 2 * d->na >= d->nx || d->na >= d->nz || (d->kind == SWPC_KIND_3D && 2 * d->na >= d->ny))
         return fail(set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid"));
     if (d->nt < 1) return fail(set_err(c, SWPC_ERR_ARG, "nt must be positive"));
-    if (d->precision < SWPC_PREC_F32 || d->precision > SWPC_PREC_F16_SR ||
+    if (d->precision < SWPC_PREC_F32 || d->precision > SWPC_PREC_F16_R ||
         (d->kind != SWPC_KIND_3D && d->precision != SWPC_PREC_F32))
-        return fail(set_err(c, SWPC_ERR_ARG, "precision must be SWPC_PREC_F32/BF16_R/F16_SR (3D) or SWPC_PREC_F32"));
+        return fail(set_err(c, SWPC_ERR_ARG,
+                            "precision must be SWPC_PREC_F32/BF16_R/F16_SR/F16_R (3D) or SWPC_PREC_F32"));
     c->prec = d->precision;
     if (!(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0) || (d->kind == SWPC_KIND_3D && !(d->dy > 0)))
         return fail(set_err(c, SWPC_ERR_ARG, "dx, dy, dz, dt must be positive"));
@@ -1024,7 +1025,8 @@ TmaTiles tma_tiles(const swpc_ctx *c, int bi, int bj, int nmem, int mpc, int nfi
     t.f_v = 0;
     t.f_state = 3;
     t.f_member = 0;
-    t.f_med = c->prec == SWPC_PREC_F32 ? 9 + 6 * c->d.nm : c->prec == SWPC_PREC_BF16_R ? 9 : 3;
+    t.f_med = c->prec == SWPC_PREC_F32 ? 9 + 6 * c->d.nm
+            : (c->prec == SWPC_PREC_BF16_R || c->prec == SWPC_PREC_F16_R) ? 9 : 3;
     t.f_b = t.f_med + 7;
     t.f_h = 0;
     t.so = 0;

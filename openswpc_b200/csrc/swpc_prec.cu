@@ -4,6 +4,8 @@
 // Three storage forms share the FP32 arithmetic of the kernels:
 //   SWPC_PREC_F32     : S and R in FP32 (the reference's MP = SP build)
 //   SWPC_PREC_BF16_R  : the 18 memory variables R in BF16 (2 bytes)
+//   SWPC_PREC_F16_R   : the memory variables R in FP16 with per-array
+//                       power-of-two scales as below, S in FP32
 //   SWPC_PREC_F16_SR  : the 6 stresses S and the memory variables R in FP16,
 //                       each array with its own power-of-two scale s = 2^e:
 //                       value = stored * s.  swpc_rescale moves e so that
@@ -68,7 +70,7 @@ namespace swpc {
 int field_storage(const swpc_ctx *c, int field) {
     if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return c->prec == SWPC_PREC_F16_SR ? 2 : 0;
     if (field >= SWPC_F_R && field < SWPC_F_R + 18)
-        return c->prec == SWPC_PREC_F16_SR ? 2 : (c->prec == SWPC_PREC_BF16_R ? 1 : 0);
+        return (c->prec == SWPC_PREC_F16_SR || c->prec == SWPC_PREC_F16_R) ? 2 : (c->prec == SWPC_PREC_BF16_R ? 1 : 0);
     return 0;
 }
 
@@ -100,12 +102,14 @@ int prec_from_f32(swpc_ctx *c, int field, const float *tmp, float *stored) {
 extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
     if (!c) return SWPC_ERR_ARG;
     if (changed) *changed = 0;
-    if (c->prec != SWPC_PREC_F16_SR) return SWPC_OK;
+    if (c->prec != SWPC_PREC_F16_SR && c->prec != SWPC_PREC_F16_R) return SWPC_OK;
     if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, SWPC_ERR_CUDA, "cudaSetDevice failed");
-    const int nf = 6 + 3 * c->d.nm;
+    const bool with_s = c->prec == SWPC_PREC_F16_SR;   // F16_R keeps S in FP32
+    const int nf = (with_s ? 6 : 0) + 6 * c->d.nm;
     std::vector<float *> fields;
     std::vector<int *> expo;
-    for (int q = 0; q < 6; q++) { fields.push_back(c->S[q]); expo.push_back(&c->eS[q]); }
+    if (with_s)
+        for (int q = 0; q < 6; q++) { fields.push_back(c->S[q]); expo.push_back(&c->eS[q]); }
     for (int comp = 0; comp < 6; comp++)
         for (int m = 0; m < c->d.nm; m++) { fields.push_back(c->R[comp * 3 + m]); expo.push_back(&c->eR[comp * 3 + m]); }
     unsigned int *d_max = nullptr;

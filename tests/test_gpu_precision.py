@@ -1,5 +1,6 @@
 """Reduced-precision storage forms of the 3D step (BF16 memory variables;
-FP16 stress and memory variables with per-array power-of-two scales).  The
+FP16 memory variables; FP16 stress and memory variables; the FP16 arrays with
+per-array power-of-two scales).  The
 arithmetic stays FP32, so each form is checked against the FP32 form and
 against the all-double oracle with a stated tolerance, and the error is
 recorded."""
@@ -16,7 +17,7 @@ pytestmark = pytest.mark.gpu
 # rel-L2 bars of the reduced forms against the f64 oracle after 80 steps:
 # BF16 keeps 8 significand bits (2^-9 relative rounding) for R, FP16 keeps 11
 # (2^-12) for S and R; both stay far below 1e-2 on this case
-TOL = {"f32": 1e-5, "bf16r": 1e-2, "f16sr": 1e-2}
+TOL = {"f32": 1e-5, "bf16r": 1e-2, "f16r": 1e-3, "f16sr": 1e-2}
 
 
 def rel_l2(a, b):
@@ -34,7 +35,7 @@ def reference():
     return p, xi, o
 
 
-@pytest.mark.parametrize("form", ["f32", "bf16r", "f16sr"])
+@pytest.mark.parametrize("form", ["f32", "bf16r", "f16r", "f16sr"])
 def test_precision_form_error_against_f64(form, reference, record_property):
     p, xi, o = reference
     g = Swpc3D(p, xi, precision=form)
@@ -88,7 +89,7 @@ def test_reduced_storage_roundtrip_and_rescale():
 
 
 @pytest.mark.parametrize("nm,grid", [(3, (40, 36, 32)), (1, (42, 38, 45)), (0, (42, 38, 45)), (2, (40, 36, 32))])
-@pytest.mark.parametrize("form", ["bf16r", "f16sr"])
+@pytest.mark.parametrize("form", ["bf16r", "f16r", "f16sr"])
 def test_staged_reduced_forms_equal_the_flat_kernels(form, nm, grid):
     """The TMA-staged kernels of the reduced storage forms (2-byte tiles of S
     and R) give the bits of the one-cell kernels of the same form: traces,
@@ -114,7 +115,7 @@ def test_staged_reduced_forms_equal_the_flat_kernels(form, nm, grid):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), fid
 
 
-@pytest.mark.parametrize("form", ["bf16r", "f16sr"])
+@pytest.mark.parametrize("form", ["bf16r", "f16r", "f16sr"])
 def test_reduced_forms_on_every_compiled_staged_tile(form):
     """The reduced forms compile stress and velocity tiles (4, 4) and (4, 2):
     each combination gives the bits of the flat kernels."""
@@ -134,3 +135,21 @@ def test_reduced_forms_on_every_compiled_staged_tile(form):
             a = g.download(fid)
             assert np.array_equal(a.view(np.uint32), ref[fid].view(np.uint32)), (sbj, vbj, fid)
         g.close()
+
+
+def test_f16r_keeps_stress_in_fp32_and_rescales_memory_variables():
+    """FP16 memory variables with FP32 stress: uploads of S keep every bit,
+    R rounds to FP16, and a rescale centres the R scales only."""
+    p = small3d(nt=40)
+    g = Swpc3D(p, precision="f16r")
+    g.run(1, 30)
+    x = np.random.default_rng(5).standard_normal((p.ny + 6, p.nx + 6, p.nz + 6)).astype(np.float32)
+    inner = (slice(3, -3), slice(3, -3), slice(3, -3))
+    g.upload(_lib.F_SXX, x)
+    assert np.array_equal(g.download(_lib.F_SXX)[inner].view(np.uint32), x[inner].view(np.uint32))
+    r = g.download(_lib.F_R)
+    big = np.abs(r).max()
+    assert big > 0
+    g.rescale()
+    assert g.rescale() == 0
+    assert np.abs(g.download(_lib.F_R) - r).max() <= big * 2.0 ** -20
