@@ -140,7 +140,20 @@ int swpc_destroy(swpc_ctx *ctx);
 const char *swpc_last_error(const swpc_ctx *ctx);
 /* cudaStream_t of the context, as void*. */
 void *swpc_stream(swpc_ctx *ctx);
+/* Waits for the context's stream.  Returns SWPC_ERR_CUDA when a staged
+ * kernel's tile copy did not complete within its bounded wait (the kernel
+ * then skipped its cells and raised the context's error word).  The fields
+ * that launch and every later launch wrote are then undefined, and every
+ * later swpc_sync reports the error until the caller restores the state --
+ * swpc_reset_state (a run from rest, which also clears the word) or uploads
+ * of every field followed by swpc_clear_error.  No counterpart in the
+ * reference. */
 int swpc_sync(swpc_ctx *ctx);
+int swpc_clear_error(swpc_ctx *ctx);
+/* Failure injection for the error paths of a driver: raises the error word
+ * from the host exactly as a timed-out tile wait does (no kernel waits, no
+ * device fault).  No counterpart in the reference. */
+int swpc_raise_copy_error(swpc_ctx *ctx);
 
 /* ---- setup ------------------------------------------------------------- */
 

@@ -915,6 +915,8 @@ extern "C" int swpc_reset_state(swpc_ctx *c) {
     ACK(cudaSetDevice(c->device));
     int rc = zero_state(c);
     if (rc) return rc;
+    // a state from rest replaces any wavefield a failed tile copy left undefined
+    if (c->d_err) ACK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
 

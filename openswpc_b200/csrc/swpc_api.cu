@@ -314,6 +314,29 @@ extern "C" int swpc_sync(swpc_ctx *c) {
     return SWPC_OK;
 }
 
+// The error word of the staged kernels: raised by a tile wait that ran out, it
+// stays up (every later swpc_sync reports it) until the caller has restored
+// the fields and clears it.
+extern "C" int swpc_clear_error(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!c->d_err) return SWPC_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWPC_OK;
+}
+
+// host-side failure injection for error-path tests of a driver: the word a
+// timed-out tile wait raises, set from the host (no kernel waits or faults)
+extern "C" int swpc_raise_copy_error(swpc_ctx *c) {
+    if (!c) return SWPC_ERR_ARG;
+    if (!c->d_err) return set_err(c, SWPC_ERR_STATE, "this context has no error word");
+    CK(cudaSetDevice(c->device));
+    const int one = 1;
+    CK(cudaMemcpy(c->d_err, &one, sizeof(int), cudaMemcpyHostToDevice));
+    return SWPC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // layout conversion between the Fortran memory box and the device columns
 // ---------------------------------------------------------------------------

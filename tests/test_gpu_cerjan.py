@@ -108,15 +108,26 @@ def test_cerjan_2d_body_force(kind):
     compare2d(g, o, p)
 
 
+@pytest.mark.parametrize("staged", [True, False])
+@pytest.mark.parametrize("bf", [False, True])
 @pytest.mark.parametrize("kind", ["psv", "sh"])
-def test_cerjan_2d_batch_members_equal_independent_runs(kind):
+def test_cerjan_2d_batch_members_equal_independent_runs(kind, bf, staged):
     """A batch that mixes Cerjan and PML members of uneven size: every
-    member's traces and fields equal its own independent run bitwise."""
-    ps = [small2d(kind, nx=120, nz=60, nt=60, abc_type="cerjan"),
-          small2d(kind, nx=96, nz=72, nt=60, seed=9),
-          small2d(kind, nx=140, nz=50, nt=60, seed=11, abc_type="cerjan")]
+    member's traces and fields equal its own independent run bitwise, with
+    moment sources or body forces (P-SV applies them between the interior
+    update and the sponge, SH after the sponge) and with the staged or the
+    tile-walking batch kernels."""
+    kw = {}
+    if bf:
+        kw = dict(bf_mode=True, sources=[Source(0.4, 0.0, 3.0, 0.0, 0.7, fx=1.0, fy=0.8, fz=-0.5),
+                                         Source(-9.9, 0.0, 1.0, 0.1, 0.6, fx=0.3, fy=1.0, fz=1.0)])
+    ps = [small2d(kind, nx=120, nz=60, nt=60, abc_type="cerjan", **kw),
+          small2d(kind, nx=96, nz=72, nt=60, seed=9, **kw),
+          small2d(kind, nx=140, nz=50, nt=60, seed=11, abc_type="cerjan", **kw)]
     members = [Swpc2D(p, kind) for p in ps]
     batch = Batch2D(members)
+    if not staged:
+        batch.set_staged(0, 0)
     batch.run(1, 60)
     for p in ps:
         g = Swpc2D(p, kind)

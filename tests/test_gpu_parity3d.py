@@ -427,3 +427,31 @@ def test_plane_wave_run_matches_oracle(ps):
         h.global__comm_vel()
     for n in range(9):
         assert same_bits(h.download(n), g.download(n)), n
+
+
+def test_failed_tile_copy_is_reported_until_the_state_is_restored():
+    """The error word of a timed-out tile wait, raised from the host (no
+    kernel made to wait or fault): swpc_sync reports it, keeps reporting it
+    across further steps, and a reset to rest (or a restored state and
+    swpc_clear_error) clears it; the run from rest then equals a fresh one."""
+    p = small3d(nt=20)
+    g = Swpc3D(p)
+    lib, ctx = g.lib, g.ctx
+    g.run(1, 5)
+    assert lib.swpc_sync(ctx) == _lib.SWPC_OK
+    assert lib.swpc_raise_copy_error(ctx) == _lib.SWPC_OK
+    assert lib.swpc_sync(ctx) == _lib.SWPC_ERR_CUDA
+    assert b"did not complete" in lib.swpc_last_error(ctx)
+    with pytest.raises(_lib.SwpcError):
+        g.run(6, 3)     # the run's own sync raises while the word is up
+    assert lib.swpc_sync(ctx) == _lib.SWPC_ERR_CUDA
+    _lib.check(ctx, lib.swpc_reset_state(ctx))
+    assert lib.swpc_sync(ctx) == _lib.SWPC_OK
+    g.run(1, p.nt)
+    h = Swpc3D(p)
+    h.run(1, p.nt)
+    for n in range(9):
+        assert same_bits(g.download(n), h.download(n))
+    assert lib.swpc_raise_copy_error(ctx) == _lib.SWPC_OK
+    _lib.check(ctx, lib.swpc_clear_error(ctx))
+    assert lib.swpc_sync(ctx) == _lib.SWPC_OK
