@@ -154,7 +154,8 @@ def c2a_cells(ps):
 def bench_c2a(args, world, rank, local):
     """Batched 2D P-SV ensemble (one persistent launch per half step, CUDA
     graph) against the plain per-model loop on the same GPU."""
-    ps_all = make_c2a_models()[:args.models]
+    ps_all = make_c2a_models()
+    ps_all = [ps_all[args.only_model]] if args.only_model is not None else ps_all[:args.models]
     ps = replicas.shard(ps_all, world, rank)   # members shard across GPUs
     wl = {"workload": f"batched ensemble of {len(ps_all)} uneven 2D P-SV models (nx 256-2048, nz 128-1024, nm=3, "
                       f"PML 20)",
@@ -790,6 +791,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3"])
     ap.add_argument("--models", type=int, default=64, help="c2a: the first N of the 64 models (profiling runs)")
+    ap.add_argument("--only-model", type=int, default=None, help="c2a: model I of the 64 alone (profiling runs)")
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (c3 profiling runs)")

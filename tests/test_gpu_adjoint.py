@@ -43,12 +43,9 @@ def fields(p):
     return out
 
 
-@pytest.mark.parametrize("staged", [1, 0])
-@pytest.mark.parametrize("nm", [3, 1])
-def test_adjoint_dot_product(nm, staged):
-    """staged: the TMA-staged stress-phase weights (1, the default) or the
-    one-cell-per-thread kernel (0)."""
-    p = small3d(nx=36, ny=30, nz=28, na=6, nt=10, nm=nm)
+def dot_product(p, staged):
+    """<L x, y> and <x, L^T y> on seeded random states x, y (every state
+    cell of the domain; memory variables on the kernel region)."""
     xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
     g = Swpc3D(p, xi)
     lib, ctx = g.lib, g.ctx
@@ -57,19 +54,19 @@ def test_adjoint_dot_product(nm, staged):
     dom, ker = domain_mask(p), kernel_mask(p)
     shape = dom.shape
     ld_k, ld_i = p.nz + 6, p.nx + 6
-    x, y = {}, {}
+    zero = np.float32(0.0)
+
+    def rand(mask):
+        return np.where(mask, rng.standard_normal(shape, dtype=np.float32), zero)
+
+    check(ctx, lib.swpc_adj_reset(ctx))
+    xe, ye = {}, {}
     for fid, kind in fields(p):
         mask = dom if kind != "ker" else ker
-        x[fid] = np.where(mask, rng.standard_normal(shape), 0.0).astype(np.float32)
-        y[fid] = np.where(mask, rng.standard_normal(shape), 0.0).astype(np.float32)
-    check(ctx, lib.swpc_adj_reset(ctx))
-    for fid, _ in fields(p):
-        g.upload(fid, x[fid])
-        check(ctx, lib.swpc_adj_upload(ctx, fid, fptr(y[fid]), ld_k, ld_i))
-    # the effective inputs (uploads keep only cells that are state)
-    xe = {fid: g.download(fid) for fid, _ in fields(p)}
-    ye = {}
-    for fid, _ in fields(p):
+        g.upload(fid, rand(mask))
+        check(ctx, lib.swpc_adj_upload(ctx, fid, fptr(rand(mask)), ld_k, ld_i))
+        # the effective inputs (uploads keep only cells that are state)
+        xe[fid] = g.download(fid)
         b = np.zeros(shape, np.float32)
         check(ctx, lib.swpc_adj_download(ctx, fid, fptr(b), ld_k, ld_i))
         ye[fid] = b
@@ -82,8 +79,26 @@ def test_adjoint_dot_product(nm, staged):
         Lx = g.download(fid)
         Lty = np.zeros(shape, np.float32)
         check(ctx, lib.swpc_adj_download(ctx, fid, fptr(Lty), ld_k, ld_i))
-        lhs += float(np.sum(Lx[mask].astype(np.float64) * ye[fid][mask]))
-        rhs += float(np.sum(xe[fid][mask].astype(np.float64) * Lty[mask]))
+        lhs += float(np.dot(Lx[mask].astype(np.float64), ye[fid][mask].astype(np.float64)))
+        rhs += float(np.dot(xe[fid][mask].astype(np.float64), Lty[mask].astype(np.float64)))
+    g.close()
+    return lhs, rhs
+
+
+@pytest.mark.parametrize("staged", [1, 0])
+@pytest.mark.parametrize("nm", [3, 1])
+def test_adjoint_dot_product(nm, staged):
+    """staged: the TMA-staged stress-phase weights (1, the default) or the
+    one-cell-per-thread kernel (0)."""
+    lhs, rhs = dot_product(small3d(nx=36, ny=30, nz=28, na=6, nt=10, nm=nm), staged)
+    assert abs(lhs - rhs) <= DOT_TOL * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def test_adjoint_dot_product_at_the_gradient_benchmark_grid():
+    """The same identity on the gradient benchmark's grid: 256 x 256 x 128
+    cells, PML 20, nm = 3, staged stress-phase weights."""
+    lhs, rhs = dot_product(small3d(nx=256, ny=256, nz=128, na=20, nt=10, nm=3), 1)
+    print("256x256x128 dot product:", lhs, rhs, abs(lhs - rhs) / max(abs(lhs), abs(rhs)))
     assert abs(lhs - rhs) <= DOT_TOL * max(abs(lhs), abs(rhs)), (lhs, rhs)
 
 
