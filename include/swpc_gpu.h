@@ -285,6 +285,39 @@ int swpc_green_source(swpc_ctx *ctx, int it);       /* m_green.f90:597-632   */
  * for call-order fidelity. */
 int swpc_comm_stress(swpc_ctx *ctx);
 int swpc_comm_vel(swpc_ctx *ctx);
+
+/* ---- decomposed grids (m_global.f90:236-303, 349-378, 393-609) ----------
+ * A context becomes one block of a grid split over nproc_x x nproc_y
+ * blocks (nproc_x for P-SV and SH): desc.nx / desc.ny are the block's
+ * extents, nx_global / ny_global the grid's, and the block's first cell is
+ * global cell (ioff + 1, joff + 1); the caller sizes the blocks as
+ * global__setup2 does (m_global.f90:236-300).  Call it right after
+ * swpc_create, before any medium, kernel or absorber setup: the kernel
+ * region then follows the global absorber layout, and the medium, absorber
+ * profiles, sources and stations are passed in block coordinates (the
+ * medium over the block's memory box, which includes the 3-cell sleeve;
+ * source cells anywhere in the sleeve, entries outside the block dropped as
+ * the sleeve exchange would overwrite them).  Not with the plane-wave mode,
+ * the adjoint or the batches. */
+int swpc_set_subdomain(swpc_ctx *ctx, int nx_global, int ny_global, int ioff, int joff);
+/* One step of a block: half 0 runs main.f90:125-136 up to
+ * global__comm_stress (wav__store, green__store, snapshots, the stress
+ * update, absorber, stress glut), half 1 the rest up to global__comm_vel.
+ * Between the halves and after half 1 the caller trades the halos. */
+int swpc_step_half(swpc_ctx *ctx, int it, int half);
+/* Halo exchange after half `half` (0: stress, 1: velocity) with the
+ * neighbour on side `side` (0 -x, 1 +x, 2 -y, 3 +y): the planes
+ * global__comm_* sends that way (m_global.f90:413-490, 521-603; P-SV and SH
+ * from their own m_global.f90) as one flat message of *count floats.
+ * swpc_halo_pack writes the message that the neighbour on `side` receives to
+ * dst (any device memory this GPU can store to, a peer-mapped buffer
+ * included), swpc_halo_unpack writes the message that neighbour sent into
+ * this block's sleeve; both are asynchronous on the context's stream.  A
+ * side without a neighbour is left alone (its sleeve stays zero, as
+ * MPI_PROC_NULL leaves it). */
+int swpc_halo_count(swpc_ctx *ctx, int half, int side, long long *count);
+int swpc_halo_pack(swpc_ctx *ctx, int half, int side, float *dst);
+int swpc_halo_unpack(swpc_ctx *ctx, int half, int side, const float *src);
 /* Plane-wave mode (pw_mode, src/swpc_3d/m_source.f90:67-79): with on != 0
  * the absorber updates first extrapolate the ghost planes of the four side
  * faces from inside (V before the stress update, S before the velocity

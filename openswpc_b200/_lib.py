@@ -51,6 +51,7 @@ EXPORTS = [
     "swpc_x2i", "swpc_i2x", "swpc_momentrate", "swpc_sdr2moment", "swpc_visco_setup", "swpc_kbeg_a",
     "swpc_vmodel_lhm", "swpc_vmodel_lhm_opt", "swpc_seawater_vel", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
     "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt", "swpc_rmedia_generate", "swpc_pw_setup", "swpc_set_pw_mode", "swpc_clear_error", "swpc_raise_copy_error",
+    "swpc_set_subdomain", "swpc_step_half", "swpc_halo_count", "swpc_halo_pack", "swpc_halo_unpack",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
@@ -204,6 +205,11 @@ def load():
         "swpc_rmedia_generate": (i, [C.POINTER(RmediaDesc), _FP, i, i, vp]),
         "swpc_pw_setup": (i, [C.POINTER(Grid), _FP, _FP, _FP, f, f, i, f, f, f, i] + [_FP] * 9 + [_FP]),
         "swpc_set_pw_mode": (i, [vp, i]),
+        "swpc_set_subdomain": (i, [vp, i, i, i, i]),
+        "swpc_step_half": (i, [vp, i, i]),
+        "swpc_halo_count": (i, [vp, i, i, C.POINTER(C.c_longlong)]),
+        "swpc_halo_pack": (i, [vp, i, i, vp]),
+        "swpc_halo_unpack": (i, [vp, i, i, vp]),
         "swpc_clear_error": (i, [vp]),
         "swpc_raise_copy_error": (i, [vp]),
         "swpc_batch_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),

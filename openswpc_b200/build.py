@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-f
               "-Xptxas", "-O3"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 
-CU_SOURCES = ["swpc3d_kernels.cu", "swpc3d_march.cu", "swpc3d_vec.cu", "swpc2d_kernels.cu", "swpc_api.cu", "swpc2d_api.cu", "swpc_noalloc.cu", "swpc_snap.cu", "swpc_prec.cu", "swpc_adjoint.cu", "swpc_fbatch.cu", "swpc3d_tma.cu", "swpc2d_tma.cu", "swpc_medium.cu", "swpc_green.cu", "swpc_rmedia.cu", "swpc_pw.cu"]
+CU_SOURCES = ["swpc3d_kernels.cu", "swpc3d_march.cu", "swpc3d_vec.cu", "swpc2d_kernels.cu", "swpc_api.cu", "swpc2d_api.cu", "swpc_noalloc.cu", "swpc_snap.cu", "swpc_prec.cu", "swpc_adjoint.cu", "swpc_fbatch.cu", "swpc3d_tma.cu", "swpc2d_tma.cu", "swpc_medium.cu", "swpc_green.cu", "swpc_rmedia.cu", "swpc_pw.cu", "swpc_decomp.cu"]
 CPP_SOURCES = ["swpc_host.cpp", "swpc_io.cpp"]
 
 

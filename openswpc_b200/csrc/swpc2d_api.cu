@@ -128,15 +128,15 @@ int cerjan_setup_2d(swpc_ctx *c, const float *gx_c, const float *gx_b, const flo
 // absorb_c__update_stress / _vel of P-SV (src/swpc_psv/m_absorb_c.f90:
 // 90-160) and SH (src/swpc_sh/m_absorb_c.f90:82-135) in the reference's
 // product order; cells with both factors 1 are not visited (same bits)
-__global__ void cerjan2d_kernel(int psv, int phase, int nx, int nz, int na, int Kp, const float *__restrict__ cj,
-                                float *f0, float *f1, float *f2) {
+__global__ void cerjan2d_kernel(int psv, int phase, int nx, int nz, int na, int ioff, int nxg, int Kp,
+                                const float *__restrict__ cj, float *f0, float *f1, float *f2) {
     const float *gxc = cj, *gxb = cj + nx, *gzc = cj + 2 * nx, *gzb = gzc + nz;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     // one warp per column, lanes along k: every k of the side columns, the
     // bottom na cells of the others
     for (int i = 1 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i <= nx; i += nw) {
-        const bool side = i <= na || i > nx - na;
+        const bool side = i + ioff <= na || i + ioff > nxg - na;   // global column
         const float xc = gxc[i - 1], xb = gxb[i - 1];
         for (int k = (side ? 1 : nz - na + 1) + lane; k <= nz; k += 32) {
             const long long e = (long long)(i + 2) * Kp + (k - 1 + KH);
@@ -172,8 +172,8 @@ static int launch_cerjan2d(swpc_ctx *c, int phase, cudaStream_t stream) {
         f0 = psv ? c->V[0] : c->V[1];
         f1 = psv ? c->V[2] : nullptr;
     }
-    cerjan2d_kernel<<<148 * 4, 256, 0, stream>>>(psv ? 1 : 0, phase, c->g.nx, c->g.nz, c->d.na, c->g.Kp, c->cj, f0,
-                                                  f1, f2);
+    cerjan2d_kernel<<<148 * 4, 256, 0, stream>>>(psv ? 1 : 0, phase, c->g.nx, c->g.nz, c->d.na, c->ioff, c->nxg,
+                                                  c->g.Kp, c->cj, f0, f1, f2);
     return cuda_check(c, cudaGetLastError(), "cerjan2d launch");
 }
 

@@ -121,6 +121,7 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     if (d->kind != SWPC_KIND_3D) { c->jbk = 1; c->jek = 1; }
     c->kbk = 1;
     c->kek = nz - na;
+    c->nxg = nx; c->nyg = ny;
     Geo &g = c->g;
     g.nx = nx; g.ny = ny; g.nz = nz;
     g.Kp = ((nz + 3 + KH) + 7) / 8 * 8;
@@ -658,8 +659,9 @@ extern "C" int swpc_absorb_setup_cerjan(swpc_ctx *c, const float *gx_c, const fl
 // lanes along k: every k of the side columns, the bottom na cells of the
 // others.  The cells skipped have all factors 1, and a product with 1
 // leaves the bits unchanged.
-__global__ void cerjan3d_kernel(Geo g, int na, int phase, const float *__restrict__ cj, float *f0, float *f1,
-                                float *f2, float *f3, float *f4, float *f5) {
+__global__ void cerjan3d_kernel(Geo g, int na, int ioff, int joff, int nxg, int nyg, int phase,
+                                const float *__restrict__ cj, float *f0, float *f1, float *f2, float *f3, float *f4,
+                                float *f5) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const float *gxc = cj, *gxb = cj + nx, *gyc = cj + 2 * nx, *gyb = gyc + ny, *gzc = gyc + 2 * ny, *gzb = gzc + nz;
     const int lane = threadIdx.x & 31;
@@ -667,7 +669,8 @@ __global__ void cerjan3d_kernel(Geo g, int na, int phase, const float *__restric
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < ncol; w += nw) {
         const int i = 1 + (int)(w % nx), j = 1 + (int)(w / nx);
-        const bool side = i <= na || i > nx - na || j <= na || j > ny - na;
+        const int ig = i + ioff, jg = j + joff;   // global column
+        const bool side = ig <= na || ig > nxg - na || jg <= na || jg > nyg - na;
         const float xc = gxc[i - 1], xb = gxb[i - 1], yc = gyc[j - 1], yb = gyb[j - 1];
         for (int k = (side ? 1 : nz - na + 1) + lane; k <= nz; k += 32) {
             const long long e = cell_index(g, k, i, j);
@@ -691,7 +694,8 @@ __global__ void cerjan3d_kernel(Geo g, int na, int phase, const float *__restric
 
 static int launch_cerjan(swpc_ctx *c, int phase) {
     float *const *f = phase == 0 ? c->S : c->V;
-    cerjan3d_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, c->d.na, phase, c->cj, f[0], f[1], f[2],
+    cerjan3d_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, c->d.na, c->ioff, c->joff, c->nxg, c->nyg, phase, c->cj,
+                                                     f[0], f[1], f[2],
                                                      phase == 0 ? f[3] : nullptr, phase == 0 ? f[4] : nullptr,
                                                      phase == 0 ? f[5] : nullptr);
     return cuda_check(c, cudaGetLastError(), "cerjan3d launch");
@@ -1261,17 +1265,19 @@ extern "C" int swpc_comm_vel(swpc_ctx *c) {
 extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(c, it, nullptr); }
 
 // main.f90:125-144 loop body (report__progress is driven by the caller
-// between steps); with record = false the wavefield advances without
-// wav__store, green__store and snap__write
-static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
+// between steps) in two halves: up to global__comm_stress (half 0) and from
+// there up to global__comm_vel (half 1); with record = false the wavefield
+// advances without wav__store, green__store and snap__write
+static int step_half0(swpc_ctx *c, int it, const int *d_it, bool record) {
     if (record) {
         RC(launch_wav(c, it, d_it));
         RC(green_store_launch(c, it, d_it));
         RC(snap_launch(c, it, d_it));
     }
     RC(launch_stress(c, 3));
-    RC(launch_glut(c, it, d_it));
-    RC(pw_comm_zero(c, 1));   // global__comm_stress (no-op outside plane-wave mode)
+    return launch_glut(c, it, d_it);
+}
+static int step_half1(swpc_ctx *c, int it, const int *d_it) {
     if (c->kind == SWPC_KIND_PSV && c->ninj_bf > 0) {
         // P-SV applies body forces between the interior and absorber velocity
         // updates (src/swpc_psv/main.f90:106-110)
@@ -1282,9 +1288,24 @@ static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
         RC(launch_vel(c, 3));
         RC(launch_bf(c, it, d_it));
     }
-    RC(launch_green(c, it, d_it));
+    return launch_green(c, it, d_it);
+}
+
+static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
+    RC(step_half0(c, it, d_it, record));
+    RC(pw_comm_zero(c, 1));   // global__comm_stress (no-op outside plane-wave mode)
+    RC(step_half1(c, it, d_it));
     RC(pw_comm_zero(c, 0));   // global__comm_vel
     return SWPC_OK;
+}
+
+extern "C" int swpc_step_half(swpc_ctx *c, int it, int half) {
+    if (!c) return SWPC_ERR_ARG;
+    if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
+    if (half != 0 && half != 1) return set_err(c, SWPC_ERR_ARG, "half must be 0 (stress) or 1 (velocity)");
+    if (c->pw_mode) return set_err(c, SWPC_ERR_STATE, "the plane-wave mode steps whole steps (swpc_step)");
+    PREP(c);
+    return half == 0 ? step_half0(c, it, nullptr, true) : step_half1(c, it, nullptr);
 }
 
 extern "C" int swpc_step(swpc_ctx *c, int it) {
@@ -1362,10 +1383,11 @@ extern "C" int swpc_vmax(swpc_ctx *c, float out[3]) {
         const int margin = 5, na = c->d.na;
         VmaxArgs a;
         a.g = c->g;
-        a.j0 = std::max(na + margin + 1, c->jbk);
-        a.j1 = std::min(c->g.ny - na - margin, c->jek);
-        a.i0 = std::max(na + margin + 1, c->ibk);
-        a.i1 = std::min(c->g.nx - na - margin, c->iek);
+        // global bounds of m_kernel.f90:343-344 in this box's coordinates
+        a.j0 = std::max(na + margin + 1 - c->joff, c->jbk);
+        a.j1 = std::min(c->nyg - na - margin - c->joff, c->jek);
+        a.i0 = std::max(na + margin + 1 - c->ioff, c->ibk);
+        a.i1 = std::min(c->nxg - na - margin - c->ioff, c->iek);
         a.kob = c->kob;
         a.Vx = c->V[0]; a.Vy = c->V[1]; a.Vz = c->V[2];
         a.out = c->vmax_buf;

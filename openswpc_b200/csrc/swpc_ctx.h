@@ -72,6 +72,10 @@ struct swpc_ctx {
 
     // kernel region (m_global.f90:349-378)
     int ibk, iek, jbk, jek, kbk, kek;
+    // subdomain of a decomposed grid (m_global.f90:236-303): the global
+    // extents and this box's offsets (nxg = nx, ioff = 0 on a single domain)
+    int nxg = 0, nyg = 0, ioff = 0, joff = 0;
+    bool sub = false;
 
     // full-grid fields
     float *V[3] = {nullptr, nullptr, nullptr};          // Vx Vy Vz (2D: Vx Vz / Vy)

@@ -126,6 +126,7 @@ extern "C" int swpc_set_pw_mode(swpc_ctx *c, int on) {
     if (on && c->prec != SWPC_PREC_F32) return set_err(c, SWPC_ERR_ARG, "the plane-wave mode needs FP32 storage");
     if (on && c->abc != 0) return set_err(c, SWPC_ERR_ARG, "the plane-wave boundary belongs to the PML (abc_type 'pml')");
     if (on && (c->g.nx < 2 || c->g.ny < 2)) return set_err(c, SWPC_ERR_ARG, "the plane-wave mode needs nx, ny >= 2");
+    if (on && c->sub) return set_err(c, SWPC_ERR_ARG, "the plane-wave mode runs on a single domain");
     c->pw_mode = on ? 1 : 0;
     c->desc_dirty = true;
     if (c->graph_exec) {

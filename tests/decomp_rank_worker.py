@@ -1,0 +1,36 @@
+"""One rank of the one-GPU test of BlockRank3D (tests/test_gpu_decomp.py):
+joins a gloo group from the torchrun-style environment, runs its block of the
+decomposed test case on cuda:0 (the halo messages staged through host
+memory), and saves its traces, station indices, block extents, fields and
+report values to <outdir>/rank<r>.npz."""
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+import numpy as np  # noqa: E402
+
+from openswpc_b200 import _lib, replicas  # noqa: E402
+from openswpc_b200.decomp import BlockRank3D  # noqa: E402
+from tests.test_gpu_decomp import FIELDS, decomp_case  # noqa: E402
+
+
+def main():
+    nproc_x, nproc_y, outdir = int(sys.argv[1]), int(sys.argv[2]), Path(sys.argv[3])
+    ranks = replicas.init("gloo", timeout_s=120)
+    p, xi = decomp_case()
+    r = BlockRank3D(p, nproc_x, nproc_y, xi, device=0)
+    rep = r.run(1, p.nt)
+    b = r.block
+    out = {"wav": r.waveforms(_lib.WAV_V), "stations": b.stations, "ext": np.array([b.ib, b.ie, b.jb, b.je]),
+           "reports": np.array([v for _, v in rep])}
+    for f in FIELDS:
+        out[f"f{f}"] = b.download(f)
+    np.savez(outdir / f"rank{ranks.rank}.npz", **out)
+    ranks.barrier()
+    r.close()
+    ranks.close()
+
+
+if __name__ == "__main__":
+    main()
