@@ -241,22 +241,13 @@ class _Run:
         return reports
 
 
-class Decomposed3D(_Run):
-    """All blocks of a nproc_x x nproc_y split in this process.  ``devices``
-    lists the CUDA device of each block (default: all on device 0); the
-    halo messages travel through device buffers, across devices by copy."""
+class _InProcess(_Run):
+    """All blocks in this process; the halo messages travel through device
+    buffers, across devices by copy."""
 
-    def __init__(self, p: Params, nproc_x: int, nproc_y: int, xi=None, devices=None, medium: Medium | None = None,
-                 precision: str = "f32"):
+    def _buffers(self):
         import torch
 
-        p.check()
-        self.p = p
-        self.sh = _Shared(p, xi, medium)
-        nb = nproc_x * nproc_y
-        devices = list(devices) if devices is not None else [0] * nb
-        self.blocks = [Block3D(self.sh, r % nproc_x, r // nproc_x, nproc_x, nproc_y, devices[r], precision)
-                       for r in range(nb)]
         # one outgoing buffer per (block, half, side with a neighbour), on the sender's device
         self.buf = {}
         for r, b in enumerate(self.blocks):
@@ -273,6 +264,7 @@ class Decomposed3D(_Run):
                     b.pack(half, side, self.buf[r, half, side].data_ptr())
         for b in self.blocks:
             b.sync()
+        held = []   # copies across devices stay alive until the unpacks are done
         for r, b in enumerate(self.blocks):
             for side, nbr in enumerate(b.neighbours):
                 if nbr is None:
@@ -280,9 +272,11 @@ class Decomposed3D(_Run):
                 msg = self.buf[nbr, half, OPPOSITE[side]]
                 if msg.device.index != b.device:
                     msg = msg.to(f"cuda:{b.device}")
+                    held.append(msg)
                 b.unpack(half, side, msg.data_ptr())
         for b in self.blocks:
             b.sync()
+        del held
 
     def step(self, it: int):
         for b in self.blocks:
@@ -294,6 +288,39 @@ class Decomposed3D(_Run):
 
     def vmax(self) -> np.ndarray:
         return np.max(np.stack([b.vmax() for b in self.blocks]), axis=0)
+
+    def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
+        """Every block's traces in the global station order."""
+        parts = [(b.stations, b.waveforms(what)) for b in self.blocks if b.nst]
+        if not parts:
+            return np.zeros((0, 0, 0), np.float32)
+        ncmp, ntw = parts[0][1].shape[1:]
+        out = np.zeros((len(self.sh.ist), ncmp, ntw), np.float32)
+        for idx, w in parts:
+            out[idx] = w
+        return out
+
+    def close(self):
+        for b in self.blocks:
+            b.close()
+        self.blocks = []
+
+
+class Decomposed3D(_InProcess):
+    """All blocks of a nproc_x x nproc_y split of a 3D run in this process.
+    ``devices`` lists the CUDA device of each block (default: all on device
+    0)."""
+
+    def __init__(self, p: Params, nproc_x: int, nproc_y: int, xi=None, devices=None, medium: Medium | None = None,
+                 precision: str = "f32"):
+        p.check()
+        self.p = p
+        self.sh = _Shared(p, xi, medium)
+        nb = nproc_x * nproc_y
+        devices = list(devices) if devices is not None else [0] * nb
+        self.blocks = [Block3D(self.sh, r % nproc_x, r // nproc_x, nproc_x, nproc_y, devices[r], precision)
+                       for r in range(nb)]
+        self._buffers()
 
     def download(self, field: int) -> np.ndarray:
         """The field over the global memory box (interior cells of every
@@ -310,21 +337,156 @@ class Decomposed3D(_Run):
             out[b.joff + j0:b.joff + j1, b.ioff + i0:b.ioff + i1, :] = a[j0:j1, i0:i1, :]
         return out
 
-    def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
-        parts = [(b.stations, b.waveforms(what)) for b in self.blocks if b.nst]
-        n = len(self.sh.ist)
-        if not parts:
-            return np.zeros((0, 3, 0), np.float32)
-        ncmp, ntw = parts[0][1].shape[1:]
-        out = np.zeros((n, ncmp, ntw), np.float32)
-        for idx, w in parts:
-            out[idx] = w
+
+
+class _Shared2D:
+    """The whole-grid part of a 2D run's setup (P-SV or SH)."""
+
+    def __init__(self, p: Params, kind: str):
+        from .swpc2d import Medium2D, grid2d, source_grid2d, station_grid2d
+
+        lib = _lib.load()
+        self.lib, self.p, self.kind = lib, p, kind
+        self.medium = Medium2D(p)
+        self.src = source_grid2d(p, kind)
+        self.stf = _lib.STF_CODES[p.stftype]
+        self.what = (_lib.WAV_V * p.sw_wav_v) | (_lib.WAV_U * p.sw_wav_u)
+        m = self.medium
+        if p.stations and self.what:
+            self.ist, self.kst = station_grid2d(p, m.kfs, m.kob)
+        else:
+            self.ist = self.kst = np.zeros(0, np.int32)
+        g = grid2d(p)
+        if p.abc_type == "cerjan":
+            self.cprof = {k: np.zeros(p.nx if k[1] == "x" else p.nz, np.float32)
+                          for k in ("gx_c", "gx_b", "gz_c", "gz_b")}
+            cp = self.cprof
+            lib.swpc_cerjan_profiles(C.byref(g), fptr(cp["gx_c"]), fptr(cp["gx_b"]), None, None, fptr(cp["gz_c"]),
+                                     fptr(cp["gz_b"]))
+        else:
+            self.gprof = {k: np.zeros((p.nx if k[1] == "x" else p.nz, 4), np.float32)
+                          for k in ("gxc", "gxe", "gzc", "gze")}
+            gp = self.gprof
+            lib.swpc_damping_profiles(C.byref(g), float(f32(self.src.fcut)), fptr(gp["gxc"]), fptr(gp["gxe"]), None,
+                                      None, fptr(gp["gzc"]), fptr(gp["gze"]))
+
+
+class Block2D:
+    """Block px of a P-SV or SH grid split nproc_x ways across x (the 2D
+    codes' global__setup2, src/swpc_psv/m_global.f90)."""
+
+    def __init__(self, sh: _Shared2D, px: int, nproc_x: int, device: int = 0):
+        from .swpc2d import KINDS, Medium2D
+
+        p, lib = sh.p, sh.lib
+        self.lib, self.p, self.kind = lib, p, sh.kind
+        self.ib, self.ie = block_range(p.nx, nproc_x, px)
+        self.ioff, self.nx = self.ib - 1, self.ie - self.ib + 1
+        if self.nx < 4:
+            raise ValueError("blocks must be at least 4 cells wide")
+        self.neighbours = neighbours(px, 0, nproc_x, 1)
+        self.device = device
+        desc = _lib.Desc(KINDS[sh.kind], self.nx, 1, p.nz, p.na, p.nm, p.nt, p.dx, p.dx, p.dz, p.dt, p.tbeg, device)
+        ctx = C.c_void_p()
+        rc = lib.swpc_create(C.byref(desc), C.byref(ctx))
+        self.ctx = ctx
+        if rc:
+            msg = lib.swpc_last_error(ctx) if ctx else b""
+            lib.swpc_destroy(ctx)
+            self.ctx = None
+            raise _lib.SwpcError(rc, msg.decode() if msg else "swpc_create failed")
+        check(ctx, lib.swpc_set_subdomain(ctx, p.nx, 1, self.ioff, 0))
+        gm = sh.medium
+        cols = slice(self.ioff, self.ioff + self.nx + 6)
+        m = Medium2D.__new__(Medium2D)
+        for name in Medium2D.FIELDS:
+            setattr(m, name, np.ascontiguousarray(getattr(gm, name)[cols]))
+        for name in Medium2D.MAPS:
+            setattr(m, name, np.ascontiguousarray(getattr(gm, name)[cols]))
+        m.ts = gm.ts
+        self.medium = m
+        check(ctx, lib.swpc_upload_medium(ctx, C.byref(m.view())))
+        check(ctx, lib.swpc_kernel_setup(ctx, fptr(m.ts)))
+        s = sh.src
+        keep = (s.isrc >= self.ib - 2) & (s.isrc <= self.ie + 3)   # src/swpc_psv/m_source.f90:182
+        isrc = np.ascontiguousarray(s.isrc[keep] - self.ioff, np.int32)
+        ksrc = np.ascontiguousarray(s.ksrc[keep], np.int32)
+        prm = np.ascontiguousarray(s.srcprm[keep], np.float32)
+        if p.bf_mode:
+            check(ctx, lib.swpc_bodyforce_setup(ctx, len(isrc), iptr(isrc), None, iptr(ksrc), fptr(prm),
+                                                fptr(np.ascontiguousarray(s.f3[keep], np.float32)), sh.stf))
+        else:
+            check(ctx, lib.swpc_source_setup(ctx, len(isrc), iptr(isrc), None, iptr(ksrc), fptr(prm),
+                                             fptr(np.ascontiguousarray(s.mo[keep], np.float32)),
+                                             fptr(np.ascontiguousarray(s.m6[keep], np.float32)), sh.stf))
+        ix = slice(self.ioff, self.ioff + self.nx)
+        if p.abc_type == "cerjan":
+            cp = {k: np.ascontiguousarray(v[ix] if k[1] == "x" else v) for k, v in sh.cprof.items()}
+            check(ctx, lib.swpc_absorb_setup_cerjan(ctx, fptr(cp["gx_c"]), fptr(cp["gx_b"]), None, None,
+                                                    fptr(cp["gz_c"]), fptr(cp["gz_b"])))
+        else:
+            gp = {k: np.ascontiguousarray(v[ix] if k[1] == "x" else v) for k, v in sh.gprof.items()}
+            check(ctx, lib.swpc_absorb_setup(ctx, fptr(gp["gxc"]), fptr(gp["gxe"]), None, None, fptr(gp["gzc"]),
+                                             fptr(gp["gze"])))
+        own = (sh.ist >= self.ib) & (sh.ist <= self.ie)   # src/swpc_psv/m_wav.f90:503
+        self.stations = np.nonzero(own)[0]
+        self.nst = len(self.stations)
+        if self.nst:
+            ist = np.ascontiguousarray(sh.ist[own] - self.ioff, np.int32)
+            kst = np.ascontiguousarray(sh.kst[own], np.int32)
+            check(ctx, lib.swpc_wav_setup(ctx, self.nst, iptr(ist), None, iptr(kst), p.ntdec_w, sh.what, s.M0, s.UC))
+        self.halo_count = [[0] * SIDES for _ in range(2)]
+        n = C.c_longlong()
+        for half in (0, 1):
+            for side in (0, 1):
+                check(ctx, lib.swpc_halo_count(ctx, half, side, C.byref(n)))
+                self.halo_count[half][side] = int(n.value)
+
+    step_half, pack, unpack, sync, close, __del__ = (Block3D.step_half, Block3D.pack, Block3D.unpack, Block3D.sync,
+                                                      Block3D.close, Block3D.__del__)
+
+    def vmax(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(self.ctx, self.lib.swpc_vmax(self.ctx, fptr(out)))
+        return out[:2] if self.kind == "psv" else out[:1]
+
+    def download(self, field: int) -> np.ndarray:
+        out = np.zeros((self.nx + 6, self.p.nz + 6), np.float32)
+        check(self.ctx, self.lib.swpc_download_field(self.ctx, field, fptr(out), self.p.nz + 6, self.nx + 6))
         return out
 
-    def close(self):
+    def waveforms(self, what: int = _lib.WAV_V) -> np.ndarray:
+        ntw, nst = C.c_int(), C.c_int()
+        check(self.ctx, self.lib.swpc_wav_dims(self.ctx, C.byref(ntw), C.byref(nst)))
+        nc = 2 if self.kind == "psv" else 1
+        out = np.zeros((nst.value, nc, ntw.value), np.float32)
+        if nst.value:
+            check(self.ctx, self.lib.swpc_wav_fetch(self.ctx, what, fptr(out)))
+        return out
+
+
+class Decomposed2D(_InProcess):
+    """A P-SV or SH run split into nproc_x blocks across x, all in this
+    process (``devices``: the CUDA device of each block)."""
+
+    def __init__(self, p: Params, kind: str, nproc_x: int, devices=None):
+        p.check()
+        self.p = p
+        self.sh = _Shared2D(p, kind)
+        devices = list(devices) if devices is not None else [0] * nproc_x
+        self.blocks = [Block2D(self.sh, q, nproc_x, devices[q]) for q in range(nproc_x)]
+        self._buffers()
+
+    def download(self, field: int) -> np.ndarray:
+        """The field over the global memory box (nx+6, nz+6)."""
+        p = self.p
+        out = np.zeros((p.nx + 6, p.nz + 6), np.float32)
         for b in self.blocks:
-            b.close()
-        self.blocks = []
+            a = b.download(field)
+            i0 = 0 if b.ioff == 0 else 3
+            i1 = b.nx + 6 if b.ie == p.nx else b.nx + 3
+            out[b.ioff + i0:b.ioff + i1] = a[i0:i1]
+        return out
 
 
 class HaloTransport:

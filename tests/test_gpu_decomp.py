@@ -154,3 +154,31 @@ def test_block_ranks_over_gloo_on_one_gpu(tmp_path):
             assert_same_bits(a[3:-3, 3:-3, :], ref[f][jb + 2:je + 3, ib + 2:ie + 3, :], f"rank {rank} field {f}")
         assert_same_bits(z["reports"], ref["reports"], "reports")
     assert_same_bits(wav, ref["wav"], "traces")
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh"])
+def test_decomposed_2d_run_gives_the_single_domain_bits(kind):
+    """P-SV and SH split into 3 blocks across x (the 2D codes' own
+    global__comm_*), with sources and stations on the seams."""
+    from openswpc_b200.decomp import Decomposed2D
+    from openswpc_b200.swpc2d import Swpc2D
+    from tests.models import small2d
+
+    p = small2d(kind, nx=124, nz=60, na=10, nt=80)
+    # block seams of a 3-way split of 124 cells: 41|42 and 82|83 (x = xbeg + i dx)
+    for n, i in enumerate((41, 42, 82)):
+        s = p.sources[0]
+        p.sources.append(type(s)(**{**s.__dict__, "x": float(p.xbeg + (i - 0.3) * p.dx), "z": 3.0 + n}))
+        st = p.stations[0]
+        p.stations.append(type(st)(**{**st.__dict__, "x": float(p.xbeg + (i - 0.5) * p.dx), "name": f"seam{n}"}))
+    g = Swpc2D(p, kind)
+    g.run(1, p.nt)
+    d = Decomposed2D(p, kind, 3)
+    d.run(1, p.nt)
+    assert_same_bits(d.waveforms(_lib.WAV_V), g.waveforms(_lib.WAV_V), "traces")
+    ids = [_lib.F_VX, _lib.F_VZ, _lib.F_SXX, _lib.F_SZZ, _lib.F_SXZ] if kind == "psv" else [_lib.F_VY, _lib.F_SXY,
+                                                                                            _lib.F_SYZ]
+    for f in ids:
+        assert_same_bits(d.download(f), g.download(f), f"field {f}")
+    d.close()
+    g.close()
