@@ -6,21 +6,13 @@
 // src/swpc_3d/m_absorb_p.f90:126-505) is linear in the wavefield state
 // (V, S, R, PML auxiliaries).  This file applies its exact transpose, in the
 // reverse order, as two kinds of passes per half step:
-//   weights: per cell, the adjoint of that cell's own update that carries
-//            state -- memory variables and PML auxiliaries in place -- and
-//            the cell's share of the difference operators it applied: in
-//            absorber cells the 2nd-order weight of each of the nine
-//            (field, axis) operators, in interior cells of the stress phase
-//            the six distinct operator inputs ld (the 4th-order coefficient
-//            pair multiplies them in the gather);
+//   weights: per cell, the adjoint of that cell's own update -- memory
+//            variables and PML auxiliaries in place, and for each of the
+//            nine (field, axis) difference operators the two weights that
+//            multiply the 4th-order coefficient pair (2nd-order difference
+//            r20 and zero in absorber cells);
 //   gather:  per cell, the transposed stencil: every neighbour that read this
-//            cell adds its weight with the sign of the difference.  The
-//            weights of an interior neighbour are formed on the fly: e40 * x
-//            and e41 * x with x its stored ld (stress phase) or, in the
-//            velocity phase, b dt lambda_V from the adjoint velocity itself,
-//            so interior cells store nothing in that phase.  Every product
-//            and sum is the one a stored-weight form would compute, so the
-//            result is the same to the bit.
+//            cell adds its weight with the sign of the difference.
 // Receiver residuals enter as sources at the transposed recorder cells
 // (wav__store, src/swpc_3d/m_wav.f90:530-535).  The gradient imaging
 // condition pairs the adjoint with the forward derivatives of the same step
@@ -54,11 +46,10 @@ using namespace swpc;
 // adjoint state of a context
 struct swpc_adj_state {
     float *lV[3] = {}, *lS[6] = {}, *lR[18] = {}, *laux[18] = {};
-    float *laux_alt[9] = {};             // second buffer of the velocity-phase auxiliaries (laux 9-17)
     float *slab = nullptr;               // lV, lS, lR in the forward slab's field order (V, S, R)
     int slab_nf = 0;
     swpc::TmaMaps *maps = nullptr;       // staged stress-phase weights: state, s6 (adjoint slab), med, vh (slots)
-    float *W[9] = {};                    // difference-operator weights (absorber) and ld (interior)
+    float *w40[9] = {}, *w41[9] = {};    // difference-operator weights
     double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
     int ckpt = 0, nseg = 0;
@@ -72,6 +63,21 @@ namespace {
 
 constexpr int kThreadsK = 32;
 
+struct AdjVelArgs {
+    Geo g;
+    int ibk, iek, jbk, jek, kek;
+    const float *lV[3];
+    const float *b[3];
+    const int4 *band;
+    const int2 *pmlcol;
+    float *laS[9];               // adjoint of the velocity-phase PML auxiliaries
+    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
+    float e40[3][2], e41[3][2], r20[3], dt;
+    float *w40[9], *w41[9];
+    const float *S[6];           // forward S after the stress update (gradient)
+    double *gb[3];               // gradient of bx, by, bz (null: none)
+};
+
 struct AdjStrArgs {
     Geo g;
     int ibk, iek, jbk, jek, kek, nm;
@@ -84,29 +90,15 @@ struct AdjStrArgs {
     const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
     float e40[3][2], e41[3][2], r20[3], dt;
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
-    float *W[9];
+    float *w40[9], *w41[9];
     const float *V[3];           // forward V before the stress update (gradient)
     double *gm[5];               // gradient of lam, mu, muyz, muxz, muxy (null: none)
 };
 
 struct GatherArgs {
     Geo g;
-    int ibk, iek, jbk, jek, kek;
-    const int4 *band;
-    float e40[3][2], e41[3][2], dt;
-    const float *W[9];           // absorber weights; interior ld (stress phase)
     float *dst[6];
-    // velocity phase: the weights of every cell are formed from b dt lambda_V
-    // and, in absorber cells, the auxiliaries before the step (laS_old); the
-    // auxiliaries after it go to laS_new
-    const float *lV[3], *b[3];
-    const int2 *pmlcol;
-    const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
-    const float *laS_old[9];
-    float *laS_new[9];
-    float r20[3];
-    const float *S[6];           // forward S after the stress update (gradient)
-    double *gb[3];               // gradient of bx, by, bz (null: none)
+    const float *w40[9], *w41[9];
 };
 
 __device__ __forceinline__ bool cell_of(const Geo &g, int &k, int &i, int &j) {
@@ -132,150 +124,118 @@ constexpr int BI = 4, BJ = 4, NT = KT * BI * BJ;
 }  // namespace adjt
 
 // ---------------------------------------------------------------------------
-// the transposed stencil: neighbour classes and weight pairs
-// ---------------------------------------------------------------------------
-// class of cell (k, i, j): -1 outside the grid (no weights), -2 absorber cell
-// (a stored 2nd-order weight, no 4th-order term), else the band sign of an
-// interior cell
-__device__ __forceinline__ int cell_class(const GatherArgs &a, int k, int i, int j) {
-    const Geo &g = a.g;
-    if (k < 1 || k > g.nz || i < 1 || i > g.nx || j < 1 || j > g.ny) return -1;
-    if (i < a.ibk || i > a.iek || j < a.jbk || j > a.jek || k > a.kek) return -2;
-    return band_sign(__ldg(&a.band[col_index(g, i, j)]), k);
-}
-
-// classes of the cells at offsets -2..2 along x, y and z of a cell
-struct Classes {
-    int c[3][5];
-};
-__device__ __forceinline__ Classes classes_of(const GatherArgs &a, int k, int i, int j) {
-    Classes r;
-    const int own = cell_class(a, k, i, j);
-#pragma unroll
-    for (int o = -2; o <= 2; o++) {
-        r.c[0][o + 2] = o == 0 ? own : cell_class(a, k, i + o, j);
-        r.c[1][o + 2] = o == 0 ? own : cell_class(a, k, i, j + o);
-        r.c[2][o + 2] = o == 0 ? own : cell_class(a, k + o, i, j);
-    }
-    return r;
-}
-
-// the weights (w40, w41) that multiply the 4th-order coefficient pair
-struct W2 {
-    float w40, w41;
-};
-__device__ __forceinline__ W2 interior_w(const GatherArgs &a, int ax, int cl, float x) {
-    const float e40 = cl ? a.e40[ax][1] : a.e40[ax][0];
-    const float e41 = cl ? a.e41[ax][1] : a.e41[ax][0];
-    return W2{e40 * x, e41 * x};
-}
-
-// transpose of a forward difference (f[e+P] - f[e]) * A40 - (f[e+2P] - f[e-P]) * A41;
-// w(o, class) gives the weights of the cell at offset o along the operator's
-// axis, cl the classes at offsets -2..2
-template <class F>
-__device__ __forceinline__ float tfwd(const F &w, const int *cl) {
-    return w(-1, cl[1]).w40 - w(0, cl[2]).w40 - w(-2, cl[0]).w41 + w(1, cl[3]).w41;
-}
-// transpose of a backward difference (f[e] - f[e-P]) * A40 - (f[e+P] - f[e-2P]) * A41
-template <class F>
-__device__ __forceinline__ float tbwd(const F &w, const int *cl) {
-    return w(0, cl[2]).w40 - w(1, cl[3]).w40 - w(-1, cl[1]).w41 + w(2, cl[4]).w41;
-}
-
-// ---------------------------------------------------------------------------
-// transpose of the velocity update
+// transpose of the velocity update: weights
 // pairs p: 0 (Vx,Sxx,x) 1 (Vx,Sxy,y) 2 (Vx,Sxz,z) 3 (Vy,Sxy,x) 4 (Vy,Syy,y)
 //          5 (Vy,Syz,z) 6 (Vz,Sxz,x) 7 (Vz,Syz,y) 8 (Vz,Szz,z)
 // ---------------------------------------------------------------------------
-// The weights of pair p at a cell: with u = b dt lambda_V, e40 u and e41 u in
-// an interior cell; in an absorber cell (m_absorb_p.f90:126-228: V += b (g.x D
-// + g.y aux_old) dt, aux = g.z aux + g.w D dt) r20 lD with lD = u g.x + g.w dt
-// aux_old, and no 4th-order term.
-struct VelW {
-    const GatherArgs &a;
-    int p;                       // pair: component p / 3, axis p % 3
-    long long f, P;              // the gathering cell and the stride of the axis
-    int k, i, j;
-    __device__ __forceinline__ W2 operator()(int o, int cl) const {
-        if (cl == -1) return W2{0.0f, 0.0f};
-        const int c = p / 3, ax = p % 3;
-        const long long x = f + o * P;
-        const float u = a.b[c][x] * a.dt * a.lV[c][x];
-        if (cl >= 0) return interior_w(a, ax, cl, u);
-        const int kk = k + (ax == 2 ? o : 0), ii = i + (ax == 0 ? o : 0), jj = j + (ax == 1 ? o : 0);
-        const int2 pc = __ldg(&a.pmlcol[col_index(a.g, ii, jj)]);
-        const long long q = (long long)pc.y + (kk - pc.x);
-        const float4 gp = vel_profile(a, p, kk, ii, jj);
-        const float lD = u * gp.x + gp.w * a.dt * a.laS_old[p][q];
-        return W2{a.r20[ax] * lD, 0.0f};
-    }
-    // the pair's PML profile at cell (k, i, j): x edge (p 0), centre (3, 6);
-    // y centre (1, 7), edge (4); z centre (2, 5), edge (8)
-    __device__ __forceinline__ static float4 vel_profile(const GatherArgs &a, int p, int k, int i, int j) {
-        switch (p) {
-        case 0: return __ldg(&a.gxe[i - 1]);
-        case 3: case 6: return __ldg(&a.gxc[i - 1]);
-        case 4: return __ldg(&a.gye[j - 1]);
-        case 1: case 7: return __ldg(&a.gyc[j - 1]);
-        case 8: return __ldg(&a.gze[k - 1]);
-        default: return __ldg(&a.gzc[k - 1]);
-        }
+// Operands of one cell: lV(c) the adjoint velocity, b(c) the buoyancy,
+// S(f, dk, di, dj) the forward stress after the stress update (f: xx yy zz
+// yz xz xy).
+struct GAdjVelOps {
+    const AdjVelArgs &a;
+    long long e, PI, PJ;
+    __device__ __forceinline__ float lV(int c) const { return a.lV[c][e]; }
+    __device__ __forceinline__ float b(int c) const { return a.b[c][e]; }
+    __device__ __forceinline__ float S(int f, int dk, int di, int dj) const {
+        return a.S[f][e + dk + di * PI + dj * PJ];
     }
 };
 
-// The whole transposed velocity update in one pass: lambda_S += D_S^T
-// weights (dst = lS: xx yy zz yz xz xy) with every weight formed on the fly,
-// the cell's own PML auxiliaries advanced (absorber cells), the gradient of
-// the buoyancies accumulated (interior cells).
-template <bool GRAD>
-__global__ void __launch_bounds__(128) adj_vel_kernel(const GatherArgs a) {
+struct Gb3 {
+    double v[3];
+};
+__device__ __forceinline__ Gb3 gb_load(const AdjVelArgs &a, long long e) {
+    Gb3 g;
+#pragma unroll
+    for (int q = 0; q < 3; q++) g.v[q] = a.gb[q][e];
+    return g;
+}
+
+// interior (s >= 0: band sign) or absorber (s < 0) cell
+template <class O>
+__device__ __forceinline__ void adj_vel_cell(const AdjVelArgs &a, const O &o, long long col, int k, int i, int j,
+                                             long long e, int s, const Gb3 &g0) {
+    const float dt = a.dt;
+    const float l[3] = {o.lV(0), o.lV(1), o.lV(2)};
+    const float u[3] = {o.b(0) * dt * l[0], o.b(1) * dt * l[1], o.b(2) * dt * l[2]};
+    if (s >= 0) {
+#pragma unroll
+        for (int p = 0; p < 9; p++) {
+            const int c = p / 3, ax = p % 3;
+            a.w40[p][e] = a.e40[ax][s] * u[c];
+            a.w41[p][e] = a.e41[ax][s] * u[c];
+        }
+        if (a.gb[0]) {
+            // d(Vx)/d(bx) = d3Sx3 * dt on the forward S after the stress update
+            const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
+            const float re40z = a.e40[2][s], re41z = a.e41[2][s];
+            const float d3Sx3 = (o.S(0, 0, 1, 0) - o.S(0, 0, 0, 0)) * re40x - (o.S(0, 0, 2, 0) - o.S(0, 0, -1, 0)) * re41x
+                              + (o.S(5, 0, 0, 0) - o.S(5, 0, 0, -1)) * re40y - (o.S(5, 0, 0, 1) - o.S(5, 0, 0, -2)) * re41y
+                              + (o.S(4, 0, 0, 0) - o.S(4, -1, 0, 0)) * re40z - (o.S(4, 1, 0, 0) - o.S(4, -2, 0, 0)) * re41z;
+            const float d3Sy3 = (o.S(5, 0, 0, 0) - o.S(5, 0, -1, 0)) * re40x - (o.S(5, 0, 1, 0) - o.S(5, 0, -2, 0)) * re41x
+                              + (o.S(1, 0, 0, 1) - o.S(1, 0, 0, 0)) * re40y - (o.S(1, 0, 0, 2) - o.S(1, 0, 0, -1)) * re41y
+                              + (o.S(3, 0, 0, 0) - o.S(3, -1, 0, 0)) * re40z - (o.S(3, 1, 0, 0) - o.S(3, -2, 0, 0)) * re41z;
+            const float d3Sz3 = (o.S(4, 0, 0, 0) - o.S(4, 0, -1, 0)) * re40x - (o.S(4, 0, 1, 0) - o.S(4, 0, -2, 0)) * re41x
+                              + (o.S(3, 0, 0, 0) - o.S(3, 0, 0, -1)) * re40y - (o.S(3, 0, 0, 1) - o.S(3, 0, 0, -2)) * re41y
+                              + (o.S(2, 1, 0, 0) - o.S(2, 0, 0, 0)) * re40z - (o.S(2, 2, 0, 0) - o.S(2, -1, 0, 0)) * re41z;
+            a.gb[0][e] = g0.v[0] + (double)l[0] * d3Sx3 * dt;
+            a.gb[1][e] = g0.v[1] + (double)l[1] * d3Sy3 * dt;
+            a.gb[2][e] = g0.v[2] + (double)l[2] * d3Sz3 * dt;
+        }
+        return;
+    }
+    // absorber cell: V += b * (g.x * D + g.y * aux_old) * dt, aux = g.z * aux + g.w * D * dt
+    const int2 pc = __ldg(&a.pmlcol[col]);
+    const long long q = (long long)pc.y + (k - pc.x);
+    const float4 gp[9] = {__ldg(&a.gxe[i - 1]), __ldg(&a.gyc[j - 1]), __ldg(&a.gzc[k - 1]),
+                          __ldg(&a.gxc[i - 1]), __ldg(&a.gye[j - 1]), __ldg(&a.gzc[k - 1]),
+                          __ldg(&a.gxc[i - 1]), __ldg(&a.gyc[j - 1]), __ldg(&a.gze[k - 1])};
+#pragma unroll
+    for (int p = 0; p < 9; p++) {
+        const int c = p / 3, ax = p % 3;
+        const float la = a.laS[p][q];
+        const float lD = u[c] * gp[p].x + gp[p].w * dt * la;
+        a.laS[p][q] = gp[p].z * la + u[c] * gp[p].y;
+        a.w40[p][e] = a.r20[ax] * lD;
+        a.w41[p][e] = 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const GAdjVelOps o{a, e, (long long)g.Kp, (long long)g.Kp * g.Ip};
+    const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
+    const int s = interior ? band_sign(__ldg(&a.band[col]), k) : -1;
+    const Gb3 g0 = (interior && a.gb[0]) ? gb_load(a, e) : Gb3{};
+    adj_vel_cell(a, o, col, k, i, j, e, s, g0);
+}
+
+// transpose of a forward difference (f[e+P] - f[e]) * A40 - (f[e+2P] - f[e-P]) * A41
+__device__ __forceinline__ float tfwd(const float *w40, const float *w41, long long f, long long P) {
+    return w40[f - P] - w40[f] - w41[f - 2 * P] + w41[f + P];
+}
+// transpose of a backward difference (f[e] - f[e-P]) * A40 - (f[e+P] - f[e-2P]) * A41
+__device__ __forceinline__ float tbwd(const float *w40, const float *w41, long long f, long long P) {
+    return w40[f] - w40[f + P] - w41[f - P] + w41[f + 2 * P];
+}
+
+// lambda_S += D_S^T weights (dst = lS: xx yy zz yz xz xy)
+__global__ void __launch_bounds__(128) adj_vel_gather_kernel(const GatherArgs a) {
     const Geo g = a.g;
     int k, i, j;
     if (!cell_of(g, k, i, j)) return;
     const long long f = cell_index(g, k, i, j);
     const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
-    const Classes C = classes_of(a, k, i, j);
-    const int *cx = C.c[0], *cy = C.c[1], *cz = C.c[2];
-    auto w = [&](int p, long long P) { return VelW{a, p, f, P, k, i, j}; };
-    a.dst[0][f] += tfwd(w(0, PI), cx);
-    a.dst[1][f] += tfwd(w(4, PJ), cy);
-    a.dst[2][f] += tfwd(w(8, 1), cz);
-    a.dst[3][f] += tbwd(w(5, 1), cz) + tbwd(w(7, PJ), cy);
-    a.dst[4][f] += tbwd(w(2, 1), cz) + tbwd(w(6, PI), cx);
-    a.dst[5][f] += tbwd(w(1, PJ), cy) + tbwd(w(3, PI), cx);
-    const int s = cz[2];
-    const float dt = a.dt;
-    if (s == -2) {
-        // the cell's own auxiliaries: aux' = g.z aux + u g.y
-        const int2 pc = __ldg(&a.pmlcol[col_index(g, i, j)]);
-        const long long q = (long long)pc.y + (k - pc.x);
-#pragma unroll
-        for (int p = 0; p < 9; p++) {
-            const int c = p / 3;
-            const float u = a.b[c][f] * dt * a.lV[c][f];
-            const float4 gp = VelW::vel_profile(a, p, k, i, j);
-            a.laS_new[p][q] = gp.z * a.laS_old[p][q] + u * gp.y;
-        }
-        return;
-    }
-    if (!GRAD || s < 0) return;
-    // d(Vx)/d(bx) = d3Sx3 * dt on the forward S after the stress update
-    auto S = [&](int fld, int dk, int di, int dj) { return a.S[fld][f + dk + di * PI + dj * PJ]; };
-    const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
-    const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-    const float d3Sx3 = (S(0, 0, 1, 0) - S(0, 0, 0, 0)) * re40x - (S(0, 0, 2, 0) - S(0, 0, -1, 0)) * re41x
-                      + (S(5, 0, 0, 0) - S(5, 0, 0, -1)) * re40y - (S(5, 0, 0, 1) - S(5, 0, 0, -2)) * re41y
-                      + (S(4, 0, 0, 0) - S(4, -1, 0, 0)) * re40z - (S(4, 1, 0, 0) - S(4, -2, 0, 0)) * re41z;
-    const float d3Sy3 = (S(5, 0, 0, 0) - S(5, 0, -1, 0)) * re40x - (S(5, 0, 1, 0) - S(5, 0, -2, 0)) * re41x
-                      + (S(1, 0, 0, 1) - S(1, 0, 0, 0)) * re40y - (S(1, 0, 0, 2) - S(1, 0, 0, -1)) * re41y
-                      + (S(3, 0, 0, 0) - S(3, -1, 0, 0)) * re40z - (S(3, 1, 0, 0) - S(3, -2, 0, 0)) * re41z;
-    const float d3Sz3 = (S(4, 0, 0, 0) - S(4, 0, -1, 0)) * re40x - (S(4, 0, 1, 0) - S(4, 0, -2, 0)) * re41x
-                      + (S(3, 0, 0, 0) - S(3, 0, 0, -1)) * re40y - (S(3, 0, 0, 1) - S(3, 0, 0, -2)) * re41y
-                      + (S(2, 1, 0, 0) - S(2, 0, 0, 0)) * re40z - (S(2, 2, 0, 0) - S(2, -1, 0, 0)) * re41z;
-    a.gb[0][f] = a.gb[0][f] + (double)a.lV[0][f] * d3Sx3 * dt;
-    a.gb[1][f] = a.gb[1][f] + (double)a.lV[1][f] * d3Sy3 * dt;
-    a.gb[2][f] = a.gb[2][f] + (double)a.lV[2][f] * d3Sz3 * dt;
+    a.dst[0][f] += tfwd(a.w40[0], a.w41[0], f, PI);
+    a.dst[1][f] += tfwd(a.w40[4], a.w41[4], f, PJ);
+    a.dst[2][f] += tfwd(a.w40[8], a.w41[8], f, 1);
+    a.dst[3][f] += tbwd(a.w40[5], a.w41[5], f, 1) + tbwd(a.w40[7], a.w41[7], f, PJ);
+    a.dst[4][f] += tbwd(a.w40[2], a.w41[2], f, 1) + tbwd(a.w40[6], a.w41[6], f, PI);
+    a.dst[5][f] += tbwd(a.w40[1], a.w41[1], f, PJ) + tbwd(a.w40[3], a.w41[3], f, PI);
 }
 
 // ---------------------------------------------------------------------------
@@ -348,18 +308,20 @@ __device__ __forceinline__ void adj_stress_interior(const AdjStrArgs &a, const O
         ld3 = ld3 + lam2mu * taup_plus1 * al[c] + lam2mu * taup1 * lF[c];
         lX[c] = -(mu2 * taus_plus1 * al[c] + mu2 * taus1 * lF[c]);
     }
-    // the six distinct operator inputs, in the slots of the pairs q = 0 1 2 3 5 7
-    // (pairs 4, 6 and 8 read the slot before them)
-    float ld[6];
+    float ld[9];
     ld[0] = ld3 + lX[1] + lX[2];   // dxVx appears in X_yy and X_zz
     ld[1] = ld3 + lX[0] + lX[2];
     ld[2] = ld3 + lX[0] + lX[1];
     // shear: G = mu_c taus+ D, F = mu_c taus D (c = yz xz xy)
-    ld[5] = muc[0] * taus_plus1 * al[3] + muc[0] * taus1 * lF[3];
-    ld[4] = muc[1] * taus_plus1 * al[4] + muc[1] * taus1 * lF[4];
-    ld[3] = muc[2] * taus_plus1 * al[5] + muc[2] * taus1 * lF[5];
+    const float lyz = muc[0] * taus_plus1 * al[3] + muc[0] * taus1 * lF[3];
+    const float lxz = muc[1] * taus_plus1 * al[4] + muc[1] * taus1 * lF[4];
+    const float lxy = muc[2] * taus_plus1 * al[5] + muc[2] * taus1 * lF[5];
+    ld[3] = lxy; ld[4] = lxy; ld[5] = lxz; ld[6] = lxz; ld[7] = lyz; ld[8] = lyz;
 #pragma unroll
-    for (int n = 0; n < 6; n++) a.W[n < 3 ? n : 2 * n - 3][e] = ld[n];
+    for (int q = 0; q < 9; q++) {
+        a.w40[q][e] = a.e40[qaxis(q)][s] * ld[q];
+        a.w41[q][e] = a.e41[qaxis(q)][s] * ld[q];
+    }
     if (a.gm[0]) {
         // forward strain rates on V before the stress update
         const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
@@ -439,7 +401,10 @@ __device__ __forceinline__ void adj_stress_absorber(const AdjStrArgs &a, const O
         }
     }
 #pragma unroll
-    for (int qq = 0; qq < 9; qq++) a.W[qq][e] = a.r20[qaxis(qq)] * ld[qq];
+    for (int qq = 0; qq < 9; qq++) {
+        a.w40[qq][e] = a.r20[qaxis(qq)] * ld[qq];
+        a.w41[qq][e] = 0.0f;
+    }
 }
 
 template <int NM>
@@ -528,21 +493,6 @@ __global__ void __launch_bounds__(adjt::NT, (tma::blocks_per_sm<adjt::Boxes<NM>:
     else adj_stress_absorber(a, o, col, k, i, j, e);
 }
 
-// weights of pair q at cell x: stored in absorber cells, e40 / e41 times the
-// stored ld in interior cells
-struct StrW {
-    const GatherArgs &a;
-    int q;
-    long long f, P;              // the gathering cell and the stride of the pair's axis
-    __device__ __forceinline__ W2 operator()(int o, int cl) const {
-        if (cl == -1) return W2{0.0f, 0.0f};
-        const long long x = f + o * P;
-        if (cl == -2) return W2{a.W[q][x], 0.0f};
-        const int slot = (q == 4 || q == 6 || q == 8) ? q - 1 : q;
-        return interior_w(a, qaxis(q), cl, a.W[slot][x]);
-    }
-};
-
 // lambda_V += D_V^T weights (dst = lV: x y z)
 __global__ void __launch_bounds__(128) adj_stress_gather_kernel(const GatherArgs a) {
     const Geo g = a.g;
@@ -550,12 +500,9 @@ __global__ void __launch_bounds__(128) adj_stress_gather_kernel(const GatherArgs
     if (!cell_of(g, k, i, j)) return;
     const long long f = cell_index(g, k, i, j);
     const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
-    const Classes C = classes_of(a, k, i, j);
-    const int *cx = C.c[0], *cy = C.c[1], *cz = C.c[2];
-    auto w = [&](int q, long long P) { return StrW{a, q, f, P}; };
-    a.dst[0][f] += tbwd(w(0, PI), cx) + tfwd(w(4, PJ), cy) + tfwd(w(6, 1), cz);
-    a.dst[1][f] += tbwd(w(1, PJ), cy) + tfwd(w(3, PI), cx) + tfwd(w(8, 1), cz);
-    a.dst[2][f] += tbwd(w(2, 1), cz) + tfwd(w(5, PI), cx) + tfwd(w(7, PJ), cy);
+    a.dst[0][f] += tbwd(a.w40[0], a.w41[0], f, PI) + tfwd(a.w40[4], a.w41[4], f, PJ) + tfwd(a.w40[6], a.w41[6], f, 1);
+    a.dst[1][f] += tbwd(a.w40[1], a.w41[1], f, PJ) + tfwd(a.w40[3], a.w41[3], f, PI) + tfwd(a.w40[8], a.w41[8], f, 1);
+    a.dst[2][f] += tbwd(a.w40[2], a.w41[2], f, 1) + tfwd(a.w40[5], a.w41[5], f, PI) + tfwd(a.w40[7], a.w41[7], f, PJ);
 }
 
 // transpose of the velocity recorder (m_wav.f90:530-535): residuals as sources
@@ -690,9 +637,11 @@ static int adj_alloc(swpc_ctx *c) {
         return set_err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint slab");
     if (c->npml > 0)
         for (int q = 0; q < 18; q++) { int rc = dalloc(c, &s->laux[q], c->npml); if (rc) return rc; }
-    if (c->npml > 0)
-        for (int q = 0; q < 9; q++) { int rc = dalloc(c, &s->laux_alt[q], c->npml); if (rc) return rc; }
-    for (int q = 0; q < 9; q++) { int rc = dalloc(c, &s->W[q], n); if (rc) return rc; }
+    for (int q = 0; q < 9; q++) {
+        int rc = dalloc(c, &s->w40[q], n);
+        if (!rc) rc = dalloc(c, &s->w41[q], n);
+        if (rc) return rc;
+    }
     for (int q = 0; q < 8; q++) { int rc = dalloc(c, &s->grad[q], n); if (rc) return rc; }
     return SWPC_OK;
 }
@@ -704,8 +653,8 @@ void adj_free(swpc_ctx *c) {
     if (s->slab) cudaFree(s->slab);   // lV, lS, lR
     delete s->maps;
     for (auto p : s->laux) if (p) cudaFree(p);
-    for (auto p : s->laux_alt) if (p) cudaFree(p);
-    for (auto p : s->W) if (p) cudaFree(p);
+    for (auto p : s->w40) if (p) cudaFree(p);
+    for (auto p : s->w41) if (p) cudaFree(p);
     for (auto p : s->grad) if (p) cudaFree(p);
     if (s->res) cudaFree(s->res);
     if (s->ckpool) cudaFree(s->ckpool);
@@ -762,30 +711,31 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
     const dim3 block(kThreadsK, 2, 2);
     const dim3 grid = cell_grid(c->g, block);
     const bool grad = S_after != nullptr;
-    GatherArgs ga;
-    memset(&ga, 0, sizeof(ga));
-    ga.g = c->g; ga.ibk = c->ibk; ga.iek = c->iek; ga.jbk = c->jbk; ga.jek = c->jek; ga.kek = c->kek;
-    ga.band = c->band;
-    memcpy(ga.e40, c->e40, sizeof(ga.e40)); memcpy(ga.e41, c->e41, sizeof(ga.e41));
-    ga.dt = c->d.dt;
-    for (int q = 0; q < 9; q++) ga.W[q] = s->W[q];
     {
-        for (int q = 0; q < 6; q++) ga.dst[q] = s->lS[q];
-        for (int q = 0; q < 3; q++) { ga.lV[q] = s->lV[q]; ga.b[q] = c->med[5 + q]; }
-        ga.pmlcol = c->pmlcol;
-        ga.gxc = c->gx[0]; ga.gxe = c->gx[1]; ga.gyc = c->gy[0]; ga.gye = c->gy[1]; ga.gzc = c->gz[0]; ga.gze = c->gz[1];
-        for (int q = 0; q < 9; q++) { ga.laS_old[q] = s->laux[9 + q]; ga.laS_new[q] = s->laux_alt[q]; }
-        memcpy(ga.r20, c->r20, sizeof(ga.r20));
+        AdjVelArgs a;
+        memset(&a, 0, sizeof(a));
+        a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
+        for (int q = 0; q < 3; q++) { a.lV[q] = s->lV[q]; a.b[q] = c->med[5 + q]; }
+        a.band = c->band; a.pmlcol = c->pmlcol;
+        for (int q = 0; q < 9; q++) a.laS[q] = s->laux[9 + q];
+        a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+        memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+        a.dt = c->d.dt;
+        for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
-            for (int q = 0; q < 6; q++) ga.S[q] = S_after[q];
-            for (int q = 0; q < 3; q++) ga.gb[q] = s->grad[5 + q];
-            adj_vel_kernel<true><<<grid, block, 0, c->stream>>>(ga);
-        } else {
-            adj_vel_kernel<false><<<grid, block, 0, c->stream>>>(ga);
+            for (int q = 0; q < 6; q++) a.S[q] = S_after[q];
+            for (int q = 0; q < 3; q++) a.gb[q] = s->grad[5 + q];
         }
+        // one cell per thread: the kernel is bound by its 18 weight stores, and
+        // staging its few loads (a TMA-staged form was tried) made it slower
+        adj_vel_weights_kernel<<<grid, block, 0, c->stream>>>(a);
         ACK(cudaGetLastError());
-        // the advanced auxiliaries become the current ones
-        for (int q = 0; q < 9; q++) std::swap(s->laux[9 + q], s->laux_alt[q]);
+        GatherArgs ga;
+        ga.g = c->g;
+        for (int q = 0; q < 6; q++) ga.dst[q] = s->lS[q];
+        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
+        adj_vel_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
+        ACK(cudaGetLastError());
     }
     {
         AdjStrArgs a;
@@ -802,7 +752,7 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
         a.dt = c->d.dt;
         memcpy(a.c1, c->c1, sizeof(a.c1)); memcpy(a.c2, c->c2, sizeof(a.c2)); memcpy(a.d1, c->d1, sizeof(a.d1));
         a.d2 = c->d2;
-        for (int q = 0; q < 9; q++) a.W[q] = s->W[q];
+        for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
             for (int q = 0; q < 3; q++) a.V[q] = V_before[q];
             for (int q = 0; q < 5; q++) a.gm[q] = s->grad[q];
@@ -825,8 +775,11 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
             }
             ACK(cudaGetLastError());
         }
+        GatherArgs ga;
+        ga.g = c->g;
         for (int q = 0; q < 3; q++) ga.dst[q] = s->lV[q];
         for (int q = 3; q < 6; q++) ga.dst[q] = nullptr;
+        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
         adj_stress_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
         ACK(cudaGetLastError());
     }
@@ -853,7 +806,6 @@ static int zero_adjoint(swpc_ctx *c) {
     for (auto p : s->lS) if (p) ACK(cudaMemsetAsync(p, 0, n, c->stream));
     for (auto p : s->lR) if (p) ACK(cudaMemsetAsync(p, 0, n, c->stream));
     for (auto p : s->laux) if (p) ACK(cudaMemsetAsync(p, 0, sizeof(float) * c->npml, c->stream));
-    for (auto p : s->laux_alt) if (p) ACK(cudaMemsetAsync(p, 0, sizeof(float) * c->npml, c->stream));
     for (auto p : s->grad) {
         zero_double_kernel<<<148 * 4, 256, 0, c->stream>>>(p, c->g.ncell);
         ACK(cudaGetLastError());
