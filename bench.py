@@ -389,6 +389,29 @@ def bench_c2b(args, world, rank, local):
         ms_batch = fb.time_steps(it0, args.steps)
     it0 += args.steps
     ms_batch = max_over_ranks(ms_batch)
+    sweep = None
+    if args.sweep:
+        # launch order x j block x member groups per CTA, 3 timed steps each (profiling runs); then the tuned form again
+        tuned = fb.launch()
+        sweep = []
+        for tiles_first in (1, 0):
+            for jb in (1, 2, 4, 16):
+                for bi, bj, mpc in ((4, 4, 1), (4, 2, 2), (2, 2, 2), (2, 2, 4), (4, 1, 4)):
+                    if it0 + 4 > p.nt:
+                        break
+                    _lib.check(base.ctx, lib.swpc_set_launch(base.ctx, 7, 1, jb, 1))
+                    fb.set_launch(5, mpc, bi, bj)
+                    fb.set_launch(6, mpc, bi, bj)
+                    fb.set_launch(7, tiles_first, 0, 0)
+                    fb.run(it0, 1)
+                    t = fb.time_steps(it0 + 1, 3) / 3
+                    it0 += 4
+                    sweep.append({"tiles_first": tiles_first, "jblock": jb, "tile": [bi, bj], "members_per_cta": mpc,
+                                  "ms_per_step": t, "loop_over_batch": ms_loop / args.steps / t})
+        _lib.check(base.ctx, lib.swpc_set_launch(base.ctx, 7, 1, 0, 1))
+        fb.set_launch(5, tuned["stress"][2], tuned["stress"][0], tuned["stress"][1])
+        fb.set_launch(6, tuned["velocity"][2], tuned["velocity"][0], tuned["velocity"][1])
+        fb.set_launch(7, int(tuned["tiles_first"]), 0, 0)
     n_int, n_pml = cell_counts(p)
     # algorithmic bytes: per member the 3D step without its medium reads (292 - 40 interior, 284 - 32 PML),
     # plus the medium once per step for all members
@@ -438,6 +461,8 @@ def bench_c2b(args, world, rank, local):
                     "what": "shared medium from pinned host memory (5 arrays; the 6 averaged ones formed on the "
                             "device) + per-step batch calls + every member's traces downloaded, wall clock"},
             "gpu_launches": args.steps * 5, "clocks": clk.summary()}
+    if sweep is not None:
+        line["launch_sweep"] = sweep
     fb.close()
     base.close()
     ranks.close()
@@ -792,6 +817,8 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3"])
     ap.add_argument("--models", type=int, default=64, help="c2a: the first N of the 64 models (profiling runs)")
     ap.add_argument("--only-model", type=int, default=None, help="c2a: model I of the 64 alone (profiling runs)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="c2b: also time every launch order x j block x members-per-CTA form (profiling runs)")
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
     ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (c3 profiling runs)")

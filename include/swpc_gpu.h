@@ -536,13 +536,14 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
 /* Memory-variable and PML-auxiliary fields are defined only on their
  * regions; outside them download writes 0 and upload ignores the input. */
 
-/* SWPC_PREC_F16_SR only (a no-op otherwise): re-centre the power-of-two
- * scale of every FP16 stress and memory-variable array so that its largest
- * stored magnitude lies in [2^10, 2^11) whenever it has left [2^6, 2^12);
- * that leaves 32x headroom below the FP16 overflow for growth until the next
- * call.  Scaling by a power of two is exact.  Call it between steps, e.g.
- * with every progress report; *changed (may be NULL) = arrays rescaled.
- * Blocks.  No counterpart in the reference. */
+/* SWPC_PREC_F16_SR and SWPC_PREC_F16_R (a no-op otherwise): re-centre the
+ * power-of-two scale of every FP16 stress and memory-variable array so that
+ * its largest stored magnitude lies in [2^7, 2^8) whenever it has left
+ * [2^3, 2^10); that leaves at least 64x headroom below the FP16 overflow.
+ * Scaling by a power of two is exact.  swpc_run, swpc_step and
+ * swpc_step_half call it themselves before every step whose index is a
+ * multiple of 8, so a caller need not; *changed (may be NULL) = arrays
+ * rescaled.  Blocks.  No counterpart in the reference. */
 int swpc_rescale(swpc_ctx *ctx, int *changed);
 
 /* Device bytes held by the context. */

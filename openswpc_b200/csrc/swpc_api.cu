@@ -96,8 +96,11 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     if (d->nx < 4 || d->nz < 4 || (d->kind == SWPC_KIND_3D && d->ny < 4))
         return fail(set_err(c, SWPC_ERR_ARG, "grid must be at least 4 cells per dimension"));
     if (d->nm < 0 || d->nm > NM_MAX) return fail(set_err(c, SWPC_ERR_ARG, "nm must be 0..3"));
-    if (d->na < 0 || 2 * d->na >= d->nx || d->na >= d->nz || (d->kind == SWPC_KIND_3D && 2 * d->na >= d->ny))
-        return fail(set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid"));
+    if (d->na < 0 || d->na >= d->nz) return fail(set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid"));
+    // across x and y the absorber is checked against the whole grid: this
+    // one, or the global one of swpc_set_subdomain (a block may be narrower
+    // than two absorbers)
+    c->na_wide = 2 * d->na >= d->nx || (d->kind == SWPC_KIND_3D && 2 * d->na >= d->ny);
     if (d->nt < 1) return fail(set_err(c, SWPC_ERR_ARG, "nt must be positive"));
     if (d->precision < SWPC_PREC_F32 || d->precision > SWPC_PREC_F16_R ||
         (d->kind != SWPC_KIND_3D && d->precision != SWPC_PREC_F32))
@@ -482,6 +485,7 @@ int average_medium(swpc_ctx *c) {
 // ---------------------------------------------------------------------------
 extern "C" int swpc_upload_medium(swpc_ctx *c, const swpc_medium_view *m) {
     if (!c || !m) return SWPC_ERR_ARG;
+    RC(check_na_wide(c));
     CK(cudaSetDevice(c->device));
     invalidate_graph(c);
     if (!is3d(c)) return upload_medium_2d(c, m);
@@ -1006,6 +1010,7 @@ extern "C" int swpc_wav_fetch(swpc_ctx *c, int what, float *out) {
 // the time step
 // ---------------------------------------------------------------------------
 static int check_ready(swpc_ctx *c) {
+    RC(check_na_wide(c));
     if (!c->medium_ready) return set_err(c, SWPC_ERR_STATE, "swpc_upload_medium not called");
     if (!c->kernel_ready) return set_err(c, SWPC_ERR_STATE, "swpc_kernel_setup not called");
     if (!c->absorb_ready && c->d.na > 0) return set_err(c, SWPC_ERR_STATE, "swpc_absorb_setup not called");
@@ -1299,12 +1304,15 @@ static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
     return SWPC_OK;
 }
 
+static int rescale_before(swpc_ctx *c, int it);
+
 extern "C" int swpc_step_half(swpc_ctx *c, int it, int half) {
     if (!c) return SWPC_ERR_ARG;
     if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
     if (half != 0 && half != 1) return set_err(c, SWPC_ERR_ARG, "half must be 0 (stress) or 1 (velocity)");
     if (c->pw_mode) return set_err(c, SWPC_ERR_STATE, "the plane-wave mode steps whole steps (swpc_step)");
     PREP(c);
+    if (half == 0) RC(rescale_before(c, it));
     return half == 0 ? step_half0(c, it, nullptr, true) : step_half1(c, it, nullptr);
 }
 
@@ -1312,6 +1320,7 @@ extern "C" int swpc_step(swpc_ctx *c, int it) {
     if (!c) return SWPC_ERR_ARG;
     if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
     PREP(c);
+    RC(rescale_before(c, it));
     return step_body(c, it, nullptr);
 }
 
@@ -1341,6 +1350,16 @@ static int build_graph(swpc_ctx *c) {
     return SWPC_OK;
 }
 
+// FP16 storage forms: re-centre the arrays' power-of-two scales before every
+// step whose index is a multiple of this (the same steps whatever way the
+// caller splits the loop into calls)
+constexpr int kRescaleEvery = 8;
+static bool fp16_form(const swpc_ctx *c) { return c->prec == SWPC_PREC_F16_SR || c->prec == SWPC_PREC_F16_R; }
+static int rescale_before(swpc_ctx *c, int it) {
+    if (!fp16_form(c) || it % kRescaleEvery != 0) return SWPC_OK;
+    return swpc_rescale(c, nullptr);
+}
+
 extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
     if (!c) return SWPC_ERR_ARG;
     if (nsteps <= 0) return SWPC_OK;
@@ -1348,7 +1367,13 @@ extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
     CK(cudaSetDevice(c->device));
     RC(build_graph(c));
     CK(cudaMemcpyAsync(c->d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    for (int n = 0; n < nsteps; n++) CK(cudaGraphLaunch(c->graph_exec, c->stream));
+    for (int n = 0; n < nsteps; n++) {
+        if (fp16_form(c) && (it0 + n) % kRescaleEvery == 0) {
+            RC(rescale_before(c, it0 + n));
+            RC(build_graph(c));   // a changed scale is a kernel argument: the graph is rebuilt
+        }
+        CK(cudaGraphLaunch(c->graph_exec, c->stream));
+    }
     return SWPC_OK;
 }
 

@@ -76,6 +76,7 @@ struct swpc_ctx {
     // extents and this box's offsets (nxg = nx, ioff = 0 on a single domain)
     int nxg = 0, nyg = 0, ioff = 0, joff = 0;
     bool sub = false;
+    bool na_wide = false;   // 2 na >= nx or ny of a single domain: refused at the medium upload
 
     // full-grid fields
     float *V[3] = {nullptr, nullptr, nullptr};          // Vx Vy Vz (2D: Vx Vz / Vy)
@@ -206,6 +207,11 @@ struct swpc_ctx {
 // helpers shared by the translation units
 namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
+// 2 na must fit the grid across x and y (the whole grid for a block of a
+// decomposed one); refused when the medium arrives
+inline int check_na_wide(swpc_ctx *c) {
+    return c->na_wide ? set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid") : SWPC_OK;
+}
 int snap_launch(swpc_ctx *c, int it, const int *d_it);   // swpc_snap.cu
 void snap_free(swpc_ctx *c);
 int snap_clear(swpc_ctx *c);   // frames, displacement accumulators and maxima back to zero

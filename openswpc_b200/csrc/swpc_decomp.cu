@@ -192,6 +192,7 @@ extern "C" int swpc_set_subdomain(swpc_ctx *c, int nx_global, int ny_global, int
     c->ioff = ioff;
     c->joff = joff;
     c->sub = true;
+    c->na_wide = false;   // checked against the global grid above
     return SWPC_OK;
 }
 

@@ -81,9 +81,13 @@ __global__ void green_store_kernel(const GreenArgs a) {
     const float d[9] = {dxVx, dxVy, dxVz, dyVx, dyVy, dyVz, dzVx, dzVy, dzVz};
     float u[12];
     const int ng = a.ng;
+    // the totals start from zero at it == 1, where the reference allocates
+    // them (m_green.f90:409-425): a rerun from step 1 of a context or a
+    // batch does not carry the previous run's totals
+    const bool first = it == 1;
 #pragma unroll
     for (int q = 0; q < 9; q++) {
-        u[q] = __fadd_rn(acc[q * ng + n], __fmul_rn(d[q], a.dt));
+        u[q] = __fadd_rn(first ? 0.0f : acc[q * ng + n], __fmul_rn(d[q], a.dt));
         acc[q * ng + n] = u[q];
     }
     if (a.ncmp == 9) {
@@ -91,7 +95,7 @@ __global__ void green_store_kernel(const GreenArgs a) {
         const float v3[3] = {__fadd_rn(Vx[e], Vx[e - PI]), __fadd_rn(Vy[e], Vy[e - PJ]), __fadd_rn(Vz[e], Vz[e - PK])};
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            u[9 + q] = __fadd_rn(acc[(9 + q) * ng + n], __fmul_rn(__fmul_rn(0.5f, v3[q]), a.dt));
+            u[9 + q] = __fadd_rn(first ? 0.0f : acc[(9 + q) * ng + n], __fmul_rn(__fmul_rn(0.5f, v3[q]), a.dt));
             acc[(9 + q) * ng + n] = u[9 + q];
         }
     }

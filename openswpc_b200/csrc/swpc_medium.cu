@@ -334,6 +334,7 @@ extern "C" int swpc_vmodel_lhm_device_opt(swpc_ctx *c, int nlayer, const float *
                                           int munk_profile) {
     if (!c) return SWPC_ERR_ARG;
     if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the device medium setup is for the 3D code");
+    RC(check_na_wide(c));
     if (nlayer < 1 || !depth || !rho0 || !vp0 || !vs0 || !qp0 || !qs0)
         return set_err(c, SWPC_ERR_ARG, "layer table missing");
     CK(cudaSetDevice(c->device));
@@ -384,6 +385,7 @@ extern "C" int swpc_vmodel_upload(swpc_ctx *c, const float *rho, const float *la
                                   const float *qs, int ld_k, int ld_i) {
     if (!c) return SWPC_ERR_ARG;
     if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the device medium setup is for the 3D code");
+    RC(check_na_wide(c));
     if (!rho || !lam || !mu || !qp || !qs) return set_err(c, SWPC_ERR_ARG, "model array missing");
     CK(cudaSetDevice(c->device));
     drop_graph(c);

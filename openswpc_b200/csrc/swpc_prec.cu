@@ -9,10 +9,14 @@
 //   SWPC_PREC_F16_SR  : the 6 stresses S and the memory variables R in FP16,
 //                       each array with its own power-of-two scale s = 2^e:
 //                       value = stored * s.  swpc_rescale moves e so that
-//                       every array's largest magnitude sits near 2^10 in
+//                       every array's largest magnitude sits near 2^7 in
 //                       storage, far from the FP16 overflow at 65504 and from
 //                       its subnormal range; scaling by a power of two is
-//                       exact, so rescaling adds no rounding.
+//                       exact, so rescaling adds no rounding.  The time loop
+//                       (swpc_run, swpc_step, swpc_step_half) calls it before
+//                       every step whose index is a multiple of
+//                       kRescaleEvery, so growth between two calls stays far
+//                       below the headroom.
 // This file holds the conversion kernels used by the field transfers and the
 // rescaling pass.
 #include <cuda_bf16.h>
@@ -132,12 +136,14 @@ extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
         float m;
         memcpy(&m, &h[q], sizeof(float));
         if (!(m > 0.0f) || !std::isfinite(m)) continue;
-        // stored max in [2^6, 2^12) is kept; otherwise move it to [2^10, 2^11),
-        // which leaves 32x headroom below the FP16 overflow for growth
-        // between two calls
+        // stored max in [2^3, 2^10) is kept; otherwise move it to [2^7, 2^8),
+        // which leaves at least 64x (after a move 256x) headroom below the
+        // FP16 overflow for growth between two calls: a wave front can
+        // multiply an array's maximum by ~40 in 10 steps while the source
+        // starts up
         const int ex = std::ilogb(m);   // m = f * 2^ex, 1 <= f < 2
-        if (ex >= 6 && ex < 12) continue;
-        const int shift = ex - 10;      // stored /= 2^shift, e += shift
+        if (ex >= 3 && ex < 10) continue;
+        const int shift = ex - 7;       // stored /= 2^shift, e += shift
         rescale_half_kernel<<<kGrid, 256, 0, c->stream>>>(reinterpret_cast<__half *>(fields[q]), c->g.ncell,
                                                           std::ldexp(1.0f, -shift));
         rc = cuda_check(c, cudaGetLastError(), "rescale_half_kernel");

@@ -544,8 +544,6 @@ class Swpc3D:
         it = it0
         while it <= last:
             if it % p.ntdec_r == 0:
-                if self.precision in ("f16sr", "f16r"):
-                    self.rescale()   # keep the FP16 arrays' power-of-two scales centred
                 vm = self.kernel__vmax()
                 va = vm * f32(self.UC) * f32(self.M0)
                 reports.append((it, va))

@@ -56,24 +56,31 @@ def test_precision_form_error_against_f64(form, reference, record_property):
 
 
 def test_reduced_storage_roundtrip_and_rescale():
-    """Upload/download through FP16 storage rounds to FP16; rescaling by a
-    power of two keeps the stored values."""
+    """Upload/download through FP16 storage rounds to FP16; re-centring is
+    idempotent; a field pushed out of its window is re-centred with its values
+    kept; the run goes on as without the forced move."""
     p = small3d(nt=40)
     g = Swpc3D(p, precision="f16sr")
-    g.run(1, 30)
+    g.run(1, 30)   # the loop re-centres the scales every 8 steps; the wave still grows in between
+    g.rescale()
+    assert g.rescale() == 0   # a second call finds every array centred
     before = [g.download(_lib.F_SXX + c) for c in range(6)]
     r_before = g.download(_lib.F_R + 0)
-    n = g.rescale()
-    assert n > 0   # fresh arrays start at scale 1; the run moved them out of the window
+    # Sxx 16 times larger: its stored maximum leaves the window [2^3, 2^10)
+    assert np.abs(before[0]).max() > 0
+    g.upload(_lib.F_SXX, before[0] * np.float32(16.0))
+    d1 = g.download(_lib.F_SXX)
+    assert g.rescale() >= 1
+    d2 = g.download(_lib.F_SXX)
+    # exact unless a value fell into the FP16 subnormal range
+    assert np.abs(d1 - d2).max() <= np.abs(d1).max() * 2.0 ** -20
+    assert g.rescale() == 0   # centred
+    g.upload(_lib.F_SXX, before[0])   # the run's own values again (exact: a power-of-two change of scale)
     after = [g.download(_lib.F_SXX + c) for c in range(6)]
     for a, b in zip(before, after):
-        big = np.abs(a).max()
-        assert big > 0
-        # exact unless a value fell into the FP16 subnormal range
-        assert np.abs(a - b).max() <= big * 2.0 ** -20
+        assert np.abs(a - b).max() <= np.abs(a).max() * 2.0 ** -20
     assert np.abs(g.download(_lib.F_R + 0) - r_before).max() <= np.abs(r_before).max() * 2.0 ** -20
-    assert g.rescale() == 0   # now centred
-    # the run continues correctly after a rescale: same as without it
+    # the run continues correctly: same as a run without the uploads
     h = Swpc3D(p, precision="f16sr")
     h.run(1, 30)
     g.run(31, 10)
