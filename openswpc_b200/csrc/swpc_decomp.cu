@@ -28,6 +28,10 @@
 
 using namespace swpc;
 
+namespace swpc {
+int build_tiles_2d(swpc_ctx *c);   // swpc2d_api.cu
+}
+
 #define CK(call)                                               \
     do {                                                       \
         int _rc = cuda_check(c, (call), #call);                \
@@ -193,6 +197,9 @@ extern "C" int swpc_set_subdomain(swpc_ctx *c, int nx_global, int ny_global, int
     c->joff = joff;
     c->sub = true;
     c->na_wide = false;   // checked against the global grid above
+    c->desc_dirty = true;
+    // the 2D tile list flags interior and absorber tiles by the kernel region
+    if (!threed) RC(build_tiles_2d(c));
     return SWPC_OK;
 }
 
