@@ -81,7 +81,7 @@ struct GVelOps {
     __device__ __forceinline__ float v(int c) const { return lds(&V[c][e]); }
     __device__ __forceinline__ float b(int c) const { return lds(&(c == 0 ? a.bx : c == 1 ? a.by : a.bz)[e]); }
     __device__ __forceinline__ float s(int f, int dk, int di, int dj) const {
-        return ldgS<PREC>(S[f], e + dk + di * PI + dj * PJ, a.sS[f]);
+        return ldgS<PREC>(S[f], e + dk + di * PI + dj * PJ, sc_sS(a.scale, f));
     }
 };
 
@@ -131,8 +131,8 @@ struct GStrOps {
     __device__ __forceinline__ float v(int c, int dk, int di, int dj) const {
         return __ldg(&V[c][e + dk + di * PI + dj * PJ]);
     }
-    __device__ __forceinline__ float sown(int f) const { return ldS<PREC>(S[f], e, a.sS[f]); }
-    __device__ __forceinline__ float r(int q) const { return ldR<PREC>(a.R[q] + so, e, a.sR[q]); }
+    __device__ __forceinline__ float sown(int f) const { return ldS<PREC>(S[f], e, sc_sS(a.scale, f)); }
+    __device__ __forceinline__ float r(int q) const { return ldR<PREC>(a.R[q] + so, e, sc_sR(a.scale, q)); }
     // 0 mu, 1 lam, 2 taup, 3 taus, 4 muyz, 5 muxz, 6 muxy
     __device__ __forceinline__ float med(int m) const {
         const float *p = m == 0 ? a.mu : m == 1 ? a.lam : m == 2 ? a.taup : m == 3 ? a.taus
@@ -194,9 +194,9 @@ __device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o,
     }
     const float taup_plus1 = 1 + taup1 * (1 + a.d2);
     const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-    stS<PREC>(S[0], e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, a.iS[0]);
-    stS<PREC>(S[1], e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, a.iS[1]);
-    stS<PREC>(S[2], e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, a.iS[2]);
+    stS<PREC>(S[0], e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, sc_iS(a.scale, 0));
+    stS<PREC>(S[1], e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, sc_iS(a.scale, 1));
+    stS<PREC>(S[2], e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, sc_iS(a.scale, 2));
 
     // shear components (m_kernel.f90:282-311)
     const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
@@ -215,13 +215,13 @@ __device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o,
         Rxz_n = Rxz_n + a.d1[m] * r[4][m];
         Rxy_n = Rxy_n + a.d1[m] * r[5][m];
     }
-    stS<PREC>(S[3], e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, a.iS[3]);
-    stS<PREC>(S[4], e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, a.iS[4]);
-    stS<PREC>(S[5], e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, a.iS[5]);
+    stS<PREC>(S[3], e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, sc_iS(a.scale, 3));
+    stS<PREC>(S[4], e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, sc_iS(a.scale, 4));
+    stS<PREC>(S[5], e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, sc_iS(a.scale, 5));
 #pragma unroll
     for (int c = 0; c < 6; c++)
 #pragma unroll
-        for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], a.iR[c * 3 + m]);
+        for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], sc_iR(a.scale, c * 3 + m));
 }
 
 // absorb_p__update_vel (m_absorb_p.f90:248-309) for one absorber cell: the
@@ -342,9 +342,9 @@ __device__ __forceinline__ void stress_absorber(const Str3Args &a, const Ops &o,
     const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
     const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
     const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
-    stS<PREC>(S[0], e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, a.iS[0]);
-    stS<PREC>(S[1], e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, a.iS[1]);
-    stS<PREC>(S[2], e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, a.iS[2]);
+    stS<PREC>(S[0], e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, sc_iS(a.scale, 0));
+    stS<PREC>(S[1], e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, sc_iS(a.scale, 1));
+    stS<PREC>(S[2], e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, sc_iS(a.scale, 2));
     sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
     sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
     sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
@@ -355,9 +355,9 @@ __device__ __forceinline__ void stress_absorber(const Str3Args &a, const Ops &o,
     const float dyVz = (vzjp - vz0) * r20y;
     const float dzVx = (vxkp - vx0) * r20z;
     const float dzVy = (vykp - vy0) * r20z;
-    stS<PREC>(S[3], e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, a.iS[3]);
-    stS<PREC>(S[4], e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, a.iS[4]);
-    stS<PREC>(S[5], e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, a.iS[5]);
+    stS<PREC>(S[3], e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, sc_iS(a.scale, 3));
+    stS<PREC>(S[4], e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, sc_iS(a.scale, 4));
+    stS<PREC>(S[5], e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, sc_iS(a.scale, 5));
     sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
     sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
     sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
@@ -529,7 +529,7 @@ __device__ __forceinline__ void wav_station(const Wav3Args &a, int n) {
         if (a.s_half) {
             // FP16 stress arrays: the same expressions on the scaled values
             auto S = [&](const float *p, int c, long long q) {
-                return __half2float(reinterpret_cast<const __half *>(p)[q]) * a.sS[c];
+                return __half2float(reinterpret_cast<const __half *>(p)[q]) * sc_sS(a.scale, c);
             };
             w[0 * ntw] = S(a.Sxx, 0, e) * M0 * UC * 1e6f;
             w[1 * ntw] = S(a.Syy, 1, e) * M0 * UC * 1e6f;

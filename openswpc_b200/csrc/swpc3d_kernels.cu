@@ -108,9 +108,9 @@ void launch_stress3d(const Str3Args &a, int nm, int minb, int prec, dim3 grid, d
 __device__ __forceinline__ void glut_half(const InjArgs &a, const InjEntry &en, float sdrop, int div) {
     __half *h = reinterpret_cast<__half *>(a.fields[en.field]);
     const int c = en.field - SWPC_F_SXX;
-    const float v = __half2float(h[en.cell]) * a.sS[c];
+    const float v = __half2float(h[en.cell]) * sc_sS(a.scale, c);
     const float w = div == 1 ? v - en.coef * sdrop : v - en.coef * sdrop / div;
-    h[en.cell] = __float2half_rn(w * a.iS[c]);
+    h[en.cell] = __float2half_rn(w * sc_iS(a.scale, c));
 }
 
 __device__ __forceinline__ void apply_entry(const InjArgs &a, const InjEntry &en, int it) {

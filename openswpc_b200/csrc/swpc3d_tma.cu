@@ -94,16 +94,16 @@ struct SStrOps {
         return sv[((c * (BJ + 4) + tz + 2 + dj) * (BI + 4) + ty + 2 + di) * KB + tx + 4 + dk];
     }
     __device__ __forceinline__ float sown(int f) const {
-        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(f)]) * a.sS[f];
+        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(f)]) * sc_sS(a.scale, f);
         else return ss[at(f)];
     }
     __device__ __forceinline__ float r(int q) const {
         const int f = (q / 3) * NM + q % 3;
-        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(6 + f)]) * a.sR[q];
+        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(6 + f)]) * sc_sR(a.scale, q);
         else if constexpr (PREC == PREC_BF16_R)
             return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(ss + StrBoxes<NM, BI, BJ, 1, PREC>::oR)[at(f)]);
         else if constexpr (PREC == PREC_F16_R)
-            return __half2float(reinterpret_cast<const __half *>(ss + StrBoxes<NM, BI, BJ, 1, PREC>::oR)[at(f)]) * a.sR[q];
+            return __half2float(reinterpret_cast<const __half *>(ss + StrBoxes<NM, BI, BJ, 1, PREC>::oR)[at(f)]) * sc_sR(a.scale, q);
         else return ss[at(6 + f)];
     }
     // 0 mu, 1 lam, 2 taup, 3 taus, 4 muyz, 5 muxz, 6 muxy
@@ -232,7 +232,7 @@ struct SVelOps {
     __device__ __forceinline__ float b(int c) const { return sb[at(c)]; }
     // element q of the box at float offset o
     __device__ __forceinline__ float el(int f, int o, int q) const {
-        if constexpr (L::H) return __half2float(reinterpret_cast<const __half *>(mem + o)[q]) * a.sS[f];
+        if constexpr (L::H) return __half2float(reinterpret_cast<const __half *>(mem + o)[q]) * sc_sS(a.scale, f);
         else return mem[o + q];
     }
     __device__ __forceinline__ float s(int f, int dk, int di, int dj) const {

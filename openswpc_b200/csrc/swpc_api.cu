@@ -74,6 +74,17 @@ int graph_invalidate(swpc_ctx *c) {
     invalidate_graph(c);
     return SWPC_OK;
 }
+// the FP16 scales 2^eS, 2^-eS, 2^eR, 2^-eR to device memory, where the kernels
+// read them (no launch argument changes when they are re-centred)
+int upload_scales(swpc_ctx *c) {
+    for (int q = 0; q < 6; q++) { c->h_scale[q] = ldexpf(1.0f, c->eS[q]); c->h_scale[6 + q] = ldexpf(1.0f, -c->eS[q]); }
+    for (int q = 0; q < 18; q++) {
+        c->h_scale[12 + q] = ldexpf(1.0f, c->eR[q]);
+        c->h_scale[30 + q] = ldexpf(1.0f, -c->eR[q]);
+    }
+    CK(cudaMemcpyAsync(c->d_scale, c->h_scale, sizeof(c->h_scale), cudaMemcpyHostToDevice, c->stream));
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
 }  // namespace swpc
 
 // ---------------------------------------------------------------------------
@@ -197,6 +208,8 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     }
     if (!rc) rc = dalloc(c, &c->vmax_buf, 4);
     if (!rc) rc = dalloc(c, &c->d_it, 1);
+    if (!rc) rc = dalloc(c, &c->d_scale, kScaleFloats);
+    if (!rc) rc = upload_scales(c);
     if (!rc) rc = cuda_check(c, cudaMallocHost((void **)&c->h_vmax, 4 * sizeof(unsigned int)), "cudaMallocHost");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     if (rc) return fail(rc);
@@ -224,6 +237,7 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
         for (auto &p : c->med) p = nullptr;
     }
     if (c->d_err) cudaFree(c->d_err);
+    if (c->d_scale) cudaFree(c->d_scale);
     if (c->stage) cudaFree(c->stage);
     if (c->cj) cudaFree(c->cj);
     delete static_cast<TmaMaps *>(c->tmaps);
@@ -1102,8 +1116,7 @@ static int launch_stress_kernel(swpc_ctx *c, int mask) {
     a.d2 = c->d2;
     a.dt = c->d.dt;
     a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
-    for (int q = 0; q < 6; q++) { a.sS[q] = ldexpf(1.0f, c->eS[q]); a.iS[q] = ldexpf(1.0f, -c->eS[q]); }
-    for (int q = 0; q < 18; q++) { a.sR[q] = ldexpf(1.0f, c->eR[q]); a.iR[q] = ldexpf(1.0f, -c->eR[q]); }
+    a.scale = c->d_scale;
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
     if (c->stress_tma && c->slab) {
@@ -1146,7 +1159,7 @@ static int launch_vel_kernel(swpc_ctx *c, int mask) {
     a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
-    for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
+    a.scale = c->d_scale;
     if (c->vel_tma && c->slab) {
         RC(tma_ready(c));
         const TmaTiles t = tma_tiles(c, c->vel_tbi, c->vel_tbj, 1, 1, kVelFields, 1);
@@ -1164,7 +1177,7 @@ static void fill_inj_fields(swpc_ctx *c, InjArgs &a) {
     for (int q = 0; q < 3; q++) a.fields[q] = c->V[q];
     for (int q = 0; q < 6; q++) a.fields[3 + q] = c->S[q];
     a.s_half = c->prec == SWPC_PREC_F16_SR;
-    for (int q = 0; q < 6; q++) { a.sS[q] = ldexpf(1.0f, c->eS[q]); a.iS[q] = ldexpf(1.0f, -c->eS[q]); }
+    a.scale = c->d_scale;
     if (is3d(c)) { a.bfields[0] = c->med[5]; a.bfields[1] = c->med[6]; a.bfields[2] = c->med[7]; }
     else { a.bfields[0] = c->med[0]; a.bfields[1] = c->med[0]; a.bfields[2] = c->med[0]; }
 }
@@ -1230,7 +1243,7 @@ static int launch_wav(swpc_ctx *c, int it, const int *d_it) {
     a.M0 = c->M0; a.UC = c->UC; a.dt = c->d.dt;
     memcpy(a.r40, c->r40, sizeof(a.r40)); memcpy(a.r41, c->r41, sizeof(a.r41));
     a.s_half = c->prec == SWPC_PREC_F16_SR;
-    for (int q = 0; q < 6; q++) a.sS[q] = ldexpf(1.0f, c->eS[q]);
+    a.scale = c->d_scale;
     // outside sampling steps the kernel only integrates u / strain
     if (!d_it && (it - 1) % c->ntdec_w != 0 && !(c->wav_what & (SWPC_WAV_U | SWPC_WAV_STRAIN))) return SWPC_OK;
     launch_wav3d(a, c->stream);
@@ -1368,10 +1381,8 @@ extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
     RC(build_graph(c));
     CK(cudaMemcpyAsync(c->d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     for (int n = 0; n < nsteps; n++) {
-        if (fp16_form(c) && (it0 + n) % kRescaleEvery == 0) {
-            RC(rescale_before(c, it0 + n));
-            RC(build_graph(c));   // a changed scale is a kernel argument: the graph is rebuilt
-        }
+        // the graph stays: the kernels read the scales from device memory
+        if (fp16_form(c) && (it0 + n) % kRescaleEvery == 0) RC(rescale_before(c, it0 + n));
         CK(cudaGraphLaunch(c->graph_exec, c->stream));
     }
     return SWPC_OK;

@@ -66,6 +66,8 @@ struct swpc_ctx {
     int prec = SWPC_PREC_F32;   // storage of S and R (3D)
     int eS[6] = {0, 0, 0, 0, 0, 0};   // FP16 scale exponents: value = stored * 2^e
     int eR[18] = {0};
+    float *d_scale = nullptr;           // 2^eS, 2^-eS, 2^eR, 2^-eR in device memory (swpc_kernels.cuh sc_sS)
+    float h_scale[48];                  // its host image
     int device;
     cudaStream_t stream;
     std::string err;
@@ -209,6 +211,7 @@ namespace swpc {
 int set_err(swpc_ctx *c, int code, const std::string &msg);
 // 2 na must fit the grid across x and y (the whole grid for a block of a
 // decomposed one); refused when the medium arrives
+int upload_scales(swpc_ctx *c);   // swpc_api.cu
 inline int check_na_wide(swpc_ctx *c) {
     return c->na_wide ? set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid") : SWPC_OK;
 }

@@ -400,7 +400,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         a.wav_v = b->wav[0]; a.wav_u = b->wav[1]; a.wav_s = b->wav[2]; a.wav_e = b->wav[3];
         a.M0 = c->M0; a.UC = c->UC; a.dt = c->d.dt;
         memcpy(a.r40, c->r40, sizeof(a.r40)); memcpy(a.r41, c->r41, sizeof(a.r41));
-        for (int q = 0; q < 6; q++) a.sS[q] = 1.0f;
+        a.scale = c->d_scale;   // FP32 storage: every scale 1
         const bool sample = d_it || (it - 1) % c->ntdec_w == 0 || (c->wav_what & (SWPC_WAV_U | SWPC_WAV_STRAIN));
         if (sample) {
             wav3d_batch_kernel<<<dim3((c->nst + 127) / 128, b->nmem), 128, 0, c->stream>>>(a, b->stride, 3, 6);
@@ -431,8 +431,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         a.d2 = c->d2;
         a.dt = c->d.dt;
         a.mask = mask;
-        for (int q = 0; q < 6; q++) { a.sS[q] = 1.0f; a.iS[q] = 1.0f; }
-        for (int q = 0; q < 18; q++) { a.sR[q] = 1.0f; a.iR[q] = 1.0f; }
+        a.scale = c->d_scale;   // FP32 storage: every scale 1
         if (b->staged) {
             FRC(fb_tma_ready(b));
             const TmaTiles t = fb_tiles(b, b->sbi, b->sbj, b->smpc, kStressFields(b->c));
@@ -466,7 +465,7 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
         a.dt = c->d.dt;
         a.mask = mask;
-        for (int q = 0; q < 6; q++) a.sS[q] = 1.0f;
+        a.scale = c->d_scale;   // FP32 storage: every scale 1
         if (b->staged) {
             FRC(fb_tma_ready(b));
             const TmaTiles t = fb_tiles(b, b->vbi, b->vbj, b->vmpc, kVelFields);

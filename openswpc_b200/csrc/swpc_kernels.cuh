@@ -9,6 +9,16 @@ namespace swpc {
 
 enum InjMode { INJ_GLUT = 0, INJ_GLUT4 = 1, INJ_GLUT2 = 2, INJ_BF3 = 3, INJ_GREEN = 4, INJ_BFPSV = 5, INJ_BFSH = 6 };
 
+// Power-of-two scales of the FP16 storage forms, 48 floats in device memory
+// (so that re-centring them needs no new launch arguments): value = stored *
+// sS[f] for the six stresses, stored = value * iS[f], and likewise sR, iR for
+// the 18 memory variables (component * 3 + m).  FP32 storage keeps them 1.
+constexpr int kScaleFloats = 48;
+__device__ __forceinline__ float sc_sS(const float *s, int f) { return __ldg(s + f); }
+__device__ __forceinline__ float sc_iS(const float *s, int f) { return __ldg(s + 6 + f); }
+__device__ __forceinline__ float sc_sR(const float *s, int q) { return __ldg(s + 12 + q); }
+__device__ __forceinline__ float sc_iR(const float *s, int q) { return __ldg(s + 30 + q); }
+
 struct Vel3Args {
     Geo g;
     int ibk, iek, jbk, jek, kek;
@@ -23,7 +33,7 @@ struct Vel3Args {
     float r20[3];
     float dt;
     int mask;       // bit 0: interior cells, bit 1: absorber cells
-    float sS[6];    // stored -> value scale of the FP16 stress arrays (PREC_F16_SR)
+    const float *scale;   // FP16 scales in device memory (see sc_sS)
 };
 
 struct Str3Args {
@@ -42,8 +52,7 @@ struct Str3Args {
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     float dt;
     int mask;
-    float sS[6], iS[6];     // FP16 stress scales (value = stored * sS, stored = value * iS)
-    float sR[18], iR[18];   // FP16 memory-variable scales
+    const float *scale;     // FP16 stress and memory-variable scales in device memory (see sc_sS)
 };
 
 struct InjArgs {
@@ -61,7 +70,7 @@ struct InjArgs {
     const float *bfields[3];
     const long long *rho_cell;   // (nsrc) density cell of 2D body forces
     int s_half;          // S stored in FP16 (SWPC_PREC_F16_SR)
-    float sS[6], iS[6];  // its scales: value = stored * sS
+    const float *scale;  // its scales in device memory (see sc_sS)
 };
 
 struct Wav3Args {
@@ -77,7 +86,7 @@ struct Wav3Args {
     float M0, UC, dt;
     float r40[3], r41[3];
     int s_half;          // S stored in FP16 (SWPC_PREC_F16_SR)
-    float sS[6];
+    const float *scale;
 };
 
 struct VmaxArgs {

@@ -151,7 +151,8 @@ extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
         *expo[q] += shift;
         nchg++;
     }
-    if (nchg) graph_invalidate(c);   // the scales are kernel arguments
     if (changed) *changed = nchg;
+    // the kernels read the scales from device memory: no new launch arguments
+    if (nchg) return upload_scales(c);
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }

@@ -495,7 +495,8 @@ class HaloTransport:
     point-to-point operations (NCCL over NVLink on GPUs; gloo works for the
     exchange logic on CPU tensors).  Each half step's messages are matched by
     the order of the batch, which every rank builds the same way (sides in
-    order 0..3)."""
+    order 0..3).  With NCCL the waits order the caller's current CUDA stream
+    behind the transfers and return at once."""
 
     def __init__(self, neighbours: list[int | None], group=None):
         self.neighbours = neighbours
@@ -544,10 +545,26 @@ class BlockRank3D(_Run):
         self.recv = {(h, s): torch.empty(b.halo_count[h][OPPOSITE[s]], dtype=torch.float32, device=dev)
                      for h in (0, 1) for s in range(SIDES) if b.neighbours[s] is not None}
         self.staged = dist.get_backend() != "nccl"
+        # the context's stream as a torch stream, for the stream-ordered NCCL exchange
+        self.stream = torch.cuda.ExternalStream(b.lib.swpc_stream(b.ctx), device=dev)
 
     def _exchange(self, half: int):
+        import torch
+
         b = self.block
         sides = [s for s in range(SIDES) if b.neighbours[s] is not None]
+        if not self.staged:
+            # NCCL: everything stream-ordered on the block's own stream, no host
+            # wait: the sends start after the pack kernels, the unpacks after the
+            # receives (work.wait() orders the current stream, not the host)
+            with torch.cuda.stream(self.stream):
+                for s in sides:
+                    b.pack(half, s, self.send[half, s].data_ptr())
+                self.transport.exchange({s: self.send[half, s] for s in sides},
+                                        {s: self.recv[half, s] for s in sides})
+                for s in sides:
+                    b.unpack(half, s, self.recv[half, s].data_ptr())
+            return
         for s in sides:
             b.pack(half, s, self.send[half, s].data_ptr())
         b.sync()
