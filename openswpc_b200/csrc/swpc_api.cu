@@ -77,11 +77,7 @@ int graph_invalidate(swpc_ctx *c) {
 // the FP16 scales 2^eS, 2^-eS, 2^eR, 2^-eR to device memory, where the kernels
 // read them (no launch argument changes when they are re-centred)
 int upload_scales(swpc_ctx *c) {
-    for (int q = 0; q < 6; q++) { c->h_scale[q] = ldexpf(1.0f, c->eS[q]); c->h_scale[6 + q] = ldexpf(1.0f, -c->eS[q]); }
-    for (int q = 0; q < 18; q++) {
-        c->h_scale[12 + q] = ldexpf(1.0f, c->eR[q]);
-        c->h_scale[30 + q] = ldexpf(1.0f, -c->eR[q]);
-    }
+    for (int q = 0; q < 48; q++) c->h_scale[q] = 1.0f;   // exponents 0 (dalloc zeroes d_exp)
     CK(cudaMemcpyAsync(c->d_scale, c->h_scale, sizeof(c->h_scale), cudaMemcpyHostToDevice, c->stream));
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
@@ -209,6 +205,10 @@ extern "C" int swpc_create(const swpc_desc *d, swpc_ctx **out) {
     if (!rc) rc = dalloc(c, &c->vmax_buf, 4);
     if (!rc) rc = dalloc(c, &c->d_it, 1);
     if (!rc) rc = dalloc(c, &c->d_scale, kScaleFloats);
+    if (!rc) rc = dalloc(c, &c->d_exp, 24);
+    if (!rc) rc = dalloc(c, &c->d_rmax, 24);
+    if (!rc) rc = dalloc(c, &c->d_rfactor, 24);
+    if (!rc) rc = dalloc(c, &c->d_rchanged, 1);
     if (!rc) rc = upload_scales(c);
     if (!rc) rc = cuda_check(c, cudaMallocHost((void **)&c->h_vmax, 4 * sizeof(unsigned int)), "cudaMallocHost");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
@@ -237,7 +237,8 @@ extern "C" int swpc_destroy(swpc_ctx *c) {
         for (auto &p : c->med) p = nullptr;
     }
     if (c->d_err) cudaFree(c->d_err);
-    if (c->d_scale) cudaFree(c->d_scale);
+    for (void *p : {(void *)c->d_scale, (void *)c->d_exp, (void *)c->d_rmax, (void *)c->d_rfactor, (void *)c->d_rchanged})
+        if (p) cudaFree(p);
     if (c->stage) cudaFree(c->stage);
     if (c->cj) cudaFree(c->cj);
     delete static_cast<TmaMaps *>(c->tmaps);
@@ -1287,6 +1288,7 @@ extern "C" int swpc_wav_store(swpc_ctx *c, int it) { PREP(c); return launch_wav(
 // there up to global__comm_vel (half 1); with record = false the wavefield
 // advances without wav__store, green__store and snap__write
 static int step_half0(swpc_ctx *c, int it, const int *d_it, bool record) {
+    RC(rescale_launch(c, it, d_it, false));   // FP16 forms: re-centre the scales every 8 steps, on the device
     if (record) {
         RC(launch_wav(c, it, d_it));
         RC(green_store_launch(c, it, d_it));
@@ -1317,15 +1319,12 @@ static int step_body(swpc_ctx *c, int it, const int *d_it, bool record = true) {
     return SWPC_OK;
 }
 
-static int rescale_before(swpc_ctx *c, int it);
-
 extern "C" int swpc_step_half(swpc_ctx *c, int it, int half) {
     if (!c) return SWPC_ERR_ARG;
     if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
     if (half != 0 && half != 1) return set_err(c, SWPC_ERR_ARG, "half must be 0 (stress) or 1 (velocity)");
     if (c->pw_mode) return set_err(c, SWPC_ERR_STATE, "the plane-wave mode steps whole steps (swpc_step)");
     PREP(c);
-    if (half == 0) RC(rescale_before(c, it));
     return half == 0 ? step_half0(c, it, nullptr, true) : step_half1(c, it, nullptr);
 }
 
@@ -1333,7 +1332,6 @@ extern "C" int swpc_step(swpc_ctx *c, int it) {
     if (!c) return SWPC_ERR_ARG;
     if (it < 1 || it > c->d.nt) return set_err(c, SWPC_ERR_ARG, "time step index outside 1..nt");
     PREP(c);
-    RC(rescale_before(c, it));
     return step_body(c, it, nullptr);
 }
 
@@ -1363,16 +1361,6 @@ static int build_graph(swpc_ctx *c) {
     return SWPC_OK;
 }
 
-// FP16 storage forms: re-centre the arrays' power-of-two scales before every
-// step whose index is a multiple of this (the same steps whatever way the
-// caller splits the loop into calls)
-constexpr int kRescaleEvery = 8;
-static bool fp16_form(const swpc_ctx *c) { return c->prec == SWPC_PREC_F16_SR || c->prec == SWPC_PREC_F16_R; }
-static int rescale_before(swpc_ctx *c, int it) {
-    if (!fp16_form(c) || it % kRescaleEvery != 0) return SWPC_OK;
-    return swpc_rescale(c, nullptr);
-}
-
 extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
     if (!c) return SWPC_ERR_ARG;
     if (nsteps <= 0) return SWPC_OK;
@@ -1380,11 +1368,7 @@ extern "C" int swpc_run(swpc_ctx *c, int it0, int nsteps) {
     CK(cudaSetDevice(c->device));
     RC(build_graph(c));
     CK(cudaMemcpyAsync(c->d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    for (int n = 0; n < nsteps; n++) {
-        // the graph stays: the kernels read the scales from device memory
-        if (fp16_form(c) && (it0 + n) % kRescaleEvery == 0) RC(rescale_before(c, it0 + n));
-        CK(cudaGraphLaunch(c->graph_exec, c->stream));
-    }
+    for (int n = 0; n < nsteps; n++) CK(cudaGraphLaunch(c->graph_exec, c->stream));
     return SWPC_OK;
 }
 

@@ -64,10 +64,15 @@ struct swpc_ctx {
     swpc::Geo g;
     swpc_desc d;
     int prec = SWPC_PREC_F32;   // storage of S and R (3D)
-    int eS[6] = {0, 0, 0, 0, 0, 0};   // FP16 scale exponents: value = stored * 2^e
-    int eR[18] = {0};
-    float *d_scale = nullptr;           // 2^eS, 2^-eS, 2^eR, 2^-eR in device memory (swpc_kernels.cuh sc_sS)
-    float h_scale[48];                  // its host image
+    // FP16 forms: the scales 2^e, 2^-e of the stresses and memory variables
+    // (swpc_kernels.cuh sc_sS) and the exponents, in device memory, where the
+    // re-centring kernels of swpc_prec.cu keep them
+    float *d_scale = nullptr;
+    float h_scale[48];
+    int *d_exp = nullptr;                  // 24: stresses, then memory variables (component * 3 + m)
+    unsigned int *d_rmax = nullptr;        // re-centring scratch: maxima, factors, moved count
+    float *d_rfactor = nullptr;
+    int *d_rchanged = nullptr;
     int device;
     cudaStream_t stream;
     std::string err;
@@ -212,6 +217,7 @@ int set_err(swpc_ctx *c, int code, const std::string &msg);
 // 2 na must fit the grid across x and y (the whole grid for a block of a
 // decomposed one); refused when the medium arrives
 int upload_scales(swpc_ctx *c);   // swpc_api.cu
+int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force);   // swpc_prec.cu
 inline int check_na_wide(swpc_ctx *c) {
     return c->na_wide ? set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid") : SWPC_OK;
 }

@@ -1,24 +1,23 @@
 // swpc_prec.cu -- reduced-precision storage of the 3D stress and
 // memory-variable arrays.
 //
-// Three storage forms share the FP32 arithmetic of the kernels:
+// The storage forms share the FP32 arithmetic of the kernels:
 //   SWPC_PREC_F32     : S and R in FP32 (the reference's MP = SP build)
 //   SWPC_PREC_BF16_R  : the 18 memory variables R in BF16 (2 bytes)
 //   SWPC_PREC_F16_R   : the memory variables R in FP16 with per-array
 //                       power-of-two scales as below, S in FP32
 //   SWPC_PREC_F16_SR  : the 6 stresses S and the memory variables R in FP16,
 //                       each array with its own power-of-two scale s = 2^e:
-//                       value = stored * s.  swpc_rescale moves e so that
-//                       every array's largest magnitude sits near 2^7 in
-//                       storage, far from the FP16 overflow at 65504 and from
-//                       its subnormal range; scaling by a power of two is
-//                       exact, so rescaling adds no rounding.  The time loop
-//                       (swpc_run, swpc_step, swpc_step_half) calls it before
-//                       every step whose index is a multiple of
-//                       kRescaleEvery, so growth between two calls stays far
-//                       below the headroom.
-// This file holds the conversion kernels used by the field transfers and the
-// rescaling pass.
+//                       value = stored * s.
+// Re-centring the FP16 scales runs on the device, inside every step's launch
+// sequence (and so inside the captured graph): before each step whose index is
+// a multiple of kRescaleEvery, one kernel takes the largest stored magnitude of
+// every FP16 array, one single-block kernel moves e so that an array whose
+// maximum left [2^3, 2^10) has it near 2^7 again (at least 64x headroom below
+// the FP16 overflow at 65504, far from the subnormal range) and writes the new
+// scales where the kernels read them, and one kernel multiplies the stored
+// values of the moved arrays by the power of two (exact).  On other steps the
+// three kernels return at once.  The host never waits for them.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -36,32 +35,108 @@ using namespace swpc;
 
 namespace {
 
-__global__ void to_f32_kernel(const void *src, int kind, float s, float *dst, long long n) {
+constexpr int kRescaleEvery = 8;   // re-centre before every step whose index is a multiple of this
+
+// s: the array's scale (FP16) in device memory, read once
+__global__ void to_f32_kernel(const void *src, int kind, const float *s, float *dst, long long n) {
+    const float sc = kind == 1 ? 1.0f : *s;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         dst[q] = kind == 1 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(src)[q])
-                           : __half2float(reinterpret_cast<const __half *>(src)[q]) * s;
+                           : __half2float(reinterpret_cast<const __half *>(src)[q]) * sc;
 }
 
-__global__ void from_f32_kernel(const float *src, int kind, float is, void *dst, long long n) {
+__global__ void from_f32_kernel(const float *src, int kind, const float *is, void *dst, long long n) {
+    const float isc = kind == 1 ? 1.0f : *is;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         if (kind == 1) reinterpret_cast<__nv_bfloat16 *>(dst)[q] = __float2bfloat16_rn(src[q]);
-        else reinterpret_cast<__half *>(dst)[q] = __float2half_rn(src[q] * is);
+        else reinterpret_cast<__half *>(dst)[q] = __float2half_rn(src[q] * isc);
     }
 }
 
-// max |stored| of one FP16 array into out (float bits, atomicMax)
-__global__ void absmax_half_kernel(const __half *p, long long n, unsigned int *out) {
-    unsigned int m = 0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        m = max(m, __float_as_uint(fabsf(__half2float(p[q]))));
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+// the FP16 arrays of a context and the exponent slot of each: 0..5 the
+// stresses, 6 + component * 3 + m the memory variables
+struct RescaleArgs {
+    __half *p[24];
+    int slot[24];
+    int nf;
+    long long n;          // halves per array (a multiple of 8)
+    const int *d_it;      // step counter of graph replays (null: it)
+    int it;
+    int force;            // re-centre now, whatever the step
+    unsigned int *d_max;  // per array, zero between re-centrings
+    int *d_exp;           // exponent per slot (24)
+    float *d_scale;       // the 48 scales the kernels read (swpc_kernels.cuh)
+    float *d_factor;      // per array: 2^-shift of this re-centring, 1 if none
+    int *d_changed;       // arrays moved (swpc_rescale's count)
+};
+
+__device__ __forceinline__ bool rescale_now(const RescaleArgs &r) {
+    return r.force || (r.d_it ? *r.d_it : r.it) % kRescaleEvery == 0;
 }
 
-// stored *= f (a power of two)
-__global__ void rescale_half_kernel(__half *p, long long n, float f) {
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        p[q] = __float2half_rn(__half2float(p[q]) * f);
+// max |stored| of every FP16 array (blockIdx.y) into d_max (float bits,
+// atomicMax), 8 halves a thread per load
+__global__ void rescale_max_kernel(const RescaleArgs r) {
+    if (!rescale_now(r)) return;
+    const uint4 *p8 = reinterpret_cast<const uint4 *>(r.p[blockIdx.y]);
+    unsigned int m = 0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < r.n / 8;
+         q += (long long)gridDim.x * blockDim.x) {
+        const uint4 w = __ldcs(p8 + q);
+        const unsigned int v[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&v[h]));
+            m = max(m, max(__float_as_uint(fabsf(f.x)), __float_as_uint(fabsf(f.y))));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(r.d_max + blockIdx.y, m);
+}
+
+// the new exponents and scales (one thread per array)
+__global__ void rescale_decide_kernel(const RescaleArgs r) {
+    if (!rescale_now(r)) return;
+    const int y = threadIdx.x;
+    if (y >= r.nf) return;
+    const float m = __uint_as_float(r.d_max[y]);
+    r.d_max[y] = 0u;
+    float factor = 1.0f;
+    if (m > 0.0f && isfinite(m)) {
+        const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
+        if (ex < 3 || ex >= 10) {
+            const int shift = ex - 7;   // stored /= 2^shift, e += shift
+            const int sl = r.slot[y];
+            const int e = r.d_exp[sl] + shift;
+            r.d_exp[sl] = e;
+            const float sc = ldexpf(1.0f, e), inv = ldexpf(1.0f, -e);
+            if (sl < 6) { r.d_scale[sl] = sc; r.d_scale[6 + sl] = inv; }
+            else { r.d_scale[12 + sl - 6] = sc; r.d_scale[30 + sl - 6] = inv; }
+            factor = ldexpf(1.0f, -shift);
+            atomicAdd(r.d_changed, 1);
+        }
+    }
+    r.d_factor[y] = factor;
+}
+
+// stored *= factor (a power of two) for the moved arrays
+__global__ void rescale_apply_kernel(const RescaleArgs r) {
+    if (!rescale_now(r)) return;
+    const float f = r.d_factor[blockIdx.y];
+    if (f == 1.0f) return;
+    uint4 *p8 = reinterpret_cast<uint4 *>(r.p[blockIdx.y]);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < r.n / 8;
+         q += (long long)gridDim.x * blockDim.x) {
+        uint4 w = p8[q];
+        unsigned int *v = reinterpret_cast<unsigned int *>(&w);
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            const float2 x = __half22float2(*reinterpret_cast<const __half2 *>(&v[h]));
+            const __half2 o = __floats2half2_rn(x.x * f, x.y * f);
+            v[h] = *reinterpret_cast<const unsigned int *>(&o);
+        }
+        p8[q] = w;
+    }
 }
 
 constexpr int kGrid = 148 * 8;
@@ -78,10 +153,11 @@ int field_storage(const swpc_ctx *c, int field) {
     return 0;
 }
 
-float field_scale(const swpc_ctx *c, int field) {
-    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return std::ldexp(1.0f, c->eS[field - SWPC_F_SXX]);
-    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return std::ldexp(1.0f, c->eR[field - SWPC_F_R]);
-    return 1.0f;
+// the device addresses of a field's scale (stored -> value) and inverse
+static const float *field_scale(const swpc_ctx *c, int field, bool inverse) {
+    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return c->d_scale + (inverse ? 6 : 0) + (field - SWPC_F_SXX);
+    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return c->d_scale + (inverse ? 30 : 12) + (field - SWPC_F_R);
+    return c->d_scale;   // unused (FP32 or BF16)
 }
 
 // Converts a reduced-precision field to / from a temporary FP32 copy on the
@@ -90,17 +166,44 @@ int prec_to_f32(swpc_ctx *c, int field, const float *stored, float **tmp) {
     *tmp = nullptr;
     cudaError_t e = cudaMalloc((void **)tmp, sizeof(float) * c->g.ncell);
     if (e != cudaSuccess) return set_err(c, SWPC_ERR_NOMEM, "cudaMalloc of the conversion buffer failed");
-    to_f32_kernel<<<kGrid, 256, 0, c->stream>>>(stored, field_storage(c, field), field_scale(c, field), *tmp,
+    to_f32_kernel<<<kGrid, 256, 0, c->stream>>>(stored, field_storage(c, field), field_scale(c, field, false), *tmp,
                                                c->g.ncell);
     return cuda_check(c, cudaGetLastError(), "to_f32_kernel");
 }
 
 int prec_from_f32(swpc_ctx *c, int field, const float *tmp, float *stored) {
-    from_f32_kernel<<<kGrid, 256, 0, c->stream>>>(tmp, field_storage(c, field), 1.0f / field_scale(c, field),
+    from_f32_kernel<<<kGrid, 256, 0, c->stream>>>(tmp, field_storage(c, field), field_scale(c, field, true),
                                                  stored, c->g.ncell);
     return cuda_check(c, cudaGetLastError(), "from_f32_kernel");
 }
 
+}  // namespace swpc
+
+namespace swpc {
+// the three re-centring kernels, on the context's stream (it or d_it: the
+// step about to run; force: now)
+int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force) {
+    if (c->prec != SWPC_PREC_F16_SR && c->prec != SWPC_PREC_F16_R) return SWPC_OK;
+    RescaleArgs r;
+    memset(&r, 0, sizeof(r));
+    if (c->prec == SWPC_PREC_F16_SR)
+        for (int q = 0; q < 6; q++) { r.p[r.nf] = reinterpret_cast<__half *>(c->S[q]); r.slot[r.nf++] = q; }
+    for (int comp = 0; comp < 6; comp++)
+        for (int m = 0; m < c->d.nm; m++) {
+            r.p[r.nf] = reinterpret_cast<__half *>(c->R[comp * 3 + m]);
+            r.slot[r.nf++] = 6 + comp * 3 + m;
+        }
+    if (r.nf == 0) return SWPC_OK;
+    r.n = c->g.ncell;
+    r.d_it = d_it; r.it = it; r.force = force ? 1 : 0;
+    r.d_max = c->d_rmax; r.d_exp = c->d_exp; r.d_scale = c->d_scale; r.d_factor = c->d_rfactor;
+    r.d_changed = c->d_rchanged;
+    const dim3 grid(148 * 2, r.nf);
+    rescale_max_kernel<<<grid, 256, 0, c->stream>>>(r);
+    rescale_decide_kernel<<<1, 32, 0, c->stream>>>(r);
+    rescale_apply_kernel<<<grid, 256, 0, c->stream>>>(r);
+    return cuda_check(c, cudaGetLastError(), "rescale kernels");
+}
 }  // namespace swpc
 
 extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
@@ -108,51 +211,13 @@ extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
     if (changed) *changed = 0;
     if (c->prec != SWPC_PREC_F16_SR && c->prec != SWPC_PREC_F16_R) return SWPC_OK;
     if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, SWPC_ERR_CUDA, "cudaSetDevice failed");
-    const bool with_s = c->prec == SWPC_PREC_F16_SR;   // F16_R keeps S in FP32
-    const int nf = (with_s ? 6 : 0) + 6 * c->d.nm;
-    std::vector<float *> fields;
-    std::vector<int *> expo;
-    if (with_s)
-        for (int q = 0; q < 6; q++) { fields.push_back(c->S[q]); expo.push_back(&c->eS[q]); }
-    for (int comp = 0; comp < 6; comp++)
-        for (int m = 0; m < c->d.nm; m++) { fields.push_back(c->R[comp * 3 + m]); expo.push_back(&c->eR[comp * 3 + m]); }
-    unsigned int *d_max = nullptr;
-    if (cudaMalloc((void **)&d_max, sizeof(unsigned int) * nf) != cudaSuccess)
-        return set_err(c, SWPC_ERR_NOMEM, "cudaMalloc failed");
-    int rc = cuda_check(c, cudaMemsetAsync(d_max, 0, sizeof(unsigned int) * nf, c->stream), "cudaMemsetAsync");
-    for (int q = 0; q < nf && !rc; q++) {
-        absmax_half_kernel<<<kGrid, 256, 0, c->stream>>>(reinterpret_cast<const __half *>(fields[q]), c->g.ncell,
-                                                         d_max + q);
-        rc = cuda_check(c, cudaGetLastError(), "absmax_half_kernel");
-    }
-    std::vector<unsigned int> h(nf, 0);
-    if (!rc) rc = cuda_check(c, cudaMemcpyAsync(h.data(), d_max, sizeof(unsigned int) * nf, cudaMemcpyDeviceToHost,
-                                                c->stream), "cudaMemcpyAsync");
+    int rc = cuda_check(c, cudaMemsetAsync(c->d_rchanged, 0, sizeof(int), c->stream), "cudaMemsetAsync");
+    if (!rc) rc = rescale_launch(c, 0, nullptr, true);
+    int n = 0;
+    if (!rc) rc = cuda_check(c, cudaMemcpyAsync(&n, c->d_rchanged, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                             "cudaMemcpyAsync");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
-    cudaFree(d_max);
     if (rc) return rc;
-    int nchg = 0;
-    for (int q = 0; q < nf; q++) {
-        float m;
-        memcpy(&m, &h[q], sizeof(float));
-        if (!(m > 0.0f) || !std::isfinite(m)) continue;
-        // stored max in [2^3, 2^10) is kept; otherwise move it to [2^7, 2^8),
-        // which leaves at least 64x (after a move 256x) headroom below the
-        // FP16 overflow for growth between two calls: a wave front can
-        // multiply an array's maximum by ~40 in 10 steps while the source
-        // starts up
-        const int ex = std::ilogb(m);   // m = f * 2^ex, 1 <= f < 2
-        if (ex >= 3 && ex < 10) continue;
-        const int shift = ex - 7;       // stored /= 2^shift, e += shift
-        rescale_half_kernel<<<kGrid, 256, 0, c->stream>>>(reinterpret_cast<__half *>(fields[q]), c->g.ncell,
-                                                          std::ldexp(1.0f, -shift));
-        rc = cuda_check(c, cudaGetLastError(), "rescale_half_kernel");
-        if (rc) return rc;
-        *expo[q] += shift;
-        nchg++;
-    }
-    if (changed) *changed = nchg;
-    // the kernels read the scales from device memory: no new launch arguments
-    if (nchg) return upload_scales(c);
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    if (changed) *changed = n;
+    return SWPC_OK;
 }
