@@ -104,8 +104,9 @@ typedef struct swpc_desc {
 
 /* Storage precision of the 3D stress (S) and memory-variable (R) arrays; the
  * arithmetic is FP32 in every form.  F32 is the reference's MP = SP build;
- * BF16_R stores R in BF16; F16_SR stores S and R in FP16 with one
- * power-of-two scale per array (see swpc_rescale).  Every form runs the
+ * BF16_R stores R in BF16; F16_R stores R in FP16 and F16_SR stores S and R
+ * in FP16, with one power-of-two scale for the stresses and one for the
+ * memory variables (see swpc_rescale).  Every form runs the
  * TMA-staged kernels by default (swpc_set_launch kernels 5 and 6); the
  * one-cell-per-thread kernels 0 and 1 stay selectable. */
 #define SWPC_PREC_F32 0
@@ -537,13 +538,14 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
  * regions; outside them download writes 0 and upload ignores the input. */
 
 /* SWPC_PREC_F16_SR and SWPC_PREC_F16_R (a no-op otherwise): re-centre the
- * power-of-two scale of every FP16 stress and memory-variable array so that
- * its largest stored magnitude lies in [2^7, 2^8) whenever it has left
+ * power-of-two scale of every FP16 stress and memory-variable array now, so
+ * that its largest stored magnitude lies in [2^7, 2^8) whenever it has left
  * [2^3, 2^10); that leaves at least 64x headroom below the FP16 overflow.
- * Scaling by a power of two is exact.  swpc_run, swpc_step and
- * swpc_step_half call it themselves before every step whose index is a
- * multiple of 8, so a caller need not; *changed (may be NULL) = arrays
- * rescaled.  Blocks.  No counterpart in the reference. */
+ * Scaling by a power of two is exact.  The time step does the same on the
+ * device before every step whose index is a multiple of 8 (swpc_run,
+ * swpc_step, swpc_step_half; inside the captured graph, without waiting on
+ * the host), so a caller need not; *changed (may be NULL) = arrays moved.
+ * Blocks.  No counterpart in the reference. */
 int swpc_rescale(swpc_ctx *ctx, int *changed);
 
 /* Device bytes held by the context. */

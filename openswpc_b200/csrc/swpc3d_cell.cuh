@@ -19,9 +19,10 @@ __device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
 // arithmetic is FP32 in every form.
 //   PREC_F32   : S and R in FP32 (the reference's MP = SP build)
 //   PREC_BF16_R: R stored in BF16
-//   PREC_F16_SR: S and R stored in FP16, each array with its own power-of-two
-//                scale: value = stored * s, stored = value * (1 / s) (exact)
-//   PREC_F16_R : R stored in FP16 with the same per-array scales, S in FP32
+//   PREC_F16_SR: S and R stored in FP16, with one power-of-two scale for the
+//                stresses and one for the memory variables: value = stored *
+//                s, stored = value * (1 / s) (exact)
+//   PREC_F16_R : R stored in FP16 with its scale, S in FP32
 enum { PREC_F32 = 0, PREC_BF16_R = 1, PREC_F16_SR = 2, PREC_F16_R = 3 };
 // the forms whose R lives in the 2-byte slab and S in the FP32 one
 template <int PREC>

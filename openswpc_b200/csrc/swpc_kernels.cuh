@@ -9,15 +9,19 @@ namespace swpc {
 
 enum InjMode { INJ_GLUT = 0, INJ_GLUT4 = 1, INJ_GLUT2 = 2, INJ_BF3 = 3, INJ_GREEN = 4, INJ_BFPSV = 5, INJ_BFSH = 6 };
 
-// Power-of-two scales of the FP16 storage forms, 48 floats in device memory
-// (so that re-centring them needs no new launch arguments): value = stored *
-// sS[f] for the six stresses, stored = value * iS[f], and likewise sR, iR for
-// the 18 memory variables (component * 3 + m).  FP32 storage keeps them 1.
+// Power-of-two scales of the FP16 storage forms, in device memory (so that
+// re-centring them needs no new launch arguments): value = stored * sS for
+// the stresses, stored = value * iS, and likewise sR, iR for the memory
+// variables.  One scale per group: FP16 keeps 11 significant bits over 29
+// binades, so arrays of one group that differ by orders of magnitude lose
+// nothing by sharing it, and a kernel reads each scale from one read-only
+// address, which the compiler loads once.  FP32 storage keeps them 1.  The 48
+// floats hold sS, iS, sR, iR at 0, 6, 12, 30 (the rest repeat them).
 constexpr int kScaleFloats = 48;
-__device__ __forceinline__ float sc_sS(const float *s, int f) { return __ldg(s + f); }
-__device__ __forceinline__ float sc_iS(const float *s, int f) { return __ldg(s + 6 + f); }
-__device__ __forceinline__ float sc_sR(const float *s, int q) { return __ldg(s + 12 + q); }
-__device__ __forceinline__ float sc_iR(const float *s, int q) { return __ldg(s + 30 + q); }
+__device__ __forceinline__ float sc_sS(const float *s, int) { return __ldg(s); }
+__device__ __forceinline__ float sc_iS(const float *s, int) { return __ldg(s + 6); }
+__device__ __forceinline__ float sc_sR(const float *s, int) { return __ldg(s + 12); }
+__device__ __forceinline__ float sc_iR(const float *s, int) { return __ldg(s + 30); }
 
 struct Vel3Args {
     Geo g;

@@ -4,15 +4,15 @@
 // The storage forms share the FP32 arithmetic of the kernels:
 //   SWPC_PREC_F32     : S and R in FP32 (the reference's MP = SP build)
 //   SWPC_PREC_BF16_R  : the 18 memory variables R in BF16 (2 bytes)
-//   SWPC_PREC_F16_R   : the memory variables R in FP16 with per-array
-//                       power-of-two scales as below, S in FP32
+//   SWPC_PREC_F16_R   : the memory variables R in FP16 with a power-of-two
+//                       scale as below, S in FP32
 //   SWPC_PREC_F16_SR  : the 6 stresses S and the memory variables R in FP16,
-//                       each array with its own power-of-two scale s = 2^e:
-//                       value = stored * s.
+//                       with a power-of-two scale s = 2^e per group (the
+//                       stresses, the memory variables): value = stored * s.
 // Re-centring the FP16 scales runs on the device, inside every step's launch
 // sequence (and so inside the captured graph): before each step whose index is
 // a multiple of kRescaleEvery, one kernel takes the largest stored magnitude of
-// every FP16 array, one single-block kernel moves e so that an array whose
+// every FP16 array, one single-warp kernel moves e so that a group whose
 // maximum left [2^3, 2^10) has it near 2^7 again (at least 64x headroom below
 // the FP16 overflow at 65504, far from the subnormal range) and writes the new
 // scales where the kernels read them, and one kernel multiplies the stored
@@ -94,29 +94,45 @@ __global__ void rescale_max_kernel(const RescaleArgs r) {
     if ((threadIdx.x & 31) == 0) atomicMax(r.d_max + blockIdx.y, m);
 }
 
-// the new exponents and scales (one thread per array)
+// the new exponent and scales of each group (stresses: slots 0-5, memory
+// variables: slots 6-23), from the largest stored magnitude over its arrays;
+// one warp, thread y owns array y
 __global__ void rescale_decide_kernel(const RescaleArgs r) {
     if (!rescale_now(r)) return;
     const int y = threadIdx.x;
-    if (y >= r.nf) return;
-    const float m = __uint_as_float(r.d_max[y]);
-    r.d_max[y] = 0u;
-    float factor = 1.0f;
-    if (m > 0.0f && isfinite(m)) {
+    const bool mine = y < r.nf;
+    const unsigned int mb = mine ? r.d_max[y] : 0u;
+    if (mine) r.d_max[y] = 0u;
+    const bool is_r = mine && r.slot[y] >= 6;
+    // group maxima (bit patterns of non-negative floats order like the values)
+    unsigned int ms = (mine && !is_r) ? mb : 0u, mr = is_r ? mb : 0u;
+    for (int o = 16; o > 0; o >>= 1) {
+        ms = max(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+        mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    }
+    float gfac[2] = {1.0f, 1.0f};
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+        const float m = __uint_as_float(g == 0 ? ms : mr);
+        if (!(m > 0.0f) || !isfinite(m)) continue;
         const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
-        if (ex < 3 || ex >= 10) {
-            const int shift = ex - 7;   // stored /= 2^shift, e += shift
-            const int sl = r.slot[y];
-            const int e = r.d_exp[sl] + shift;
-            r.d_exp[sl] = e;
+        if (ex >= 3 && ex < 10) continue;
+        const int shift = ex - 7;   // stored /= 2^shift, e += shift
+        const int e = r.d_exp[g == 0 ? 0 : 6] + shift;   // every thread reads before thread 0 writes
+        gfac[g] = ldexpf(1.0f, -shift);
+        __syncwarp();
+        if (y == 0) {
+            r.d_exp[g == 0 ? 0 : 6] = e;
             const float sc = ldexpf(1.0f, e), inv = ldexpf(1.0f, -e);
-            if (sl < 6) { r.d_scale[sl] = sc; r.d_scale[6 + sl] = inv; }
-            else { r.d_scale[12 + sl - 6] = sc; r.d_scale[30 + sl - 6] = inv; }
-            factor = ldexpf(1.0f, -shift);
-            atomicAdd(r.d_changed, 1);
+            const int base = g == 0 ? 0 : 12, n = g == 0 ? 6 : 18;
+            for (int q = 0; q < n; q++) { r.d_scale[base + q] = sc; r.d_scale[base + n + q] = inv; }
         }
     }
-    r.d_factor[y] = factor;
+    if (mine) {
+        const float f = gfac[is_r ? 1 : 0];
+        r.d_factor[y] = f;
+        if (f != 1.0f) atomicAdd(r.d_changed, 1);
+    }
 }
 
 // stored *= factor (a power of two) for the moved arrays
@@ -200,7 +216,7 @@ int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force) {
     r.d_changed = c->d_rchanged;
     const dim3 grid(148 * 2, r.nf);
     rescale_max_kernel<<<grid, 256, 0, c->stream>>>(r);
-    rescale_decide_kernel<<<1, 32, 0, c->stream>>>(r);
+    rescale_decide_kernel<<<1, 32, 0, c->stream>>>(r);   // nf <= 24: one warp
     rescale_apply_kernel<<<grid, 256, 0, c->stream>>>(r);
     return cuda_check(c, cudaGetLastError(), "rescale kernels");
 }

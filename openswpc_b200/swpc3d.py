@@ -304,8 +304,8 @@ class Swpc3D:
                  precision: str = "f32", average_on_device: bool = False, medium_on_device: bool = False):
         """``precision`` is the storage of stress and memory variables:
         "f32" (the reference's MP = SP build), "bf16r" (memory variables in
-        BF16), "f16r" (memory variables in FP16 with per-array power-of-two
-        scales) or "f16sr" (stress too in FP16); the arithmetic is FP32 in every form.  With
+        BF16), "f16r" (memory variables in FP16 with a power-of-two
+        scale) or "f16sr" (stress too in FP16); the arithmetic is FP32 in every form.  With
         ``average_on_device`` the upload sends rho instead of the six averaged
         fields, which the library forms in HBM (same bits); with
         ``medium_on_device`` the whole medium is built in HBM from the layers
