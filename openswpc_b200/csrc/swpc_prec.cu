@@ -12,12 +12,12 @@
 // Re-centring the FP16 scales runs on the device, inside every step's launch
 // sequence (and so inside the captured graph): before each step whose index is
 // a multiple of kRescaleEvery, one kernel takes the largest stored magnitude of
-// every FP16 array, one single-warp kernel moves e so that a group whose
-// maximum left [2^3, 2^10) has it near 2^7 again (at least 64x headroom below
-// the FP16 overflow at 65504, far from the subnormal range) and writes the new
-// scales where the kernels read them, and one kernel multiplies the stored
-// values of the moved arrays by the power of two (exact).  On other steps the
-// three kernels return at once.  The host never waits for them.
+// each group, and its last block moves e so that a group whose maximum left
+// [2^3, 2^10) has it near 2^7 again (at least 64x headroom below the FP16
+// overflow at 65504, far from the subnormal range) and writes the new scales
+// where the kernels read them; a second kernel multiplies the stored values of
+// the moved groups by the power of two (exact).  On other steps both kernels
+// return at once.  The host never waits for them.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -53,20 +53,20 @@ __global__ void from_f32_kernel(const float *src, int kind, const float *is, voi
     }
 }
 
-// the FP16 arrays of a context and the exponent slot of each: 0..5 the
-// stresses, 6 + component * 3 + m the memory variables
+// the FP16 arrays of a context: the stresses (F16_SR) first, then the
+// memory variables
 struct RescaleArgs {
     __half *p[24];
-    int slot[24];
-    int nf;
-    long long n;          // halves per array (a multiple of 8)
+    int ns, nf;           // stress arrays, all arrays
+    long long n8;         // 16-byte words per array (ncell / 8)
     const int *d_it;      // step counter of graph replays (null: it)
     int it;
     int force;            // re-centre now, whatever the step
-    unsigned int *d_max;  // per array, zero between re-centrings
-    int *d_exp;           // exponent per slot (24)
+    unsigned int *d_max;  // 2 group maxima (float bits), zero between re-centrings
+    unsigned int *d_done; // blocks finished with the maxima, zero between re-centrings
+    int *d_exp;           // group exponents (stresses at 0, memory variables at 6)
     float *d_scale;       // the 48 scales the kernels read (swpc_kernels.cuh)
-    float *d_factor;      // per array: 2^-shift of this re-centring, 1 if none
+    float *d_factor;      // 2 group factors 2^-shift of this re-centring, 1 if none
     int *d_changed;       // arrays moved (swpc_rescale's count)
 };
 
@@ -74,84 +74,89 @@ __device__ __forceinline__ bool rescale_now(const RescaleArgs &r) {
     return r.force || (r.d_it ? *r.d_it : r.it) % kRescaleEvery == 0;
 }
 
-// max |stored| of every FP16 array (blockIdx.y) into d_max (float bits,
-// atomicMax), 8 halves a thread per load
-__global__ void rescale_max_kernel(const RescaleArgs r) {
+// the group's new exponent, scales and factor from its largest stored magnitude
+__device__ void rescale_group(const RescaleArgs &r, int g, float m) {
+    float factor = 1.0f;
+    if (m > 0.0f && isfinite(m)) {
+        const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
+        if (ex < 3 || ex >= 10) {
+            const int shift = ex - 7;   // stored /= 2^shift, e += shift
+            const int e = r.d_exp[g == 0 ? 0 : 6] + shift;
+            r.d_exp[g == 0 ? 0 : 6] = e;
+            const float sc = ldexpf(1.0f, e), inv = ldexpf(1.0f, -e);
+            const int base = g == 0 ? 0 : 12, n = g == 0 ? 6 : 18;
+            for (int q = 0; q < n; q++) { r.d_scale[base + q] = sc; r.d_scale[base + n + q] = inv; }
+            factor = ldexpf(1.0f, -shift);
+            atomicAdd(r.d_changed, g == 0 ? r.ns : r.nf - r.ns);
+        }
+    }
+    r.d_factor[g] = factor;
+}
+
+// Largest stored magnitude of each group (8 halves a thread per load, a
+// grid-stride walk over every array); the last block to finish sets the new
+// exponents and scales.
+__global__ void __launch_bounds__(256) rescale_max_kernel(const RescaleArgs r) {
     if (!rescale_now(r)) return;
-    const uint4 *p8 = reinterpret_cast<const uint4 *>(r.p[blockIdx.y]);
-    unsigned int m = 0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < r.n / 8;
-         q += (long long)gridDim.x * blockDim.x) {
-        const uint4 w = __ldcs(p8 + q);
-        const unsigned int v[4] = {w.x, w.y, w.z, w.w};
+    unsigned int ms = 0, mr = 0;
+    const long long total = r.n8 * r.nf;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+         w += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(w / r.n8);
+        const uint4 v4 = __ldcs(reinterpret_cast<const uint4 *>(r.p[y]) + (w - (long long)y * r.n8));
+        const unsigned int v[4] = {v4.x, v4.y, v4.z, v4.w};
+        unsigned int m = 0;
 #pragma unroll
         for (int h = 0; h < 4; h++) {
             const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&v[h]));
             m = max(m, max(__float_as_uint(fabsf(f.x)), __float_as_uint(fabsf(f.y))));
         }
+        if (y < r.ns) ms = max(ms, m);
+        else mr = max(mr, m);
     }
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(r.d_max + blockIdx.y, m);
-}
-
-// the new exponent and scales of each group (stresses: slots 0-5, memory
-// variables: slots 6-23), from the largest stored magnitude over its arrays;
-// one warp, thread y owns array y
-__global__ void rescale_decide_kernel(const RescaleArgs r) {
-    if (!rescale_now(r)) return;
-    const int y = threadIdx.x;
-    const bool mine = y < r.nf;
-    const unsigned int mb = mine ? r.d_max[y] : 0u;
-    if (mine) r.d_max[y] = 0u;
-    const bool is_r = mine && r.slot[y] >= 6;
-    // group maxima (bit patterns of non-negative floats order like the values)
-    unsigned int ms = (mine && !is_r) ? mb : 0u, mr = is_r ? mb : 0u;
     for (int o = 16; o > 0; o >>= 1) {
         ms = max(ms, __shfl_xor_sync(0xffffffffu, ms, o));
         mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
     }
-    float gfac[2] = {1.0f, 1.0f};
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-        const float m = __uint_as_float(g == 0 ? ms : mr);
-        if (!(m > 0.0f) || !isfinite(m)) continue;
-        const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
-        if (ex >= 3 && ex < 10) continue;
-        const int shift = ex - 7;   // stored /= 2^shift, e += shift
-        const int e = r.d_exp[g == 0 ? 0 : 6] + shift;   // every thread reads before thread 0 writes
-        gfac[g] = ldexpf(1.0f, -shift);
-        __syncwarp();
-        if (y == 0) {
-            r.d_exp[g == 0 ? 0 : 6] = e;
-            const float sc = ldexpf(1.0f, e), inv = ldexpf(1.0f, -e);
-            const int base = g == 0 ? 0 : 12, n = g == 0 ? 6 : 18;
-            for (int q = 0; q < n; q++) { r.d_scale[base + q] = sc; r.d_scale[base + n + q] = inv; }
-        }
+    if ((threadIdx.x & 31) == 0) {
+        if (ms) atomicMax(r.d_max, ms);
+        if (mr) atomicMax(r.d_max + 1, mr);
     }
-    if (mine) {
-        const float f = gfac[is_r ? 1 : 0];
-        r.d_factor[y] = f;
-        if (f != 1.0f) atomicAdd(r.d_changed, 1);
-    }
+    // the last block decides (the maxima of every block are visible to it)
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(r.d_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned int gs = atomicExch(r.d_max, 0u), gr = atomicExch(r.d_max + 1, 0u);
+    *r.d_done = 0u;
+    rescale_group(r, 0, __uint_as_float(gs));
+    rescale_group(r, 1, __uint_as_float(gr));
 }
 
-// stored *= factor (a power of two) for the moved arrays
-__global__ void rescale_apply_kernel(const RescaleArgs r) {
+// stored *= factor (a power of two) in the moved groups
+__global__ void __launch_bounds__(256) rescale_apply_kernel(const RescaleArgs r) {
     if (!rescale_now(r)) return;
-    const float f = r.d_factor[blockIdx.y];
-    if (f == 1.0f) return;
-    uint4 *p8 = reinterpret_cast<uint4 *>(r.p[blockIdx.y]);
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < r.n / 8;
-         q += (long long)gridDim.x * blockDim.x) {
-        uint4 w = p8[q];
-        unsigned int *v = reinterpret_cast<unsigned int *>(&w);
+    const float fs = r.d_factor[0], fr = r.d_factor[1];
+    if (fs == 1.0f && fr == 1.0f) return;
+    const long long total = r.n8 * r.nf;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+         w += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(w / r.n8);
+        const float f = y < r.ns ? fs : fr;
+        if (f == 1.0f) continue;
+        uint4 *p = reinterpret_cast<uint4 *>(r.p[y]) + (w - (long long)y * r.n8);
+        uint4 v4 = *p;
+        unsigned int *v = reinterpret_cast<unsigned int *>(&v4);
 #pragma unroll
         for (int h = 0; h < 4; h++) {
             const float2 x = __half22float2(*reinterpret_cast<const __half2 *>(&v[h]));
             const __half2 o = __floats2half2_rn(x.x * f, x.y * f);
             v[h] = *reinterpret_cast<const unsigned int *>(&o);
         }
-        p8[q] = w;
+        *p = v4;
     }
 }
 
@@ -203,21 +208,18 @@ int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force) {
     RescaleArgs r;
     memset(&r, 0, sizeof(r));
     if (c->prec == SWPC_PREC_F16_SR)
-        for (int q = 0; q < 6; q++) { r.p[r.nf] = reinterpret_cast<__half *>(c->S[q]); r.slot[r.nf++] = q; }
+        for (int q = 0; q < 6; q++) r.p[r.nf++] = reinterpret_cast<__half *>(c->S[q]);
+    r.ns = r.nf;
     for (int comp = 0; comp < 6; comp++)
-        for (int m = 0; m < c->d.nm; m++) {
-            r.p[r.nf] = reinterpret_cast<__half *>(c->R[comp * 3 + m]);
-            r.slot[r.nf++] = 6 + comp * 3 + m;
-        }
+        for (int m = 0; m < c->d.nm; m++) r.p[r.nf++] = reinterpret_cast<__half *>(c->R[comp * 3 + m]);
     if (r.nf == 0) return SWPC_OK;
-    r.n = c->g.ncell;
+    r.n8 = c->g.ncell / 8;   // ncell is a multiple of 8 (Kp is)
     r.d_it = d_it; r.it = it; r.force = force ? 1 : 0;
-    r.d_max = c->d_rmax; r.d_exp = c->d_exp; r.d_scale = c->d_scale; r.d_factor = c->d_rfactor;
-    r.d_changed = c->d_rchanged;
-    const dim3 grid(148 * 2, r.nf);
-    rescale_max_kernel<<<grid, 256, 0, c->stream>>>(r);
-    rescale_decide_kernel<<<1, 32, 0, c->stream>>>(r);   // nf <= 24: one warp
-    rescale_apply_kernel<<<grid, 256, 0, c->stream>>>(r);
+    r.d_max = c->d_rmax; r.d_done = c->d_rmax + 2; r.d_exp = c->d_exp; r.d_scale = c->d_scale;
+    r.d_factor = c->d_rfactor; r.d_changed = c->d_rchanged;
+    // small grids: the kernels return at once on the steps between re-centrings
+    rescale_max_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
+    rescale_apply_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
     return cuda_check(c, cudaGetLastError(), "rescale kernels");
 }
 }  // namespace swpc

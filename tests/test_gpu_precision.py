@@ -66,16 +66,19 @@ def test_reduced_storage_roundtrip_and_rescale():
     assert g.rescale() == 0   # a second call finds every array centred
     before = [g.download(_lib.F_SXX + c) for c in range(6)]
     r_before = g.download(_lib.F_R + 0)
-    # Sxx 16 times larger: its stored maximum leaves the window [2^3, 2^10)
+    # every stress 16 times larger: the group's stored maximum leaves the window [2^3, 2^10)
     assert np.abs(before[0]).max() > 0
-    g.upload(_lib.F_SXX, before[0] * np.float32(16.0))
-    d1 = g.download(_lib.F_SXX)
-    assert g.rescale() >= 1
-    d2 = g.download(_lib.F_SXX)
-    # exact unless a value fell into the FP16 subnormal range
-    assert np.abs(d1 - d2).max() <= np.abs(d1).max() * 2.0 ** -20
+    for c in range(6):
+        g.upload(_lib.F_SXX + c, before[c] * np.float32(16.0))
+    d1 = [g.download(_lib.F_SXX + c) for c in range(6)]
+    assert g.rescale() == 6   # the six stress arrays move together (one scale per group)
+    d2 = [g.download(_lib.F_SXX + c) for c in range(6)]
+    for a, b in zip(d1, d2):
+        # exact unless a value fell into the FP16 subnormal range
+        assert np.abs(a - b).max() <= np.abs(a).max() * 2.0 ** -20
     assert g.rescale() == 0   # centred
-    g.upload(_lib.F_SXX, before[0])   # the run's own values again (exact: a power-of-two change of scale)
+    for c in range(6):   # the run's own values again (exact: a power-of-two change of scale)
+        g.upload(_lib.F_SXX + c, before[c])
     after = [g.download(_lib.F_SXX + c) for c in range(6)]
     for a, b in zip(before, after):
         assert np.abs(a - b).max() <= np.abs(a).max() * 2.0 ** -20
