@@ -542,10 +542,11 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
  * that its largest stored magnitude lies in [2^7, 2^8) whenever it has left
  * [2^3, 2^10); that leaves at least 64x headroom below the FP16 overflow.
  * Scaling by a power of two is exact.  The time step does the same on the
- * device before every step whose index is a multiple of 8 (swpc_run,
- * swpc_step, swpc_step_half; inside the captured graph, without waiting on
- * the host), so a caller need not; *changed (may be NULL) = arrays moved.
- * Blocks.  No counterpart in the reference. */
+ * device at every step at no extra pass (swpc_run, swpc_step,
+ * swpc_step_half: the stress update measures what it stores, and the next
+ * one converts as it rewrites; inside the captured graph, without the host),
+ * so a caller need not; *changed (may be NULL) = arrays moved.  Blocks.  No
+ * counterpart in the reference. */
 int swpc_rescale(swpc_ctx *ctx, int *changed);
 
 /* Device bytes held by the context. */

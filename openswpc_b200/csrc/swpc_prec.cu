@@ -9,15 +9,16 @@
 //   SWPC_PREC_F16_SR  : the 6 stresses S and the memory variables R in FP16,
 //                       with a power-of-two scale s = 2^e per group (the
 //                       stresses, the memory variables): value = stored * s.
-// Re-centring the FP16 scales runs on the device, inside every step's launch
-// sequence (and so inside the captured graph): before each step whose index is
-// a multiple of kRescaleEvery, one kernel takes the largest stored magnitude of
-// each group, and its last block moves e so that a group whose maximum left
-// [2^3, 2^10) has it near 2^7 again (at least 64x headroom below the FP16
-// overflow at 65504, far from the subnormal range) and writes the new scales
-// where the kernels read them; a second kernel multiplies the stored values of
-// the moved groups by the power of two (exact).  On other steps both kernels
-// return at once.  The host never waits for them.
+// Re-centring the FP16 scales costs the time loop no pass of its own: the
+// stress update keeps the largest magnitude it stores in each group; before
+// the next update a one-thread kernel moves the exponent of a group whose
+// maximum left [2^3, 2^10) so that it sits near 2^7 again (at least 64x
+// headroom below the FP16 overflow at 65504, far from the subnormal range);
+// the update reads with the old scale and writes with the new one, which
+// converts every value it rewrites (a power of two: exact); a second
+// one-thread kernel then makes the new scale the read scale.  All of it runs
+// in the step's launch sequence, inside the captured graph, without the host.
+// swpc_rescale does the same between steps with a pass of its own.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -35,7 +36,6 @@ using namespace swpc;
 
 namespace {
 
-constexpr int kRescaleEvery = 8;   // re-centre before every step whose index is a multiple of this
 
 // s: the array's scale (FP16) in device memory, read once
 __global__ void to_f32_kernel(const void *src, int kind, const float *s, float *dst, long long n) {
@@ -59,45 +59,17 @@ struct RescaleArgs {
     __half *p[24];
     int ns, nf;           // stress arrays, all arrays
     long long n8;         // 16-byte words per array (ncell / 8)
-    const int *d_it;      // step counter of graph replays (null: it)
-    int it;
-    int force;            // re-centre now, whatever the step
-    unsigned int *d_max;  // 2 group maxima (float bits), zero between re-centrings
-    unsigned int *d_done; // blocks finished with the maxima, zero between re-centrings
-    int *d_exp;           // group exponents (stresses at 0, memory variables at 6)
-    float *d_scale;       // the 48 scales the kernels read (swpc_kernels.cuh)
+    unsigned int *d_max;  // 2 group maxima of stored magnitudes (float bits)
+    int *d_exp;           // group exponents (stresses at 0, memory variables at 1)
+    float *d_scale;       // the scales the kernels read (swpc_kernels.cuh sc_sS)
     float *d_factor;      // 2 group factors 2^-shift of this re-centring, 1 if none
     int *d_changed;       // arrays moved (swpc_rescale's count)
 };
 
-__device__ __forceinline__ bool rescale_now(const RescaleArgs &r) {
-    return r.force || (r.d_it ? *r.d_it : r.it) % kRescaleEvery == 0;
-}
-
-// the group's new exponent, scales and factor from its largest stored magnitude
-__device__ void rescale_group(const RescaleArgs &r, int g, float m) {
-    float factor = 1.0f;
-    if (m > 0.0f && isfinite(m)) {
-        const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
-        if (ex < 3 || ex >= 10) {
-            const int shift = ex - 7;   // stored /= 2^shift, e += shift
-            const int e = r.d_exp[g == 0 ? 0 : 6] + shift;
-            r.d_exp[g == 0 ? 0 : 6] = e;
-            const float sc = ldexpf(1.0f, e), inv = ldexpf(1.0f, -e);
-            const int base = g == 0 ? 0 : 12, n = g == 0 ? 6 : 18;
-            for (int q = 0; q < n; q++) { r.d_scale[base + q] = sc; r.d_scale[base + n + q] = inv; }
-            factor = ldexpf(1.0f, -shift);
-            atomicAdd(r.d_changed, g == 0 ? r.ns : r.nf - r.ns);
-        }
-    }
-    r.d_factor[g] = factor;
-}
-
-// Largest stored magnitude of each group (8 halves a thread per load, a
-// grid-stride walk over every array); the last block to finish sets the new
-// exponents and scales.
+// Largest stored magnitude of each group, by a pass over every array (a
+// re-centring asked for between steps; in the time loop the stress update
+// measures it while it stores)
 __global__ void __launch_bounds__(256) rescale_max_kernel(const RescaleArgs r) {
-    if (!rescale_now(r)) return;
     unsigned int ms = 0, mr = 0;
     const long long total = r.n8 * r.nf;
     for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
@@ -122,23 +94,36 @@ __global__ void __launch_bounds__(256) rescale_max_kernel(const RescaleArgs r) {
         if (ms) atomicMax(r.d_max, ms);
         if (mr) atomicMax(r.d_max + 1, mr);
     }
-    // the last block decides (the maxima of every block are visible to it)
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(r.d_done, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last || threadIdx.x != 0) return;
-    __threadfence();
-    const unsigned int gs = atomicExch(r.d_max, 0u), gr = atomicExch(r.d_max + 1, 0u);
-    *r.d_done = 0u;
-    rescale_group(r, 0, __uint_as_float(gs));
-    rescale_group(r, 1, __uint_as_float(gr));
 }
 
-// stored *= factor (a power of two) in the moved groups
+// From the group maxima (then cleared): a group whose stored maximum left
+// [2^3, 2^10) gets the exponent that puts it near 2^7, in the scales [2..5]
+// that the next stress update writes with.  One thread.
+__global__ void rescale_decide_kernel(const RescaleArgs r) {
+    for (int g = 0; g < 2; g++) {
+        const float m = __uint_as_float(r.d_max[g]);
+        r.d_max[g] = 0u;
+        float factor = 1.0f;
+        const int n = g == 0 ? r.ns : r.nf - r.ns;
+        if (n > 0 && m > 0.0f && isfinite(m)) {
+            const int ex = ilogbf(m);   // m = f 2^ex, 1 <= f < 2
+            if (ex < 3 || ex >= 10) {
+                const int shift = ex - 7;   // stored /= 2^shift, e += shift
+                const int e = r.d_exp[g] + shift;
+                r.d_exp[g] = e;
+                r.d_scale[g == 0 ? 2 : 4] = ldexpf(1.0f, e);
+                r.d_scale[g == 0 ? 3 : 5] = ldexpf(1.0f, -e);
+                factor = ldexpf(1.0f, -shift);
+                *r.d_changed += n;
+            }
+        }
+        r.d_factor[g] = factor;
+    }
+}
+
+// stored *= factor (a power of two) in the moved groups: a re-centring asked
+// for between steps converts the data itself
 __global__ void __launch_bounds__(256) rescale_apply_kernel(const RescaleArgs r) {
-    if (!rescale_now(r)) return;
     const float fs = r.d_factor[0], fr = r.d_factor[1];
     if (fs == 1.0f && fr == 1.0f) return;
     const long long total = r.n8 * r.nf;
@@ -160,6 +145,12 @@ __global__ void __launch_bounds__(256) rescale_apply_kernel(const RescaleArgs r)
     }
 }
 
+// what the stored values mean from now on (sc_sS_in, sc_sR_in)
+__global__ void rescale_commit_kernel(float *d_scale) {
+    d_scale[0] = d_scale[2];
+    d_scale[1] = d_scale[4];
+}
+
 constexpr int kGrid = 148 * 8;
 
 }  // namespace
@@ -176,8 +167,8 @@ int field_storage(const swpc_ctx *c, int field) {
 
 // the device addresses of a field's scale (stored -> value) and inverse
 static const float *field_scale(const swpc_ctx *c, int field, bool inverse) {
-    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return c->d_scale + (inverse ? 6 : 0) + (field - SWPC_F_SXX);
-    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return c->d_scale + (inverse ? 30 : 12) + (field - SWPC_F_R);
+    if (field >= SWPC_F_SXX && field <= SWPC_F_SXY) return c->d_scale + (inverse ? 3 : 2);
+    if (field >= SWPC_F_R && field < SWPC_F_R + 18) return c->d_scale + (inverse ? 5 : 4);
     return c->d_scale;   // unused (FP32 or BF16)
 }
 
@@ -201,10 +192,7 @@ int prec_from_f32(swpc_ctx *c, int field, const float *tmp, float *stored) {
 }  // namespace swpc
 
 namespace swpc {
-// the three re-centring kernels, on the context's stream (it or d_it: the
-// step about to run; force: now)
-int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force) {
-    if (c->prec != SWPC_PREC_F16_SR && c->prec != SWPC_PREC_F16_R) return SWPC_OK;
+static RescaleArgs rescale_args(swpc_ctx *c) {
     RescaleArgs r;
     memset(&r, 0, sizeof(r));
     if (c->prec == SWPC_PREC_F16_SR)
@@ -212,25 +200,44 @@ int rescale_launch(swpc_ctx *c, int it, const int *d_it, bool force) {
     r.ns = r.nf;
     for (int comp = 0; comp < 6; comp++)
         for (int m = 0; m < c->d.nm; m++) r.p[r.nf++] = reinterpret_cast<__half *>(c->R[comp * 3 + m]);
-    if (r.nf == 0) return SWPC_OK;
     r.n8 = c->g.ncell / 8;   // ncell is a multiple of 8 (Kp is)
-    r.d_it = d_it; r.it = it; r.force = force ? 1 : 0;
-    r.d_max = c->d_rmax; r.d_done = c->d_rmax + 2; r.d_exp = c->d_exp; r.d_scale = c->d_scale;
+    r.d_max = c->d_rmax; r.d_exp = c->d_exp; r.d_scale = c->d_scale;
     r.d_factor = c->d_rfactor; r.d_changed = c->d_rchanged;
-    // small grids: the kernels return at once on the steps between re-centrings
-    rescale_max_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
-    rescale_apply_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
-    return cuda_check(c, cudaGetLastError(), "rescale kernels");
+    return r;
+}
+
+static bool fp16_form(const swpc_ctx *c) { return c->prec == SWPC_PREC_F16_SR || c->prec == SWPC_PREC_F16_R; }
+
+// Around each step's stress update (FP16 forms): before it, the new scales
+// from the maxima the previous update stored (it then converts every value
+// it rewrites); after it, the read scales follow.  Two one-thread kernels.
+int rescale_before_stress(swpc_ctx *c) {
+    if (!fp16_form(c)) return SWPC_OK;
+    rescale_decide_kernel<<<1, 1, 0, c->stream>>>(rescale_args(c));
+    return cuda_check(c, cudaGetLastError(), "rescale_decide_kernel");
+}
+int rescale_after_stress(swpc_ctx *c) {
+    if (!fp16_form(c)) return SWPC_OK;
+    rescale_commit_kernel<<<1, 1, 0, c->stream>>>(c->d_scale);
+    return cuda_check(c, cudaGetLastError(), "rescale_commit_kernel");
 }
 }  // namespace swpc
 
 extern "C" int swpc_rescale(swpc_ctx *c, int *changed) {
     if (!c) return SWPC_ERR_ARG;
     if (changed) *changed = 0;
-    if (c->prec != SWPC_PREC_F16_SR && c->prec != SWPC_PREC_F16_R) return SWPC_OK;
+    if (!fp16_form(c)) return SWPC_OK;
     if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, SWPC_ERR_CUDA, "cudaSetDevice failed");
+    const RescaleArgs r = rescale_args(c);
     int rc = cuda_check(c, cudaMemsetAsync(c->d_rchanged, 0, sizeof(int), c->stream), "cudaMemsetAsync");
-    if (!rc) rc = rescale_launch(c, 0, nullptr, true);
+    if (!rc) rc = cuda_check(c, cudaMemsetAsync(c->d_rmax, 0, 2 * sizeof(unsigned int), c->stream), "cudaMemsetAsync");
+    if (!rc && r.nf > 0) {
+        rescale_max_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
+        rescale_decide_kernel<<<1, 1, 0, c->stream>>>(r);
+        rescale_apply_kernel<<<148 * 4, 256, 0, c->stream>>>(r);
+        rescale_commit_kernel<<<1, 1, 0, c->stream>>>(c->d_scale);
+        rc = cuda_check(c, cudaGetLastError(), "rescale kernels");
+    }
     int n = 0;
     if (!rc) rc = cuda_check(c, cudaMemcpyAsync(&n, c->d_rchanged, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                              "cudaMemcpyAsync");
