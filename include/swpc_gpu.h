@@ -105,8 +105,8 @@ typedef struct swpc_desc {
 /* Storage precision of the 3D stress (S) and memory-variable (R) arrays; the
  * arithmetic is FP32 in every form.  F32 is the reference's MP = SP build;
  * BF16_R stores R in BF16; F16_R stores R in FP16 and F16_SR stores S and R
- * in FP16, with one power-of-two scale for the stresses and one for the
- * memory variables (see swpc_rescale).  Every form runs the
+ * in FP16, with a power-of-two scale per stress array and one for the memory
+ * variables (see swpc_rescale).  Every form runs the
  * TMA-staged kernels by default (swpc_set_launch kernels 5 and 6); the
  * one-cell-per-thread kernels 0 and 1 stay selectable. */
 #define SWPC_PREC_F32 0
@@ -542,11 +542,11 @@ int swpc_upload_field(swpc_ctx *ctx, int field, const float *in, int ld_k, int l
  * that its largest stored magnitude lies in [2^7, 2^8) whenever it has left
  * [2^3, 2^10); that leaves at least 64x headroom below the FP16 overflow.
  * Scaling by a power of two is exact.  The time step does the same on the
- * device at every step at no extra pass (swpc_run, swpc_step,
- * swpc_step_half: the stress update measures what it stores, and the next
- * one converts as it rewrites; inside the captured graph, without the host),
- * so a caller need not; *changed (may be NULL) = arrays moved.  Blocks.  No
- * counterpart in the reference. */
+ * device every 8 steps (swpc_run, swpc_step, swpc_step_half: a measuring
+ * kernel before the stress update, which converts the values as it rewrites
+ * them; inside the captured graph, without the host), so a caller need not;
+ * *changed (may be NULL) = arrays moved.  Blocks.  No counterpart in the
+ * reference. */
 int swpc_rescale(swpc_ctx *ctx, int *changed);
 
 /* Device bytes held by the context. */

@@ -19,9 +19,9 @@ __device__ __forceinline__ void sts(float *p, float v) { __stcs(p, v); }
 // arithmetic is FP32 in every form.
 //   PREC_F32   : S and R in FP32 (the reference's MP = SP build)
 //   PREC_BF16_R: R stored in BF16
-//   PREC_F16_SR: S and R stored in FP16, with one power-of-two scale for the
-//                stresses and one for the memory variables: value = stored *
-//                s, stored = value * (1 / s) (exact)
+//   PREC_F16_SR: S and R stored in FP16, with a power-of-two scale per
+//                stress array and one for the memory variables: value =
+//                stored * s, stored = value * (1 / s) (exact)
 //   PREC_F16_R : R stored in FP16 with its scale, S in FP32
 enum { PREC_F32 = 0, PREC_BF16_R = 1, PREC_F16_SR = 2, PREC_F16_R = 3 };
 // the forms whose R lives in the 2-byte slab and S in the FP32 one
@@ -38,17 +38,10 @@ __device__ __forceinline__ float ldgS(const float *p, long long e, float s) {
     if constexpr (PREC == PREC_F16_SR) return __half2float(__ldg(reinterpret_cast<const __half *>(p) + e)) * s;
     else return __ldg(p + e);
 }
-// FP16 stores also raise *mx to the largest stored magnitude (the stress
-// update's share of the re-centring: swpc_prec.cu)
 template <int PREC>
-__device__ __forceinline__ void stS(float *p, long long e, float v, float is, float *mx) {
-    if constexpr (PREC == PREC_F16_SR) {
-        const __half h = __float2half_rn(v * is);
-        __stcs(reinterpret_cast<__half *>(p) + e, h);
-        *mx = fmaxf(*mx, fabsf(__half2float(h)));
-    } else {
-        __stcs(p + e, v);
-    }
+__device__ __forceinline__ void stS(float *p, long long e, float v, float is) {
+    if constexpr (PREC == PREC_F16_SR) __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
+    else __stcs(p + e, v);
 }
 template <int PREC>
 __device__ __forceinline__ float ldR(const float *p, long long e, float s) {
@@ -59,31 +52,11 @@ __device__ __forceinline__ float ldR(const float *p, long long e, float s) {
     else return __ldcs(p + e);
 }
 template <int PREC>
-__device__ __forceinline__ void stR(float *p, long long e, float v, float is, float *mx) {
-    if constexpr (PREC == PREC_F16_SR || PREC == PREC_F16_R) {
-        const __half h = __float2half_rn(v * is);
-        __stcs(reinterpret_cast<__half *>(p) + e, h);
-        *mx = fmaxf(*mx, fabsf(__half2float(h)));
-    } else if constexpr (PREC == PREC_BF16_R) {
-        __stcs(reinterpret_cast<__nv_bfloat16 *>(p) + e, __float2bfloat16_rn(v));
-    } else {
-        __stcs(p + e, v);
-    }
-}
-
-// FP16 forms: fold this thread's stored maxima (mx[0] stresses, mx[1] memory
-// variables) into the launch's, one atomic per warp and only when larger
-template <int PREC>
-__device__ __forceinline__ void flush_max(unsigned int *dmax, const float *mx) {
-    if constexpr (PREC == PREC_F16_SR || PREC == PREC_F16_R) {
-        const unsigned int act = __activemask();
-        const unsigned int ms = __reduce_max_sync(act, __float_as_uint(mx[0]));
-        const unsigned int mr = __reduce_max_sync(act, __float_as_uint(mx[1]));
-        if ((threadIdx.x & 31) == __ffs(act) - 1) {   // blockDim.x is 32: the lane is threadIdx.x
-            if (ms > *reinterpret_cast<volatile unsigned int *>(dmax)) atomicMax(dmax, ms);
-            if (mr > *reinterpret_cast<volatile unsigned int *>(dmax + 1)) atomicMax(dmax + 1, mr);
-        }
-    }
+__device__ __forceinline__ void stR(float *p, long long e, float v, float is) {
+    if constexpr (PREC == PREC_F16_SR || PREC == PREC_F16_R)
+        __stcs(reinterpret_cast<__half *>(p) + e, __float2half_rn(v * is));
+    else if constexpr (PREC == PREC_BF16_R) __stcs(reinterpret_cast<__nv_bfloat16 *>(p) + e, __float2bfloat16_rn(v));
+    else __stcs(p + e, v);
 }
 
 // 2nd-order band of the free surface / ocean bottom (m_kernel.f90:103-108):
@@ -159,8 +132,7 @@ struct GStrOps {
     __device__ __forceinline__ float v(int c, int dk, int di, int dj) const {
         return __ldg(&V[c][e + dk + di * PI + dj * PJ]);
     }
-    float *mx;   // FP16: stored maxima (stresses, memory variables)
-    __device__ __forceinline__ float sown(int f) const { return ldS<PREC>(S[f], e, sc_sS_in(a.scale)); }
+    __device__ __forceinline__ float sown(int f) const { return ldS<PREC>(S[f], e, sc_sS_in(a.scale, f)); }
     __device__ __forceinline__ float r(int q) const { return ldR<PREC>(a.R[q] + so, e, sc_sR_in(a.scale)); }
     // 0 mu, 1 lam, 2 taup, 3 taus, 4 muyz, 5 muxz, 6 muxy
     __device__ __forceinline__ float med(int m) const {
@@ -223,9 +195,9 @@ __device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o,
     }
     const float taup_plus1 = 1 + taup1 * (1 + a.d2);
     const float taus_plus1 = 1 + taus1 * (1 + a.d2);
-    stS<PREC>(S[0], e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, sc_iS(a.scale, 0), o.mx);
-    stS<PREC>(S[1], e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, sc_iS(a.scale, 1), o.mx);
-    stS<PREC>(S[2], e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, sc_iS(a.scale, 2), o.mx);
+    stS<PREC>(S[0], e, sxx + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dyVy_dzVz + Rxx_n) * dt, sc_iS(a.scale, 0));
+    stS<PREC>(S[1], e, syy + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dzVz + Ryy_n) * dt, sc_iS(a.scale, 1));
+    stS<PREC>(S[2], e, szz + (lam2mu * taup_plus1 * d3v3 - mu2 * taus_plus1 * dxVx_dyVy + Rzz_n) * dt, sc_iS(a.scale, 2));
 
     // shear components (m_kernel.f90:282-311)
     const float dxVy_dyVx = (vyip - vy0) * re40x - (vyip2 - vyim) * re41x
@@ -244,13 +216,13 @@ __device__ __forceinline__ void stress_interior(const Str3Args &a, const Ops &o,
         Rxz_n = Rxz_n + a.d1[m] * r[4][m];
         Rxy_n = Rxy_n + a.d1[m] * r[5][m];
     }
-    stS<PREC>(S[3], e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, sc_iS(a.scale, 3), o.mx);
-    stS<PREC>(S[4], e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, sc_iS(a.scale, 4), o.mx);
-    stS<PREC>(S[5], e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, sc_iS(a.scale, 5), o.mx);
+    stS<PREC>(S[3], e, syz + (muyz * taus_plus1 * dyVz_dzVy + Ryz_n) * dt, sc_iS(a.scale, 3));
+    stS<PREC>(S[4], e, sxz + (muxz * taus_plus1 * dxVz_dzVx + Rxz_n) * dt, sc_iS(a.scale, 4));
+    stS<PREC>(S[5], e, sxy + (muxy * taus_plus1 * dxVy_dyVx + Rxy_n) * dt, sc_iS(a.scale, 5));
 #pragma unroll
     for (int c = 0; c < 6; c++)
 #pragma unroll
-        for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], sc_iR(a.scale, c * 3 + m), o.mx + 1);
+        for (int m = 0; m < NM; m++) stR<PREC>(a.R[c * 3 + m] + so, e, r[c][m], sc_iR(a.scale, c * 3 + m));
 }
 
 // absorb_p__update_vel (m_absorb_p.f90:248-309) for one absorber cell: the
@@ -371,9 +343,9 @@ __device__ __forceinline__ void stress_absorber(const Str3Args &a, const Ops &o,
     const float dxVx_ade = gxc.x * dxVx + gxc.y * vaxVx;
     const float dyVy_ade = gyc.x * dyVy + gyc.y * vayVy;
     const float dzVz_ade = gzc.x * dzVz + gzc.y * vazVz;
-    stS<PREC>(S[0], e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, sc_iS(a.scale, 0), o.mx);
-    stS<PREC>(S[1], e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, sc_iS(a.scale, 1), o.mx);
-    stS<PREC>(S[2], e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, sc_iS(a.scale, 2), o.mx);
+    stS<PREC>(S[0], e, sxx + (lam2mu_R * dxVx_ade + lam_R * (dyVy_ade + dzVz_ade)) * dt, sc_iS(a.scale, 0));
+    stS<PREC>(S[1], e, syy + (lam2mu_R * dyVy_ade + lam_R * (dxVx_ade + dzVz_ade)) * dt, sc_iS(a.scale, 1));
+    stS<PREC>(S[2], e, szz + (lam2mu_R * dzVz_ade + lam_R * (dxVx_ade + dyVy_ade)) * dt, sc_iS(a.scale, 2));
     sts(&axVx[q], gxc.z * vaxVx + gxc.w * dxVx * dt);
     sts(&ayVy[q], gyc.z * vayVy + gyc.w * dyVy * dt);
     sts(&azVz[q], gzc.z * vazVz + gzc.w * dzVz * dt);
@@ -384,9 +356,9 @@ __device__ __forceinline__ void stress_absorber(const Str3Args &a, const Ops &o,
     const float dyVz = (vzjp - vz0) * r20y;
     const float dzVx = (vxkp - vx0) * r20z;
     const float dzVy = (vykp - vy0) * r20z;
-    stS<PREC>(S[3], e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, sc_iS(a.scale, 3), o.mx);
-    stS<PREC>(S[4], e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, sc_iS(a.scale, 4), o.mx);
-    stS<PREC>(S[5], e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, sc_iS(a.scale, 5), o.mx);
+    stS<PREC>(S[3], e, syz + muyz * (gye.x * dyVz + gze.x * dzVy + gye.y * vayVz + gze.y * vazVy) * dt, sc_iS(a.scale, 3));
+    stS<PREC>(S[4], e, sxz + muxz * (gxe.x * dxVz + gze.x * dzVx + gxe.y * vaxVz + gze.y * vazVx) * dt, sc_iS(a.scale, 4));
+    stS<PREC>(S[5], e, sxy + muxy * (gxe.x * dxVy + gye.x * dyVx + gxe.y * vaxVy + gye.y * vayVx) * dt, sc_iS(a.scale, 5));
     sts(&ayVx[q], gye.z * vayVx + gye.w * dyVx * dt);
     sts(&azVx[q], gze.z * vazVx + gze.w * dzVx * dt);
     sts(&axVy[q], gxe.z * vaxVy + gxe.w * dxVy * dt);
@@ -444,8 +416,8 @@ __device__ __forceinline__ void vel_cell(const Vel3Args &a, int k, int i, int j,
 // One cell (k, i, j) of the fused stress and memory-variable update; like
 // vel_cell, every load of the cell is issued before its first store.
 template <int NM, int PREC>
-__device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int j, long long so, long long ao,
-                                            float *mx) {
+__device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int j, long long so = 0,
+                                            long long ao = 0) {
     const Geo g = a.g;
     const long long col = col_index(g, i, j);
     const long long e = col * g.Kp + (k - 1 + KH);
@@ -464,7 +436,7 @@ __device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int
 
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         if (!(a.mask & 1)) return;
-        const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}, mx};
+        const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}};
         float *const Sp[6] = {Sxx, Syy, Szz, Syz, Sxz, Sxy};
         stress_interior<NM, PREC>(a, o, band_sign_of(a.band, col, k), Sp, e, so);
         return;
@@ -473,7 +445,7 @@ __device__ __forceinline__ void stress_cell(const Str3Args &a, int k, int i, int
     // absorber cell (m_absorb_p.f90:445-491)
     if (!(a.mask & 2)) return;
     const Aux9 x = aux_load(a.aV, ao, a.pmlcol, g, k, i, j);
-    const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}, mx};
+    const GStrOps<NM, PREC> o{a, e, PI, PJ, so, {Vx, Vy, Vz}, {Sxx, Syy, Szz, Syz, Sxz, Sxy}};
     float *const Sp[6] = {Sxx, Syy, Szz, Syz, Sxz, Sxy};
     stress_absorber<PREC>(a, o, x, k, i, j, e, ao, Sp);
 }

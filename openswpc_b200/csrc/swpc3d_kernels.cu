@@ -48,9 +48,7 @@ __global__ void __launch_bounds__(256, MINB) stress3d_kernel(const Str3Args a) {
     const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int j = 1 + blockIdx.z * blockDim.z + threadIdx.z;
     if (k > g.nz || i > g.nx || j > g.ny) return;
-    float mx[2] = {0.0f, 0.0f};
-    stress_cell<NM, PREC>(a, k, i, j, 0, 0, mx);
-    flush_max<PREC>(a.dmax, mx);
+    stress_cell<NM, PREC>(a, k, i, j);
 }
 
 // MINB (minimum resident blocks per SM) trades registers for occupancy; the

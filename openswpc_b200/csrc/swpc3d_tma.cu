@@ -89,13 +89,12 @@ struct SStrOps {
     const float *sm;   // medium box: lam mu taup taus muyz muxz muxy
     int tx, ty, tz;
     const Str3Args &a;   // FP16 scales of S and R (PREC_F16_SR)
-    float *mx;           // FP16: stored maxima (stresses, memory variables)
     __device__ __forceinline__ int at(int f) const { return ((f * BJ + tz) * BI + ty) * KT + tx; }
     __device__ __forceinline__ float v(int c, int dk, int di, int dj) const {
         return sv[((c * (BJ + 4) + tz + 2 + dj) * (BI + 4) + ty + 2 + di) * KB + tx + 4 + dk];
     }
     __device__ __forceinline__ float sown(int f) const {
-        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(f)]) * sc_sS_in(a.scale);
+        if constexpr (PREC == PREC_F16_SR) return __half2float(reinterpret_cast<const __half *>(ss)[at(f)]) * sc_sS_in(a.scale, f);
         else return ss[at(f)];
     }
     __device__ __forceinline__ float r(int q) const {
@@ -172,13 +171,12 @@ __global__ void __launch_bounds__(KT * BI * BJ,
     }
     __syncthreads();   // barrier initialised, wait limit set
     if (!wait_tiles(&bar, t.err, limit) || !mine) return;   // the copy failed, or no cell of this launch here
-    float mx[2] = {0.0f, 0.0f};
 #pragma unroll
     for (int mm = 0; mm < M; mm++) {
         if (mm >= T.nmem) break;
         const long long so = (long long)(T.m0 + mm) * t.so, ao = (long long)(T.m0 + mm) * t.ao;
         const float *p = sm + L::oMem(mm);
-        const SStrOps<NM, BI, BJ, PREC> o{p, p + up32(L::nState), sm, tx, ty, tz, a, mx};
+        const SStrOps<NM, BI, BJ, PREC> o{p, p + up32(L::nState), sm, tx, ty, tz, a};
         float *const Sp[6] = {a.Sxx + so, a.Syy + so, a.Szz + so, a.Syz + so, a.Sxz + so, a.Sxy + so};
         if (interior) {
             stress_interior<NM, PREC>(a, o, sgn, Sp, e, so);
@@ -187,7 +185,6 @@ __global__ void __launch_bounds__(KT * BI * BJ,
             stress_absorber<PREC>(a, o, x, k, i, j, e, ao, Sp);
         }
     }
-    flush_max<PREC>(a.dmax, mx);
 }
 
 // ---------------------------------------------------------------------------

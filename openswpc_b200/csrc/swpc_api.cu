@@ -1118,7 +1118,6 @@ static int launch_stress_kernel(swpc_ctx *c, int mask) {
     a.dt = c->d.dt;
     a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
     a.scale = c->d_scale;
-    a.dmax = c->d_rmax;
     dim3 block(32, c->bi, c->bj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->bi - 1) / c->bi, (c->g.ny + c->bj - 1) / c->bj);
     if (c->stress_tma && c->slab) {
@@ -1294,7 +1293,7 @@ static int step_half0(swpc_ctx *c, int it, const int *d_it, bool record) {
         RC(green_store_launch(c, it, d_it));
         RC(snap_launch(c, it, d_it));
     }
-    RC(rescale_before_stress(c));   // FP16 forms: re-centre the scales, on the device (swpc_prec.cu)
+    RC(rescale_before_stress(c, it, d_it));   // FP16 forms: re-centre the scales, on the device (swpc_prec.cu)
     RC(launch_stress(c, 3));
     RC(rescale_after_stress(c));
     return launch_glut(c, it, d_it);

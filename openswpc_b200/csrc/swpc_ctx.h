@@ -69,7 +69,7 @@ struct swpc_ctx {
     // re-centring kernels of swpc_prec.cu keep them
     float *d_scale = nullptr;
     float h_scale[48];
-    int *d_exp = nullptr;                  // group exponents: stresses, memory variables
+    int *d_exp = nullptr;                  // exponents: each stress array, the memory variables
     unsigned int *d_rmax = nullptr;        // re-centring scratch: maxima, factors, moved count
     float *d_rfactor = nullptr;
     int *d_rchanged = nullptr;
@@ -217,7 +217,7 @@ int set_err(swpc_ctx *c, int code, const std::string &msg);
 // 2 na must fit the grid across x and y (the whole grid for a block of a
 // decomposed one); refused when the medium arrives
 int upload_scales(swpc_ctx *c);   // swpc_api.cu
-int rescale_before_stress(swpc_ctx *c);   // swpc_prec.cu
+int rescale_before_stress(swpc_ctx *c, int it, const int *d_it);   // swpc_prec.cu
 int rescale_after_stress(swpc_ctx *c);
 inline int check_na_wide(swpc_ctx *c) {
     return c->na_wide ? set_err(c, SWPC_ERR_ARG, "absorber thickness na too large for the grid") : SWPC_OK;

@@ -103,8 +103,7 @@ template <int NM>
 __global__ void __launch_bounds__(256, 2) stress3d_batch_kernel(const Str3Args a, const BatchGrid bg) {
     int m, k, i, j;
     if (!batch_cell(bg, a.g, m, k, i, j)) return;
-    float mx[2];   // FP32: unused
-    stress_cell<NM, PREC_F32>(a, k, i, j, m * bg.stride, m * bg.astride, mx);
+    stress_cell<NM, PREC_F32>(a, k, i, j, m * bg.stride, m * bg.astride);
 }
 
 __global__ void __launch_bounds__(256, 3) vel3d_batch_kernel(const Vel3Args a, const BatchGrid bg) {
@@ -432,7 +431,6 @@ static int fb_step_body(swpc_fbatch *b, int it, const int *d_it) {
         a.d2 = c->d2;
         a.dt = c->d.dt;
         a.mask = mask;
-        a.dmax = c->d_rmax;     // FP32: the stress kernels keep no maxima
         a.scale = c->d_scale;   // FP32 storage: every scale 1
         if (b->staged) {
             FRC(fb_tma_ready(b));

@@ -10,24 +10,24 @@ namespace swpc {
 enum InjMode { INJ_GLUT = 0, INJ_GLUT4 = 1, INJ_GLUT2 = 2, INJ_BF3 = 3, INJ_GREEN = 4, INJ_BFPSV = 5, INJ_BFSH = 6 };
 
 // Power-of-two scales of the FP16 storage forms, in device memory (so that
-// re-centring them needs no new launch arguments): value = stored * sS for
-// the stresses, stored = value * iS, and likewise sR, iR for the memory
-// variables.  One scale per group: FP16 keeps 11 significant bits over 29
-// binades, so arrays of one group that differ by orders of magnitude lose
-// nothing by sharing it, and a kernel reads each scale from one read-only
-// address, which the compiler loads once.  Layout: [0] sS_in, [1] sR_in (what
-// the stored values meant before this step's stress update: only the stress
-// kernel reads them), [2] sS, [3] iS, [4] sR, [5] iR (what it writes, and what
-// every other kernel and transfer uses).  A re-centring changes [2..5] before
-// the stress update, which converts every stored value as it rewrites it; [0],
-// [1] follow after it.  FP32 storage keeps them 1.
+// re-centring them needs no new launch arguments): value = stored * sS[f]
+// for stress array f, stored = value * iS[f], and sR, iR for the memory
+// variables, which share one scale (FP16 keeps 11 significant bits over 29
+// binades, so arrays that differ by orders of magnitude lose nothing by
+// sharing it, and the stress kernel reads it from one read-only address).
+// Layout: [0..5] sS_in, [6] sR_in (what the stored values meant before this
+// step's stress update: only the stress kernel reads them), [7..12] sS,
+// [13..18] iS, [19] sR, [20] iR (what it writes, and what every other kernel
+// and transfer uses).  A re-centring changes the latter before the stress
+// update, which converts every value as it rewrites it; the former follow
+// after it.  FP32 storage keeps them 1.
 constexpr int kScaleFloats = 48;
-__device__ __forceinline__ float sc_sS_in(const float *s) { return __ldg(s); }
-__device__ __forceinline__ float sc_sR_in(const float *s) { return __ldg(s + 1); }
-__device__ __forceinline__ float sc_sS(const float *s, int) { return __ldg(s + 2); }
-__device__ __forceinline__ float sc_iS(const float *s, int) { return __ldg(s + 3); }
-__device__ __forceinline__ float sc_sR(const float *s, int) { return __ldg(s + 4); }
-__device__ __forceinline__ float sc_iR(const float *s, int) { return __ldg(s + 5); }
+__device__ __forceinline__ float sc_sS_in(const float *s, int f) { return __ldg(s + f); }
+__device__ __forceinline__ float sc_sR_in(const float *s) { return __ldg(s + 6); }
+__device__ __forceinline__ float sc_sS(const float *s, int f) { return __ldg(s + 7 + f); }
+__device__ __forceinline__ float sc_iS(const float *s, int f) { return __ldg(s + 13 + f); }
+__device__ __forceinline__ float sc_sR(const float *s, int) { return __ldg(s + 19); }
+__device__ __forceinline__ float sc_iR(const float *s, int) { return __ldg(s + 20); }
 
 struct Vel3Args {
     Geo g;
@@ -63,7 +63,6 @@ struct Str3Args {
     float dt;
     int mask;
     const float *scale;     // FP16 stress and memory-variable scales in device memory (see sc_sS)
-    unsigned int *dmax;     // FP16: largest stored magnitude written, stresses and memory variables (float bits)
 };
 
 struct InjArgs {
