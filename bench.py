@@ -470,6 +470,99 @@ def bench_c2b(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def bench_decomp(args, world, rank, local):
+    """The c4 grid split into blocks as the reference's MPI split lays them
+    out (m_global.f90:236-303, default 2 x 2), all blocks on one GPU, against
+    the single-domain run of the same grid: the decomposed step's rate with
+    the sleeve exchange after each half step, and the exchange's pack / unpack
+    kernels against HBM."""
+    px, py = (int(v) for v in args.split.lower().split("x"))
+    p = make_params("c4")
+    wl = {"workload": f"decomposed 3D forward: the 512x512x256 grid (nm=3, PML 32) split {px}x{py}, all blocks on one "
+                      f"GPU, sleeves exchanged through device buffers", "nx": p.nx, "ny": p.ny, "nz": p.nz,
+          "split": [px, py], "l2": "inputs larger than L2 (whole wavefield + medium resident)",
+          "parallelism": f"{px * py} blocks on one GPU"}
+    metric = "Gcell-updates/s (3D visco, FP32)"
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference splits a grid only through its MPI "
+                                                                  "build, which cannot be built here"}), flush=True)
+        return
+    if rank != 0:
+        return
+    import torch
+    from openswpc_b200 import _lib
+    from openswpc_b200.decomp import SIDES, Decomposed3D
+    from openswpc_b200.swpc3d import Medium, Swpc3D
+
+    cells = p.nx * p.ny * p.nz
+    xi = rmed(p, device=f"cuda:{local}")
+    med = Medium(p, xi)
+    torch.cuda.empty_cache()
+    # the single-domain run: graph replays of the step
+    g = Swpc3D(p, device=local, medium=med)
+    g.run(1, args.warmup)
+    ms1 = C.c_float()
+    _lib.check(g.ctx, g.lib.swpc_time_steps(g.ctx, 1 + args.warmup, args.steps, C.byref(ms1)))
+    ms_single = ms1.value / args.steps
+    g.close()
+    torch.cuda.empty_cache()
+    # the decomposed run: per block and half step a launch, then the exchange
+    d = Decomposed3D(p, px, py, medium=med, devices=[local] * (px * py))
+    for it in range(1, args.warmup + 1):
+        d.step(it)
+    for b in d.blocks:
+        b.sync()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for n in range(args.steps):
+            d.step(1 + args.warmup + n)
+        for b in d.blocks:
+            b.sync()
+        ms_dec = (time.perf_counter() - t0) * 1e3 / args.steps
+    # the exchange kernels of the block with the most neighbours, timed on its stream
+    b = max(d.blocks, key=lambda q: sum(n is not None for n in q.neighbours))
+    lib = b.lib
+    stream = torch.cuda.ExternalStream(lib.swpc_stream(b.ctx), device=local)
+    sides = [s for s in range(SIDES) if b.neighbours[s] is not None]
+    bufs = {(h, s): torch.empty(max(b.halo_count[h][s], b.halo_count[h][s ^ 1]), dtype=torch.float32,
+                                device=f"cuda:{local}") for h in (0, 1) for s in sides}
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.sync()
+    e0.record(stream)
+    for _ in range(reps):
+        for h in (0, 1):
+            for s in sides:
+                b.pack(h, s, bufs[h, s].data_ptr())
+            for s in sides:
+                b.unpack(h, s, bufs[h, s].data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms_halo = e0.elapsed_time(e1) / reps
+    # bytes of one step's exchange on this block: pack reads and writes its messages, unpack the same
+    floats = sum(b.halo_count[h][s] + b.halo_count[h][s ^ 1] for h in (0, 1) for s in sides)
+    halo_bytes = 2 * 4 * floats
+    peak, peak_kind = hbm_peak()
+    ach = halo_bytes / (ms_halo / 1e3) / 1e9
+    d.close()
+    line = {"metric": metric, "value": cells / (ms_dec / 1e3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dec, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered + von Karman medium)",
+            "config": wl,
+            "single_domain": {"value": cells / (ms_single / 1e3) / 1e9, "ms_per_step": ms_single,
+                              "what": "the same grid as one context, CUDA-graph replays"},
+            "decomposed_over_single": ms_single / ms_dec,
+            "exchange": {"block": [b.px, b.py], "sides": len(sides), "ms_per_step": ms_halo,
+                         "bytes_per_step": halo_bytes, "message_bytes_per_step": 4 * floats,
+                         "achieved_gbs": ach, "peak": peak, "peak_kind": peak_kind, "frac": ach / peak,
+                         "what": "pack + unpack kernels of both half steps on one block, CUDA events on its stream"},
+            "timing": "wall clock around the steps (the in-process exchange synchronises the blocks' streams after "
+                      "each pack and unpack round)",
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def Params_copy(p):
     from openswpc_b200.params import Params
 
@@ -814,7 +907,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c4", "c2a", "c2b", "c3", "decomp"])
+    ap.add_argument("--split", default="2x2", help="decomp: blocks along x and y (nproc_x x nproc_y)")
     ap.add_argument("--models", type=int, default=64, help="c2a: the first N of the 64 models (profiling runs)")
     ap.add_argument("--only-model", type=int, default=None, help="c2a: model I of the 64 alone (profiling runs)")
     ap.add_argument("--sweep", action="store_true",
@@ -844,6 +938,8 @@ def main():
         return bench_c3(args, world, rank, local)
     if args.workload == "c2b":
         return bench_c2b(args, world, rank, local)
+    if args.workload == "decomp":
+        return bench_decomp(args, world, rank, local)
     p = make_params(args.workload)
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.lower().split("x"))

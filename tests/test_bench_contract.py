@@ -46,3 +46,8 @@ def test_reference_arm_prints_the_contract_line(workload):
 def test_reference_arm_without_an_adjoint_says_so():
     line = run_reference("c3")
     assert line == {"impl": "reference", "unavailable": "the reference has no adjoint or gradient path"}
+
+
+def test_reference_arm_of_the_decomposition_says_so():
+    line = run_reference("decomp")
+    assert line["impl"] == "reference" and "MPI" in line["unavailable"]
