@@ -243,7 +243,8 @@ class _Run:
 
 class _InProcess(_Run):
     """All blocks in this process; the halo messages travel through device
-    buffers, across devices by copy."""
+    buffers (on one device ordered by events between the blocks' streams,
+    across devices by copy with host waits)."""
 
     def _buffers(self):
         import torch
@@ -256,8 +257,33 @@ class _InProcess(_Run):
                     if nbr is not None:
                         self.buf[r, half, side] = torch.empty(b.halo_count[half][side], dtype=torch.float32,
                                                               device=f"cuda:{b.device}")
+        # blocks on one device trade their messages without the host: each
+        # block's stream waits for its neighbours' pack kernels (an event) before
+        # it unpacks; a neighbour overwrites a message only after the next
+        # exchange, which in turn waited for this block's later pack
+        self.one_device = len({b.device for b in self.blocks}) == 1
+        self.streams = [torch.cuda.ExternalStream(b.lib.swpc_stream(b.ctx), device=f"cuda:{b.device}")
+                        for b in self.blocks]
 
     def _exchange(self, half: int):
+        if self.one_device:
+            import torch
+
+            packed = []
+            for r, b in enumerate(self.blocks):
+                for side, nbr in enumerate(b.neighbours):
+                    if nbr is not None:
+                        b.pack(half, side, self.buf[r, half, side].data_ptr())
+                ev = torch.cuda.Event()
+                ev.record(self.streams[r])
+                packed.append(ev)
+            for r, b in enumerate(self.blocks):
+                for side, nbr in enumerate(b.neighbours):
+                    if nbr is None:
+                        continue
+                    self.streams[r].wait_event(packed[nbr])
+                    b.unpack(half, side, self.buf[nbr, half, OPPOSITE[side]].data_ptr())
+            return
         for r, b in enumerate(self.blocks):
             for side, nbr in enumerate(b.neighbours):
                 if nbr is not None:
@@ -300,7 +326,13 @@ class _InProcess(_Run):
             out[idx] = w
         return out
 
+    def sync(self):
+        for b in self.blocks:
+            b.sync()
+
     def close(self):
+        for b in self.blocks:
+            b.sync()
         for b in self.blocks:
             b.close()
         self.blocks = []
