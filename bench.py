@@ -557,8 +557,8 @@ def bench_decomp(args, world, rank, local):
                          "bytes_per_step": halo_bytes, "message_bytes_per_step": 4 * floats,
                          "achieved_gbs": ach, "peak": peak, "peak_kind": peak_kind, "frac": ach / peak,
                          "what": "pack + unpack kernels of both half steps on one block, CUDA events on its stream"},
-            "timing": "wall clock around the steps (the in-process exchange synchronises the blocks' streams after "
-                      "each pack and unpack round)",
+            "timing": "wall clock around the steps, the host waiting for the blocks only at the end (the exchange "
+                      "orders the blocks' streams by events)",
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
