@@ -554,10 +554,11 @@ class BlockRank3D(_Run):
     the neighbour ranks through ``HaloTransport``: device buffers with NCCL,
     host copies of them with a backend that moves host tensors (gloo).
     Traces and fields stay with their block; ``vmax`` reduces over the ranks
-    (report__progress's mpi_reduce)."""
+    (report__progress's mpi_reduce).  ``kind`` "psv" or "sh" runs a 2D block
+    of an nproc_x split (nproc_y = 1) the same way."""
 
     def __init__(self, p: Params, nproc_x: int, nproc_y: int, xi=None, device: int = 0,
-                 medium: Medium | None = None, precision: str = "f32"):
+                 medium: Medium | None = None, precision: str = "f32", kind: str = "3d"):
         import torch
         import torch.distributed as dist
 
@@ -566,8 +567,14 @@ class BlockRank3D(_Run):
         rank, world = dist.get_rank(), dist.get_world_size()
         if world != nproc_x * nproc_y:
             raise ValueError("the world size must equal nproc_x * nproc_y")
-        self.sh = _Shared(p, xi, medium)
-        self.block = Block3D(self.sh, rank % nproc_x, rank // nproc_x, nproc_x, nproc_y, device, precision)
+        if kind == "3d":
+            self.sh = _Shared(p, xi, medium)
+            self.block = Block3D(self.sh, rank % nproc_x, rank // nproc_x, nproc_x, nproc_y, device, precision)
+        else:
+            if nproc_y != 1:
+                raise ValueError("the 2D codes split across x only (nproc_y = 1)")
+            self.sh = _Shared2D(p, kind)
+            self.block = Block2D(self.sh, rank, nproc_x, device)
         self.transport = HaloTransport(self.block.neighbours)
         dev = f"cuda:{device}"
         b = self.block

@@ -8,8 +8,9 @@ one GPU.
   single-domain run's bits: every trace, every cell of V, S and the memory
   variables, every report; with sources and stations on the block seams,
   with the Cerjan sponge and with body forces;
-* BlockRank3D, one block per process: two gloo ranks on the one GPU (the
-  messages staged through host memory; no kernel waits on another).
+* BlockRank3D, one block per process (3D, and a P-SV block): two gloo ranks
+  on the one GPU (the messages staged through host memory; no kernel waits on
+  another).
 """
 import os
 import subprocess
@@ -47,6 +48,23 @@ def decomp_case(**kw):
                                Station(0.0, 0.0, 0.0, "s00", "fsb")]
     xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
     return p, xi
+
+
+FIELDS_PSV = [_lib.F_VX, _lib.F_VZ, _lib.F_SXX, _lib.F_SZZ, _lib.F_SXZ]
+
+
+def decomp_case_2d(kind):
+    """A 124 x 60 P-SV or SH run with sources and stations on the seams of a
+    3-way split (cells 41|42 and 82|83) and of a 2-way split (62|63)."""
+    from tests.models import small2d
+
+    p = small2d(kind, nx=124, nz=60, na=10, nt=80)
+    for n, i in enumerate((41, 42, 82, 63)):
+        s = p.sources[0]
+        p.sources.append(type(s)(**{**s.__dict__, "x": float(p.xbeg + (i - 0.3) * p.dx), "z": 3.0 + n}))
+        st = p.stations[0]
+        p.stations.append(type(st)(**{**st.__dict__, "x": float(p.xbeg + (i - 0.5) * p.dx), "name": f"seam{n}"}))
+    return p
 
 
 def assert_same_bits(a, b, what):
@@ -129,16 +147,28 @@ def test_decomposed_variants(variant):
     d.close()
 
 
-def test_block_ranks_over_gloo_on_one_gpu(tmp_path):
-    p, xi = decomp_case()
-    ref = single_run(p, xi)
+@pytest.mark.parametrize("kind", ["3d", "psv"])
+def test_block_ranks_over_gloo_on_one_gpu(tmp_path, kind):
+    if kind == "3d":
+        p, xi = decomp_case()
+        ref = single_run(p, xi)
+    else:
+        from openswpc_b200.swpc2d import Swpc2D
+
+        p = decomp_case_2d(kind)
+        g = Swpc2D(p, kind)
+        g.run(1, p.nt)
+        ref = {"wav": g.waveforms(_lib.WAV_V)}
+        for f in FIELDS_PSV:
+            ref[f] = g.download(f)
+        g.close()
     worker = Path(__file__).resolve().parent / "decomp_rank_worker.py"
     port = free_port()
     procs = []
     for rank in range(2):
         env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank),
                    LOCAL_RANK=str(rank))
-        procs.append(subprocess.Popen([sys.executable, str(worker), "2", "1", str(tmp_path)], env=env,
+        procs.append(subprocess.Popen([sys.executable, str(worker), "2", "1", str(tmp_path), kind], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
     for pr in procs:
         _, err = pr.communicate(timeout=600)
@@ -149,10 +179,14 @@ def test_block_ranks_over_gloo_on_one_gpu(tmp_path):
         wav[z["stations"]] = z["wav"]
         ib, ie, jb, je = (int(v) for v in z["ext"])
         assert (ib, ie) == block_range(p.nx, 2, rank)
-        for f in FIELDS:
+        for f in (FIELDS if kind == "3d" else FIELDS_PSV):
             a = z[f"f{f}"]
-            assert_same_bits(a[3:-3, 3:-3, :], ref[f][jb + 2:je + 3, ib + 2:ie + 3, :], f"rank {rank} field {f}")
-        assert_same_bits(z["reports"], ref["reports"], "reports")
+            if kind == "3d":
+                assert_same_bits(a[3:-3, 3:-3, :], ref[f][jb + 2:je + 3, ib + 2:ie + 3, :], f"rank {rank} field {f}")
+            else:
+                assert_same_bits(a[3:-3, :], ref[f][ib + 2:ie + 3, :], f"rank {rank} field {f}")
+        if kind == "3d":
+            assert_same_bits(z["reports"], ref["reports"], "reports")
     assert_same_bits(wav, ref["wav"], "traces")
 
 
@@ -162,15 +196,8 @@ def test_decomposed_2d_run_gives_the_single_domain_bits(kind):
     global__comm_*), with sources and stations on the seams."""
     from openswpc_b200.decomp import Decomposed2D
     from openswpc_b200.swpc2d import Swpc2D
-    from tests.models import small2d
 
-    p = small2d(kind, nx=124, nz=60, na=10, nt=80)
-    # block seams of a 3-way split of 124 cells: 41|42 and 82|83 (x = xbeg + i dx)
-    for n, i in enumerate((41, 42, 82)):
-        s = p.sources[0]
-        p.sources.append(type(s)(**{**s.__dict__, "x": float(p.xbeg + (i - 0.3) * p.dx), "z": 3.0 + n}))
-        st = p.stations[0]
-        p.stations.append(type(st)(**{**st.__dict__, "x": float(p.xbeg + (i - 0.5) * p.dx), "name": f"seam{n}"}))
+    p = decomp_case_2d(kind)
     g = Swpc2D(p, kind)
     g.run(1, p.nt)
     d = Decomposed2D(p, kind, 3)
