@@ -30,10 +30,6 @@
 
 #include "swpc_ctx.h"
 
-namespace swpc {
-int graph_invalidate(swpc_ctx *c);
-}
-
 using namespace swpc;
 
 namespace {
