@@ -319,6 +319,11 @@ int swpc_step_half(swpc_ctx *ctx, int it, int half);
 int swpc_halo_count(swpc_ctx *ctx, int half, int side, long long *count);
 int swpc_halo_pack(swpc_ctx *ctx, int half, int side, float *dst);
 int swpc_halo_unpack(swpc_ctx *ctx, int half, int side, const float *src);
+/* Lets kernels on `device` store to memory of `peer` (cudaDeviceEnablePeerAccess),
+ * so that swpc_halo_pack can write a message straight into the receive buffer
+ * of a neighbour on another GPU of this process (NVLink peer stores).
+ * SWPC_ERR_CUDA when the pair has no peer access. */
+int swpc_enable_peer_access(int device, int peer);
 /* Plane-wave mode (pw_mode, src/swpc_3d/m_source.f90:67-79): with on != 0
  * the absorber updates first extrapolate the ghost planes of the four side
  * faces from inside (V before the stress update, S before the velocity

@@ -52,6 +52,7 @@ EXPORTS = [
     "swpc_vmodel_lhm", "swpc_vmodel_lhm_opt", "swpc_seawater_vel", "swpc_setup_medium", "swpc_damping_profiles", "swpc_setup_medium_2d", "swpc_cerjan_profiles",
     "swpc_setup_medium_opt", "swpc_setup_medium_2d_opt", "swpc_rmedia_generate", "swpc_pw_setup", "swpc_set_pw_mode", "swpc_clear_error", "swpc_raise_copy_error",
     "swpc_set_subdomain", "swpc_step_half", "swpc_halo_count", "swpc_halo_pack", "swpc_halo_unpack",
+    "swpc_enable_peer_access",
     "swpc_batch_create", "swpc_batch_step", "swpc_batch_run", "swpc_batch_sync", "swpc_batch_time_steps", "swpc_batch_autotune",
     "swpc_batch_set_shape", "swpc_batch_set_staged", "swpc_batch_get_launch",
     "swpc_fbatch_create", "swpc_fbatch_destroy", "swpc_fbatch_green_source", "swpc_fbatch_set_strip",
@@ -210,6 +211,7 @@ def load():
         "swpc_halo_count": (i, [vp, i, i, C.POINTER(C.c_longlong)]),
         "swpc_halo_pack": (i, [vp, i, i, vp]),
         "swpc_halo_unpack": (i, [vp, i, i, vp]),
+        "swpc_enable_peer_access": (i, [i, i]),
         "swpc_clear_error": (i, [vp]),
         "swpc_raise_copy_error": (i, [vp]),
         "swpc_batch_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),

@@ -222,3 +222,23 @@ extern "C" int swpc_halo_unpack(swpc_ctx *c, int half, int side, const float *sr
     if (!c) return SWPC_ERR_ARG;
     return halo_run(c, half, side, const_cast<float *>(src), false);
 }
+
+// Lets kernels running on `device` store to (and load from) memory of `peer`,
+// so that a block's pack kernel can write its message straight into a
+// neighbour's receive buffer on another GPU (NVLink peer stores).  Returns
+// SWPC_ERR_CUDA when the pair has no peer access; enabling it twice is fine.
+extern "C" int swpc_enable_peer_access(int device, int peer) {
+    if (device == peer) return SWPC_OK;
+    int can = 0;
+    if (cudaDeviceCanAccessPeer(&can, device, peer) != cudaSuccess || !can) return SWPC_ERR_CUDA;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    cudaError_t e = cudaDeviceEnablePeerAccess(peer, 0);
+    if (e == cudaErrorPeerAccessAlreadyEnabled) {
+        cudaGetLastError();   // the call left this as the last error: clear it
+        e = cudaSuccess;
+    }
+    cudaSetDevice(cur);
+    return e == cudaSuccess ? SWPC_OK : SWPC_ERR_CUDA;
+}

@@ -242,67 +242,53 @@ class _Run:
 
 
 class _InProcess(_Run):
-    """All blocks in this process; the halo messages travel through device
-    buffers (on one device ordered by events between the blocks' streams,
-    across devices by copy with host waits)."""
+    """All blocks in this process.  Every message goes into a receive buffer
+    on the receiving block's device: a block's pack kernel stores it there
+    directly (NVLink peer stores when the neighbour sits on another GPU), an
+    event on the sender's stream marks it complete, and the receiver's stream
+    waits for that event before its unpack kernel.  The host never waits.  A
+    buffer is overwritten only by the sender's pack two exchanges later, which
+    its stream reaches only after waiting for the receiver's own later pack,
+    itself after the receiver's unpack: the order holds without more events."""
 
     def _buffers(self):
         import torch
 
-        # one outgoing buffer per (block, half, side with a neighbour), on the sender's device
+        # receive buffers: (receiver, half, side the message comes from), on the receiver's device
         self.buf = {}
         for r, b in enumerate(self.blocks):
             for half in (0, 1):
                 for side, nbr in enumerate(b.neighbours):
                     if nbr is not None:
-                        self.buf[r, half, side] = torch.empty(b.halo_count[half][side], dtype=torch.float32,
-                                                              device=f"cuda:{b.device}")
-        # blocks on one device trade their messages without the host: each
-        # block's stream waits for its neighbours' pack kernels (an event) before
-        # it unpacks; a neighbour overwrites a message only after the next
-        # exchange, which in turn waited for this block's later pack
-        self.one_device = len({b.device for b in self.blocks}) == 1
+                        self.buf[r, half, side] = torch.empty(b.halo_count[half][OPPOSITE[side]],
+                                                              dtype=torch.float32, device=f"cuda:{b.device}")
+        lib = self.blocks[0].lib if self.blocks else None
+        for b in self.blocks:
+            for nbr in b.neighbours:
+                if nbr is not None and self.blocks[nbr].device != b.device:
+                    if lib.swpc_enable_peer_access(b.device, self.blocks[nbr].device):
+                        raise RuntimeError(f"no peer access from cuda:{b.device} to cuda:{self.blocks[nbr].device}")
         self.streams = [torch.cuda.ExternalStream(b.lib.swpc_stream(b.ctx), device=f"cuda:{b.device}")
                         for b in self.blocks]
 
     def _exchange(self, half: int):
-        if self.one_device:
-            import torch
+        import torch
 
-            packed = []
-            for r, b in enumerate(self.blocks):
-                for side, nbr in enumerate(b.neighbours):
-                    if nbr is not None:
-                        b.pack(half, side, self.buf[r, half, side].data_ptr())
-                ev = torch.cuda.Event()
-                ev.record(self.streams[r])
-                packed.append(ev)
-            for r, b in enumerate(self.blocks):
-                for side, nbr in enumerate(b.neighbours):
-                    if nbr is None:
-                        continue
-                    self.streams[r].wait_event(packed[nbr])
-                    b.unpack(half, side, self.buf[nbr, half, OPPOSITE[side]].data_ptr())
-            return
+        packed = []
         for r, b in enumerate(self.blocks):
             for side, nbr in enumerate(b.neighbours):
                 if nbr is not None:
-                    b.pack(half, side, self.buf[r, half, side].data_ptr())
-        for b in self.blocks:
-            b.sync()
-        held = []   # copies across devices stay alive until the unpacks are done
+                    # into the neighbour's buffer for messages from the opposite side
+                    b.pack(half, side, self.buf[nbr, half, OPPOSITE[side]].data_ptr())
+            ev = torch.cuda.Event()
+            ev.record(self.streams[r])
+            packed.append(ev)
         for r, b in enumerate(self.blocks):
             for side, nbr in enumerate(b.neighbours):
                 if nbr is None:
                     continue
-                msg = self.buf[nbr, half, OPPOSITE[side]]
-                if msg.device.index != b.device:
-                    msg = msg.to(f"cuda:{b.device}")
-                    held.append(msg)
-                b.unpack(half, side, msg.data_ptr())
-        for b in self.blocks:
-            b.sync()
-        del held
+                self.streams[r].wait_event(packed[nbr])
+                b.unpack(half, side, self.buf[r, half, side].data_ptr())
 
     def step(self, it: int):
         for b in self.blocks:
@@ -368,7 +354,6 @@ class Decomposed3D(_InProcess):
             j1 = b.ny + 6 if b.je == p.ny else b.ny + 3
             out[b.joff + j0:b.joff + j1, b.ioff + i0:b.ioff + i1, :] = a[j0:j1, i0:i1, :]
         return out
-
 
 
 class _Shared2D:
