@@ -589,17 +589,15 @@ class BlockRank3D(_Run):
                 for s in sides:
                     b.unpack(half, s, self.recv[half, s].data_ptr())
             return
+        # a backend that moves host tensors: the messages staged through host memory
         for s in sides:
             b.pack(half, s, self.send[half, s].data_ptr())
         b.sync()
-        if self.staged:
-            send = {s: self.send[half, s].cpu() for s in sides}
-            recv = {s: self.recv[half, s].cpu() for s in sides}
-            self.transport.exchange(send, recv)
-            for s in sides:
-                self.recv[half, s].copy_(recv[s])
-        else:
-            self.transport.exchange({s: self.send[half, s] for s in sides}, {s: self.recv[half, s] for s in sides})
+        send = {s: self.send[half, s].cpu() for s in sides}
+        recv = {s: self.recv[half, s].cpu() for s in sides}
+        self.transport.exchange(send, recv)
+        for s in sides:
+            self.recv[half, s].copy_(recv[s])
         for s in sides:
             b.unpack(half, s, self.recv[half, s].data_ptr())
 

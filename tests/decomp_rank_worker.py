@@ -1,8 +1,11 @@
-"""One rank of the one-GPU test of BlockRank3D (tests/test_gpu_decomp.py):
-joins a gloo group from the torchrun-style environment, runs its block of the
-decomposed test case (3D, or P-SV with kind psv) on cuda:0 (the halo
-messages staged through host memory), and saves its traces, station indices,
-block extents, fields and report values to <outdir>/rank<r>.npz."""
+"""One rank of the BlockRank3D tests (tests/test_gpu_decomp.py): joins a
+gloo group (every rank on cuda:0, the halo messages staged through host
+memory) or an NCCL group (rank r on cuda:r, the messages device to device)
+from the torchrun-style environment, runs its block of the decomposed test
+case (3D, or P-SV with kind psv), and saves its traces, station indices,
+block extents, fields and report values to <outdir>/rank<r>.npz.
+
+usage: decomp_rank_worker.py nproc_x nproc_y outdir [kind [backend]]"""
 import sys
 from pathlib import Path
 
@@ -18,14 +21,16 @@ from tests.test_gpu_decomp import FIELDS, FIELDS_PSV, decomp_case, decomp_case_2
 def main():
     nproc_x, nproc_y, outdir = int(sys.argv[1]), int(sys.argv[2]), Path(sys.argv[3])
     kind = sys.argv[4] if len(sys.argv) > 4 else "3d"
-    ranks = replicas.init("gloo", timeout_s=120)
+    backend = sys.argv[5] if len(sys.argv) > 5 else "gloo"
+    ranks = replicas.init(backend, timeout_s=120)
+    device = ranks.local if backend == "nccl" else 0
     if kind == "3d":
         p, xi = decomp_case()
-        r = BlockRank3D(p, nproc_x, nproc_y, xi, device=0)
+        r = BlockRank3D(p, nproc_x, nproc_y, xi, device=device)
         fields = FIELDS
     else:
         p = decomp_case_2d(kind)
-        r = BlockRank3D(p, nproc_x, nproc_y, device=0, kind=kind)
+        r = BlockRank3D(p, nproc_x, nproc_y, device=device, kind=kind)
         fields = FIELDS_PSV
     rep = r.run(1, p.nt)
     b = r.block

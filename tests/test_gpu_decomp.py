@@ -11,6 +11,9 @@ one GPU.
 * BlockRank3D, one block per process (3D, and a P-SV block): two gloo ranks
   on the one GPU (the messages staged through host memory; no kernel waits on
   another).
+
+With two GPUs or more, the same 2 x 2 split with its blocks spread over two
+GPUs (peer stores) and two NCCL ranks on two GPUs run as well.
 """
 import os
 import subprocess
@@ -147,8 +150,30 @@ def test_decomposed_variants(variant):
     d.close()
 
 
-@pytest.mark.parametrize("kind", ["3d", "psv"])
-def test_block_ranks_over_gloo_on_one_gpu(tmp_path, kind):
+def multi_gpu():
+    import torch
+
+    return torch.cuda.device_count() >= 2
+
+
+@pytest.mark.skipif(not multi_gpu(), reason="needs two GPUs")
+def test_decomposed_run_across_two_gpus():
+    """The 2 x 2 split with the blocks on alternating GPUs: the pack kernels
+    store the messages into the neighbours' buffers over NVLink."""
+    p, xi = decomp_case()
+    ref = single_run(p, xi)
+    d = Decomposed3D(p, 2, 2, xi, devices=[0, 1, 1, 0])
+    rep = d.run(1, p.nt)
+    assert_same_bits(d.waveforms(_lib.WAV_V), ref["wav"], "traces")
+    for f in FIELDS:
+        assert_same_bits(d.download(f), ref[f], f"field {f}")
+    assert_same_bits(np.array([v for _, v in rep]), ref["reports"], "reports")
+    d.close()
+
+
+def block_ranks(tmp_path, kind, backend):
+    """Two ranks of BlockRank3D (a 2 x 1 split) against the single-domain
+    run: every trace, the block's cells of every field, every report."""
     if kind == "3d":
         p, xi = decomp_case()
         ref = single_run(p, xi)
@@ -168,7 +193,9 @@ def test_block_ranks_over_gloo_on_one_gpu(tmp_path, kind):
     for rank in range(2):
         env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank),
                    LOCAL_RANK=str(rank))
-        procs.append(subprocess.Popen([sys.executable, str(worker), "2", "1", str(tmp_path), kind], env=env,
+        if backend == "nccl":
+            env["NCCL_NVLS_ENABLE"] = "0"
+        procs.append(subprocess.Popen([sys.executable, str(worker), "2", "1", str(tmp_path), kind, backend], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
     for pr in procs:
         _, err = pr.communicate(timeout=600)
@@ -188,6 +215,19 @@ def test_block_ranks_over_gloo_on_one_gpu(tmp_path, kind):
         if kind == "3d":
             assert_same_bits(z["reports"], ref["reports"], "reports")
     assert_same_bits(wav, ref["wav"], "traces")
+
+
+@pytest.mark.parametrize("kind", ["3d", "psv"])
+def test_block_ranks_over_gloo_on_one_gpu(tmp_path, kind):
+    block_ranks(tmp_path, kind, "gloo")
+
+
+@pytest.mark.skipif(not multi_gpu(), reason="needs two GPUs")
+@pytest.mark.parametrize("kind", ["3d", "psv"])
+def test_block_ranks_over_nccl_on_two_gpus(tmp_path, kind):
+    """One rank per GPU, the halo messages stream-ordered NCCL point-to-point
+    transfers between the blocks' device buffers."""
+    block_ranks(tmp_path, kind, "nccl")
 
 
 @pytest.mark.parametrize("kind", ["psv", "sh"])
