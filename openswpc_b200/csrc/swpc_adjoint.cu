@@ -15,8 +15,11 @@
 //            cell adds its weight with the sign of the difference.
 // Receiver residuals enter as sources at the transposed recorder cells
 // (wav__store, src/swpc_3d/m_wav.f90:530-535).  The gradient imaging
-// condition pairs the adjoint with the forward derivatives of the same step
-// and accumulates in FP64; it is formed on the interior kernel region, whose
+// condition pairs the adjoint with the forward derivatives of the same step;
+// each step's term is formed in FP64 and added into an FP32 partial sum that
+// covers one checkpoint segment (at most ckpt steps), and every segment's
+// partials are folded into the FP64 totals (blocked summation: the FP32 sums
+// hold ckpt terms, the FP64 ones the segments).  It is formed on the interior kernel region, whose
 // cells are the model parameters (absorber cells copy the medium of the
 // interior edge and are not parameters).  swpc_gradient runs the forward with
 // checkpoints every `ckpt` steps, then per segment recomputes the forward
@@ -50,7 +53,8 @@ struct swpc_adj_state {
     int slab_nf = 0;
     swpc::TmaMaps *maps = nullptr;       // staged stress-phase weights: state, s6 (adjoint slab), med, vh (slots)
     float *w40[9] = {}, *w41[9] = {};    // difference-operator weights
-    double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz
+    double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz: FP64 totals
+    float *gpart[8] = {};                // the same, FP32 partial sums of the current segment
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
     int ckpt = 0, nseg = 0;
     float *ckpool = nullptr;             // checkpoints: V S R aux per segment
@@ -75,7 +79,7 @@ struct AdjVelArgs {
     float e40[3][2], e41[3][2], r20[3], dt;
     float *w40[9], *w41[9];
     const float *S[6];           // forward S after the stress update (gradient)
-    double *gb[3];               // gradient of bx, by, bz (null: none)
+    float *gb[3];                // segment partials of the bx, by, bz gradient (null: none)
 };
 
 struct AdjStrArgs {
@@ -92,7 +96,7 @@ struct AdjStrArgs {
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     float *w40[9], *w41[9];
     const float *V[3];           // forward V before the stress update (gradient)
-    double *gm[5];               // gradient of lam, mu, muyz, muxz, muxy (null: none)
+    float *gm[5];                // segment partials of the lam, mu, muyz, muxz, muxy gradient (null: none)
 };
 
 struct GatherArgs {
@@ -142,7 +146,7 @@ struct GAdjVelOps {
 };
 
 struct Gb3 {
-    double v[3];
+    float v[3];
 };
 __device__ __forceinline__ Gb3 gb_load(const AdjVelArgs &a, long long e) {
     Gb3 g;
@@ -178,9 +182,9 @@ __device__ __forceinline__ void adj_vel_cell(const AdjVelArgs &a, const O &o, lo
             const float d3Sz3 = (o.S(4, 0, 0, 0) - o.S(4, 0, -1, 0)) * re40x - (o.S(4, 0, 1, 0) - o.S(4, 0, -2, 0)) * re41x
                               + (o.S(3, 0, 0, 0) - o.S(3, 0, 0, -1)) * re40y - (o.S(3, 0, 0, 1) - o.S(3, 0, 0, -2)) * re41y
                               + (o.S(2, 1, 0, 0) - o.S(2, 0, 0, 0)) * re40z - (o.S(2, 2, 0, 0) - o.S(2, -1, 0, 0)) * re41z;
-            a.gb[0][e] = g0.v[0] + (double)l[0] * d3Sx3 * dt;
-            a.gb[1][e] = g0.v[1] + (double)l[1] * d3Sy3 * dt;
-            a.gb[2][e] = g0.v[2] + (double)l[2] * d3Sz3 * dt;
+            a.gb[0][e] = (float)(g0.v[0] + (double)l[0] * d3Sx3 * dt);
+            a.gb[1][e] = (float)(g0.v[1] + (double)l[1] * d3Sy3 * dt);
+            a.gb[2][e] = (float)(g0.v[2] + (double)l[2] * d3Sz3 * dt);
         }
         return;
     }
@@ -266,7 +270,7 @@ struct GAdjStrOps {
 // the five imaging accumulators of a cell before this step (read early by
 // the staged kernel)
 struct Gm5 {
-    double v[5];
+    float v[5];
 };
 __device__ __forceinline__ Gm5 gm_load(const AdjStrArgs &a, long long e) {
     Gm5 g;
@@ -345,11 +349,11 @@ __device__ __forceinline__ void adj_stress_interior(const AdjStrArgs &a, const O
             gmu += (double)al[c] * (2.0 * taup_plus1 * d3 - 2.0 * taus_plus1 * X[c])
                  + (double)lF[c] * (2.0 * taup1 * d3 - 2.0 * taus1 * X[c]);
         }
-        a.gm[0][e] = g0.v[0] + glam;
-        a.gm[1][e] = g0.v[1] + gmu;
-        a.gm[2][e] = g0.v[2] + ((double)al[3] * taus_plus1 + (double)lF[3] * taus1) * syz;
-        a.gm[3][e] = g0.v[3] + ((double)al[4] * taus_plus1 + (double)lF[4] * taus1) * sxz;
-        a.gm[4][e] = g0.v[4] + ((double)al[5] * taus_plus1 + (double)lF[5] * taus1) * sxy;
+        a.gm[0][e] = (float)(g0.v[0] + glam);
+        a.gm[1][e] = (float)(g0.v[1] + gmu);
+        a.gm[2][e] = (float)(g0.v[2] + ((double)al[3] * taus_plus1 + (double)lF[3] * taus1) * syz);
+        a.gm[3][e] = (float)(g0.v[3] + ((double)al[4] * taus_plus1 + (double)lF[4] * taus1) * sxz);
+        a.gm[4][e] = (float)(g0.v[4] + ((double)al[5] * taus_plus1 + (double)lF[5] * taus1) * sxy);
     }
 }
 
@@ -529,6 +533,21 @@ __global__ void zero_double_kernel(double *p, long long n) {
         p[q] = 0.0;
 }
 
+// the segment's FP32 partial sums into the FP64 totals; the partials restart from zero
+struct FoldArgs {
+    double *total[8];
+    float *part[8];
+};
+__global__ void fold_gradient_kernel(const FoldArgs a, long long n) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int f = 0; f < 8; f++) {
+            a.total[f][q] += (double)a.part[f][q];
+            a.part[f][q] = 0.0f;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // chain rule from the medium arrays to per-cell vp, vs, rho (Q fixed)
 //
@@ -643,6 +662,7 @@ static int adj_alloc(swpc_ctx *c) {
         if (rc) return rc;
     }
     for (int q = 0; q < 8; q++) { int rc = dalloc(c, &s->grad[q], n); if (rc) return rc; }
+    for (int q = 0; q < 8; q++) { int rc = dalloc(c, &s->gpart[q], n); if (rc) return rc; }
     return SWPC_OK;
 }
 
@@ -656,6 +676,7 @@ void adj_free(swpc_ctx *c) {
     for (auto p : s->w40) if (p) cudaFree(p);
     for (auto p : s->w41) if (p) cudaFree(p);
     for (auto p : s->grad) if (p) cudaFree(p);
+    for (auto p : s->gpart) if (p) cudaFree(p);
     if (s->res) cudaFree(s->res);
     if (s->ckpool) cudaFree(s->ckpool);
     if (s->slots) cudaFree(s->slots);
@@ -724,7 +745,7 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
         for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
             for (int q = 0; q < 6; q++) a.S[q] = S_after[q];
-            for (int q = 0; q < 3; q++) a.gb[q] = s->grad[5 + q];
+            for (int q = 0; q < 3; q++) a.gb[q] = s->gpart[5 + q];
         }
         // one cell per thread: the kernel is bound by its 18 weight stores, and
         // staging its few loads (a TMA-staged form was tried) made it slower
@@ -755,7 +776,7 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
         for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
             for (int q = 0; q < 3; q++) a.V[q] = V_before[q];
-            for (int q = 0; q < 5; q++) a.gm[q] = s->grad[q];
+            for (int q = 0; q < 5; q++) a.gm[q] = s->gpart[q];
         }
         if (c->adj_tma && (!grad || fv >= 0)) {
             const TmaTiles t = tma_tiles(c, adjt::BI, adjt::BJ, 1, 1, kStressFields(c), 1);
@@ -810,7 +831,15 @@ static int zero_adjoint(swpc_ctx *c) {
         zero_double_kernel<<<148 * 4, 256, 0, c->stream>>>(p, c->g.ncell);
         ACK(cudaGetLastError());
     }
+    for (auto p : s->gpart) ACK(cudaMemsetAsync(p, 0, n, c->stream));
     return SWPC_OK;
+}
+
+static int fold_gradient(swpc_ctx *c) {
+    FoldArgs a;
+    for (int q = 0; q < 8; q++) { a.total[q] = c->adj->grad[q]; a.part[q] = c->adj->gpart[q]; }
+    fold_gradient_kernel<<<148 * 4, 256, 0, c->stream>>>(a, c->g.ncell);
+    return cuda_check(c, cudaGetLastError(), "fold_gradient_kernel");
 }
 
 // the adjoint array of a field id (V, S, R, PML auxiliaries)
@@ -990,6 +1019,7 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             rc = adj_step(c, Sa, Vb, (it - it0) * 9);
             if (!rc) rc = adj_source(c, it);
         }
+        if (!rc) rc = fold_gradient(c);
         if (rc) return rc;
     }
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
