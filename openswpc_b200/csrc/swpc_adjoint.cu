@@ -19,12 +19,12 @@
 // each step's term is formed in FP64 and added into an FP32 partial sum that
 // covers one checkpoint segment (at most ckpt steps), and every segment's
 // partials are folded into the FP64 totals (blocked summation: the FP32 sums
-// hold ckpt terms, the FP64 ones the segments).  It is formed on the interior kernel region, whose
-// cells are the model parameters (absorber cells copy the medium of the
-// interior edge and are not parameters).  swpc_gradient runs the forward with
-// checkpoints every `ckpt` steps, then per segment recomputes the forward
-// from its checkpoint, keeping V and S of every step, and steps the adjoint
-// back through it.
+// hold ckpt terms, the FP64 ones the segments).  It is formed on the interior
+// kernel region, whose cells are the model parameters (absorber cells copy the
+// medium of the interior edge and are not parameters).  swpc_gradient runs
+// the forward with checkpoints every `ckpt` steps, then per segment
+// recomputes the forward from its checkpoint, keeping V and the stress
+// divergences of every step, and steps the adjoint back through it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,7 +58,7 @@ struct swpc_adj_state {
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
     int ckpt = 0, nseg = 0;
     float *ckpool = nullptr;             // checkpoints: V S R aux per segment
-    float *slots = nullptr;              // V and S after each step of a segment
+    float *slots = nullptr;              // V and the stress divergences after each step of a segment
     size_t ck_floats = 0;
     long long bytes = 0;
 };
@@ -78,7 +78,7 @@ struct AdjVelArgs {
     const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
     float e40[3][2], e41[3][2], r20[3], dt;
     float *w40[9], *w41[9];
-    const float *S[6];           // forward S after the stress update (gradient)
+    const float *divS[3];        // forward stress divergences after the stress update (gradient)
     float *gb[3];                // segment partials of the bx, by, bz gradient (null: none)
 };
 
@@ -132,18 +132,33 @@ constexpr int BI = 4, BJ = 4, NT = KT * BI * BJ;
 // pairs p: 0 (Vx,Sxx,x) 1 (Vx,Sxy,y) 2 (Vx,Sxz,z) 3 (Vy,Sxy,x) 4 (Vy,Syy,y)
 //          5 (Vy,Syz,z) 6 (Vz,Sxz,x) 7 (Vz,Syz,y) 8 (Vz,Szz,z)
 // ---------------------------------------------------------------------------
-// Operands of one cell: lV(c) the adjoint velocity, b(c) the buoyancy,
-// S(f, dk, di, dj) the forward stress after the stress update (f: xx yy zz
-// yz xz xy).
+// Operands of one cell: lV(c) the adjoint velocity, b(c) the buoyancy.
 struct GAdjVelOps {
     const AdjVelArgs &a;
-    long long e, PI, PJ;
+    long long e;
     __device__ __forceinline__ float lV(int c) const { return a.lV[c][e]; }
     __device__ __forceinline__ float b(int c) const { return a.b[c][e]; }
-    __device__ __forceinline__ float S(int f, int dk, int di, int dj) const {
-        return a.S[f][e + dk + di * PI + dj * PJ];
-    }
 };
+
+// The stress divergences of the velocity update, d3Sx3 d3Sy3 d3Sz3 of an
+// interior cell (m_kernel.f90:103-125) on S(f, dk, di, dj), the forward stress
+// after the stress update (f: xx yy zz yz xz xy), with the coefficient pairs
+// of band sign s.
+template <class F>
+__device__ __forceinline__ void stress_divergence(const float (&e40)[3][2], const float (&e41)[3][2], int s, const F &S,
+                                                  float (&d)[3]) {
+    const float re40x = e40[0][s], re41x = e41[0][s], re40y = e40[1][s], re41y = e41[1][s];
+    const float re40z = e40[2][s], re41z = e41[2][s];
+    d[0] = (S(0, 0, 1, 0) - S(0, 0, 0, 0)) * re40x - (S(0, 0, 2, 0) - S(0, 0, -1, 0)) * re41x
+         + (S(5, 0, 0, 0) - S(5, 0, 0, -1)) * re40y - (S(5, 0, 0, 1) - S(5, 0, 0, -2)) * re41y
+         + (S(4, 0, 0, 0) - S(4, -1, 0, 0)) * re40z - (S(4, 1, 0, 0) - S(4, -2, 0, 0)) * re41z;
+    d[1] = (S(5, 0, 0, 0) - S(5, 0, -1, 0)) * re40x - (S(5, 0, 1, 0) - S(5, 0, -2, 0)) * re41x
+         + (S(1, 0, 0, 1) - S(1, 0, 0, 0)) * re40y - (S(1, 0, 0, 2) - S(1, 0, 0, -1)) * re41y
+         + (S(3, 0, 0, 0) - S(3, -1, 0, 0)) * re40z - (S(3, 1, 0, 0) - S(3, -2, 0, 0)) * re41z;
+    d[2] = (S(4, 0, 0, 0) - S(4, 0, -1, 0)) * re40x - (S(4, 0, 1, 0) - S(4, 0, -2, 0)) * re41x
+         + (S(3, 0, 0, 0) - S(3, 0, 0, -1)) * re40y - (S(3, 0, 0, 1) - S(3, 0, 0, -2)) * re41y
+         + (S(2, 1, 0, 0) - S(2, 0, 0, 0)) * re40z - (S(2, 2, 0, 0) - S(2, -1, 0, 0)) * re41z;
+}
 
 struct Gb3 {
     float v[3];
@@ -170,21 +185,10 @@ __device__ __forceinline__ void adj_vel_cell(const AdjVelArgs &a, const O &o, lo
             a.w41[p][e] = a.e41[ax][s] * u[c];
         }
         if (a.gb[0]) {
-            // d(Vx)/d(bx) = d3Sx3 * dt on the forward S after the stress update
-            const float re40x = a.e40[0][s], re41x = a.e41[0][s], re40y = a.e40[1][s], re41y = a.e41[1][s];
-            const float re40z = a.e40[2][s], re41z = a.e41[2][s];
-            const float d3Sx3 = (o.S(0, 0, 1, 0) - o.S(0, 0, 0, 0)) * re40x - (o.S(0, 0, 2, 0) - o.S(0, 0, -1, 0)) * re41x
-                              + (o.S(5, 0, 0, 0) - o.S(5, 0, 0, -1)) * re40y - (o.S(5, 0, 0, 1) - o.S(5, 0, 0, -2)) * re41y
-                              + (o.S(4, 0, 0, 0) - o.S(4, -1, 0, 0)) * re40z - (o.S(4, 1, 0, 0) - o.S(4, -2, 0, 0)) * re41z;
-            const float d3Sy3 = (o.S(5, 0, 0, 0) - o.S(5, 0, -1, 0)) * re40x - (o.S(5, 0, 1, 0) - o.S(5, 0, -2, 0)) * re41x
-                              + (o.S(1, 0, 0, 1) - o.S(1, 0, 0, 0)) * re40y - (o.S(1, 0, 0, 2) - o.S(1, 0, 0, -1)) * re41y
-                              + (o.S(3, 0, 0, 0) - o.S(3, -1, 0, 0)) * re40z - (o.S(3, 1, 0, 0) - o.S(3, -2, 0, 0)) * re41z;
-            const float d3Sz3 = (o.S(4, 0, 0, 0) - o.S(4, 0, -1, 0)) * re40x - (o.S(4, 0, 1, 0) - o.S(4, 0, -2, 0)) * re41x
-                              + (o.S(3, 0, 0, 0) - o.S(3, 0, 0, -1)) * re40y - (o.S(3, 0, 0, 1) - o.S(3, 0, 0, -2)) * re41y
-                              + (o.S(2, 1, 0, 0) - o.S(2, 0, 0, 0)) * re40z - (o.S(2, 2, 0, 0) - o.S(2, -1, 0, 0)) * re41z;
-            a.gb[0][e] = (float)(g0.v[0] + (double)l[0] * d3Sx3 * dt);
-            a.gb[1][e] = (float)(g0.v[1] + (double)l[1] * d3Sy3 * dt);
-            a.gb[2][e] = (float)(g0.v[2] + (double)l[2] * d3Sz3 * dt);
+            // d(Vx)/d(bx) = d3Sx3 * dt, the divergences of the forward S after
+            // the stress update (formed once per step of the recompute)
+#pragma unroll
+            for (int q = 0; q < 3; q++) a.gb[q][e] = (float)(g0.v[q] + (double)l[q] * __ldcs(a.divS[q] + e) * dt);
         }
         return;
     }
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a
     if (!cell_of(g, k, i, j)) return;
     const long long col = col_index(g, i, j);
     const long long e = col * g.Kp + (k - 1 + KH);
-    const GAdjVelOps o{a, e, (long long)g.Kp, (long long)g.Kp * g.Ip};
+    const GAdjVelOps o{a, e};
     const bool interior = i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek;
     const int s = interior ? band_sign(__ldg(&a.band[col]), k) : -1;
     const Gb3 g0 = (interior && a.gb[0]) ? gb_load(a, e) : Gb3{};
@@ -533,6 +537,31 @@ __global__ void zero_double_kernel(double *p, long long n) {
         p[q] = 0.0;
 }
 
+// one slot of the recompute: the stress divergences of the interior cells,
+// on the forward S just after the stress update of that step
+struct SlotDivArgs {
+    Geo g;
+    int ibk, iek, jbk, jek, kek;
+    const float *S[6];
+    const int4 *band;
+    float e40[3][2], e41[3][2];
+    float *divS[3];
+};
+__global__ void __launch_bounds__(128) slot_div_kernel(const SlotDivArgs a) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    if (!(i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek)) return;
+    const long long col = col_index(g, i, j);
+    const long long e = col * g.Kp + (k - 1 + KH);
+    const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
+    const auto S = [&](int f, int dk, int di, int dj) { return a.S[f][e + dk + di * PI + dj * PJ]; };
+    float d[3];
+    stress_divergence(a.e40, a.e41, band_sign(__ldg(&a.band[col]), k), S, d);
+#pragma unroll
+    for (int q = 0; q < 3; q++) __stcs(a.divS[q] + e, d[q]);
+}
+
 // the segment's FP32 partial sums into the FP64 totals; the partials restart from zero
 struct FoldArgs {
     double *total[8];
@@ -727,11 +756,11 @@ static cudaError_t adj_stress_tma(const swpc_adj_state *s, const AdjStrArgs &a, 
 // one transposed step: vel^T then stress^T; with gradient when S_after /
 // V_before are given (for the staged stress-phase weights, V_before is field
 // fv of the slots buffer)
-static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const *V_before, int fv) {
+static int adj_step(swpc_ctx *c, const float *const *divS_after, const float *const *V_before, int fv) {
     swpc_adj_state *s = c->adj;
     const dim3 block(kThreadsK, 2, 2);
     const dim3 grid = cell_grid(c->g, block);
-    const bool grad = S_after != nullptr;
+    const bool grad = divS_after != nullptr;
     {
         AdjVelArgs a;
         memset(&a, 0, sizeof(a));
@@ -744,7 +773,7 @@ static int adj_step(swpc_ctx *c, const float *const *S_after, const float *const
         a.dt = c->d.dt;
         for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
-            for (int q = 0; q < 6; q++) a.S[q] = S_after[q];
+            for (int q = 0; q < 3; q++) a.divS[q] = divS_after[q];
             for (int q = 0; q < 3; q++) a.gb[q] = s->gpart[5 + q];
         }
         // one cell per thread: the kernel is bound by its 18 weight stores, and
@@ -917,13 +946,23 @@ static int copy_state(swpc_ctx *c, float *ck, bool save) {
     return SWPC_OK;
 }
 
+// Slot `slot` of the recompute: V (the whole memory box, read with its halo by
+// the stress-phase weights) and the stress divergences of the interior cells
+// (the velocity-phase gradient), kSlotFields fields of ncell floats.
+constexpr int kSlotFields = 6;
 static int save_slot(swpc_ctx *c, int slot) {
     const size_t n = c->g.ncell;
-    float *base = c->adj->slots + (size_t)slot * 9 * n;
+    float *base = c->adj->slots + (size_t)slot * kSlotFields * n;
     for (int q = 0; q < 3; q++) ACK(cudaMemcpyAsync(base + q * n, c->V[q], n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-    for (int q = 0; q < 6; q++)
-        ACK(cudaMemcpyAsync(base + (3 + q) * n, c->S[q], n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-    return SWPC_OK;
+    SlotDivArgs a;
+    a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
+    for (int q = 0; q < 6; q++) a.S[q] = c->S[q];
+    a.band = c->band;
+    memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41));
+    for (int q = 0; q < 3; q++) a.divS[q] = base + (3 + q) * n;
+    const dim3 block(kThreadsK, 2, 2);
+    slot_div_kernel<<<cell_grid(c->g, block), block, 0, c->stream>>>(a);
+    return cuda_check(c, cudaGetLastError(), "slot_div_kernel");
 }
 
 static int zero_state(swpc_ctx *c) {
@@ -961,7 +1000,7 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     state_arrays(c, &sz);
     size_t ckf = 0;
     for (size_t v : sz) ckf += v;
-    const size_t need_ck = ckf * nseg, need_slots = (size_t)9 * c->g.ncell * (ckpt + 1);
+    const size_t need_ck = ckf * nseg, need_slots = (size_t)kSlotFields * c->g.ncell * (ckpt + 1);
     if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf) {
         if (s->ckpool) cudaFree(s->ckpool);
         if (s->slots) cudaFree(s->slots);
@@ -971,7 +1010,7 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints (raise ckpt or shrink the grid)");
         s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf;
         // the staged stress-phase weights read the forward V of a slot with its halo
-        if (!tma_encode_box(s->maps->vh, s->slots, c->g, 9LL * (ckpt + 1), tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
+        if (!tma_encode_box(s->maps->vh, s->slots, c->g, (long long)kSlotFields * (ckpt + 1), tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
             return err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the recompute slots");
     }
     const size_t nres = (size_t)c->nst * 3 * c->ntw;
@@ -1011,12 +1050,12 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             if (!rc) rc = save_slot(c, it - it0 + 1);
         }
         for (int it = it1; it >= it0 && !rc; it--) {
-            const float *base_a = s->slots + (size_t)(it - it0 + 1) * 9 * n;
-            const float *base_b = s->slots + (size_t)(it - it0) * 9 * n;
-            const float *Sa[6], *Vb[3];
-            for (int q = 0; q < 6; q++) Sa[q] = base_a + (3 + q) * n;
+            const float *base_a = s->slots + (size_t)(it - it0 + 1) * kSlotFields * n;
+            const float *base_b = s->slots + (size_t)(it - it0) * kSlotFields * n;
+            const float *Da[3], *Vb[3];
+            for (int q = 0; q < 3; q++) Da[q] = base_a + (3 + q) * n;
             for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
-            rc = adj_step(c, Sa, Vb, (it - it0) * 9);
+            rc = adj_step(c, Da, Vb, (it - it0) * kSlotFields);
             if (!rc) rc = adj_source(c, it);
         }
         if (!rc) rc = fold_gradient(c);
