@@ -99,18 +99,21 @@ B_PSV_INT, B_PSV_PML = 38 * 4, 34 * 4
 # DRAM traffic of the staged 2D kernels over their algorithmic bytes, measured by ncu on the first 16 c2A models
 # (stress 0.941 + 0.546 GB, velocity 0.328 + 0.087 GB against 1.481 + 0.430 GB; the 2D batch summary under profiles/)
 TRAFFIC_PER_ALGORITHMIC_2D = (0.941275 + 0.545625 + 0.328020 + 0.086632) / (1.4813472 + 0.429801472)
-# one adjoint step per cell (FP32 state, FP64 gradients, nm = 3), interior / absorber: velocity weights (lV, b
-# read, nine w40 + nine w41 written, S of the slot read, three b gradients read and written; absorber: nine PML
-# auxiliaries read and written instead of S and the gradients), velocity gather (18 weights read, six lS read and
-# written), stress weights (lS, seven medium fields, 18 lR read and written, 18 weights written, V of the slot, five
-# medium gradients read and written; absorber: lS, five medium fields, nine auxiliaries, 18 weights), stress gather
-# (18 weights read, three lV read and written)
-B_ADJ_INT = (12 + 12 + 72 + 24 + 48) + (72 + 48) + (24 + 28 + 144 + 72 + 12 + 80) + (72 + 24)
+# one adjoint step per cell (FP32 state, FP32 segment sums of the gradients, nm = 3), interior / absorber:
+# velocity weights (lV, b read, nine w40 + nine w41 written, the three stress divergences of the slot read, three b
+# gradient sums read and written; absorber: nine PML auxiliaries read and written instead of the divergences and
+# sums), velocity gather (18 weights read, six lS read and written), stress weights (lS, seven medium fields, 18 lR
+# read and written, 18 weights written, V of the slot, five medium gradient sums read and written; absorber: lS,
+# five medium fields, nine auxiliaries, 18 weights), stress gather (18 weights read, three lV read and written)
+B_ADJ_INT = (12 + 12 + 72 + 12 + 24) + (72 + 48) + (24 + 28 + 144 + 72 + 12 + 40) + (72 + 24)
 B_ADJ_PML = (12 + 12 + 72 + 72) + (72 + 48) + (24 + 20 + 72 + 72) + (72 + 24)
-# V and S of every recomputed step copied into the segment's slots (read and written)
-B_SLOT = 9 * 4 * 2
-# V, S and R (27 fields) saved at each checkpoint and restored before the segment's recompute
-B_CKPT = 27 * 4 * 2 * 2
+# every recomputed step: V copied into the segment's slot (read and written, every cell), and the three stress
+# divergences of the interior cells formed from S (six read, three written)
+B_SLOT = 3 * 4 * 2
+B_SLOT_INT = 6 * 4 + 3 * 4
+# V, S and R (27 fields) saved at each checkpoint and restored before the segment's recompute; at the end of each
+# segment the eight FP32 gradient sums (read, zeroed) folded into the FP64 totals (read and written)
+B_CKPT = 27 * 4 * 2 * 2 + 8 * (4 * 2 + 8 * 2)
 
 
 def make_c2a_models(n: int = 64, seed: int = 20260203):
@@ -618,7 +621,7 @@ def bench_c3(args, world, rank, local):
           "nt": nt, "ckpt": ckpt,
           "l2": "inputs larger than L2 (wavefield, checkpoints and adjoint state resident, tens of GB)",
           "parallelism": f"replicas x{world}"}
-    metric = "Gcell-updates/s (3D visco adjoint gradient, FP32 + FP64 accumulation)"
+    metric = "Gcell-updates/s (3D visco adjoint gradient, FP32, imaging sums folded into FP64 per checkpoint segment)"
     if args.impl == "reference":
         if rank != 0:
             return
@@ -681,7 +684,7 @@ def bench_c3(args, world, rank, local):
     n_int, n_pml = cell_counts(p)
     nseg = -(-p.nt // ckpt)
     b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
-    b_grad = (p.nt * (2 * b_fwd + (n_int + n_pml) * B_SLOT + n_int * B_ADJ_INT + n_pml * B_ADJ_PML)
+    b_grad = (p.nt * (2 * b_fwd + (n_int + n_pml) * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
               + nseg * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()
     ach = b_grad / (grad / 1e3) / 1e9

@@ -5,7 +5,7 @@ velocity traces that wav__store records (src/swpc_3d/m_wav.f90:530-535) of a
 run from rest over steps 1..nt.  Its gradient with respect to per-cell vp, vs
 and rho (Q held fixed) comes from the library's discrete adjoint of the step
 (``swpc_gradient``: checkpointed forward, recompute per segment, transposed
-step, FP64 accumulation) and the chain rule of ``swpc_gradient_model``.  Both
+step, imaging sums in FP32 per checkpoint segment folded into FP64) and the chain rule of ``swpc_gradient_model``.  Both
 run on the GPU; this module only moves the model in and the gradient out.
 
 The parameters are the cells of the kernel region: absorber cells copy the
