@@ -639,7 +639,9 @@ def bench_c3(args, world, rank, local):
     _lib.check(true.ctx, true.lib.swpc_run(true.ctx, 1, p.nt))
     obs = true.waveforms(_lib.WAV_V)
     true.close()
-    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, device=local, ckpt=ckpt)
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, device=local, ckpt=ckpt,
+                    slot_memory=0 if args.recompute_all else "auto")
+    kept = prob.kept_steps()
     s = prob.solver
     lib, ctx = s.lib, s.ctx
     stream = torch.cuda.ExternalStream(lib.swpc_stream(ctx), device=local)
@@ -679,13 +681,15 @@ def bench_c3(args, world, rank, local):
     t_e2e = time.perf_counter() - t0
     h2d = sum(a.nbytes for a in (vp, vs, rho)) * 2 + obsf.nbytes
     d2h = sum(t.grad.numel() * 8 for t in tv) + obsf.nbytes
-    # algorithmic bytes of one gradient: forward and recompute (the 3D step each), slot copies, the adjoint step,
-    # checkpoint save and restore
+    # algorithmic bytes of one gradient: the forward and the recompute of the steps whose slots are not kept (the
+    # 3D step each), slot copies, the adjoint step, checkpoint save and restore of the recomputed segments
     n_int, n_pml = cell_counts(p)
     nseg = -(-p.nt // ckpt)
+    nrec = -(-(p.nt - kept) // ckpt)
     b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
-    b_grad = (p.nt * (2 * b_fwd + (n_int + n_pml) * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
-              + nseg * (n_int + n_pml) * B_CKPT)
+    b_grad = ((2 * p.nt - kept) * b_fwd
+              + p.nt * ((n_int + n_pml) * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
+              + nrec * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()
     ach = b_grad / (grad / 1e3) / 1e9
     ach_fwd = p.nt * b_fwd / (fwd / 1e3) / 1e9
@@ -693,11 +697,13 @@ def bench_c3(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": grad, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + "
             "Gaussian vs blob)", "config": wl,
-            "what": "one step = one gradient evaluation (forward with checkpoints, per-segment recompute, "
-                    "adjoint); value counts cells x nt per gradient",
+            "what": "one step = one gradient evaluation (forward with checkpoints, keeping the forward slots of "
+                    "the trailing segments that fit in free HBM, per-segment recompute of the others, adjoint); "
+                    "value counts cells x nt per gradient",
             "misfit": J.value,
             "forward_ms": fwd, "forward_gcells": cells * p.nt / (fwd / 1e3) / 1e9,
             "gradient_over_forward": grad / fwd,
+            "kept_steps": kept, "recomputed_steps": p.nt - kept, "slot_memory_bytes": prob.slot_memory,
             "algorithmic_gradient_over_forward": b_grad / (p.nt * b_fwd),
             "roofline": {"bound": "hbm", "kernel": "whole gradient: stress3d_tma_kernel + vel3d_tma_kernel (forward "
                                                      "and recompute), adj_*_kernel (adjoint step), slot and "
@@ -712,7 +718,7 @@ def bench_c3(args, world, rank, local):
                             "upload, gradient, chain rule, gradients back, wall clock"},
             # per gradient: forward and recompute steps (wav, stress, injection, velocity, step counter), the
             # adjoint steps (two weight and two gather kernels, residual injection), zeroing of 8 gradients
-            "gpu_launches": args.steps * (p.nt * (5 + 4 + 5) + 8), "clocks": clk.summary()}
+            "gpu_launches": args.steps * ((2 * p.nt - kept) * 5 + p.nt * (4 + 5) + 8), "clocks": clk.summary()}
     prob.close()
     if rank == 0 and not args.no_cpu_baseline:
         # the reference has no adjoint: its CPU cost of a gradient is at least its forward run, timed here
@@ -846,6 +852,16 @@ def cpu_reference(p, xi, steps: int, warmup: int, threads: int, budget_s: float 
     return cells * n / dt / 1e9, n, cells, dt
 
 
+def sample_mix(p) -> str:
+    """What the CPU sample of a 3D workload is, against the workload."""
+    ns = min(256, p.nx), min(256, p.ny)
+    n_int, n_pml = cell_counts(p)
+    si = (ns[0] - 2 * p.na) * (ns[1] - 2 * p.na) * (p.nz - p.na)
+    frac = 1 - si / (ns[0] * ns[1] * p.nz)
+    return (f"a grid of its own with the workload's {p.na}-cell PML on every side ({100 * frac:.0f} % absorber "
+            f"cells against the workload's {100 * n_pml / (n_int + n_pml):.0f} %), one double couple, no stations")
+
+
 def accuracy_sample(p, precision: str, device: int, steps: int = 200):
     """rel-L2 error of one storage form against the all-double oracle on a
     128 x 128 x 64 sample of the workload (same spacing, medium statistics,
@@ -918,6 +934,8 @@ def main():
                     help="c2b: also time every launch order x j block x members-per-CTA form (profiling runs)")
     ap.add_argument("--grid", default=None, help="override the grid as NXxNYxNZ (profiling runs)")
     ap.add_argument("--na", type=int, default=None, help="override the PML width (profiling runs)")
+    ap.add_argument("--recompute-all", action="store_true",
+                    help="c3: keep no forward slots, recompute every segment (the smallest-memory form)")
     ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (c3 profiling runs)")
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16r", "f16r", "f16sr"],
                     help="storage of stress and memory variables (arithmetic is FP32)")
@@ -980,7 +998,8 @@ def main():
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                  "sample": f"oracle f32 (CPU restatement of the Fortran path; the Fortran "
                                            f"reference cannot be compiled here), one step per timed step over "
-                                           f"the centre {256}x{256}x{p.nz} column block of the same medium"},
+                                           f"the centre {256}x{256}x{p.nz} column block of the same medium as "
+                                           f"{sample_mix(p)}"},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -1136,8 +1155,8 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         v, n, sc, dt = cpu_reference(p, xi, 1000, 1, os.cpu_count() or 1, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                                "sample": f"oracle f32 on the centre 256x256x{p.nz} column block, {n} steps "
-                                          f"after 1 warm-up ({dt:.1f} s)"}
+                                "sample": f"oracle f32 on the centre 256x256x{p.nz} column block of the same "
+                                          f"medium as {sample_mix(p)}, {n} steps after 1 warm-up ({dt:.1f} s)"}
     ranks.close()
     if rank == 0 and world == 1 and args.workload == "c1" and args.precision == "f32" and not args.no_secondary:
         line["secondary"] = secondary_lines()
@@ -1154,7 +1173,7 @@ SECONDARY = [
                                                   "roofline", "e2e", "clocks")),
     ("c3", ["--steps", "1", "--warmup", "3", "--no-cpu-baseline"],
      ("value", "ms_per_step", "forward_ms", "gradient_over_forward", "algorithmic_gradient_over_forward",
-      "roofline", "roofline_forward", "e2e", "clocks")),
+      "kept_steps", "roofline", "roofline_forward", "e2e", "clocks")),
     ("c4", ["--steps", "10", "--warmup", "3", "--no-cpu-baseline", "--no-secondary", "--accuracy",
             "--precision", "bf16r"], ("value", "ms_per_step", "storage", "roofline", "accuracy",
                                       "accuracy_full_grid", "clocks")),

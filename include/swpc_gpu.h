@@ -378,11 +378,22 @@ int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const i
  * steps 1..nt, and its gradient with respect to the medium arrays of the
  * kernel region.  It runs the forward with a checkpoint every `ckpt` steps,
  * then per segment recomputes the forward from the checkpoint and steps the
- * adjoint back through it, accumulating the gradient in FP64.  Device memory:
- * nt/ckpt checkpoints of the state plus ckpt+1 copies of V and S.  Every
+ * adjoint back through it, summing each segment's imaging terms in FP32 and
+ * folding them into FP64 totals.  Device memory: one checkpoint of the state
+ * per recomputed segment plus the slots (V and the three stress divergences
+ * after a step) of max(ckpt + 1, kept steps + 1) steps.  Every
  * recorder (traces, green__store, snapshots) records the forward run once:
  * the recompute advances the wavefield without them, so what they hold after
  * the call equals a plain run of steps 1..nt from rest.
+ * swpc_gradient_set_slot_memory: bytes of HBM that the slots of trailing
+ * segments may take (default 0).  The first forward pass then keeps the slot
+ * of every step of as many trailing segments as the bytes hold, and only the
+ * segments before them are checkpointed and recomputed; the gradient, the
+ * misfit and the recorders are bitwise those of the default.  The setting
+ * holds for the later swpc_gradient calls of the context.
+ * swpc_gradient_memory: bytes of one checkpoint and of one slot, for sizing
+ * that budget (free memory from cudaMemGetInfo, say, less what the
+ * checkpoints take).
  * swpc_gradient_fetch: which = 0 lam, 1 mu, 2 muyz, 3 muxz, 4 muxy, 5 bx,
  * 6 by, 7 bz; out = double array over the memory box. */
 int swpc_adj_reset(swpc_ctx *ctx);
@@ -397,6 +408,8 @@ int swpc_adj_step_linear(swpc_ctx *ctx);
 int swpc_adj_upload(swpc_ctx *ctx, int field, const float *in, int ld_k, int ld_i);
 int swpc_adj_download(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
 int swpc_gradient(swpc_ctx *ctx, const float *obs, int ckpt, double *misfit);
+int swpc_gradient_set_slot_memory(swpc_ctx *ctx, long long bytes);
+int swpc_gradient_memory(swpc_ctx *ctx, long long *ckpt_bytes, long long *slot_bytes);
 int swpc_gradient_fetch(swpc_ctx *ctx, int which, double *out, int ld_k, int ld_i);
 /* The gradient of the last swpc_gradient with respect to per-cell vp, vs and
  * rho with Q held fixed: the chain rule through vmodel_lhm's moduli

@@ -45,6 +45,7 @@ EXPORTS = [
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
     "swpc_adj_reset", "swpc_adj_step_linear", "swpc_adj_upload", "swpc_adj_download", "swpc_gradient",
+    "swpc_gradient_set_slot_memory", "swpc_gradient_memory",
     "swpc_gradient_fetch", "swpc_gradient_model", "swpc_reset_state",
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
@@ -178,6 +179,8 @@ def load():
         "swpc_adj_upload": (i, [vp, i, _FP, i, i]),
         "swpc_adj_download": (i, [vp, i, _FP, i, i]),
         "swpc_gradient": (i, [vp, _FP, i, C.POINTER(C.c_double)]),
+        "swpc_gradient_set_slot_memory": (i, [vp, C.c_longlong]),
+        "swpc_gradient_memory": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "swpc_gradient_fetch": (i, [vp, i, C.POINTER(C.c_double), i, i]),
         "swpc_gradient_model": (i, [vp, _FP, _FP, _FP, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),

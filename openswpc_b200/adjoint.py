@@ -41,16 +41,63 @@ class Misfit3D:
     per-cell (vp, vs, rho) against observed velocity traces ``obs`` of shape
     (nst, 3, ntw), the layout of ``Swpc3D.waveforms``."""
 
-    def __init__(self, p: Params, vp, vs, rho, qp, qs, obs: np.ndarray, device: int = 0, ckpt: int = 50):
+    def __init__(self, p: Params, vp, vs, rho, qp, qs, obs: np.ndarray, device: int = 0, ckpt: int = 50,
+                 slot_memory: int | str = 0):
         self.p = p
         self.qp = np.ascontiguousarray(qp, np.float32)
         self.qs = np.ascontiguousarray(qs, np.float32)
         self.ckpt = int(ckpt)
+        self.device = device
         m = Medium.from_model(p, vp, vs, rho, self.qp, self.qs)
         self.solver = Swpc3D(p, device=device, medium=m)
         self.obs = np.ascontiguousarray(obs, np.float32)
         if self.obs.shape != (self.solver.nst, 3, self.ntw):
             raise ValueError(f"observed traces must have shape {(self.solver.nst, 3, self.ntw)}")
+        self.set_slot_memory(slot_memory)
+
+    def memory(self) -> tuple[int, int]:
+        """Bytes of one checkpoint and of one slot of the gradient."""
+        ck, sl = C.c_longlong(), C.c_longlong()
+        check(self.solver.ctx, self.solver.lib.swpc_gradient_memory(self.solver.ctx, C.byref(ck), C.byref(sl)))
+        return ck.value, sl.value
+
+    def set_slot_memory(self, nbytes: int | str, reserve: int = 4 << 30) -> int:
+        """HBM that the slots of trailing segments may take
+        (``swpc_gradient_set_slot_memory``): those segments keep their
+        forward slots from the first pass instead of being recomputed, with
+        bitwise the same gradient.  ``"auto"`` keeps the most trailing
+        segments whose slots, with the checkpoints of the segments before
+        them, fit in the device's free memory less ``reserve`` bytes (call it
+        before the first gradient, whose buffers it would count as used).
+        Returns the bytes set."""
+        s = self.solver
+        if nbytes == "auto":
+            free, _ = torch.cuda.mem_get_info(self.device)
+            ck, sl = self.memory()
+            nt, k = self.p.nt, self.ckpt
+            nseg = -(-nt // k)
+            nbytes, steps = 0, 0
+            for t in range(1, nseg + 1):
+                steps += min(k, nt - (nseg - t) * k)
+                if (max(steps, k) + 1) * sl + max(nseg - t, 1) * ck > free - reserve:
+                    break
+                nbytes = (steps + 1) * sl
+        check(s.ctx, s.lib.swpc_gradient_set_slot_memory(s.ctx, int(nbytes)))
+        self.slot_memory = int(nbytes)
+        return self.slot_memory
+
+    def kept_steps(self) -> int:
+        """Steps of the trailing segments whose slots the gradient keeps from
+        its forward pass (the rule of swpc_gradient)."""
+        _, sl = self.memory()
+        cap, nt, ck = self.slot_memory // sl, self.p.nt, self.ckpt
+        nseg, n = -(-nt // ck), 0
+        for g in range(nseg - 1, -1, -1):
+            ln = min(ck, nt - g * ck)
+            if n + ln + 1 > cap:
+                break
+            n += ln
+        return n
 
     @property
     def ntw(self) -> int:

@@ -58,8 +58,11 @@ struct swpc_adj_state {
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
     int ckpt = 0, nseg = 0;
     float *ckpool = nullptr;             // checkpoints: V S R aux per segment
-    float *slots = nullptr;              // V and the stress divergences after each step of a segment
-    size_t ck_floats = 0;
+    float *slots = nullptr;              // V and the stress divergences after each step of a segment, or of
+                                         // the trailing segments kept from the first forward pass
+    size_t ck_floats = 0, slot_cap = 0;  // floats per checkpoint; slots allocated
+    long long slot_budget = 0;           // bytes the slots of trailing segments may take (0: recompute all)
+    int ntail = 0;                       // trailing segments whose slots the forward pass keeps
     long long bytes = 0;
 };
 
@@ -988,6 +991,41 @@ extern "C" int swpc_reset_state(swpc_ctx *c) {
     return cuda_check(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 }
 
+extern "C" int swpc_gradient_set_slot_memory(swpc_ctx *c, long long bytes) {
+    int rc = adj_ready(c);
+    if (rc) return rc;
+    if (bytes < 0) return err(c, SWPC_ERR_ARG, "slot memory must be >= 0 bytes");
+    c->adj->slot_budget = bytes;
+    return SWPC_OK;
+}
+
+extern "C" int swpc_gradient_memory(swpc_ctx *c, long long *ckpt_bytes, long long *slot_bytes) {
+    if (!c || !ckpt_bytes || !slot_bytes) return SWPC_ERR_ARG;
+    if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "the adjoint is implemented for the 3D solver");
+    std::vector<size_t> sz;
+    state_arrays(c, &sz);
+    long long ckf = 0;
+    for (size_t v : sz) ckf += (long long)v;
+    *ckpt_bytes = ckf * (long long)sizeof(float);
+    *slot_bytes = (long long)kSlotFields * c->g.ncell * (long long)sizeof(float);
+    return SWPC_OK;
+}
+
+// Trailing segments of a gradient whose slots (one per step plus the state
+// before the first) fit in `cap` slots; their steps in *steps.
+static int tail_segments(int nt, int ckpt, int nseg, long long cap, long long *steps) {
+    int ntail = 0;
+    long long n = 0;
+    while (ntail < nseg) {
+        const int it0 = (nseg - 1 - ntail) * ckpt + 1, len = std::min(ckpt, nt - it0 + 1);
+        if (n + len + 1 > cap) break;
+        n += len;
+        ntail++;
+    }
+    *steps = n;
+    return ntail;
+}
+
 extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *misfit) {
     int rc = adj_ready(c);
     if (rc) return rc;
@@ -1000,31 +1038,52 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     state_arrays(c, &sz);
     size_t ckf = 0;
     for (size_t v : sz) ckf += v;
-    const size_t need_ck = ckf * nseg, need_slots = (size_t)kSlotFields * c->g.ncell * (ckpt + 1);
-    if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf) {
+    const size_t n = c->g.ncell, slot_floats = (size_t)kSlotFields * n;
+    // the trailing segments whose slots fit the budget keep them from the first forward pass and are not
+    // recomputed (nor checkpointed); the earlier segments recompute into the same slots once those are spent
+    long long tail_steps = 0;
+    const int ntail = tail_segments(nt, ckpt, nseg, s->slot_budget / (long long)(slot_floats * sizeof(float)),
+                                    &tail_steps);
+    const int gT = nseg - ntail, itT0 = gT * ckpt + 1;
+    const size_t cap = std::max((size_t)ckpt + 1, (size_t)tail_steps + 1);
+    const size_t need_ck = ckf * std::max(gT, 1), need_slots = slot_floats * cap;
+    if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf || s->slot_cap != cap || s->ntail != ntail) {
         if (s->ckpool) cudaFree(s->ckpool);
         if (s->slots) cudaFree(s->slots);
         s->ckpool = s->slots = nullptr;
+        s->ckpt = s->nseg = s->ntail = 0;
+        s->ck_floats = s->slot_cap = 0;
         if (cudaMalloc((void **)&s->ckpool, need_ck * sizeof(float)) != cudaSuccess ||
-            cudaMalloc((void **)&s->slots, need_slots * sizeof(float)) != cudaSuccess)
-            return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints (raise ckpt or shrink the grid)");
-        s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf;
+            cudaMalloc((void **)&s->slots, need_slots * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints and slots (raise ckpt, lower the slot "
+                                          "memory or shrink the grid)");
+        }
+        s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf; s->slot_cap = cap; s->ntail = ntail;
         // the staged stress-phase weights read the forward V of a slot with its halo
-        if (!tma_encode_box(s->maps->vh, s->slots, c->g, (long long)kSlotFields * (ckpt + 1), tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
+        if (!tma_encode_box(s->maps->vh, s->slots, c->g, (long long)kSlotFields * cap, tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
             return err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the recompute slots");
     }
     const size_t nres = (size_t)c->nst * 3 * c->ntw;
     if (!s->res) ACK(cudaMalloc((void **)&s->res, nres * sizeof(float)));
-    // 1. forward from rest with a checkpoint before every segment
+    // 1. forward from rest with a checkpoint before every recomputed segment; the trailing segments keep the
+    //    slot of every step instead (the recorders run in both)
     rc = zero_state(c);
     if (rc) return rc;
-    for (int g = 0; g < nseg; g++) {
-        const int it0 = g * ckpt + 1, n = std::min(ckpt, nt - it0 + 1);
-        rc = copy_state(c, s->ckpool + (size_t)g * ckf, true);
-        if (rc) return rc;
-        rc = swpc_run(c, it0, n);
-        if (rc) return rc;
+    for (int g = 0; g < nseg && !rc; g++) {
+        const int it0 = g * ckpt + 1, len = std::min(ckpt, nt - it0 + 1);
+        if (g < gT) {
+            rc = copy_state(c, s->ckpool + (size_t)g * ckf, true);
+            if (!rc) rc = swpc_run(c, it0, len);
+            continue;
+        }
+        if (g == gT) rc = save_slot(c, 0);
+        for (int it = it0; it < it0 + len && !rc; it++) {
+            rc = swpc_run(c, it, 1);
+            if (!rc) rc = save_slot(c, it - itT0 + 1);
+        }
     }
+    if (rc) return rc;
     // 2. residuals and misfit
     std::vector<float> syn(nres);
     ACK(cudaMemcpyAsync(syn.data(), c->wav[0], nres * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
@@ -1039,23 +1098,29 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     // 3. adjoint, segment by segment from the last
     rc = zero_adjoint(c);
     if (rc) return rc;
-    const size_t n = c->g.ncell;
     for (int g = nseg - 1; g >= 0; g--) {
         const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt);
-        rc = copy_state(c, s->ckpool + (size_t)g * ckf, false);
-        if (!rc) rc = save_slot(c, 0);
-        // the recompute advances the wavefield only: the recorders already hold these steps
-        for (int it = it0; it <= it1 && !rc; it++) {
-            rc = step_state(c, it);
-            if (!rc) rc = save_slot(c, it - it0 + 1);
+        // slot of the state before step it0: kept from the forward pass, or recomputed from the checkpoint
+        size_t base = 0;
+        if (g >= gT) {
+            base = (size_t)(it0 - itT0);
+        } else {
+            rc = copy_state(c, s->ckpool + (size_t)g * ckf, false);
+            if (!rc) rc = save_slot(c, 0);
+            // the recompute advances the wavefield only: the recorders already hold these steps
+            for (int it = it0; it <= it1 && !rc; it++) {
+                rc = step_state(c, it);
+                if (!rc) rc = save_slot(c, it - it0 + 1);
+            }
         }
         for (int it = it1; it >= it0 && !rc; it--) {
-            const float *base_a = s->slots + (size_t)(it - it0 + 1) * kSlotFields * n;
-            const float *base_b = s->slots + (size_t)(it - it0) * kSlotFields * n;
+            const size_t sa = base + (size_t)(it - it0 + 1), sb = base + (size_t)(it - it0);
+            const float *base_a = s->slots + sa * slot_floats;
+            const float *base_b = s->slots + sb * slot_floats;
             const float *Da[3], *Vb[3];
             for (int q = 0; q < 3; q++) Da[q] = base_a + (3 + q) * n;
             for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
-            rc = adj_step(c, Da, Vb, (it - it0) * kSlotFields);
+            rc = adj_step(c, Da, Vb, (int)(sb * kSlotFields));
             if (!rc) rc = adj_source(c, it);
         }
         if (!rc) rc = fold_gradient(c);

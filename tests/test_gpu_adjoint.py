@@ -154,6 +154,54 @@ def test_staged_adjoint_weights_give_the_bits_of_the_one_cell_kernel():
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), fid
 
 
+def _gradient_bits(g, p, obsf, ckpt):
+    shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+    J = C.c_double()
+    check(g.ctx, g.lib.swpc_gradient(g.ctx, fptr(obsf), ckpt, C.byref(J)))
+    grads = []
+    for w in range(8):
+        out = np.zeros(shape, np.float64)
+        check(g.ctx, g.lib.swpc_gradient_fetch(g.ctx, w, out.ctypes.data_as(C.POINTER(C.c_double)), p.nz + 6,
+                                               p.nx + 6))
+        grads.append(out)
+    adj = []
+    for fid, _ in fields(p):
+        b = np.zeros(shape, np.float32)
+        check(g.ctx, g.lib.swpc_adj_download(g.ctx, fid, fptr(b), p.nz + 6, p.nx + 6))
+        adj.append(b)
+    return J.value, grads, adj, g.waveforms(_lib.WAV_V)
+
+
+def test_gradient_with_kept_slots_gives_the_bits_of_the_full_recompute():
+    """Slots of trailing segments kept from the first forward pass
+    (swpc_gradient_set_slot_memory) replace their recompute: with room for
+    none, for the short last segment, for the last three segments and for
+    every segment, the misfit, the eight gradients, the final adjoint state
+    and the traces are bit for bit those of the default, on one context and
+    across budget changes."""
+    p, xi, obs = misfit_case()   # nt = 70, ckpt 16: segments of 16, 16, 16, 16 and 6 steps
+    obsf = np.ascontiguousarray(obs, np.float32)
+    ref = Swpc3D(p, xi)
+    J0, g0, a0, w0 = _gradient_bits(ref, p, obsf, 16)
+    ref.close()
+    assert any(np.abs(x).max() > 0 for x in g0)
+    g = Swpc3D(p, xi)
+    ck, sl = C.c_longlong(), C.c_longlong()
+    check(g.ctx, g.lib.swpc_gradient_memory(g.ctx, C.byref(ck), C.byref(sl)))
+    assert ck.value > 0 and sl.value > 0
+    for slots in (7, 40, 71, 1 << 20, 0):   # kept steps: 6, 38, 70, 70, none
+        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, slots * sl.value))
+        J1, g1, a1, w1 = _gradient_bits(g, p, obsf, 16)
+        assert J1 == J0, slots
+        for w, (x, y) in enumerate(zip(g1, g0)):
+            assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), (slots, w)
+        for (fid, _), x, y in zip(fields(p), a1, a0):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (slots, fid)
+        assert np.array_equal(w1.view(np.uint32), w0.view(np.uint32)), slots
+    assert g.lib.swpc_gradient_set_slot_memory(g.ctx, -1) == _lib.SWPC_ERR_ARG
+    g.close()
+
+
 def forward_misfit(g, p, obs):
     check(g.ctx, g.lib.swpc_upload_medium(g.ctx, C.byref(g.medium.view())))
     for fid in range(9):
