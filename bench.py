@@ -107,6 +107,9 @@ TRAFFIC_PER_ALGORITHMIC_2D = (0.941275 + 0.545625 + 0.328020 + 0.086632) / (1.48
 # five medium fields, nine auxiliaries, 18 weights), stress gather (18 weights read, three lV read and written)
 B_ADJ_INT = (12 + 12 + 72 + 12 + 24) + (72 + 48) + (24 + 28 + 144 + 72 + 12 + 40) + (72 + 24)
 B_ADJ_PML = (12 + 12 + 72 + 72) + (72 + 48) + (24 + 20 + 72 + 72) + (72 + 24)
+# inside a checkpoint segment the stress gather of each step forms the velocity weights of the next from the lV it
+# has just summed, so every step but the first of a segment reads lV once instead of twice
+B_ADJ_FUSED_SAVES = 12
 # every recomputed step: V copied into the segment's slot (read and written, every cell), and the three stress
 # divergences of the interior cells formed from S (six read, three written)
 B_SLOT = 3 * 4 * 2
@@ -689,6 +692,7 @@ def bench_c3(args, world, rank, local):
     b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
     b_grad = ((2 * p.nt - kept) * b_fwd
               + p.nt * ((n_int + n_pml) * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
+              - (p.nt - nseg) * (n_int + n_pml) * B_ADJ_FUSED_SAVES
               + nrec * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()
     ach = b_grad / (grad / 1e3) / 1e9
@@ -718,7 +722,8 @@ def bench_c3(args, world, rank, local):
                             "upload, gradient, chain rule, gradients back, wall clock"},
             # per gradient: forward and recompute steps (wav, stress, injection, velocity, step counter), the
             # adjoint steps (two weight and two gather kernels, residual injection), zeroing of 8 gradients
-            "gpu_launches": args.steps * ((2 * p.nt - kept) * 5 + p.nt * (4 + 5) + 8), "clocks": clk.summary()}
+            "gpu_launches": args.steps * ((2 * p.nt - kept) * 5 + p.nt * (3 + 5) + nseg + 8),
+            "clocks": clk.summary()}
     prob.close()
     if rank == 0 and not args.no_cpu_baseline:
         # the reference has no adjoint: its CPU cost of a gradient is at least its forward run, timed here

@@ -592,6 +592,11 @@ long long swpc_device_bytes(const swpc_ctx *ctx);
  * kernel 8 (3D) selects the stress-phase weights kernel of the adjoint step
  * (swpc_adj_*, swpc_gradient): bi = 1 the TMA-staged kernel (default), 0 the
  * one-cell-per-thread kernel.
+ * kernel 9 (3D) selects how swpc_gradient forms the velocity-phase weights
+ * of the adjoint step: bi = 1 (default) inside the stress-phase gather of the
+ * step before, from the lambda_V it has just summed (the cells whose
+ * lambda_V receiver residuals change afterwards are formed again after the
+ * injection), 0 by a kernel of their own in every step.
  * 2D contexts (P-SV, SH) take kernels 0 / 1 (the tile-walking stress /
  * velocity kernels) and 5 / 6 (the staged ones: a CTA per 32 x 16 tile with
  * bi = 4, 8 or 16 threads along i, minb 1, bj 1); they start with kernels

@@ -52,7 +52,12 @@ struct swpc_adj_state {
     float *slab = nullptr;               // lV, lS, lR in the forward slab's field order (V, S, R)
     int slab_nf = 0;
     swpc::TmaMaps *maps = nullptr;       // staged stress-phase weights: state, s6 (adjoint slab), med, vh (slots)
-    float *w40[9] = {}, *w41[9] = {};    // difference-operator weights
+    float *w40[9] = {}, *w41[9] = {};    // difference-operator weights of the stress phase
+    float *w40v[9] = {}, *w41v[9] = {};  // and of the velocity phase (formed while the stress-phase ones are read)
+    unsigned char *srcmask = nullptr;    // cells whose lambda_V a receiver residual changes
+    int *srccells = nullptr;             // the same cells: (k, i, j) triplets, then nsrc + 1 offsets into the
+                                         // contributions (station << 2 | component), in station order
+    int nsrc = 0, nsrc_contrib = 0;
     double *grad[8] = {};                // lam mu muyz muxz muxy bx by bz: FP64 totals
     float *gpart[8] = {};                // the same, FP32 partial sums of the current segment
     float *res = nullptr;                // receiver residuals (nst, 3, ntw)
@@ -223,6 +228,11 @@ __global__ void __launch_bounds__(128) adj_vel_weights_kernel(const AdjVelArgs a
     const int s = interior ? band_sign(__ldg(&a.band[col]), k) : -1;
     const Gb3 g0 = (interior && a.gb[0]) ? gb_load(a, e) : Gb3{};
     adj_vel_cell(a, o, col, k, i, j, e, s, g0);
+}
+
+__global__ void mark_cells_kernel(Geo g, const int *cells, int n, unsigned char *mask) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) mask[cell_index(g, cells[3 * q], cells[3 * q + 1], cells[3 * q + 2])] = 1;
 }
 
 // transpose of a forward difference (f[e+P] - f[e]) * A40 - (f[e+2P] - f[e-P]) * A41
@@ -516,23 +526,87 @@ __global__ void __launch_bounds__(128) adj_stress_gather_kernel(const GatherArgs
     a.dst[2][f] += tbwd(a.w40[2], a.w41[2], f, 1) + tfwd(a.w40[5], a.w41[5], f, PI) + tfwd(a.w40[7], a.w41[7], f, PJ);
 }
 
-// transpose of the velocity recorder (m_wav.f90:530-535): residuals as sources
-__global__ void adj_source_kernel(Geo g, const int *st, int nst, int ntw, int itw, const float *res, float scale,
-                                  float *lVx, float *lVy, float *lVz) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= nst) return;
-    const int i = st[3 * n], j = st[3 * n + 1], k = st[3 * n + 2];
-    const long long e = cell_index(g, k, i, j);
+// Operands of the fused kernel below: lambda_V from registers, b from memory.
+struct RAdjVelOps {
+    const AdjVelArgs &a;
+    long long e;
+    float l[3];
+    __device__ __forceinline__ float lV(int c) const { return l[c]; }
+    __device__ __forceinline__ float b(int c) const { return a.b[c][e]; }
+};
+
+// lambda_V += D_V^T weights as adj_stress_gather_kernel, then, from the new
+// lambda_V of the cell, the velocity-phase weights of the next adjoint step
+// (the cell-local transpose of the velocity update, adj_vel_cell), so that
+// lambda_V is read once for both and the weights need no launch of their
+// own.  Cells of `mask` (when given: a step whose receiver residuals still
+// change their lambda_V) leave their weights to adj_source_cells_kernel.
+__global__ void __launch_bounds__(128) adj_stress_gather_vel_kernel(const GatherArgs a, const AdjVelArgs v,
+                                                                     const unsigned char *mask) {
+    const Geo g = a.g;
+    int k, i, j;
+    if (!cell_of(g, k, i, j)) return;
+    const long long f = cell_index(g, k, i, j);
     const long long PI = g.Kp, PJ = (long long)g.Kp * g.Ip;
-    const float rx = res[((long long)n * 3 + 0) * ntw + itw - 1] * scale;
-    const float ry = res[((long long)n * 3 + 1) * ntw + itw - 1] * scale;
-    const float rz = res[((long long)n * 3 + 2) * ntw + itw - 1] * scale;
-    atomicAdd(&lVx[e], rx);
-    atomicAdd(&lVx[e - PI], rx);
-    atomicAdd(&lVy[e], ry);
-    atomicAdd(&lVy[e - PJ], ry);
-    atomicAdd(&lVz[e], -rz);
-    atomicAdd(&lVz[e - 1], -rz);
+    const float l0 = a.dst[0][f] + (tbwd(a.w40[0], a.w41[0], f, PI) + tfwd(a.w40[4], a.w41[4], f, PJ) +
+                                    tfwd(a.w40[6], a.w41[6], f, 1));
+    const float l1 = a.dst[1][f] + (tbwd(a.w40[1], a.w41[1], f, PJ) + tfwd(a.w40[3], a.w41[3], f, PI) +
+                                    tfwd(a.w40[8], a.w41[8], f, 1));
+    const float l2 = a.dst[2][f] + (tbwd(a.w40[2], a.w41[2], f, 1) + tfwd(a.w40[5], a.w41[5], f, PI) +
+                                    tfwd(a.w40[7], a.w41[7], f, PJ));
+    a.dst[0][f] = l0;
+    a.dst[1][f] = l1;
+    a.dst[2][f] = l2;
+    if (mask && mask[f]) return;
+    const long long col = col_index(g, i, j);
+    const bool interior = i >= v.ibk && i <= v.iek && j >= v.jbk && j <= v.jek && k <= v.kek;
+    const int s = interior ? band_sign(__ldg(&v.band[col]), k) : -1;
+    const Gb3 g0 = (interior && v.gb[0]) ? gb_load(v, f) : Gb3{};
+    const RAdjVelOps o{v, f, {l0, l1, l2}};
+    adj_vel_cell(v, o, col, k, i, j, f, s, g0);
+}
+
+// transpose of the velocity recorder (m_wav.f90:530-535): residuals as
+// sources.  A recorder averages two cells per component (Vx at i and i-1, Vy
+// at j and j-1, Vz at k and k-1, the latter with the sign of an upward z), so
+// its residual r enters both; one thread per receiving cell adds the
+// residuals of its stations in station order (cells that several stations
+// share get the same bits in every run).  With WEIGHTS the thread then forms
+// the velocity-phase weights of the next adjoint step for its cell from the
+// new lambda_V (the cells the fused gather left out).
+struct SrcArgs {
+    Geo g;
+    const int *cells;       // (k, i, j) per receiving cell
+    const int *offs;        // n + 1 offsets into contrib
+    const int *contrib;     // station << 2 | component
+    int n, ntw, itw;
+    const float *res;
+    float scale;
+    float *lV[3];
+};
+
+template <bool WEIGHTS>
+__global__ void __launch_bounds__(128) adj_source_cells_kernel(const SrcArgs a, const AdjVelArgs v) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.n) return;
+    const Geo g = a.g;
+    const int k = a.cells[3 * q], i = a.cells[3 * q + 1], j = a.cells[3 * q + 2];
+    const long long e = cell_index(g, k, i, j);
+    float l[3] = {a.lV[0][e], a.lV[1][e], a.lV[2][e]};
+    for (int t = a.offs[q]; t < a.offs[q + 1]; t++) {
+        const int w = a.contrib[t], n = w >> 2, c = w & 3;
+        const float r = a.res[((long long)n * 3 + c) * a.ntw + a.itw - 1] * a.scale;
+        l[c] = l[c] + (c == 2 ? -r : r);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) a.lV[c][e] = l[c];
+    if (!WEIGHTS || k < 1 || k > g.nz || i < 1 || i > g.nx || j < 1 || j > g.ny) return;
+    const long long col = col_index(g, i, j);
+    const bool interior = i >= v.ibk && i <= v.iek && j >= v.jbk && j <= v.jek && k <= v.kek;
+    const int s = interior ? band_sign(__ldg(&v.band[col]), k) : -1;
+    const Gb3 g0 = (interior && v.gb[0]) ? gb_load(v, e) : Gb3{};
+    const RAdjVelOps o{v, e, {l[0], l[1], l[2]}};
+    adj_vel_cell(v, o, col, k, i, j, e, s, g0);
 }
 
 __global__ void zero_double_kernel(double *p, long long n) {
@@ -691,6 +765,8 @@ static int adj_alloc(swpc_ctx *c) {
     for (int q = 0; q < 9; q++) {
         int rc = dalloc(c, &s->w40[q], n);
         if (!rc) rc = dalloc(c, &s->w41[q], n);
+        if (!rc) rc = dalloc(c, &s->w40v[q], n);
+        if (!rc) rc = dalloc(c, &s->w41v[q], n);
         if (rc) return rc;
     }
     for (int q = 0; q < 8; q++) { int rc = dalloc(c, &s->grad[q], n); if (rc) return rc; }
@@ -707,6 +783,10 @@ void adj_free(swpc_ctx *c) {
     for (auto p : s->laux) if (p) cudaFree(p);
     for (auto p : s->w40) if (p) cudaFree(p);
     for (auto p : s->w41) if (p) cudaFree(p);
+    for (auto p : s->w40v) if (p) cudaFree(p);
+    for (auto p : s->w41v) if (p) cudaFree(p);
+    if (s->srcmask) cudaFree(s->srcmask);
+    if (s->srccells) cudaFree(s->srccells);
     for (auto p : s->grad) if (p) cudaFree(p);
     for (auto p : s->gpart) if (p) cudaFree(p);
     if (s->res) cudaFree(s->res);
@@ -756,37 +836,58 @@ static cudaError_t adj_stress_tma(const swpc_adj_state *s, const AdjStrArgs &a, 
     return cudaGetLastError();
 }
 
+// Arguments of the velocity-phase weights: from lambda_V into the
+// velocity-phase weight arrays, with the gradient of b when divS (the forward
+// stress divergences of that step) is given.
+static AdjVelArgs vel_args(swpc_ctx *c, const float *const *divS) {
+    swpc_adj_state *s = c->adj;
+    AdjVelArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
+    for (int q = 0; q < 3; q++) { a.lV[q] = s->lV[q]; a.b[q] = c->med[5 + q]; }
+    a.band = c->band; a.pmlcol = c->pmlcol;
+    for (int q = 0; q < 9; q++) a.laS[q] = s->laux[9 + q];
+    a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
+    memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
+    a.dt = c->d.dt;
+    for (int q = 0; q < 9; q++) { a.w40[q] = s->w40v[q]; a.w41[q] = s->w41v[q]; }
+    if (divS) {
+        for (int q = 0; q < 3; q++) a.divS[q] = divS[q];
+        for (int q = 0; q < 3; q++) a.gb[q] = s->gpart[5 + q];
+    }
+    return a;
+}
+
+// What the stress-phase gather of a step also does: form the velocity-phase
+// weights of the next adjoint step (on = true), with that step's forward
+// stress divergences divS (gradient) and leaving the cells that receiver
+// residuals change this step to the injection (skip_src).
+struct AdjNext {
+    bool on = false, skip_src = false;
+    const float *const *divS = nullptr;
+};
+
 // one transposed step: vel^T then stress^T; with gradient when S_after /
 // V_before are given (for the staged stress-phase weights, V_before is field
-// fv of the slots buffer)
-static int adj_step(swpc_ctx *c, const float *const *divS_after, const float *const *V_before, int fv) {
+// fv of the slots buffer); vel_done: the velocity-phase weights were formed
+// by the previous step's stress-phase gather
+static int adj_step(swpc_ctx *c, const float *const *divS_after, const float *const *V_before, int fv,
+                    bool vel_done = false, const AdjNext &next = AdjNext()) {
     swpc_adj_state *s = c->adj;
     const dim3 block(kThreadsK, 2, 2);
     const dim3 grid = cell_grid(c->g, block);
     const bool grad = divS_after != nullptr;
     {
-        AdjVelArgs a;
-        memset(&a, 0, sizeof(a));
-        a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
-        for (int q = 0; q < 3; q++) { a.lV[q] = s->lV[q]; a.b[q] = c->med[5 + q]; }
-        a.band = c->band; a.pmlcol = c->pmlcol;
-        for (int q = 0; q < 9; q++) a.laS[q] = s->laux[9 + q];
-        a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
-        memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
-        a.dt = c->d.dt;
-        for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
-        if (grad) {
-            for (int q = 0; q < 3; q++) a.divS[q] = divS_after[q];
-            for (int q = 0; q < 3; q++) a.gb[q] = s->gpart[5 + q];
+        if (!vel_done) {
+            // one cell per thread: the kernel is bound by its 18 weight stores, and
+            // staging its few loads (a TMA-staged form was tried) made it slower
+            adj_vel_weights_kernel<<<grid, block, 0, c->stream>>>(vel_args(c, grad ? divS_after : nullptr));
+            ACK(cudaGetLastError());
         }
-        // one cell per thread: the kernel is bound by its 18 weight stores, and
-        // staging its few loads (a TMA-staged form was tried) made it slower
-        adj_vel_weights_kernel<<<grid, block, 0, c->stream>>>(a);
-        ACK(cudaGetLastError());
         GatherArgs ga;
         ga.g = c->g;
         for (int q = 0; q < 6; q++) ga.dst[q] = s->lS[q];
-        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
+        for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40v[q]; ga.w41[q] = s->w41v[q]; }
         adj_vel_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
         ACK(cudaGetLastError());
     }
@@ -833,23 +934,102 @@ static int adj_step(swpc_ctx *c, const float *const *divS_after, const float *co
         for (int q = 0; q < 3; q++) ga.dst[q] = s->lV[q];
         for (int q = 3; q < 6; q++) ga.dst[q] = nullptr;
         for (int q = 0; q < 9; q++) { ga.w40[q] = s->w40[q]; ga.w41[q] = s->w41[q]; }
-        adj_stress_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
+        if (next.on)
+            adj_stress_gather_vel_kernel<<<grid, block, 0, c->stream>>>(ga, vel_args(c, next.divS),
+                                                                         next.skip_src ? s->srcmask : nullptr);
+        else
+            adj_stress_gather_kernel<<<grid, block, 0, c->stream>>>(ga);
         ACK(cudaGetLastError());
     }
     return SWPC_OK;
 }
 
-static int adj_source(swpc_ctx *c, int it) {
+// whether adj_source injects receiver residuals at step it
+static bool source_at(const swpc_ctx *c, int it) {
+    const swpc_adj_state *s = c->adj;
+    if (!s->res || c->nst <= 0 || !(c->wav_what & SWPC_WAV_V)) return false;
+    if ((it - 1) % c->ntdec_w != 0) return false;
+    return (it - 1) / c->ntdec_w + 1 <= c->ntw;
+}
+
+// residuals of step it into lambda_V; with divS_next (the fused path) the
+// receiving cells also form the velocity-phase weights of step it - 1
+static int adj_source(swpc_ctx *c, int it, const float *const *divS_next = nullptr, bool weights = false) {
     swpc_adj_state *s = c->adj;
-    if (!s->res || c->nst <= 0 || !(c->wav_what & SWPC_WAV_V)) return SWPC_OK;
-    if ((it - 1) % c->ntdec_w != 0) return SWPC_OK;
-    const int itw = (it - 1) / c->ntdec_w + 1;
-    if (itw > c->ntw) return SWPC_OK;
+    if (!source_at(c, it) || s->nsrc <= 0) return SWPC_OK;
+    SrcArgs a;
+    a.g = c->g;
+    a.cells = s->srccells;
+    a.offs = s->srccells + 3 * s->nsrc;
+    a.contrib = a.offs + s->nsrc + 1;
+    a.n = s->nsrc;
+    a.ntw = c->ntw;
+    a.itw = (it - 1) / c->ntdec_w + 1;
+    a.res = s->res;
     // d(trace)/dV = 0.5 M0 UC 1e9 per cell of the two-cell average
-    const float scale = 0.5f * c->M0 * c->UC * 1e9f;
-    adj_source_kernel<<<(c->nst + 127) / 128, 128, 0, c->stream>>>(c->g, c->st_ijk, c->nst, c->ntw, itw, s->res, scale,
-                                                                    s->lV[0], s->lV[1], s->lV[2]);
-    return cuda_check(c, cudaGetLastError(), "adj_source_kernel");
+    a.scale = 0.5f * c->M0 * c->UC * 1e9f;
+    for (int q = 0; q < 3; q++) a.lV[q] = s->lV[q];
+    const unsigned nb = (unsigned)((s->nsrc + 127) / 128);
+    if (weights) adj_source_cells_kernel<true><<<nb, 128, 0, c->stream>>>(a, vel_args(c, divS_next));
+    else adj_source_cells_kernel<false><<<nb, 128, 0, c->stream>>>(a, AdjVelArgs{});
+    return cuda_check(c, cudaGetLastError(), "adj_source_cells_kernel");
+}
+
+// The cells whose lambda_V adj_source changes (both cells of each recorder's
+// two-cell averages, inside the memory box or not), with the residuals each
+// receives in station order, and the mask of those cells.
+static int source_cells(swpc_ctx *c) {
+    swpc_adj_state *s = c->adj;
+    const Geo &g = c->g;
+    std::vector<int> st(3 * (size_t)std::max(c->nst, 0));
+    if (c->nst > 0) {
+        ACK(cudaMemcpyAsync(st.data(), c->st_ijk, st.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        ACK(cudaStreamSynchronize(c->stream));
+    }
+    struct Contrib { long long e; int k, i, j, n, cmp; };
+    std::vector<Contrib> all;
+    for (int n = 0; n < c->nst; n++) {
+        const int i = st[3 * n], j = st[3 * n + 1], k = st[3 * n + 2];
+        const int nb[6][4] = {{k, i, j, 0}, {k, i - 1, j, 0}, {k, i, j, 1}, {k, i, j - 1, 1}, {k, i, j, 2},
+                              {k - 1, i, j, 2}};
+        for (auto &q : nb) all.push_back({cell_index(g, q[0], q[1], q[2]), q[0], q[1], q[2], n, q[3]});
+    }
+    // by cell, then station: the order of each cell's sums
+    std::stable_sort(all.begin(), all.end(), [](const Contrib &a, const Contrib &b) {
+        return a.e != b.e ? a.e < b.e : a.n < b.n;
+    });
+    std::vector<int> cells, offs, contrib;
+    for (size_t t = 0; t < all.size(); t++) {
+        if (t == 0 || all[t].e != all[t - 1].e) {
+            cells.insert(cells.end(), {all[t].k, all[t].i, all[t].j});
+            offs.push_back((int)t);
+        }
+        contrib.push_back(all[t].n << 2 | all[t].cmp);
+    }
+    offs.push_back((int)all.size());
+    const int ncell = (int)cells.size() / 3;
+    std::vector<int> packed(cells);
+    packed.insert(packed.end(), offs.begin(), offs.end());
+    packed.insert(packed.end(), contrib.begin(), contrib.end());
+    if (s->srccells) { cudaFree(s->srccells); s->srccells = nullptr; }
+    s->nsrc = s->nsrc_contrib = 0;
+    if (!s->srcmask && cudaMalloc((void **)&s->srcmask, (size_t)g.ncell) != cudaSuccess) {
+        cudaGetLastError();
+        s->srcmask = nullptr;
+        return err(c, SWPC_ERR_NOMEM, "no room for the receiver cell mask");
+    }
+    ACK(cudaMemsetAsync(s->srcmask, 0, (size_t)g.ncell, c->stream));
+    if (ncell > 0) {
+        ACK(cudaMalloc((void **)&s->srccells, packed.size() * sizeof(int)));
+        ACK(cudaMemcpyAsync(s->srccells, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            c->stream));
+        s->nsrc = ncell;
+        s->nsrc_contrib = (int)contrib.size();
+        mark_cells_kernel<<<(ncell + 127) / 128, 128, 0, c->stream>>>(g, s->srccells, ncell, s->srcmask);
+        ACK(cudaGetLastError());
+        ACK(cudaStreamSynchronize(c->stream));   // the host list goes out of scope
+    }
+    return SWPC_OK;
 }
 
 static int zero_adjoint(swpc_ctx *c) {
@@ -1096,7 +1276,8 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     *misfit = J;
     ACK(cudaMemcpyAsync(s->res, syn.data(), nres * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     // 3. adjoint, segment by segment from the last
-    rc = zero_adjoint(c);
+    rc = source_cells(c);
+    if (!rc) rc = zero_adjoint(c);
     if (rc) return rc;
     for (int g = nseg - 1; g >= 0; g--) {
         const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt);
@@ -1113,15 +1294,24 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
                 if (!rc) rc = save_slot(c, it - it0 + 1);
             }
         }
+        // within a segment each stress-phase gather also forms the velocity-phase weights of the step before
+        // (kernel 9 of swpc_set_launch); the first step of a segment forms its own
+        bool vel_done = false;
         for (int it = it1; it >= it0 && !rc; it--) {
             const size_t sa = base + (size_t)(it - it0 + 1), sb = base + (size_t)(it - it0);
             const float *base_a = s->slots + sa * slot_floats;
             const float *base_b = s->slots + sb * slot_floats;
-            const float *Da[3], *Vb[3];
+            const float *Da[3], *Vb[3], *Dn[3];
             for (int q = 0; q < 3; q++) Da[q] = base_a + (3 + q) * n;
             for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
-            rc = adj_step(c, Da, Vb, (int)(sb * kSlotFields));
-            if (!rc) rc = adj_source(c, it);
+            for (int q = 0; q < 3; q++) Dn[q] = base_b + (3 + q) * n;   // divergences of step it - 1
+            AdjNext nx;
+            nx.on = c->adj_fuse && it > it0;
+            nx.skip_src = source_at(c, it);
+            nx.divS = Dn;
+            rc = adj_step(c, Da, Vb, (int)(sb * kSlotFields), vel_done, nx);
+            if (!rc) rc = adj_source(c, it, Dn, nx.on);
+            vel_done = nx.on;
         }
         if (!rc) rc = fold_gradient(c);
         if (rc) return rc;

@@ -286,6 +286,13 @@ extern "C" int swpc_set_launch(swpc_ctx *c, int kernel, int minb, int bi, int bj
         c->adj_tma = bi == 1;
         return SWPC_OK;
     }
+    if (kernel == 9) {
+        // adjoint velocity-phase weights: bi = 1 formed by the stress-phase gather of the step before (the
+        // gradient's default), 0 by their own kernel
+        if (!is3d(c) || (bi != 0 && bi != 1)) return set_err(c, SWPC_ERR_ARG, "kernel 9 (3D): bi = 0 or 1");
+        c->adj_fuse = bi == 1;
+        return SWPC_OK;
+    }
     if (kernel == 7) {
         // launch order of the staged kernels: blocks of bi j tiles (0: chosen by size)
         if (bi < 0 || bi > 1024) return set_err(c, SWPC_ERR_ARG, "kernel 7: bi = j tiles per block, 0..1024");

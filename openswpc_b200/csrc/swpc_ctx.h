@@ -189,6 +189,7 @@ struct swpc_ctx {
     bool stress_tma = false, vel_tma = false;
     int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 4;
     bool adj_tma = true;          // staged stress-phase adjoint weights (swpc_adjoint.cu)
+    bool adj_fuse = true;         // velocity-phase adjoint weights formed by the stress-phase gather before
     int tile_jblock = 0;          // j tiles per block of the staged launch order (0: by size, see tma_tiles)
     void *tmaps = nullptr;        // swpc::TmaMaps
     int tma_key[4] = {-1, -1, -1, -1};

@@ -202,6 +202,43 @@ def test_gradient_with_kept_slots_gives_the_bits_of_the_full_recompute():
     g.close()
 
 
+@pytest.mark.parametrize("ntdec_w", [1, 3])
+def test_velocity_weights_formed_in_the_stress_gather_give_the_same_bits(ntdec_w):
+    """The velocity-phase weights formed inside the stress-phase gather of the
+    step before (swpc_set_launch kernel 9, the default) against their own
+    kernel in every step: same misfit, gradients, final adjoint state, bit for
+    bit.  Stations share cells (i and i+1 neighbours, two at one point), one
+    sits in the PML, and with ntdec_w = 3 residuals enter every third step
+    only; with and without kept slots."""
+    from openswpc_b200.params import Station
+    p = small3d(nt=45, ntdec_w=ntdec_w)
+    xb, yb = p.xbeg, p.ybeg
+    extra = [Station(xb + 14.25, yb + 11.25, 2.0, "a", "dep"), Station(xb + 14.75, yb + 11.25, 2.0, "b", "dep"),
+             Station(xb + 14.75, yb + 11.25, 2.0, "c", "dep"), Station(xb + 14.75, yb + 11.75, 2.5, "d", "dep"),
+             Station(xb + 1.75, yb + 9.25, 4.0, "pml", "dep")]
+    p.stations = list(p.stations) + extra
+    xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+    runs = []
+    for fuse, slots in ((0, 0), (1, 0), (1, 20)):
+        g = Swpc3D(p, xi)
+        check(g.ctx, g.lib.swpc_set_launch(g.ctx, 9, 1, fuse, 1))
+        ck, sl = C.c_longlong(), C.c_longlong()
+        check(g.ctx, g.lib.swpc_gradient_memory(g.ctx, C.byref(ck), C.byref(sl)))
+        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, slots * sl.value))
+        rng = np.random.default_rng(3)
+        obs = (rng.standard_normal((g.nst, 3, (p.nt - 1) // ntdec_w + 1)) * 1e-3).astype(np.float32)
+        runs.append(_gradient_bits(g, p, obs, 10))
+        g.close()
+    J0, g0, a0, _ = runs[0]
+    assert any(np.abs(x).max() > 0 for x in g0)
+    for J1, g1, a1, _ in runs[1:]:
+        assert J1 == J0
+        for w, (x, y) in enumerate(zip(g1, g0)):
+            assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), w
+        for (fid, _), x, y in zip(fields(p), a1, a0):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), fid
+
+
 def forward_misfit(g, p, obs):
     check(g.ctx, g.lib.swpc_upload_medium(g.ctx, C.byref(g.medium.view())))
     for fid in range(9):
