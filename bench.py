@@ -110,8 +110,9 @@ B_ADJ_PML = (12 + 12 + 72 + 72) + (72 + 48) + (24 + 20 + 72 + 72) + (72 + 24)
 # inside a checkpoint segment the stress gather of each step forms the velocity weights of the next from the lV it
 # has just summed, so every step but the first of a segment reads lV once instead of twice
 B_ADJ_FUSED_SAVES = 12
-# every recomputed step: V copied into the segment's slot (read and written, every cell), and the three stress
-# divergences of the interior cells formed from S (six read, three written)
+# every forward step whose slot is kept or recomputed: V copied into the slot over the kernel region with a two-cell
+# halo in i, j and k (read and written), and the three stress divergences of the interior cells formed from S (six
+# read, three written)
 B_SLOT = 3 * 4 * 2
 B_SLOT_INT = 6 * 4 + 3 * 4
 # V, S and R (27 fields) saved at each checkpoint and restored before the segment's recompute; at the end of each
@@ -690,8 +691,9 @@ def bench_c3(args, world, rank, local):
     nseg = -(-p.nt // ckpt)
     nrec = -(-(p.nt - kept) // ckpt)
     b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
+    n_slot = (p.nx - 2 * p.na + 4) * (p.ny - 2 * p.na + 4) * (p.nz - p.na + 2)
     b_grad = ((2 * p.nt - kept) * b_fwd
-              + p.nt * ((n_int + n_pml) * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
+              + p.nt * (n_slot * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
               - (p.nt - nseg) * (n_int + n_pml) * B_ADJ_FUSED_SAVES
               + nrec * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()

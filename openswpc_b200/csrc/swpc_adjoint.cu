@@ -75,6 +75,20 @@ namespace {
 
 constexpr int kThreadsK = 32;
 
+// Layout of a recompute slot: the box of the kernel region with a two-cell
+// halo in i and j (i0 = ibk - 2, j0 = jbk - 2) over k up to kek + 2, the part
+// of V the imaging condition reads (the stress-phase gradient takes V at
+// i-2..i+2, j-2..j+2, k-2..k+2 of interior cells) and of the divergences it
+// needs (interior cells).  Cell (k, i, j) at ((j - j0) * Ip + (i - i0)) * Kp +
+// (k - 1 + KH): the k origin of the memory box, so TMA boxes keep their x.
+struct SlotGeo {
+    int Kp, Ip, Jp, i0, j0;
+    long long n;
+};
+__host__ __device__ __forceinline__ long long slot_index(const SlotGeo &s, int k, int i, int j) {
+    return ((long long)(j - s.j0) * s.Ip + (i - s.i0)) * s.Kp + (k - 1 + KH);
+}
+
 struct AdjVelArgs {
     Geo g;
     int ibk, iek, jbk, jek, kek;
@@ -86,8 +100,9 @@ struct AdjVelArgs {
     const float4 *gxc, *gxe, *gyc, *gye, *gzc, *gze;
     float e40[3][2], e41[3][2], r20[3], dt;
     float *w40[9], *w41[9];
-    const float *divS[3];        // forward stress divergences after the stress update (gradient)
+    const float *divS[3];        // forward stress divergences after the stress update (gradient, slot layout)
     float *gb[3];                // segment partials of the bx, by, bz gradient (null: none)
+    SlotGeo sg;
 };
 
 struct AdjStrArgs {
@@ -103,8 +118,9 @@ struct AdjStrArgs {
     float e40[3][2], e41[3][2], r20[3], dt;
     float c1[NM_MAX], c2[NM_MAX], d1[NM_MAX], d2;
     float *w40[9], *w41[9];
-    const float *V[3];           // forward V before the stress update (gradient)
+    const float *V[3];           // forward V before the stress update (gradient, slot layout)
     float *gm[5];                // segment partials of the lam, mu, muyz, muxz, muxy gradient (null: none)
+    SlotGeo sg;
 };
 
 struct GatherArgs {
@@ -196,7 +212,8 @@ __device__ __forceinline__ void adj_vel_cell(const AdjVelArgs &a, const O &o, lo
             // d(Vx)/d(bx) = d3Sx3 * dt, the divergences of the forward S after
             // the stress update (formed once per step of the recompute)
 #pragma unroll
-            for (int q = 0; q < 3; q++) a.gb[q][e] = (float)(g0.v[q] + (double)l[q] * __ldcs(a.divS[q] + e) * dt);
+            const long long es = slot_index(a.sg, k, i, j);
+            for (int q = 0; q < 3; q++) a.gb[q][e] = (float)(g0.v[q] + (double)l[q] * __ldcs(a.divS[q] + es) * dt);
         }
         return;
     }
@@ -271,7 +288,7 @@ __global__ void __launch_bounds__(128) adj_vel_gather_kernel(const GatherArgs a)
 // memory, the staged kernel from the tiles TMA copied to shared memory.
 struct GAdjStrOps {
     const AdjStrArgs &a;
-    long long e, PI, PJ;
+    long long e, es, PI, PJ;     // es, PI, PJ: V in the slot layout
     __device__ __forceinline__ float lS(int c) const { return a.lS[c][e]; }
     __device__ __forceinline__ float lR(int q) const { return a.lR[q][e]; }
     __device__ __forceinline__ float med(int m) const {
@@ -280,7 +297,7 @@ struct GAdjStrOps {
         return p[e];
     }
     __device__ __forceinline__ float V(int c, int dk, int di, int dj) const {
-        return a.V[c][e + dk + di * PI + dj * PJ];
+        return a.V[c][es + dk + di * PI + dj * PJ];
     }
 };
 
@@ -435,7 +452,7 @@ __global__ void __launch_bounds__(128) adj_stress_weights_kernel(const AdjStrArg
     if (!cell_of(g, k, i, j)) return;
     const long long col = col_index(g, i, j);
     const long long e = col * g.Kp + (k - 1 + KH);
-    const GAdjStrOps o{a, e, (long long)g.Kp, (long long)g.Kp * g.Ip};
+    const GAdjStrOps o{a, e, slot_index(a.sg, k, i, j), (long long)a.sg.Kp, (long long)a.sg.Kp * a.sg.Ip};
     if (i >= a.ibk && i <= a.iek && j >= a.jbk && j <= a.jek && k <= a.kek) {
         const Gm5 g0 = a.gm[0] ? gm_load(a, e) : Gm5{};
         adj_stress_interior<NM>(a, o, band_sign(__ldg(&a.band[col]), k), e, g0);
@@ -497,7 +514,9 @@ __global__ void __launch_bounds__(adjt::NT, (tma::blocks_per_sm<adjt::Boxes<NM>:
         const int x0 = T.k0 - 1 + KH;
         load_4d(sm, &tm_med, x0, T.i0 + 2, T.j0 + 2, t.f_med, &bar);
         load_4d(sm + L::oState, with_r ? &tm_state : &tm_s, x0, T.i0 + 2, T.j0 + 2, t.f_state, &bar);
-        if (GRAD) load_4d(sm + L::oV, &tm_v, x0 - 4, T.i0, T.j0, fv, &bar);
+        // V with its halo from the slot: the box starts at cell (k0 - 4, i0 - 2, j0 - 2); tiles of the absorber
+        // may reach outside the slot box, where the copy fills zeros that no interior cell reads
+        if (GRAD) load_4d(sm + L::oV, &tm_v, x0 - 4, T.i0 - 2 - a.sg.i0, T.j0 - 2 - a.sg.j0, fv, &bar);
         limit = wait_limit(t.err);
     }
     const int k = T.k0 + tx, i = T.i0 + ty, j = T.j0 + tz;
@@ -622,7 +641,8 @@ struct SlotDivArgs {
     const float *S[6];
     const int4 *band;
     float e40[3][2], e41[3][2];
-    float *divS[3];
+    float *divS[3];              // slot layout
+    SlotGeo sg;
 };
 __global__ void __launch_bounds__(128) slot_div_kernel(const SlotDivArgs a) {
     const Geo g = a.g;
@@ -636,7 +656,28 @@ __global__ void __launch_bounds__(128) slot_div_kernel(const SlotDivArgs a) {
     float d[3];
     stress_divergence(a.e40, a.e41, band_sign(__ldg(&a.band[col]), k), S, d);
 #pragma unroll
-    for (int q = 0; q < 3; q++) __stcs(a.divS[q] + e, d[q]);
+    const long long es = slot_index(a.sg, k, i, j);
+#pragma unroll
+    for (int q = 0; q < 3; q++) __stcs(a.divS[q] + es, d[q]);
+}
+
+// V over the slot box into a slot (float4 along k: both pitches are multiples
+// of 8 floats and the slot's k extent is not larger than the memory box's)
+__global__ void slot_v_kernel(Geo g, SlotGeo sg, const float *vx, const float *vy, const float *vz, float *dst) {
+    const int k4 = sg.Kp / 4;
+    const long long per = (long long)sg.Jp * sg.Ip * k4;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * per;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / per);
+        const long long r = t - c * per;
+        const int kq = (int)(r % k4);
+        const long long colq = r / k4;
+        const int is = (int)(colq % sg.Ip), js = (int)(colq / sg.Ip);
+        const float *src = c == 0 ? vx : c == 1 ? vy : vz;
+        const long long from = col_index(g, is + sg.i0, js + sg.j0) * g.Kp + 4LL * kq;
+        const long long to = (long long)c * sg.n + colq * sg.Kp + 4LL * kq;
+        __stcs(reinterpret_cast<float4 *>(dst + to), __ldcs(reinterpret_cast<const float4 *>(src + from)));
+    }
 }
 
 // the segment's FP32 partial sums into the FP64 totals; the partials restart from zero
@@ -836,6 +877,17 @@ static cudaError_t adj_stress_tma(const swpc_adj_state *s, const AdjStrArgs &a, 
     return cudaGetLastError();
 }
 
+static SlotGeo slot_geo(const swpc_ctx *c) {
+    SlotGeo sg;
+    sg.i0 = c->ibk - 2;
+    sg.j0 = c->jbk - 2;
+    sg.Ip = c->iek - c->ibk + 5;
+    sg.Jp = c->jek - c->jbk + 5;
+    sg.Kp = ((c->kek + 3 + KH) + 7) / 8 * 8;
+    sg.n = (long long)sg.Kp * sg.Ip * sg.Jp;
+    return sg;
+}
+
 // Arguments of the velocity-phase weights: from lambda_V into the
 // velocity-phase weight arrays, with the gradient of b when divS (the forward
 // stress divergences of that step) is given.
@@ -850,6 +902,7 @@ static AdjVelArgs vel_args(swpc_ctx *c, const float *const *divS) {
     a.gxc = c->gx[0]; a.gxe = c->gx[1]; a.gyc = c->gy[0]; a.gye = c->gy[1]; a.gzc = c->gz[0]; a.gze = c->gz[1];
     memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
     a.dt = c->d.dt;
+    a.sg = slot_geo(c);
     for (int q = 0; q < 9; q++) { a.w40[q] = s->w40v[q]; a.w41[q] = s->w41v[q]; }
     if (divS) {
         for (int q = 0; q < 3; q++) a.divS[q] = divS[q];
@@ -906,6 +959,7 @@ static int adj_step(swpc_ctx *c, const float *const *divS_after, const float *co
         a.dt = c->d.dt;
         memcpy(a.c1, c->c1, sizeof(a.c1)); memcpy(a.c2, c->c2, sizeof(a.c2)); memcpy(a.d1, c->d1, sizeof(a.d1));
         a.d2 = c->d2;
+        a.sg = slot_geo(c);
         for (int q = 0; q < 9; q++) { a.w40[q] = s->w40[q]; a.w41[q] = s->w41[q]; }
         if (grad) {
             for (int q = 0; q < 3; q++) a.V[q] = V_before[q];
@@ -1129,20 +1183,22 @@ static int copy_state(swpc_ctx *c, float *ck, bool save) {
     return SWPC_OK;
 }
 
-// Slot `slot` of the recompute: V (the whole memory box, read with its halo by
+// Slot `slot` of the recompute: V over the slot box (read with its halo by
 // the stress-phase weights) and the stress divergences of the interior cells
-// (the velocity-phase gradient), kSlotFields fields of ncell floats.
+// (the velocity-phase gradient), kSlotFields fields in the slot layout.
 constexpr int kSlotFields = 6;
 static int save_slot(swpc_ctx *c, int slot) {
-    const size_t n = c->g.ncell;
-    float *base = c->adj->slots + (size_t)slot * kSlotFields * n;
-    for (int q = 0; q < 3; q++) ACK(cudaMemcpyAsync(base + q * n, c->V[q], n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    const SlotGeo sg = slot_geo(c);
+    float *base = c->adj->slots + (size_t)slot * kSlotFields * sg.n;
+    slot_v_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], base);
+    ACK(cudaGetLastError());
     SlotDivArgs a;
     a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
     for (int q = 0; q < 6; q++) a.S[q] = c->S[q];
     a.band = c->band;
     memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41));
-    for (int q = 0; q < 3; q++) a.divS[q] = base + (3 + q) * n;
+    for (int q = 0; q < 3; q++) a.divS[q] = base + (3 + q) * sg.n;
+    a.sg = sg;
     const dim3 block(kThreadsK, 2, 2);
     slot_div_kernel<<<cell_grid(c->g, block), block, 0, c->stream>>>(a);
     return cuda_check(c, cudaGetLastError(), "slot_div_kernel");
@@ -1187,7 +1243,7 @@ extern "C" int swpc_gradient_memory(swpc_ctx *c, long long *ckpt_bytes, long lon
     long long ckf = 0;
     for (size_t v : sz) ckf += (long long)v;
     *ckpt_bytes = ckf * (long long)sizeof(float);
-    *slot_bytes = (long long)kSlotFields * c->g.ncell * (long long)sizeof(float);
+    *slot_bytes = (long long)kSlotFields * slot_geo(c).n * (long long)sizeof(float);
     return SWPC_OK;
 }
 
@@ -1218,7 +1274,8 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     state_arrays(c, &sz);
     size_t ckf = 0;
     for (size_t v : sz) ckf += v;
-    const size_t n = c->g.ncell, slot_floats = (size_t)kSlotFields * n;
+    const SlotGeo sg = slot_geo(c);
+    const size_t n = (size_t)sg.n, slot_floats = (size_t)kSlotFields * n;
     // the trailing segments whose slots fit the budget keep them from the first forward pass and are not
     // recomputed (nor checkpointed); the earlier segments recompute into the same slots once those are spent
     long long tail_steps = 0;
@@ -1241,7 +1298,9 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
         }
         s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf; s->slot_cap = cap; s->ntail = ntail;
         // the staged stress-phase weights read the forward V of a slot with its halo
-        if (!tma_encode_box(s->maps->vh, s->slots, c->g, (long long)kSlotFields * cap, tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
+        Geo gs = c->g;
+        gs.Kp = sg.Kp; gs.Ip = sg.Ip; gs.Jp = sg.Jp; gs.ncell = sg.n;
+        if (!tma_encode_box(s->maps->vh, s->slots, gs, (long long)kSlotFields * cap, tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
             return err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the recompute slots");
     }
     const size_t nres = (size_t)c->nst * 3 * c->ntw;
