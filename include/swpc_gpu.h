@@ -193,6 +193,13 @@ int swpc_vmodel_lhm_device_opt(swpc_ctx *ctx, int nlayer, const float *depth, co
                                float zbeg, const float *xi, int ld_k, int ld_i, int munk_profile);
 int swpc_vmodel_upload(swpc_ctx *ctx, const float *rho, const float *lam, const float *mu, const float *qp,
                        const float *qs, int ld_k, int ld_i);
+/* Step 1 from device memory: per-cell vp, vs, rho, qp, qs as device arrays
+ * over the memory box (leading extents ld_k, ld_i), the moduli formed on the
+ * device as vmodel_lhm forms them (m_vmodel_lhm.f90:146-148, mu = rho vs vs,
+ * lam = rho (vp vp - 2 vs vs)); bitwise swpc_vmodel_upload of the moduli a
+ * host computes in that order.  For models that already live on the GPU. */
+int swpc_vmodel_velocity_device(swpc_ctx *ctx, const float *vp, const float *vs, const float *rho, const float *qp,
+                                const float *qs, int ld_k, int ld_i);
 int swpc_medium_setup_device(swpc_ctx *ctx, float fq_min, float fq_max, float fq_ref, float *ts, float *scal,
                              int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top, int *kob_bot, int *kbeg_a,
                              int ld_i2);
@@ -424,6 +431,10 @@ int swpc_gradient_fetch(swpc_ctx *ctx, int which, double *out, int ld_k, int ld_
  * lacks the terms of averaged entries that fall in the absorber. */
 int swpc_gradient_model(swpc_ctx *ctx, const float *vp, const float *vs, const float *rho, int ld_k, int ld_i,
                         double *gvp, double *gvs, double *grho);
+/* The same with vp, vs, rho and the three gradients as device arrays over
+ * the memory box (no host copies). */
+int swpc_gradient_model_device(swpc_ctx *ctx, const float *vp, const float *vs, const float *rho, int ld_k, int ld_i,
+                               double *gvp, double *gvs, double *grho);
 
 /* ---- reciprocity batch (3D) ---------------------------------------------- */
 

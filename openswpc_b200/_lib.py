@@ -45,7 +45,8 @@ EXPORTS = [
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
     "swpc_adj_reset", "swpc_adj_step_linear", "swpc_adj_upload", "swpc_adj_download", "swpc_gradient",
-    "swpc_gradient_set_slot_memory", "swpc_gradient_memory",
+    "swpc_gradient_set_slot_memory", "swpc_gradient_memory", "swpc_gradient_model_device",
+    "swpc_vmodel_velocity_device",
     "swpc_gradient_fetch", "swpc_gradient_model", "swpc_reset_state",
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
     # swpc_setup.h
@@ -144,6 +145,7 @@ def load():
         "swpc_vmodel_lhm_device": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i]),
         "swpc_vmodel_lhm_device_opt": (i, [vp, i, _FP, _FP, _FP, _FP, _FP, _FP, f, f, f, _FP, i, i, i]),
         "swpc_vmodel_upload": (i, [vp, _FP, _FP, _FP, _FP, _FP, i, i]),
+        "swpc_vmodel_velocity_device": (i, [vp, vp, vp, vp, vp, vp, i, i]),
         "swpc_medium_setup_device": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i]),
         "swpc_medium_setup_device_opt": (i, [vp, f, f, f, _FP, _FP, _IP, _IP, _IP, _IP, _IP, _IP, _IP, i, i]),
         "swpc_kernel_setup": (i, [vp, _FP]),
@@ -184,6 +186,7 @@ def load():
         "swpc_gradient_fetch": (i, [vp, i, C.POINTER(C.c_double), i, i]),
         "swpc_gradient_model": (i, [vp, _FP, _FP, _FP, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),
+        "swpc_gradient_model_device": (i, [vp, vp, vp, vp, i, i, vp, vp, vp]),
         "swpc_device_bytes": (C.c_longlong, [vp]),
         "swpc_set_launch": (i, [vp, i, i, i, i]),
         "swpc_x2i": (i, [f, f, f]),

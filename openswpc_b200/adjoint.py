@@ -106,12 +106,41 @@ class Misfit3D:
     def close(self):
         self.solver.close()
 
+    def _on_device(self, *ts) -> bool:
+        """Whether the model tensors are CUDA tensors on the problem's device
+        (the model then stays in HBM)."""
+        dev = torch.device(f"cuda:{self.device}" if isinstance(self.device, int) else self.device)
+        return all(isinstance(t, torch.Tensor) and t.is_cuda and t.device == dev for t in ts)
+
+    def _dev(self, a) -> torch.Tensor:
+        p = self.p
+        shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        dev = torch.device(f"cuda:{self.device}" if isinstance(self.device, int) else self.device)
+        return torch.as_tensor(a).detach().to(dev, torch.float32).reshape(shape).contiguous()
+
     def _set_model(self, vp, vs, rho):
         """The medium of per-cell vp, vs, rho: the moduli formed as
         vmodel_lhm forms them (m_vmodel_lhm.f90:158-160, FP32), then
         medium__setup in HBM (swpc_vmodel_upload, swpc_medium_setup_device;
-        bitwise the host setup of ``Medium.from_model``)."""
+        bitwise the host setup of ``Medium.from_model``).  CUDA tensors on the
+        problem's device stay there: swpc_vmodel_velocity_device forms the
+        moduli in HBM with the same expressions."""
         s, p = self.solver, self.p
+        if self._on_device(vp, vs, rho):
+            if not hasattr(self, "_q_dev"):
+                self._q_dev = (self._dev(self.qp), self._dev(self.qs))
+            vp, vs, rho = (self._dev(t) for t in (vp, vs, rho))
+            qp, qs = self._q_dev
+            torch.cuda.current_stream(vp.device).synchronize()   # the library works on its own stream
+            check(s.ctx, s.lib.swpc_vmodel_velocity_device(s.ctx, *(C.c_void_p(t.data_ptr()) for t in
+                                                                    (vp, vs, rho, qp, qs)), p.nz + 6, p.nx + 6))
+            m = _MediumMaps(p)
+            check(s.ctx, s.lib.swpc_medium_setup_device_opt(s.ctx, p.fq_min, p.fq_max, p.fq_ref, fptr(m.ts),
+                                                            fptr(m.scal),
+                                                            *(_lib.iptr(getattr(m, n)) for n in Medium.MAPS),
+                                                            p.nx + 6, int(p.stabilize_pml)))
+            s.medium = m
+            return m
         if p.stabilize_pml:
             m = Medium.from_model(p, vp, vs, rho, self.qp, self.qs)
             check(s.ctx, s.lib.swpc_upload_medium(s.ctx, C.byref(m.view(average_on_device=True))))
@@ -141,12 +170,22 @@ class Misfit3D:
 
     def gradient(self, vp, vs, rho):
         """(J, dJ/dvp, dJ/dvs, dJ/drho); the gradients are float64 arrays
-        over the memory box."""
+        over the memory box, or float64 CUDA tensors when the model is given
+        as CUDA tensors on the problem's device (then nothing crosses to the
+        host but the traces and the misfit)."""
         s, p = self.solver, self.p
+        on_dev = self._on_device(vp, vs, rho)
         self._set_model(vp, vs, rho)
         J = C.c_double()
         check(s.ctx, s.lib.swpc_gradient(s.ctx, fptr(self.obs), self.ckpt, C.byref(J)))
         shape = (p.ny + 6, p.nx + 6, p.nz + 6)
+        if on_dev:
+            m = [self._dev(t) for t in (vp, vs, rho)]
+            out = [torch.empty(shape, dtype=torch.float64, device=m[0].device) for _ in range(3)]
+            ptr = lambda t: C.c_void_p(t.data_ptr())
+            check(s.ctx, s.lib.swpc_gradient_model_device(s.ctx, ptr(m[0]), ptr(m[1]), ptr(m[2]), p.nz + 6,
+                                                          p.nx + 6, ptr(out[0]), ptr(out[1]), ptr(out[2])))
+            return J.value, out[0], out[1], out[2]
         f = lambda a: np.ascontiguousarray(a, np.float32).reshape(shape)
         out = [np.zeros(shape, np.float64) for _ in range(3)]
         dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
@@ -170,11 +209,12 @@ class WaveformMisfit(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor, problem: Misfit3D):
-        args = (_host(vp), _host(vs), _host(rho))
+        # CUDA tensors on the problem's device stay in HBM; others go through host memory
+        args = (vp, vs, rho) if problem._on_device(vp, vs, rho) else (_host(vp), _host(vs), _host(rho))
         if any(ctx.needs_input_grad[:3]):
             J, gvp, gvs, grho = problem.gradient(*args)
-            ctx.save_for_backward(*(torch.from_numpy(g).to(t.device) for g, t in ((gvp, vp), (gvs, vs),
-                                                                                  (grho, rho))))
+            as_t = lambda g, t: g.reshape(t.shape) if isinstance(g, torch.Tensor) else torch.from_numpy(g).to(t.device)
+            ctx.save_for_backward(*(as_t(g, t) for g, t in ((gvp, vp), (gvs, vs), (grho, rho))))
             ctx.dtypes = (vp.dtype, vs.dtype, rho.dtype)
         else:
             J = problem.misfit(*args)

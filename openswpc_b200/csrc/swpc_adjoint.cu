@@ -1400,9 +1400,48 @@ extern "C" int swpc_gradient_fetch(swpc_ctx *c, int which, double *out, int ld_k
     return fetch_double(c, c->adj->grad[which], out, ld_k, ld_i);
 }
 
+// device double array -> device memory box (leading extents ld_k, ld_i)
+__global__ void unpack_double_kernel(Geo g, const double *__restrict__ src, double *dst, int ld_k, int ld_i) {
+    const int nkb = g.nz + 6, nib = g.nx + 6;
+    const long long n = (long long)nkb * nib * (g.ny + 6);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int kb = (int)(t % nkb);
+        const long long col = t / nkb;
+        const int ib = (int)(col % nib), jb = (int)(col / nib);
+        dst[((long long)jb * ld_i + ib) * ld_k + kb] = src[cell_index(g, kb - 2, ib - 2, jb - 2)];
+    }
+}
+
+static bool is_device_array(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static int gradient_model(swpc_ctx *c, const float *vp, const float *vs, const float *rho, int ld_k, int ld_i,
+                          double *gvp, double *gvs, double *grho, bool on_device);
+
 extern "C" int swpc_gradient_model(swpc_ctx *c, const float *vp, const float *vs, const float *rho, int ld_k,
                                    int ld_i, double *gvp, double *gvs, double *grho) {
+    return gradient_model(c, vp, vs, rho, ld_k, ld_i, gvp, gvs, grho, false);
+}
+
+extern "C" int swpc_gradient_model_device(swpc_ctx *c, const float *vp, const float *vs, const float *rho, int ld_k,
+                                          int ld_i, double *gvp, double *gvs, double *grho) {
+    return gradient_model(c, vp, vs, rho, ld_k, ld_i, gvp, gvs, grho, true);
+}
+
+static int gradient_model(swpc_ctx *c, const float *vp, const float *vs, const float *rho, int ld_k, int ld_i,
+                          double *gvp, double *gvs, double *grho, bool on_device) {
     if (!c || !vp || !vs || !rho || !gvp || !gvs || !grho) return SWPC_ERR_ARG;
+    if (on_device)
+        for (const void *p : {(const void *)vp, (const void *)vs, (const void *)rho, (const void *)gvp,
+                              (const void *)gvs, (const void *)grho})
+            if (!is_device_array(p)) return err(c, SWPC_ERR_ARG, "swpc_gradient_model_device takes device arrays");
     if (!c->adj) return err(c, SWPC_ERR_STATE, "swpc_gradient not called");
     const Geo &g = c->g;
     if (ld_k < g.nz + 6 || ld_i < g.nx + 6) return err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
@@ -1414,7 +1453,8 @@ extern "C" int swpc_gradient_model(swpc_ctx *c, const float *vp, const float *vs
     for (int q = 0; q < 3 && !rc; q++) {
         rc = dalloc(c, &dm[q], g.ncell);
         if (!rc) rc = dalloc(c, &dg[q], g.ncell);
-        if (!rc) rc = copy_box(c, dm[q], hm[q], nullptr, ld_k, ld_i);
+        if (!rc) rc = on_device ? copy_box_from_device(c, dm[q], hm[q], ld_k, ld_i)
+                                : copy_box(c, dm[q], hm[q], nullptr, ld_k, ld_i);
     }
     if (!rc) {
         ModelGradArgs a;
@@ -1429,7 +1469,14 @@ extern "C" int swpc_gradient_model(swpc_ctx *c, const float *vp, const float *vs
         rc = cuda_check(c, cudaGetLastError(), "model_grad_kernel");
     }
     double *ho[3] = {gvp, gvs, grho};
-    for (int q = 0; q < 3 && !rc; q++) rc = fetch_double(c, dg[q], ho[q], ld_k, ld_i);
+    for (int q = 0; q < 3 && !rc; q++) {
+        if (on_device) {
+            unpack_double_kernel<<<148 * 8, 256, 0, c->stream>>>(g, dg[q], ho[q], ld_k, ld_i);
+            rc = cuda_check(c, cudaGetLastError(), "unpack_double_kernel");
+        } else {
+            rc = fetch_double(c, dg[q], ho[q], ld_k, ld_i);
+        }
+    }
     cudaStreamSynchronize(c->stream);
     for (int q = 0; q < 3; q++) {
         if (dm[q]) { cudaFree(dm[q]); c->bytes -= (long long)g.ncell * sizeof(float); }

@@ -400,6 +400,48 @@ extern "C" int swpc_vmodel_upload(swpc_ctx *c, const float *rho, const float *la
     return SWPC_OK;
 }
 
+// Moduli of per-cell velocities over the memory box, in the expression order
+// of vmodel_lhm (m_vmodel_lhm.f90:146-148): mu = rho vs vs, lam = rho (vp vp -
+// 2 vs vs).  On entry lam holds vp and mu holds vs.
+__global__ void moduli_kernel(Geo g, const float *__restrict__ rho, float *lam, float *mu) {
+    const int nkb = g.nz + 6, nib = g.nx + 6;
+    const long long n = (long long)nkb * nib * (g.ny + 6);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % nkb) - 2;
+        const long long col = t / nkb;
+        const int i = (int)(col % nib) - 2, j = (int)(col / nib) - 2;
+        const long long e = cell_index(g, k, i, j);
+        const float r = rho[e], vp = lam[e], vs = mu[e];
+        mu[e] = r * vs * vs;
+        lam[e] = r * (vp * vp - 2.0f * vs * vs);
+    }
+}
+
+extern "C" int swpc_vmodel_velocity_device(swpc_ctx *c, const float *vp, const float *vs, const float *rho,
+                                           const float *qp, const float *qs, int ld_k, int ld_i) {
+    if (!c) return SWPC_ERR_ARG;
+    if (c->kind != SWPC_KIND_3D) return set_err(c, SWPC_ERR_ARG, "the device medium setup is for the 3D code");
+    RC(check_na_wide(c));
+    if (!vp || !vs || !rho || !qp || !qs) return set_err(c, SWPC_ERR_ARG, "model array missing");
+    for (const float *p : {vp, vs, rho, qp, qs})
+        if (!device_pointer(p)) return set_err(c, SWPC_ERR_ARG, "swpc_vmodel_velocity_device takes device arrays");
+    if (ld_k < c->g.nz + 6 || ld_i < c->g.nx + 6) return set_err(c, SWPC_ERR_ARG, "leading extents smaller than the memory box");
+    CK(cudaSetDevice(c->device));
+    drop_graph(c);
+    c->medium_ready = false;
+    c->vmodel_ready = false;
+    RC(copy_box_from_device(c, c->med[8], rho, ld_k, ld_i));
+    RC(copy_box_from_device(c, c->med[1], vp, ld_k, ld_i));
+    RC(copy_box_from_device(c, c->med[2], vs, ld_k, ld_i));
+    RC(copy_box_from_device(c, c->med[3], qp, ld_k, ld_i));
+    RC(copy_box_from_device(c, c->med[4], qs, ld_k, ld_i));
+    moduli_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, c->med[8], c->med[1], c->med[2]);
+    CK(cudaGetLastError());
+    c->vmodel_ready = true;
+    return SWPC_OK;
+}
+
 extern "C" int swpc_medium_setup_device(swpc_ctx *c, float fq_min, float fq_max, float fq_ref, float *ts,
                                         float *scal, int *kfs, int *kob, int *kfs_top, int *kfs_bot, int *kob_top,
                                         int *kob_bot, int *kbeg_a, int ld_i2) {

@@ -414,6 +414,33 @@ def test_waveform_misfit_autograd():
     prob.close()
 
 
+@pytest.mark.parametrize("stabilize", [False, True])
+def test_waveform_misfit_from_cuda_tensors_stays_on_the_device(stabilize):
+    """A model given as CUDA tensors is set up and differentiated in HBM
+    (swpc_vmodel_velocity_device, swpc_gradient_model_device): the misfit and
+    the three gradients are bitwise those of the same model from host
+    arrays, and the gradients come back as CUDA tensors."""
+    import torch
+    from openswpc_b200.adjoint import Misfit3D, waveform_misfit
+    p, (vp, vs, rho, qp, qs), obs = model_case(nt=40)
+    p.stabilize_pml = stabilize
+    prob = Misfit3D(p, vp, vs, rho, qp, qs, obs, ckpt=8)
+    J_ref, gvp, gvs, grho = prob.gradient(vp, vs, rho)
+    tv = [torch.tensor(a, device="cuda:0", requires_grad=True) for a in (vp, vs, rho)]
+    J = waveform_misfit(*tv, prob)
+    J.backward()
+    assert J.is_cuda and float(J) == J_ref
+    for t, g in zip(tv, (gvp, gvs, grho)):
+        assert t.grad.is_cuda and t.grad.dtype == torch.float32
+        assert np.array_equal(t.grad.cpu().numpy(), g.astype(np.float32))
+    J_dev, *g_dev = prob.gradient(*[t.detach() for t in tv])
+    assert J_dev == J_ref
+    for a, b in zip(g_dev, (gvp, gvs, grho)):
+        assert a.is_cuda and a.dtype == torch.float64
+        assert np.array_equal(a.cpu().numpy().view(np.uint64), b.view(np.uint64))
+    prob.close()
+
+
 def _recorders(g, ig):
     """Everything the recorders of a run hold: velocity, displacement,
     stress and strain traces, green__store's Green's functions."""
