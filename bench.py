@@ -692,8 +692,12 @@ def bench_c3(args, world, rank, local):
     nrec = -(-(p.nt - kept) // ckpt)
     b_fwd = n_int * (B_STRESS_INT + B_VEL_INT) + n_pml * (B_STRESS_PML + B_VEL_PML)
     n_slot = (p.nx - 2 * p.na + 4) * (p.ny - 2 * p.na + 4) * (p.nz - p.na + 2)
+    # a kept step saves V of the shell (the slot box less the interior: written, and read back when the segment's
+    # V is rebuilt) and rebuilds the interior V from its divergences (12 B read, 12 B written)
+    n_shell = n_slot - n_int
     b_grad = ((2 * p.nt - kept) * b_fwd
-              + p.nt * (n_slot * B_SLOT + n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
+              + (p.nt - kept) * n_slot * B_SLOT + kept * (n_shell * B_SLOT + n_int * 24)
+              + p.nt * (n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
               - (p.nt - nseg) * (n_int + n_pml) * B_ADJ_FUSED_SAVES
               + nrec * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()
@@ -703,9 +707,9 @@ def bench_c3(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": grad, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + "
             "Gaussian vs blob)", "config": wl,
-            "what": "one step = one gradient evaluation (forward with checkpoints, keeping the forward slots of "
-                    "the trailing segments that fit in free HBM, per-segment recompute of the others, adjoint); "
-                    "value counts cells x nt per gradient",
+            "what": "one step = one gradient evaluation (forward, keeping the stress divergences and the shell V of "
+                    "every step of the trailing segments that fit in free HBM, checkpoints and per-segment "
+                    "recompute of the others, adjoint); value counts cells x nt per gradient",
             "misfit": J.value,
             "forward_ms": fwd, "forward_gcells": cells * p.nt / (fwd / 1e3) / 1e9,
             "gradient_over_forward": grad / fwd,

@@ -387,20 +387,26 @@ int swpc_vmax_noalloc(const float *vx, const float *vy, const float *vz, const i
  * then per segment recomputes the forward from the checkpoint and steps the
  * adjoint back through it, summing each segment's imaging terms in FP32 and
  * folding them into FP64 totals.  Device memory: one checkpoint of the state
- * per recomputed segment plus the slots (V and the three stress divergences
- * after a step) of max(ckpt + 1, kept steps + 1) steps.  Every
+ * per recomputed segment, ckpt + 1 working slots (V and the three stress
+ * divergences after a step) and the kept steps below.  Every
  * recorder (traces, green__store, snapshots) records the forward run once:
  * the recompute advances the wavefield without them, so what they hold after
  * the call equals a plain run of steps 1..nt from rest.
- * swpc_gradient_set_slot_memory: bytes of HBM that the slots of trailing
- * segments may take (default 0).  The first forward pass then keeps the slot
- * of every step of as many trailing segments as the bytes hold, and only the
- * segments before them are checkpointed and recomputed; the gradient, the
- * misfit and the recorders are bitwise those of the default.  The setting
- * holds for the later swpc_gradient calls of the context.
- * swpc_gradient_memory: bytes of one checkpoint and of one slot, for sizing
- * that budget (free memory from cudaMemGetInfo, say, less what the
- * checkpoints take).
+ * swpc_gradient_set_slot_memory: bytes of HBM that the kept steps of
+ * trailing segments may take (default 0).  The first forward pass then keeps,
+ * for as many trailing segments as the bytes hold, V of each segment's first
+ * state and per step the stress divergences and V on the shell around the
+ * kernel region (V of the whole slot box where body forces or green__source
+ * write V); those segments are neither checkpointed nor recomputed, their
+ * interior V is rebuilt from the divergences with the velocity update's own
+ * expression, and only the segments before them are recomputed.  The
+ * gradient, the misfit and the recorders are bitwise those of the default.
+ * The setting holds for the later swpc_gradient calls of the context.
+ * swpc_gradient_memory: bytes of one checkpoint and of one kept step;
+ * swpc_gradient_segment_bytes: bytes of a kept segment's first V and of the
+ * working slots of a given ckpt; for sizing that budget (free memory from
+ * cudaMemGetInfo, say, less the working slots and the checkpoints of the
+ * recomputed segments).
  * swpc_gradient_fetch: which = 0 lam, 1 mu, 2 muyz, 3 muxz, 4 muxy, 5 bx,
  * 6 by, 7 bz; out = double array over the memory box. */
 int swpc_adj_reset(swpc_ctx *ctx);
@@ -417,6 +423,7 @@ int swpc_adj_download(swpc_ctx *ctx, int field, float *out, int ld_k, int ld_i);
 int swpc_gradient(swpc_ctx *ctx, const float *obs, int ckpt, double *misfit);
 int swpc_gradient_set_slot_memory(swpc_ctx *ctx, long long bytes);
 int swpc_gradient_memory(swpc_ctx *ctx, long long *ckpt_bytes, long long *slot_bytes);
+int swpc_gradient_segment_bytes(swpc_ctx *ctx, long long *seg_bytes, long long *work_bytes, int ckpt);
 int swpc_gradient_fetch(swpc_ctx *ctx, int which, double *out, int ld_k, int ld_i);
 /* The gradient of the last swpc_gradient with respect to per-cell vp, vs and
  * rho with Q held fixed: the chain rule through vmodel_lhm's moduli

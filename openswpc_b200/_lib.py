@@ -45,7 +45,8 @@ EXPORTS = [
     "swpc_vmax", "swpc_vmax_noalloc", "swpc_step", "swpc_run", "swpc_time_steps", "swpc_wav_fetch", "swpc_wav_dims",
     "swpc_snap_setup", "swpc_snap_write", "swpc_snap_dims", "swpc_snap_fetch", "swpc_snap_fetch_max",
     "swpc_adj_reset", "swpc_adj_step_linear", "swpc_adj_upload", "swpc_adj_download", "swpc_gradient",
-    "swpc_gradient_set_slot_memory", "swpc_gradient_memory", "swpc_gradient_model_device",
+    "swpc_gradient_set_slot_memory", "swpc_gradient_memory", "swpc_gradient_segment_bytes",
+    "swpc_gradient_model_device",
     "swpc_vmodel_velocity_device",
     "swpc_gradient_fetch", "swpc_gradient_model", "swpc_reset_state",
     "swpc_download_field", "swpc_upload_field", "swpc_rescale", "swpc_device_bytes", "swpc_set_launch",
@@ -183,6 +184,7 @@ def load():
         "swpc_gradient": (i, [vp, _FP, i, C.POINTER(C.c_double)]),
         "swpc_gradient_set_slot_memory": (i, [vp, C.c_longlong]),
         "swpc_gradient_memory": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+        "swpc_gradient_segment_bytes": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), i]),
         "swpc_gradient_fetch": (i, [vp, i, C.POINTER(C.c_double), i, i]),
         "swpc_gradient_model": (i, [vp, _FP, _FP, _FP, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),

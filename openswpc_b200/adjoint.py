@@ -55,49 +55,58 @@ class Misfit3D:
             raise ValueError(f"observed traces must have shape {(self.solver.nst, 3, self.ntw)}")
         self.set_slot_memory(slot_memory)
 
-    def memory(self) -> tuple[int, int]:
-        """Bytes of one checkpoint and of one slot of the gradient."""
-        ck, sl = C.c_longlong(), C.c_longlong()
-        check(self.solver.ctx, self.solver.lib.swpc_gradient_memory(self.solver.ctx, C.byref(ck), C.byref(sl)))
-        return ck.value, sl.value
+    def memory(self) -> tuple[int, int, int, int]:
+        """Bytes of one checkpoint, of one kept step, of a kept segment's
+        first V and of the working slots of this problem's ckpt."""
+        s = self.solver
+        ck, st, sg, wk = (C.c_longlong() for _ in range(4))
+        check(s.ctx, s.lib.swpc_gradient_memory(s.ctx, C.byref(ck), C.byref(st)))
+        check(s.ctx, s.lib.swpc_gradient_segment_bytes(s.ctx, C.byref(sg), C.byref(wk), self.ckpt))
+        return ck.value, st.value, sg.value, wk.value
+
+    def _tail(self, budget: int) -> tuple[int, int]:
+        """Trailing segments and their steps that `budget` bytes keep (the
+        rule of swpc_gradient)."""
+        _, st, sg, _ = self.memory()
+        nt, k = self.p.nt, self.ckpt
+        nseg, t, n = -(-nt // k), 0, 0
+        while t < nseg:
+            ln = min(k, nt - (nseg - 1 - t) * k)
+            if (n + ln) * st + (t + 1) * sg > budget:
+                break
+            n, t = n + ln, t + 1
+        return t, n
 
     def set_slot_memory(self, nbytes: int | str, reserve: int = 4 << 30) -> int:
-        """HBM that the slots of trailing segments may take
-        (``swpc_gradient_set_slot_memory``): those segments keep their
-        forward slots from the first pass instead of being recomputed, with
-        bitwise the same gradient.  ``"auto"`` keeps the most trailing
-        segments whose slots, with the checkpoints of the segments before
-        them, fit in the device's free memory less ``reserve`` bytes (call it
-        before the first gradient, whose buffers it would count as used).
-        Returns the bytes set."""
+        """HBM that the kept steps of trailing segments may take
+        (``swpc_gradient_set_slot_memory``): those segments keep what their
+        adjoint needs from the first forward pass instead of being
+        recomputed, with bitwise the same gradient.  ``"auto"`` keeps the most
+        trailing segments that fit, with the working slots and the
+        checkpoints of the segments before them, in the device's free memory
+        less ``reserve`` bytes (call it before the first gradient, whose
+        buffers it would count as used).  Returns the bytes set."""
         s = self.solver
         if nbytes == "auto":
             free, _ = torch.cuda.mem_get_info(self.device)
-            ck, sl = self.memory()
+            ck, st, sg, wk = self.memory()
             nt, k = self.p.nt, self.ckpt
             nseg = -(-nt // k)
             nbytes, steps = 0, 0
             for t in range(1, nseg + 1):
                 steps += min(k, nt - (nseg - t) * k)
-                if (max(steps, k) + 1) * sl + max(nseg - t, 1) * ck > free - reserve:
+                keep = steps * st + t * sg
+                if keep + max(nseg - t, 1) * ck + wk > free - reserve:
                     break
-                nbytes = (steps + 1) * sl
+                nbytes = keep
         check(s.ctx, s.lib.swpc_gradient_set_slot_memory(s.ctx, int(nbytes)))
         self.slot_memory = int(nbytes)
         return self.slot_memory
 
     def kept_steps(self) -> int:
-        """Steps of the trailing segments whose slots the gradient keeps from
-        its forward pass (the rule of swpc_gradient)."""
-        _, sl = self.memory()
-        cap, nt, ck = self.slot_memory // sl, self.p.nt, self.ckpt
-        nseg, n = -(-nt // ck), 0
-        for g in range(nseg - 1, -1, -1):
-            ln = min(ck, nt - g * ck)
-            if n + ln + 1 > cap:
-                break
-            n += ln
-        return n
+        """Steps of the trailing segments that the gradient keeps from its
+        forward pass."""
+        return self._tail(self.slot_memory)[1]
 
     @property
     def ntw(self) -> int:

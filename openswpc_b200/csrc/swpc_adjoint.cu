@@ -66,8 +66,12 @@ struct swpc_adj_state {
     float *slots = nullptr;              // V and the stress divergences after each step of a segment, or of
                                          // the trailing segments kept from the first forward pass
     size_t ck_floats = 0, slot_cap = 0;  // floats per checkpoint; slots allocated
-    long long slot_budget = 0;           // bytes the slots of trailing segments may take (0: recompute all)
-    int ntail = 0;                       // trailing segments whose slots the forward pass keeps
+    long long slot_budget = 0;           // bytes the kept steps of trailing segments may take (0: recompute all)
+    int ntail = 0;                       // trailing segments whose steps the forward pass keeps
+    float *keep = nullptr;               // kept segments: V of each segment's first state, then per kept step the
+    size_t keep_floats = 0;              //   divergences and V on the slot box's shell (or the whole box)
+    int *shell = nullptr;                // slot-box indices of the shell cells (slot box less the interior)
+    int nshell = 0;
     long long bytes = 0;
 };
 
@@ -680,6 +684,74 @@ __global__ void slot_v_kernel(Geo g, SlotGeo sg, const float *vx, const float *v
     }
 }
 
+// V of the shell cells of the slot box (slot-box indices `shell`) into a kept
+// step: dst[c * n + q] = V_c at shell cell q
+__global__ void shell_save_kernel(Geo g, SlotGeo sg, const float *vx, const float *vy, const float *vz,
+                                  const int *shell, int n, float *dst) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3LL * n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / n), q = (int)(t - (long long)c * n);
+        const long long es = shell[q];
+        const int kd = (int)(es % sg.Kp);
+        const long long cs = es / sg.Kp;
+        const int is = (int)(cs % sg.Ip), js = (int)(cs / sg.Ip);
+        const float *src = c == 0 ? vx : c == 1 ? vy : vz;
+        dst[t] = src[col_index(g, is + sg.i0, js + sg.j0) * g.Kp + kd];
+    }
+}
+
+// the shell values of kept steps 1..len into the V of slots 1..len (slot
+// stride sstride floats, kept-step stride kstride floats)
+__global__ void shell_load_kernel(const float *keep1, size_t kstride, const int *shell, int n, int len, long long ns,
+                                  float *slot1, size_t sstride) {
+    const long long per = 3LL * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per * len;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(t / per);
+        const long long r = t - m * per;
+        const int c = (int)(r / n), q = (int)(r - (long long)c * n);
+        slot1[m * sstride + c * ns + shell[q]] = keep1[m * kstride + r];
+    }
+}
+
+// V of the interior cells through a kept segment: the velocity update of an
+// interior cell is V + b * d * dt with d its stress divergence
+// (kernel__update_vel, m_kernel.f90:103-125, the expression of vel_interior),
+// so from V of slot 0 and the kept divergences d(1..len) the V of slots
+// 1..len follow with the update's own rounding
+struct ReconArgs {
+    Geo g;
+    SlotGeo sg;
+    int ibk, iek, jbk, jek, kek, len;
+    const float *b[3];
+    float dt;
+    const float *div1;      // divergences of kept step 1 (field c at div1 + c * sg.n)
+    size_t kstride;         // floats between kept steps
+    float *slot0;           // V of slot 0 (field c at slot0 + c * sg.n), slots every sstride floats
+    size_t sstride;
+};
+__global__ void recon_kernel(const ReconArgs a) {
+    const int ni = a.iek - a.ibk + 1, nj = a.jek - a.jbk + 1;
+    const long long n = (long long)a.kek * ni * nj;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = 1 + (int)(t % a.kek);
+        const long long r = t / a.kek;
+        const int i = a.ibk + (int)(r % ni), j = a.jbk + (int)(r / ni);
+        const long long es = slot_index(a.sg, k, i, j), e = cell_index(a.g, k, i, j);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float b = a.b[c][e], dt = a.dt;
+            float v = a.slot0[c * a.sg.n + es];
+            for (int m = 1; m <= a.len; m++) {
+                const float d = __ldcs(a.div1 + (m - 1) * a.kstride + c * a.sg.n + es);
+                v = v + b * d * dt;
+                __stcs(a.slot0 + m * a.sstride + c * a.sg.n + es, v);
+            }
+        }
+    }
+}
+
 // the segment's FP32 partial sums into the FP64 totals; the partials restart from zero
 struct FoldArgs {
     double *total[8];
@@ -833,6 +905,8 @@ void adj_free(swpc_ctx *c) {
     if (s->res) cudaFree(s->res);
     if (s->ckpool) cudaFree(s->ckpool);
     if (s->slots) cudaFree(s->slots);
+    if (s->keep) cudaFree(s->keep);
+    if (s->shell) cudaFree(s->shell);
     delete s;
     c->adj = nullptr;
 }
@@ -1235,6 +1309,37 @@ extern "C" int swpc_gradient_set_slot_memory(swpc_ctx *c, long long bytes) {
     return SWPC_OK;
 }
 
+// Whether a kept step may hold V on the shell of the slot box only: with no
+// injection into V (body forces, green__source) the interior V of every step
+// follows from the kept divergences (recon_kernel).
+static bool keeps_shell(const swpc_ctx *c) { return c->ninj_bf == 0 && !c->green; }
+
+// cells of the shell: slot-box cells with k = -1 .. kek + 2 outside the interior
+static std::vector<int> shell_cells(const swpc_ctx *c, const SlotGeo &sg) {
+    std::vector<int> out;
+    for (int js = 0; js < sg.Jp; js++)
+        for (int is = 0; is < sg.Ip; is++) {
+            const int i = is + sg.i0, j = js + sg.j0;
+            const bool col_in = i >= c->ibk && i <= c->iek && j >= c->jbk && j <= c->jek;
+            for (int k = -1; k <= c->kek + 2; k++)
+                if (!(col_in && k >= 1 && k <= c->kek)) out.push_back((int)slot_index(sg, k, i, j));
+        }
+    return out;
+}
+
+// floats of one kept step (divergences, then V of the shell or the slot box) and of a kept segment's first V
+static void keep_sizes(const swpc_ctx *c, size_t *step, size_t *seg, int *nshell) {
+    const SlotGeo sg = slot_geo(c);
+    int ns = 0;
+    if (keeps_shell(c)) {
+        const int ni = c->iek - c->ibk + 1, nj = c->jek - c->jbk + 1;
+        ns = (int)((long long)sg.Ip * sg.Jp * (c->kek + 4) - (long long)ni * nj * c->kek);
+    }
+    *step = 3 * (size_t)sg.n + (keeps_shell(c) ? 3 * (size_t)ns : 3 * (size_t)sg.n);
+    *seg = 3 * (size_t)sg.n;
+    if (nshell) *nshell = ns;
+}
+
 extern "C" int swpc_gradient_memory(swpc_ctx *c, long long *ckpt_bytes, long long *slot_bytes) {
     if (!c || !ckpt_bytes || !slot_bytes) return SWPC_ERR_ARG;
     if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "the adjoint is implemented for the 3D solver");
@@ -1242,24 +1347,59 @@ extern "C" int swpc_gradient_memory(swpc_ctx *c, long long *ckpt_bytes, long lon
     state_arrays(c, &sz);
     long long ckf = 0;
     for (size_t v : sz) ckf += (long long)v;
+    size_t step, seg;
+    keep_sizes(c, &step, &seg, nullptr);
     *ckpt_bytes = ckf * (long long)sizeof(float);
-    *slot_bytes = (long long)kSlotFields * slot_geo(c).n * (long long)sizeof(float);
+    *slot_bytes = (long long)(step * sizeof(float));
     return SWPC_OK;
 }
 
-// Trailing segments of a gradient whose slots (one per step plus the state
-// before the first) fit in `cap` slots; their steps in *steps.
-static int tail_segments(int nt, int ckpt, int nseg, long long cap, long long *steps) {
+extern "C" int swpc_gradient_segment_bytes(swpc_ctx *c, long long *seg_bytes, long long *work_bytes, int ckpt) {
+    if (!c || !seg_bytes || !work_bytes || ckpt < 1) return SWPC_ERR_ARG;
+    if (c->kind != SWPC_KIND_3D) return err(c, SWPC_ERR_ARG, "the adjoint is implemented for the 3D solver");
+    size_t step, seg;
+    keep_sizes(c, &step, &seg, nullptr);
+    *seg_bytes = (long long)(seg * sizeof(float));
+    *work_bytes = (long long)((size_t)kSlotFields * slot_geo(c).n * (ckpt + 1) * sizeof(float));
+    return SWPC_OK;
+}
+
+// Trailing segments whose kept steps (step floats each) and first V (seg floats each) fit in `budget` floats;
+// their steps in *steps.
+static int tail_segments(int nt, int ckpt, int nseg, long long budget, size_t step, size_t seg, long long *steps) {
     int ntail = 0;
     long long n = 0;
     while (ntail < nseg) {
         const int it0 = (nseg - 1 - ntail) * ckpt + 1, len = std::min(ckpt, nt - it0 + 1);
-        if (n + len + 1 > cap) break;
+        if ((long long)((n + len) * step + (ntail + 1) * seg) > budget) break;
         n += len;
         ntail++;
     }
     *steps = n;
     return ntail;
+}
+
+// Kept step it of the trailing segments: the three divergences after step it
+// in the slot layout, then V of the shell (or of the slot box).
+static int save_kept(swpc_ctx *c, float *dst) {
+    swpc_adj_state *s = c->adj;
+    const SlotGeo sg = slot_geo(c);
+    SlotDivArgs a;
+    a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
+    for (int q = 0; q < 6; q++) a.S[q] = c->S[q];
+    a.band = c->band;
+    memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41));
+    for (int q = 0; q < 3; q++) a.divS[q] = dst + q * sg.n;
+    a.sg = sg;
+    const dim3 block(kThreadsK, 2, 2);
+    slot_div_kernel<<<cell_grid(c->g, block), block, 0, c->stream>>>(a);
+    ACK(cudaGetLastError());
+    if (keeps_shell(c))
+        shell_save_kernel<<<148 * 4, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], s->shell, s->nshell,
+                                                          dst + 3 * sg.n);
+    else
+        slot_v_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], dst + 3 * sg.n);
+    return cuda_check(c, cudaGetLastError(), "save_kept");
 }
 
 extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *misfit) {
@@ -1276,37 +1416,57 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     for (size_t v : sz) ckf += v;
     const SlotGeo sg = slot_geo(c);
     const size_t n = (size_t)sg.n, slot_floats = (size_t)kSlotFields * n;
-    // the trailing segments whose slots fit the budget keep them from the first forward pass and are not
-    // recomputed (nor checkpointed); the earlier segments recompute into the same slots once those are spent
+    // the trailing segments whose steps fit the budget keep them from the first forward pass (the divergences
+    // and V of the shell every step, V of the first state): they are neither checkpointed nor recomputed, and
+    // their V is rebuilt into the working slots; the earlier segments are recomputed into the working slots
+    size_t kstep, kseg;
+    int nshell = 0;
+    keep_sizes(c, &kstep, &kseg, &nshell);
     long long tail_steps = 0;
-    const int ntail = tail_segments(nt, ckpt, nseg, s->slot_budget / (long long)(slot_floats * sizeof(float)),
+    const int ntail = tail_segments(nt, ckpt, nseg, s->slot_budget / (long long)sizeof(float), kstep, kseg,
                                     &tail_steps);
     const int gT = nseg - ntail, itT0 = gT * ckpt + 1;
-    const size_t cap = std::max((size_t)ckpt + 1, (size_t)tail_steps + 1);
-    const size_t need_ck = ckf * std::max(gT, 1), need_slots = slot_floats * cap;
-    if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf || s->slot_cap != cap || s->ntail != ntail) {
+    const size_t cap = (size_t)ckpt + 1;
+    const size_t need_ck = ckf * std::max(gT, 1), need_keep = (size_t)tail_steps * kstep + (size_t)ntail * kseg;
+    if (s->ckpt != ckpt || s->nseg != nseg || s->ck_floats != ckf || s->slot_cap != cap || s->ntail != ntail ||
+        s->keep_floats != need_keep) {
         if (s->ckpool) cudaFree(s->ckpool);
         if (s->slots) cudaFree(s->slots);
-        s->ckpool = s->slots = nullptr;
+        if (s->keep) cudaFree(s->keep);
+        s->ckpool = s->slots = s->keep = nullptr;
         s->ckpt = s->nseg = s->ntail = 0;
-        s->ck_floats = s->slot_cap = 0;
+        s->ck_floats = s->slot_cap = s->keep_floats = 0;
         if (cudaMalloc((void **)&s->ckpool, need_ck * sizeof(float)) != cudaSuccess ||
-            cudaMalloc((void **)&s->slots, need_slots * sizeof(float)) != cudaSuccess) {
+            cudaMalloc((void **)&s->slots, slot_floats * cap * sizeof(float)) != cudaSuccess ||
+            (need_keep && cudaMalloc((void **)&s->keep, need_keep * sizeof(float)) != cudaSuccess)) {
             cudaGetLastError();
             return err(c, SWPC_ERR_NOMEM, "no room for the checkpoints and slots (raise ckpt, lower the slot "
                                           "memory or shrink the grid)");
         }
         s->ckpt = ckpt; s->nseg = nseg; s->ck_floats = ckf; s->slot_cap = cap; s->ntail = ntail;
+        s->keep_floats = need_keep;
         // the staged stress-phase weights read the forward V of a slot with its halo
         Geo gs = c->g;
         gs.Kp = sg.Kp; gs.Ip = sg.Ip; gs.Jp = sg.Jp; gs.ncell = sg.n;
         if (!tma_encode_box(s->maps->vh, s->slots, gs, (long long)kSlotFields * cap, tma::KB, adjt::BI + 4, adjt::BJ + 4, 3))
             return err(c, SWPC_ERR_CUDA, "cuTensorMapEncodeTiled failed for the recompute slots");
     }
+    if (ntail > 0 && keeps_shell(c) && s->nshell != nshell) {
+        const std::vector<int> sh = shell_cells(c, sg);
+        if (s->shell) cudaFree(s->shell);
+        s->shell = nullptr;
+        s->nshell = 0;
+        ACK(cudaMalloc((void **)&s->shell, sh.size() * sizeof(int)));
+        ACK(cudaMemcpy(s->shell, sh.data(), sh.size() * sizeof(int), cudaMemcpyHostToDevice));
+        s->nshell = (int)sh.size();
+    }
+    // kept segment g >= gT: its first V at keep + (g - gT) * kseg, its steps after all first Vs
+    auto kept_first = [&](int g) { return s->keep + (size_t)(g - gT) * kseg; };
+    auto kept_step = [&](int it) { return s->keep + (size_t)ntail * kseg + (size_t)(it - itT0) * kstep; };
     const size_t nres = (size_t)c->nst * 3 * c->ntw;
     if (!s->res) ACK(cudaMalloc((void **)&s->res, nres * sizeof(float)));
-    // 1. forward from rest with a checkpoint before every recomputed segment; the trailing segments keep the
-    //    slot of every step instead (the recorders run in both)
+    // 1. forward from rest with a checkpoint before every recomputed segment; the trailing segments keep their
+    //    steps instead (the recorders run in both)
     rc = zero_state(c);
     if (rc) return rc;
     for (int g = 0; g < nseg && !rc; g++) {
@@ -1316,10 +1476,11 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
             if (!rc) rc = swpc_run(c, it0, len);
             continue;
         }
-        if (g == gT) rc = save_slot(c, 0);
+        slot_v_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], kept_first(g));
+        rc = cuda_check(c, cudaGetLastError(), "slot_v_kernel");
         for (int it = it0; it < it0 + len && !rc; it++) {
             rc = swpc_run(c, it, 1);
-            if (!rc) rc = save_slot(c, it - itT0 + 1);
+            if (!rc) rc = save_kept(c, kept_step(it));
         }
     }
     if (rc) return rc;
@@ -1339,11 +1500,31 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
     if (!rc) rc = zero_adjoint(c);
     if (rc) return rc;
     for (int g = nseg - 1; g >= 0; g--) {
-        const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt);
-        // slot of the state before step it0: kept from the forward pass, or recomputed from the checkpoint
-        size_t base = 0;
-        if (g >= gT) {
-            base = (size_t)(it0 - itT0);
+        const int it0 = g * ckpt + 1, it1 = std::min(it0 + ckpt - 1, nt), len = it1 - it0 + 1;
+        // the forward V of the segment in the working slots 0..len, and where the divergences of each step are
+        const bool kept = g >= gT;
+        if (kept) {
+            ACK(cudaMemcpyAsync(s->slots, kept_first(g), 3 * n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+            if (keeps_shell(c)) {
+                ReconArgs ra;
+                ra.g = c->g; ra.sg = sg; ra.ibk = c->ibk; ra.iek = c->iek; ra.jbk = c->jbk; ra.jek = c->jek;
+                ra.kek = c->kek; ra.len = len;
+                for (int q = 0; q < 3; q++) ra.b[q] = c->med[5 + q];
+                ra.dt = c->d.dt;
+                ra.div1 = kept_step(it0);
+                ra.kstride = kstep;
+                ra.slot0 = s->slots;
+                ra.sstride = slot_floats;
+                recon_kernel<<<148 * 8, 256, 0, c->stream>>>(ra);
+                ACK(cudaGetLastError());
+                shell_load_kernel<<<148 * 4, 256, 0, c->stream>>>(kept_step(it0) + 3 * n, kstep, s->shell, s->nshell,
+                                                                  len, sg.n, s->slots + slot_floats, slot_floats);
+                ACK(cudaGetLastError());
+            } else {
+                for (int m = 1; m <= len; m++)
+                    ACK(cudaMemcpyAsync(s->slots + m * slot_floats, kept_step(it0 + m - 1) + 3 * n,
+                                        3 * n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+            }
         } else {
             rc = copy_state(c, s->ckpool + (size_t)g * ckf, false);
             if (!rc) rc = save_slot(c, 0);
@@ -1353,17 +1534,20 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
                 if (!rc) rc = save_slot(c, it - it0 + 1);
             }
         }
+        // divergences after step it: the kept step, or the working slot
+        auto divs = [&](int it, const float **D) {
+            const float *base = kept ? kept_step(it) : s->slots + (size_t)(it - it0 + 1) * slot_floats + 3 * n;
+            for (int q = 0; q < 3; q++) D[q] = base + q * n;
+        };
         // within a segment each stress-phase gather also forms the velocity-phase weights of the step before
         // (kernel 9 of swpc_set_launch); the first step of a segment forms its own
         bool vel_done = false;
         for (int it = it1; it >= it0 && !rc; it--) {
-            const size_t sa = base + (size_t)(it - it0 + 1), sb = base + (size_t)(it - it0);
-            const float *base_a = s->slots + sa * slot_floats;
-            const float *base_b = s->slots + sb * slot_floats;
-            const float *Da[3], *Vb[3], *Dn[3];
-            for (int q = 0; q < 3; q++) Da[q] = base_a + (3 + q) * n;
-            for (int q = 0; q < 3; q++) Vb[q] = base_b + q * n;
-            for (int q = 0; q < 3; q++) Dn[q] = base_b + (3 + q) * n;   // divergences of step it - 1
+            const size_t sb = (size_t)(it - it0);
+            const float *Da[3], *Vb[3], *Dn[3] = {nullptr, nullptr, nullptr};
+            divs(it, Da);
+            for (int q = 0; q < 3; q++) Vb[q] = s->slots + sb * slot_floats + q * n;
+            if (it > it0) divs(it - 1, Dn);   // divergences of step it - 1
             AdjNext nx;
             nx.on = c->adj_fuse && it > it0;
             nx.skip_src = source_at(c, it);

@@ -172,32 +172,48 @@ def _gradient_bits(g, p, obsf, ckpt):
     return J.value, grads, adj, g.waveforms(_lib.WAV_V)
 
 
-def test_gradient_with_kept_slots_gives_the_bits_of_the_full_recompute():
-    """Slots of trailing segments kept from the first forward pass
+@pytest.mark.parametrize("body_force", [False, True])
+def test_gradient_with_kept_slots_gives_the_bits_of_the_full_recompute(body_force):
+    """Steps of trailing segments kept from the first forward pass
     (swpc_gradient_set_slot_memory) replace their recompute: with room for
-    none, for the short last segment, for the last three segments and for
-    every segment, the misfit, the eight gradients, the final adjoint state
-    and the traces are bit for bit those of the default, on one context and
-    across budget changes."""
-    p, xi, obs = misfit_case()   # nt = 70, ckpt 16: segments of 16, 16, 16, 16 and 6 steps
-    obsf = np.ascontiguousarray(obs, np.float32)
+    none, for the short last segment, for three segments and for every
+    segment, the misfit, the eight gradients, the final adjoint state and the
+    traces are bit for bit those of the default, on one context and across
+    budget changes.  Without body forces a kept step holds V on the shell of
+    the kernel region only and the interior V is rebuilt from the kept
+    divergences; with body forces (which write V) it holds the whole V."""
+    if body_force:
+        from openswpc_b200.params import Source
+        srcs = [Source(0.2, -0.4, 5.0, 0.0, 1.0, fx=1.0, fy=0.5, fz=-2.0),
+                Source(-2.0, 1.5, 3.0, 0.1, 0.8, fx=0.0, fy=1.0, fz=0.0)]
+        p = small3d(nx=40, ny=36, nz=32, na=8, nt=70, bf_mode=True, sources=srcs)
+        xi = vonkarman_xi((p.ny + 6, p.nx + 6, p.nz + 6))
+        rng = np.random.default_rng(5)
+        obs = None
+    else:
+        p, xi, obs = misfit_case()   # nt = 70, ckpt 16: segments of 16, 16, 16, 16 and 6 steps
     ref = Swpc3D(p, xi)
+    if obs is None:
+        obs = (rng.standard_normal((ref.nst, 3, p.nt)) * 1e-3).astype(np.float32)
+    obsf = np.ascontiguousarray(obs, np.float32)
     J0, g0, a0, w0 = _gradient_bits(ref, p, obsf, 16)
     ref.close()
     assert any(np.abs(x).max() > 0 for x in g0)
     g = Swpc3D(p, xi)
-    ck, sl = C.c_longlong(), C.c_longlong()
-    check(g.ctx, g.lib.swpc_gradient_memory(g.ctx, C.byref(ck), C.byref(sl)))
-    assert ck.value > 0 and sl.value > 0
-    for slots in (7, 40, 71, 1 << 20, 0):   # kept steps: 6, 38, 70, 70, none
-        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, slots * sl.value))
+    ck, st, sg, wk = (C.c_longlong() for _ in range(4))
+    check(g.ctx, g.lib.swpc_gradient_memory(g.ctx, C.byref(ck), C.byref(st)))
+    check(g.ctx, g.lib.swpc_gradient_segment_bytes(g.ctx, C.byref(sg), C.byref(wk), 16))
+    assert ck.value > 0 and st.value > 0 and sg.value > 0 and wk.value > 0
+    budgets = [6 * st.value + sg.value, 38 * st.value + 3 * sg.value, 70 * st.value + 5 * sg.value, 1 << 40, 0]
+    for budget in budgets:   # kept steps: 6, 38, 70, 70, none
+        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, budget))
         J1, g1, a1, w1 = _gradient_bits(g, p, obsf, 16)
-        assert J1 == J0, slots
+        assert J1 == J0, budget
         for w, (x, y) in enumerate(zip(g1, g0)):
-            assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), (slots, w)
+            assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), (budget, w)
         for (fid, _), x, y in zip(fields(p), a1, a0):
-            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (slots, fid)
-        assert np.array_equal(w1.view(np.uint32), w0.view(np.uint32)), slots
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (budget, fid)
+        assert np.array_equal(w1.view(np.uint32), w0.view(np.uint32)), budget
     assert g.lib.swpc_gradient_set_slot_memory(g.ctx, -1) == _lib.SWPC_ERR_ARG
     g.close()
 
@@ -224,7 +240,7 @@ def test_velocity_weights_formed_in_the_stress_gather_give_the_same_bits(ntdec_w
         check(g.ctx, g.lib.swpc_set_launch(g.ctx, 9, 1, fuse, 1))
         ck, sl = C.c_longlong(), C.c_longlong()
         check(g.ctx, g.lib.swpc_gradient_memory(g.ctx, C.byref(ck), C.byref(sl)))
-        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, slots * sl.value))
+        check(g.ctx, g.lib.swpc_gradient_set_slot_memory(g.ctx, slots * sl.value))   # some trailing segments
         rng = np.random.default_rng(3)
         obs = (rng.standard_normal((g.nst, 3, (p.nt - 1) // ntdec_w + 1)) * 1e-3).astype(np.float32)
         runs.append(_gradient_bits(g, p, obs, 10))
