@@ -697,7 +697,9 @@ def bench_c3(args, world, rank, local):
     n_shell = n_slot - n_int
     b_grad = ((2 * p.nt - kept) * b_fwd
               + (p.nt - kept) * n_slot * B_SLOT + kept * (n_shell * B_SLOT + n_int * 24)
-              + p.nt * (n_int * (B_SLOT_INT + B_ADJ_INT) + n_pml * B_ADJ_PML)
+              # kept steps: the velocity update itself stores the divergences (12 B); recomputed: slot_div_kernel
+              + ((p.nt - kept) * B_SLOT_INT + kept * 12) * n_int
+              + p.nt * (n_int * B_ADJ_INT + n_pml * B_ADJ_PML)
               - (p.nt - nseg) * (n_int + n_pml) * B_ADJ_FUSED_SAVES
               + nrec * (n_int + n_pml) * B_CKPT)
     peak, peak_kind = hbm_peak()

@@ -121,6 +121,14 @@ __device__ __forceinline__ void vel_interior(const Vel3Args &a, const Ops &o, in
     sts(&Vx[e], vx + bx * d3Sx3 * dt);
     sts(&Vy[e], vy + by * d3Sy3 * dt);
     sts(&Vz[e], vz + bz * d3Sz3 * dt);
+    if (a.divo) {
+        const long long col = e / a.g.Kp;
+        const int kd = (int)(e - col * a.g.Kp), ic = (int)(col % a.g.Ip), jc = (int)(col / a.g.Ip);
+        const long long es = ((long long)(jc - 2 - a.dj0) * a.dIp + (ic - 2 - a.di0)) * a.dKp + kd;
+        __stcs(a.divo + es, d3Sx3);
+        __stcs(a.divo + a.dn + es, d3Sy3);
+        __stcs(a.divo + 2 * a.dn + es, d3Sz3);
+    }
 }
 
 template <int NM, int PREC>

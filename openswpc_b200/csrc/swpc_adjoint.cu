@@ -1380,10 +1380,13 @@ static int tail_segments(int nt, int ckpt, int nseg, long long budget, size_t st
 }
 
 // Kept step it of the trailing segments: the three divergences after step it
-// in the slot layout, then V of the shell (or of the slot box).
-static int save_kept(swpc_ctx *c, float *dst) {
+// in the slot layout (unless the velocity update stored them, div_done), then
+// V of the shell (or of the slot box).
+static int save_kept(swpc_ctx *c, float *dst, bool div_done) {
     swpc_adj_state *s = c->adj;
     const SlotGeo sg = slot_geo(c);
+    if (div_done) goto vpart;
+    {
     SlotDivArgs a;
     a.g = c->g; a.ibk = c->ibk; a.iek = c->iek; a.jbk = c->jbk; a.jek = c->jek; a.kek = c->kek;
     for (int q = 0; q < 6; q++) a.S[q] = c->S[q];
@@ -1394,6 +1397,8 @@ static int save_kept(swpc_ctx *c, float *dst) {
     const dim3 block(kThreadsK, 2, 2);
     slot_div_kernel<<<cell_grid(c->g, block), block, 0, c->stream>>>(a);
     ACK(cudaGetLastError());
+    }
+vpart:
     if (keeps_shell(c))
         shell_save_kernel<<<148 * 4, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], s->shell, s->nshell,
                                                           dst + 3 * sg.n);
@@ -1478,9 +1483,20 @@ extern "C" int swpc_gradient(swpc_ctx *c, const float *obs, int ckpt, double *mi
         }
         slot_v_kernel<<<148 * 8, 256, 0, c->stream>>>(c->g, sg, c->V[0], c->V[1], c->V[2], kept_first(g));
         rc = cuda_check(c, cudaGetLastError(), "slot_v_kernel");
+        // the staged and the one-cell velocity kernels store the divergences as they update V (their own
+        // values, so the same bits as slot_div_kernel); the other variants leave them to slot_div_kernel
+        const bool in_vel = !c->vel_march && !c->vel_vec;
         for (int it = it0; it < it0 + len && !rc; it++) {
-            rc = swpc_run(c, it, 1);
-            if (!rc) rc = save_kept(c, kept_step(it));
+            if (in_vel) {
+                c->div_out = kept_step(it);
+                c->div_geo[0] = sg.Kp; c->div_geo[1] = sg.Ip; c->div_geo[2] = sg.i0; c->div_geo[3] = sg.j0;
+                c->div_n = sg.n;
+                rc = swpc_step(c, it);
+                c->div_out = nullptr;
+            } else {
+                rc = swpc_run(c, it, 1);
+            }
+            if (!rc) rc = save_kept(c, kept_step(it), in_vel);
         }
     }
     if (rc) return rc;

@@ -1165,6 +1165,9 @@ static int launch_vel_kernel(swpc_ctx *c, int mask) {
     memcpy(a.e40, c->e40, sizeof(a.e40)); memcpy(a.e41, c->e41, sizeof(a.e41)); memcpy(a.r20, c->r20, sizeof(a.r20));
     a.dt = c->d.dt;
     a.mask = (c->d.na > 0 && c->abc == 0) ? mask : (mask & 1);
+    a.divo = c->div_out;
+    a.dKp = c->div_geo[0]; a.dIp = c->div_geo[1]; a.di0 = c->div_geo[2]; a.dj0 = c->div_geo[3];
+    a.dn = c->div_n;
     dim3 block(32, c->vbi, c->vbj);
     dim3 grid((c->g.nz + 31) / 32, (c->g.nx + c->vbi - 1) / c->vbi, (c->g.ny + c->vbj - 1) / c->vbj);
     a.scale = c->d_scale;

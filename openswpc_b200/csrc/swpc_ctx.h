@@ -190,6 +190,9 @@ struct swpc_ctx {
     int stress_tbi = 4, stress_tbj = 4, vel_tbi = 4, vel_tbj = 4;
     bool adj_tma = true;          // staged stress-phase adjoint weights (swpc_adjoint.cu)
     bool adj_fuse = true;         // velocity-phase adjoint weights formed by the stress-phase gather before
+    float *div_out = nullptr;     // the gradient's kept step: the velocity update stores the stress divergences here
+    int div_geo[4] = {0, 0, 0, 0};   // its layout: Kp, Ip, i0, j0 (Vel3Args divo)
+    long long div_n = 0;
     int tile_jblock = 0;          // j tiles per block of the staged launch order (0: by size, see tma_tiles)
     void *tmaps = nullptr;        // swpc::TmaMaps
     int tma_key[4] = {-1, -1, -1, -1};

@@ -44,6 +44,11 @@ struct Vel3Args {
     float dt;
     int mask;       // bit 0: interior cells, bit 1: absorber cells
     const float *scale;   // FP16 scales in device memory (see sc_sS)
+    // where not null, the interior cells also store their stress divergences (the gradient's kept steps): field c
+    // of cell (k, i, j) at divo[c * dn + ((j - dj0) * dIp + (i - di0)) * dKp + k - 1 + KH]
+    float *divo;
+    int dKp, dIp, di0, dj0;
+    long long dn;
 };
 
 struct Str3Args {
